@@ -1,0 +1,326 @@
+"""ORACLE -- test infrastructure only.
+
+FP64 CPU restatement of the reference's per-k-point H/O setup and IBS force,
+used as the checker by the tests, by the smoke check and by the benchmark's
+CPU-baseline leg.  Never imported by the library itself.
+
+* ``match``                    -- src/match.f90:83-191 (C: oracle_lapw.c)
+* ``hamiltonsetup``            -- src/src_eigensystem/hamiltonsetup.f90:53-176
+* ``overlapsetup``             -- src/src_eigensystem/overlapsetup.f90:47-166
+* ``hamiltonandoverlapsetup``  -- both of the above, then copy_UL, on zeroed
+                                  matrices as ``newsystem`` leaves them
+                                  (src/src_eigensystem/modfvsystem.f90:48-101)
+* ``forcek``                   -- src/forcek.f90:83-390 (no second variation:
+                                  ``tevecsv`` false, spin-unpolarised)
+
+The zgemm calls go to numpy (OpenBLAS); the scalar loops are in C.
+Parity against the reference itself is not pinned for H, O or the IBS force
+(no Fortran compiler exists here and the reference ships no H/O dump); the
+pieces that do have reference data (G-vector counts, per-k matrix sizes) and
+the special functions (checked against scipy) are pinned in the tests.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build():
+    """Compile oracle/liboracle.so (make in this directory)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        i, d = ctypes.c_int, ctypes.c_double
+        L.orc_sbessel.argtypes = [i, d, P]
+        L.orc_sbessel.restype = i
+        L.orc_sbesseldm.argtypes = [i, i, d, P]
+        L.orc_sbesseldm.restype = i
+        L.orc_genylm.argtypes = [i, P, P]
+        L.orc_genylm.restype = i
+        L.orc_polynom.argtypes = [i, i, P, P, P, d]
+        L.orc_polynom.restype = d
+        L.orc_match.argtypes = [i, i, P, P, P, i, P, i, i, P, P, d, i, P, P, P]
+        L.orc_match.restype = i
+        L.orc_hmlistln_olpistln.argtypes = [i, P, P, i, P, P, P, i, P, P, P, P, i, P, P]
+        L.orc_hmlistln_olpistln.restype = None
+        L.orc_copy_ul.argtypes = [i, i, P]
+        L.orc_copy_ul.restype = None
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f(a, dtype):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+# ---------------------------------------------------------------- special functions
+def sbessel(lmax, x):
+    out = np.zeros(lmax + 1)
+    if lib().orc_sbessel(lmax, float(x), _p(out)) != 0:
+        raise ValueError("sbessel: argument out of range")
+    return out
+
+
+def sbesseldm(m, lmax, x):
+    out = np.zeros(lmax + 1)
+    if lib().orc_sbesseldm(m, lmax, float(x), _p(out)) != 0:
+        raise ValueError("sbesseldm: argument out of range")
+    return out
+
+
+def genylm(lmax, tp):
+    out = np.zeros((lmax + 1) ** 2, dtype=np.complex128)
+    tp = np.asarray(tp, dtype=np.float64)
+    if lib().orc_genylm(lmax, _p(tp), _p(out)) != 0:
+        raise ValueError("genylm: lmax out of range")
+    return out
+
+
+def polynom(m, xa, ya, x):
+    xa = np.asarray(xa, dtype=np.float64)
+    ya = np.asarray(ya, dtype=np.float64)
+    c = np.zeros(len(xa))
+    return lib().orc_polynom(m, len(xa), _p(xa), _p(ya), _p(c), float(x))
+
+
+# ---------------------------------------------------------------- match
+def match(sys, gk, ngkmax=None):
+    """apwalm(ngkmax, apwordmax, lmmaxapw, natmtot) for one G+k set."""
+    from exciting_b200.crystal import gensfacgp
+    b = sys.basis
+    ngkmax = ngkmax or gk.ngp
+    gpc = np.zeros(ngkmax); gpc[: gk.ngp] = gk.gpc
+    tpgpc = np.zeros((2, ngkmax), order="F"); tpgpc[:, : gk.ngp] = gk.tpgpc
+    sf = np.zeros((ngkmax, sys.natmtot), dtype=np.complex128, order="F")
+    sf[: gk.ngp] = gensfacgp(gk.vgpc, sys.crystal.atposc)
+    apword = _f(np.array(b.apword).T, np.int32)       # (lmaxapw+1, nspecies)
+    species = np.asarray(b.atom_species, dtype=np.int32)
+    apwalm = np.zeros((ngkmax, b.apwordmax, b.lmmaxapw, sys.natmtot), dtype=np.complex128, order="F")
+    nsing = lib().orc_match(gk.ngp, ngkmax, _p(gpc), _p(tpgpc), _p(sf), sys.natmtot, _p(species),
+                            b.lmaxapw, b.apwordmax, _p(apword), _p(_f(sys.rmt, np.float64)),
+                            sys.crystal.omega, sys.np_tail, _p(_f(sys.spr_tail, np.float64)),
+                            _p(_f(sys.apwfr_tail, np.float64)), _p(apwalm))
+    return apwalm, nsing
+
+
+def _apwi(sys, apwalm, ngp, ias):
+    """apwi(maxaa, ngp): rows (l, m, io), l <= lmaxmat (hamiltonsetup.f90:59-71)."""
+    b = sys.basis
+    is_ = b.atom_species[ias]
+    apwi = np.zeros((b.maxaa, ngp), dtype=np.complex128)
+    f = 0
+    for l in range(b.lmaxmat + 1):
+        for m in range(-l, l + 1):
+            lm = l * (l + 1) + m
+            for io in range(b.apword[is_][l]):
+                apwi[f] = apwalm[:ngp, io, lm, ias]
+                f += 1
+    return apwi
+
+
+def _lo_range(sys, ngp, ias):
+    b = sys.basis
+    is_ = b.atom_species[ias]
+    off = b.lo_offset(ias)
+    return ngp + off, ngp + off + b.losize[is_]
+
+
+# ---------------------------------------------------------------- hamiltonsetup
+def hamiltonsetup(sys, gk, apwalm, h):
+    """H += MT (APW-APW, APW-lo, lo-lo) + interstitial upper triangle."""
+    b = sys.basis
+    ngp = gk.ngp
+    for ias in range(sys.natmtot):
+        is_ = b.atom_species[ias]
+        apwi = _apwi(sys, apwalm, ngp, ias)
+        zm = sys.mt_aa[:, :, ias] @ apwi                       # hamiltonsetup.f90:75-88
+        h[:ngp, :ngp] += apwi.conj().T @ zm                    # :90-103
+        if b.lorbl[is_]:
+            j1, j3 = _lo_range(sys, ngp, ias)
+            n = j3 - j1
+            h[j1:j3, :ngp] += sys.mt_loa[:n, :, ias] @ apwi     # :131-145
+            h[:ngp, j1:j3] = np.conj(h[j1:j3, :ngp]).T          # :147-149
+            h[j1:j3, j1:j3] += sys.mt_lolo[:n, :n, ias]         # :154-161
+    _interstitial(sys, gk, h, None)                            # hmlistln
+
+
+# ---------------------------------------------------------------- overlapsetup
+def overlapsetup(sys, gk, apwalm, o):
+    """O += MT (APW-APW with the optional h1aa, APW-lo, lo-lo) + interstitial."""
+    b = sys.basis
+    ngp = gk.ngp
+    for ias in range(sys.natmtot):
+        is_ = b.atom_species[ias]
+        apwi = _apwi(sys, apwalm, ngp, ias)
+        apwi2 = apwi.conj().T                                   # (ngp, maxaa), conj
+        zm = np.zeros((ngp, b.maxaa), dtype=np.complex128)      # overlapsetup.f90:72-87
+        f = 0
+        for l in range(b.lmaxmat + 1):
+            for m in range(-l, l + 1):
+                n_io = b.apword[is_][l]
+                for io2 in range(n_io):
+                    if sys.h1aa is not None:
+                        for io1 in range(n_io):
+                            zm[:, f + io2] += sys.h1aa[io1, io2, l, ias] * apwi2[:, f + io1]
+                    zm[:, f + io2] += apwi2[:, f + io2]
+                f += n_io
+        o[:ngp, :ngp] += apwi.conj().T @ zm.conj().T            # zgemm('C','C') :88-101
+        if b.lorbl[is_]:
+            for ilo, l in enumerate(b.lorbl[is_]):              # :111-127
+                lm1, lm2 = l * (l + 1) - l, l * (l + 1) + l
+                j1 = ngp + int(b.idxlo[lm1, ilo, ias]) - 1
+                j2 = ngp + int(b.idxlo[lm2, ilo, ias]) - 1
+                for io in range(b.apword[is_][l]):
+                    w = sys.oalo[io, ilo, ias] + (0.0 if sys.h1loa is None else sys.h1loa[io, ilo, ias])
+                    o[:ngp, j1:j2 + 1] += np.conj(apwalm[:ngp, io, lm1:lm2 + 1, ias] * w)
+                o[j1:j2 + 1, :ngp] = np.conj(o[:ngp, j1:j2 + 1]).T
+            for ilo1, l in enumerate(b.lorbl[is_]):              # :131-146
+                for ilo2, l2 in enumerate(b.lorbl[is_]):
+                    if l2 != l:
+                        continue
+                    lm1 = l * (l + 1) - l
+                    j1 = ngp + int(b.idxlo[lm1, ilo1, ias]) - 1
+                    j2 = ngp + int(b.idxlo[lm1, ilo2, ias]) - 1
+                    w = sys.ololo[ilo1, ilo2, ias] + (0.0 if sys.h1lolo is None else sys.h1lolo[ilo1, ilo2, ias])
+                    for mm in range(2 * l + 1):
+                        o[j1 + mm, j2 + mm] += w
+    _interstitial(sys, gk, None, o)                            # olpistln
+
+
+def _interstitial(sys, gk, h, o):
+    gv = sys.gv
+    ld = (h if h is not None else o).shape[0]
+    ivg = _f(gv.ivg, np.int32)
+    ivgig = np.asfortranarray(gv.ivgig, dtype=np.int32)
+    intgv = _f(gv.intgv, np.int32)
+    vgpc = _f(gk.vgpc, np.float64)
+    igpig = _f(gk.igpig, np.int32)
+    kinw = _f(sys.kinetic_weight, np.complex128)
+    m2 = None if sys.m2effig is None else _f(sys.m2effig, np.complex128)
+    lib().orc_hmlistln_olpistln(gk.ngp, _p(igpig), _p(vgpc), ld, _p(ivg), _p(ivgig), _p(intgv),
+                                gv.ngvec, _p(sys.veffig), _p(kinw), _p(sys.cfunig), _p(m2),
+                                int(sys.h1on), _p(h), _p(o))
+
+
+def hamiltonandoverlapsetup(sys, gk, apwalm=None):
+    """Full Hermitian H and O (nmat x nmat, Fortran order) for one k-point."""
+    if apwalm is None:
+        apwalm, _ = match(sys, gk)
+    nmat = sys.nmat(gk)
+    h = np.zeros((nmat, nmat), dtype=np.complex128, order="F")
+    o = np.zeros((nmat, nmat), dtype=np.complex128, order="F")
+    hamiltonsetup(sys, gk, apwalm, h)
+    overlapsetup(sys, gk, apwalm, o)
+    lib().orc_copy_ul(nmat, nmat, _p(h))                       # hamiltonoverlapocopy_UL
+    lib().orc_copy_ul(nmat, nmat, _p(o))
+    return h, o
+
+
+# ---------------------------------------------------------------- forcek (IBS)
+def forcek(sys, gk, evecfv, evalfv, occsv, wkpt, apwalm=None):
+    """IBS force contribution of one k-point, forceibs(3, natmtot) (src/forcek.f90).
+
+    ``evecfv`` (nmat, nstfv), ``evalfv`` (nstfv), ``occsv`` (nstfv).
+    """
+    from exciting_b200.crystal import ffacg_species
+    b = sys.basis
+    gv = sys.gv
+    ngp = gk.ngp
+    nmat = sys.nmat(gk)
+    if apwalm is None:
+        apwalm, _ = match(sys, gk)
+    evecfv = np.asarray(evecfv)[:nmat]
+    evecfv2 = evecfv * np.asarray(evalfv)[None, :]             # forcek.f90:76-80
+    # ijgij with the modulo wrap into the FFT box, and dpij (forcek.f90:93-100)
+    ivg_k = gv.ivg[:, gk.igpig - 1]
+    iv = ivg_k[:, :, None] - ivg_k[:, None, :]
+    lo = gv.intgv[:, 0][:, None, None]
+    ng = gv.ngrid[:, None, None]
+    iv = np.mod(iv - lo, ng) + lo
+    ijgij = gv.ivgig_lookup(iv) - 1                           # 0-based
+    dpij = 0.5 * (gk.vgpc.T @ gk.vgpc)
+    ffacg = [ffacg_species(gv.gc[: gv.ngvec], r, sys.crystal.omega) for r in sys.rmt]
+    forceibs = np.zeros((3, sys.natmtot))
+    for ias in range(sys.natmtot):
+        is_ = b.atom_species[ias]
+        h = np.zeros((nmat, nmat), dtype=np.complex128)
+        o = np.zeros((nmat, nmat), dtype=np.complex128)
+        apwi = _apwi(sys, apwalm, ngp, ias)
+        h[:ngp, :ngp] += apwi.conj().T @ (sys.mt_aa[:, :, ias] @ apwi)      # :139-166
+        if b.lorbl[is_]:
+            j1, j3 = _lo_range(sys, ngp, ias)
+            n = j3 - j1
+            h[j1:j3, :ngp] += sys.mt_loa[:n, :, ias] @ apwi                  # :174-190
+            h[:ngp, j1:j3] = np.conj(h[j1:j3, :ngp]).T
+        if sys.relativity != "iora*":
+            o[:ngp, :ngp] += apwi.conj().T @ apwi                           # :196-210
+        else:
+            tmp = np.zeros((nmat, nmat), dtype=np.complex128, order="F")
+            overlapsetup_atom_aa(sys, apwalm, ngp, ias, tmp)
+            o[:ngp, :ngp] += tmp[:ngp, :ngp]
+        if b.lorbl[is_]:
+            for ilo, l in enumerate(b.lorbl[is_]):                           # :246-259
+                lm1, lm2 = l * (l + 1) - l, l * (l + 1) + l
+                j1 = ngp + int(b.idxlo[lm1, ilo, ias]) - 1
+                j2 = ngp + int(b.idxlo[lm2, ilo, ias]) - 1
+                for io in range(b.apword[is_][l]):
+                    w = sys.oalo[io, ilo, ias] + (0.0 if sys.h1loa is None else sys.h1loa[io, ilo, ias])
+                    o[:ngp, j1:j2 + 1] += np.conj(apwalm[:ngp, io, lm1:lm2 + 1, ias] * w)
+                o[j1:j2 + 1, :ngp] = np.conj(o[:ngp, j1:j2 + 1]).T
+        t = gv.vgc[:, ijgij]                                  # (3, ngp, ngp)
+        at = sys.crystal.atposc[:, ias]
+        sfac = np.exp(1j * (gv.vgc[:, ijgij].transpose(1, 2, 0) @ at))
+        zt1 = -ffacg[is_][ijgij] * np.conj(sfac)
+        for l in range(3):                                     # :262-287
+            dlh = np.zeros((nmat, nmat), dtype=np.complex128)
+            dlo = np.zeros((nmat, nmat), dtype=np.complex128)
+            t1 = t[l]
+            dlh[:ngp, :ngp] = (dpij * zt1 + h[:ngp, :ngp]) * t1 * 1j
+            dlo[:ngp, :ngp] = -(zt1 + o[:ngp, :ngp]) * t1 * 1j
+            tk = gk.vgpc[l][:, None]
+            dlh[:ngp, ngp:] = h[:ngp, ngp:] * tk * 1j
+            dlh[ngp:, :ngp] = np.conj(dlh[:ngp, ngp:]).T
+            dlo[:ngp, ngp:] = -o[:ngp, ngp:] * tk * 1j
+            dlo[ngp:, :ngp] = np.conj(dlo[:ngp, ngp:]).T
+            zm = dlh @ evecfv + dlo @ evecfv2                  # :295-322
+            ffv_diag = np.einsum("ij,ij->j", evecfv.conj(), zm)  # diag of evecfv^H zm, :323-337
+            forceibs[l, ias] += wkpt * float(np.sum(np.asarray(occsv) * ffv_diag.real))  # :373-383
+    return forceibs
+
+
+def overlapsetup_atom_aa(sys, apwalm, ngp, ias, o):
+    """APW-APW overlap of one atom with the IORA h1aa term (overlapsetup.f90:72-101)."""
+    b = sys.basis
+    is_ = b.atom_species[ias]
+    apwi = _apwi(sys, apwalm, ngp, ias)
+    apwi2 = apwi.conj().T
+    zm = np.zeros((ngp, b.maxaa), dtype=np.complex128)
+    f = 0
+    for l in range(b.lmaxmat + 1):
+        for m in range(-l, l + 1):
+            n_io = b.apword[is_][l]
+            for io2 in range(n_io):
+                if sys.h1aa is not None:
+                    for io1 in range(n_io):
+                        zm[:, f + io2] += sys.h1aa[io1, io2, l, ias] * apwi2[:, f + io1]
+                zm[:, f + io2] += apwi2[:, f + io2]
+            f += n_io
+    o[:ngp, :ngp] += apwi.conj().T @ zm.conj().T

@@ -1,0 +1,473 @@
+/*
+ * ORACLE -- test infrastructure only.  A plain-C, FP64 restatement of the
+ * reference's per-k-point LAPW H/O setup, used by the tests, by the smoke
+ * check and by the benchmark's CPU-baseline leg as the checker.  It is never
+ * part of the shipped library and nothing on the product path calls it.
+ *
+ * Each routine follows the reference Fortran named beside it (paths relative
+ * to the exciting source tree).  Arrays use the reference's column-major
+ * layout; integer tables keep the reference's 1-based values.
+ *
+ * The dense zgemm products of hamiltonsetup/overlapsetup/forcek are done in
+ * the Python half of the oracle (numpy, OpenBLAS); this file holds the special
+ * functions, the matching coefficients, the interstitial gathers and the
+ * local-orbital blocks.
+ */
+#include <complex.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <stdlib.h>
+
+typedef double complex zdouble;
+
+#define ORC_FOURPI 12.566370614359172954
+
+/* ---- src/src_lib/factnm.f90:13-88 (only what sbesseldm needs) ---------- */
+static double orc_factnm(int n, int m)
+{
+    static const double f1[24] = {1., 2., 6., 24., 120., 720., 5040., 40320., 362880.,
+        3628800., 39916800., 479001600., 6227020800., 87178291200., 1307674368000.,
+        20922789888000., 355687428096000., 6402373705728000., 121645100408832000.,
+        2432902008176640000., 51090942171709440000., 1124000727777607680000.,
+        25852016738884976640000., 620448401733239439360000.};
+    static const double f2[38] = {1., 2., 3., 8., 15., 48., 105., 384., 945., 3840.,
+        10395., 46080., 135135., 645120., 2027025., 10321920., 34459425., 185794560.,
+        654729075., 3715891200., 13749310575., 81749606400., 316234143225.,
+        1961990553600., 7905853580625., 51011754393600., 213458046676875.,
+        1428329123020800., 6190283353629375., 42849873690624000.,
+        191898783962510625., 1371195958099968000., 6332659870762850625.,
+        46620662575398912000., 221643095476699771875., 1678343852714360832000.,
+        8200794532637891559375., 63777066403145711616000.};
+    if (n == 0) return 1.0;
+    if (m == 1 && n >= 1 && n <= 24) return f1[n - 1];
+    if (m == 2 && n >= 1 && n <= 38) return f2[n - 1];
+    double r;
+    if (m == 1) {
+        r = f1[23];
+        for (int i = 25; i <= n; i++) r *= (double)i;
+    } else {
+        int j = n / m;
+        if (n % m == 0) j--;
+        r = (double)n;
+        for (int i = 1; i <= j; i++) r *= (double)(n - i * m);
+    }
+    return r;
+}
+
+/* ---- src/src_lib/factr.f90 ------------------------------------------- */
+static double orc_factr(int n, int d)
+{
+    double r;
+    if (n < d) {
+        r = 1.0 / (double)(n + 1);
+        for (int i = n + 2; i <= d; i++) r /= (double)i;
+    } else if (n == d) {
+        r = 1.0;
+    } else {
+        r = (double)(d + 1);
+        for (int i = d + 2; i <= n; i++) r *= (double)i;
+    }
+    return r;
+}
+
+/* ---- src/src_lib/sbessel.f90:48-147 ------------------------------------
+ * j_l(x) for l = 0..lmax: series for x < 1e-8, Miller downward recursion from
+ * lmax+25 with rescaling for x < lmax, upward recursion otherwise.
+ * Returns 0, or -1 for an argument outside the reference's accepted range. */
+int orc_sbessel(int lmax, double x, double *jl)
+{
+    const int lst = 25;
+    const double rsc = 1e150, rsci = 1.0 / 1e150;
+    if (lmax < 0 || lmax > 50) return -1;
+    if (x < 0.0 || x > 1e5) return -1;
+    if (x < 1e-8) {
+        jl[0] = 1.0;
+        double t1 = 1.0, t2 = 1.0;
+        for (int l = 1; l <= lmax; l++) {
+            t1 = t1 / (double)(2 * l + 1);
+            t2 = t2 * x;
+            jl[l] = t2 * t1;
+        }
+        return 0;
+    }
+    double xi = 1.0 / x;
+    if (x < (double)lmax) {
+        double j0 = 0.6370354636449841609 * rsci;
+        double j1 = 0.3532702964695481204 * rsci;
+        double jt;
+        for (int l = lmax + lst; l >= lmax + 1; l--) {
+            jt = j0 * (double)(2 * l + 1) * xi - j1;
+            j1 = j0;
+            j0 = jt;
+            if (fabs(j0) > rsc) {
+                jt *= rsci; j1 *= rsci; j0 *= rsci;
+            }
+        }
+        for (int l = lmax; l >= 0; l--) {
+            jt = j0 * (double)(2 * l + 1) * xi - j1;
+            j1 = j0;
+            j0 = jt;
+            if (fabs(j0) > rsc) {
+                jt *= rsci; j1 *= rsci; j0 *= rsci;
+                for (int k = l + 1; k <= lmax; k++) jl[k] *= rsci;
+            }
+            jl[l] = j1;
+        }
+        double t1 = 1.0 / ((jl[0] - x * jl[1]) * cos(x) + x * jl[0] * sin(x));
+        for (int l = 0; l <= lmax; l++) jl[l] = t1 * jl[l];
+        return 0;
+    }
+    jl[0] = sin(x) * xi;
+    if (lmax == 0) return 0;
+    jl[1] = (jl[0] - cos(x)) * xi;
+    if (lmax == 1) return 0;
+    double j0 = jl[0], j1 = jl[1], jt;
+    for (int l = 2; l <= lmax; l++) {
+        jt = (double)(2 * l - 1) * j1 * xi - j0;
+        j0 = j1;
+        j1 = jt;
+        jl[l] = j1;
+    }
+    return 0;
+}
+
+/* ---- src/src_lib/sbesseldm.f90:40-130 ----------------------------------
+ * m-th derivative of j_l(x), l = 0..lmax (m <= 6, lmax <= 30). */
+int orc_sbesseldm(int m, int lmax, double x, double *djl)
+{
+    const int maxm = 6, maxns = 20;
+    if (m < 0 || m > maxm) return -1;
+    if (lmax < 0 || lmax > 30) return -1;
+    if (x < 0.0 || x > 1e5) return -1;
+    if (m == 0) return orc_sbessel(lmax, x, djl);
+    if (x > 1.0) {
+        double jl[32];
+        int a[8], a1[8], b[8], b1[8];
+        orc_sbessel(lmax + 1, x, jl);
+        for (int l = 0; l <= lmax; l++) {
+            for (int i = 1; i <= m + 1; i++) a[i] = 0;
+            a[0] = 1;
+            for (int i = 0; i <= m + 1; i++) a1[i] = 0;
+            for (int i = 1; i <= m; i++) {
+                b[0] = 0;
+                b1[0] = 0;
+                for (int j = 0; j <= i; j++) {
+                    b[j + 1] = a[j] * (l - j);
+                    b1[j + 1] = -a1[j] * (j + l + 2);
+                }
+                for (int j = 0; j <= i; j++) {
+                    b1[j] = b1[j] - a[j];
+                    b[j] = b[j] + a1[j];
+                }
+                for (int j = 0; j <= i + 1; j++) { a[j] = b[j]; a1[j] = b1[j]; }
+            }
+            double t1 = 1.0;
+            double sum = (double)a[0] * jl[l] + (double)a1[0] * jl[l + 1];
+            for (int i = 1; i <= m + 1; i++) {
+                t1 = t1 * x;
+                sum = sum + ((double)a[i] * jl[l] + (double)a1[i] * jl[l + 1]) / t1;
+            }
+            djl[l] = sum;
+        }
+    } else {
+        double x2 = x * x;
+        for (int l = 0; l <= lmax; l++) {
+            int i0 = (m - l + 1) / 2;
+            if (i0 < 0) i0 = 0;
+            /* Fortran integer division truncates toward zero, as C's does */
+            int j = 2 * i0 + l - m;
+            double t1 = (j == 0) ? 1.0 : pow(x, (double)j);
+            double p2 = 1.0;
+            for (int k = 0; k < i0; k++) p2 *= -2.0;
+            t1 = orc_factr(j + m, j) * t1 / (orc_factnm(i0, 1) * orc_factnm(j + l + m + 1, 2) * p2);
+            double sum = t1;
+            for (int i = i0 + 1; i <= maxns; i++) {
+                j = 2 * i + l;
+                t1 = -t1 * (double)((j - 1) * j) * x2
+                     / (double)((j - l) * (j - m - 1) * (j - m) * (j + l + 1));
+                if (fabs(t1) <= 1e-40) break;
+                sum = sum + t1;
+            }
+            djl[l] = sum;
+        }
+    }
+    return 0;
+}
+
+/* ---- src/src_lib/genylm.f90:36-93 --------------------------------------
+ * Complex Y_lm with the Condon-Shortley phase, packed lm = l(l+1)+m (0-based),
+ * Masters & Richards-Dinger recursion. */
+int orc_genylm(int lmax, const double *tp, zdouble *ylm)
+{
+    if (lmax < 0 || lmax > 50) return -1;
+    double x[51];
+    zdouble z[51];
+    ylm[0] = 0.28209479177387814347;
+    if (lmax == 0) return 0;
+    double sn = sin(tp[0]), cs = cos(tp[0]);
+    for (int m = 1; m <= lmax; m++) {
+        double t1 = (double)m * tp[1];
+        z[m] = cos(t1) + I * sin(t1);
+    }
+    for (int l = 1; l <= lmax; l++) {
+        x[l] = (l % 2 == 0) ? 1.0 : -1.0;
+        double dx = 0.0;
+        for (int m = l; m >= 1; m--) {
+            double t1 = sqrt((double)((l + m) * (l - m + 1)));
+            x[m - 1] = -(sn * dx + (double)(2 * m) * cs * x[m]) / t1;
+            dx = sn * x[m] * t1;
+        }
+        double t1 = sn, sum = 0.0;
+        for (int m = 1; m <= l; m++) {
+            x[m] = t1 * x[m];
+            sum = sum + x[m] * x[m];
+            t1 = t1 * sn;
+        }
+        sum = 2.0 * sum + x[0] * x[0];
+        t1 = sqrt((double)(2 * l + 1) / (ORC_FOURPI * sum));
+        int lm1 = l * (l + 1), lm2 = lm1;
+        ylm[lm1] = t1 * x[0];
+        for (int m = 1; m <= l; m++) {
+            lm1++;
+            lm2--;
+            ylm[lm1] = t1 * x[m] * z[m];
+            ylm[lm2] = conj(ylm[lm1]);
+            if (m % 2 != 0) ylm[lm2] = -ylm[lm2];
+        }
+    }
+    return 0;
+}
+
+/* ---- src/src_lib/polynom.f90:11-196 ------------------------------------
+ * m-th derivative at x of the polynomial through np points (m >= 0 only;
+ * the integral branch m < 0 is not used on this path). */
+double orc_polynom(int m, int np, const double *xa, const double *ya, double *c, double x)
+{
+    double x0, x1, x2, x3, y1, y2, y3, t1, t2, t3, t4, t5, t6, t7, sum;
+    switch (np) {
+    case 1:
+        return (m == 0) ? ya[0] : 0.0;
+    case 2:
+        c[1] = (ya[1] - ya[0]) / (xa[1] - xa[0]);
+        t1 = x - xa[0];
+        if (m == 0) return c[1] * t1 + ya[0];
+        if (m == 1) return c[1];
+        return 0.0;
+    case 3:
+        x1 = xa[1] - xa[0]; x2 = xa[2] - xa[0];
+        y1 = ya[1] - ya[0]; y2 = ya[2] - ya[0];
+        t1 = 1.0 / (x1 * x2 * (x2 - x1));
+        t2 = x1 * y2; t3 = x2 * y1;
+        c[1] = t1 * (x2 * t3 - x1 * t2);
+        c[2] = t1 * (t2 - t3);
+        t1 = x - xa[0];
+        if (m == 0) return ya[0] + t1 * (c[1] + c[2] * t1);
+        if (m == 1) return 2.0 * c[2] * t1 + c[1];
+        if (m == 2) return 2.0 * c[2];
+        return 0.0;
+    case 4:
+        x1 = xa[1] - xa[0]; x2 = xa[2] - xa[0]; x3 = xa[3] - xa[0];
+        y1 = ya[1] - ya[0]; y2 = ya[2] - ya[0]; y3 = ya[3] - ya[0];
+        t1 = 1.0 / (x1 * x2 * x3 * (x1 - x2) * (x1 - x3) * (x2 - x3));
+        t2 = x1 * x2 * y3; t3 = x2 * x3 * y1; t4 = x3 * x1 * y2;
+        t5 = x1 * x1; t6 = x2 * x2; t7 = x3 * x3;
+        c[1] = t1 * (t3 * (x3 * t6 - x2 * t7) + t4 * (x1 * t7 - x3 * t5) + t2 * (x2 * t5 - x1 * t6));
+        c[2] = t1 * (t3 * (t7 - t6) + t4 * (t5 - t7) + t2 * (t6 - t5));
+        c[3] = t1 * (t3 * (x2 - x3) + t4 * (x3 - x1) + t2 * (x1 - x2));
+        t1 = x - xa[0];
+        if (m == 0) return ya[0] + t1 * (c[1] + t1 * (c[2] + c[3] * t1));
+        if (m == 1) return c[1] + t1 * (2.0 * c[2] + 3.0 * c[3] * t1);
+        if (m == 2) return 6.0 * c[3] * t1 + 2.0 * c[2];
+        if (m == 3) return 6.0 * c[3];
+        return 0.0;
+    default:
+        break;
+    }
+    if (np <= 0 || m >= np) return 0.0;
+    for (int i = 0; i < np; i++) c[i] = ya[i];
+    for (int i = 2; i <= np; i++)
+        for (int j = np; j >= i; j--)
+            c[j - 1] = (c[j - 1] - c[j - 2]) / (xa[j - 1] - xa[j - i]);
+    if (m == 0) {
+        sum = c[0];
+        t1 = 1.0;
+        for (int i = 2; i <= np; i++) {
+            t1 = t1 * (x - xa[i - 2]);
+            sum = sum + c[i - 1] * t1;
+        }
+        return sum;
+    }
+    x0 = xa[0];
+    for (int j = 1; j <= np - 1; j++)
+        for (int i = 1; i <= np - j; i++) {
+            int k = np - i;
+            c[k - 1] = c[k - 1] + (x0 - xa[k - j]) * c[k];
+        }
+    for (int j = 1; j <= m; j++)
+        for (int i = m + 1; i <= np; i++) c[i - 1] = c[i - 1] * (double)(i - j);
+    t1 = c[np - 1];
+    t2 = x - x0;
+    for (int i = np - 1; i >= m + 1; i--) t1 = t1 * t2 + c[i - 1];
+    return t1;
+}
+
+/* ---- small dense solve, the steps of LAPACK zgesv for n <= 4 -------------
+ * D (n x n, real-valued as the reference's zd) is factored with partial
+ * pivoting (largest |d|), the sub-diagonal scaled by the reciprocal of the
+ * pivot, then each right-hand side is permuted, forward- and back-substituted
+ * (division by the U diagonal).  Returns 0, or k > 0 if U(k,k) is exactly 0,
+ * in which case the right-hand sides are left untouched (zgesv's contract). */
+int orc_lu_factor(int n, double *d /* n*n col-major, overwritten */, int *ipiv)
+{
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double best = fabs(d[k + k * n]);
+        for (int i = k + 1; i < n; i++)
+            if (fabs(d[i + k * n]) > best) { best = fabs(d[i + k * n]); p = i; }
+        ipiv[k] = p;
+        if (d[p + k * n] == 0.0) return k + 1;
+        if (p != k)
+            for (int j = 0; j < n; j++) {
+                double t = d[k + j * n]; d[k + j * n] = d[p + j * n]; d[p + j * n] = t;
+            }
+        double r = 1.0 / d[k + k * n];
+        for (int i = k + 1; i < n; i++) d[i + k * n] *= r;
+        for (int j = k + 1; j < n; j++)
+            for (int i = k + 1; i < n; i++) d[i + j * n] -= d[i + k * n] * d[k + j * n];
+    }
+    return 0;
+}
+
+void orc_lu_solve(int n, const double *d, const int *ipiv, zdouble *b)
+{
+    for (int k = 0; k < n; k++)
+        if (ipiv[k] != k) { zdouble t = b[k]; b[k] = b[ipiv[k]]; b[ipiv[k]] = t; }
+    for (int k = 0; k < n; k++)
+        for (int i = k + 1; i < n; i++) b[i] -= b[k] * d[i + k * n];
+    for (int k = n - 1; k >= 0; k--) {
+        b[k] = b[k] / d[k + k * n];
+        for (int i = 0; i < k; i++) b[i] -= b[k] * d[i + k * n];
+    }
+}
+
+/* ---- src/match.f90:83-191 ---------------------------------------------
+ * apwalm(ngkmax, apwordmax, lmmaxapw, natmtot).  The last np radial points of
+ * the mesh and of the radial functions are passed as tails:
+ *   spr_tail(np, nspecies), apwfr_tail(np, apwordmax, 0:lmaxapw, natmtot).
+ * Returns the number of (atom, l) pairs whose matching system was singular
+ * (the reference prints those and carries on, match.f90:166-175). */
+int orc_match(int ngp, int ngkmax, const double *gpc, const double *tpgpc, const zdouble *sfacgp,
+              int natmtot, const int *atom_species, int lmaxapw, int apwordmax,
+              const int *apword /* (lmaxapw+1, nspecies) */, const double *rmt, double omega,
+              int np, const double *spr_tail, const double *apwfr_tail, zdouble *apwalm)
+{
+    const int lmmaxapw = (lmaxapw + 1) * (lmaxapw + 1);
+    const double fpso = ORC_FOURPI / sqrt(omega);
+    int nsing = 0;
+    zdouble *ylmgp = (zdouble *)malloc(sizeof(zdouble) * lmmaxapw * (ngp > 0 ? ngp : 1));
+    double *djl = (double *)malloc(sizeof(double) * (lmaxapw + 1) * apwordmax * (ngp > 0 ? ngp : 1));
+    /* spherical harmonics of the G+p vectors (match.f90:93-101) */
+#pragma omp parallel for schedule(static)
+    for (int igp = 0; igp < ngp; igp++) orc_genylm(lmaxapw, tpgpc + 2 * igp, ylmgp + (size_t)lmmaxapw * igp);
+    int last_is = -1;
+    for (int ias = 0; ias < natmtot; ias++) {
+        const int is = atom_species[ias];
+        const int *apw = apword + (size_t)(lmaxapw + 1) * is;
+        if (is != last_is) {
+            /* Bessel derivatives for this species (match.f90:104-126) */
+            int omax = 0;
+            for (int l = 0; l <= lmaxapw; l++) if (apw[l] > omax) omax = apw[l];
+#pragma omp parallel for schedule(static)
+            for (int igp = 0; igp < ngp; igp++) {
+                double *dj = djl + (size_t)(lmaxapw + 1) * apwordmax * igp;
+                double t1 = gpc[igp] * rmt[is];
+                for (int io1 = 1; io1 <= omax; io1++) orc_sbesseldm(io1 - 1, lmaxapw, t1, dj + (lmaxapw + 1) * (io1 - 1));
+                t1 = 1.0;
+                for (int io1 = 2; io1 <= omax; io1++) {
+                    t1 = t1 * gpc[igp];
+                    for (int l = 0; l <= lmaxapw; l++) dj[l + (lmaxapw + 1) * (io1 - 1)] *= t1;
+                }
+            }
+            last_is = is;
+        }
+        for (int l = 0; l <= lmaxapw; l++) {
+            /* zt1 = fpso * i^l */
+            zdouble zil;
+            switch (l % 4) { case 0: zil = 1.0; break; case 1: zil = I; break; case 2: zil = -1.0; break; default: zil = -I; }
+            zdouble zt1 = fpso * zil;
+            const int n = apw[l];
+            double dmat[16];
+            int ipiv[4];
+            double c[8];
+            const double *xa = spr_tail + (size_t)np * is;
+            for (int io2 = 0; io2 < n; io2++)
+                for (int io1 = 0; io1 < n; io1++) {
+                    const double *ya = apwfr_tail + (size_t)np * (io2 + apwordmax * (l + (lmaxapw + 1) * (size_t)ias));
+                    dmat[io1 + n * io2] = orc_polynom(io1, np, xa, ya, c, rmt[is]);
+                }
+            int info = orc_lu_factor(n, dmat, ipiv);
+            if (info != 0) nsing++;
+#pragma omp parallel for schedule(static)
+            for (int igp = 0; igp < ngp; igp++) {
+                const double *dj = djl + (size_t)(lmaxapw + 1) * apwordmax * igp;
+                zdouble zt2 = zt1 * sfacgp[igp + (size_t)ngkmax * ias];
+                for (int m = -l; m <= l; m++) {
+                    int lm = l * (l + 1) + m;
+                    zdouble b[4];
+                    zdouble cy = conj(ylmgp[lm + (size_t)lmmaxapw * igp]);
+                    for (int io1 = 0; io1 < n; io1++) b[io1] = dj[l + (lmaxapw + 1) * io1] * zt2 * cy;
+                    if (info == 0) orc_lu_solve(n, dmat, ipiv, b);
+                    for (int io1 = 0; io1 < n; io1++)
+                        apwalm[igp + (size_t)ngkmax * (io1 + (size_t)apwordmax * (lm + (size_t)lmmaxapw * ias))] = b[io1];
+                }
+            }
+        }
+    }
+    free(ylmgp);
+    free(djl);
+    return nsing;
+}
+
+/* ---- src/src_eigensystem/hmlistln.f90:61-86 and olpistln.f90:53-82 ------
+ * Interstitial H and O, added to the upper triangle za(i, j), i <= j
+ * (Hermitianmatrix_indexedupdate, modfvsystem.f90:126-143).
+ * kinw is meffig (ValenceRelativity /= "none") or cfunig ("none").
+ * With h1on (iora*), O also gets 0.5*a2*(vgpc_i.vgpc_j)*m2effig. */
+void orc_hmlistln_olpistln(int ngp, const int *igpig, const double *vgpc, int ld,
+                           const int *ivg, const int *ivgig, const int *intgv /* (3,2) */, int ngvec,
+                           const zdouble *veffig, const zdouble *kinw, const zdouble *cfunig,
+                           const zdouble *m2effig, int h1on, zdouble *h, zdouble *o)
+{
+    const double alpha = 1.0 / 137.03599911, a2 = 0.5 * alpha * alpha;
+    const int n1 = intgv[3] - intgv[0] + 1, n2 = intgv[4] - intgv[1] + 1;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int j = 0; j < ngp; j++) {
+        const int gj = igpig[j] - 1;
+        for (int i = 0; i <= j; i++) {
+            const int gi = igpig[i] - 1;
+            int iv1 = ivg[3 * gi + 0] - ivg[3 * gj + 0];
+            int iv2 = ivg[3 * gi + 1] - ivg[3 * gj + 1];
+            int iv3 = ivg[3 * gi + 2] - ivg[3 * gj + 2];
+            int ig = ivgig[(iv1 - intgv[0]) + n1 * ((iv2 - intgv[1]) + n2 * (iv3 - intgv[2]))];
+            if (ig > 0 && ig <= ngvec) {
+                double dp = vgpc[3 * i] * vgpc[3 * j] + vgpc[3 * i + 1] * vgpc[3 * j + 1] + vgpc[3 * i + 2] * vgpc[3 * j + 2];
+                double t1 = 0.5 * dp;
+                if (h) h[i + (size_t)ld * j] += veffig[ig - 1] + t1 * kinw[ig - 1];
+                if (o) {
+                    if (h1on) o[i + (size_t)ld * j] += (0.5 * a2 * dp) * m2effig[ig - 1] + cfunig[ig - 1];
+                    else o[i + (size_t)ld * j] += cfunig[ig - 1];
+                }
+            }
+        }
+    }
+}
+
+/* ---- src/src_eigensystem/hamiltonoverlapocopy_UL.f90:16-28 --------------
+ * za(i+1:, i) = conj(za(i, i+1:)) */
+void orc_copy_ul(int n, int ld, zdouble *a)
+{
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n - 1; i++)
+        for (int j = i + 1; j < n; j++) a[j + (size_t)ld * i] = conj(a[i + (size_t)ld * j]);
+}
