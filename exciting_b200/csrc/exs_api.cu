@@ -1,0 +1,691 @@
+// C-ABI of libexciting_b200: context, input upload, and the entry points that
+// replace the reference's match / hamiltonandoverlapsetup calls.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "exs_internal.cuh"
+
+using exs::AtomDesc;
+using exs::DevParams;
+using exs::KDesc;
+
+namespace {
+
+int fail(exs_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->last_error = msg;
+    return code;
+}
+
+int cuda_fail(exs_ctx *c, cudaError_t e, const char *where)
+{
+    return fail(c, EXS_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define EXS_CUDA(call)                                          \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);  \
+    } while (0)
+
+template <class T>
+cudaError_t dalloc(T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) return cudaSuccess;
+    return cudaMalloc((void **)p, n * sizeof(T));
+}
+
+template <class T>
+cudaError_t upload(T **p, const T *h, size_t n, cudaStream_t s)
+{
+    cudaError_t e = dalloc(p, n);
+    if (e != cudaSuccess || n == 0) return e;
+    return cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+exs::DevParams exs_ctx::params() const
+{
+    DevParams p{};
+    p.natmtot = natmtot;
+    p.lmaxapw = lmaxapw;
+    p.lmaxmat = lmaxmat;
+    p.apwordmax = apwordmax;
+    p.lmmaxapw = (lmaxapw + 1) * (lmaxapw + 1);
+    p.np_tail = np_tail;
+    p.ngkmax = ngkmax;
+    p.npad = npad;
+    p.K = K;
+    p.Kpad = Kpad;
+    p.nlotot = nlotot;
+    p.maxnlo = maxnlo;
+    p.nlomax = nlomax;
+    p.lolmmax = lolmmax;
+    p.ngvec = ngvec;
+    p.ngrtot = ngrtot;
+    for (int i = 0; i < 3; i++) {
+        p.intgv_lo[i] = intgv[i];
+        p.intgv_n[i] = intgv[3 + i] - intgv[i] + 1;
+    }
+    p.relativity = relativity;
+    p.omega = omega;
+    p.atoms = d_atoms;
+    p.apword = d_apword;
+    p.rmt = d_rmt;
+    p.spr_tail = d_spr_tail;
+    p.apwfr_tail = d_apwfr_tail;
+    p.ivg = d_ivg;
+    p.ivgig = d_ivgig;
+    p.veffig = d_veffig;
+    p.kinw = d_kinw;
+    p.cfunig = d_cfunig;
+    p.m2effig = d_m2effig;
+    p.lolo = d_lolo;
+    p.ololo = d_ololo;
+    p.h1lolo = d_h1lolo;
+    p.oalo = d_oalo;
+    p.h1loa = d_h1loa;
+    p.h1aa = d_h1aa;
+    p.idxlo = d_idxlo;
+    p.lorbl = d_lorbl;
+    p.nlorb = d_nlorb;
+    p.err = d_err;
+    return p;
+}
+
+extern "C" {
+
+const char *exs_last_error(const exs_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int exs_ctx_sizes(const exs_ctx *c, int *maxaa, int *maxnlo, int *nlotot)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (maxaa) *maxaa = c->maxaa;
+    if (maxnlo) *maxnlo = c->maxnlo;
+    if (nlotot) *nlotot = c->nlotot;
+    return EXS_OK;
+}
+
+int exs_ctx_destroy(exs_ctx *c)
+{
+    if (!c) return EXS_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *dev[] = {c->d_atoms, c->d_apword, c->d_ivg, c->d_ivgig, c->d_idxlo, c->d_lorbl, c->d_nlorb, c->d_rmt,
+                   c->d_haa_r, c->d_haa_i, c->d_loa_r, c->d_loa_i, c->d_lolo, c->d_oalo, c->d_ololo, c->d_h1aa,
+                   c->d_h1loa, c->d_h1lolo, c->d_veffig, c->d_kinw, c->d_cfunig, c->d_m2effig, c->d_spr_tail,
+                   c->d_apwfr_tail, c->d_work, c->d_ho, c->d_igpig, c->d_vgpc, c->d_err, c->d_tables,
+                   c->d_match_in, c->d_match_sf, c->d_apwalm};
+    for (void *p : dev)
+        if (p) cudaFree(p);
+    if (c->h_tables) cudaFreeHost(c->h_tables);
+    if (c->h_igpig_pinned) cudaFreeHost(c->h_igpig_pinned);
+    if (c->h_vgpc_pinned) cudaFreeHost(c->h_vgpc_pinned);
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->tables_free) cudaEventDestroy(c->tables_free);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return EXS_OK;
+}
+
+int exs_ctx_create(const exs_config *cfg, exs_ctx **out)
+{
+    if (!out) return EXS_ERR_ARG;
+    *out = nullptr;
+    if (!cfg || !cfg->atom_species || !cfg->apword || !cfg->rmt || !cfg->atposc || !cfg->bvec || !cfg->intgv ||
+        !cfg->ivg || !cfg->ivgig)
+        return EXS_ERR_ARG;
+    if (cfg->natmtot <= 0 || cfg->nspecies <= 0 || cfg->ngkmax <= 0 || cfg->ngrtot <= 0 || cfg->ngvec <= 0 ||
+        cfg->ngvec > cfg->ngrtot || cfg->max_batch <= 0)
+        return EXS_ERR_ARG;
+    if (cfg->lmaxapw < 0 || cfg->lmaxapw > EXS_LMAX_APW || cfg->lmaxmat < 0 || cfg->lmaxmat > cfg->lmaxapw)
+        return EXS_ERR_SIZE;
+    if (cfg->apwordmax < 1 || cfg->apwordmax > EXS_APWORD_MAX) return EXS_ERR_SIZE;
+    if (cfg->np_tail != std::max(cfg->apwordmax + 1, 4)) return EXS_ERR_ARG;
+    if (cfg->relativity < EXS_REL_NONE || cfg->relativity > EXS_REL_IORA) return EXS_ERR_ARG;
+
+    exs_ctx *c = new (std::nothrow) exs_ctx();
+    if (!c) return EXS_ERR_NOMEM;
+    cudaGetDevice(&c->device);
+    c->natmtot = cfg->natmtot;
+    c->nspecies = cfg->nspecies;
+    c->lmaxapw = cfg->lmaxapw;
+    c->lmaxmat = cfg->lmaxmat;
+    c->apwordmax = cfg->apwordmax;
+    c->nlomax = std::max(cfg->nlomax, 1);
+    c->omega = cfg->omega;
+    c->ngkmax = cfg->ngkmax;
+    c->ngrtot = cfg->ngrtot;
+    c->ngvec = cfg->ngvec;
+    c->relativity = cfg->relativity;
+    c->np_tail = cfg->np_tail;
+    c->max_batch = cfg->max_batch;
+    std::memcpy(c->intgv, cfg->intgv, sizeof(c->intgv));
+    c->atom_species.assign(cfg->atom_species, cfg->atom_species + c->natmtot);
+    c->apword.assign(cfg->apword, cfg->apword + (size_t)(c->lmaxapw + 1) * c->nspecies);
+    c->nlorb.assign(c->nspecies, 0);
+    if (cfg->nlorb) c->nlorb.assign(cfg->nlorb, cfg->nlorb + c->nspecies);
+    c->lorbl.assign((size_t)c->nlomax * c->nspecies, 0);
+    if (cfg->lorbl && cfg->nlomax > 0) c->lorbl.assign(cfg->lorbl, cfg->lorbl + (size_t)cfg->nlomax * c->nspecies);
+    c->rmt.assign(cfg->rmt, cfg->rmt + c->nspecies);
+    c->atposc.assign(cfg->atposc, cfg->atposc + 3 * (size_t)c->natmtot);
+    c->bvec.assign(cfg->bvec, cfg->bvec + 9);
+
+    // ---- validation of the basis description
+    for (int ias = 0; ias < c->natmtot; ias++) {
+        const int s = c->atom_species[ias];
+        if (s < 0 || s >= c->nspecies || (ias > 0 && s < c->atom_species[ias - 1])) {
+            exs_ctx_destroy(c);
+            return EXS_ERR_ARG;  // atoms must be grouped by species (idxas order)
+        }
+    }
+    for (int is = 0; is < c->nspecies; is++) {
+        for (int l = 0; l <= c->lmaxapw; l++) {
+            const int a = c->apword[l + (size_t)(c->lmaxapw + 1) * is];
+            if (a < 1 || a > c->apwordmax) { exs_ctx_destroy(c); return EXS_ERR_ARG; }
+        }
+        if (c->nlorb[is] < 0 || c->nlorb[is] > c->nlomax) { exs_ctx_destroy(c); return EXS_ERR_ARG; }
+        for (int ilo = 0; ilo < c->nlorb[is]; ilo++) {
+            const int l = c->lorbl[ilo + (size_t)c->nlomax * is];
+            if (l < 0 || l > c->lmaxmat) { exs_ctx_destroy(c); return EXS_ERR_SIZE; }
+            c->lolmax = std::max(c->lolmax, l);
+        }
+    }
+    for (int i = 0; i < 3; i++)
+        if (c->intgv[3 + i] < c->intgv[i]) { exs_ctx_destroy(c); return EXS_ERR_ARG; }
+    const long nbox = (long)(c->intgv[3] - c->intgv[0] + 1) * (c->intgv[4] - c->intgv[1] + 1) * (c->intgv[5] - c->intgv[2] + 1);
+
+    // ---- MaxAPWs, genidxlo, MTInitAll
+    auto napw_species = [&](int is) {
+        int n = 0;
+        for (int l = 0; l <= c->lmaxmat; l++) n += (2 * l + 1) * c->apword[l + (size_t)(c->lmaxapw + 1) * is];
+        return n;
+    };
+    c->maxaa = 0;
+    for (int is = 0; is < c->nspecies; is++) c->maxaa = std::max(c->maxaa, napw_species(is));
+    c->lolmmax = (c->lolmax + 1) * (c->lolmax + 1);
+    c->idxlo.assign((size_t)c->lolmmax * c->nlomax * c->natmtot, 0);
+    int i = 0;
+    for (int is = 0; is < c->nspecies; is++)
+        for (int ias = 0; ias < c->natmtot; ias++) {
+            if (c->atom_species[ias] != is) continue;
+            for (int ilo = 0; ilo < c->nlorb[is]; ilo++) {
+                const int l = c->lorbl[ilo + (size_t)c->nlomax * is];
+                for (int m = -l; m <= l; m++) {
+                    i++;
+                    c->idxlo[(l * (l + 1) + m) + (size_t)c->lolmmax * (ilo + (size_t)c->nlomax * ias)] = i;
+                }
+            }
+        }
+    c->nlotot = i;
+    c->losize.assign(c->nspecies, 0);
+    c->maxnlo = 0;
+    for (int is = 0; is < c->nspecies; is++) {
+        int n = 0;
+        for (int ilo = 0; ilo < c->nlorb[is]; ilo++) n += 2 * c->lorbl[ilo + (size_t)c->nlomax * is] + 1;
+        c->losize[is] = n;
+        c->maxnlo = std::max(c->maxnlo, n);
+    }
+    c->atoms.resize(c->natmtot);
+    int off = 0;
+    for (int ias = 0; ias < c->natmtot; ias++) {
+        AtomDesc &a = c->atoms[ias];
+        const int is = c->atom_species[ias];
+        a.species = is;
+        a.apw_off = off;
+        a.napw = napw_species(is);
+        off += a.napw;
+        a.losize = c->losize[is];
+        if (c->nlorb[is] > 0) {
+            const int l = c->lorbl[(size_t)c->nlomax * is];
+            a.lo_off = c->idxlo[(l * (l + 1) - l) + (size_t)c->lolmmax * ((size_t)c->nlomax * ias)] - 1;
+        } else {
+            a.lo_off = -1;
+        }
+        for (int k = 0; k < 3; k++) a.pos[k] = c->atposc[3 * (size_t)ias + k];
+    }
+    c->K = off;
+    c->Kpad = round_up(c->K, 16);
+    c->npad = round_up(c->ngkmax, 64);
+    c->nmatmax = c->ngkmax + c->nlotot;
+    c->ldh = round_up(c->maxaa, 8);
+    c->ldlo = round_up(std::max(c->maxnlo, 1), 2);
+    c->nplanes = (c->relativity == EXS_REL_IORA) ? 6 : 4;
+    c->plane = (size_t)c->Kpad * c->npad;
+
+    // ---- device objects
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        exs_ctx_destroy(c);
+        return EXS_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    for (auto &ev : c->ev) cudaEventCreate(&ev);
+    cudaEventCreateWithFlags(&c->tables_free, cudaEventDisableTiming);
+    cudaStream_t s = c->stream;
+    e = upload(&c->d_atoms, c->atoms.data(), c->atoms.size(), s);
+    if (e == cudaSuccess) e = upload(&c->d_apword, c->apword.data(), c->apword.size(), s);
+    if (e == cudaSuccess) e = upload(&c->d_ivg, cfg->ivg, 3 * (size_t)c->ngrtot, s);
+    if (e == cudaSuccess) e = upload(&c->d_ivgig, cfg->ivgig, (size_t)nbox, s);
+    if (e == cudaSuccess) e = upload(&c->d_idxlo, c->idxlo.data(), c->idxlo.size(), s);
+    if (e == cudaSuccess) e = upload(&c->d_lorbl, c->lorbl.data(), c->lorbl.size(), s);
+    if (e == cudaSuccess) e = upload(&c->d_nlorb, c->nlorb.data(), c->nlorb.size(), s);
+    if (e == cudaSuccess) e = upload(&c->d_rmt, c->rmt.data(), c->rmt.size(), s);
+    if (e == cudaSuccess) e = dalloc(&c->d_err, 4);
+    if (e == cudaSuccess) e = dalloc(&c->d_work, c->plane * c->nplanes * c->max_batch);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_work, 0, c->plane * c->nplanes * c->max_batch * sizeof(double), s);
+    if (e == cudaSuccess) e = dalloc(&c->d_ho, 2 * (size_t)c->nmatmax * c->nmatmax * c->max_batch);
+    if (e == cudaSuccess) e = dalloc(&c->d_igpig, (size_t)c->ngkmax * c->max_batch);
+    if (e == cudaSuccess) e = dalloc(&c->d_vgpc, 3 * (size_t)c->ngkmax * c->max_batch);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_igpig_pinned, sizeof(int) * (size_t)c->ngkmax * c->max_batch);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_vgpc_pinned, sizeof(double) * 3 * (size_t)c->ngkmax * c->max_batch);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        int code = (e == cudaErrorMemoryAllocation) ? EXS_ERR_NOMEM : EXS_ERR_CUDA;
+        exs_ctx_destroy(c);
+        return code;
+    }
+    *out = c;
+    return EXS_OK;
+}
+
+int exs_set_precision(exs_ctx *c, int mode, int slices)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (mode == EXS_PREC_FP64) {
+        c->prec_mode = mode;
+        return EXS_OK;
+    }
+    if (mode == EXS_PREC_OZAKI_INT8) {
+        if (slices < 3 || slices > 9) return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
+        return fail(c, EXS_ERR_ARG, "the int8 split-precision contraction is not built into this library");
+    }
+    return fail(c, EXS_ERR_ARG, "unknown precision mode");
+}
+
+int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
+{
+    if (!c || !in || !in->mt_aa || !in->veffig || !in->cfunig || !in->spr_tail || !in->apwfr_tail || !in->oalo ||
+        !in->ololo)
+        return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: missing input array");
+    if (c->nlotot > 0 && (!in->mt_loa || !in->mt_lolo)) return fail(c, EXS_ERR_ARG, "missing loa/lolo");
+    if (c->relativity != EXS_REL_NONE && !in->meffig) return fail(c, EXS_ERR_ARG, "missing meffig");
+    if (c->relativity == EXS_REL_IORA && (!in->m2effig || !in->h1aa || !in->h1loa || !in->h1lolo))
+        return fail(c, EXS_ERR_ARG, "missing iora* inputs");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    EXS_CUDA(cudaStreamSynchronize(s));
+    // free the previous iteration's copies
+    void **old[] = {(void **)&c->d_haa_r, (void **)&c->d_haa_i, (void **)&c->d_loa_r, (void **)&c->d_loa_i,
+                    (void **)&c->d_lolo, (void **)&c->d_oalo, (void **)&c->d_ololo, (void **)&c->d_h1aa,
+                    (void **)&c->d_h1loa, (void **)&c->d_h1lolo, (void **)&c->d_veffig, (void **)&c->d_kinw,
+                    (void **)&c->d_cfunig, (void **)&c->d_m2effig, (void **)&c->d_spr_tail, (void **)&c->d_apwfr_tail};
+    for (void **p : old)
+        if (*p) { cudaFree(*p); *p = nullptr; }
+    c->have_inputs = false;
+    const int nat = c->natmtot, maxaa = c->maxaa, maxnlo = std::max(c->maxnlo, 1);
+    // h_a: aa(f, f', ias) -> planar [ias][f'][f] with leading dim ldh
+    {
+        std::vector<double> re((size_t)nat * c->ldh * c->ldh, 0.0), im(re.size(), 0.0);
+        for (int ias = 0; ias < nat; ias++)
+            for (int f2 = 0; f2 < maxaa; f2++)
+                for (int f1 = 0; f1 < maxaa; f1++) {
+                    const exs_complex z = in->mt_aa[f1 + (size_t)maxaa * (f2 + (size_t)maxaa * ias)];
+                    re[f1 + (size_t)c->ldh * (f2 + (size_t)c->ldh * ias)] = z.re;
+                    im[f1 + (size_t)c->ldh * (f2 + (size_t)c->ldh * ias)] = z.im;
+                }
+        EXS_CUDA(upload(&c->d_haa_r, re.data(), re.size(), s));
+        EXS_CUDA(upload(&c->d_haa_i, im.data(), im.size(), s));
+        EXS_CUDA(cudaStreamSynchronize(s));
+    }
+    // loa(r, f, ias) -> planar [ias][f][r] with leading dim ldlo
+    {
+        std::vector<double> re((size_t)nat * c->ldlo * maxaa, 0.0), im(re.size(), 0.0);
+        if (in->mt_loa)
+            for (int ias = 0; ias < nat; ias++)
+                for (int f = 0; f < maxaa; f++)
+                    for (int r = 0; r < c->maxnlo; r++) {
+                        const exs_complex z = in->mt_loa[r + (size_t)maxnlo * (f + (size_t)maxaa * ias)];
+                        re[r + (size_t)c->ldlo * (f + (size_t)maxaa * ias)] = z.re;
+                        im[r + (size_t)c->ldlo * (f + (size_t)maxaa * ias)] = z.im;
+                    }
+        EXS_CUDA(upload(&c->d_loa_r, re.data(), re.size(), s));
+        EXS_CUDA(upload(&c->d_loa_i, im.data(), im.size(), s));
+        EXS_CUDA(cudaStreamSynchronize(s));
+    }
+    std::vector<exs_complex> zero_lolo;
+    const exs_complex *lolo = in->mt_lolo;
+    if (!lolo) { zero_lolo.assign((size_t)maxnlo * maxnlo * nat, exs_complex{0, 0}); lolo = zero_lolo.data(); }
+    EXS_CUDA(upload(&c->d_lolo, lolo, (size_t)maxnlo * maxnlo * nat, s));
+    EXS_CUDA(upload(&c->d_oalo, in->oalo, (size_t)c->apwordmax * c->nlomax * nat, s));
+    EXS_CUDA(upload(&c->d_ololo, in->ololo, (size_t)c->nlomax * c->nlomax * nat, s));
+    if (c->relativity == EXS_REL_IORA) {
+        EXS_CUDA(upload(&c->d_h1aa, in->h1aa, (size_t)c->apwordmax * c->apwordmax * (c->lmaxapw + 1) * nat, s));
+        EXS_CUDA(upload(&c->d_h1loa, in->h1loa, (size_t)c->apwordmax * c->nlomax * nat, s));
+        EXS_CUDA(upload(&c->d_h1lolo, in->h1lolo, (size_t)c->nlomax * c->nlomax * nat, s));
+        EXS_CUDA(upload(&c->d_m2effig, in->m2effig, (size_t)c->ngvec, s));
+    }
+    EXS_CUDA(upload(&c->d_veffig, in->veffig, (size_t)c->ngvec, s));
+    EXS_CUDA(upload(&c->d_cfunig, in->cfunig, (size_t)c->ngvec, s));
+    EXS_CUDA(upload(&c->d_kinw, c->relativity == EXS_REL_NONE ? in->cfunig : in->meffig, (size_t)c->ngvec, s));
+    EXS_CUDA(upload(&c->d_spr_tail, in->spr_tail, (size_t)c->np_tail * c->nspecies, s));
+    EXS_CUDA(upload(&c->d_apwfr_tail, in->apwfr_tail,
+                    (size_t)c->np_tail * c->apwordmax * (c->lmaxapw + 1) * nat, s));
+    EXS_CUDA(cudaStreamSynchronize(s));
+    c->have_inputs = true;
+    return EXS_OK;
+}
+
+int exs_synchronize(exs_ctx *c)
+{
+    if (!c) return EXS_ERR_ARG;
+    cudaSetDevice(c->device);
+    EXS_CUDA(cudaStreamSynchronize(c->stream));
+    int err = 0;
+    EXS_CUDA(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 4; i++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]) == cudaSuccess) c->last_t[i] = ms;
+    }
+    float tot = 0.f;
+    if (cudaEventElapsedTime(&tot, c->ev[0], c->ev[4]) == cudaSuccess) c->last_t[4] = tot;
+    if (err & exs::DEV_ERR_INDEX)
+        return fail(c, EXS_ERR_INDEX, "a G-G' difference fell outside the ivgig box");
+    if (err & exs::DEV_WARN_SINGULAR) {
+        c->last_error = "a matching system D_l was singular (match.f90:166-175)";
+        return EXS_WARN_SINGULAR;
+    }
+    return EXS_OK;
+}
+
+int exs_set_stream(exs_ctx *c, void *stream)
+{
+    if (!c) return EXS_ERR_ARG;
+    cudaSetDevice(c->device);
+    EXS_CUDA(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return EXS_OK;
+}
+
+int exs_last_timings(exs_ctx *c, double *t, int n)
+{
+    if (!c || !t) return EXS_ERR_ARG;
+    for (int i = 0; i < n && i < 5; i++) t[i] = c->last_t[i];
+    return EXS_OK;
+}
+
+int exs_match(exs_ctx *c, int ngp, const double *gpc, const double *tpgpc, const exs_complex *sfacgp,
+              exs_complex *apwalm)
+{
+    if (!c || !gpc || !tpgpc || !sfacgp || !apwalm) return fail(c, EXS_ERR_ARG, "exs_match: null argument");
+    if (ngp < 0 || ngp > c->ngkmax) return fail(c, EXS_ERR_SIZE, "exs_match: ngp outside 0..ngkmax");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    const int lmmax = (c->lmaxapw + 1) * (c->lmaxapw + 1);
+    const size_t nalm = (size_t)c->ngkmax * c->apwordmax * lmmax * c->natmtot;
+    if (!c->d_apwalm) {
+        EXS_CUDA(dalloc(&c->d_apwalm, nalm));
+        EXS_CUDA(dalloc(&c->d_match_in, 3 * (size_t)c->ngkmax));
+        EXS_CUDA(dalloc(&c->d_match_sf, (size_t)c->ngkmax * c->natmtot));
+    }
+    if (ngp == 0) return EXS_OK;
+    EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+    EXS_CUDA(cudaMemcpyAsync(c->d_match_in, gpc, sizeof(double) * ngp, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaMemcpyAsync(c->d_match_in + c->ngkmax, tpgpc, sizeof(double) * 2 * ngp, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaMemcpy2DAsync(c->d_match_sf, sizeof(exs_complex) * c->ngkmax, sfacgp, sizeof(exs_complex) * c->ngkmax,
+                               sizeof(exs_complex) * ngp, c->natmtot, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaEventRecord(c->ev[0], s));
+    EXS_CUDA(exs::launch_match_ref(c->params(), ngp, c->ngkmax, c->d_match_in, c->d_match_in + c->ngkmax,
+                                   c->d_match_sf, c->d_apwalm, s));
+    for (int i = 1; i <= 4; i++) EXS_CUDA(cudaEventRecord(c->ev[i], s));
+    // only the first ngp rows of each column are defined by match
+    EXS_CUDA(cudaMemcpy2DAsync(apwalm, sizeof(exs_complex) * c->ngkmax, c->d_apwalm, sizeof(exs_complex) * c->ngkmax,
+                               sizeof(exs_complex) * ngp, nalm / c->ngkmax, cudaMemcpyDeviceToHost, s));
+    return exs_synchronize(c);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- setup pipeline
+namespace {
+
+// Pack the k descriptors and the grouped-GEMM tables into the pinned staging
+// buffer, upload them with one copy and return the device addresses.
+struct Uploaded {
+    const KDesc *d_k;
+    const void *d_probs[4];
+    const void *d_work[4];
+    int nwork[4];
+};
+
+int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
+{
+    exs::build_gemm_tables(c, ks, c->gt);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t need = al(ks.size() * sizeof(KDesc));
+    for (int q = 0; q < 4; q++)
+        need += al(c->gt.probs[q].size() * sizeof(exs::GemmProb)) + al(c->gt.work[q].size() * sizeof(exs::TileWork));
+    // the previous upload must have left the staging buffer
+    EXS_CUDA(cudaEventSynchronize(c->tables_free));
+    if (need > c->tables_bytes) {
+        if (c->h_tables) cudaFreeHost(c->h_tables);
+        if (c->d_tables) cudaFree(c->d_tables);
+        c->h_tables = c->d_tables = nullptr;
+        c->tables_bytes = 0;
+        const size_t cap = need * 2;
+        EXS_CUDA(cudaMallocHost(&c->h_tables, cap));
+        EXS_CUDA(cudaMalloc(&c->d_tables, cap));
+        c->tables_bytes = cap;
+    }
+    char *h = (char *)c->h_tables;
+    char *d = (char *)c->d_tables;
+    size_t off = 0;
+    std::memcpy(h + off, ks.data(), ks.size() * sizeof(KDesc));
+    u.d_k = (const KDesc *)(d + off);
+    off += al(ks.size() * sizeof(KDesc));
+    for (int q = 0; q < 4; q++) {
+        const size_t pb = c->gt.probs[q].size() * sizeof(exs::GemmProb);
+        if (pb) std::memcpy(h + off, c->gt.probs[q].data(), pb);
+        u.d_probs[q] = d + off;
+        off += al(pb);
+        const size_t wb = c->gt.work[q].size() * sizeof(exs::TileWork);
+        if (wb) std::memcpy(h + off, c->gt.work[q].data(), wb);
+        u.d_work[q] = d + off;
+        u.nwork[q] = (int)c->gt.work[q].size();
+        off += al(wb);
+    }
+    EXS_CUDA(cudaMemcpyAsync(c->d_tables, c->h_tables, off, cudaMemcpyHostToDevice, c->stream));
+    EXS_CUDA(cudaEventRecord(c->tables_free, c->stream));
+    return EXS_OK;
+}
+
+// Run the whole setup for the k descriptors in ks (device arrays filled).
+// If have_planes, the A planes are already in place (apwalm given).
+int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
+{
+    cudaStream_t s = c->stream;
+    const DevParams p = c->params();
+    int ngp_max = 0;
+    for (auto &k : ks) ngp_max = std::max(ngp_max, k.ngp);
+    Uploaded u{};
+    int rc = upload_tables(c, ks, u);
+    if (rc != EXS_OK) return rc;
+    EXS_CUDA(cudaEventRecord(c->ev[0], s));
+    if (!have_planes) EXS_CUDA(exs::launch_match_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
+    if (c->relativity == EXS_REL_IORA) EXS_CUDA(exs::launch_iora_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
+    EXS_CUDA(cudaEventRecord(c->ev[1], s));
+    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
+                                   u.nwork[exs::EPI_PLANAR], u.d_k, s));
+    EXS_CUDA(cudaEventRecord(c->ev[2], s));
+    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
+                                   u.nwork[exs::EPI_HAM], u.d_k, s));
+    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_OVL, p, u.d_probs[exs::EPI_OVL], u.d_work[exs::EPI_OVL],
+                                   u.nwork[exs::EPI_OVL], u.d_k, s));
+    EXS_CUDA(cudaEventRecord(c->ev[3], s));
+    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_LOROWS, p, u.d_probs[exs::EPI_LOROWS], u.d_work[exs::EPI_LOROWS],
+                                   u.nwork[exs::EPI_LOROWS], u.d_k, s));
+    EXS_CUDA(exs::launch_olp_apwlo(p, u.d_k, (int)ks.size(), ngp_max, s));
+    EXS_CUDA(exs::launch_lolo_blocks(p, u.d_k, (int)ks.size(), s));
+    EXS_CUDA(cudaEventRecord(c->ev[4], s));
+    return EXS_OK;
+}
+
+KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double *d_vgpc, exs_complex *h, exs_complex *o)
+{
+    KDesc k{};
+    k.ngp = ngp;
+    k.nmat = ngp + c->nlotot;
+    k.igpig = d_igpig;
+    k.vgpc = d_vgpc;
+    k.h = h;
+    k.o = o;
+    double *w = c->d_work + (size_t)slot * c->nplanes * c->plane;
+    k.ar = w;
+    k.ai = w + c->plane;
+    k.br = w + 2 * c->plane;
+    k.bi = w + 3 * c->plane;
+    if (c->relativity == EXS_REL_IORA) {
+        k.cr = w + 4 * c->plane;
+        k.ci = w + 5 * c->plane;
+    } else {
+        k.cr = k.ar;
+        k.ci = k.ai;
+    }
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int exs_setup_batched_device(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,
+                             exs_complex *const *h_dev, exs_complex *const *o_dev)
+{
+    if (!c || nk < 0 || (nk > 0 && (!ngp || !igpig_dev || !vgpc_dev || !h_dev || !o_dev)))
+        return fail(c, EXS_ERR_ARG, "exs_setup_batched_device: bad argument");
+    if (nk > c->max_batch) return fail(c, EXS_ERR_SIZE, "nk exceeds max_batch");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    for (int k = 0; k < nk; k++)
+        if (ngp[k] <= 0 || ngp[k] > c->ngkmax || !h_dev[k] || !o_dev[k])
+            return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax or null output");
+    cudaSetDevice(c->device);
+    EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    std::vector<KDesc> ks;
+    for (int k = 0; k < nk; k++)
+        ks.push_back(slot_desc(c, k, ngp[k], igpig_dev + (size_t)c->ngkmax * k, vgpc_dev + 3 * (size_t)c->ngkmax * k,
+                               h_dev[k], o_dev[k]));
+    if (nk == 0) return EXS_OK;
+    return run_setup(c, ks, false);
+}
+
+int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, const double *vgpc,
+                      exs_complex *const *h, exs_complex *const *o)
+{
+    if (!c || nk < 0 || (nk > 0 && (!ngp || !igpig || !vgpc || !h || !o)))
+        return fail(c, EXS_ERR_ARG, "exs_setup_batched: bad argument");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    for (int k = 0; k < nk; k++) {
+        if (ngp[k] <= 0 || ngp[k] > c->ngkmax || !h[k] || !o[k])
+            return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax or null output");
+        for (int i = 0; i < ngp[k]; i++) {
+            const int g = igpig[(size_t)c->ngkmax * k + i];
+            if (g < 1 || g > c->ngrtot) return fail(c, EXS_ERR_INDEX, "igpig entry outside 1..ngrtot");
+        }
+    }
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    int worst = EXS_OK;
+    for (int k0 = 0; k0 < nk; k0 += c->max_batch) {
+        const int nb = std::min(c->max_batch, nk - k0);
+        EXS_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(c->h_igpig_pinned, igpig + (size_t)c->ngkmax * k0, sizeof(int) * (size_t)c->ngkmax * nb);
+        std::memcpy(c->h_vgpc_pinned, vgpc + 3 * (size_t)c->ngkmax * k0, sizeof(double) * 3 * (size_t)c->ngkmax * nb);
+        EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+        EXS_CUDA(cudaMemcpyAsync(c->d_igpig, c->h_igpig_pinned, sizeof(int) * (size_t)c->ngkmax * nb,
+                                 cudaMemcpyHostToDevice, s));
+        EXS_CUDA(cudaMemcpyAsync(c->d_vgpc, c->h_vgpc_pinned, sizeof(double) * 3 * (size_t)c->ngkmax * nb,
+                                 cudaMemcpyHostToDevice, s));
+        std::vector<KDesc> ks;
+        for (int k = 0; k < nb; k++) {
+            exs_complex *dh = c->d_ho + (size_t)2 * k * c->nmatmax * c->nmatmax;
+            exs_complex *dob = dh + (size_t)c->nmatmax * c->nmatmax;
+            ks.push_back(slot_desc(c, k, ngp[k0 + k], c->d_igpig + (size_t)c->ngkmax * k,
+                                   c->d_vgpc + 3 * (size_t)c->ngkmax * k, dh, dob));
+        }
+        int rc = run_setup(c, ks, false);
+        if (rc < 0) return rc;
+        for (int k = 0; k < nb; k++) {
+            const size_t bytes = sizeof(exs_complex) * (size_t)ks[k].nmat * ks[k].nmat;
+            EXS_CUDA(cudaMemcpyAsync(h[k0 + k], ks[k].h, bytes, cudaMemcpyDeviceToHost, s));
+            EXS_CUDA(cudaMemcpyAsync(o[k0 + k], ks[k].o, bytes, cudaMemcpyDeviceToHost, s));
+        }
+        rc = exs_synchronize(c);
+        if (rc < 0) return rc;
+        if (rc > worst) worst = rc;
+    }
+    return worst;
+}
+
+int exs_hamiltonandoverlapsetup(exs_ctx *c, int ngp, const exs_complex *apwalm, const int *igpig,
+                                const double *vgpc, exs_complex *h, exs_complex *o)
+{
+    if (!c || !igpig || !vgpc || !h || !o) return fail(c, EXS_ERR_ARG, "exs_hamiltonandoverlapsetup: null argument");
+    if (ngp <= 0 || ngp > c->ngkmax) return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    if (!apwalm) {
+        exs_complex *hh[1] = {h}, *oo[1] = {o};
+        // single k-point: the batched path with nk = 1 (igpig/vgpc carry ngkmax rows)
+        std::vector<int> ig((size_t)c->ngkmax, 0);
+        std::vector<double> vg(3 * (size_t)c->ngkmax, 0.0);
+        std::memcpy(ig.data(), igpig, sizeof(int) * ngp);
+        std::memcpy(vg.data(), vgpc, sizeof(double) * 3 * ngp);
+        return exs_setup_batched(c, 1, &ngp, ig.data(), vg.data(), hh, oo);
+    }
+    for (int i = 0; i < ngp; i++)
+        if (igpig[i] < 1 || igpig[i] > c->ngrtot) return fail(c, EXS_ERR_INDEX, "igpig entry outside 1..ngrtot");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    EXS_CUDA(cudaStreamSynchronize(s));
+    const int lmmax = (c->lmaxapw + 1) * (c->lmaxapw + 1);
+    const size_t nalm = (size_t)c->ngkmax * c->apwordmax * lmmax * c->natmtot;
+    if (!c->d_apwalm) {
+        EXS_CUDA(dalloc(&c->d_apwalm, nalm));
+        EXS_CUDA(dalloc(&c->d_match_in, 3 * (size_t)c->ngkmax));
+        EXS_CUDA(dalloc(&c->d_match_sf, (size_t)c->ngkmax * c->natmtot));
+    }
+    EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+    EXS_CUDA(cudaMemcpy2DAsync(c->d_apwalm, sizeof(exs_complex) * c->ngkmax, apwalm, sizeof(exs_complex) * c->ngkmax,
+                               sizeof(exs_complex) * ngp, nalm / c->ngkmax, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaMemcpyAsync(c->d_igpig, igpig, sizeof(int) * ngp, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaMemcpyAsync(c->d_vgpc, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyHostToDevice, s));
+    std::vector<KDesc> ks;
+    ks.push_back(slot_desc(c, 0, ngp, c->d_igpig, c->d_vgpc, c->d_ho, c->d_ho + (size_t)c->nmatmax * c->nmatmax));
+    EXS_CUDA(exs::launch_apwalm_to_planes(c->params(), ngp, c->d_apwalm, ks[0].ar, ks[0].ai, s));
+    int rc = run_setup(c, ks, true);
+    if (rc < 0) return rc;
+    const size_t bytes = sizeof(exs_complex) * (size_t)ks[0].nmat * ks[0].nmat;
+    EXS_CUDA(cudaMemcpyAsync(h, ks[0].h, bytes, cudaMemcpyDeviceToHost, s));
+    EXS_CUDA(cudaMemcpyAsync(o, ks[0].o, bytes, cudaMemcpyDeviceToHost, s));
+    return exs_synchronize(c);
+}
+
+int exs_forcek(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int nstfv, const exs_complex *evecfv,
+               int ldv, const double *evalfv, const double *occsv, double wkpt, const double *ffacg,
+               const double *vgc, double *forceibs)
+{
+    (void)ngp; (void)igpig; (void)vgpc; (void)nstfv; (void)evecfv; (void)ldv; (void)evalfv; (void)occsv;
+    (void)wkpt; (void)ffacg; (void)vgc; (void)forceibs;
+    return fail(c, EXS_ERR_STATE, "exs_forcek is not built into this library yet");
+}
+
+}  // extern "C"

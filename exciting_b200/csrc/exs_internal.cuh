@@ -1,0 +1,182 @@
+// Internal definitions shared by the CUDA translation units of libexciting_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/exciting_b200.h"
+#include "special.cuh"
+
+namespace exs {
+
+// Device error flags (bit set), read back after each public call.
+enum : int {
+    DEV_ERR_INDEX = 1,   // ivgig lookup outside the box
+    DEV_WARN_SINGULAR = 2,
+};
+
+// One atom's place in the device layouts.
+struct AtomDesc {
+    int species;
+    int apw_off;     // first row of this atom in the stacked APW rows (A, B planes)
+    int napw;        // m_a: APW rows of this atom (l <= lmaxmat)
+    int lo_off;      // first row of this atom inside the lo block (0-based), -1 if none
+    int losize;      // lo rows of this atom
+    double pos[3];   // atposc
+};
+
+// Per-k-point descriptor of a batched call (device copy).
+struct KDesc {
+    int ngp;
+    int nmat;
+    const int *igpig;        // (ngkmax) device, 1-based G indices
+    const double *vgpc;      // (3, ngkmax) device
+    exs_complex *h;          // (nmat, nmat) device, column-major
+    exs_complex *o;
+    double *ar, *ai;         // A planes  [Kpad][npad]
+    double *br, *bi;         // B = blockdiag(h_a) A planes
+    double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
+};
+
+// Constant per-context device parameters passed by value to kernels.
+struct DevParams {
+    int natmtot, lmaxapw, lmaxmat, apwordmax, lmmaxapw, np_tail;
+    int ngkmax, npad, K, Kpad;
+    int nlotot, maxnlo, nlomax, lolmmax;
+    int ngvec, ngrtot;
+    int intgv_lo[3], intgv_n[3];
+    int relativity;
+    double omega;
+    const AtomDesc *atoms;       // natmtot
+    const int *apword;           // (lmaxapw+1, nspecies)
+    const double *rmt;           // nspecies
+    const double *spr_tail;      // (np, nspecies)
+    const double *apwfr_tail;    // (np, apwordmax, lmaxapw+1, natmtot)
+    const int *ivg;              // (3, ngrtot)
+    const int *ivgig;            // box
+    const exs_complex *veffig;   // ngvec
+    const exs_complex *kinw;     // ngvec (meffig or cfunig)
+    const exs_complex *cfunig;   // ngvec
+    const exs_complex *m2effig;  // ngvec or null
+    const exs_complex *lolo;     // (maxnlo, maxnlo, natmtot)
+    const double *ololo;         // (nlomax, nlomax, natmtot)
+    const double *h1lolo;        // (nlomax, nlomax, natmtot) or null
+    const double *oalo;          // (apwordmax, nlomax, natmtot)
+    const double *h1loa;         // or null
+    const double *h1aa;          // (apwordmax, apwordmax, lmaxapw+1, natmtot) or null
+    const int *idxlo;            // (lolmmax, nlomax, natmtot), 1-based values
+    const int *lorbl;            // (nlomax, nspecies)
+    const int *nlorb;            // nspecies
+    int *err;                    // device error flags
+};
+
+enum EpiKind { EPI_PLANAR = 0, EPI_HAM = 1, EPI_OVL = 2, EPI_LOROWS = 3 };
+
+// One complex product C = op(X) Y of a grouped launch, X stored [k][m],
+// Y stored [k][n], real and imaginary planes apart.
+struct GemmProb {
+    const double *xr, *xi;
+    long ldx;
+    const double *yr, *yi;
+    long ldy;
+    int M, N, K;
+    int conjx;
+    double *outr, *outi;   // EPI_PLANAR output [m][n]
+    long ldo;
+    exs_complex *z;        // EPI_HAM / EPI_OVL / EPI_LOROWS: za(ldz, *)
+    long ldz;
+    int row0;              // EPI_LOROWS: za row of m = 0
+    int kidx;              // k-point of this problem (interstitial tables)
+};
+
+struct TileWork {
+    int prob, tm, tn;
+};
+
+struct GemmTables {
+    std::vector<GemmProb> probs[4];
+    std::vector<TileWork> work[4];
+};
+
+}  // namespace exs
+
+// Host-side context.
+struct exs_ctx {
+    // configuration
+    int natmtot = 0, nspecies = 0, lmaxapw = 0, lmaxmat = 0, apwordmax = 0, nlomax = 0;
+    std::vector<int> atom_species, apword, nlorb, lorbl;
+    std::vector<double> rmt, atposc, bvec;
+    double omega = 0.0;
+    int ngkmax = 0, ngrtot = 0, ngvec = 0, relativity = 0, np_tail = 4, max_batch = 1;
+    int intgv[6] = {0, 0, 0, 0, 0, 0};
+    // derived
+    int maxaa = 0, maxnlo = 0, nlotot = 0, lolmmax = 1, lolmax = 0;
+    std::vector<int> idxlo, losize;
+    std::vector<exs::AtomDesc> atoms;
+    int K = 0, Kpad = 0, npad = 0, nmatmax = 0;
+    int ldh = 0, ldlo = 0;       // leading dims of the planar h_a and loa copies
+    // device tables
+    exs::AtomDesc *d_atoms = nullptr;
+    int *d_apword = nullptr, *d_ivg = nullptr, *d_ivgig = nullptr, *d_idxlo = nullptr;
+    int *d_lorbl = nullptr, *d_nlorb = nullptr;
+    double *d_rmt = nullptr;
+    // SCF inputs
+    bool have_inputs = false;
+    double *d_haa_r = nullptr, *d_haa_i = nullptr;   // [ias][f'][f] ld ldh
+    double *d_loa_r = nullptr, *d_loa_i = nullptr;   // [ias][f][r] ld ldlo
+    exs_complex *d_lolo = nullptr;
+    double *d_oalo = nullptr, *d_ololo = nullptr, *d_h1aa = nullptr, *d_h1loa = nullptr, *d_h1lolo = nullptr;
+    exs_complex *d_veffig = nullptr, *d_kinw = nullptr, *d_cfunig = nullptr, *d_m2effig = nullptr;
+    double *d_spr_tail = nullptr, *d_apwfr_tail = nullptr;
+    // work space (max_batch slots)
+    size_t plane = 0;            // Kpad * npad doubles per plane
+    double *d_work = nullptr;    // A, B (and C) planes for all slots
+    int nplanes = 4;
+    exs_complex *d_ho = nullptr; // H and O of all slots (host-facing calls)
+    int *d_igpig = nullptr;
+    double *d_vgpc = nullptr;
+    int *d_err = nullptr;
+    // per-call tables (k descriptors, grouped-GEMM problems and tiles):
+    // packed in pinned host memory, uploaded with one copy
+    void *h_tables = nullptr, *d_tables = nullptr;
+    size_t tables_bytes = 0;
+    cudaEvent_t tables_free = nullptr;   // recorded after the upload
+    exs::GemmTables gt;
+    // pinned staging for host-facing calls
+    int *h_igpig_pinned = nullptr;
+    double *h_vgpc_pinned = nullptr;
+    // match-only buffers
+    double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
+    exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
+    exs_complex *d_apwalm = nullptr;   // (ngkmax, apwordmax, lmmaxapw, natmtot)
+    // precision
+    int prec_mode = EXS_PREC_FP64;
+    int slices = 7;
+    // runtime
+    int device = 0;
+    cudaStream_t stream = nullptr;      // stream the work runs on
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    cudaEvent_t ev[8] = {};
+    double last_t[5] = {0, 0, 0, 0, 0};
+    std::string last_error;
+
+    exs::DevParams params() const;
+};
+
+// Launch helpers implemented in the .cu files.
+namespace exs {
+cudaError_t launch_match_planes(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
+cudaError_t launch_match_ref(const DevParams &p, int ngp, int ngkmax, const double *gpc, const double *tpgpc,
+                             const exs_complex *sfacgp, exs_complex *apwalm, cudaStream_t s);
+cudaError_t launch_apwalm_to_planes(const DevParams &p, int ngp, const exs_complex *apwalm, double *ar,
+                                    double *ai, cudaStream_t s);
+cudaError_t launch_iora_planes(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
+cudaError_t launch_lolo_blocks(const DevParams &p, const KDesc *d_k, int nk, cudaStream_t s);
+cudaError_t launch_olp_apwlo(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
+// Grouped FP64 GEMM stages (setup_f64.cu)
+void build_gemm_tables(const exs_ctx *c, const std::vector<KDesc> &ks, GemmTables &t);
+cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, const void *d_work, int nwork,
+                             const KDesc *d_k, cudaStream_t s);
+}  // namespace exs

@@ -1,0 +1,216 @@
+"""Host-side mirror of the reference's per-k-point H/O setup interface.
+
+``Setup`` owns one library context for one ``LapwSystem`` and exposes the
+reference's calls with the reference's argument meaning:
+
+* ``match(gk)``                        -- call match(ngp, gpc, tpgpc, sfacgp, apwalm)
+* ``hamiltonandoverlapsetup(gk, apwalm=None)``
+                                        -- call hamiltonandoverlapsetup(system, ngp,
+                                           apwalm, igpig, vgpc) on newsystem's
+                                           zeroed matrices, then copy_UL
+* ``setup_batched(gks)``               -- the k-loop of one SCF iteration
+* ``forcek(gk, evecfv, evalfv, occsv, wkpt)``
+                                        -- the IBS part of call forcek(ik, ffacg)
+
+Everything is computed by libexciting_b200.so on the GPU; errors of the
+library raise ``ExsError``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import abi
+from .crystal import ffacg_species, gensfacgp
+from .system import RELATIVITY, LapwSystem
+
+_keep = []
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _f(a, dtype):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+class Setup:
+    def __init__(self, sys: LapwSystem, *, ngkmax: int | None = None, max_batch: int = 1):
+        self.sys = sys
+        self.lib = abi.load()
+        b = sys.basis
+        gv = sys.gv
+        gks = sys.gksets() if (ngkmax is None and sys.kpoints is not None) else None
+        self.ngkmax = int(ngkmax if ngkmax is not None else max(g.ngp for g in gks))
+        nsp = b.nspecies
+        nlomax = max(b.nlomax, 1)
+        self._arrays = dict(
+            atom_species=_f(b.atom_species, np.int32),
+            apword=_f(np.array(b.apword).T, np.int32),
+            nlorb=_f([len(x) for x in b.lorbl], np.int32),
+            lorbl=_f(np.array([list(x) + [0] * (nlomax - len(x)) for x in b.lorbl]).T.reshape(nlomax, nsp), np.int32),
+            rmt=_f(sys.rmt, np.float64),
+            atposc=_f(sys.crystal.atposc, np.float64),
+            bvec=_f(sys.crystal.bvec, np.float64),
+            intgv=_f(gv.intgv, np.int32),
+            ivg=_f(gv.ivg, np.int32),
+            ivgig=np.asfortranarray(gv.ivgig, dtype=np.int32),
+        )
+        A = self._arrays
+        cfg = abi.exs_config()
+        cfg.natmtot = sys.natmtot
+        cfg.nspecies = nsp
+        cfg.atom_species = A["atom_species"].ctypes.data
+        cfg.lmaxapw = b.lmaxapw
+        cfg.lmaxmat = b.lmaxmat
+        cfg.apwordmax = b.apwordmax
+        cfg.apword = A["apword"].ctypes.data
+        cfg.nlomax = nlomax
+        cfg.nlorb = A["nlorb"].ctypes.data
+        cfg.lorbl = A["lorbl"].ctypes.data
+        cfg.rmt = A["rmt"].ctypes.data
+        cfg.omega = sys.crystal.omega
+        cfg.atposc = A["atposc"].ctypes.data
+        cfg.bvec = A["bvec"].ctypes.data
+        cfg.ngkmax = self.ngkmax
+        cfg.ngrtot = gv.ngrtot
+        cfg.ngvec = gv.ngvec
+        cfg.intgv = A["intgv"].ctypes.data
+        cfg.ivg = A["ivg"].ctypes.data
+        cfg.ivgig = A["ivgig"].ctypes.data
+        cfg.relativity = RELATIVITY[sys.relativity]
+        cfg.np_tail = sys.np_tail
+        cfg.max_batch = max_batch
+        self.max_batch = max_batch
+        ctx = ctypes.c_void_p()
+        rc = self.lib.exs_ctx_create(ctypes.byref(cfg), ctypes.byref(ctx))
+        if rc != 0:
+            raise abi.ExsError(rc, "exs_ctx_create failed")
+        self.ctx = ctx
+        sizes = (ctypes.c_int * 3)()
+        self.lib.exs_ctx_sizes(ctx, ctypes.byref(sizes, 0), ctypes.byref(sizes, 4), ctypes.byref(sizes, 8))
+        self.maxaa, self.maxnlo, self.nlotot = int(sizes[0]), int(sizes[1]), int(sizes[2])
+        self.set_scf_inputs()
+
+    # ------------------------------------------------------------------
+    def _check(self, rc):
+        return abi.check(self.lib, self.ctx, rc)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.exs_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_scf_inputs(self, sys: LapwSystem | None = None):
+        s = sys or self.sys
+        keep = dict(
+            mt_aa=_f(s.mt_aa, np.complex128), mt_loa=_f(s.mt_loa, np.complex128),
+            mt_lolo=_f(s.mt_lolo, np.complex128), oalo=_f(s.oalo, np.float64),
+            ololo=_f(s.ololo, np.float64), veffig=_f(s.veffig, np.complex128),
+            cfunig=_f(s.cfunig, np.complex128), spr_tail=_f(s.spr_tail, np.float64),
+            apwfr_tail=_f(s.apwfr_tail, np.float64),
+            meffig=None if s.meffig is None else _f(s.meffig, np.complex128),
+            m2effig=None if s.m2effig is None else _f(s.m2effig, np.complex128),
+            h1aa=None if s.h1aa is None else _f(s.h1aa, np.float64),
+            h1loa=None if s.h1loa is None else _f(s.h1loa, np.float64),
+            h1lolo=None if s.h1lolo is None else _f(s.h1lolo, np.float64),
+        )
+        inp = abi.exs_scf_inputs()
+        for k, v in keep.items():
+            setattr(inp, k, None if v is None else v.ctypes.data)
+        self._check(self.lib.exs_set_scf_inputs(self.ctx, ctypes.byref(inp)))
+
+    def set_precision(self, mode: str = "fp64", slices: int = 7):
+        m = {"fp64": 0, "ozaki": 1}[mode]
+        self._check(self.lib.exs_set_precision(self.ctx, m, slices))
+
+    # ------------------------------------------------------------------
+    def match(self, gk):
+        """apwalm(ngkmax, apwordmax, lmmaxapw, natmtot) from the reference's match inputs."""
+        b = self.sys.basis
+        n = self.ngkmax
+        gpc = np.zeros(n); gpc[: gk.ngp] = gk.gpc
+        tpgpc = np.zeros((2, n), order="F"); tpgpc[:, : gk.ngp] = gk.tpgpc
+        sf = np.zeros((n, self.sys.natmtot), dtype=np.complex128, order="F")
+        sf[: gk.ngp] = gensfacgp(gk.vgpc, self.sys.crystal.atposc)
+        apwalm = np.zeros((n, b.apwordmax, b.lmmaxapw, self.sys.natmtot), dtype=np.complex128, order="F")
+        rc = self._check(self.lib.exs_match(self.ctx, gk.ngp, _ptr(gpc), _ptr(tpgpc), _ptr(sf), _ptr(apwalm)))
+        return apwalm, rc
+
+    def _gk_arrays(self, gk):
+        ig = np.zeros(self.ngkmax, dtype=np.int32); ig[: gk.ngp] = gk.igpig
+        vg = np.zeros((3, self.ngkmax), order="F"); vg[:, : gk.ngp] = gk.vgpc
+        return ig, vg
+
+    def hamiltonandoverlapsetup(self, gk, apwalm=None):
+        nmat = gk.ngp + self.nlotot
+        h = np.empty((nmat, nmat), dtype=np.complex128, order="F")
+        o = np.empty((nmat, nmat), dtype=np.complex128, order="F")
+        ig, vg = self._gk_arrays(gk)
+        a = None if apwalm is None else _f(apwalm, np.complex128)
+        self._check(self.lib.exs_hamiltonandoverlapsetup(self.ctx, gk.ngp, _ptr(a), _ptr(ig), _ptr(vg),
+                                                         _ptr(h), _ptr(o)))
+        return h, o
+
+    def setup_batched(self, gks, out=None):
+        """H and O of every k-point in gks; out = optional list of (h, o) host arrays."""
+        nk = len(gks)
+        ngp = np.array([g.ngp for g in gks], dtype=np.int32)
+        ig = np.zeros((self.ngkmax, nk), dtype=np.int32, order="F")
+        vg = np.zeros((3, self.ngkmax, nk), order="F")
+        for k, g in enumerate(gks):
+            ig[: g.ngp, k] = g.igpig
+            vg[:, : g.ngp, k] = g.vgpc
+        if out is None:
+            out = []
+            for g in gks:
+                nmat = g.ngp + self.nlotot
+                out.append((np.empty((nmat, nmat), dtype=np.complex128, order="F"),
+                            np.empty((nmat, nmat), dtype=np.complex128, order="F")))
+        hp = (ctypes.c_void_p * nk)(*[o[0].ctypes.data for o in out])
+        op = (ctypes.c_void_p * nk)(*[o[1].ctypes.data for o in out])
+        self._check(self.lib.exs_setup_batched(self.ctx, nk, _ptr(ngp), _ptr(ig), _ptr(vg), hp, op))
+        return out
+
+    def setup_batched_device(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs):
+        """Device-resident batched setup: pointers are device addresses (ints)."""
+        nk = len(ngp)
+        ngp = np.asarray(ngp, dtype=np.int32)
+        hp = (ctypes.c_void_p * nk)(*h_ptrs)
+        op = (ctypes.c_void_p * nk)(*o_ptrs)
+        return self._check(self.lib.exs_setup_batched_device(self.ctx, nk, _ptr(ngp), ctypes.c_void_p(igpig_dev_ptr),
+                                                             ctypes.c_void_p(vgpc_dev_ptr), hp, op))
+
+    def set_stream(self, stream_ptr: int | None):
+        """Run on a caller-owned cudaStream_t (its integer handle); None = own stream."""
+        return self._check(self.lib.exs_set_stream(self.ctx, None if not stream_ptr else ctypes.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        return self._check(self.lib.exs_synchronize(self.ctx))
+
+    def last_timings(self):
+        t = np.zeros(5)
+        self.lib.exs_last_timings(self.ctx, _ptr(t), 5)
+        return t
+
+    def forcek(self, gk, evecfv, evalfv, occsv, wkpt, forceibs=None):
+        """IBS force of one k-point accumulated into forceibs(3, natmtot)."""
+        s = self.sys
+        ig, vg = self._gk_arrays(gk)
+        ev = _f(evecfv, np.complex128)
+        ffacg = _f(np.stack([ffacg_species(s.gv.gc[: s.gv.ngvec], r, s.crystal.omega) for r in s.rmt], axis=1),
+                   np.float64)
+        vgc = _f(s.gv.vgc[:, : s.gv.ngvec], np.float64)
+        f = np.zeros((3, s.natmtot), order="F") if forceibs is None else forceibs
+        self._check(self.lib.exs_forcek(self.ctx, gk.ngp, _ptr(ig), _ptr(vg), ev.shape[1], _ptr(ev), ev.shape[0],
+                                        _ptr(_f(evalfv, np.float64)), _ptr(_f(occsv, np.float64)), float(wkpt),
+                                        _ptr(ffacg), _ptr(vgc), _ptr(f)))
+        return f

@@ -1,0 +1,157 @@
+/*
+ * exciting_b200 -- C-ABI of the B200 (sm_100a) per-k-point LAPW H/O setup.
+ *
+ * Drop-in for the reference's (exciting) per-k-point first-variational
+ * Hamiltonian/overlap setup path.  Every array argument follows the
+ * reference's Fortran declaration: column-major, complex(8) as two
+ * interleaved doubles, integer index tables with their 1-based values.
+ * All pointers are HOST pointers unless the entry point says "_device".
+ *
+ * Return codes: 0 success, > 0 warning (the call completed), < 0 error
+ * (the outputs are undefined; exs_last_error() gives the text).
+ */
+#ifndef EXCITING_B200_H
+#define EXCITING_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct exs_complex { double re, im; } exs_complex;   /* Fortran complex(8) */
+typedef struct exs_ctx exs_ctx;
+
+enum {
+    EXS_OK = 0,
+    EXS_WARN_SINGULAR = 1,   /* a matching system D_l was singular (match.f90:166-175) */
+    EXS_ERR_ARG = -1,        /* bad argument (null pointer, negative size, ...) */
+    EXS_ERR_CUDA = -2,       /* a CUDA runtime call failed */
+    EXS_ERR_SIZE = -3,       /* a size above the compiled limits or the context's maxima */
+    EXS_ERR_INDEX = -4,      /* a G-G' difference fell outside the ivgig box */
+    EXS_ERR_STATE = -5,      /* exs_set_scf_inputs has not been called */
+    EXS_ERR_NOMEM = -6       /* a device allocation failed */
+};
+
+enum { EXS_REL_NONE = 0, EXS_REL_ZORA = 1, EXS_REL_IORA = 2 };   /* ValenceRelativity */
+enum { EXS_PREC_FP64 = 0, EXS_PREC_OZAKI_INT8 = 1 };             /* MT contraction path */
+
+/* Per-run description: what init0/init1 leave in the reference's modules. */
+typedef struct exs_config {
+    int natmtot, nspecies;
+    const int *atom_species;  /* (natmtot) 0-based species of atom ias; atoms grouped by species (idxas order) */
+    int lmaxapw, lmaxmat;     /* input%groundstate%lmaxapw, lmaxmat */
+    int apwordmax;
+    const int *apword;        /* apword(0:lmaxapw, nspecies) */
+    int nlomax;
+    const int *nlorb;         /* nlorb(nspecies) */
+    const int *lorbl;         /* lorbl(nlomax, nspecies) */
+    const double *rmt;        /* rmt(nspecies) */
+    double omega;             /* unit-cell volume */
+    const double *atposc;     /* atposc(3, natmtot), Cartesian */
+    const double *bvec;       /* bvec(3,3), reciprocal lattice vectors as columns */
+    int ngkmax;               /* maximum number of G+k over all k */
+    int ngrtot, ngvec;
+    const int *intgv;         /* intgv(3,2): inclusive integer box of ivgig */
+    const int *ivg;           /* ivg(3, ngrtot) */
+    const int *ivgig;         /* ivgig(intgv(1,1):intgv(1,2), ..., ...) */
+    int relativity;           /* EXS_REL_* (input%groundstate%ValenceRelativity) */
+    int np_tail;              /* max(apwordmax+1, 4) radial points used by match (match.f90:87) */
+    int max_batch;            /* most k-points handed to one batched call (>= 1) */
+} exs_config;
+
+/* Per-SCF-iteration inputs (what scf_cycle recomputes before the k-loop). */
+typedef struct exs_scf_inputs {
+    const exs_complex *mt_aa;    /* mt_hscf%main%aa(maxaa, maxaa, natmtot) */
+    const exs_complex *mt_loa;   /* mt_hscf%main%loa(maxnlo, maxaa, natmtot) (may be NULL if no lo) */
+    const exs_complex *mt_lolo;  /* mt_hscf%main%lolo(maxnlo, maxnlo, natmtot) */
+    const double *oalo;          /* oalo(apwordmax, nlomax, natmtot) */
+    const double *ololo;         /* ololo(nlomax, nlomax, natmtot) */
+    const double *h1aa;          /* h1aa(apwordmax, apwordmax, 0:lmaxapw, natmtot), iora* only, else NULL */
+    const double *h1loa;         /* h1loa(apwordmax, nlomax, natmtot), iora* only, else NULL */
+    const double *h1lolo;        /* h1lolo(nlomax, nlomax, natmtot), iora* only, else NULL */
+    const exs_complex *veffig;   /* veffig(ngvec) */
+    const exs_complex *meffig;   /* meffig(ngvec), relativity /= none, else NULL */
+    const exs_complex *cfunig;   /* cfunig(ngrtot) (only the first ngvec are read) */
+    const exs_complex *m2effig;  /* m2effig(ngvec), iora* only, else NULL */
+    const double *spr_tail;      /* spr(nrmt-np+1:nrmt, nspecies) */
+    const double *apwfr_tail;    /* apwfr(nrmt-np+1:nrmt, 1, 1:apwordmax, 0:lmaxapw, natmtot) */
+} exs_scf_inputs;
+
+/* Create a context on the current CUDA device: validates the basis, builds
+ * maxaa (MaxAPWs, mod_eigensystem.F90:151-184), losize/maxnlo (MTInitAll,
+ * :194-235) and idxlo (genidxlo.f90), uploads the G-vector tables and sizes
+ * the device work space for max_batch k-points of ngkmax G+k each. */
+int exs_ctx_create(const exs_config *cfg, exs_ctx **out);
+int exs_ctx_destroy(exs_ctx *ctx);
+const char *exs_last_error(const exs_ctx *ctx);
+
+/* Sizes the context derived: maxaa, maxnlo, nlotot (so a caller can size za). */
+int exs_ctx_sizes(const exs_ctx *ctx, int *maxaa, int *maxnlo, int *nlotot);
+
+/* Upload the per-SCF-iteration inputs (copied; the caller may free them). */
+int exs_set_scf_inputs(exs_ctx *ctx, const exs_scf_inputs *in);
+
+/* Select the MT contraction arithmetic: EXS_PREC_FP64 (native FP64) or
+ * EXS_PREC_OZAKI_INT8 with `slices` int8 slices per operand (3..9). */
+int exs_set_precision(exs_ctx *ctx, int mode, int slices);
+
+/* Replaces  call match(ngp, gpc, tpgpc, sfacgp, apwalm)   (src/match.f90:13).
+ *   gpc(ngkmax), tpgpc(2, ngkmax), sfacgp(ngkmax, natmtot)  in;
+ *   apwalm(ngkmax, apwordmax, lmmaxapw, natmtot)              out.
+ * Returns EXS_WARN_SINGULAR if some D_l was singular; as the reference, the
+ * unsolved right-hand sides are then returned for that (atom, l). */
+int exs_match(exs_ctx *ctx, int ngp, const double *gpc, const double *tpgpc,
+              const exs_complex *sfacgp, exs_complex *apwalm);
+
+/* Replaces  call hamiltonandoverlapsetup(system, ngp, apwalm, igpig, vgpc)
+ * (src/src_eigensystem/hamiltonandoverlapsetup.f90:8), equivalently the live
+ * pair  call hamiltonsetup(...); call overlapsetup(...)  (src/seceqnfv.f90:76-77)
+ * on the zeroed matrices newsystem allocates.
+ *   igpig(ngkmax), vgpc(3, ngkmax) in; apwalm in, or NULL to compute the
+ *   matching coefficients on the device from vgpc;
+ *   h, o: za(nmat, nmat) with nmat = ngp + nlotot, OVERWRITTEN with the full
+ *   Hermitian matrices (upper triangle as set up, lower = conjugate, as
+ *   hamiltonoverlapocopy_UL leaves them). */
+int exs_hamiltonandoverlapsetup(exs_ctx *ctx, int ngp, const exs_complex *apwalm,
+                                const int *igpig, const double *vgpc,
+                                exs_complex *h, exs_complex *o);
+
+/* The whole k-point list of one SCF iteration in one call (the reference's
+ * k-loop over seceqn, scf_cycle.f90:237-278): nk <= max_batch k-points;
+ *   ngp(nk); igpig(ngkmax, nk); vgpc(3, ngkmax, nk);
+ *   h[ik], o[ik]: za(nmat_k, nmat_k), nmat_k = ngp(ik) + nlotot (host). */
+int exs_setup_batched(exs_ctx *ctx, int nk, const int *ngp, const int *igpig,
+                      const double *vgpc, exs_complex *const *h, exs_complex *const *o);
+
+/* Same with every array already in device memory (h, o: nk device pointers
+ * in a host array).  Asynchronous on the context's stream; exs_synchronize
+ * waits for it. */
+int exs_setup_batched_device(exs_ctx *ctx, int nk, const int *ngp_host,
+                             const int *igpig_dev, const double *vgpc_dev,
+                             exs_complex *const *h_dev, exs_complex *const *o_dev);
+int exs_synchronize(exs_ctx *ctx);
+
+/* Replaces the IBS part of  call forcek(ik, ffacg)  (src/forcek.f90:13) for
+ * one k-point without second variation:
+ *   igpig(ngkmax), vgpc(3, ngkmax), evecfv(nmatmax, nstfv) (leading dim ldv),
+ *   evalfv(nstfv), occsv(nstfv), wkpt(ik);
+ *   ffacg(ngvec, nspecies) (genffacg), vgc(3, ngvec);
+ *   forceibs(3, natmtot) is ACCUMULATED into, as the reference does. */
+int exs_forcek(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc,
+               int nstfv, const exs_complex *evecfv, int ldv, const double *evalfv,
+               const double *occsv, double wkpt, const double *ffacg, const double *vgc,
+               double *forceibs);
+
+/* Run the context's work on a caller-owned CUDA stream (a cudaStream_t
+ * passed as void*); NULL returns to the context's own stream. */
+int exs_set_stream(exs_ctx *ctx, void *stream);
+
+/* Device time of the phases of the last setup call, milliseconds:
+ * t[0] match, t[1] h_a A, t[2] MT contraction + interstitial, t[3] lo blocks, t[4] total. */
+int exs_last_timings(exs_ctx *ctx, double *t, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -88,15 +88,15 @@ def sbesseldm(m, lmax, x):
 
 def genylm(lmax, tp):
     out = np.zeros((lmax + 1) ** 2, dtype=np.complex128)
-    tp = np.asarray(tp, dtype=np.float64)
+    tp = np.ascontiguousarray(tp, dtype=np.float64)
     if lib().orc_genylm(lmax, _p(tp), _p(out)) != 0:
         raise ValueError("genylm: lmax out of range")
     return out
 
 
 def polynom(m, xa, ya, x):
-    xa = np.asarray(xa, dtype=np.float64)
-    ya = np.asarray(ya, dtype=np.float64)
+    xa = np.ascontiguousarray(xa, dtype=np.float64)
+    ya = np.ascontiguousarray(ya, dtype=np.float64)
     c = np.zeros(len(xa))
     return lib().orc_polynom(m, len(xa), _p(xa), _p(ya), _p(c), float(x))
 

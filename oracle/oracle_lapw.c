@@ -55,6 +55,18 @@ static double orc_factnm(int n, int m)
     return r;
 }
 
+/* x**j for integer j >= 0 by binary powering (Fortran real**integer) */
+static double orc_powi(double x, int j)
+{
+    double r = 1.0;
+    while (j > 0) {
+        if (j & 1) r *= x;
+        x *= x;
+        j >>= 1;
+    }
+    return r;
+}
+
 /* ---- src/src_lib/factr.f90 ------------------------------------------- */
 static double orc_factr(int n, int d)
 {
@@ -177,9 +189,8 @@ int orc_sbesseldm(int m, int lmax, double x, double *djl)
             if (i0 < 0) i0 = 0;
             /* Fortran integer division truncates toward zero, as C's does */
             int j = 2 * i0 + l - m;
-            double t1 = (j == 0) ? 1.0 : pow(x, (double)j);
-            double p2 = 1.0;
-            for (int k = 0; k < i0; k++) p2 *= -2.0;
+            double t1 = (j == 0) ? 1.0 : orc_powi(x, j);
+            double p2 = orc_powi(-2.0, i0);
             t1 = orc_factr(j + m, j) * t1 / (orc_factnm(i0, 1) * orc_factnm(j + l + m + 1, 2) * p2);
             double sum = t1;
             for (int i = i0 + 1; i <= maxns; i++) {
