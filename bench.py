@@ -174,6 +174,47 @@ def run_reference(args):
     return 0
 
 
+def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier):
+    """Setups/s through exs_setup_batched: pinned host igpig/vgpc in, pinned host H/O out."""
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+    nk = len(ngp)
+    h_ig = torch.from_numpy(np.ascontiguousarray(ig)).pin_memory()      # (nk, ngkmax) == Fortran (ngkmax, nk)
+    h_vg = torch.from_numpy(np.ascontiguousarray(vg)).pin_memory()      # (nk, ngkmax, 3) == Fortran (3, ngkmax, nk)
+    h_out = [(torch.empty(2 * m * m, dtype=torch.float64).pin_memory(),
+              torch.empty(2 * m * m, dtype=torch.float64).pin_memory()) for m in nmat]
+    ngp_np = np.array(ngp, dtype=np.int32)
+    hpp = (ctypes.c_void_p * nk)(*[a.data_ptr() for a, _ in h_out])
+    opp = (ctypes.c_void_p * nk)(*[b.data_ptr() for _, b in h_out])
+
+    def step_host():
+        rc = st.lib.exs_setup_batched(st.ctx, nk, ngp_np.ctypes.data_as(ctypes.c_void_p),
+                                      ctypes.c_void_p(h_ig.data_ptr()), ctypes.c_void_p(h_vg.data_ptr()), hpp, opp)
+        if rc < 0:
+            raise RuntimeError(st.lib.exs_last_error(st.ctx))
+
+    for _ in range(max(1, args.warmup)):
+        step_host()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_host()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    value = ws * nk * args.steps / (float(t.item()) * 1e-3)
+    h2d = ig.nbytes + vg.nbytes
+    d2h = sum(2 * 16 * m * m for m in nmat)
+    return value, h2d, d2h
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -192,7 +233,7 @@ def run_ours(args):
             dist.barrier()
 
     s = W.si_cube8()
-    gks = s.gksets()
+    gks = s.gksets()[: args.nk]
     nk = len(gks)
     st = Setup(s, max_batch=nk)
     stream = torch.cuda.Stream()
@@ -219,7 +260,6 @@ def run_ours(args):
     for _ in range(args.warmup):
         step_device()
     st.synchronize()
-    barrier()
     rows, stop = [], threading.Event()
     th = threading.Thread(target=_clock_sampler, args=(stop, rows), daemon=True)
     th.start()
@@ -247,59 +287,29 @@ def run_ours(args):
     value = ws * nk * args.steps / (ms_max * 1e-3)
     phase /= max(args.steps, 1)
 
-    # ---- end to end through the host-pointer entry point (pinned host buffers)
-    h_ig = torch.from_numpy(np.asfortranarray(ig.T)).pin_memory()
-    h_vg = torch.from_numpy(np.ascontiguousarray(vg)).pin_memory()        # (nk, ngkmax, 3) == Fortran (3, ngkmax, nk)
-    h_out = [(torch.empty(2 * m * m, dtype=torch.float64).pin_memory(),
-              torch.empty(2 * m * m, dtype=torch.float64).pin_memory()) for m in nmat]
-    import ctypes
-    ngp_np = np.array(ngp, dtype=np.int32)
-    hpp = (ctypes.c_void_p * nk)(*[a.data_ptr() for a, _ in h_out])
-    opp = (ctypes.c_void_p * nk)(*[b.data_ptr() for _, b in h_out])
-    ig_host = np.asfortranarray(ig.T)
+    # ---- end to end through the host-pointer entry point
+    if args.skip_e2e:
+        e2e_value, h2d, d2h = None, 0, 0
+    else:
+        e2e_value, h2d, d2h = _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier)
 
-    def step_host():
-        rc = st.lib.exs_setup_batched(st.ctx, nk, ngp_np.ctypes.data_as(ctypes.c_void_p),
-                                      ctypes.c_void_p(h_ig.data_ptr()), ctypes.c_void_p(h_vg.data_ptr()), hpp, opp)
-        if rc < 0:
-            raise RuntimeError(st.lib.exs_last_error(st.ctx))
-
-    for _ in range(max(1, args.warmup)):
-        step_host()
-    barrier()
-    torch.cuda.synchronize()
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        for _ in range(args.steps):
-            step_host()
-        e1.record(stream)
-    torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1)
-    t = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = ws * nk * args.steps / (float(t.item()) * 1e-3)
-    h2d = ig.nbytes + vg.nbytes
-    d2h = sum(2 * 16 * m * m for m in nmat)
-
-    # spot parity of one k-point against the last host result (cheap, device vs device)
-    out = {}
     if rank == 0:
         fl = main_flops(s, gks)
         main_ms = phase[2]
         peak64 = _measured_fp64_peak(torch)
         achieved = fl / (main_ms * 1e-3) / 1e12
         clocks = _clock_summary(rows, local)
-        cpu_v, cpu_n, cpu_dt = cpu_sample(s, gks, budget_s=12.0)
+        cpu_v, cpu_n, cpu_dt = (None, 0, 0.0) if args.skip_cpu else cpu_sample(s, gks, budget_s=12.0)
         out = {
             "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "k_per_step": nk, "ngp": [min(ngp), max(ngp)],
                        "nmat": [min(nmat), max(nmat)], "precision": "fp64 (DMMA)",
-                       "l2": "working set 3.1 GB (A/B planes 1.7 GB, H/O 1.3 GB) > 126 MB L2, no flush"},
-            "e2e": {"value": e2e_value, "unit": "setups/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                       "l2": "working set > 126 MB L2 (A/B planes 63 MB and H/O 48 MB per k-point), no flush"},
+            "e2e": None if e2e_value is None else {
+                "value": e2e_value, "unit": "setups/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
             "roofline": {"bound": "tensor", "kernel": "zgemm_dmma_kernel<EPI_HAM>+<EPI_OVL> (MT contraction)",
@@ -307,9 +317,10 @@ def run_ours(args):
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in "
                                         "MEASURED_PEAKS.json)",
                          "algorithmic_flops_per_step": fl, "traffic": None},
-            "cpu_baseline": {"value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
-                             "sample": f"{cpu_n} k-points of the 27-k set in {cpu_dt:.1f} s by the FP64 CPU "
-                                       "restatement (C + OpenMP + OpenBLAS zgemm)"},
+            "cpu_baseline": None if cpu_v is None else {
+                "value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": f"{cpu_n} k-points of the 27-k set in {cpu_dt:.1f} s by the FP64 CPU "
+                          "restatement (C + OpenMP + OpenBLAS zgemm)"},
             "clocks": clocks,
             "gpu_launches": 7 * args.steps,
             "setup_flops_per_step": setup_flops(s, gks),
@@ -329,6 +340,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nk", type=int, default=27, help="k-points per step (profiling runs use fewer)")
+    ap.add_argument("--skip-cpu", action="store_true", help="no CPU-baseline leg (profiling runs)")
+    ap.add_argument("--skip-e2e", action="store_true", help="no host-pointer leg (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
