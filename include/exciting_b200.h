@@ -151,6 +151,25 @@ int exs_set_stream(exs_ctx *ctx, void *stream);
  * t[0] match, t[1] h_a A, t[2] MT contraction + interstitial, t[3] lo blocks, t[4] total. */
 int exs_last_timings(exs_ctx *ctx, double *t, int n);
 
+/* For callers that cannot allocate device memory (no exs_ctx: creating one
+ * allocates).  No counterpart in the reference: it is the APW-APW muffin-tin
+ * block of hamiltonsetup/overlapsetup without the interstitial term, on
+ * caller-owned DEVICE arrays, with all work space in one 32 MiB static
+ * device array inside this library (held by every GPU that loads it):
+ *   apwi(maxaa, ngp, natmtot): each atom's matching coefficients in the
+ *     reference's row order (l, m, io) (hamiltonsetup.f90:59-71), zero past
+ *     napw[ias] rows;  aa(maxaa, maxaa, natmtot): mt_hscf%main%aa;
+ *   napw: HOST array (natmtot) of APW rows per atom;
+ *   h, o: za(ld, ngp) outputs, H = sum_a apwi^H aa apwi and O = sum_a
+ *     apwi^H apwi as full Hermitian matrices (lower = conjugate of upper).
+ * Allocates nothing; EXS_ERR_SIZE when the work space exceeds 32 MiB.  The
+ * first call on a device looks up the array's device address (make it
+ * before any stream capture).  Calls share the array: calls that overlap on
+ * the GPU race, so serialise them.  stream: a cudaStream_t, or NULL. */
+int exs_mt_contract_noalloc(int natmtot, int maxaa, const int *napw, int ngp,
+                            const exs_complex *apwi, const exs_complex *aa,
+                            exs_complex *h, exs_complex *o, int ld, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
