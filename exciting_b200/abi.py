@@ -48,6 +48,7 @@ SIGNATURES = {
     "exs_setup_batched_device": ([P, c_int, P, P, P, P, P], c_int),
     "exs_synchronize": ([P], c_int),
     "exs_forcek": ([P, c_int, P, P, c_int, P, c_int, P, P, c_double, P, P, P], c_int),
+    "exs_adjoint": ([P, c_int, P, P, c_int, P, c_int, P, P, P, P, P, P, P], c_int),
     "exs_set_stream": ([P, P], c_int),
     "exs_last_timings": ([P, P, c_int], c_int),
     "exs_mt_contract_noalloc": ([c_int, c_int, P, c_int, P, P, P, P, c_int, P], c_int),

@@ -126,6 +126,11 @@ int exs_ctx_destroy(exs_ctx *c)
                    c->d_match_in, c->d_match_sf, c->d_apwalm};
     for (void *p : dev)
         if (p) cudaFree(p);
+    if (c->d_oz) cudaFree(c->d_oz);
+    if (c->d_ozscale) cudaFree(c->d_ozscale);
+    if (c->fk_dev) cudaFree(c->fk_dev);
+    if (c->fk_tab_d) cudaFree(c->fk_tab_d);
+    if (c->fk_tab_h) cudaFreeHost(c->fk_tab_h);
     if (c->h_tables) cudaFreeHost(c->h_tables);
     if (c->h_igpig_pinned) cudaFreeHost(c->h_igpig_pinned);
     if (c->h_vgpc_pinned) cudaFreeHost(c->h_vgpc_pinned);
@@ -305,11 +310,29 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         c->prec_mode = mode;
         return EXS_OK;
     }
-    if (mode == EXS_PREC_OZAKI_INT8) {
-        if (slices < 3 || slices > 9) return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
-        return fail(c, EXS_ERR_ARG, "the int8 split-precision contraction is not built into this library");
+    if (mode != EXS_PREC_OZAKI_INT8) return fail(c, EXS_ERR_ARG, "unknown precision mode");
+    if (slices < 3 || slices > 9) return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
+    if (c->relativity == EXS_REL_IORA)
+        return fail(c, EXS_ERR_ARG, "the split-precision contraction does not take the iora* overlap term");
+    if (2 * (size_t)c->Kpad * 127 * 127 * slices >= (size_t)1 << 31)
+        return fail(c, EXS_ERR_SIZE, "K too large for exact int32 accumulation of one diagonal");
+    cudaSetDevice(c->device);
+    EXS_CUDA(cudaStreamSynchronize(c->stream));
+    const int kp8 = round_up(c->K, 128);
+    const size_t slot = (size_t)6 * slices * c->npad * kp8;
+    if (c->d_oz) { cudaFree(c->d_oz); c->d_oz = nullptr; }
+    if (c->d_ozscale) { cudaFree(c->d_ozscale); c->d_ozscale = nullptr; }
+    cudaError_t e = cudaMalloc((void **)&c->d_oz, slot * c->max_batch);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 2 * c->npad * c->max_batch);
+    if (e != cudaSuccess) {
+        c->prec_mode = EXS_PREC_FP64;
+        return fail(c, EXS_ERR_NOMEM, "split-precision work space");
     }
-    return fail(c, EXS_ERR_ARG, "unknown precision mode");
+    c->kp8 = kp8;
+    c->oz_slot_bytes = slot;
+    c->slices = slices;
+    c->prec_mode = mode;
+    return EXS_OK;
 }
 
 int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
@@ -392,14 +415,20 @@ int exs_synchronize(exs_ctx *c)
     EXS_CUDA(cudaStreamSynchronize(c->stream));
     int err = 0;
     EXS_CUDA(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < 4; i++) {
-        float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]) == cudaSuccess) c->last_t[i] = ms;
+    if (c->timed) {   // phase events were recorded by the last setup call
+        for (int i = 0; i < 4; i++) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]) == cudaSuccess) c->last_t[i] = ms;
+        }
+        float tot = 0.f;
+        if (cudaEventElapsedTime(&tot, c->ev[0], c->ev[4]) == cudaSuccess) c->last_t[4] = tot;
+        c->timed = false;
+        (void)cudaGetLastError();   // an event query must not leave a sticky error for the next call
     }
-    float tot = 0.f;
-    if (cudaEventElapsedTime(&tot, c->ev[0], c->ev[4]) == cudaSuccess) c->last_t[4] = tot;
     if (err & exs::DEV_ERR_INDEX)
         return fail(c, EXS_ERR_INDEX, "a G-G' difference fell outside the ivgig box");
+    if (err & exs::DEV_ERR_TIMEOUT)
+        return fail(c, EXS_ERR_CUDA, "a tensor-core pipeline wait expired (kernel gave up)");
     if (err & exs::DEV_WARN_SINGULAR) {
         c->last_error = "a matching system D_l was singular (match.f90:166-175)";
         return EXS_WARN_SINGULAR;
@@ -444,10 +473,12 @@ int exs_match(exs_ctx *c, int ngp, const double *gpc, const double *tpgpc, const
     EXS_CUDA(cudaMemcpyAsync(c->d_match_in + c->ngkmax, tpgpc, sizeof(double) * 2 * ngp, cudaMemcpyHostToDevice, s));
     EXS_CUDA(cudaMemcpy2DAsync(c->d_match_sf, sizeof(exs_complex) * c->ngkmax, sfacgp, sizeof(exs_complex) * c->ngkmax,
                                sizeof(exs_complex) * ngp, c->natmtot, cudaMemcpyHostToDevice, s));
+    (void)cudaGetLastError();
     EXS_CUDA(cudaEventRecord(c->ev[0], s));
     EXS_CUDA(exs::launch_match_ref(c->params(), ngp, c->ngkmax, c->d_match_in, c->d_match_in + c->ngkmax,
                                    c->d_match_sf, c->d_apwalm, s));
     for (int i = 1; i <= 4; i++) EXS_CUDA(cudaEventRecord(c->ev[i], s));
+    c->timed = true;
     // only the first ngp rows of each column are defined by match
     EXS_CUDA(cudaMemcpy2DAsync(apwalm, sizeof(exs_complex) * c->ngkmax, c->d_apwalm, sizeof(exs_complex) * c->ngkmax,
                                sizeof(exs_complex) * ngp, nalm / c->ngkmax, cudaMemcpyDeviceToHost, s));
@@ -466,19 +497,40 @@ struct Uploaded {
     const void *d_probs[4];
     const void *d_work[4];
     int nwork[4];
+    const void *d_oztiles;
+    int noztiles;
 };
+
+// Upper tiles (128 rows x 32 columns) of the split-precision contraction.
+void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t)
+{
+    t.clear();
+    for (size_t k = 0; k < ks.size(); k++) {
+        const int n = ks[k].ngp;
+        for (int ib = 0; ib < (n + 127) / 128; ib++)
+            for (int jb = 0; jb < (n + 31) / 32; jb++)
+                if (jb * 32 + 31 >= ib * 128) { t.push_back((int)k); t.push_back(ib); t.push_back(jb); }
+    }
+}
 
 int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
 {
     exs::build_gemm_tables(c, ks, c->gt);
+    std::vector<int> ozt;
+    if (c->prec_mode == EXS_PREC_OZAKI_INT8) oz_tiles(ks, ozt);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    size_t need = al(ks.size() * sizeof(KDesc));
+    size_t need = al(ks.size() * sizeof(KDesc)) + al(ozt.size() * sizeof(int));
     for (int q = 0; q < 4; q++)
         need += al(c->gt.probs[q].size() * sizeof(exs::GemmProb)) + al(c->gt.work[q].size() * sizeof(exs::TileWork));
     // the previous upload must have left the staging buffer
     EXS_CUDA(cudaEventSynchronize(c->tables_free));
     if (need > c->tables_bytes) {
-        if (c->h_tables) cudaFreeHost(c->h_tables);
+        if (c->d_oz) cudaFree(c->d_oz);
+    if (c->d_ozscale) cudaFree(c->d_ozscale);
+    if (c->fk_dev) cudaFree(c->fk_dev);
+    if (c->fk_tab_d) cudaFree(c->fk_tab_d);
+    if (c->fk_tab_h) cudaFreeHost(c->fk_tab_h);
+    if (c->h_tables) cudaFreeHost(c->h_tables);
         if (c->d_tables) cudaFree(c->d_tables);
         c->h_tables = c->d_tables = nullptr;
         c->tables_bytes = 0;
@@ -504,6 +556,10 @@ int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
         u.nwork[q] = (int)c->gt.work[q].size();
         off += al(wb);
     }
+    if (!ozt.empty()) std::memcpy(h + off, ozt.data(), ozt.size() * sizeof(int));
+    u.d_oztiles = d + off;
+    u.noztiles = (int)(ozt.size() / 3);
+    off += al(ozt.size() * sizeof(int));
     EXS_CUDA(cudaMemcpyAsync(c->d_tables, c->h_tables, off, cudaMemcpyHostToDevice, c->stream));
     EXS_CUDA(cudaEventRecord(c->tables_free, c->stream));
     return EXS_OK;
@@ -513,6 +569,7 @@ int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
 // If have_planes, the A planes are already in place (apwalm given).
 int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
 {
+    (void)cudaGetLastError();   // launch checks below read the last error: start clean
     cudaStream_t s = c->stream;
     const DevParams p = c->params();
     int ngp_max = 0;
@@ -527,16 +584,22 @@ int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
     EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
                                    u.nwork[exs::EPI_PLANAR], u.d_k, s));
     EXS_CUDA(cudaEventRecord(c->ev[2], s));
-    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
-                                   u.nwork[exs::EPI_HAM], u.d_k, s));
-    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_OVL, p, u.d_probs[exs::EPI_OVL], u.d_work[exs::EPI_OVL],
-                                   u.nwork[exs::EPI_OVL], u.d_k, s));
+    if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
+        EXS_CUDA(exs::launch_oz_prepare(p, u.d_k, (int)ks.size(), c->slices, c->kp8, s));
+        EXS_CUDA(exs::launch_oz_mma(p, u.d_k, u.d_oztiles, u.noztiles, c->slices, c->kp8, s));
+    } else {
+        EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
+                                       u.nwork[exs::EPI_HAM], u.d_k, s));
+        EXS_CUDA(exs::launch_gemm_kind(exs::EPI_OVL, p, u.d_probs[exs::EPI_OVL], u.d_work[exs::EPI_OVL],
+                                       u.nwork[exs::EPI_OVL], u.d_k, s));
+    }
     EXS_CUDA(cudaEventRecord(c->ev[3], s));
     EXS_CUDA(exs::launch_gemm_kind(exs::EPI_LOROWS, p, u.d_probs[exs::EPI_LOROWS], u.d_work[exs::EPI_LOROWS],
                                    u.nwork[exs::EPI_LOROWS], u.d_k, s));
     EXS_CUDA(exs::launch_olp_apwlo(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_CUDA(exs::launch_lolo_blocks(p, u.d_k, (int)ks.size(), s));
     EXS_CUDA(cudaEventRecord(c->ev[4], s));
+    c->timed = true;
     return EXS_OK;
 }
 
@@ -561,6 +624,8 @@ KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double 
         k.cr = k.ar;
         k.ci = k.ai;
     }
+    k.oz_slices = c->d_oz ? c->d_oz + (size_t)slot * c->oz_slot_bytes : nullptr;
+    k.oz_scale = c->d_ozscale ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
     return k;
 }
 
@@ -677,15 +742,6 @@ int exs_hamiltonandoverlapsetup(exs_ctx *c, int ngp, const exs_complex *apwalm, 
     EXS_CUDA(cudaMemcpyAsync(h, ks[0].h, bytes, cudaMemcpyDeviceToHost, s));
     EXS_CUDA(cudaMemcpyAsync(o, ks[0].o, bytes, cudaMemcpyDeviceToHost, s));
     return exs_synchronize(c);
-}
-
-int exs_forcek(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int nstfv, const exs_complex *evecfv,
-               int ldv, const double *evalfv, const double *occsv, double wkpt, const double *ffacg,
-               const double *vgc, double *forceibs)
-{
-    (void)ngp; (void)igpig; (void)vgpc; (void)nstfv; (void)evecfv; (void)ldv; (void)evalfv; (void)occsv;
-    (void)wkpt; (void)ffacg; (void)vgc; (void)forceibs;
-    return fail(c, EXS_ERR_STATE, "exs_forcek is not built into this library yet");
 }
 
 }  // extern "C"

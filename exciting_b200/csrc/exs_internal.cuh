@@ -15,6 +15,7 @@ namespace exs {
 enum : int {
     DEV_ERR_INDEX = 1,   // ivgig lookup outside the box
     DEV_WARN_SINGULAR = 2,
+    DEV_ERR_TIMEOUT = 4,  // a bounded wait in a kernel expired
 };
 
 // One atom's place in the device layouts.
@@ -38,6 +39,8 @@ struct KDesc {
     double *ar, *ai;         // A planes  [Kpad][npad]
     double *br, *bi;         // B = blockdiag(h_a) A planes
     double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
+    int8_t *oz_slices;       // split-precision path: int8 slices [6][S][npad][kp8]
+    double *oz_scale;        // split-precision path: column scales of A and B [2][npad]
 };
 
 // Constant per-context device parameters passed by value to kernels.
@@ -151,15 +154,25 @@ struct exs_ctx {
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
     exs_complex *d_apwalm = nullptr;   // (ngkmax, apwordmax, lmmaxapw, natmtot)
+    // IBS force / adjoint work space (grown on demand)
+    void *fk_dev = nullptr;
+    size_t fk_bytes = 0;
+    void *fk_tab_h = nullptr, *fk_tab_d = nullptr;
+    size_t fk_tab_hbytes = 0, fk_tab_dbytes = 0;
     // precision
     int prec_mode = EXS_PREC_FP64;
     int slices = 7;
+    int kp8 = 0;                 // K rounded up to 128 (int8 slice rows)
+    int8_t *d_oz = nullptr;      // int8 slices of all slots
+    double *d_ozscale = nullptr; // column scales of all slots
+    size_t oz_slot_bytes = 0;
     // runtime
     int device = 0;
     cudaStream_t stream = nullptr;      // stream the work runs on
     cudaStream_t own_stream = nullptr;  // the context's own stream
     cudaEvent_t ev[8] = {};
     double last_t[5] = {0, 0, 0, 0, 0};
+    bool timed = false;          // ev[0..4] recorded by the last setup call
     std::string last_error;
 
     exs::DevParams params() const;
@@ -179,4 +192,8 @@ cudaError_t launch_olp_apwlo(const DevParams &p, const KDesc *d_k, int nk, int n
 void build_gemm_tables(const exs_ctx *c, const std::vector<KDesc> &ks, GemmTables &t);
 cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, const void *d_work, int nwork,
                              const KDesc *d_k, cudaStream_t s);
+// Split-precision contraction (ozaki.cu)
+cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s);
+cudaError_t launch_oz_mma(const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8,
+                          cudaStream_t s);
 }  // namespace exs

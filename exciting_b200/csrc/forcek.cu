@@ -1,0 +1,574 @@
+// IBS force (src/forcek.f90) and the adjoint of the H/O setup on the device.
+//
+// The reference builds, per atom a and direction x, the full nmat x nmat
+// derivative matrices dlh and dlo (forcek.f90:262-287) and projects them on
+// the eigenvectors with three zgemm calls each (:295-337), i.e.
+// O(natoms * 3 * nmat^2 * nstfv).  Here the same quantity
+//     F(x, a) = sum_n w_n Re[ c_n^H (dlh + eps_n dlo) c_n ],  w_n = wkpt occ_n
+// is evaluated in factored form, never forming dlh/dlo:
+//   * MT APW-APW (dlh = i(G_i-G_j)_x H_a, dlo = -i(G_i-G_j)_x O_a):
+//       with U = A_a C_G and U_x = A_a V_x C_G (V_x = diag((k+G)_x)),
+//       term = sum_n w_n Re{ i (u_x^H h u - u^H h u_x) - i eps_n (u_x^H M u - u^H M u_x) }
+//       (M = 1, or 1 + h1aa for iora*; C_G the APW rows of the eigenvectors);
+//   * APW-lo (dlh = i(k+G_i)_x H_a(i, lo), dlo = -i(k+G_i)_x O_a(i, lo), mirrored):
+//       term = 2 Re sum_n w_n sum_j C_lo(j,n) conj( i (loa U_x)(j,n) - i eps_n (S U_x)(j,n) )^*
+//       with S the oalo(+h1loa) map of overlapsetup.f90:111-127;
+//   * interstitial step function (the zt1 = -ffacg conj(sfacg) terms):
+//       R_H(g) = sum_{G_i-G_j=g} dp_ij P(j,i), R_O(g) = sum_{G_i-G_j=g} Q(j,i),
+//       P = C_G W C_G^H, Q = C_G W eps C_G^H, then
+//       term = sum_g Re[ i g_x zt1_a(g) (R_H(g) - R_O(g)) ].
+// The scatter sums also give the gradient of L = sum_n w_n c_n^H (H - eps_n O) c_n
+// with respect to V(G), and U gives the gradient with respect to h_a.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "exs_internal.cuh"
+
+namespace exs {
+
+struct ForceWork {
+    int ngp, nst, nstp, ldt;         // ldt = Kpad (leading dim of At)
+    const KDesc *k;                  // A planes of the k-point (slot 0)
+    double *atr, *ati;               // At [G][f]
+    double *ct[4][2];                // Ct, Ct_x [G][n]  (q = 0: plain, 1..3: scaled by (k+G)_x)
+    double *cn[2], *wc[2], *wec[2];  // [n][G]
+    double *u[4][2];                 // U_q [f][n]
+    double *hu[4][2];                // h_a U_q
+    double *mu[4][2];                // M U_q (iora*) or == u
+    double *pt[2], *qt[2];           // P^T, Q^T [i][j], ld npad
+    exs_complex *evec;               // (nmat, nst) dense
+    const double *w, *eps;           // (nst)
+    exs_complex *rh, *ro, *rv;       // (ngvec)
+    const double *ffacg;             // (ngvec, nspecies)
+    const double *vgc;               // (3, ngvec)
+    double *force;                   // (3, natmtot)
+};
+
+__global__ void fk_transpose_a(int K, int ngp, int npad, int ldt, const double *ar, const double *ai, double *atr,
+                               double *ati)
+{
+    __shared__ double tr[32][33], ti[32][33];
+    const int f0 = blockIdx.y * 32, g0 = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int f = f0 + r, g = g0 + threadIdx.x;
+        tr[r][threadIdx.x] = (f < K && g < ngp) ? ar[(size_t)f * npad + g] : 0.0;
+        ti[r][threadIdx.x] = (f < K && g < ngp) ? ai[(size_t)f * npad + g] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int g = g0 + r, f = f0 + threadIdx.x;
+        if (g < ngp && f < K) {
+            atr[(size_t)g * ldt + f] = tr[threadIdx.x][r];
+            ati[(size_t)g * ldt + f] = ti[threadIdx.x][r];
+        }
+    }
+}
+
+// Eigenvector packings: Ct_q[G][n] (q=0 plain, q=1..3 times (k+G)_x),
+// C[n][G], w C[n][G], w eps C[n][G]; zero for n >= nst.
+__global__ void fk_pack_evec(ForceWork fw, int npad, const double *vgpc, int nmat)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = blockIdx.y;
+    if (g >= fw.ngp || n >= fw.nstp) return;
+    double re = 0.0, im = 0.0, w = 0.0, we = 0.0;
+    if (n < fw.nst) {
+        const exs_complex z = fw.evec[g + (size_t)nmat * n];
+        re = z.re;
+        im = z.im;
+        w = fw.w[n];
+        we = fw.w[n] * fw.eps[n];
+    }
+    const size_t it = (size_t)g * fw.nstp + n;
+    fw.ct[0][0][it] = re;
+    fw.ct[0][1][it] = im;
+    for (int x = 0; x < 3; x++) {
+        const double v = vgpc[3 * g + x];
+        fw.ct[1 + x][0][it] = v * re;
+        fw.ct[1 + x][1][it] = v * im;
+    }
+    const size_t in = (size_t)n * npad + g;
+    fw.cn[0][in] = re;
+    fw.cn[1][in] = im;
+    fw.wc[0][in] = w * re;
+    fw.wc[1][in] = w * im;
+    fw.wec[0][in] = we * re;
+    fw.wec[1][in] = we * im;
+}
+
+// M U_q = U_q + h1aa U_q per (l, m) block (overlapsetup.f90:72-87), iora* only.
+__global__ void fk_iora_u(DevParams p, ForceWork fw)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ias = blockIdx.y;
+    const int q = blockIdx.z;
+    if (n >= fw.nstp) return;
+    const AtomDesc at = p.atoms[ias];
+    const int *apw = p.apword + (size_t)(p.lmaxapw + 1) * at.species;
+    int f = at.apw_off;
+    for (int l = 0; l <= p.lmaxmat; l++) {
+        const int no = apw[l];
+        const double *h1 = p.h1aa + (size_t)p.apwordmax * p.apwordmax * (l + (size_t)(p.lmaxapw + 1) * ias);
+        for (int m = -l; m <= l; m++, f += no)
+            for (int io2 = 0; io2 < no; io2++) {
+                double re = fw.u[q][0][(size_t)(f + io2) * fw.nstp + n];
+                double im = fw.u[q][1][(size_t)(f + io2) * fw.nstp + n];
+                for (int io1 = 0; io1 < no; io1++) {
+                    const double w = h1[io1 + (size_t)p.apwordmax * io2];
+                    re += w * fw.u[q][0][(size_t)(f + io1) * fw.nstp + n];
+                    im += w * fw.u[q][1][(size_t)(f + io1) * fw.nstp + n];
+                }
+                fw.mu[q][0][(size_t)(f + io2) * fw.nstp + n] = re;
+                fw.mu[q][1][(size_t)(f + io2) * fw.nstp + n] = im;
+            }
+    }
+}
+
+__device__ inline double block_sum(double v, double *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += sh[i];
+    return s;
+}
+
+// conj(a) . b over the f rows [f0, f0+nf) of column n of two planar [f][n] arrays
+__device__ inline void cdot(const double *ar, const double *ai, const double *br, const double *bi, int f0, int nf,
+                            int ld, int n, double &re, double &im)
+{
+    re = 0.0;
+    im = 0.0;
+    for (int f = f0; f < f0 + nf; f++) {
+        const size_t i = (size_t)f * ld + n;
+        re += ar[i] * br[i] + ai[i] * bi[i];
+        im += ar[i] * bi[i] - ai[i] * br[i];
+    }
+}
+
+// MT APW-APW terms, one block per (atom, direction).
+__global__ void fk_terms_mt(DevParams p, ForceWork fw)
+{
+    __shared__ double sh[32];
+    const int ias = blockIdx.x, x = blockIdx.y;
+    const AtomDesc at = p.atoms[ias];
+    double acc = 0.0;
+    for (int n = threadIdx.x; n < fw.nst; n += blockDim.x) {
+        double zr, zi, z2r, z2i, yr, yi, y2r, y2i;
+        // z = u_x^H h u, z' = u^H h u_x, y = u_x^H M u, y' = u^H M u_x
+        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.hu[0][0], fw.hu[0][1], at.apw_off, at.napw, fw.nstp, n, zr, zi);
+        cdot(fw.u[0][0], fw.u[0][1], fw.hu[1 + x][0], fw.hu[1 + x][1], at.apw_off, at.napw, fw.nstp, n, z2r, z2i);
+        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.mu[0][0], fw.mu[0][1], at.apw_off, at.napw, fw.nstp, n, yr, yi);
+        cdot(fw.u[0][0], fw.u[0][1], fw.mu[1 + x][0], fw.mu[1 + x][1], at.apw_off, at.napw, fw.nstp, n, y2r, y2i);
+        // Re[i w (z - z')] + Re[-i w eps (y - y')]
+        acc += -fw.w[n] * (zi - z2i) + fw.w[n] * fw.eps[n] * (yi - y2i);
+    }
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) atomicAdd(&fw.force[x + 3 * ias], s);
+}
+
+// APW-lo terms, one block per (atom, direction); threads over (lo row, state).
+__global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, const double *loa_i, int ldlo, int maxaa)
+{
+    __shared__ double sh[32];
+    const int ias = blockIdx.x, x = blockIdx.y;
+    const AtomDesc at = p.atoms[ias];
+    const int is = at.species;
+    const int *apw = p.apword + (size_t)(p.lmaxapw + 1) * is;
+    const int nmat = fw.ngp + p.nlotot;
+    double acc = 0.0;
+    const double *uxr = fw.u[1 + x][0], *uxi = fw.u[1 + x][1];
+    for (int t = threadIdx.x; t < at.losize * fw.nst; t += blockDim.x) {
+        const int r = t % at.losize, n = t / at.losize;
+        // (loa U_x)(r, n)
+        double lr = 0.0, li = 0.0;
+        const double *lar = loa_r + (size_t)ldlo * maxaa * ias, *lai = loa_i + (size_t)ldlo * maxaa * ias;
+        for (int f = 0; f < at.napw; f++) {
+            const double ar = lar[r + (size_t)ldlo * f], ai = lai[r + (size_t)ldlo * f];
+            const size_t iu = (size_t)(at.apw_off + f) * fw.nstp + n;
+            lr += ar * uxr[iu] - ai * uxi[iu];
+            li += ar * uxi[iu] + ai * uxr[iu];
+        }
+        // (S U_x)(r, n): lo row r = (ilo, m), S picks the APW rows (l, m, io) with oalo(io, ilo)
+        int ilo = 0, base = 0, l = 0;
+        for (; ilo < p.nlorb[is]; ilo++) {
+            l = p.lorbl[ilo + p.nlomax * is];
+            if (r < base + 2 * l + 1) break;
+            base += 2 * l + 1;
+        }
+        const int m = r - base - l;
+        int f = at.apw_off;
+        for (int ll = 0; ll < l; ll++) f += (2 * ll + 1) * apw[ll];
+        f += (m + l) * apw[l];
+        double sr = 0.0, si = 0.0;
+        for (int io = 0; io < apw[l]; io++) {
+            double w = p.oalo[io + (size_t)p.apwordmax * (ilo + (size_t)p.nlomax * ias)];
+            if (p.h1loa) w += p.h1loa[io + (size_t)p.apwordmax * (ilo + (size_t)p.nlomax * ias)];
+            const size_t iu = (size_t)(f + io) * fw.nstp + n;
+            sr += w * uxr[iu];
+            si += w * uxi[iu];
+        }
+        const exs_complex cl = fw.evec[(size_t)(fw.ngp + at.lo_off + r) + (size_t)nmat * n];
+        // 2 Re[ i w cl conj(L) ] + 2 Re[ -i w eps cl conj(S) ];  Re(i z) = -Im z
+        const double im_l = cl.im * lr - cl.re * li;      // Im(cl * conj(L))
+        const double im_s = cl.im * sr - cl.re * si;      // Im(cl * conj(S))
+        acc += -2.0 * fw.w[n] * im_l + 2.0 * fw.w[n] * fw.eps[n] * im_s;
+    }
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) atomicAdd(&fw.force[x + 3 * ias], s);
+}
+
+// Scatter of P(j,i), dp_ij P(j,i) and Q(j,i) onto G_i - G_j (all i, j < ngp).
+__global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= fw.ngp) return;
+    const int gi = kd->igpig[i] - 1, gj = kd->igpig[j] - 1;
+    if (gi < 0 || gi >= p.ngrtot || gj < 0 || gj >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); return; }
+    const int d0 = p.ivg[3 * gi] - p.ivg[3 * gj] - p.intgv_lo[0];
+    const int d1 = p.ivg[3 * gi + 1] - p.ivg[3 * gj + 1] - p.intgv_lo[1];
+    const int d2 = p.ivg[3 * gi + 2] - p.ivg[3 * gj + 2] - p.intgv_lo[2];
+    if ((unsigned)d0 >= (unsigned)p.intgv_n[0] || (unsigned)d1 >= (unsigned)p.intgv_n[1] ||
+        (unsigned)d2 >= (unsigned)p.intgv_n[2]) {
+        atomicOr(p.err, DEV_ERR_INDEX);
+        return;
+    }
+    const int ig = p.ivgig[d0 + p.intgv_n[0] * (d1 + p.intgv_n[1] * d2)];
+    if (ig <= 0 || ig > p.ngvec) return;
+    const double *vi = kd->vgpc + 3 * i, *vj = kd->vgpc + 3 * j;
+    const double dp = 0.5 * (vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2]);
+    const size_t e = (size_t)i * p.npad + j;
+    const double pr = fw.pt[0][e], pi = fw.pt[1][e], qr = fw.qt[0][e], qi = fw.qt[1][e];
+    double *rh = reinterpret_cast<double *>(fw.rh + (ig - 1));
+    double *ro = reinterpret_cast<double *>(fw.ro + (ig - 1));
+    double *rv = reinterpret_cast<double *>(fw.rv + (ig - 1));
+    atomicAdd(rh, dp * pr);
+    atomicAdd(rh + 1, dp * pi);
+    atomicAdd(ro, qr);
+    atomicAdd(ro + 1, qi);
+    atomicAdd(rv, pr);
+    atomicAdd(rv + 1, pi);
+}
+
+// Interstitial step-function terms, one block per atom, the three directions.
+__global__ void fk_terms_theta(DevParams p, ForceWork fw, int ngvec)
+{
+    __shared__ double sh[32];
+    const int ias = blockIdx.x;
+    const AtomDesc at = p.atoms[ias];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int g = threadIdx.x; g < ngvec; g += blockDim.x) {
+        const double *v = fw.vgc + 3 * (size_t)g;
+        const double ff = fw.ffacg[g + (size_t)ngvec * at.species];
+        double s, c;
+        sincos(v[0] * at.pos[0] + v[1] * at.pos[1] + v[2] * at.pos[2], &s, &c);
+        // zt1 = -ffacg conj(sfacg) = -ff (c - i s)
+        const double zr = -ff * c, zi = ff * s;
+        const double dr = fw.rh[g].re - fw.ro[g].re, di = fw.rh[g].im - fw.ro[g].im;
+        const double im = zr * di + zi * dr;          // Im(zt1 * D)
+        for (int x = 0; x < 3; x++) acc[x] += -v[x] * im;   // Re(i g_x zt1 D) = -g_x Im(zt1 D)
+    }
+    for (int x = 0; x < 3; x++) {
+        const double s = block_sum(acc[x], sh);
+        if (threadIdx.x == 0) atomicAdd(&fw.force[x + 3 * ias], s);
+    }
+}
+
+// dL/dh_a(f, f') = sum_n w_n conj(U(f, n)) U(f', n) per atom, into (maxaa, maxaa, natmtot).
+__global__ void fk_dh(DevParams p, ForceWork fw, exs_complex *dh, int maxaa)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f2 = blockIdx.y;
+    const int ias = blockIdx.z;
+    if (f >= maxaa || f2 >= maxaa) return;
+    const AtomDesc at = p.atoms[ias];
+    double re = 0.0, im = 0.0;
+    if (f < at.napw && f2 < at.napw) {
+        const double *ur = fw.u[0][0], *ui = fw.u[0][1];
+        for (int n = 0; n < fw.nst; n++) {
+            const size_t a = (size_t)(at.apw_off + f) * fw.nstp + n, b = (size_t)(at.apw_off + f2) * fw.nstp + n;
+            re += fw.w[n] * (ur[a] * ur[b] + ui[a] * ui[b]);
+            im += fw.w[n] * (ur[a] * ui[b] - ui[a] * ur[b]);
+        }
+    }
+    exs_complex z;
+    z.re = re;
+    z.im = im;
+    dh[f + (size_t)maxaa * (f2 + (size_t)maxaa * ias)] = z;
+}
+
+}  // namespace exs
+
+// ---------------------------------------------------------------- host side
+namespace {
+
+using exs::ForceWork;
+using exs::GemmProb;
+using exs::KDesc;
+using exs::TileWork;
+
+int ffail(exs_ctx *c, int code, const char *msg)
+{
+    c->last_error = msg;
+    return code;
+}
+
+#define FK_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            c->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+            return EXS_ERR_CUDA;                                                           \
+        }                                                                                  \
+    } while (0)
+
+inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+cudaError_t grow(void **p, size_t *cap, size_t need, bool pinned)
+{
+    if (need <= *cap) return cudaSuccess;
+    if (*p) { if (pinned) cudaFreeHost(*p); else cudaFree(*p); }
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = pinned ? cudaMallocHost(p, need) : cudaMalloc(p, need);
+    if (e == cudaSuccess) *cap = need;
+    return e;
+}
+
+void add_tiles(std::vector<TileWork> &w, int pi, int M, int N, bool upper)
+{
+    const int tm = (M + 63) / 64, tn = (N + 63) / 64;
+    for (int a = 0; a < tm; a++)
+        for (int b = upper ? a : 0; b < tn; b++) w.push_back({pi, a, b});
+}
+
+// The whole adjoint of one k-point.  Fills c->fk_force (device, 3*natmtot),
+// the scatter sums and U; returns an EXS_ code.
+int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int nst, const exs_complex *evec, int ldv,
+                const double *w_host, const double *eps_host, const double *ffacg, const double *vgc,
+                ForceWork &fw, exs_complex **d_rv_out)
+{
+    cudaStream_t s = c->stream;
+    const int nmat = ngp + c->nlotot;
+    const int nstp = (nst + 1) / 2 * 2;
+    const int npad = c->npad, Kp = c->Kpad;
+    // ---- device work space
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = al256(off + bytes); return o; };
+    const size_t o_at = take(2 * sizeof(double) * (size_t)npad * Kp);
+    const size_t o_ct = take(8 * sizeof(double) * (size_t)npad * nstp);
+    const size_t o_cn = take(6 * sizeof(double) * (size_t)nstp * npad);
+    const size_t o_u = take(8 * sizeof(double) * (size_t)Kp * nstp);
+    const size_t o_hu = take(8 * sizeof(double) * (size_t)Kp * nstp);
+    const bool iora = c->relativity == EXS_REL_IORA;
+    const size_t o_mu = take(iora ? 8 * sizeof(double) * (size_t)Kp * nstp : 0);
+    const size_t o_pq = take(4 * sizeof(double) * (size_t)npad * npad);
+    const size_t o_ev = take(sizeof(exs_complex) * (size_t)nmat * nst);
+    const size_t o_we = take(2 * sizeof(double) * (size_t)nst);
+    const size_t o_r = take(3 * sizeof(exs_complex) * (size_t)c->ngvec);
+    const size_t o_ff = take(sizeof(double) * (size_t)c->ngvec * c->nspecies);
+    const size_t o_vg = take(3 * sizeof(double) * (size_t)c->ngvec);
+    const size_t o_f = take(3 * sizeof(double) * (size_t)c->natmtot);
+    FK_CUDA(cudaStreamSynchronize(s));
+    FK_CUDA(grow(&c->fk_dev, &c->fk_bytes, off, false));
+    char *b = (char *)c->fk_dev;
+    fw.ngp = ngp; fw.nst = nst; fw.nstp = nstp; fw.ldt = Kp;
+    fw.atr = (double *)(b + o_at); fw.ati = fw.atr + (size_t)npad * Kp;
+    for (int q = 0; q < 4; q++)
+        for (int r = 0; r < 2; r++) fw.ct[q][r] = (double *)(b + o_ct) + (size_t)(2 * q + r) * npad * nstp;
+    double *cn = (double *)(b + o_cn);
+    fw.cn[0] = cn; fw.cn[1] = cn + (size_t)nstp * npad;
+    fw.wc[0] = cn + 2 * (size_t)nstp * npad; fw.wc[1] = cn + 3 * (size_t)nstp * npad;
+    fw.wec[0] = cn + 4 * (size_t)nstp * npad; fw.wec[1] = cn + 5 * (size_t)nstp * npad;
+    for (int q = 0; q < 4; q++)
+        for (int r = 0; r < 2; r++) {
+            fw.u[q][r] = (double *)(b + o_u) + (size_t)(2 * q + r) * Kp * nstp;
+            fw.hu[q][r] = (double *)(b + o_hu) + (size_t)(2 * q + r) * Kp * nstp;
+            fw.mu[q][r] = iora ? (double *)(b + o_mu) + (size_t)(2 * q + r) * Kp * nstp : fw.u[q][r];
+        }
+    double *pq = (double *)(b + o_pq);
+    fw.pt[0] = pq; fw.pt[1] = pq + (size_t)npad * npad;
+    fw.qt[0] = pq + 2 * (size_t)npad * npad; fw.qt[1] = pq + 3 * (size_t)npad * npad;
+    fw.evec = (exs_complex *)(b + o_ev);
+    double *we = (double *)(b + o_we);
+    fw.w = we;
+    fw.eps = we + nst;
+    fw.rh = (exs_complex *)(b + o_r);
+    fw.ro = fw.rh + c->ngvec;
+    fw.rv = fw.ro + c->ngvec;
+    fw.ffacg = (const double *)(b + o_ff);
+    fw.vgc = (const double *)(b + o_vg);
+    fw.force = (double *)(b + o_f);
+    *d_rv_out = fw.rv;
+
+    // ---- uploads
+    FK_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+    FK_CUDA(cudaMemcpyAsync(c->d_igpig, igpig, sizeof(int) * ngp, cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemcpyAsync(c->d_vgpc, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemcpy2DAsync(fw.evec, sizeof(exs_complex) * nmat, evec, sizeof(exs_complex) * ldv,
+                              sizeof(exs_complex) * nmat, nst, cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemcpyAsync(we, w_host, sizeof(double) * nst, cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemcpyAsync(we + nst, eps_host, sizeof(double) * nst, cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemcpyAsync((void *)fw.ffacg, ffacg, sizeof(double) * (size_t)c->ngvec * c->nspecies,
+                            cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemcpyAsync((void *)fw.vgc, vgc, 3 * sizeof(double) * (size_t)c->ngvec, cudaMemcpyHostToDevice, s));
+    FK_CUDA(cudaMemsetAsync(fw.rh, 0, 3 * sizeof(exs_complex) * (size_t)c->ngvec, s));
+    FK_CUDA(cudaMemsetAsync(fw.force, 0, 3 * sizeof(double) * (size_t)c->natmtot, s));
+
+    // ---- k descriptor (slot 0 work planes) and GEMM tables, one upload
+    KDesc kd{};
+    kd.ngp = ngp;
+    kd.nmat = nmat;
+    kd.igpig = c->d_igpig;
+    kd.vgpc = c->d_vgpc;
+    double *wk = c->d_work;
+    kd.ar = wk; kd.ai = wk + c->plane; kd.br = wk + 2 * c->plane; kd.bi = wk + 3 * c->plane;
+    kd.cr = kd.ar; kd.ci = kd.ai;
+    std::vector<GemmProb> probs;
+    std::vector<TileWork> w1, w2;
+    for (int q = 0; q < 4; q++) {              // U_q = A C_q   (contraction over G)
+        GemmProb P{};
+        P.xr = fw.atr; P.xi = fw.ati; P.ldx = Kp;
+        P.yr = fw.ct[q][0]; P.yi = fw.ct[q][1]; P.ldy = nstp;
+        P.M = c->K; P.N = nstp; P.K = ngp; P.conjx = 0;
+        P.outr = fw.u[q][0]; P.outi = fw.u[q][1]; P.ldo = nstp;
+        add_tiles(w1, (int)probs.size(), P.M, P.N, false);
+        probs.push_back(P);
+    }
+    for (int which = 0; which < 2; which++) {  // P^T = conj(C)^T (w C), Q^T = conj(C)^T (w eps C)
+        GemmProb P{};
+        P.xr = fw.cn[0]; P.xi = fw.cn[1]; P.ldx = npad;
+        P.yr = which == 0 ? fw.wc[0] : fw.wec[0]; P.yi = which == 0 ? fw.wc[1] : fw.wec[1]; P.ldy = npad;
+        P.M = ngp; P.N = ngp; P.K = nst; P.conjx = 1;
+        P.outr = which == 0 ? fw.pt[0] : fw.qt[0]; P.outi = which == 0 ? fw.pt[1] : fw.qt[1]; P.ldo = npad;
+        add_tiles(w1, (int)probs.size(), P.M, P.N, false);
+        probs.push_back(P);
+    }
+    for (int q = 0; q < 4; q++)                // h_a U_q per atom
+        for (int ias = 0; ias < c->natmtot; ias++) {
+            const exs::AtomDesc &a = c->atoms[ias];
+            GemmProb P{};
+            P.xr = c->d_haa_r + (size_t)ias * c->ldh * c->ldh; P.xi = c->d_haa_i + (size_t)ias * c->ldh * c->ldh;
+            P.ldx = c->ldh;
+            P.yr = fw.u[q][0] + (size_t)a.apw_off * nstp; P.yi = fw.u[q][1] + (size_t)a.apw_off * nstp; P.ldy = nstp;
+            P.M = a.napw; P.N = nstp; P.K = a.napw; P.conjx = 0;
+            P.outr = fw.hu[q][0] + (size_t)a.apw_off * nstp; P.outi = fw.hu[q][1] + (size_t)a.apw_off * nstp;
+            P.ldo = nstp;
+            add_tiles(w2, (int)probs.size(), P.M, P.N, false);
+            probs.push_back(P);
+        }
+    const size_t kb = al256(sizeof(KDesc)), pb = al256(sizeof(GemmProb) * probs.size());
+    const size_t wb = sizeof(TileWork) * (w1.size() + w2.size());
+    const size_t tb = kb + pb + wb;
+    FK_CUDA(grow(&c->fk_tab_h, &c->fk_tab_hbytes, tb, true));
+    FK_CUDA(grow(&c->fk_tab_d, &c->fk_tab_dbytes, tb, false));
+    char *th = (char *)c->fk_tab_h;
+    std::memcpy(th, &kd, sizeof(KDesc));
+    std::memcpy(th + kb, probs.data(), sizeof(GemmProb) * probs.size());
+    std::memcpy(th + kb + pb, w1.data(), sizeof(TileWork) * w1.size());
+    std::memcpy(th + kb + pb + sizeof(TileWork) * w1.size(), w2.data(), sizeof(TileWork) * w2.size());
+    FK_CUDA(cudaMemcpyAsync(c->fk_tab_d, th, tb, cudaMemcpyHostToDevice, s));
+    char *td = (char *)c->fk_tab_d;
+    const KDesc *d_k = (const KDesc *)td;
+    const GemmProb *d_p = (const GemmProb *)(td + kb);
+    const TileWork *d_w1 = (const TileWork *)(td + kb + pb);
+    const TileWork *d_w2 = d_w1 + w1.size();
+
+    // ---- launches
+    (void)cudaGetLastError();   // launch checks below read the last error: start clean
+    const exs::DevParams p = c->params();
+    FK_CUDA(exs::launch_match_planes(p, d_k, 1, ngp, s));
+    {
+        dim3 blk(32, 8), grd((ngp + 31) / 32, (c->K + 31) / 32);
+        exs::fk_transpose_a<<<grd, blk, 0, s>>>(c->K, ngp, npad, Kp, kd.ar, kd.ai, fw.atr, fw.ati);
+        exs::fk_pack_evec<<<dim3((ngp + 127) / 128, nstp), 128, 0, s>>>(fw, npad, c->d_vgpc, nmat);
+        FK_CUDA(cudaGetLastError());
+    }
+    FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_w1, (int)w1.size(), d_k, s));
+    FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_w2, (int)w2.size(), d_k, s));
+    if (iora) exs::fk_iora_u<<<dim3((nstp + 63) / 64, c->natmtot, 4), 64, 0, s>>>(p, fw);
+    exs::fk_terms_mt<<<dim3(c->natmtot, 3), 128, 0, s>>>(p, fw);
+    if (c->nlotot > 0)
+        exs::fk_terms_lo<<<dim3(c->natmtot, 3), 256, 0, s>>>(p, fw, c->d_loa_r, c->d_loa_i, c->ldlo, c->maxaa);
+    exs::fk_scatter<<<dim3((ngp + 127) / 128, ngp), 128, 0, s>>>(p, fw, d_k);
+    exs::fk_terms_theta<<<c->natmtot, 256, 0, s>>>(p, fw, c->ngvec);
+    FK_CUDA(cudaGetLastError());
+    return EXS_OK;
+}
+
+int check_adjoint_args(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int nst, const exs_complex *evec,
+                       int ldv, const double *ffacg, const double *vgc)
+{
+    if (!igpig || !vgpc || !evec || !ffacg || !vgc) return ffail(c, EXS_ERR_ARG, "null argument");
+    if (ngp <= 0 || ngp > c->ngkmax) return ffail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax");
+    if (nst <= 0 || ldv < ngp + c->nlotot) return ffail(c, EXS_ERR_ARG, "nstfv <= 0 or ldv < nmat");
+    if (!c->have_inputs) return ffail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    for (int i = 0; i < ngp; i++)
+        if (igpig[i] < 1 || igpig[i] > c->ngrtot) return ffail(c, EXS_ERR_INDEX, "igpig entry outside 1..ngrtot");
+    return EXS_OK;
+}
+
+}  // namespace
+
+extern "C" int exs_forcek(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int nstfv,
+                          const exs_complex *evecfv, int ldv, const double *evalfv, const double *occsv,
+                          double wkpt, const double *ffacg, const double *vgc, double *forceibs)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (!evalfv || !occsv || !forceibs) return ffail(c, EXS_ERR_ARG, "null argument");
+    int rc = check_adjoint_args(c, ngp, igpig, vgpc, nstfv, evecfv, ldv, ffacg, vgc);
+    if (rc != EXS_OK) return rc;
+    cudaSetDevice(c->device);
+    std::vector<double> w(nstfv);
+    for (int n = 0; n < nstfv; n++) w[n] = wkpt * occsv[n];
+    ForceWork fw{};
+    exs_complex *rv = nullptr;
+    rc = run_adjoint(c, ngp, igpig, vgpc, nstfv, evecfv, ldv, w.data(), evalfv, ffacg, vgc, fw, &rv);
+    if (rc != EXS_OK) return rc;
+    std::vector<double> f(3 * (size_t)c->natmtot);
+    FK_CUDA(cudaMemcpyAsync(f.data(), fw.force, sizeof(double) * f.size(), cudaMemcpyDeviceToHost, c->stream));
+    rc = exs_synchronize(c);
+    if (rc < 0) return rc;
+    for (size_t i = 0; i < f.size(); i++) forceibs[i] += f[i];    // forcek accumulates (forcek.f90:373-383)
+    return rc;
+}
+
+extern "C" int exs_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int nst, const exs_complex *cvec,
+                           int ldv, const double *w, const double *eps, const double *ffacg, const double *vgc,
+                           double *dtau, exs_complex *dveffig, exs_complex *dh)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (!w || !eps || !dtau) return ffail(c, EXS_ERR_ARG, "null argument");
+    int rc = check_adjoint_args(c, ngp, igpig, vgpc, nst, cvec, ldv, ffacg, vgc);
+    if (rc != EXS_OK) return rc;
+    cudaSetDevice(c->device);
+    ForceWork fw{};
+    exs_complex *rv = nullptr;
+    rc = run_adjoint(c, ngp, igpig, vgpc, nst, cvec, ldv, w, eps, ffacg, vgc, fw, &rv);
+    if (rc != EXS_OK) return rc;
+    cudaStream_t s = c->stream;
+    std::vector<double> f(3 * (size_t)c->natmtot);
+    FK_CUDA(cudaMemcpyAsync(f.data(), fw.force, sizeof(double) * f.size(), cudaMemcpyDeviceToHost, s));
+    if (dveffig)
+        FK_CUDA(cudaMemcpyAsync(dveffig, rv, sizeof(exs_complex) * (size_t)c->ngvec, cudaMemcpyDeviceToHost, s));
+    exs_complex *d_dh = nullptr;
+    if (dh) {
+        const size_t n = (size_t)c->maxaa * c->maxaa * c->natmtot;
+        FK_CUDA(cudaMalloc(&d_dh, sizeof(exs_complex) * n));
+        exs::fk_dh<<<dim3((c->maxaa + 63) / 64, c->maxaa, c->natmtot), 64, 0, s>>>(c->params(), fw, d_dh, c->maxaa);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dh, d_dh, sizeof(exs_complex) * n, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) { cudaFree(d_dh); return ffail(c, EXS_ERR_CUDA, cudaGetErrorString(e)); }
+    }
+    rc = exs_synchronize(c);
+    if (d_dh) cudaFree(d_dh);
+    if (rc < 0) return rc;
+    for (size_t i = 0; i < f.size(); i++) dtau[i] = -f[i];          // dL/dtau = -F_IBS
+    return rc;
+}

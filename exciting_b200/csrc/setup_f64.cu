@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "exs_internal.cuh"
+#include "interstitial.cuh"
 
 namespace exs {
 
@@ -41,7 +42,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }
@@ -71,43 +72,6 @@ __device__ __forceinline__ void load_stage(double *st, const GemmProb &P, int m0
             cp_async16(st + 3 * GB_PLANE + row * GB_LDS + col, P.yi + off, v);
         }
     }
-}
-
-// Interstitial term of element (i, j), i <= j < ngp (hmlistln.f90:61-86,
-// olpistln.f90:53-82).  Returns false when nothing is added.
-__device__ __forceinline__ bool interstitial(const DevParams &p, int kind, const int *ivi, const int *ivj,
-                                             const double *vi, const double *vj, double &zr, double &zi)
-{
-    const int d0 = ivi[0] - ivj[0] - p.intgv_lo[0];
-    const int d1 = ivi[1] - ivj[1] - p.intgv_lo[1];
-    const int d2 = ivi[2] - ivj[2] - p.intgv_lo[2];
-    if ((unsigned)d0 >= (unsigned)p.intgv_n[0] || (unsigned)d1 >= (unsigned)p.intgv_n[1] ||
-        (unsigned)d2 >= (unsigned)p.intgv_n[2]) {
-        atomicOr(p.err, DEV_ERR_INDEX);
-        return false;
-    }
-    const int ig = p.ivgig[d0 + p.intgv_n[0] * (d1 + p.intgv_n[1] * d2)];
-    if (ig <= 0 || ig > p.ngvec) return false;
-    const double dp = vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2];
-    if (kind == EPI_HAM) {
-        const double t1 = 0.5 * dp;
-        const exs_complex v = p.veffig[ig - 1], w = p.kinw[ig - 1];
-        zr = v.re + t1 * w.re;
-        zi = v.im + t1 * w.im;
-    } else {
-        const exs_complex c = p.cfunig[ig - 1];
-        if (p.relativity == EXS_REL_IORA) {
-            const double alpha = 1.0 / 137.03599911, a2 = 0.5 * alpha * alpha;
-            const double t1 = 0.5 * a2 * dp;
-            const exs_complex w = p.m2effig[ig - 1];
-            zr = t1 * w.re + c.re;
-            zi = t1 * w.im + c.im;
-        } else {
-            zr = c.re;
-            zi = c.im;
-        }
-    }
-    return true;
 }
 
 template <int KIND>
@@ -160,15 +124,24 @@ zgemm_dmma_kernel(DevParams p, const GemmProb *probs, const TileWork *work, cons
                 br[j] = st[2 * GB_PLANE + kr * GB_LDS + nn];
                 bi[j] = st[3 * GB_PLANE + kr * GB_LDS + nn];
             }
+            // four passes over the 4x4 sub-tiles so that the two products
+            // accumulated into one register pair are 16 DMMAs apart
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    dmma(cre[i][j][0], cre[i][j][1], ar[i], br[j]);
-                    dmma(cre[i][j][0], cre[i][j][1], aim[i], bi[j]);
-                    dmma(cim[i][j][0], cim[i][j][1], ar[i], bi[j]);
-                    dmma(cim[i][j][0], cim[i][j][1], naim[i], br[j]);
-                }
+                for (int j = 0; j < 4; j++) dmma(cre[i][j][0], cre[i][j][1], ar[i], br[j]);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(cim[i][j][0], cim[i][j][1], ar[i], bi[j]);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(cre[i][j][0], cre[i][j][1], aim[i], bi[j]);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(cim[i][j][0], cim[i][j][1], naim[i], br[j]);
         }
     }
     cp_async_wait<0>();

@@ -143,6 +143,20 @@ int exs_forcek(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc,
                const double *occsv, double wkpt, const double *ffacg, const double *vgc,
                double *forceibs);
 
+/* Adjoint of the setup for L = sum_n w_n c_n^H (H - eps_n O) c_n with the
+ * weighted factors given (no counterpart routine in the reference; it
+ * generalises forcek.f90): c(ldv, nst) with nmat = ngp + nlotot rows,
+ * w(nst), eps(nst); ffacg(ngvec, nspecies), vgc(3, ngvec) as for exs_forcek.
+ * Outputs (overwritten): dtau(3, natmtot) = dL/dtau (= -F_IBS);
+ * dveffig(ngvec) (may be NULL): for any perturbation with
+ * dV(-G) = conj dV(G), dL = sum_g dveffig(g) dV(g);
+ * dh(maxaa, maxaa, natmtot) (may be NULL): dL = sum dh(f,f',a) d aa(f,f',a)
+ * for Hermitian perturbations of mt_hscf%main%aa. */
+int exs_adjoint(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc, int nst,
+                const exs_complex *c, int ldv, const double *w, const double *eps,
+                const double *ffacg, const double *vgc, double *dtau,
+                exs_complex *dveffig, exs_complex *dh);
+
 /* Run the context's work on a caller-owned CUDA stream (a cudaStream_t
  * passed as void*); NULL returns to the context's own stream. */
 int exs_set_stream(exs_ctx *ctx, void *stream);
