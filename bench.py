@@ -106,6 +106,42 @@ def _measured_fp64_peak(torch):
     return best
 
 
+def _measured_int8_peak(torch):
+    """cuBLASLt int8 GEMM 8192^3 rate (TOP/s, torch._int_mm): the int8 tensor roofline denominator."""
+    a = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+    b = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+    for _ in range(2):
+        torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def ozaki_int8_ops(sys_, gks, slices):
+    """int8 MMA operations the split-precision kernel issues: per 128 x 32 tile
+    (4 outputs -> N = 128), S(S+1)/2 slice pairs x 2 x 128 x 128 x K', K' = 2 kp8."""
+    K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
+    kp8 = (K + 127) // 128 * 128
+    pairs = slices * (slices + 1) // 2
+    tiles = 0
+    for g in gks:
+        n = g.ngp
+        for ib in range((n + 127) // 128):
+            for jb in range((n + 31) // 32):
+                if jb * 32 + 31 >= ib * 128:
+                    tiles += 1
+    return tiles * pairs * 2.0 * 128 * 128 * 2 * kp8
+
+
 def main_flops(sys_, gks):
     """Algorithmic flops of the MT contraction stage (upper triangles of A^H B and A^H A):
     sum over k of 8 N (N+1) K, K = sum_a m_a."""
@@ -236,6 +272,8 @@ def run_ours(args):
     gks = s.gksets()[: args.nk]
     nk = len(gks)
     st = Setup(s, max_batch=nk)
+    if args.precision == "ozaki":
+        st.set_precision("ozaki", args.slices)
     stream = torch.cuda.Stream()
     st.set_stream(stream.cuda_stream)
     ngkmax, nlotot = st.ngkmax, st.nlotot
@@ -293,11 +331,69 @@ def run_ours(args):
     else:
         e2e_value, h2d, d2h = _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier)
 
+    # ---- split precision: its error against the native FP64 path (k-point 0)
+    # and the FP64 path's own device-resident rate for comparison
+    accuracy, fp64_value = None, None
+    if args.precision == "ozaki":
+        st.setup_batched_device(ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op)
+        st.synchronize()
+        h_oz = d_h[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
+        o_oz = d_o[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
+        st.set_precision("fp64")
+        for _ in range(2):
+            step_device()
+        st.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                step_device()
+            st.synchronize()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fp64_value = ws * nk * args.steps / (float(t.item()) * 1e-3)
+        h64 = d_h[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
+        o64 = d_o[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
+        if rank == 0:
+            import scipy.linalg as sl
+            w = sl.eigh(h_oz, o_oz, eigvals_only=True, subset_by_index=[0, 39])
+            wr = sl.eigh(h64, o64, eigvals_only=True, subset_by_index=[0, 39])
+            small = np.abs(wr) <= 1.0
+            accuracy = {
+                "against": "native FP64 GPU path (itself within 1e-14 of the CPU oracle), k-point 0",
+                "rel_fro_H": float(np.linalg.norm(h_oz - h64) / np.linalg.norm(h64)),
+                "rel_fro_O": float(np.linalg.norm(o_oz - o64) / np.linalg.norm(o64)),
+                "max_abs_eig_dev_lowest40_Ha": float(np.max(np.abs(w - wr))),
+                "max_rel_eig_dev_lowest40": float(np.max(np.abs(w - wr) / np.maximum(1.0, np.abs(wr)))),
+                "max_abs_eig_dev_abs_le_1Ha": float(np.max(np.abs(w - wr)[small])) if small.any() else None,
+            }
+
     if rank == 0:
         fl = main_flops(s, gks)
         main_ms = phase[2]
         peak64 = _measured_fp64_peak(torch)
         achieved = fl / (main_ms * 1e-3) / 1e12
+        if args.precision == "ozaki":
+            ops = ozaki_int8_ops(s, gks, args.slices)
+            peak8 = _measured_int8_peak(torch)
+            a8 = ops / (main_ms * 1e-3) / 1e12
+            roof = {"bound": "tensor", "kernel": "oz_mma_kernel (tcgen05.mma kind::i8, MT contraction)",
+                    "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
+                    "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
+                    "int8_ops_per_step": ops, "traffic": None,
+                    "fp64_equivalent": {"achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                                        "frac": achieved / peak64,
+                                        "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}}
+        else:
+            roof = {"bound": "tensor", "kernel": "zgemm_dmma_kernel<EPI_HAM>+<EPI_OVL> (MT contraction)",
+                    "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in "
+                                   "MEASURED_PEAKS.json)",
+                    "algorithmic_flops_per_step": fl, "traffic": None}
         clocks = _clock_summary(rows, local)
         cpu_v, cpu_n, cpu_dt = (None, 0, 0.0) if args.skip_cpu else cpu_sample(s, gks, budget_s=12.0)
         out = {
@@ -305,18 +401,16 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "k_per_step": nk, "ngp": [min(ngp), max(ngp)],
-                       "nmat": [min(nmat), max(nmat)], "precision": "fp64 (DMMA)",
+                       "nmat": [min(nmat), max(nmat)],
+                       "precision": ("split int8 x%d slices (tcgen05), FP64 recombination" % args.slices
+                                     if args.precision == "ozaki" else "fp64 (DMMA)"),
                        "l2": "working set > 126 MB L2 (A/B planes 63 MB and H/O 48 MB per k-point), no flush"},
             "e2e": None if e2e_value is None else {
                 "value": e2e_value, "unit": "setups/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
-            "roofline": {"bound": "tensor", "kernel": "zgemm_dmma_kernel<EPI_HAM>+<EPI_OVL> (MT contraction)",
-                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in "
-                                        "MEASURED_PEAKS.json)",
-                         "algorithmic_flops_per_step": fl, "traffic": None},
+            "roofline": roof,
             "cpu_baseline": None if cpu_v is None else {
                 "value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
                 "sample": f"{cpu_n} k-points of the 27-k set in {cpu_dt:.1f} s by the FP64 CPU "
@@ -324,6 +418,8 @@ def run_ours(args):
             "clocks": clocks,
             "gpu_launches": 7 * args.steps,
             "setup_flops_per_step": setup_flops(s, gks),
+            "accuracy": accuracy,
+            "fp64_path_value": fp64_value,
         }
         print(json.dumps(out), flush=True)
     st.set_stream(None)
@@ -343,6 +439,9 @@ def main():
     ap.add_argument("--nk", type=int, default=27, help="k-points per step (profiling runs use fewer)")
     ap.add_argument("--skip-cpu", action="store_true", help="no CPU-baseline leg (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="no host-pointer leg (profiling runs)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki"],
+                    help="MT contraction arithmetic")
+    ap.add_argument("--slices", type=int, default=7, help="int8 slices per operand (ozaki)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

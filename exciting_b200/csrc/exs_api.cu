@@ -2,6 +2,7 @@
 // replace the reference's match / hamiltonandoverlapsetup calls.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -137,6 +138,9 @@ int exs_ctx_destroy(exs_ctx *c)
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->tables_free) cudaEventDestroy(c->tables_free);
+    for (auto &e : c->ev_group)
+        if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return EXS_OK;
@@ -274,6 +278,12 @@ int exs_ctx_create(const exs_config *cfg, exs_ctx **out)
         return EXS_ERR_CUDA;
     }
     c->stream = c->own_stream;
+    if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        exs_ctx_destroy(c);
+        return EXS_ERR_CUDA;
+    }
+    cudaEventCreateWithFlags(&c->ev_group[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_group[1], cudaEventDisableTiming);
     for (auto &ev : c->ev) cudaEventCreate(&ev);
     cudaEventCreateWithFlags(&c->tables_free, cudaEventDisableTiming);
     cudaStream_t s = c->stream;
@@ -330,6 +340,17 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     }
     c->kp8 = kp8;
     c->oz_slot_bytes = slot;
+    {   // EXS_OZAKI_KERNEL=cpasync selects the single-role cp.async kernel (comparison runs)
+        const char *kv = getenv("EXS_OZAKI_KERNEL");
+        c->oz_ws = !(kv && std::strcmp(kv, "cpasync") == 0);
+    }
+    if (!exs::make_oz_tensor_maps(c->d_oz, (size_t)6 * slices * c->npad * c->max_batch, kp8, &c->oz_mapA,
+                                  &c->oz_mapB)) {
+        cudaFree(c->d_oz); c->d_oz = nullptr;
+        cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
+        c->prec_mode = EXS_PREC_FP64;
+        return fail(c, EXS_ERR_CUDA, "cuTensorMapEncodeTiled failed for the slice array");
+    }
     c->slices = slices;
     c->prec_mode = mode;
     return EXS_OK;
@@ -525,12 +546,7 @@ int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
     // the previous upload must have left the staging buffer
     EXS_CUDA(cudaEventSynchronize(c->tables_free));
     if (need > c->tables_bytes) {
-        if (c->d_oz) cudaFree(c->d_oz);
-    if (c->d_ozscale) cudaFree(c->d_ozscale);
-    if (c->fk_dev) cudaFree(c->fk_dev);
-    if (c->fk_tab_d) cudaFree(c->fk_tab_d);
-    if (c->fk_tab_h) cudaFreeHost(c->fk_tab_h);
-    if (c->h_tables) cudaFreeHost(c->h_tables);
+        if (c->h_tables) cudaFreeHost(c->h_tables);
         if (c->d_tables) cudaFree(c->d_tables);
         c->h_tables = c->d_tables = nullptr;
         c->tables_bytes = 0;
@@ -586,7 +602,11 @@ int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
     EXS_CUDA(cudaEventRecord(c->ev[2], s));
     if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
         EXS_CUDA(exs::launch_oz_prepare(p, u.d_k, (int)ks.size(), c->slices, c->kp8, s));
-        EXS_CUDA(exs::launch_oz_mma(p, u.d_k, u.d_oztiles, u.noztiles, c->slices, c->kp8, s));
+        if (c->oz_ws)
+            EXS_CUDA(exs::launch_oz_mma_ws(&c->oz_mapA, &c->oz_mapB, p, u.d_k, u.d_oztiles, u.noztiles, c->slices,
+                                           c->kp8, s));
+        else
+            EXS_CUDA(exs::launch_oz_mma(p, u.d_k, u.d_oztiles, u.noztiles, c->slices, c->kp8, s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
                                        u.nwork[exs::EPI_HAM], u.d_k, s));
@@ -626,6 +646,7 @@ KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double 
     }
     k.oz_slices = c->d_oz ? c->d_oz + (size_t)slot * c->oz_slot_bytes : nullptr;
     k.oz_scale = c->d_ozscale ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
+    k.oz_row0 = slot * 6 * c->slices * c->npad;
     return k;
 }
 
@@ -673,6 +694,7 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
     for (int k0 = 0; k0 < nk; k0 += c->max_batch) {
         const int nb = std::min(c->max_batch, nk - k0);
         EXS_CUDA(cudaStreamSynchronize(s));
+        EXS_CUDA(cudaStreamSynchronize(c->copy_stream));
         std::memcpy(c->h_igpig_pinned, igpig + (size_t)c->ngkmax * k0, sizeof(int) * (size_t)c->ngkmax * nb);
         std::memcpy(c->h_vgpc_pinned, vgpc + 3 * (size_t)c->ngkmax * k0, sizeof(double) * 3 * (size_t)c->ngkmax * nb);
         EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
@@ -680,20 +702,42 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
                                  cudaMemcpyHostToDevice, s));
         EXS_CUDA(cudaMemcpyAsync(c->d_vgpc, c->h_vgpc_pinned, sizeof(double) * 3 * (size_t)c->ngkmax * nb,
                                  cudaMemcpyHostToDevice, s));
-        std::vector<KDesc> ks;
+        std::vector<KDesc> all;
         for (int k = 0; k < nb; k++) {
             exs_complex *dh = c->d_ho + (size_t)2 * k * c->nmatmax * c->nmatmax;
             exs_complex *dob = dh + (size_t)c->nmatmax * c->nmatmax;
-            ks.push_back(slot_desc(c, k, ngp[k0 + k], c->d_igpig + (size_t)c->ngkmax * k,
-                                   c->d_vgpc + 3 * (size_t)c->ngkmax * k, dh, dob));
+            all.push_back(slot_desc(c, k, ngp[k0 + k], c->d_igpig + (size_t)c->ngkmax * k,
+                                    c->d_vgpc + 3 * (size_t)c->ngkmax * k, dh, dob));
         }
-        int rc = run_setup(c, ks, false);
+        // Groups of k-points: the device-to-host copies of group g run on the
+        // copy stream while group g+1 is set up on the compute stream.
+        const int ngroups = nb >= 8 ? 4 : (nb >= 2 ? 2 : 1);
+        const int per = (nb + ngroups - 1) / ngroups;
+        auto group = [&](int g) {
+            const int a = g * per, e = std::min(nb, a + per);
+            return std::vector<KDesc>(all.begin() + a, all.begin() + e);
+        };
+        int rc = EXS_OK;
+        std::vector<KDesc> cur = group(0);
+        rc = run_setup(c, cur, false);
         if (rc < 0) return rc;
-        for (int k = 0; k < nb; k++) {
-            const size_t bytes = sizeof(exs_complex) * (size_t)ks[k].nmat * ks[k].nmat;
-            EXS_CUDA(cudaMemcpyAsync(h[k0 + k], ks[k].h, bytes, cudaMemcpyDeviceToHost, s));
-            EXS_CUDA(cudaMemcpyAsync(o[k0 + k], ks[k].o, bytes, cudaMemcpyDeviceToHost, s));
+        for (int g = 0; g < ngroups && g * per < nb; g++) {
+            EXS_CUDA(cudaEventRecord(c->ev_group[g & 1], s));
+            if ((g + 1) * per < nb) {           // enqueue the next group before copying this one
+                std::vector<KDesc> nxt = group(g + 1);
+                rc = run_setup(c, nxt, false);
+                if (rc < 0) return rc;
+            }
+            EXS_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_group[g & 1], 0));
+            for (const KDesc &k : cur) {
+                const int kk = k0 + (int)(&k - &cur[0]) + g * per;
+                const size_t bytes = sizeof(exs_complex) * (size_t)k.nmat * k.nmat;
+                EXS_CUDA(cudaMemcpyAsync(h[kk], k.h, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+                EXS_CUDA(cudaMemcpyAsync(o[kk], k.o, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+            }
+            if ((g + 1) * per < nb) cur = group(g + 1);
         }
+        EXS_CUDA(cudaStreamSynchronize(c->copy_stream));
         rc = exs_synchronize(c);
         if (rc < 0) return rc;
         if (rc > worst) worst = rc;

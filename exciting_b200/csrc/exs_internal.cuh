@@ -1,5 +1,6 @@
 // Internal definitions shared by the CUDA translation units of libexciting_b200.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -41,6 +42,7 @@ struct KDesc {
     double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
     int8_t *oz_slices;       // split-precision path: int8 slices [6][S][npad][kp8]
     double *oz_scale;        // split-precision path: column scales of A and B [2][npad]
+    int oz_row0;             // split-precision path: first row of this slot in the slice tensor map
 };
 
 // Constant per-context device parameters passed by value to kernels.
@@ -166,10 +168,14 @@ struct exs_ctx {
     int8_t *d_oz = nullptr;      // int8 slices of all slots
     double *d_ozscale = nullptr; // column scales of all slots
     size_t oz_slot_bytes = 0;
+    CUtensorMap oz_mapA, oz_mapB;     // TMA views of d_oz
+    bool oz_ws = true;                // warp-specialised TMA kernel (else the cp.async kernel)
     // runtime
     int device = 0;
     cudaStream_t stream = nullptr;      // stream the work runs on
     cudaStream_t own_stream = nullptr;  // the context's own stream
+    cudaStream_t copy_stream = nullptr; // device-to-host copies of the host-facing calls
+    cudaEvent_t ev_group[2] = {};
     cudaEvent_t ev[8] = {};
     double last_t[5] = {0, 0, 0, 0, 0};
     bool timed = false;          // ev[0..4] recorded by the last setup call
@@ -196,4 +202,7 @@ cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, 
 cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s);
 cudaError_t launch_oz_mma(const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8,
                           cudaStream_t s);
+bool make_oz_tensor_maps(void *base, size_t rows, int kp8, CUtensorMap *mapA, CUtensorMap *mapB);
+cudaError_t launch_oz_mma_ws(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
+                             const void *d_tiles, int ntiles, int S, int kp8, cudaStream_t s);
 }  // namespace exs

@@ -25,6 +25,8 @@
 // [128,384) of a 512-column allocation.  Every wait on an mbarrier is bounded
 // (about one second); on expiry the kernel records an error, drains its own
 // copies, frees tensor memory and returns.
+#include <cuda.h>
+
 #include <cstdint>
 
 #include "exs_internal.cuh"
@@ -459,6 +461,339 @@ cudaError_t launch_oz_mma(const DevParams &p, const KDesc *d_k, const void *d_ti
     }
     oz_mma_kernel<<<ntiles, 128, OZ_SMEM, s>>>(p, d_k, (const OzTile *)d_tiles, S, kp8);
     return cudaGetLastError();
+}
+
+}  // namespace exs
+
+namespace exs {
+
+// ============================================================================
+// Warp-specialised variant: TMA-fed 6-stage pipeline, one producer warp, one
+// MMA warp, four epilogue warps, and two int32 accumulators in tensor memory
+// so that the FP64 fold of diagonal d overlaps the MMAs of diagonal d+1.
+//
+// Operand tiles are loaded by TMA with 128-byte swizzling from the same int8
+// slice array (viewed as a 2D tensor [rows][kp8 bytes]); the MMA descriptors
+// use the matching SWIZZLE_128B K-major layout (8-row x 128-byte atoms,
+// 1024-byte stride between 8-row groups, K advanced 32 bytes per MMA).
+// Tensor memory (512 columns): int32 accumulators at [0,128) and [128,256),
+// FP64 accumulator (two 32-bit words per value) at [256,512).
+// ============================================================================
+constexpr int WS_STAGES = 6;
+constexpr int WS_THREADS = 192;
+constexpr int WS_SMEM = WS_STAGES * OZ_STAGE + 1024;
+constexpr int WS_FP64_COL = 256;
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            dst),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait that also gives up as soon as another role raised `abort`.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort)
+{
+    const uint32_t a = smem_u32(bar);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (*abort) return false;
+        if (clock64() - t0 > OZ_WAIT_CYCLES) {
+            *abort = 1;
+            return false;
+        }
+    }
+}
+
+// K-major SWIZZLE_128B descriptor (8-row x 128-byte atoms, 1024 B between 8-row groups).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                   // leading byte offset (unused by swizzled K-major): 16 B
+    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
+    d |= (uint64_t)1 << 46;                   // descriptor version of sm_100
+    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+    return d;
+}
+
+__global__ void __launch_bounds__(WS_THREADS, 1)
+oz_mma_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
+                 const KDesc *ks, const OzTile *tiles, int S, int kp8)
+{
+    extern __shared__ __align__(1024) uint8_t ws_smem[];
+    __shared__ uint64_t full[WS_STAGES], empty[WS_STAGES], accf[2], acce[2];
+    __shared__ uint32_t tmem_sh;
+    __shared__ int abort_sh;
+    __shared__ int jiv[OZ_BJ][3];
+    __shared__ double jv[OZ_BJ][3];
+    volatile int *abort = &abort_sh;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const OzTile tl = tiles[blockIdx.x];
+    const KDesc kd = ks[tl.k];
+    const int i0 = tl.ib * OZ_BM, j0 = tl.jb * OZ_BJ;
+    const uint32_t sbase = (smem_u32(ws_smem) + 1023u) & ~1023u;
+
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(OZ_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < WS_STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int b = 0; b < 2; b++) { mbar_init(&accf[b], 1); mbar_init(&acce[b], 4); }
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (tid >= 64 && tid < 64 + OZ_BJ) {        // column data of the final epilogue
+        const int c = tid - 64, j = j0 + c;
+        if (j < kd.ngp) {
+            int g = kd.igpig[j] - 1;
+            if (g < 0 || g >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); g = 0; }
+            for (int x = 0; x < 3; x++) { jiv[c][x] = p.ivg[3 * g + x]; jv[c][x] = kd.vgpc[3 * j + x]; }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = tmem_sh;
+    const int nkb_half = kp8 / OZ_BK, nkb = 2 * nkb_half;
+    const int npad = p.npad;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            uint32_t fills[WS_STAGES] = {0, 0, 0, 0, 0, 0};
+            long it = 0;
+            bool bad = false;
+            for (int d = 2; d <= S + 1 && !bad; d++) {
+                const int s_lo = max(1, d - S), s_hi = min(S, d - 1);
+                for (int s = s_lo; s <= s_hi && !bad; s++) {
+                    const int t = d - s;
+                    for (int kb = 0; kb < nkb; kb++, it++) {
+                        const int st = (int)(it % WS_STAGES);
+                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) { bad = true; break; }
+                        mbar_expect_tx(&full[st], OZ_STAGE);
+                        const int h = kb / nkb_half, kk = (kb % nkb_half) * OZ_BK;
+                        const uint32_t sa = sbase + st * OZ_STAGE;
+                        tma_load_2d(sa, &mapA, kk, kd.oz_row0 + (h * S + (s - 1)) * npad + i0, &full[st]);
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            tma_load_2d(sa + OZ_TILE + q * 4096, &mapB, kk,
+                                        kd.oz_row0 + (oz_barr(q, h) * S + (t - 1)) * npad + j0, &full[st]);
+                        fills[st]++;
+                    }
+                }
+            }
+            if (bad)   // let the copies already issued land before the CTA goes away
+                for (int st = 0; st < WS_STAGES; st++)
+                    if (fills[st] > 0) (void)mbar_wait(&full[st], (fills[st] - 1) & 1);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_i8(128, OZ_N);
+            uint32_t uses[WS_STAGES] = {0, 0, 0, 0, 0, 0};
+            int accuse[2] = {0, 0};
+            long it = 0;
+            bool bad = false;
+            for (int d = 2; d <= S + 1 && !bad; d++) {
+                const int b = (d - 2) & 1;
+                if (accuse[b] > 0 && !mbar_wait_ab(&acce[b], (accuse[b] - 1) & 1, abort)) { bad = true; break; }
+                tc_fence_after();
+                const uint32_t dtm = tbase + b * 128;
+                const int s_lo = max(1, d - S), s_hi = min(S, d - 1);
+                bool first = true;
+                for (int s = s_lo; s <= s_hi && !bad; s++)
+                    for (int kb = 0; kb < nkb; kb++, it++) {
+                        const int st = (int)(it % WS_STAGES);
+                        if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) { bad = true; break; }
+                        tc_fence_after();
+                        const uint32_t sa = sbase + st * OZ_STAGE, sb = sa + OZ_TILE;
+#pragma unroll
+                        for (int q = 0; q < OZ_BK / 32; q++) {
+                            umma_i8(dtm, umma_desc_sw128(sa + q * 32), umma_desc_sw128(sb + q * 32), idesc,
+                                    (first && q == 0) ? 0u : 1u);
+                        }
+                        first = false;
+                        umma_commit(&empty[st]);
+                        uses[st]++;
+                    }
+                if (!bad) {
+                    umma_commit(&accf[b]);
+                    accuse[b]++;
+                }
+            }
+            if (bad)   // MMAs already issued must finish before tensor memory is freed
+                for (int st = 0; st < WS_STAGES; st++)
+                    if (uses[st] > 0) (void)mbar_wait(&empty[st], (uses[st] - 1) & 1);
+        }
+    } else {
+        // ------------------------------------------------ epilogue (warps 2..5)
+        const int qd = warp & 3;                                   // tensor-memory lane quadrant
+        const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
+        int accn[2] = {0, 0};
+        bool bad = false;
+        for (int d = 2; d <= S + 1; d++) {
+            const int b = (d - 2) & 1;
+            // warp-uniform outcome: the tcgen05.ld/st below need the whole warp
+            const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf[b], accn[b] & 1, abort));
+            if (!ok) { bad = true; break; }
+            accn[b]++;
+            tc_fence_after();
+            const double scale = ldexp(1.0, -7 * d);
+#pragma unroll 1
+            for (int c = 0; c < OZ_N / 16; c++) {
+                uint32_t iv[16], lo[16], hi[16];
+                tm_ld16(t_lane + b * 128 + c * 16, iv);
+                if (d > 2) {
+                    tm_ld16(t_lane + WS_FP64_COL + c * 32, lo);
+                    tm_ld16(t_lane + WS_FP64_COL + c * 32 + 16, hi);
+                }
+                tm_wait_ld();
+                uint32_t o0[16], o1[16];
+#pragma unroll
+                for (int e = 0; e < 16; e++) {
+                    double a = 0.0;
+                    if (d > 2) {
+                        const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
+                        const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
+                        a = __hiloint2double((int)w1, (int)w0);
+                    }
+                    a += scale * (double)(int)iv[e];
+                    const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
+                    if (e < 8) { o0[2 * e] = w0; o0[2 * e + 1] = w1; }
+                    else { o1[2 * (e - 8)] = w0; o1[2 * (e - 8) + 1] = w1; }
+                }
+                tm_st16(t_lane + WS_FP64_COL + c * 32, o0);
+                tm_st16(t_lane + WS_FP64_COL + c * 32 + 16, o1);
+            }
+            tm_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[b]);
+        }
+        if (__all_sync(0xffffffffu, !bad && !*abort)) {
+            const int i = i0 + qd * 32 + lane;
+            int ivi[3] = {0, 0, 0};
+            double vi[3] = {0.0, 0.0, 0.0};
+            const bool row_ok = i < kd.ngp;
+            if (row_ok) {
+                int g = kd.igpig[i] - 1;
+                if (g < 0 || g >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); g = 0; }
+                for (int x = 0; x < 3; x++) { ivi[x] = p.ivg[3 * g + x]; vi[x] = kd.vgpc[3 * i + x]; }
+            }
+            const double sai = row_ok ? kd.oz_scale[i] : 0.0;
+#pragma unroll 1
+            for (int jc = 0; jc < OZ_BJ; jc += 8) {
+                double val[4][8];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    uint32_t w[16];
+                    tm_ld16(t_lane + WS_FP64_COL + 2 * (q * 32 + jc), w);
+                    tm_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 8; e++) val[q][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+                }
+                if (!row_ok) continue;
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int jj = jc + e, j = j0 + jj;
+                    if (j >= kd.ngp || i > j) continue;
+                    const double sbj = kd.oz_scale[npad + j], saj = kd.oz_scale[j];
+                    double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
+                    double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
+                    double ar, ai;
+                    if (interstitial(p, EPI_HAM, ivi, jiv[jj], vi, jv[jj], ar, ai)) { hr += ar; hi += ai; }
+                    if (interstitial(p, EPI_OVL, ivi, jiv[jj], vi, jv[jj], ar, ai)) { orr += ar; oi += ai; }
+                    exs_complex hv, ov;
+                    hv.re = hr; hv.im = hi;
+                    ov.re = orr; ov.im = oi;
+                    kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
+                    kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
+                    if (i < j) {
+                        hv.im = -hi;
+                        ov.im = -oi;
+                        kd.h[(size_t)j + (size_t)kd.nmat * i] = hv;
+                        kd.o[(size_t)j + (size_t)kd.nmat * i] = ov;
+                    }
+                }
+            }
+        }
+    }
+    if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(OZ_TMEM_COLS));
+    }
+}
+
+cudaError_t launch_oz_mma_ws(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
+                             const void *d_tiles, int ntiles, int S, int kp8, cudaStream_t s)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(oz_mma_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    oz_mma_ws_kernel<<<ntiles, WS_THREADS, WS_SMEM, s>>>(*mapA, *mapB, p, d_k, (const OzTile *)d_tiles, S, kp8);
+    return cudaGetLastError();
+}
+
+// Tensor maps over the int8 slices of all slots: [rows][kp8] bytes, boxes of
+// 128 x 128 (A tile) and 32 x 128 (one B sub-block), 128-byte swizzle.
+bool make_oz_tensor_maps(void *base, size_t rows, int kp8, CUtensorMap *mapA, CUtensorMap *mapB)
+{
+    typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeFn encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+            return false;
+        encode = (EncodeFn)fn;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)kp8, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kp8};
+    const cuuint32_t es[2] = {1, 1};
+    const cuuint32_t boxA[2] = {128, 128}, boxB[2] = {128, 32};
+    if (encode(mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+        return false;
+    if (encode(mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+        return false;
+    return true;
 }
 
 }  // namespace exs
