@@ -128,9 +128,10 @@ def _measured_int8_peak(torch):
 
 def ozaki_int8_ops(sys_, gks, slices):
     """int8 MMA operations the split-precision kernel issues: per 128 x 32 tile
-    (4 outputs -> N = 128), S(S+1)/2 slice pairs x 2 x 128 x 128 x K', K' = 2 kp8."""
+    (B operand [Br|Bi|Ar|Ai] -> N = 128), S(S+1)/2 slice pairs x two A operands
+    (Ar, Ai) x 2 x 128 x 128 x kp8 (K padded to 256)."""
     K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
-    kp8 = (K + 127) // 128 * 128
+    kp8 = (K + 255) // 256 * 256
     pairs = slices * (slices + 1) // 2
     tiles = 0
     for g in gks:

@@ -324,12 +324,12 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     if (slices < 3 || slices > 9) return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
     if (c->relativity == EXS_REL_IORA)
         return fail(c, EXS_ERR_ARG, "the split-precision contraction does not take the iora* overlap term");
-    if (2 * (size_t)c->Kpad * 127 * 127 * slices >= (size_t)1 << 31)
-        return fail(c, EXS_ERR_SIZE, "K too large for exact int32 accumulation of one diagonal");
+    const int kp8 = exs::oz_kpad(c->K);
+    const int seg = exs::oz_seg_pairs(slices, kp8);
+    if (seg < 1) return fail(c, EXS_ERR_SIZE, "K too large for exact int32 accumulation of one slice pair");
     cudaSetDevice(c->device);
     EXS_CUDA(cudaStreamSynchronize(c->stream));
-    const int kp8 = round_up(c->K, 128);
-    const size_t slot = (size_t)6 * slices * c->npad * kp8;
+    const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8);
     if (c->d_oz) { cudaFree(c->d_oz); c->d_oz = nullptr; }
     if (c->d_ozscale) { cudaFree(c->d_ozscale); c->d_ozscale = nullptr; }
     cudaError_t e = cudaMalloc((void **)&c->d_oz, slot * c->max_batch);
@@ -339,12 +339,10 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         return fail(c, EXS_ERR_NOMEM, "split-precision work space");
     }
     c->kp8 = kp8;
+    c->oz_seg = seg;
     c->oz_slot_bytes = slot;
-    {   // EXS_OZAKI_KERNEL=cpasync selects the single-role cp.async kernel (comparison runs)
-        const char *kv = getenv("EXS_OZAKI_KERNEL");
-        c->oz_ws = !(kv && std::strcmp(kv, "cpasync") == 0);
-    }
-    if (!exs::make_oz_tensor_maps(c->d_oz, (size_t)6 * slices * c->npad * c->max_batch, kp8, &c->oz_mapA,
+    // one tensor-map group = 128 rows (4 arrays x 32 G) of one slice of one slot
+    if (!exs::make_oz_tensor_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8, &c->oz_mapA,
                                   &c->oz_mapB)) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
@@ -602,11 +600,8 @@ int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
     EXS_CUDA(cudaEventRecord(c->ev[2], s));
     if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
         EXS_CUDA(exs::launch_oz_prepare(p, u.d_k, (int)ks.size(), c->slices, c->kp8, s));
-        if (c->oz_ws)
-            EXS_CUDA(exs::launch_oz_mma_ws(&c->oz_mapA, &c->oz_mapB, p, u.d_k, u.d_oztiles, u.noztiles, c->slices,
-                                           c->kp8, s));
-        else
-            EXS_CUDA(exs::launch_oz_mma(p, u.d_k, u.d_oztiles, u.noztiles, c->slices, c->kp8, s));
+        EXS_CUDA(exs::launch_oz_mma(&c->oz_mapA, &c->oz_mapB, p, u.d_k, u.d_oztiles, u.noztiles, c->slices, c->kp8,
+                                    c->oz_seg, s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
                                        u.nwork[exs::EPI_HAM], u.d_k, s));
@@ -646,7 +641,7 @@ KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double 
     }
     k.oz_slices = c->d_oz ? c->d_oz + (size_t)slot * c->oz_slot_bytes : nullptr;
     k.oz_scale = c->d_ozscale ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
-    k.oz_row0 = slot * 6 * c->slices * c->npad;
+    k.oz_slot = slot;
     return k;
 }
 

@@ -40,9 +40,9 @@ struct KDesc {
     double *ar, *ai;         // A planes  [Kpad][npad]
     double *br, *bi;         // B = blockdiag(h_a) A planes
     double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
-    int8_t *oz_slices;       // split-precision path: int8 slices [6][S][npad][kp8]
+    int8_t *oz_slices;       // split-precision path: int8 slices of this slot [S][npad/32][4][32][kp8]
     double *oz_scale;        // split-precision path: column scales of A and B [2][npad]
-    int oz_row0;             // split-precision path: first row of this slot in the slice tensor map
+    int oz_slot;             // split-precision path: slot index in the slice tensor maps
 };
 
 // Constant per-context device parameters passed by value to kernels.
@@ -164,12 +164,12 @@ struct exs_ctx {
     // precision
     int prec_mode = EXS_PREC_FP64;
     int slices = 7;
-    int kp8 = 0;                 // K rounded up to 128 (int8 slice rows)
+    int kp8 = 0;                 // K rounded up to 256 (int8 slice rows)
+    int oz_seg = 0;              // slice pairs per exact int32 segment
     int8_t *d_oz = nullptr;      // int8 slices of all slots
     double *d_ozscale = nullptr; // column scales of all slots
     size_t oz_slot_bytes = 0;
     CUtensorMap oz_mapA, oz_mapB;     // TMA views of d_oz
-    bool oz_ws = true;                // warp-specialised TMA kernel (else the cp.async kernel)
     // runtime
     int device = 0;
     cudaStream_t stream = nullptr;      // stream the work runs on
@@ -200,9 +200,10 @@ cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, 
                              const KDesc *d_k, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)
 cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s);
-cudaError_t launch_oz_mma(const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8,
-                          cudaStream_t s);
-bool make_oz_tensor_maps(void *base, size_t rows, int kp8, CUtensorMap *mapA, CUtensorMap *mapB);
-cudaError_t launch_oz_mma_ws(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
-                             const void *d_tiles, int ntiles, int S, int kp8, cudaStream_t s);
+cudaError_t launch_oz_mma(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
+                          const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s);
+bool make_oz_tensor_maps(void *base, size_t groups, int kp8, CUtensorMap *mapA, CUtensorMap *mapB);
+int oz_kpad(int K);
+size_t oz_slot_bytes(int S, int npad, int kp8);
+int oz_seg_pairs(int S, int kp8);
 }  // namespace exs

@@ -1,30 +1,44 @@
 // Split-precision (Ozaki scheme, int8 slices) MT contraction on the 5th-gen
 // tensor cores (tcgen05.mma kind::i8, int32 accumulators in tensor memory).
 //
-// The APW-APW blocks H = A^H B and O = A^H A are written as one real product
-// with the contraction index K' = 2K (real and imaginary rows stacked):
-//   L  = [Ar; Ai]                      (left operand, shared)
-//   R1 = [Br; Bi],  R2 = [Bi; -Br]      Re H = L^T R1,  Im H = L^T R2
-//   R3 = [Ar; Ai],  R4 = [Ai; -Ar]      Re O = L^T R3,  Im O = L^T R4
+// H = A^H B and O = A^H A in real arithmetic: with the real and imaginary
+// planes of A and B,
+//   Re H = Ar^T Br + Ai^T Bi    Im H = Ar^T Bi - Ai^T Br
+//   Re O = Ar^T Ar + Ai^T Ai    Im O = Ar^T Ai - Ai^T Ar
+// so one B operand tile [Br | Bi | Ar | Ai] (32 columns G_j each, N = 128)
+// against the two A operands Ar and Ai (two int32 accumulators r and i)
+// yields all four: Re H = r0 + i1, Im H = r1 - i0, Re O = r2 + i3,
+// Im O = r3 - i2 (rq = block q of accumulator r).
+//
 // Every column G of A (and of B) is scaled by a power of two sigma(G) >
 // max|column| and cut into S int8 slices of 7 bits each by truncation,
-//   x = sigma * sum_s q_s 2^{-7s} + r,  |q_s| <= 127,  |r| < sigma 2^{-7S}
-// (exact in FP64).  The product keeps the slice pairs s + t <= S + 1; pairs
-// of one diagonal d = s + t share one int32 accumulator (exact: at most S
-// products of K' <= 2^17 terms of |q q'| <= 127^2 stay below 2^31), and each
-// finished diagonal is added in FP64 as 2^{-7d} times the int32 sum into an
+//   x = sigma * sum_s q_s 2^{-7s} + rest,  |q_s| <= 127,  |rest| < sigma 2^{-7S}
+// (exact in FP64).  The product keeps the slice pairs s + t <= S + 1.  Pairs
+// are accumulated in int32 in segments short enough to be exact (the pairs of
+// one diagonal d = s + t in groups of P with P * K * 127^2 < 2^31), and each
+// finished segment is added in FP64 as 2^{-7d} times its int32 sums to an
 // FP64 accumulator that also lives in tensor memory.  The final epilogue
 // multiplies by sigma_A(i) sigma_B(j), adds the interstitial term and writes
 // the upper triangle and its conjugate mirror, as the FP64 path does.
 //
-// Tile: 128 rows (G_i) x 32 columns (G_j) x 4 outputs (Re H, Im H, Re O,
-// Im O) = one M=128, N=128 MMA shape; K staged 128 bytes at a time through a
-// 4-deep cp.async pipeline in the canonical no-swizzle K-major layout
-// (8-row x 16-byte core matrices).  Tensor memory: int32 accumulator in
-// columns [0,128), FP64 accumulator (two 32-bit columns per value) in
-// [128,384) of a 512-column allocation.  Every wait on an mbarrier is bounded
-// (about one second); on expiry the kernel records an error, drains its own
-// copies, frees tensor memory and returns.
+// Slice storage (int8, K contiguous, K padded to kp8 = multiple of 256):
+//   [slot][slice][32-row block of G][array: Br, Bi, Ar, Ai][32 rows][kp8]
+// so that a B tile (one G block, all four arrays) is 128 consecutive rows and
+// an A tile (one array of four consecutive G blocks) is a regular stride:
+// each operand tile of a pipeline stage (two 128-byte K chunks) is ONE TMA
+// box of 32 KB.  Boxes are written with 128-byte swizzling; the MMA
+// descriptors use the matching SWIZZLE_128B K-major layout (8-row x 128-byte
+// atoms, 1024 B between 8-row groups, K advanced 32 bytes per MMA).
+//
+// Roles (one CTA per 128 x 32 output tile, 256 threads):
+//   warps 0-2  one TMA producer thread each (A_r, A_i and B box of a stage)
+//   warp 3     MMA issuer (one thread); allocates tensor memory
+//   warps 4-7  epilogue: segment folds and the final store
+// Tensor memory (512 columns): r at [0,128), i at [128,256), FP64 sums (two
+// 32-bit columns per value) at [256,512).  Every wait on an mbarrier is
+// bounded (about one second) and gives up early once another role has given
+// up; the kernel then records an error, lets its own copies and MMAs drain
+// (bounded), frees tensor memory and returns.
 #include <cuda.h>
 
 #include <cstdint>
@@ -37,59 +51,96 @@ namespace exs {
 constexpr int OZ_BM = 128;                       // tile rows (G_i)
 constexpr int OZ_BJ = 32;                        // tile columns (G_j); MMA N = 4 * OZ_BJ
 constexpr int OZ_N = 4 * OZ_BJ;
-constexpr int OZ_BK = 128;                       // bytes of K per pipeline stage (4 MMAs of K = 32)
-constexpr int OZ_STAGES = 4;
-constexpr int OZ_PREFETCH = 2;                  // loads run two iterations ahead of the MMAs
-constexpr int OZ_TILE = 128 * OZ_BK;             // 16 KB per operand tile
-constexpr int OZ_STAGE = 2 * OZ_TILE;            // A + B
+constexpr int OZ_NARR = 4;                       // Br, Bi, Ar, Ai
+constexpr int OZ_CHUNK = 128;                    // bytes of K in one swizzle row
+constexpr int OZ_KCH = 2;                        // K chunks per pipeline stage
+constexpr int OZ_TILE = 128 * OZ_CHUNK;          // 16 KB: one K chunk of a 128-row operand
+constexpr int OZ_BOX = OZ_KCH * OZ_TILE;         // 32 KB: one TMA box
+constexpr int OZ_STAGE = 3 * OZ_BOX;             // A_r, A_i, B
+constexpr int OZ_STAGES = 2;
 constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE + 1024;
+constexpr int OZ_THREADS = 256;
 constexpr int OZ_TMEM_COLS = 512;
-constexpr int OZ_NARR = 6;                       // Ar, Ai, Br, Bi, -Br, -Ar
+constexpr int OZ_FP64_COL = 256;
 constexpr long long OZ_WAIT_CYCLES = 2000000000LL;   // ~1 s at 2 GHz
+
+struct OzTile {
+    int k, ib, jb;
+};
 
 // ------------------------------------------------------------ device helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void oz_cp16(uint32_t dst, const void *src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
-}
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// Bounded wait for the phase with the given parity; false on expiry.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
 {
-    const uint32_t a = smem_u32(bar);
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait that also gives up as soon as another role raised `abort`.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort)
+{
     const long long t0 = clock64();
     while (true) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if (clock64() - t0 > OZ_WAIT_CYCLES) return false;
+        if (mbar_try(bar, parity)) return true;
+        if (*abort) return false;
+        if (clock64() - t0 > OZ_WAIT_CYCLES) {
+            *abort = 1;
+            return false;
+        }
     }
 }
 
-// K-major, no-swizzle shared-memory matrix descriptor: core matrices of
-// 8 rows x 16 bytes; lbo = byte step between the two 16-byte K chunks of one
-// MMA, sbo = byte step between 8-row groups.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+// Bounded wait used while draining after an abort.
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity) && clock64() - t0 < OZ_WAIT_CYCLES) {
+    }
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];\n" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// K-major SWIZZLE_128B descriptor (8-row x 128-byte atoms, 1024 B between 8-row groups).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;                  // descriptor version of sm_100
-    return d;                                // base offset 0, layout type 0 (no swizzle)
+    d |= (uint64_t)1 << 16;                   // leading byte offset (unused by swizzled K-major): 16 B
+    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
+    d |= (uint64_t)1 << 46;                   // descriptor version of sm_100
+    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+    return d;
 }
 
 // kind::i8 instruction descriptor: s8 x s8 -> s32, K-major A and B, M x N.
@@ -158,392 +209,55 @@ __global__ void oz_colscale_kernel(DevParams p, const KDesc *ks)
     k.oz_scale[p.npad + g] = ldexp(1.0, eb);
 }
 
-// Slices of the six operand arrays, K-major int8 [arr][s][G][f], f padded to
-// kp8 with zeros.  A 32(f) x 32(G) tile per block, transposed through shared
-// memory.
+// Byte offset of (slice s, array a, row G, K index f) inside one slot.
+__device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int nblk, int kp8)
+{
+    return ((((size_t)s * nblk + (g >> 5)) * OZ_NARR + a) * 32 + (g & 31)) * (size_t)kp8 + f;
+}
+
+// The S slices of the four arrays.  A 32(f) x 32(G) tile per block,
+// transposed through shared memory (reads G-contiguous planes, writes
+// K-contiguous int8 rows).
 __global__ void oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
 {
-    __shared__ double t[4][32][33];
+    __shared__ double t[OZ_NARR][32][33];
     const KDesc k = ks[blockIdx.z];
     const int f0 = blockIdx.x * 32, g0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;      // 32 x 8
+    const int nblk = p.npad / 32;
     for (int r = ty; r < 32; r += 8) {
         const int f = f0 + r, g = g0 + tx;
         const bool v = f < p.K && g < k.ngp;
         const size_t i = (size_t)f * p.npad + g;
-        t[0][r][tx] = v ? k.ar[i] : 0.0;
-        t[1][r][tx] = v ? k.ai[i] : 0.0;
-        t[2][r][tx] = v ? k.br[i] : 0.0;
-        t[3][r][tx] = v ? k.bi[i] : 0.0;
+        t[0][r][tx] = v ? k.br[i] : 0.0;
+        t[1][r][tx] = v ? k.bi[i] : 0.0;
+        t[2][r][tx] = v ? k.ar[i] : 0.0;
+        t[3][r][tx] = v ? k.ai[i] : 0.0;
     }
     __syncthreads();
-    // thread (tx = f within tile, ty..): one G per pass
     for (int r = ty; r < 32; r += 8) {
         const int g = g0 + r, f = f0 + tx;
         if (g >= p.npad || f >= kp8) continue;
         const double sa = k.oz_scale[g], sb = k.oz_scale[p.npad + g];
-        double x[4] = {t[0][tx][r] / sa, t[1][tx][r] / sa, t[2][tx][r] / sb, t[3][tx][r] / sb};
-        for (int s = 0; s < S; s++) {
-            int8_t q[4];
-            for (int a = 0; a < 4; a++) {
+        double x[OZ_NARR] = {t[0][tx][r] / sb, t[1][tx][r] / sb, t[2][tx][r] / sa, t[3][tx][r] / sa};
+        for (int s = 0; s < S; s++)
+#pragma unroll
+            for (int a = 0; a < OZ_NARR; a++) {
                 x[a] *= 128.0;
                 const double tq = trunc(x[a]);
                 x[a] -= tq;
-                q[a] = (int8_t)tq;
+                k.oz_slices[oz_off(s, a, g, f, nblk, kp8)] = (int8_t)tq;
             }
-            // arrays: 0 Ar, 1 Ai, 2 Br, 3 Bi, 4 -Br, 5 -Ar
-            const int8_t vals[OZ_NARR] = {q[0], q[1], q[2], q[3], (int8_t)(-q[2]), (int8_t)(-q[0])};
-            for (int a = 0; a < OZ_NARR; a++)
-                k.oz_slices[(((size_t)a * S + s) * p.npad + g) * kp8 + f] = vals[a];
-        }
     }
 }
 
 // ------------------------------------------------------------ main kernel
-struct OzTile {
-    int k, ib, jb;
-};
-
-// Source array of sub-block q of the B tile, K half h (see the header).
-__device__ __forceinline__ int oz_barr(int q, int h)
-{
-    const int t0[4] = {2, 3, 0, 1}, t1[4] = {3, 4, 1, 5};
-    return h == 0 ? t0[q] : t1[q];
-}
-
-__global__ void __launch_bounds__(128, 1)
-oz_mma_kernel(DevParams p, const KDesc *ks, const OzTile *tiles, int S, int kp8)
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
+              const KDesc *ks, const OzTile *tiles, int S, int kp8, int seg_pairs)
 {
     extern __shared__ __align__(1024) uint8_t oz_smem[];
-    __shared__ uint64_t bars[OZ_STAGES];
-    __shared__ uint32_t tmem_base_sh;
-    __shared__ int fail_sh;
-    __shared__ int jiv[OZ_BJ][3];
-    __shared__ double jv[OZ_BJ][3];
-
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const OzTile tl = tiles[blockIdx.x];
-    const KDesc kd = ks[tl.k];
-    const int i0 = tl.ib * OZ_BM, j0 = tl.jb * OZ_BJ;
-    // stage buffers at a 1024-byte aligned offset
-    const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
-    uint8_t *sgen = oz_smem + (sbase - smem_u32(oz_smem));
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base_sh)),
-                     "r"(OZ_TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
-    }
-    if (tid == 0) {
-        for (int s = 0; s < OZ_STAGES; s++) mbar_init(&bars[s], 1);
-        fail_sh = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tbase = tmem_base_sh;
-    const uint32_t t_lane = tbase + ((uint32_t)(warp * 32) << 16);   // this warp's 32 lanes
-    const uint32_t idesc = umma_idesc_i8(128, OZ_N);
-    const int nkb_half = kp8 / OZ_BK;
-    const int nkb = 2 * nkb_half;                    // k-blocks per slice pair (both K halves)
-    const size_t arr_stride = (size_t)S * p.npad * kp8;
-    const size_t slice_stride = (size_t)p.npad * kp8;
-    uint32_t uses[OZ_STAGES] = {0, 0, 0, 0};          // completed-commit count per stage
-    long git = 0;                                     // global pipeline iteration
-    bool failed = false;
-
-    // Load the A and B tiles of flat iteration `it` of diagonal d into stage st.
-    auto load_stage = [&](int d, int s_lo, int it, int st) {
-        const int pair = it / nkb, kb = it % nkb;
-        const int s = s_lo + pair, t = d - s;        // 1-based slice indices
-        const int h = kb / nkb_half, kk = (kb % nkb_half) * OZ_BK;
-        const uint32_t sa = sbase + st * OZ_STAGE, sb = sa + OZ_TILE;
-        const int8_t *abase = kd.oz_slices + (size_t)h * arr_stride + (size_t)(s - 1) * slice_stride;
-#pragma unroll
-        for (int it2 = 0; it2 < 8; it2++) {
-            const int qd = tid + 128 * it2;          // chunk 0..1023
-            const int r8 = qd & 7, c = (qd >> 3) & 7, grp = qd >> 6;
-            const int row = grp * 8 + r8;            // 0..127
-            const uint32_t soff = grp * 1024 + c * 128 + r8 * 16;
-            // A: row -> G_i = i0 + row (rows past npad read row npad-1: in bounds, results discarded)
-            const int gi = min(i0 + row, p.npad - 1);
-            oz_cp16(sa + soff, abase + (size_t)gi * kp8 + kk + c * 16);
-            // B: row -> sub-block q = row / 32, G_j = j0 + row % 32
-            const int q = row >> 5;
-            const int gj = min(j0 + (row & 31), p.npad - 1);
-            const int8_t *bb = kd.oz_slices + (size_t)oz_barr(q, h) * arr_stride + (size_t)(t - 1) * slice_stride;
-            oz_cp16(sb + soff, bb + (size_t)gj * kp8 + kk + c * 16);
-        }
-    };
-
-    for (int d = 2; d <= S + 1 && !failed; d++) {
-        const int s_lo = max(1, d - S), s_hi = min(S, d - 1);
-        const int total = (s_hi - s_lo + 1) * nkb;
-        // prologue: the first OZ_PREFETCH iterations
-        for (int it = 0; it < OZ_PREFETCH; it++) {
-            if (it < total) {
-                const int st = (int)((git + it) % OZ_STAGES);
-                if (uses[st] > 0 && !mbar_wait(&bars[st], (uses[st] - 1) & 1)) failed = true;
-                load_stage(d, s_lo, it, st);
-            }
-            asm volatile("cp.async.commit_group;\n" ::);
-        }
-        for (int it = 0; it < total; it++) {
-            const int st = (int)((git + it) % OZ_STAGES);
-            asm volatile("cp.async.wait_group %0;\n" ::"n"(OZ_PREFETCH - 1));   // iteration it has landed
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            if (__syncthreads_or(failed)) { failed = true; break; }
-            if (tid == 0) {
-                tc_fence_after();
-                const uint32_t sa = sbase + st * OZ_STAGE, sb = sa + OZ_TILE;
-#pragma unroll
-                for (int q = 0; q < OZ_BK / 32; q++) {
-                    const uint64_t ad = umma_desc(sa + q * 256, 128, 1024);
-                    const uint64_t bd = umma_desc(sb + q * 256, 128, 1024);
-                    umma_i8(tbase, ad, bd, idesc, (it == 0 && q == 0) ? 0u : 1u);
-                }
-                umma_commit(&bars[st]);
-            }
-            uses[st]++;
-            // prefetch iteration it + OZ_PREFETCH into the stage the MMAs of
-            // iteration it + OZ_PREFETCH - OZ_STAGES read (two batches ago)
-            const int nt = it + OZ_PREFETCH;
-            if (nt < total) {
-                const int sn = (int)((git + nt) % OZ_STAGES);
-                if (uses[sn] > 0 && !mbar_wait(&bars[sn], (uses[sn] - 1) & 1)) failed = true;
-                load_stage(d, s_lo, nt, sn);
-            }
-            asm volatile("cp.async.commit_group;\n" ::);
-        }
-        git += total;
-        // all MMAs of this diagonal done: the last commit completes after every earlier one
-        if (!failed) {
-            const int stl = (int)((git - 1) % OZ_STAGES);
-            if (!mbar_wait(&bars[stl], (uses[stl] - 1) & 1)) failed = true;
-        }
-        if (__syncthreads_or(failed)) { failed = true; break; }
-        tc_fence_after();
-        // fold the int32 diagonal sum into the FP64 accumulator: acc += 2^{-7d} C_d
-        const double scale = ldexp(1.0, -7 * d);
-#pragma unroll 1
-        for (int c = 0; c < OZ_N / 16; c++) {
-            uint32_t iv[16], lo[16], hi[16];
-            tm_ld16(t_lane + c * 16, iv);
-            if (d > 2) {
-                tm_ld16(t_lane + 128 + c * 32, lo);
-                tm_ld16(t_lane + 128 + c * 32 + 16, hi);
-            }
-            tm_wait_ld();
-            uint32_t o0[16], o1[16];
-#pragma unroll
-            for (int e = 0; e < 16; e++) {
-                double a = 0.0;
-                if (d > 2) {
-                    const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
-                    const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
-                    a = __hiloint2double((int)w1, (int)w0);
-                }
-                a += scale * (double)(int)iv[e];
-                const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
-                if (e < 8) { o0[2 * e] = w0; o0[2 * e + 1] = w1; }
-                else { o1[2 * (e - 8)] = w0; o1[2 * (e - 8) + 1] = w1; }
-            }
-            tm_st16(t_lane + 128 + c * 32, o0);
-            tm_st16(t_lane + 128 + c * 32 + 16, o1);
-        }
-        tm_wait_st();
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-    }
-
-    if (!failed) {
-        // ---------------- final epilogue: scale, interstitial, store H and O
-        if (tid < OZ_BJ) {
-            const int j = j0 + tid;
-            if (j < kd.ngp) {
-                int g = kd.igpig[j] - 1;
-                if (g < 0 || g >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); g = 0; }
-                for (int x = 0; x < 3; x++) {
-                    jiv[tid][x] = p.ivg[3 * g + x];
-                    jv[tid][x] = kd.vgpc[3 * j + x];
-                }
-            }
-        }
-        __syncthreads();
-        const int i = i0 + warp * 32 + lane;            // this thread's row
-        int ivi[3] = {0, 0, 0};
-        double vi[3] = {0.0, 0.0, 0.0};
-        const bool row_ok = i < kd.ngp;
-        if (row_ok) {
-            int g = kd.igpig[i] - 1;
-            if (g < 0 || g >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); g = 0; }
-            for (int x = 0; x < 3; x++) {
-                ivi[x] = p.ivg[3 * g + x];
-                vi[x] = kd.vgpc[3 * i + x];
-            }
-        }
-        const double sai = row_ok ? kd.oz_scale[i] : 0.0;
-        // FP64 accumulator columns: value v at TMEM columns 128 + 2v, 129 + 2v;
-        // v = q * 32 + jj for output q (Re H, Im H, Re O, Im O) and column jj.
-#pragma unroll 1
-        for (int jc = 0; jc < OZ_BJ; jc += 8) {
-            double val[4][8];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                uint32_t w[16];
-                tm_ld16(t_lane + 128 + 2 * (q * 32 + jc), w);
-                tm_wait_ld();
-#pragma unroll
-                for (int e = 0; e < 8; e++) val[q][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
-            }
-            if (!row_ok) continue;
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-                const int jj = jc + e, j = j0 + jj;
-                if (j >= kd.ngp || i > j) continue;
-                const double sbj = kd.oz_scale[p.npad + j], saj = kd.oz_scale[j];
-                double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
-                double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
-                double ar, ai;
-                if (interstitial(p, EPI_HAM, ivi, jiv[jj], vi, jv[jj], ar, ai)) { hr += ar; hi += ai; }
-                if (interstitial(p, EPI_OVL, ivi, jiv[jj], vi, jv[jj], ar, ai)) { orr += ar; oi += ai; }
-                exs_complex h, o;
-                h.re = hr; h.im = hi;
-                o.re = orr; o.im = oi;
-                kd.h[(size_t)i + (size_t)kd.nmat * j] = h;
-                kd.o[(size_t)i + (size_t)kd.nmat * j] = o;
-                if (i < j) {
-                    h.im = -hi;
-                    o.im = -oi;
-                    kd.h[(size_t)j + (size_t)kd.nmat * i] = h;
-                    kd.o[(size_t)j + (size_t)kd.nmat * i] = o;
-                }
-            }
-        }
-    } else if (tid == 0) {
-        atomicOr(p.err, DEV_ERR_TIMEOUT);
-    }
-    // teardown: drain own copies, make sure no MMA is still reading, free TMEM
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    if (failed && tid == 0) {
-        for (int st = 0; st < OZ_STAGES; st++)
-            if (uses[st] > 0) (void)mbar_wait(&bars[st], (uses[st] - 1) & 1);
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(OZ_TMEM_COLS));
-    }
-}
-
-// ------------------------------------------------------------ launchers
-cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s)
-{
-    oz_colscale_kernel<<<dim3((p.npad + 127) / 128, nk), 128, 0, s>>>(p, d_k);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    oz_split_kernel<<<dim3(kp8 / 32, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_oz_mma(const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8,
-                          cudaStream_t s)
-{
-    if (ntiles <= 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    oz_mma_kernel<<<ntiles, 128, OZ_SMEM, s>>>(p, d_k, (const OzTile *)d_tiles, S, kp8);
-    return cudaGetLastError();
-}
-
-}  // namespace exs
-
-namespace exs {
-
-// ============================================================================
-// Warp-specialised variant: TMA-fed 6-stage pipeline, one producer warp, one
-// MMA warp, four epilogue warps, and two int32 accumulators in tensor memory
-// so that the FP64 fold of diagonal d overlaps the MMAs of diagonal d+1.
-//
-// Operand tiles are loaded by TMA with 128-byte swizzling from the same int8
-// slice array (viewed as a 2D tensor [rows][kp8 bytes]); the MMA descriptors
-// use the matching SWIZZLE_128B K-major layout (8-row x 128-byte atoms,
-// 1024-byte stride between 8-row groups, K advanced 32 bytes per MMA).
-// Tensor memory (512 columns): int32 accumulators at [0,128) and [128,256),
-// FP64 accumulator (two 32-bit words per value) at [256,512).
-// ============================================================================
-constexpr int WS_STAGES = 6;
-constexpr int WS_THREADS = 192;
-constexpr int WS_SMEM = WS_STAGES * OZ_STAGE + 1024;
-constexpr int WS_FP64_COL = 256;
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-            dst),
-        "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// Bounded wait that also gives up as soon as another role raised `abort`.
-__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort)
-{
-    const uint32_t a = smem_u32(bar);
-    const long long t0 = clock64();
-    while (true) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if (*abort) return false;
-        if (clock64() - t0 > OZ_WAIT_CYCLES) {
-            *abort = 1;
-            return false;
-        }
-    }
-}
-
-// K-major SWIZZLE_128B descriptor (8-row x 128-byte atoms, 1024 B between 8-row groups).
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;                   // leading byte offset (unused by swizzled K-major): 16 B
-    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
-    d |= (uint64_t)1 << 46;                   // descriptor version of sm_100
-    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
-    return d;
-}
-
-__global__ void __launch_bounds__(WS_THREADS, 1)
-oz_mma_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
-                 const KDesc *ks, const OzTile *tiles, int S, int kp8)
-{
-    extern __shared__ __align__(1024) uint8_t ws_smem[];
-    __shared__ uint64_t full[WS_STAGES], empty[WS_STAGES], accf[2], acce[2];
+    __shared__ uint64_t full[OZ_STAGES], empty[OZ_STAGES], accf, acce;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
     __shared__ int jiv[OZ_BJ][3];
@@ -554,146 +268,190 @@ oz_mma_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
     const OzTile tl = tiles[blockIdx.x];
     const KDesc kd = ks[tl.k];
     const int i0 = tl.ib * OZ_BM, j0 = tl.jb * OZ_BJ;
-    const uint32_t sbase = (smem_u32(ws_smem) + 1023u) & ~1023u;
+    const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
+    const int nblk = p.npad / 32;
+    const int nst = kp8 / (OZ_KCH * OZ_CHUNK);        // pipeline stages per slice pair
 
-    if (warp == 1) {
+    if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
                      "r"(OZ_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 0) {
-        for (int s = 0; s < WS_STAGES; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-        for (int b = 0; b < 2; b++) { mbar_init(&accf[b], 1); mbar_init(&acce[b], 4); }
+        for (int s = 0; s < OZ_STAGES; s++) {
+            mbar_init(&full[s], 3);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accf, 1);
+        mbar_init(&acce, 4);
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    if (tid >= 64 && tid < 64 + OZ_BJ) {        // column data of the final epilogue
-        const int c = tid - 64, j = j0 + c;
+    if (tid >= 128 && tid < 128 + OZ_BJ) {        // column data of the final epilogue
+        const int c = tid - 128, j = j0 + c;
         if (j < kd.ngp) {
             int g = kd.igpig[j] - 1;
-            if (g < 0 || g >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); g = 0; }
-            for (int x = 0; x < 3; x++) { jiv[c][x] = p.ivg[3 * g + x]; jv[c][x] = kd.vgpc[3 * j + x]; }
+            if (g < 0 || g >= p.ngrtot) {
+                atomicOr(p.err, DEV_ERR_INDEX);
+                g = 0;
+            }
+            for (int x = 0; x < 3; x++) {
+                jiv[c][x] = p.ivg[3 * g + x];
+                jv[c][x] = kd.vgpc[3 * j + x];
+            }
         }
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = tmem_sh;
-    const int nkb_half = kp8 / OZ_BK, nkb = 2 * nkb_half;
-    const int npad = p.npad;
 
-    if (warp == 0) {
-        // ------------------------------------------------ TMA producer
+    // All roles walk the same sequence: diagonal d = 2..S+1, slice s of the
+    // left operand = d-1 .. 1 (t = d - s of the right one), segments of
+    // seg_pairs consecutive pairs within a diagonal.
+    if (warp < 3) {
+        // ------------------------------------------------ TMA producers: warp w loads box w
         if (lane == 0) {
-            uint32_t fills[WS_STAGES] = {0, 0, 0, 0, 0, 0};
+            const int role = warp;                          // 0: A_r, 1: A_i, 2: B
+            uint32_t fills[OZ_STAGES] = {0, 0};
             long it = 0;
             bool bad = false;
-            for (int d = 2; d <= S + 1 && !bad; d++) {
-                const int s_lo = max(1, d - S), s_hi = min(S, d - 1);
-                for (int s = s_lo; s <= s_hi && !bad; s++) {
+            for (int d = 2; d <= S + 1 && !bad; d++)
+                for (int s = 1; s <= d - 1 && !bad; s++) {
                     const int t = d - s;
-                    for (int kb = 0; kb < nkb; kb++, it++) {
-                        const int st = (int)(it % WS_STAGES);
-                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) { bad = true; break; }
-                        mbar_expect_tx(&full[st], OZ_STAGE);
-                        const int h = kb / nkb_half, kk = (kb % nkb_half) * OZ_BK;
-                        const uint32_t sa = sbase + st * OZ_STAGE;
-                        tma_load_2d(sa, &mapA, kk, kd.oz_row0 + (h * S + (s - 1)) * npad + i0, &full[st]);
-#pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            tma_load_2d(sa + OZ_TILE + q * 4096, &mapB, kk,
-                                        kd.oz_row0 + (oz_barr(q, h) * S + (t - 1)) * npad + j0, &full[st]);
+                    for (int kb = 0; kb < nst; kb++, it++) {
+                        const int st = (int)(it % OZ_STAGES);
+                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
+                            bad = true;
+                            break;
+                        }
+                        mbar_expect_tx(&full[st], OZ_BOX);
+                        const uint32_t dst = sbase + st * OZ_STAGE + role * OZ_BOX;
+                        if (role < 2) {   // array Ar (2) or Ai (3) of G blocks i0/32 .. +3, slice s
+                            const int grp = (kd.oz_slot * S + (s - 1)) * nblk + (i0 >> 5);
+                            tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * OZ_KCH, &full[st]);
+                        } else {          // the four arrays of G block j0/32, slice t
+                            const int grp = (kd.oz_slot * S + (t - 1)) * nblk + (j0 >> 5);
+                            tma_load_4d(dst, &mapB, 0, 0, grp, kb * OZ_KCH, &full[st]);
+                        }
                         fills[st]++;
                     }
                 }
-            }
-            if (bad)   // let the copies already issued land before the CTA goes away
-                for (int st = 0; st < WS_STAGES; st++)
-                    if (fills[st] > 0) (void)mbar_wait(&full[st], (fills[st] - 1) & 1);
+            if (bad)   // copies already issued must land before the CTA goes away
+                for (int st = 0; st < OZ_STAGES; st++)
+                    if (fills[st] > 0) mbar_drain(&full[st], (fills[st] - 1) & 1);
         }
-    } else if (warp == 1) {
+    } else if (warp == 3) {
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = umma_idesc_i8(128, OZ_N);
-            uint32_t uses[WS_STAGES] = {0, 0, 0, 0, 0, 0};
-            int accuse[2] = {0, 0};
+            uint32_t uses[OZ_STAGES] = {0, 0};
+            int nseg = 0;
             long it = 0;
             bool bad = false;
-            for (int d = 2; d <= S + 1 && !bad; d++) {
-                const int b = (d - 2) & 1;
-                if (accuse[b] > 0 && !mbar_wait_ab(&acce[b], (accuse[b] - 1) & 1, abort)) { bad = true; break; }
-                tc_fence_after();
-                const uint32_t dtm = tbase + b * 128;
-                const int s_lo = max(1, d - S), s_hi = min(S, d - 1);
-                bool first = true;
-                for (int s = s_lo; s <= s_hi && !bad; s++)
-                    for (int kb = 0; kb < nkb; kb++, it++) {
-                        const int st = (int)(it % WS_STAGES);
-                        if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) { bad = true; break; }
-                        tc_fence_after();
-                        const uint32_t sa = sbase + st * OZ_STAGE, sb = sa + OZ_TILE;
-#pragma unroll
-                        for (int q = 0; q < OZ_BK / 32; q++) {
-                            umma_i8(dtm, umma_desc_sw128(sa + q * 32), umma_desc_sw128(sb + q * 32), idesc,
-                                    (first && q == 0) ? 0u : 1u);
-                        }
-                        first = false;
-                        umma_commit(&empty[st]);
-                        uses[st]++;
+            for (int d = 2; d <= S + 1 && !bad; d++)
+                for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
+                    const int s1 = min(d - 1, s0 + seg_pairs - 1);
+                    // the epilogue must have folded the previous segment
+                    if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
+                        bad = true;
+                        break;
                     }
-                if (!bad) {
-                    umma_commit(&accf[b]);
-                    accuse[b]++;
+                    tc_fence_after();
+                    bool first = true;
+                    for (int s = s0; s <= s1 && !bad; s++)
+                        for (int kb = 0; kb < nst; kb++, it++) {
+                            const int st = (int)(it % OZ_STAGES);
+                            if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
+                                bad = true;
+                                break;
+                            }
+                            tc_fence_after();
+                            const uint32_t sa = sbase + st * OZ_STAGE;
+#pragma unroll
+                            for (int c = 0; c < OZ_KCH; c++)
+#pragma unroll
+                                for (int q = 0; q < OZ_CHUNK / 32; q++) {
+                                    const uint32_t off = c * OZ_TILE + q * 32;
+                                    const uint64_t bd = umma_desc_sw128(sa + 2 * OZ_BOX + off);
+                                    const uint32_t acc = (first && c == 0 && q == 0) ? 0u : 1u;
+                                    umma_i8(tbase, umma_desc_sw128(sa + off), bd, idesc, acc);
+                                    umma_i8(tbase + 128, umma_desc_sw128(sa + OZ_BOX + off), bd, idesc, acc);
+                                }
+                            first = false;
+                            umma_commit(&empty[st]);
+                            uses[st]++;
+                        }
+                    if (!bad) {
+                        umma_commit(&accf);
+                        nseg++;
+                    }
                 }
-            }
             if (bad)   // MMAs already issued must finish before tensor memory is freed
-                for (int st = 0; st < WS_STAGES; st++)
-                    if (uses[st] > 0) (void)mbar_wait(&empty[st], (uses[st] - 1) & 1);
+                for (int st = 0; st < OZ_STAGES; st++)
+                    if (uses[st] > 0) mbar_drain(&empty[st], (uses[st] - 1) & 1);
         }
     } else {
-        // ------------------------------------------------ epilogue (warps 2..5)
-        const int qd = warp & 3;                                   // tensor-memory lane quadrant
+        // ------------------------------------------------ epilogue (warps 4..7)
+        const int qd = warp & 3;                                    // tensor-memory lane quadrant
         const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
-        int accn[2] = {0, 0};
+        int nseg = 0;
         bool bad = false;
-        for (int d = 2; d <= S + 1; d++) {
-            const int b = (d - 2) & 1;
-            // warp-uniform outcome: the tcgen05.ld/st below need the whole warp
-            const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf[b], accn[b] & 1, abort));
-            if (!ok) { bad = true; break; }
-            accn[b]++;
-            tc_fence_after();
+        for (int d = 2; d <= S + 1 && !bad; d++) {
             const double scale = ldexp(1.0, -7 * d);
+            for (int s0 = 1; s0 <= d - 1; s0 += seg_pairs) {
+                const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
+                if (!ok) {
+                    bad = true;
+                    break;
+                }
+                tc_fence_after();
+                const bool init = (nseg == 0);
+                // output block o (Re H, Im H, Re O, Im O) = r block o +- i block o^1
 #pragma unroll 1
-            for (int c = 0; c < OZ_N / 16; c++) {
-                uint32_t iv[16], lo[16], hi[16];
-                tm_ld16(t_lane + b * 128 + c * 16, iv);
-                if (d > 2) {
-                    tm_ld16(t_lane + WS_FP64_COL + c * 32, lo);
-                    tm_ld16(t_lane + WS_FP64_COL + c * 32 + 16, hi);
-                }
-                tm_wait_ld();
-                uint32_t o0[16], o1[16];
+                for (int o = 0; o < 4; o++) {
+                    const double sg = (o & 1) ? -1.0 : 1.0;
+#pragma unroll 1
+                    for (int jc = 0; jc < OZ_BJ; jc += 16) {
+                        uint32_t rv[16], iv[16], lo[16], hi[16];
+                        const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
+                        tm_ld16(t_lane + o * 32 + jc, rv);
+                        tm_ld16(t_lane + 128 + (o ^ 1) * 32 + jc, iv);
+                        if (!init) {
+                            tm_ld16(t_lane + fcol, lo);
+                            tm_ld16(t_lane + fcol + 16, hi);
+                        }
+                        tm_wait_ld();
+                        uint32_t o0[16], o1[16];
 #pragma unroll
-                for (int e = 0; e < 16; e++) {
-                    double a = 0.0;
-                    if (d > 2) {
-                        const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
-                        const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
-                        a = __hiloint2double((int)w1, (int)w0);
+                        for (int e = 0; e < 16; e++) {
+                            double a = 0.0;
+                            if (!init) {
+                                const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
+                                const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
+                                a = __hiloint2double((int)w1, (int)w0);
+                            }
+                            // r +- i is exact in FP64 (|int32| sums); one rounding per fold
+                            a += scale * ((double)(int)rv[e] + sg * (double)(int)iv[e]);
+                            const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
+                            if (e < 8) {
+                                o0[2 * e] = w0;
+                                o0[2 * e + 1] = w1;
+                            } else {
+                                o1[2 * (e - 8)] = w0;
+                                o1[2 * (e - 8) + 1] = w1;
+                            }
+                        }
+                        tm_st16(t_lane + fcol, o0);
+                        tm_st16(t_lane + fcol + 16, o1);
                     }
-                    a += scale * (double)(int)iv[e];
-                    const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
-                    if (e < 8) { o0[2 * e] = w0; o0[2 * e + 1] = w1; }
-                    else { o1[2 * (e - 8)] = w0; o1[2 * (e - 8) + 1] = w1; }
                 }
-                tm_st16(t_lane + WS_FP64_COL + c * 32, o0);
-                tm_st16(t_lane + WS_FP64_COL + c * 32 + 16, o1);
+                tm_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce);
+                nseg++;
             }
-            tm_wait_st();
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acce[b]);
         }
         if (__all_sync(0xffffffffu, !bad && !*abort)) {
             const int i = i0 + qd * 32 + lane;
@@ -702,35 +460,49 @@ oz_mma_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
             const bool row_ok = i < kd.ngp;
             if (row_ok) {
                 int g = kd.igpig[i] - 1;
-                if (g < 0 || g >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); g = 0; }
-                for (int x = 0; x < 3; x++) { ivi[x] = p.ivg[3 * g + x]; vi[x] = kd.vgpc[3 * i + x]; }
+                if (g < 0 || g >= p.ngrtot) {
+                    atomicOr(p.err, DEV_ERR_INDEX);
+                    g = 0;
+                }
+                for (int x = 0; x < 3; x++) {
+                    ivi[x] = p.ivg[3 * g + x];
+                    vi[x] = kd.vgpc[3 * i + x];
+                }
             }
             const double sai = row_ok ? kd.oz_scale[i] : 0.0;
 #pragma unroll 1
             for (int jc = 0; jc < OZ_BJ; jc += 8) {
                 double val[4][8];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
+                for (int o = 0; o < 4; o++) {
                     uint32_t w[16];
-                    tm_ld16(t_lane + WS_FP64_COL + 2 * (q * 32 + jc), w);
+                    tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
                     tm_wait_ld();
 #pragma unroll
-                    for (int e = 0; e < 8; e++) val[q][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+                    for (int e = 0; e < 8; e++) val[o][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
                 }
                 if (!row_ok) continue;
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
                     const int jj = jc + e, j = j0 + jj;
                     if (j >= kd.ngp || i > j) continue;
-                    const double sbj = kd.oz_scale[npad + j], saj = kd.oz_scale[j];
+                    const double sbj = kd.oz_scale[p.npad + j], saj = kd.oz_scale[j];
                     double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
                     double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
                     double ar, ai;
-                    if (interstitial(p, EPI_HAM, ivi, jiv[jj], vi, jv[jj], ar, ai)) { hr += ar; hi += ai; }
-                    if (interstitial(p, EPI_OVL, ivi, jiv[jj], vi, jv[jj], ar, ai)) { orr += ar; oi += ai; }
+                    if (interstitial(p, EPI_HAM, ivi, jiv[jj], vi, jv[jj], ar, ai)) {
+                        hr += ar;
+                        hi += ai;
+                    }
+                    if (interstitial(p, EPI_OVL, ivi, jiv[jj], vi, jv[jj], ar, ai)) {
+                        orr += ar;
+                        oi += ai;
+                    }
                     exs_complex hv, ov;
-                    hv.re = hr; hv.im = hi;
-                    ov.re = orr; ov.im = oi;
+                    hv.re = hr;
+                    hv.im = hi;
+                    ov.re = orr;
+                    ov.im = oi;
                     kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
                     kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
                     if (i < j) {
@@ -746,29 +518,60 @@ oz_mma_ws_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
     tc_fence_before();
     __syncthreads();
-    if (warp == 1) {
+    if (warp == 3) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(OZ_TMEM_COLS));
     }
 }
 
-cudaError_t launch_oz_mma_ws(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
-                             const void *d_tiles, int ntiles, int S, int kp8, cudaStream_t s)
+// ------------------------------------------------------------ host side
+int oz_kpad(int K) { return (K + 255) / 256 * 256; }
+
+size_t oz_slot_bytes(int S, int npad, int kp8) { return (size_t)S * npad * OZ_NARR * (size_t)kp8; }
+
+int oz_seg_pairs(int S, int kp8)
+{
+    // pairs whose int32 sums over K stay exact: pairs * kp8 * 127^2 < 2^31
+    const long long per = (long long)kp8 * 127 * 127;
+    long long n = (((long long)1 << 31) - 1) / per;
+    return (int)(n < 1 ? 0 : (n > S ? S : n));
+}
+
+cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s)
+{
+    oz_colscale_kernel<<<dim3((p.npad + 127) / 128, nk), 128, 0, s>>>(p, d_k);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    oz_split_kernel<<<dim3(kp8 / 32, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_oz_mma(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
+                          const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz_mma_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM);
+        cudaError_t e = cudaFuncSetAttribute(oz_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    oz_mma_ws_kernel<<<ntiles, WS_THREADS, WS_SMEM, s>>>(*mapA, *mapB, p, d_k, (const OzTile *)d_tiles, S, kp8);
+    oz_mma_kernel<<<ntiles, OZ_THREADS, OZ_SMEM, s>>>(*mapA, *mapB, p, d_k, (const OzTile *)d_tiles, S, kp8,
+                                                      seg_pairs);
     return cudaGetLastError();
 }
 
-// Tensor maps over the int8 slices of all slots: [rows][kp8] bytes, boxes of
-// 128 x 128 (A tile) and 32 x 128 (one B sub-block), 128-byte swizzle.
-bool make_oz_tensor_maps(void *base, size_t rows, int kp8, CUtensorMap *mapA, CUtensorMap *mapB)
+// TMA views of the slices of all slots (int8, 4D):
+//   d0: 128 bytes of K (one swizzle row)                     stride 1
+//   d1: the 128 rows of one (slot, slice, G block) group      stride kp8
+//       (4 arrays x 32 rows)
+//   d2: group index                                           stride 128 kp8
+//   d3: K chunk of 128 bytes                                  stride 128
+// A tile box {128, 32, 4, 2}: one array of 4 consecutive G blocks, 2 K chunks;
+// B tile box {128, 128, 1, 2}: all four arrays of one G block, 2 K chunks.
+// d3 is the outermost box dimension, so each K chunk lands in shared memory
+// as one contiguous 128-row x 128-byte tile.
+bool make_oz_tensor_maps(void *base, size_t groups, int kp8, CUtensorMap *mapA, CUtensorMap *mapB)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -781,17 +584,18 @@ bool make_oz_tensor_maps(void *base, size_t rows, int kp8, CUtensorMap *mapA, CU
             return false;
         encode = (EncodeFn)fn;
     }
-    const cuuint64_t dims[2] = {(cuuint64_t)kp8, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)kp8};
-    const cuuint32_t es[2] = {1, 1};
-    const cuuint32_t boxA[2] = {128, 128}, boxB[2] = {128, 32};
-    if (encode(mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
-        CUDA_SUCCESS)
+    if (kp8 % (OZ_KCH * OZ_CHUNK) != 0) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)OZ_CHUNK, 128, (cuuint64_t)groups, (cuuint64_t)(kp8 / OZ_CHUNK)};
+    const cuuint64_t strides[3] = {(cuuint64_t)kp8, (cuuint64_t)128 * kp8, (cuuint64_t)OZ_CHUNK};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const cuuint32_t boxA[4] = {OZ_CHUNK, 32, 4, OZ_KCH}, boxB[4] = {OZ_CHUNK, 128, 1, OZ_KCH};
+    if (encode(mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
-    if (encode(mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
-        CUDA_SUCCESS)
+    if (encode(mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
     return true;
 }
