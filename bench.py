@@ -295,6 +295,9 @@ def run_ours(args):
     def step_device():
         st.setup_batched_device(ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op)
 
+    # ---- kernel configuration chosen by the library's autotuner on this batch
+    tuned = st.autotune(ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op)
+
     # ---- device-resident timing
     for _ in range(args.warmup):
         step_device()
@@ -325,6 +328,27 @@ def run_ours(args):
     ms_max = float(t.item())
     value = ws * nk * args.steps / (ms_max * 1e-3)
     phase /= max(args.steps, 1)
+
+    # ---- the same batch replayed as one captured CUDA graph (no host work,
+    # no synchronisation between steps)
+    graph = st.graph(ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op)
+    for _ in range(args.warmup):
+        graph.launch()
+    st.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            graph.launch()
+        e1.record(stream)
+    st.synchronize()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    graph_ms = float(t.item())
+    graph.close()
 
     # ---- end to end through the host-pointer entry point
     if args.skip_e2e:
@@ -403,6 +427,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "k_per_step": nk, "ngp": [min(ngp), max(ngp)],
                        "nmat": [min(nmat), max(nmat)],
+                       "kernel_config": tuned,
                        "precision": ("split int8 x%d slices (tcgen05), FP64 recombination" % args.slices
                                      if args.precision == "ozaki" else "fp64 (DMMA)"),
                        "l2": "working set > 126 MB L2 (A/B planes 63 MB and H/O 48 MB per k-point), no flush"},
@@ -411,6 +436,9 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(d2h)},
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
+            "graph_replay": {"value": ws * nk * args.steps / (graph_ms * 1e-3), "unit": "setups/s",
+                             "ms_per_step": graph_ms / args.steps,
+                             "note": "same batch captured once (exs_graph_create) and replayed"},
             "roofline": roof,
             "cpu_baseline": None if cpu_v is None else {
                 "value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",

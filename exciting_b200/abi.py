@@ -47,6 +47,11 @@ SIGNATURES = {
     "exs_setup_batched": ([P, c_int, P, P, P, P, P], c_int),
     "exs_setup_batched_device": ([P, c_int, P, P, P, P, P], c_int),
     "exs_synchronize": ([P], c_int),
+    "exs_autotune": ([P, c_int, P, P, P, P, P, P], c_int),
+    "exs_set_kernel_config": ([P, c_int], c_int),
+    "exs_graph_create": ([P, c_int, P, P, P, P, P, P], c_int),
+    "exs_graph_launch": ([P], c_int),
+    "exs_graph_destroy": ([P], None),
     "exs_forcek": ([P, c_int, P, P, c_int, P, c_int, P, P, c_double, P, P, P], c_int),
     "exs_adjoint": ([P, c_int, P, P, c_int, P, c_int, P, P, P, P, P, P, P], c_int),
     "exs_set_stream": ([P, P], c_int),

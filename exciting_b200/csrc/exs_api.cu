@@ -41,11 +41,17 @@ cudaError_t dalloc(T **p, size_t n)
     return cudaMalloc((void **)p, n * sizeof(T));
 }
 
+// Copy n elements to the device array *p, allocating it on first use (the
+// sizes of every array uploaded more than once are fixed per context, so a
+// later upload reuses the allocation and captured graphs stay valid).
 template <class T>
 cudaError_t upload(T **p, const T *h, size_t n, cudaStream_t s)
 {
-    cudaError_t e = dalloc(p, n);
-    if (e != cudaSuccess || n == 0) return e;
+    if (n == 0) return cudaSuccess;
+    if (!*p) {
+        cudaError_t e = dalloc(p, n);
+        if (e != cudaSuccess) return e;
+    }
     return cudaMemcpyAsync(*p, h, n * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
@@ -316,6 +322,7 @@ int exs_ctx_create(const exs_config *cfg, exs_ctx **out)
 int exs_set_precision(exs_ctx *c, int mode, int slices)
 {
     if (!c) return EXS_ERR_ARG;
+    c->gen++;   // graphs captured before this call are no longer valid
     if (mode == EXS_PREC_FP64) {
         c->prec_mode = mode;
         return EXS_OK;
@@ -342,8 +349,11 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     c->oz_seg = seg;
     c->oz_slot_bytes = slot;
     // one tensor-map group = 128 rows (4 arrays x 32 G) of one slice of one slot
-    if (!exs::make_oz_tensor_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8, &c->oz_mapA,
-                                  &c->oz_mapB)) {
+    bool maps_ok = true;
+    for (int q = 0; q < exs::OZ_NCFG; q++)
+        maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8,
+                                                      exs::OZ_CFG_KCH[q], &c->oz_mapA[q], &c->oz_mapB[q]);
+    if (!maps_ok) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
         c->prec_mode = EXS_PREC_FP64;
@@ -351,6 +361,10 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     }
     c->slices = slices;
     c->prec_mode = mode;
+    {   // a configuration the autotuner chose earlier for this shape
+        auto it = c->oz_tuned.find(std::make_tuple((int)mode, c->npad, c->K, slices));
+        c->oz_cfg = it != c->oz_tuned.end() ? it->second : 0;
+    }
     return EXS_OK;
 }
 
@@ -366,13 +380,7 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
     cudaSetDevice(c->device);
     cudaStream_t s = c->stream;
     EXS_CUDA(cudaStreamSynchronize(s));
-    // free the previous iteration's copies
-    void **old[] = {(void **)&c->d_haa_r, (void **)&c->d_haa_i, (void **)&c->d_loa_r, (void **)&c->d_loa_i,
-                    (void **)&c->d_lolo, (void **)&c->d_oalo, (void **)&c->d_ololo, (void **)&c->d_h1aa,
-                    (void **)&c->d_h1loa, (void **)&c->d_h1lolo, (void **)&c->d_veffig, (void **)&c->d_kinw,
-                    (void **)&c->d_cfunig, (void **)&c->d_m2effig, (void **)&c->d_spr_tail, (void **)&c->d_apwfr_tail};
-    for (void **p : old)
-        if (*p) { cudaFree(*p); *p = nullptr; }
+    // a new SCF iteration overwrites the previous inputs in place
     c->have_inputs = false;
     const int nat = c->natmtot, maxaa = c->maxaa, maxnlo = std::max(c->maxnlo, 1);
     // h_a: aa(f, f', ias) -> planar [ias][f'][f] with leading dim ldh
@@ -532,90 +540,147 @@ void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t)
     }
 }
 
-int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
+// Layout of the packed tables (byte offsets from the start of the buffer).
+struct TableLayout {
+    size_t k, probs[4], work[4], oz, total;
+    int nwork[4], noz;
+};
+
+void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt, TableLayout &L)
 {
     exs::build_gemm_tables(c, ks, c->gt);
-    std::vector<int> ozt;
+    ozt.clear();
     if (c->prec_mode == EXS_PREC_OZAKI_INT8) oz_tiles(ks, ozt);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    size_t need = al(ks.size() * sizeof(KDesc)) + al(ozt.size() * sizeof(int));
-    for (int q = 0; q < 4; q++)
-        need += al(c->gt.probs[q].size() * sizeof(exs::GemmProb)) + al(c->gt.work[q].size() * sizeof(exs::TileWork));
+    size_t off = 0;
+    L.k = off;
+    off += al(ks.size() * sizeof(KDesc));
+    for (int q = 0; q < 4; q++) {
+        L.probs[q] = off;
+        off += al(c->gt.probs[q].size() * sizeof(exs::GemmProb));
+        L.work[q] = off;
+        off += al(c->gt.work[q].size() * sizeof(exs::TileWork));
+        L.nwork[q] = (int)c->gt.work[q].size();
+    }
+    L.oz = off;
+    off += al(ozt.size() * sizeof(int));
+    L.noz = (int)(ozt.size() / 3);
+    L.total = off;
+}
+
+void write_tables(const exs_ctx *c, const std::vector<KDesc> &ks, const std::vector<int> &ozt, const TableLayout &L,
+                  char *h)
+{
+    std::memcpy(h + L.k, ks.data(), ks.size() * sizeof(KDesc));
+    for (int q = 0; q < 4; q++) {
+        if (!c->gt.probs[q].empty())
+            std::memcpy(h + L.probs[q], c->gt.probs[q].data(), c->gt.probs[q].size() * sizeof(exs::GemmProb));
+        if (!c->gt.work[q].empty())
+            std::memcpy(h + L.work[q], c->gt.work[q].data(), c->gt.work[q].size() * sizeof(exs::TileWork));
+    }
+    if (!ozt.empty()) std::memcpy(h + L.oz, ozt.data(), ozt.size() * sizeof(int));
+}
+
+Uploaded device_view(const TableLayout &L, char *d)
+{
+    Uploaded u{};
+    u.d_k = (const KDesc *)(d + L.k);
+    for (int q = 0; q < 4; q++) {
+        u.d_probs[q] = d + L.probs[q];
+        u.d_work[q] = d + L.work[q];
+        u.nwork[q] = L.nwork[q];
+    }
+    u.d_oztiles = d + L.oz;
+    u.noztiles = L.noz;
+    return u;
+}
+
+int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
+{
+    std::vector<int> ozt;
+    TableLayout L;
+    pack_tables(c, ks, ozt, L);
     // the previous upload must have left the staging buffer
     EXS_CUDA(cudaEventSynchronize(c->tables_free));
-    if (need > c->tables_bytes) {
+    if (L.total > c->tables_bytes) {
         if (c->h_tables) cudaFreeHost(c->h_tables);
         if (c->d_tables) cudaFree(c->d_tables);
         c->h_tables = c->d_tables = nullptr;
         c->tables_bytes = 0;
-        const size_t cap = need * 2;
+        const size_t cap = L.total * 2;
         EXS_CUDA(cudaMallocHost(&c->h_tables, cap));
         EXS_CUDA(cudaMalloc(&c->d_tables, cap));
         c->tables_bytes = cap;
     }
-    char *h = (char *)c->h_tables;
-    char *d = (char *)c->d_tables;
-    size_t off = 0;
-    std::memcpy(h + off, ks.data(), ks.size() * sizeof(KDesc));
-    u.d_k = (const KDesc *)(d + off);
-    off += al(ks.size() * sizeof(KDesc));
-    for (int q = 0; q < 4; q++) {
-        const size_t pb = c->gt.probs[q].size() * sizeof(exs::GemmProb);
-        if (pb) std::memcpy(h + off, c->gt.probs[q].data(), pb);
-        u.d_probs[q] = d + off;
-        off += al(pb);
-        const size_t wb = c->gt.work[q].size() * sizeof(exs::TileWork);
-        if (wb) std::memcpy(h + off, c->gt.work[q].data(), wb);
-        u.d_work[q] = d + off;
-        u.nwork[q] = (int)c->gt.work[q].size();
-        off += al(wb);
-    }
-    if (!ozt.empty()) std::memcpy(h + off, ozt.data(), ozt.size() * sizeof(int));
-    u.d_oztiles = d + off;
-    u.noztiles = (int)(ozt.size() / 3);
-    off += al(ozt.size() * sizeof(int));
-    EXS_CUDA(cudaMemcpyAsync(c->d_tables, c->h_tables, off, cudaMemcpyHostToDevice, c->stream));
+    write_tables(c, ks, ozt, L, (char *)c->h_tables);
+    u = device_view(L, (char *)c->d_tables);
+    EXS_CUDA(cudaMemcpyAsync(c->d_tables, c->h_tables, L.total, cudaMemcpyHostToDevice, c->stream));
     EXS_CUDA(cudaEventRecord(c->tables_free, c->stream));
     return EXS_OK;
 }
 
-// Run the whole setup for the k descriptors in ks (device arrays filled).
-// If have_planes, the A planes are already in place (apwalm given).
-int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
+// Zero the column maxima that the A and B producers raise (split-precision
+// path only; the slots of one call are contiguous).
+cudaError_t oz_reset_maxima(exs_ctx *c, const std::vector<KDesc> &ks, cudaStream_t s)
 {
-    (void)cudaGetLastError();   // launch checks below read the last error: start clean
+    if (c->prec_mode != EXS_PREC_OZAKI_INT8 || ks.empty()) return cudaSuccess;
+    double *lo = ks[0].oz_scale, *hi = ks[0].oz_scale;
+    for (const KDesc &k : ks) {
+        lo = std::min(lo, k.oz_scale);
+        hi = std::max(hi, k.oz_scale);
+    }
+    return cudaMemsetAsync(lo, 0, sizeof(double) * ((size_t)(hi - lo) + 2 * (size_t)c->npad), s);
+}
+
+// Enqueue the whole setup for the k descriptors in ks (device arrays filled)
+// with the tables already on the device (u).  If have_planes, the A planes
+// are already in place (apwalm given).  With timed, the phase events
+// ev[0..4] are recorded (not while a graph is being captured).
+int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, bool have_planes, bool timed)
+{
     cudaStream_t s = c->stream;
     const DevParams p = c->params();
     int ngp_max = 0;
     for (auto &k : ks) ngp_max = std::max(ngp_max, k.ngp);
-    Uploaded u{};
-    int rc = upload_tables(c, ks, u);
-    if (rc != EXS_OK) return rc;
-    EXS_CUDA(cudaEventRecord(c->ev[0], s));
+#define EXS_EV(i) \
+    if (timed) EXS_CUDA(cudaEventRecord(c->ev[i], s))
+    EXS_EV(0);
+    if (!have_planes) EXS_CUDA(oz_reset_maxima(c, ks, s));
     if (!have_planes) EXS_CUDA(exs::launch_match_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     if (c->relativity == EXS_REL_IORA) EXS_CUDA(exs::launch_iora_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
-    EXS_CUDA(cudaEventRecord(c->ev[1], s));
+    EXS_EV(1);
     EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
                                    u.nwork[exs::EPI_PLANAR], u.d_k, s));
-    EXS_CUDA(cudaEventRecord(c->ev[2], s));
+    EXS_EV(2);
     if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
         EXS_CUDA(exs::launch_oz_prepare(p, u.d_k, (int)ks.size(), c->slices, c->kp8, s));
-        EXS_CUDA(exs::launch_oz_mma(&c->oz_mapA, &c->oz_mapB, p, u.d_k, u.d_oztiles, u.noztiles, c->slices, c->kp8,
-                                    c->oz_seg, s));
+        const int q = c->oz_cfg;
+        EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], &c->oz_mapB[q], p, u.d_k, u.d_oztiles, u.noztiles, c->slices,
+                                    c->kp8, c->oz_seg, s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
                                        u.nwork[exs::EPI_HAM], u.d_k, s));
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_OVL, p, u.d_probs[exs::EPI_OVL], u.d_work[exs::EPI_OVL],
                                        u.nwork[exs::EPI_OVL], u.d_k, s));
     }
-    EXS_CUDA(cudaEventRecord(c->ev[3], s));
+    EXS_EV(3);
     EXS_CUDA(exs::launch_gemm_kind(exs::EPI_LOROWS, p, u.d_probs[exs::EPI_LOROWS], u.d_work[exs::EPI_LOROWS],
                                    u.nwork[exs::EPI_LOROWS], u.d_k, s));
     EXS_CUDA(exs::launch_olp_apwlo(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_CUDA(exs::launch_lolo_blocks(p, u.d_k, (int)ks.size(), s));
-    EXS_CUDA(cudaEventRecord(c->ev[4], s));
-    c->timed = true;
+    EXS_EV(4);
+#undef EXS_EV
+    if (timed) c->timed = true;
     return EXS_OK;
+}
+
+int run_setup(exs_ctx *c, std::vector<KDesc> &ks, bool have_planes)
+{
+    (void)cudaGetLastError();   // launch checks below read the last error: start clean
+    Uploaded u{};
+    int rc = upload_tables(c, ks, u);
+    if (rc != EXS_OK) return rc;
+    return enqueue_setup(c, ks, u, have_planes, true);
 }
 
 KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double *d_vgpc, exs_complex *h, exs_complex *o)
@@ -640,31 +705,177 @@ KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double 
         k.ci = k.ai;
     }
     k.oz_slices = c->d_oz ? c->d_oz + (size_t)slot * c->oz_slot_bytes : nullptr;
-    k.oz_scale = c->d_ozscale ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
+    const bool oz = c->prec_mode == EXS_PREC_OZAKI_INT8 && c->d_ozscale;
+    k.oz_scale = oz ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
     k.oz_slot = slot;
     return k;
 }
 
+// Checks and k descriptors of the device-pointer entry points.
+int device_batch(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,
+                 exs_complex *const *h_dev, exs_complex *const *o_dev, std::vector<KDesc> &ks)
+{
+    if (!c || nk < 0 || (nk > 0 && (!ngp || !igpig_dev || !vgpc_dev || !h_dev || !o_dev)))
+        return fail(c, EXS_ERR_ARG, "bad argument");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    if (nk > c->max_batch) return fail(c, EXS_ERR_SIZE, "nk exceeds max_batch");
+    for (int k = 0; k < nk; k++)
+        if (ngp[k] <= 0 || ngp[k] > c->ngkmax || !h_dev[k] || !o_dev[k])
+            return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax or null output");
+    ks.clear();
+    for (int k = 0; k < nk; k++)
+        ks.push_back(slot_desc(c, k, ngp[k], igpig_dev + (size_t)c->ngkmax * k, vgpc_dev + 3 * (size_t)c->ngkmax * k,
+                               h_dev[k], o_dev[k]));
+    return EXS_OK;
+}
+
 }  // namespace
 
+struct exs_graph {
+    exs_ctx *c = nullptr;
+    unsigned gen = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void *d_tables = nullptr;
+};
+
 extern "C" {
+
+int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,
+                 exs_complex *const *h_dev, exs_complex *const *o_dev, int *choice)
+{
+    std::vector<KDesc> ks;
+    int rc = device_batch(c, nk, ngp, igpig_dev, vgpc_dev, h_dev, o_dev, ks);
+    if (rc != EXS_OK) return rc;
+    if (choice) *choice = 0;
+    if (nk == 0) return EXS_OK;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    if (c->prec_mode != EXS_PREC_OZAKI_INT8) {   // one configuration only: just run it
+        EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+        rc = run_setup(c, ks, false);
+        return rc < 0 ? rc : exs_synchronize(c);
+    }
+    (void)cudaGetLastError();
+    Uploaded u{};
+    rc = upload_tables(c, ks, u);
+    if (rc != EXS_OK) return rc;
+    constexpr int REPS = 3;
+    float best = 0.f;
+    int best_q = 0;
+    for (int q = 0; q < exs::OZ_NCFG; q++) {
+        c->oz_cfg = q;
+        EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+        rc = enqueue_setup(c, ks, u, false, false);      // warm-up
+        if (rc < 0) return rc;
+        EXS_CUDA(cudaEventRecord(c->ev[5], s));
+        for (int r = 0; r < REPS; r++) {
+            rc = enqueue_setup(c, ks, u, false, false);
+            if (rc < 0) return rc;
+        }
+        EXS_CUDA(cudaEventRecord(c->ev[6], s));
+        rc = exs_synchronize(c);
+        if (rc < 0) return rc;
+        float ms = 0.f;
+        EXS_CUDA(cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]));
+        if (q == 0 || ms < best) {
+            best = ms;
+            best_q = q;
+        }
+    }
+    c->oz_cfg = best_q;
+    c->oz_tuned[std::make_tuple((int)c->prec_mode, c->npad, c->K, c->slices)] = best_q;
+    if (choice) *choice = best_q;
+    return EXS_OK;
+}
+
+int exs_set_kernel_config(exs_ctx *c, int cfg)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (cfg < 0 || cfg >= exs::OZ_NCFG) return fail(c, EXS_ERR_ARG, "kernel configuration out of range");
+    c->oz_cfg = cfg;
+    return EXS_OK;
+}
+
+int exs_graph_create(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,
+                     exs_complex *const *h_dev, exs_complex *const *o_dev, exs_graph **out)
+{
+    if (!out) return fail(c, EXS_ERR_ARG, "exs_graph_create: null output");
+    *out = nullptr;
+    std::vector<KDesc> ks;
+    int rc = device_batch(c, nk, ngp, igpig_dev, vgpc_dev, h_dev, o_dev, ks);
+    if (rc != EXS_OK) return rc;
+    if (nk == 0) return fail(c, EXS_ERR_SIZE, "exs_graph_create: empty batch");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    (void)cudaGetLastError();
+    // the graph owns its tables: pack them once, outside the capture
+    std::vector<int> ozt;
+    TableLayout L;
+    pack_tables(c, ks, ozt, L);
+    std::vector<char> h(L.total);
+    write_tables(c, ks, ozt, L, h.data());
+    exs_graph *G = new exs_graph;
+    G->c = c;
+    G->gen = c->gen;
+    auto bail = [&](int code) {
+        if (G->exec) cudaGraphExecDestroy(G->exec);
+        if (G->graph) cudaGraphDestroy(G->graph);
+        if (G->d_tables) cudaFree(G->d_tables);
+        delete G;
+        return code;
+    };
+    if (cudaMalloc(&G->d_tables, L.total) != cudaSuccess) return bail(fail(c, EXS_ERR_NOMEM, "graph tables"));
+    if (cudaMemcpy(G->d_tables, h.data(), L.total, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(c, EXS_ERR_CUDA, "graph tables upload"));
+    const Uploaded u = device_view(L, (char *)G->d_tables);
+    // one plain run first: kernel attributes are set on first launch, outside any capture
+    if (cudaMemsetAsync(c->d_err, 0, sizeof(int), s) != cudaSuccess) return bail(fail(c, EXS_ERR_CUDA, "memset"));
+    rc = enqueue_setup(c, ks, u, false, false);
+    if (rc < 0) return bail(rc);
+    rc = exs_synchronize(c);
+    if (rc < 0) return bail(rc);
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return bail(fail(c, EXS_ERR_CUDA, "cudaStreamBeginCapture"));
+    cudaError_t e = cudaMemsetAsync(c->d_err, 0, sizeof(int), s);
+    rc = e == cudaSuccess ? enqueue_setup(c, ks, u, false, false) : EXS_ERR_CUDA;
+    cudaError_t ee = cudaStreamEndCapture(s, &G->graph);
+    if (rc < 0 || ee != cudaSuccess) return bail(rc < 0 ? rc : fail(c, EXS_ERR_CUDA, "cudaStreamEndCapture"));
+    if (cudaGraphInstantiate(&G->exec, G->graph, 0) != cudaSuccess)
+        return bail(fail(c, EXS_ERR_CUDA, "cudaGraphInstantiate"));
+    *out = G;
+    return EXS_OK;
+}
+
+int exs_graph_launch(exs_graph *G)
+{
+    if (!G) return EXS_ERR_ARG;
+    exs_ctx *c = G->c;
+    if (G->gen != c->gen) return fail(c, EXS_ERR_STATE, "graph captured before the last exs_set_precision");
+    cudaSetDevice(c->device);
+    EXS_CUDA(cudaGraphLaunch(G->exec, c->stream));
+    c->timed = false;
+    return EXS_OK;
+}
+
+void exs_graph_destroy(exs_graph *G)
+{
+    if (!G) return;
+    cudaSetDevice(G->c->device);
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    if (G->d_tables) cudaFree(G->d_tables);
+    delete G;
+}
 
 int exs_setup_batched_device(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,
                              exs_complex *const *h_dev, exs_complex *const *o_dev)
 {
-    if (!c || nk < 0 || (nk > 0 && (!ngp || !igpig_dev || !vgpc_dev || !h_dev || !o_dev)))
-        return fail(c, EXS_ERR_ARG, "exs_setup_batched_device: bad argument");
-    if (nk > c->max_batch) return fail(c, EXS_ERR_SIZE, "nk exceeds max_batch");
-    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
-    for (int k = 0; k < nk; k++)
-        if (ngp[k] <= 0 || ngp[k] > c->ngkmax || !h_dev[k] || !o_dev[k])
-            return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax or null output");
+    std::vector<KDesc> ks;
+    int rc = device_batch(c, nk, ngp, igpig_dev, vgpc_dev, h_dev, o_dev, ks);
+    if (rc != EXS_OK) return rc;
     cudaSetDevice(c->device);
     EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
-    std::vector<KDesc> ks;
-    for (int k = 0; k < nk; k++)
-        ks.push_back(slot_desc(c, k, ngp[k], igpig_dev + (size_t)c->ngkmax * k, vgpc_dev + 3 * (size_t)c->ngkmax * k,
-                               h_dev[k], o_dev[k]));
     if (nk == 0) return EXS_OK;
     return run_setup(c, ks, false);
 }
@@ -774,7 +985,8 @@ int exs_hamiltonandoverlapsetup(exs_ctx *c, int ngp, const exs_complex *apwalm, 
     EXS_CUDA(cudaMemcpyAsync(c->d_vgpc, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyHostToDevice, s));
     std::vector<KDesc> ks;
     ks.push_back(slot_desc(c, 0, ngp, c->d_igpig, c->d_vgpc, c->d_ho, c->d_ho + (size_t)c->nmatmax * c->nmatmax));
-    EXS_CUDA(exs::launch_apwalm_to_planes(c->params(), ngp, c->d_apwalm, ks[0].ar, ks[0].ai, s));
+    EXS_CUDA(oz_reset_maxima(c, ks, s));
+    EXS_CUDA(exs::launch_apwalm_to_planes(c->params(), ngp, c->d_apwalm, ks[0].ar, ks[0].ai, ks[0].oz_scale, s));
     int rc = run_setup(c, ks, true);
     if (rc < 0) return rc;
     const size_t bytes = sizeof(exs_complex) * (size_t)ks[0].nmat * ks[0].nmat;

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/exciting_b200.h"
@@ -18,6 +20,17 @@ enum : int {
     DEV_WARN_SINGULAR = 2,
     DEV_ERR_TIMEOUT = 4,  // a bounded wait in a kernel expired
 };
+
+// Pipeline configurations of the split-precision kernel.
+constexpr int OZ_NCFG = 2;
+static_assert(OZ_NCFG == EXS_OZ_NCONFIG, "public configuration count");
+
+// atomicMax for non-negative doubles: their IEEE bit patterns order like
+// unsigned integers.
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
+{
+    atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
+}
 
 // One atom's place in the device layouts.
 struct AtomDesc {
@@ -41,7 +54,7 @@ struct KDesc {
     double *br, *bi;         // B = blockdiag(h_a) A planes
     double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
     int8_t *oz_slices;       // split-precision path: int8 slices of this slot [S][npad/32][4][32][kp8]
-    double *oz_scale;        // split-precision path: column scales of A and B [2][npad]
+    double *oz_scale;        // split-precision path: column maxima of |A| and |B| [2][npad] (null: FP64 path)
     int oz_slot;             // split-precision path: slot index in the slice tensor maps
 };
 
@@ -94,6 +107,7 @@ struct GemmProb {
     long ldz;
     int row0;              // EPI_LOROWS: za row of m = 0
     int kidx;              // k-point of this problem (interstitial tables)
+    double *colmax;        // EPI_PLANAR: column maxima of |out| raised atomically (split precision), or null
 };
 
 struct TileWork {
@@ -169,7 +183,10 @@ struct exs_ctx {
     int8_t *d_oz = nullptr;      // int8 slices of all slots
     double *d_ozscale = nullptr; // column scales of all slots
     size_t oz_slot_bytes = 0;
-    CUtensorMap oz_mapA, oz_mapB;     // TMA views of d_oz
+    CUtensorMap oz_mapA[exs::OZ_NCFG], oz_mapB[exs::OZ_NCFG];   // TMA views of d_oz per pipeline configuration
+    int oz_cfg = 0;                   // pipeline configuration of the split-precision kernel
+    unsigned gen = 0;                 // bumped when device buffers that captured graphs use are replaced
+    std::map<std::tuple<int, int, int, int>, int> oz_tuned;   // (prec, npad, K, slices) -> configuration
     // runtime
     int device = 0;
     cudaStream_t stream = nullptr;      // stream the work runs on
@@ -190,7 +207,7 @@ cudaError_t launch_match_planes(const DevParams &p, const KDesc *d_k, int nk, in
 cudaError_t launch_match_ref(const DevParams &p, int ngp, int ngkmax, const double *gpc, const double *tpgpc,
                              const exs_complex *sfacgp, exs_complex *apwalm, cudaStream_t s);
 cudaError_t launch_apwalm_to_planes(const DevParams &p, int ngp, const exs_complex *apwalm, double *ar,
-                                    double *ai, cudaStream_t s);
+                                    double *ai, double *amax, cudaStream_t s);
 cudaError_t launch_iora_planes(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 cudaError_t launch_lolo_blocks(const DevParams &p, const KDesc *d_k, int nk, cudaStream_t s);
 cudaError_t launch_olp_apwlo(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
@@ -200,9 +217,11 @@ cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, 
                              const KDesc *d_k, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)
 cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s);
-cudaError_t launch_oz_mma(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
-                          const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s);
-bool make_oz_tensor_maps(void *base, size_t groups, int kp8, CUtensorMap *mapA, CUtensorMap *mapB);
+cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
+                          const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                          cudaStream_t s);
+bool make_oz_tensor_maps(void *base, size_t groups, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB);
+extern const int OZ_CFG_KCH[OZ_NCFG], OZ_CFG_NST[OZ_NCFG];
 int oz_kpad(int K);
 size_t oz_slot_bytes(int S, int npad, int kp8);
 int oz_seg_pairs(int S, int kp8);

@@ -107,11 +107,14 @@ __global__ void match_planes_kernel(DevParams p, const KDesc *ks)
     double s, c;
     sincos(v[0] * at.pos[0] + v[1] * at.pos[1] + v[2] * at.pos[2], &s, &c);
     int f = 0;
+    double amax = 0.0;
     match_point(p, ias, gpc, theta, phi, c, s, p.lmaxmat, [&](int, int, int, double re, double im) {
         ar[(size_t)f * p.npad] = re;
         ai[(size_t)f * p.npad] = im;
+        amax = fmax(amax, fmax(fabs(re), fabs(im)));
         f++;
     });
+    if (k.oz_scale) atomic_max_nonneg(k.oz_scale + g, amax);   // column maximum for the split-precision path
 }
 
 __global__ void match_ref_kernel(DevParams p, int ngp, int ngkmax, const double *gpc, const double *tpgpc,
@@ -138,7 +141,8 @@ __global__ void match_ref_kernel(DevParams p, int ngp, int ngkmax, const double 
 }
 
 // apwalm (reference layout) -> A planes of one k-point.
-__global__ void apwalm_to_planes_kernel(DevParams p, int ngp, const exs_complex *apwalm, double *ar, double *ai)
+__global__ void apwalm_to_planes_kernel(DevParams p, int ngp, const exs_complex *apwalm, double *ar, double *ai,
+                                        double *amax_out)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int ias = blockIdx.y;
@@ -146,6 +150,7 @@ __global__ void apwalm_to_planes_kernel(DevParams p, int ngp, const exs_complex 
     const AtomDesc at = p.atoms[ias];
     const int *apw = p.apword + (size_t)(p.lmaxapw + 1) * at.species;
     int f = at.apw_off;
+    double amax = 0.0;
     for (int l = 0; l <= p.lmaxmat; l++)
         for (int m = -l; m <= l; m++) {
             const int lm = l * (l + 1) + m;
@@ -157,8 +162,10 @@ __global__ void apwalm_to_planes_kernel(DevParams p, int ngp, const exs_complex 
                 }
                 ar[(size_t)f * p.npad + g] = re;
                 ai[(size_t)f * p.npad + g] = im;
+                amax = fmax(amax, fmax(fabs(re), fabs(im)));
             }
         }
+    if (amax_out) atomic_max_nonneg(amax_out + g, amax);
 }
 
 // (I + h1aa) A for the IORA overlap (overlapsetup.f90:72-87):
@@ -211,10 +218,10 @@ cudaError_t launch_match_ref(const DevParams &p, int ngp, int ngkmax, const doub
 }
 
 cudaError_t launch_apwalm_to_planes(const DevParams &p, int ngp, const exs_complex *apwalm, double *ar,
-                                    double *ai, cudaStream_t s)
+                                    double *ai, double *amax, cudaStream_t s)
 {
     dim3 grid((p.npad + 127) / 128, p.natmtot, 1);
-    apwalm_to_planes_kernel<<<grid, 128, 0, s>>>(p, ngp, apwalm, ar, ai);
+    apwalm_to_planes_kernel<<<grid, 128, 0, s>>>(p, ngp, apwalm, ar, ai, amax);
     return cudaGetLastError();
 }
 

@@ -25,10 +25,14 @@
 //   [slot][slice][32-row block of G][array: Br, Bi, Ar, Ai][32 rows][kp8]
 // so that a B tile (one G block, all four arrays) is 128 consecutive rows and
 // an A tile (one array of four consecutive G blocks) is a regular stride:
-// each operand tile of a pipeline stage (two 128-byte K chunks) is ONE TMA
-// box of 32 KB.  Boxes are written with 128-byte swizzling; the MMA
+// each operand tile of a pipeline stage (KCH 128-byte K chunks) is ONE TMA
+// box of KCH x 16 KB.  Boxes are written with 128-byte swizzling; the MMA
 // descriptors use the matching SWIZZLE_128B K-major layout (8-row x 128-byte
 // atoms, 1024 B between 8-row groups, K advanced 32 bytes per MMA).
+//
+// Pipeline configurations (chosen per problem by the autotuner):
+//   KCH K chunks per stage (box = KCH x 16 KB) x NST stages, 192 KB in all:
+//   (2, 2) and (1, 4).
 //
 // Roles (one CTA per 128 x 32 output tile, 256 threads):
 //   warps 0-2  one TMA producer thread each (A_r, A_i and B box of a stage)
@@ -53,13 +57,9 @@ constexpr int OZ_BJ = 32;                        // tile columns (G_j); MMA N = 
 constexpr int OZ_N = 4 * OZ_BJ;
 constexpr int OZ_NARR = 4;                       // Br, Bi, Ar, Ai
 constexpr int OZ_CHUNK = 128;                    // bytes of K in one swizzle row
-constexpr int OZ_KCH = 2;                        // K chunks per pipeline stage
 constexpr int OZ_TILE = 128 * OZ_CHUNK;          // 16 KB: one K chunk of a 128-row operand
-constexpr int OZ_BOX = OZ_KCH * OZ_TILE;         // 32 KB: one TMA box
-constexpr int OZ_STAGE = 3 * OZ_BOX;             // A_r, A_i, B
-constexpr int OZ_STAGES = 2;
-constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE + 1024;
 constexpr int OZ_THREADS = 256;
+constexpr int OZ_MAX_KCH = 2;                    // K chunks per stage of the widest configuration
 constexpr int OZ_TMEM_COLS = 512;
 constexpr int OZ_FP64_COL = 256;
 constexpr long long OZ_WAIT_CYCLES = 2000000000LL;   // ~1 s at 2 GHz
@@ -188,25 +188,15 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
 // ------------------------------------------------------------ preparation
-// Column scales sigma(G) = 2^e with max|column| < 2^e (frexp), for A (Ar, Ai)
-// and for B (Br, Bi).  One thread per (G, k-point).
-__global__ void oz_colscale_kernel(DevParams p, const KDesc *ks)
+// Column scale sigma(G) = 2^e with max|column| < 2^e (frexp) from the column
+// maximum m that the producers of the A and B planes left in oz_scale (the
+// matching kernels for A, the h_a A epilogue for B).  An all-zero column
+// gets sigma = 1.
+__host__ __device__ __forceinline__ double oz_sigma(double m)
 {
-    const KDesc k = ks[blockIdx.y];
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= p.npad) return;
-    double ma = 0.0, mb = 0.0;
-    if (g < k.ngp)
-        for (int f = 0; f < p.K; f++) {
-            const size_t i = (size_t)f * p.npad + g;
-            ma = fmax(ma, fmax(fabs(k.ar[i]), fabs(k.ai[i])));
-            mb = fmax(mb, fmax(fabs(k.br[i]), fabs(k.bi[i])));
-        }
-    int ea = 0, eb = 0;
-    if (ma > 0.0) frexp(ma, &ea);
-    if (mb > 0.0) frexp(mb, &eb);
-    k.oz_scale[g] = ldexp(1.0, ea);
-    k.oz_scale[p.npad + g] = ldexp(1.0, eb);
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);
+    return ldexp(1.0, e);
 }
 
 // Byte offset of (slice s, array a, row G, K index f) inside one slot.
@@ -238,7 +228,7 @@ __global__ void oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
     for (int r = ty; r < 32; r += 8) {
         const int g = g0 + r, f = f0 + tx;
         if (g >= p.npad || f >= kp8) continue;
-        const double sa = k.oz_scale[g], sb = k.oz_scale[p.npad + g];
+        const double sa = oz_sigma(k.oz_scale[g]), sb = oz_sigma(k.oz_scale[p.npad + g]);
         double x[OZ_NARR] = {t[0][tx][r] / sb, t[1][tx][r] / sb, t[2][tx][r] / sa, t[3][tx][r] / sa};
         for (int s = 0; s < S; s++)
 #pragma unroll
@@ -252,12 +242,15 @@ __global__ void oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
 }
 
 // ------------------------------------------------------------ main kernel
+template <int KCH, int NST>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
               const KDesc *ks, const OzTile *tiles, int S, int kp8, int seg_pairs)
 {
+    constexpr int BOX = KCH * OZ_TILE;          // one TMA box
+    constexpr int STAGE = 3 * BOX;              // A_r, A_i, B
     extern __shared__ __align__(1024) uint8_t oz_smem[];
-    __shared__ uint64_t full[OZ_STAGES], empty[OZ_STAGES], accf, acce;
+    __shared__ uint64_t full[NST], empty[NST], accf, acce;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
     __shared__ int jiv[OZ_BJ][3];
@@ -270,7 +263,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     const int i0 = tl.ib * OZ_BM, j0 = tl.jb * OZ_BJ;
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
     const int nblk = p.npad / 32;
-    const int nst = kp8 / (OZ_KCH * OZ_CHUNK);        // pipeline stages per slice pair
+    const int nst = kp8 / (KCH * OZ_CHUNK);           // pipeline stages per slice pair
 
     if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
@@ -278,7 +271,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 0) {
-        for (int s = 0; s < OZ_STAGES; s++) {
+        for (int s = 0; s < NST; s++) {
             mbar_init(&full[s], 3);
             mbar_init(&empty[s], 1);
         }
@@ -307,47 +300,50 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     const uint32_t tbase = tmem_sh;
 
     // All roles walk the same sequence: diagonal d = 2..S+1, slice s of the
-    // left operand = d-1 .. 1 (t = d - s of the right one), segments of
+    // left operand = 1 .. d-1 (t = d - s of the right one), segments of
     // seg_pairs consecutive pairs within a diagonal.
     if (warp < 3) {
         // ------------------------------------------------ TMA producers: warp w loads box w
         if (lane == 0) {
             const int role = warp;                          // 0: A_r, 1: A_i, 2: B
-            uint32_t fills[OZ_STAGES] = {0, 0};
-            long it = 0;
+            uint32_t fills[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) fills[q] = 0;
+            int st = 0;
             bool bad = false;
             for (int d = 2; d <= S + 1 && !bad; d++)
                 for (int s = 1; s <= d - 1 && !bad; s++) {
                     const int t = d - s;
-                    for (int kb = 0; kb < nst; kb++, it++) {
-                        const int st = (int)(it % OZ_STAGES);
+                    for (int kb = 0; kb < nst; kb++) {
                         if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
                             bad = true;
                             break;
                         }
-                        mbar_expect_tx(&full[st], OZ_BOX);
-                        const uint32_t dst = sbase + st * OZ_STAGE + role * OZ_BOX;
+                        mbar_expect_tx(&full[st], BOX);
+                        const uint32_t dst = sbase + st * STAGE + role * BOX;
                         if (role < 2) {   // array Ar (2) or Ai (3) of G blocks i0/32 .. +3, slice s
                             const int grp = (kd.oz_slot * S + (s - 1)) * nblk + (i0 >> 5);
-                            tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * OZ_KCH, &full[st]);
+                            tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * KCH, &full[st]);
                         } else {          // the four arrays of G block j0/32, slice t
                             const int grp = (kd.oz_slot * S + (t - 1)) * nblk + (j0 >> 5);
-                            tma_load_4d(dst, &mapB, 0, 0, grp, kb * OZ_KCH, &full[st]);
+                            tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
                         }
                         fills[st]++;
+                        st = (st + 1 == NST) ? 0 : st + 1;
                     }
                 }
             if (bad)   // copies already issued must land before the CTA goes away
-                for (int st = 0; st < OZ_STAGES; st++)
-                    if (fills[st] > 0) mbar_drain(&full[st], (fills[st] - 1) & 1);
+                for (int q = 0; q < NST; q++)
+                    if (fills[q] > 0) mbar_drain(&full[q], (fills[q] - 1) & 1);
         }
     } else if (warp == 3) {
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = umma_idesc_i8(128, OZ_N);
-            uint32_t uses[OZ_STAGES] = {0, 0};
-            int nseg = 0;
-            long it = 0;
+            uint32_t uses[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) uses[q] = 0;
+            int nseg = 0, st = 0;
             bool bad = false;
             for (int d = 2; d <= S + 1 && !bad; d++)
                 for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
@@ -360,27 +356,27 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     tc_fence_after();
                     bool first = true;
                     for (int s = s0; s <= s1 && !bad; s++)
-                        for (int kb = 0; kb < nst; kb++, it++) {
-                            const int st = (int)(it % OZ_STAGES);
+                        for (int kb = 0; kb < nst; kb++) {
                             if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
                                 bad = true;
                                 break;
                             }
                             tc_fence_after();
-                            const uint32_t sa = sbase + st * OZ_STAGE;
+                            const uint32_t sa = sbase + st * STAGE;
 #pragma unroll
-                            for (int c = 0; c < OZ_KCH; c++)
+                            for (int c = 0; c < KCH; c++)
 #pragma unroll
                                 for (int q = 0; q < OZ_CHUNK / 32; q++) {
                                     const uint32_t off = c * OZ_TILE + q * 32;
-                                    const uint64_t bd = umma_desc_sw128(sa + 2 * OZ_BOX + off);
+                                    const uint64_t bd = umma_desc_sw128(sa + 2 * BOX + off);
                                     const uint32_t acc = (first && c == 0 && q == 0) ? 0u : 1u;
                                     umma_i8(tbase, umma_desc_sw128(sa + off), bd, idesc, acc);
-                                    umma_i8(tbase + 128, umma_desc_sw128(sa + OZ_BOX + off), bd, idesc, acc);
+                                    umma_i8(tbase + 128, umma_desc_sw128(sa + BOX + off), bd, idesc, acc);
                                 }
                             first = false;
                             umma_commit(&empty[st]);
                             uses[st]++;
+                            st = (st + 1 == NST) ? 0 : st + 1;
                         }
                     if (!bad) {
                         umma_commit(&accf);
@@ -388,8 +384,8 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     }
                 }
             if (bad)   // MMAs already issued must finish before tensor memory is freed
-                for (int st = 0; st < OZ_STAGES; st++)
-                    if (uses[st] > 0) mbar_drain(&empty[st], (uses[st] - 1) & 1);
+                for (int q = 0; q < NST; q++)
+                    if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
         }
     } else {
         // ------------------------------------------------ epilogue (warps 4..7)
@@ -469,7 +465,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     vi[x] = kd.vgpc[3 * i + x];
                 }
             }
-            const double sai = row_ok ? kd.oz_scale[i] : 0.0;
+            const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
 #pragma unroll 1
             for (int jc = 0; jc < OZ_BJ; jc += 8) {
                 double val[4][8];
@@ -486,7 +482,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 for (int e = 0; e < 8; e++) {
                     const int jj = jc + e, j = j0 + jj;
                     if (j >= kd.ngp || i > j) continue;
-                    const double sbj = kd.oz_scale[p.npad + j], saj = kd.oz_scale[j];
+                    const double sbj = oz_sigma(kd.oz_scale[p.npad + j]), saj = oz_sigma(kd.oz_scale[j]);
                     double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
                     double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
                     double ar, ai;
@@ -525,7 +521,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
 }
 
 // ------------------------------------------------------------ host side
-int oz_kpad(int K) { return (K + 255) / 256 * 256; }
+int oz_kpad(int K) { return (K + OZ_MAX_KCH * OZ_CHUNK - 1) / (OZ_MAX_KCH * OZ_CHUNK) * (OZ_MAX_KCH * OZ_CHUNK); }
 
 size_t oz_slot_bytes(int S, int npad, int kp8) { return (size_t)S * npad * OZ_NARR * (size_t)kp8; }
 
@@ -537,28 +533,42 @@ int oz_seg_pairs(int S, int kp8)
     return (int)(n < 1 ? 0 : (n > S ? S : n));
 }
 
+const int OZ_CFG_KCH[OZ_NCFG] = {2, 1};
+const int OZ_CFG_NST[OZ_NCFG] = {2, 4};
+
 cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s)
 {
-    oz_colscale_kernel<<<dim3((p.npad + 127) / 128, nk), 128, 0, s>>>(p, d_k);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
     oz_split_kernel<<<dim3(kp8 / 32, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8);
     return cudaGetLastError();
 }
 
-cudaError_t launch_oz_mma(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
-                          const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s)
+template <int KCH, int NST>
+static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
+                              const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s)
 {
-    if (ntiles <= 0) return cudaSuccess;
+    constexpr int smem = NST * 3 * KCH * OZ_TILE + 1024;
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM);
+        cudaError_t e =
+            cudaFuncSetAttribute(oz_mma_kernel<KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    oz_mma_kernel<<<ntiles, OZ_THREADS, OZ_SMEM, s>>>(*mapA, *mapB, p, d_k, (const OzTile *)d_tiles, S, kp8,
-                                                      seg_pairs);
+    oz_mma_kernel<KCH, NST><<<ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const OzTile *)d_tiles, S, kp8,
+                                                             seg_pairs);
     return cudaGetLastError();
+}
+
+cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
+                          const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                          cudaStream_t s)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    switch (cfg) {
+    case 0: return launch_cfg<2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
+    case 1: return launch_cfg<1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 // TMA views of the slices of all slots (int8, 4D):
@@ -567,11 +577,11 @@ cudaError_t launch_oz_mma(const CUtensorMap *mapA, const CUtensorMap *mapB, cons
 //       (4 arrays x 32 rows)
 //   d2: group index                                           stride 128 kp8
 //   d3: K chunk of 128 bytes                                  stride 128
-// A tile box {128, 32, 4, 2}: one array of 4 consecutive G blocks, 2 K chunks;
-// B tile box {128, 128, 1, 2}: all four arrays of one G block, 2 K chunks.
+// A tile box {128, 32, 4, kch}: one array of 4 consecutive G blocks;
+// B tile box {128, 128, 1, kch}: all four arrays of one G block.
 // d3 is the outermost box dimension, so each K chunk lands in shared memory
 // as one contiguous 128-row x 128-byte tile.
-bool make_oz_tensor_maps(void *base, size_t groups, int kp8, CUtensorMap *mapA, CUtensorMap *mapB)
+bool make_oz_tensor_maps(void *base, size_t groups, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -584,11 +594,11 @@ bool make_oz_tensor_maps(void *base, size_t groups, int kp8, CUtensorMap *mapA, 
             return false;
         encode = (EncodeFn)fn;
     }
-    if (kp8 % (OZ_KCH * OZ_CHUNK) != 0) return false;
+    if (kch < 1 || kch > OZ_MAX_KCH || kp8 % (OZ_MAX_KCH * OZ_CHUNK) != 0) return false;
     const cuuint64_t dims[4] = {(cuuint64_t)OZ_CHUNK, 128, (cuuint64_t)groups, (cuuint64_t)(kp8 / OZ_CHUNK)};
     const cuuint64_t strides[3] = {(cuuint64_t)kp8, (cuuint64_t)128 * kp8, (cuuint64_t)OZ_CHUNK};
     const cuuint32_t es[4] = {1, 1, 1, 1};
-    const cuuint32_t boxA[4] = {OZ_CHUNK, 32, 4, OZ_KCH}, boxB[4] = {OZ_CHUNK, 128, 1, OZ_KCH};
+    const cuuint32_t boxA[4] = {OZ_CHUNK, 32, 4, (cuuint32_t)kch}, boxB[4] = {OZ_CHUNK, 128, 1, (cuuint32_t)kch};
     if (encode(mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)

@@ -148,6 +148,24 @@ zgemm_dmma_kernel(DevParams p, const GemmProb *probs, const TileWork *work, cons
     __syncthreads();
 
     if (KIND == EPI_PLANAR) {
+        // split-precision path: column maxima of |B| (rows m of this tile),
+        // reduced over the 8 row groups of a warp, then one atomic per column
+        double *bmax = P.colmax;
+        if (bmax) {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    double mx = 0.0;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) mx = fmax(mx, fmax(fabs(cre[i][j][h]), fabs(cim[i][j][h])));
+                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 4));
+                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
+                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+                    const int n = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + h;
+                    if (lane < 4 && n < P.N) atomic_max_nonneg(bmax + n, mx);
+                }
+        }
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -269,6 +287,7 @@ void build_gemm_tables(const exs_ctx *c, const std::vector<KDesc> &ks, GemmTable
                 P.outi = ks[k].bi + (size_t)a.apw_off * c->npad;
                 P.ldo = c->npad;
                 P.kidx = (int)k;
+                P.colmax = ks[k].oz_scale ? ks[k].oz_scale + c->npad : nullptr;
                 const int pi = (int)t.probs[EPI_PLANAR].size();
                 t.probs[EPI_PLANAR].push_back(P);
                 for (int tm = 0; tm < (P.M + GB_M - 1) / GB_M; tm++)

@@ -189,6 +189,33 @@ class Setup:
         return self._check(self.lib.exs_setup_batched_device(self.ctx, nk, _ptr(ngp), ctypes.c_void_p(igpig_dev_ptr),
                                                              ctypes.c_void_p(vgpc_dev_ptr), hp, op))
 
+    def _device_batch_args(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs):
+        nk = len(ngp)
+        ngp = np.asarray(ngp, dtype=np.int32)
+        hp = (ctypes.c_void_p * nk)(*h_ptrs)
+        op = (ctypes.c_void_p * nk)(*o_ptrs)
+        return (nk, ngp, hp, op), (self.ctx, nk, _ptr(ngp), ctypes.c_void_p(igpig_dev_ptr),
+                                   ctypes.c_void_p(vgpc_dev_ptr), hp, op)
+
+    def autotune(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs) -> int:
+        """Time every kernel configuration of the active precision on this batch
+        (device pointers as for setup_batched_device) and keep the fastest."""
+        keep, args = self._device_batch_args(ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs)
+        choice = ctypes.c_int(-1)
+        self._check(self.lib.exs_autotune(*args, ctypes.byref(choice)))
+        return choice.value
+
+    def set_kernel_config(self, cfg: int):
+        """Force a split-precision kernel configuration (0 .. EXS_OZ_NCONFIG-1)."""
+        return self._check(self.lib.exs_set_kernel_config(self.ctx, int(cfg)))
+
+    def graph(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs) -> "SetupGraph":
+        """Capture the batched device setup of these buffers into a CUDA graph."""
+        keep, args = self._device_batch_args(ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs)
+        g = ctypes.c_void_p()
+        self._check(self.lib.exs_graph_create(*args, ctypes.byref(g)))
+        return SetupGraph(self, g)
+
     def set_stream(self, stream_ptr: int | None):
         """Run on a caller-owned cudaStream_t (its integer handle); None = own stream."""
         return self._check(self.lib.exs_set_stream(self.ctx, None if not stream_ptr else ctypes.c_void_p(stream_ptr)))
@@ -214,3 +241,26 @@ class Setup:
                                         _ptr(_f(evalfv, np.float64)), _ptr(_f(occsv, np.float64)), float(wkpt),
                                         _ptr(ffacg), _ptr(vgc), _ptr(f)))
         return f
+
+
+class SetupGraph:
+    """A captured batched setup (exs_graph_*): launch() replays it on the
+    context's stream; Setup.synchronize() waits and reports device errors."""
+
+    def __init__(self, setup: Setup, handle):
+        self.setup = setup
+        self.handle = handle
+
+    def launch(self):
+        return self.setup._check(self.setup.lib.exs_graph_launch(self.handle))
+
+    def close(self):
+        if self.handle:
+            self.setup.lib.exs_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -132,6 +132,40 @@ int exs_setup_batched_device(exs_ctx *ctx, int nk, const int *ngp_host,
                              exs_complex *const *h_dev, exs_complex *const *o_dev);
 int exs_synchronize(exs_ctx *ctx);
 
+/* Autotuner (no counterpart in the reference): runs the batch described as
+ * for exs_setup_batched_device once per kernel configuration of the active
+ * precision mode (for the split-precision contraction: K chunks per
+ * pipeline stage and stage count), times each on the device and keeps the
+ * fastest for this (precision, padded N_G+k, APW rows, slices); a later
+ * exs_set_precision with the same shape reuses the choice.  Overwrites the
+ * outputs h_dev/o_dev with valid results.  *choice (may be NULL) receives
+ * the configuration index.  Synchronous. */
+int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev,
+                 const double *vgpc_dev, exs_complex *const *h_dev,
+                 exs_complex *const *o_dev, int *choice);
+
+/* Selects the split-precision kernel configuration by index
+ * (0 .. EXS_OZ_NCONFIG-1) instead of the autotuner's choice.  Every
+ * configuration gives bit-identical results. */
+#define EXS_OZ_NCONFIG 2
+int exs_set_kernel_config(exs_ctx *ctx, int config);
+
+/* CUDA graph of one batched device setup (no counterpart in the reference):
+ * the launches of exs_setup_batched_device for exactly these k-point sizes
+ * and device buffers, captured once and replayed by exs_graph_launch on the
+ * context's current stream (exs_synchronize waits and reports device
+ * errors).  The contents of igpig_dev/vgpc_dev and the SCF inputs
+ * (exs_set_scf_inputs overwrites them in place) may change between launches;
+ * the sizes and buffers may not.  exs_set_precision invalidates the graph
+ * (exs_graph_launch then returns EXS_ERR_STATE).  exs_graph_create runs the
+ * setup once before capturing.  Phase timings are not recorded. */
+typedef struct exs_graph exs_graph;
+int exs_graph_create(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev,
+                     const double *vgpc_dev, exs_complex *const *h_dev,
+                     exs_complex *const *o_dev, exs_graph **out);
+int exs_graph_launch(exs_graph *graph);
+void exs_graph_destroy(exs_graph *graph);
+
 /* Replaces the IBS part of  call forcek(ik, ffacg)  (src/forcek.f90:13) for
  * one k-point without second variation:
  *   igpig(ngkmax), vgpc(3, ngkmax), evecfv(nmatmax, nstfv) (leading dim ldv),
