@@ -424,7 +424,8 @@ def run_ours(args):
         out = {
             "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 slices, f64 recombination" if args.precision == "ozaki" else "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "k_per_step": nk, "ngp": [min(ngp), max(ngp)],
                        "nmat": [min(nmat), max(nmat)],
                        "kernel_config": tuned,
@@ -459,6 +460,153 @@ def run_ours(args):
     return 0
 
 
+WORKLOAD_216 = ("si_cube216 216-atom Si (3x3x3 supercell of the 8-atom cube, a = 30.78), Gamma + 3 k, "
+                "rgkmax 8, lmaxapw 8, APW order 2, 1 lo per l<=2")
+
+
+def _rel_fro_dev(a, b, chunk=1 << 27):
+    num = den = 0.0
+    for i in range(0, a.numel(), chunk):
+        x, y = a[i:i + chunk], b[i:i + chunk]
+        num += float(((x - y) ** 2).sum())
+        den += float((y ** 2).sum())
+    return (num / den) ** 0.5
+
+
+def run_large(args):
+    """The 216-atom cell: one k-point per call (H and O are ~13.7 GB each),
+    the step is the 4 k-points; split precision and native FP64 both timed."""
+    import torch
+    import torch.distributed as dist
+    from exciting_b200 import workloads as W
+    from exciting_b200.fvsystem import Setup
+    from exciting_b200.kdist import my_kpoints
+
+    ws, rank = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    s = W.si_cube216()
+    gks_all = s.gksets()[: min(args.nk, 4)]
+    gks = [gks_all[i] for i in my_kpoints(rank, len(gks_all), ws)] if ws > 1 else gks_all
+    st = Setup(s, ngkmax=max(g.ngp for g in gks_all), max_batch=1)
+    stream = torch.cuda.Stream()
+    st.set_stream(stream.cuda_stream)
+    ngkmax, nlotot = st.ngkmax, st.nlotot
+    ig, vg = [], []
+    for g in gks:
+        a = np.zeros(ngkmax, dtype=np.int32)
+        a[: g.ngp] = g.igpig
+        b = np.zeros((ngkmax, 3))
+        b[: g.ngp] = g.vgpc.T
+        ig.append(torch.from_numpy(a).cuda())
+        vg.append(torch.from_numpy(b).cuda())
+    mmax = ngkmax + nlotot
+    d_h = torch.empty(2 * mmax * mmax, dtype=torch.float64, device="cuda")
+    d_o = torch.empty_like(d_h)
+
+    def step(phase):
+        for k, g in enumerate(gks):
+            st.setup_batched_device([g.ngp], ig[k].data_ptr(), vg[k].data_ptr(), [d_h.data_ptr()],
+                                    [d_o.data_ptr()])
+            st.synchronize()
+            phase += st.last_timings()
+
+    def timed(nsteps, nwarm, sample_clocks):
+        junk = np.zeros(5)
+        for _ in range(nwarm):
+            step(junk)
+        rows, stop = [], threading.Event()
+        th = None
+        if sample_clocks:
+            th = threading.Thread(target=_clock_sampler, args=(stop, rows), daemon=True)
+            th.start()
+            time.sleep(0.3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        phase = np.zeros(5)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(nsteps):
+                step(phase)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        stop.set()
+        if th is not None:
+            th.join(timeout=3)
+        t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), phase / max(nsteps, 1), rows
+
+    st.set_precision("ozaki", args.slices)
+    ms, phase, rows = timed(args.steps, args.warmup, True)
+    value = len(gks_all) * args.steps / (ms * 1e-3)
+    # accuracy of the split precision against the native FP64 path, k-point 0, whole matrices
+    st.setup_batched_device([gks[0].ngp], ig[0].data_ptr(), vg[0].data_ptr(), [d_h.data_ptr()], [d_o.data_ptr()])
+    st.synchronize()
+    m0 = gks[0].ngp + nlotot
+    h8 = d_h[: 2 * m0 * m0].clone()
+    o8 = d_o[: 2 * m0 * m0].clone()
+    st.set_precision("fp64")
+    ms64, phase64, _ = timed(max(1, args.steps // 3), 1, False)
+    fp64_value = len(gks_all) * max(1, args.steps // 3) / (ms64 * 1e-3)
+    st.setup_batched_device([gks[0].ngp], ig[0].data_ptr(), vg[0].data_ptr(), [d_h.data_ptr()], [d_o.data_ptr()])
+    st.synchronize()
+    acc = {"against": "native FP64 GPU path, k-point 0 (Gamma), whole H and O",
+           "rel_fro_H": _rel_fro_dev(h8, d_h[: 2 * m0 * m0]), "rel_fro_O": _rel_fro_dev(o8, d_o[: 2 * m0 * m0])}
+    del h8, o8
+    if rank == 0:
+        ops = ozaki_int8_ops(s, gks_all, args.slices)
+        fl = main_flops(s, gks_all)
+        peak8 = _measured_int8_peak(torch)
+        peak64 = _measured_fp64_peak(torch)
+        mt_ms = phase[2]                                      # MT phase per step (all k)
+        a8 = ops / (mt_ms * 1e-3) / 1e12
+        out = {
+            "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "i8 slices, f64 recombination",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_216, "k_per_step": len(gks_all),
+                       "ngp": [min(g.ngp for g in gks_all), max(g.ngp for g in gks_all)],
+                       "nmat": [min(g.ngp for g in gks_all) + nlotot, max(g.ngp for g in gks_all) + nlotot],
+                       "precision": "split int8 x%d slices (tcgen05), FP64 recombination" % args.slices,
+                       "l2": "working set (A/B planes 30 GB, slices 27 GB, H/O 27 GB) far above L2, no flush"},
+            "e2e": None,
+            "e2e_note": "H and O are 13.7 GB each per k-point; host staging of that size is not measured",
+            "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
+                                   "lo_blocks": phase[3], "total": phase[4]},
+            "roofline": {"bound": "tensor", "kernel": "oz_mma_kernel (tcgen05.mma kind::i8, MT contraction)",
+                         "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
+                         "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
+                         "int8_ops_per_step": ops, "traffic": None,
+                         "fp64_equivalent": {"achieved": fl / (mt_ms * 1e-3) / 1e12, "peak": peak64,
+                                             "unit": "TFLOP/s", "frac": fl / (mt_ms * 1e-3) / 1e12 / peak64}},
+            "cpu_baseline": None,
+            "cpu_baseline_note": "the CPU restatement needs ~2e14 flops per k-point here (hours on the host)",
+            "clocks": _clock_summary(rows, local),
+            "gpu_launches": 7 * len(gks_all) * args.steps,
+            "setup_flops_per_step": setup_flops(s, gks_all),
+            "accuracy": acc,
+            "fp64_path_value": fp64_value,
+            "fp64_phases_ms_per_step": {"match": phase64[0], "h_a_A": phase64[1], "mt_contraction": phase64[2],
+                                        "lo_blocks": phase64[3], "total": phase64[4]},
+            "speedup_split_vs_fp64": value / fp64_value,
+        }
+        print(json.dumps(out), flush=True)
+    st.set_stream(None)
+    st.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -468,12 +616,16 @@ def main():
     ap.add_argument("--nk", type=int, default=27, help="k-points per step (profiling runs use fewer)")
     ap.add_argument("--skip-cpu", action="store_true", help="no CPU-baseline leg (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="no host-pointer leg (profiling runs)")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "ozaki"],
-                    help="MT contraction arithmetic")
+    ap.add_argument("--precision", default="ozaki", choices=["fp64", "ozaki"],
+                    help="MT contraction arithmetic (the native FP64 path is timed beside the split one)")
+    ap.add_argument("--workload", default="cube8", choices=["cube8", "cube216"],
+                    help="cube8: 8-atom cell, 27 k per step; cube216: 216-atom cell, 4 k per step")
     ap.add_argument("--slices", type=int, default=7, help="int8 slices per operand (ozaki)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "cube216":
+        return run_large(args)
     return run_ours(args)
 
 

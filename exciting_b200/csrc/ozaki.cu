@@ -206,9 +206,10 @@ __device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int nblk, i
 }
 
 // The S slices of the four arrays.  A 32(f) x 32(G) tile per block,
-// transposed through shared memory (reads G-contiguous planes, writes
-// K-contiguous int8 rows).
-__global__ void oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
+// transposed through shared memory: reads G-contiguous planes (a warp reads
+// 32 consecutive G), writes K-contiguous int8 rows four bytes per thread
+// (8 threads cover the tile's 32 K bytes of one G row).
+__global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
 {
     __shared__ double t[OZ_NARR][32][33];
     const KDesc k = ks[blockIdx.z];
@@ -225,20 +226,33 @@ __global__ void oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
         t[3][r][tx] = v ? k.ai[i] : 0.0;
     }
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const int g = g0 + r, f = f0 + tx;
-        if (g >= p.npad || f >= kp8) continue;
-        const double sa = oz_sigma(k.oz_scale[g]), sb = oz_sigma(k.oz_scale[p.npad + g]);
-        double x[OZ_NARR] = {t[0][tx][r] / sb, t[1][tx][r] / sb, t[2][tx][r] / sa, t[3][tx][r] / sa};
-        for (int s = 0; s < S; s++)
+    const int tid = ty * 32 + tx;
+    const int gl = tid >> 3, fl = (tid & 7) * 4;
+    const int g = g0 + gl, f = f0 + fl;
+    if (g >= p.npad || f >= kp8) return;
+    // 1/sigma is a power of two: the scaling is exact
+    const double ra = 1.0 / oz_sigma(k.oz_scale[g]), rb = 1.0 / oz_sigma(k.oz_scale[p.npad + g]);
+    double x[OZ_NARR][4];
 #pragma unroll
-            for (int a = 0; a < OZ_NARR; a++) {
-                x[a] *= 128.0;
-                const double tq = trunc(x[a]);
-                x[a] -= tq;
-                k.oz_slices[oz_off(s, a, g, f, nblk, kp8)] = (int8_t)tq;
-            }
+    for (int e = 0; e < 4; e++) {
+        x[0][e] = t[0][fl + e][gl] * rb;
+        x[1][e] = t[1][fl + e][gl] * rb;
+        x[2][e] = t[2][fl + e][gl] * ra;
+        x[3][e] = t[3][fl + e][gl] * ra;
     }
+    for (int s = 0; s < S; s++)
+#pragma unroll
+        for (int a = 0; a < OZ_NARR; a++) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                x[a][e] *= 128.0;
+                const double tq = trunc(x[a][e]);
+                x[a][e] -= tq;
+                w |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * e);
+            }
+            *reinterpret_cast<uint32_t *>(k.oz_slices + oz_off(s, a, g, f, nblk, kp8)) = w;
+        }
 }
 
 // ------------------------------------------------------------ main kernel

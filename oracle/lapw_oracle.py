@@ -234,6 +234,25 @@ def hamiltonandoverlapsetup(sys, gk, apwalm=None):
     return h, o
 
 
+def apw_block(sys, gk, idx):
+    """H and O restricted to the APW rows/columns ``idx`` (0-based G+k indices).
+
+    Every APW-APW element H(i, j) depends only on G_i + k and G_j + k (the
+    matching coefficients of the two columns, hamiltonsetup.f90:75-103, and
+    the interstitial term of G_i - G_j, hmlistln.f90:61-86), so the block is
+    the APW-APW block of the same setup over the G+k subset ``idx``.  This
+    checks single entries of H/O at sizes where the full oracle would not
+    finish."""
+    from dataclasses import replace
+    idx = np.asarray(idx)
+    sub = replace(gk, ngp=len(idx), igpig=np.ascontiguousarray(gk.igpig[idx]),
+                  vgpc=np.ascontiguousarray(gk.vgpc[:, idx]), gpc=np.ascontiguousarray(gk.gpc[idx]),
+                  tpgpc=np.ascontiguousarray(gk.tpgpc[:, idx]))
+    h, o = hamiltonandoverlapsetup(sys, sub)
+    n = len(idx)
+    return h[:n, :n], o[:n, :n]
+
+
 # ---------------------------------------------------------------- forcek (IBS)
 def forcek(sys, gk, evecfv, evalfv, occsv, wkpt, apwalm=None):
     """IBS force contribution of one k-point, forceibs(3, natmtot) (src/forcek.f90).

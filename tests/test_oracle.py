@@ -143,3 +143,15 @@ def test_eigenvalues_of_oracle_system_are_finite():
     h, o = O.hamiltonandoverlapsetup(s, gk)
     w = sl.eigh(h, o, eigvals_only=True)
     assert np.all(np.isfinite(w))
+
+
+def test_apw_block_equals_full_setup_block():
+    """The sub-set oracle used at full sizes agrees with the full oracle."""
+    from exciting_b200 import workloads as W
+    s = W.si_fcc("shipped")
+    gk = s.gkset(s.kpoints[2])
+    h, o = O.hamiltonandoverlapsetup(s, gk)
+    idx = np.sort(np.random.default_rng(0).choice(gk.ngp, 37, replace=False))
+    hb, ob = O.apw_block(s, gk, idx)
+    assert np.allclose(hb, h[np.ix_(idx, idx)], rtol=0, atol=1e-12 * np.abs(h).max())
+    assert np.allclose(ob, o[np.ix_(idx, idx)], rtol=0, atol=1e-12 * np.abs(o).max())
