@@ -59,6 +59,24 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 }  // namespace
 
+exs::OzAtomArgs exs_ctx::oz_atom_args() const
+{
+    exs::OzAtomArgs a{};
+    a.hr = d_haa_r;
+    a.hi = d_haa_i;
+    a.lr = d_loa_r;
+    a.li = d_loa_i;
+    a.ldh = ldh;
+    a.ldlo = ldlo;
+    a.maxaa = maxaa;
+    a.nfb = oz_nfb;
+    a.nxb = oz_nxb;
+    a.lw = oz_lw;
+    a.xs = d_xs;
+    a.xsig = d_xsig;
+    return a;
+}
+
 exs::DevParams exs_ctx::params() const
 {
     DevParams p{};
@@ -135,6 +153,8 @@ int exs_ctx_destroy(exs_ctx *c)
         if (p) cudaFree(p);
     if (c->d_oz) cudaFree(c->d_oz);
     if (c->d_ozscale) cudaFree(c->d_ozscale);
+    if (c->d_xs) cudaFree(c->d_xs);
+    if (c->d_xsig) cudaFree(c->d_xsig);
     if (c->fk_dev) cudaFree(c->fk_dev);
     if (c->fk_tab_d) cudaFree(c->fk_tab_d);
     if (c->fk_tab_h) cudaFreeHost(c->fk_tab_h);
@@ -267,6 +287,8 @@ int exs_ctx_create(const exs_config *cfg, exs_ctx **out)
             a.lo_off = -1;
         }
         for (int k = 0; k < 3; k++) a.pos[k] = c->atposc[3 * (size_t)ias + k];
+        a.oz_x0 = a.apw_off & ~15;
+        a.oz_nch = (a.apw_off - a.oz_x0 + a.napw + 127) / 128;
     }
     c->K = off;
     c->Kpad = round_up(c->K, 16);
@@ -339,11 +361,23 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8);
     if (c->d_oz) { cudaFree(c->d_oz); c->d_oz = nullptr; }
     if (c->d_ozscale) { cudaFree(c->d_ozscale); c->d_ozscale = nullptr; }
+    if (c->d_xs) { cudaFree(c->d_xs); c->d_xs = nullptr; }
+    if (c->d_xsig) { cudaFree(c->d_xsig); c->d_xsig = nullptr; }
+    // per-atom operands: windows of 128-byte chunks, 64-row blocks of h_a and lo rows
+    int nch = 1;
+    for (const AtomDesc &a : c->atoms) nch = std::max(nch, a.oz_nch);
+    c->oz_lw = 128 * nch;
+    c->oz_nfb = (c->maxaa + 63) / 64;
+    c->oz_nxb = c->oz_nfb + (c->maxnlo + 63) / 64;
+    c->oz_xseg = exs::oz_seg_pairs(slices, c->oz_lw);
+    const size_t xgroups = (size_t)c->natmtot * slices * c->oz_nxb;
     cudaError_t e = cudaMalloc((void **)&c->d_oz, slot * c->max_batch);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 2 * c->npad * c->max_batch);
-    if (e != cudaSuccess) {
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xs, xgroups * 128 * c->oz_lw);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xsig, sizeof(double) * c->natmtot * c->oz_nxb * 64);
+    if (e != cudaSuccess || c->oz_xseg < 1) {
         c->prec_mode = EXS_PREC_FP64;
-        return fail(c, EXS_ERR_NOMEM, "split-precision work space");
+        return fail(c, e != cudaSuccess ? EXS_ERR_NOMEM : EXS_ERR_SIZE, "split-precision work space");
     }
     c->kp8 = kp8;
     c->oz_seg = seg;
@@ -353,6 +387,8 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     for (int q = 0; q < exs::OZ_NCFG; q++)
         maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8,
                                                       exs::OZ_CFG_KCH[q], &c->oz_mapA[q], &c->oz_mapB[q]);
+    maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8,
+                                                c->d_xs, xgroups, c->oz_lw, &c->oz_mapArow, &c->oz_mapX);
     if (!maps_ok) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
@@ -361,6 +397,10 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     }
     c->slices = slices;
     c->prec_mode = mode;
+    if (c->have_inputs) {   // slices of the current h_a and loa
+        EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), slices, c->stream));
+        EXS_CUDA(cudaStreamSynchronize(c->stream));
+    }
     {   // a configuration the autotuner chose earlier for this shape
         auto it = c->oz_tuned.find(std::make_tuple((int)mode, c->npad, c->K, slices));
         c->oz_cfg = it != c->oz_tuned.end() ? it->second : 0;
@@ -430,6 +470,8 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
     EXS_CUDA(upload(&c->d_spr_tail, in->spr_tail, (size_t)c->np_tail * c->nspecies, s));
     EXS_CUDA(upload(&c->d_apwfr_tail, in->apwfr_tail,
                     (size_t)c->np_tail * c->apwordmax * (c->lmaxapw + 1) * nat, s));
+    if (c->prec_mode == EXS_PREC_OZAKI_INT8)   // slices of the new h_a and loa, in place
+        EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->slices, s));
     EXS_CUDA(cudaStreamSynchronize(s));
     c->have_inputs = true;
     return EXS_OK;
@@ -526,6 +568,8 @@ struct Uploaded {
     int nwork[4];
     const void *d_oztiles;
     int noztiles;
+    const void *d_ozatiles;   // per-atom tiles of the split-precision path
+    int nozatiles;
 };
 
 // Upper tiles (128 rows x 32 columns) of the split-precision contraction.
@@ -540,17 +584,43 @@ void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t)
     }
 }
 
+// Per-atom tiles {k, atom, G block of 128, row block of 64} of the
+// split-precision path: h_a A (row blocks 0..nfb-1) and the APW-lo rows
+// (blocks nfb..).
+void oz_atom_tiles(const exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &t)
+{
+    for (size_t k = 0; k < ks.size(); k++)
+        for (int ias = 0; ias < c->natmtot; ias++) {
+            const AtomDesc &a = c->atoms[ias];
+            for (int ib = 0; ib < (ks[k].ngp + 127) / 128; ib++) {
+                for (int xb = 0; xb < (a.napw + 63) / 64; xb++) {
+                    t.push_back((int)k); t.push_back(ias); t.push_back(ib); t.push_back(xb);
+                }
+                for (int lb = 0; lb < (a.losize + 63) / 64; lb++) {
+                    t.push_back((int)k); t.push_back(ias); t.push_back(ib); t.push_back(c->oz_nfb + lb);
+                }
+            }
+        }
+}
+
 // Layout of the packed tables (byte offsets from the start of the buffer).
 struct TableLayout {
-    size_t k, probs[4], work[4], oz, total;
-    int nwork[4], noz;
+    size_t k, probs[4], work[4], oz, oza, total;
+    int nwork[4], noz, noza;
 };
 
 void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt, TableLayout &L)
 {
     exs::build_gemm_tables(c, ks, c->gt);
     ozt.clear();
-    if (c->prec_mode == EXS_PREC_OZAKI_INT8) oz_tiles(ks, ozt);
+    std::vector<int> ozat;
+    if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
+        oz_tiles(ks, ozt);
+        oz_atom_tiles(c, ks, ozat);
+    }
+    L.noz = (int)(ozt.size() / 3);
+    L.noza = (int)(ozat.size() / 4);
+    ozt.insert(ozt.end(), ozat.begin(), ozat.end());   // HO tiles, then the per-atom tiles
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     size_t off = 0;
     L.k = off;
@@ -563,8 +633,8 @@ void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt
         L.nwork[q] = (int)c->gt.work[q].size();
     }
     L.oz = off;
+    L.oza = off + sizeof(int) * 3 * (size_t)L.noz;
     off += al(ozt.size() * sizeof(int));
-    L.noz = (int)(ozt.size() / 3);
     L.total = off;
 }
 
@@ -592,6 +662,8 @@ Uploaded device_view(const TableLayout &L, char *d)
     }
     u.d_oztiles = d + L.oz;
     u.noztiles = L.noz;
+    u.d_ozatiles = d + L.oza;
+    u.nozatiles = L.noza;
     return u;
 }
 
@@ -649,11 +721,19 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     if (!have_planes) EXS_CUDA(exs::launch_match_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     if (c->relativity == EXS_REL_IORA) EXS_CUDA(exs::launch_iora_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_EV(1);
-    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
-                                   u.nwork[exs::EPI_PLANAR], u.d_k, s));
+    const bool oz = c->prec_mode == EXS_PREC_OZAKI_INT8;
+    if (oz) {
+        // slices of A; B = h_a A and the APW-lo rows of H from the slices of h_a and loa
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 2, s));
+        EXS_CUDA(exs::launch_oz_atom(&c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles, u.nozatiles, c->slices,
+                                     c->kp8, c->oz_xseg, c->oz_atom_args(), s));
+    } else {
+        EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
+                                       u.nwork[exs::EPI_PLANAR], u.d_k, s));
+    }
     EXS_EV(2);
-    if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
-        EXS_CUDA(exs::launch_oz_prepare(p, u.d_k, (int)ks.size(), c->slices, c->kp8, s));
+    if (oz) {
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 0, s));
         const int q = c->oz_cfg;
         EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], &c->oz_mapB[q], p, u.d_k, u.d_oztiles, u.noztiles, c->slices,
                                     c->kp8, c->oz_seg, s));
@@ -664,8 +744,9 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
                                        u.nwork[exs::EPI_OVL], u.d_k, s));
     }
     EXS_EV(3);
-    EXS_CUDA(exs::launch_gemm_kind(exs::EPI_LOROWS, p, u.d_probs[exs::EPI_LOROWS], u.d_work[exs::EPI_LOROWS],
-                                   u.nwork[exs::EPI_LOROWS], u.d_k, s));
+    if (!oz)
+        EXS_CUDA(exs::launch_gemm_kind(exs::EPI_LOROWS, p, u.d_probs[exs::EPI_LOROWS], u.d_work[exs::EPI_LOROWS],
+                                       u.nwork[exs::EPI_LOROWS], u.d_k, s));
     EXS_CUDA(exs::launch_olp_apwlo(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_CUDA(exs::launch_lolo_blocks(p, u.d_k, (int)ks.size(), s));
     EXS_EV(4);

@@ -23,6 +23,20 @@ enum : int {
 
 // Pipeline configurations of the split-precision kernel.
 constexpr int OZ_NCFG = 2;
+// Modes of the split-precision kernel: H/O tiles, per-atom products (h_a A, loa A).
+enum : int { OZ_HO = 0, OZ_ATOM = 1 };
+
+// Per-atom operands of the split-precision kernel (h_a and loa, their slices).
+struct OzAtomArgs {
+    const double *hr, *hi;       // h_a planar [ias][f'][f], leading dim ldh
+    const double *lr, *li;       // loa planar [ias][f][r], leading dim ldlo
+    int ldh, ldlo, maxaa;
+    int nfb;                     // 64-row blocks of h_a rows (ceil(maxaa / 64)); blocks nfb.. hold the lo rows
+    int nxb;                     // blocks per atom (nfb + ceil(maxnlo / 64))
+    int lw;                      // window bytes per row (multiple of 128)
+    int8_t *xs;                  // slices [atom][slice][block][re, im][64][lw]
+    double *xsig;                // row scales [atom][block][64]
+};
 static_assert(OZ_NCFG == EXS_OZ_NCONFIG, "public configuration count");
 
 // atomicMax for non-negative doubles: their IEEE bit patterns order like
@@ -39,6 +53,8 @@ struct AtomDesc {
     int napw;        // m_a: APW rows of this atom (l <= lmaxmat)
     int lo_off;      // first row of this atom inside the lo block (0-based), -1 if none
     int losize;      // lo rows of this atom
+    int oz_x0;       // split precision: apw_off rounded down to 16 (start of the atom's K window)
+    int oz_nch;      // split precision: 128-byte K chunks of the window (apw_off - oz_x0 + napw)
     double pos[3];   // atposc
 };
 
@@ -185,6 +201,12 @@ struct exs_ctx {
     size_t oz_slot_bytes = 0;
     CUtensorMap oz_mapA[exs::OZ_NCFG], oz_mapB[exs::OZ_NCFG];   // TMA views of d_oz per pipeline configuration
     int oz_cfg = 0;                   // pipeline configuration of the split-precision kernel
+    // per-atom products of the split-precision path (h_a A, loa A)
+    int8_t *d_xs = nullptr;           // slices of h_a and loa
+    double *d_xsig = nullptr;         // their row scales
+    int oz_lw = 0, oz_nfb = 0, oz_nxb = 0, oz_xseg = 0;
+    CUtensorMap oz_mapArow, oz_mapX;
+    exs::OzAtomArgs oz_atom_args() const;
     unsigned gen = 0;                 // bumped when device buffers that captured graphs use are replaced
     std::map<std::tuple<int, int, int, int>, int> oz_tuned;   // (prec, npad, K, slices) -> configuration
     // runtime
@@ -216,7 +238,13 @@ void build_gemm_tables(const exs_ctx *c, const std::vector<KDesc> &ks, GemmTable
 cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, const void *d_work, int nwork,
                              const KDesc *d_k, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)
-cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s);
+cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s);
+cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStream_t s);
+cudaError_t launch_oz_atom(const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p, const KDesc *d_k,
+                           const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
+                           cudaStream_t s);
+bool make_oz_atom_maps(void *base, size_t groups, int kp8, void *xbase, size_t xgroups, int lw, CUtensorMap *mapArow,
+                       CUtensorMap *mapX);
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
                           cudaStream_t s);

@@ -38,6 +38,8 @@
 //   warps 0-2  one TMA producer thread each (A_r, A_i and B box of a stage)
 //   warp 3     MMA issuer (one thread); allocates tensor memory
 //   warps 4-7  epilogue: segment folds and the final store
+// The same kernel (MODE OZ_ATOM) forms the per-atom products B_a = h_a A_a
+// and the APW-lo rows loa_a A_a from int8 slices of h_a and loa.
 // Tensor memory (512 columns): r at [0,128), i at [128,256), FP64 sums (two
 // 32-bit columns per value) at [256,512).  Every wait on an mbarrier is
 // bounded (about one second) and gives up early once another role has given
@@ -63,10 +65,6 @@ constexpr int OZ_MAX_KCH = 2;                    // K chunks per stage of the wi
 constexpr int OZ_TMEM_COLS = 512;
 constexpr int OZ_FP64_COL = 256;
 constexpr long long OZ_WAIT_CYCLES = 2000000000LL;   // ~1 s at 2 GHz
-
-struct OzTile {
-    int k, ib, jb;
-};
 
 // ------------------------------------------------------------ device helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -205,25 +203,25 @@ __device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int nblk, i
     return ((((size_t)s * nblk + (g >> 5)) * OZ_NARR + a) * 32 + (g & 31)) * (size_t)kp8 + f;
 }
 
-// The S slices of the four arrays.  A 32(f) x 32(G) tile per block,
-// transposed through shared memory: reads G-contiguous planes (a warp reads
-// 32 consecutive G), writes K-contiguous int8 rows four bytes per thread
-// (8 threads cover the tile's 32 K bytes of one G row).
-__global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8)
+// The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
+// A 32(f) x 32(G) tile per block, transposed through shared memory: reads
+// G-contiguous planes (a warp reads 32 consecutive G), writes K-contiguous
+// int8 rows four bytes per thread (8 threads cover the tile's 32 K bytes of
+// one G row).
+__global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8, int a0)
 {
-    __shared__ double t[OZ_NARR][32][33];
+    __shared__ double t[2][32][33];
     const KDesc k = ks[blockIdx.z];
     const int f0 = blockIdx.x * 32, g0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;      // 32 x 8
     const int nblk = p.npad / 32;
+    const double *pr = a0 == 0 ? k.br : k.ar, *pi = a0 == 0 ? k.bi : k.ai;
     for (int r = ty; r < 32; r += 8) {
         const int f = f0 + r, g = g0 + tx;
         const bool v = f < p.K && g < k.ngp;
         const size_t i = (size_t)f * p.npad + g;
-        t[0][r][tx] = v ? k.br[i] : 0.0;
-        t[1][r][tx] = v ? k.bi[i] : 0.0;
-        t[2][r][tx] = v ? k.ar[i] : 0.0;
-        t[3][r][tx] = v ? k.ai[i] : 0.0;
+        t[0][r][tx] = v ? pr[i] : 0.0;
+        t[1][r][tx] = v ? pi[i] : 0.0;
     }
     __syncthreads();
     const int tid = ty * 32 + tx;
@@ -231,18 +229,16 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
     const int g = g0 + gl, f = f0 + fl;
     if (g >= p.npad || f >= kp8) return;
     // 1/sigma is a power of two: the scaling is exact
-    const double ra = 1.0 / oz_sigma(k.oz_scale[g]), rb = 1.0 / oz_sigma(k.oz_scale[p.npad + g]);
-    double x[OZ_NARR][4];
+    const double rs = 1.0 / oz_sigma(k.oz_scale[(a0 == 0 ? p.npad : 0) + g]);
+    double x[2][4];
 #pragma unroll
     for (int e = 0; e < 4; e++) {
-        x[0][e] = t[0][fl + e][gl] * rb;
-        x[1][e] = t[1][fl + e][gl] * rb;
-        x[2][e] = t[2][fl + e][gl] * ra;
-        x[3][e] = t[3][fl + e][gl] * ra;
+        x[0][e] = t[0][fl + e][gl] * rs;
+        x[1][e] = t[1][fl + e][gl] * rs;
     }
     for (int s = 0; s < S; s++)
 #pragma unroll
-        for (int a = 0; a < OZ_NARR; a++) {
+        for (int a = 0; a < 2; a++) {
             uint32_t w = 0;
 #pragma unroll
             for (int e = 0; e < 4; e++) {
@@ -251,15 +247,108 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
                 x[a][e] -= tq;
                 w |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * e);
             }
-            *reinterpret_cast<uint32_t *>(k.oz_slices + oz_off(s, a, g, f, nblk, kp8)) = w;
+            *reinterpret_cast<uint32_t *>(k.oz_slices + oz_off(s, a0 + a, g, f, nblk, kp8)) = w;
+        }
+}
+
+// ------------------------------------------------------------ per-atom operands
+// Slices of the per-atom MT integrals that multiply A from the left in the
+// per-atom products B_a = h_a A_a (hamiltonsetup.f90:75-88) and
+// H_lo,a = loa_a A_a (hamiltonsetup.f90:131-145):
+//   X(n, k) for n = output row (f of h_a in blocks of 64, then the lo rows r
+//   of loa in blocks of 64 from block nfb on), k = K byte of the atom's window: the window starts
+//   at oz_x0 (apw_off rounded down to 16) so that X(n, k) = 0 unless
+//   0 <= k - (apw_off - oz_x0) < napw.
+// Layout [atom][slice][block xb][array re, im][64 rows][lw bytes], one scale
+// sigma per row (power of two above the row maximum).
+__device__ __forceinline__ void x_value(const DevParams &p, const OzAtomArgs &xa, int ias, int xb, int n, int fp,
+                                        double &re, double &im)
+{
+    re = im = 0.0;
+    const AtomDesc at = p.atoms[ias];
+    if (fp < 0 || fp >= at.napw) return;
+    if (xb < xa.nfb) {
+        const int f = xb * 64 + n;
+        if (f >= at.napw) return;
+        const size_t i = (size_t)ias * xa.ldh * xa.ldh + (size_t)fp * xa.ldh + f;   // h(f, f') at [ias][f'][f]
+        re = xa.hr[i];
+        im = xa.hi[i];
+    } else {
+        const int r = (xb - xa.nfb) * 64 + n;
+        if (r >= at.losize) return;
+        const size_t i = (size_t)ias * xa.ldlo * xa.maxaa + (size_t)fp * xa.ldlo + r;   // loa(r, f) at [ias][f][r]
+        re = xa.lr[i];
+        im = xa.li[i];
+    }
+}
+
+// sigma of every X row: one thread per (atom, block, row).
+__global__ void oz_xsig_kernel(DevParams p, OzAtomArgs xa)
+{
+    const int n = threadIdx.x, xb = blockIdx.x, ias = blockIdx.y;
+    double m = 0.0;
+    for (int fp = 0; fp < p.atoms[ias].napw; fp++) {
+        double re, im;
+        x_value(p, xa, ias, xb, n, fp, re, im);
+        m = fmax(m, fmax(fabs(re), fabs(im)));
+    }
+    xa.xsig[((size_t)ias * xa.nxb + xb) * 64 + n] = oz_sigma(m);
+}
+
+// The slices of X: one thread per (atom, block, row, 4 window bytes).
+__global__ void oz_xsplit_kernel(DevParams p, OzAtomArgs xa, int S)
+{
+    const int ias = blockIdx.z, xb = blockIdx.y;
+    const int n = threadIdx.y + blockIdx.x * blockDim.y;        // row 0..63
+    const int k4 = threadIdx.x * 4;                             // window byte
+    if (n >= 64 || k4 >= xa.lw) return;
+    const AtomDesc at = p.atoms[ias];
+    const int delta = at.apw_off - at.oz_x0;
+    const double r = 1.0 / xa.xsig[((size_t)ias * xa.nxb + xb) * 64 + n];
+    double x[2][4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        double re, im;
+        x_value(p, xa, ias, xb, n, k4 + e - delta, re, im);
+        x[0][e] = re * r;
+        x[1][e] = im * r;
+    }
+    for (int s = 0; s < S; s++)
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            uint32_t w = 0;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                x[a][e] *= 128.0;
+                const double tq = trunc(x[a][e]);
+                x[a][e] -= tq;
+                w |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * e);
+            }
+            const size_t row = ((((size_t)ias * S + s) * xa.nxb + xb) * 2 + a) * 64 + n;
+            *reinterpret_cast<uint32_t *>(xa.xs + row * xa.lw + k4) = w;
         }
 }
 
 // ------------------------------------------------------------ main kernel
-template <int KCH, int NST>
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// MODE OZ_HO: tiles {k, ib, jb}: H and O, 128 G_i x 32 G_j, B operand
+//   [Br | Bi | Ar | Ai] of one G block, contraction over all K.
+// MODE OZ_ATOM: tiles {k, atom, ib, xb}: 128 G x 64 output rows n of one
+//   atom, B operand [X re | X im] (64 rows each), contraction over the
+//   atom's K window; writes B planes (xb < nfb) or the APW-lo rows of H.
+template <int MODE, int KCH, int NST>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
-              const KDesc *ks, const OzTile *tiles, int S, int kp8, int seg_pairs)
+              const KDesc *ks, const int *tiles, int S, int kp8, int seg_pairs, OzAtomArgs xa)
 {
     constexpr int BOX = KCH * OZ_TILE;          // one TMA box
     constexpr int STAGE = 3 * BOX;              // A_r, A_i, B
@@ -272,12 +361,23 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     volatile int *abort = &abort_sh;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const OzTile tl = tiles[blockIdx.x];
-    const KDesc kd = ks[tl.k];
-    const int i0 = tl.ib * OZ_BM, j0 = tl.jb * OZ_BJ;
+    int tk, ib, jb = 0, ias = 0, xb = 0;
+    if (MODE == OZ_HO) {
+        tk = tiles[3 * blockIdx.x];
+        ib = tiles[3 * blockIdx.x + 1];
+        jb = tiles[3 * blockIdx.x + 2];
+    } else {
+        tk = tiles[4 * blockIdx.x];
+        ias = tiles[4 * blockIdx.x + 1];
+        ib = tiles[4 * blockIdx.x + 2];
+        xb = tiles[4 * blockIdx.x + 3];
+    }
+    const KDesc kd = ks[tk];
+    const int i0 = ib * OZ_BM, j0 = jb * OZ_BJ;
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
     const int nblk = p.npad / 32;
-    const int nst = kp8 / (KCH * OZ_CHUNK);           // pipeline stages per slice pair
+    // pipeline stages per slice pair
+    const int nst = (MODE == OZ_HO) ? kp8 / (KCH * OZ_CHUNK) : p.atoms[ias].oz_nch / KCH;
 
     if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
@@ -294,7 +394,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    if (tid >= 128 && tid < 128 + OZ_BJ) {        // column data of the final epilogue
+    if (MODE == OZ_HO && tid >= 128 && tid < 128 + OZ_BJ) {   // column data of the final epilogue
         const int c = tid - 128, j = j0 + c;
         if (j < kd.ngp) {
             int g = kd.igpig[j] - 1;
@@ -325,6 +425,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             for (int q = 0; q < NST; q++) fills[q] = 0;
             int st = 0;
             bool bad = false;
+            const int x0 = (MODE == OZ_ATOM) ? p.atoms[ias].oz_x0 : 0;
             for (int d = 2; d <= S + 1 && !bad; d++)
                 for (int s = 1; s <= d - 1 && !bad; s++) {
                     const int t = d - s;
@@ -337,9 +438,15 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                         const uint32_t dst = sbase + st * STAGE + role * BOX;
                         if (role < 2) {   // array Ar (2) or Ai (3) of G blocks i0/32 .. +3, slice s
                             const int grp = (kd.oz_slot * S + (s - 1)) * nblk + (i0 >> 5);
-                            tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * KCH, &full[st]);
-                        } else {          // the four arrays of G block j0/32, slice t
+                            if (MODE == OZ_HO)
+                                tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * KCH, &full[st]);
+                            else
+                                tma_load_3d(dst, &mapA, x0 + kb * OZ_CHUNK, (2 + role) * 32, grp, &full[st]);
+                        } else if (MODE == OZ_HO) {   // the four arrays of G block j0/32, slice t
                             const int grp = (kd.oz_slot * S + (t - 1)) * nblk + (j0 >> 5);
+                            tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
+                        } else {                      // X rows of block xb, slice t
+                            const int grp = (ias * S + (t - 1)) * xa.nxb + xb;
                             tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
                         }
                         fills[st]++;
@@ -417,16 +524,18 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 }
                 tc_fence_after();
                 const bool init = (nseg == 0);
-                // output block o (Re H, Im H, Re O, Im O) = r block o +- i block o^1
+                // FP64 block o (32 values) = r block o +- i block (o ^ 1) (HO:
+                // Re H, Im H, Re O, Im O) or (o ^ 2) (ATOM: Re rows 0-63, Im rows 0-63)
 #pragma unroll 1
                 for (int o = 0; o < 4; o++) {
-                    const double sg = (o & 1) ? -1.0 : 1.0;
+                    const double sg = (MODE == OZ_HO) ? ((o & 1) ? -1.0 : 1.0) : ((o < 2) ? -1.0 : 1.0);
+                    const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
 #pragma unroll 1
-                    for (int jc = 0; jc < OZ_BJ; jc += 16) {
+                    for (int jc = 0; jc < 32; jc += 16) {
                         uint32_t rv[16], iv[16], lo[16], hi[16];
                         const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
                         tm_ld16(t_lane + o * 32 + jc, rv);
-                        tm_ld16(t_lane + 128 + (o ^ 1) * 32 + jc, iv);
+                        tm_ld16(t_lane + 128 + oi * 32 + jc, iv);
                         if (!init) {
                             tm_ld16(t_lane + fcol, lo);
                             tm_ld16(t_lane + fcol + 16, hi);
@@ -463,7 +572,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 nseg++;
             }
         }
-        if (__all_sync(0xffffffffu, !bad && !*abort)) {
+        if (MODE == OZ_HO && __all_sync(0xffffffffu, !bad && !*abort)) {
             const int i = i0 + qd * 32 + lane;
             int ivi[3] = {0, 0, 0};
             double vi[3] = {0.0, 0.0, 0.0};
@@ -524,6 +633,50 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 }
             }
         }
+        if (MODE == OZ_ATOM && __all_sync(0xffffffffu, !bad && !*abort)) {
+            // row G of the tile; values v = 0..63 real, 64..127 imaginary parts of the 64 output rows
+            const int g = i0 + qd * 32 + lane;
+            const bool g_ok = g < p.npad;
+            const AtomDesc at = p.atoms[ias];
+            const bool lorows = xb >= xa.nfb;
+            const double sa = g_ok ? oz_sigma(kd.oz_scale[g]) : 0.0;
+            const double *sig = xa.xsig + ((size_t)ias * xa.nxb + xb) * 64;
+            const size_t row0 = (size_t)kd.ngp + at.lo_off;
+            double bmax = 0.0;
+#pragma unroll 1
+            for (int jc = 0; jc < 64; jc += 8) {
+                uint32_t wr[16], wi[16];
+                tm_ld16(t_lane + OZ_FP64_COL + 2 * jc, wr);
+                tm_ld16(t_lane + OZ_FP64_COL + 2 * (64 + jc), wi);
+                tm_wait_ld();
+                if (!g_ok) continue;
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int n = jc + e;
+                    const double sc = sa * sig[n];
+                    const double re = __hiloint2double((int)wr[2 * e + 1], (int)wr[2 * e]) * sc;
+                    const double im = __hiloint2double((int)wi[2 * e + 1], (int)wi[2 * e]) * sc;
+                    if (!lorows) {
+                        const int f = xb * 64 + n;
+                        if (f >= at.napw) continue;
+                        const size_t off = (size_t)(at.apw_off + f) * p.npad + g;
+                        kd.br[off] = re;
+                        kd.bi[off] = im;
+                        bmax = fmax(bmax, fmax(fabs(re), fabs(im)));
+                    } else {
+                        const int r = (xb - xa.nfb) * 64 + n;
+                        if (r >= at.losize || g >= kd.ngp) continue;
+                        exs_complex v;
+                        v.re = re;
+                        v.im = im;
+                        kd.h[(row0 + r) + (size_t)kd.nmat * g] = v;
+                        v.im = -im;
+                        kd.h[(size_t)g + (size_t)kd.nmat * (row0 + r)] = v;
+                    }
+                }
+            }
+            if (!lorows && g_ok) atomic_max_nonneg(kd.oz_scale + p.npad + g, bmax);
+        }
     }
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
     tc_fence_before();
@@ -550,26 +703,36 @@ int oz_seg_pairs(int S, int kp8)
 const int OZ_CFG_KCH[OZ_NCFG] = {2, 1};
 const int OZ_CFG_NST[OZ_NCFG] = {2, 4};
 
-cudaError_t launch_oz_prepare(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, cudaStream_t s)
+cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
 {
-    oz_split_kernel<<<dim3(kp8 / 32, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8);
+    oz_split_kernel<<<dim3(kp8 / 32, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8, a0);
     return cudaGetLastError();
 }
 
-template <int KCH, int NST>
+cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStream_t s)
+{
+    oz_xsig_kernel<<<dim3(xa.nxb, p.natmtot), 64, 0, s>>>(p, xa);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    oz_xsplit_kernel<<<dim3(8, xa.nxb, p.natmtot), dim3(xa.lw / 4, 8), 0, s>>>(p, xa, S);
+    return cudaGetLastError();
+}
+
+template <int MODE, int KCH, int NST>
 static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
-                              const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s)
+                              const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
+                              cudaStream_t s)
 {
     constexpr int smem = NST * 3 * KCH * OZ_TILE + 1024;
     static bool attr = false;
     if (!attr) {
         cudaError_t e =
-            cudaFuncSetAttribute(oz_mma_kernel<KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaFuncSetAttribute(oz_mma_kernel<MODE, KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    oz_mma_kernel<KCH, NST><<<ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const OzTile *)d_tiles, S, kp8,
-                                                             seg_pairs);
+    oz_mma_kernel<MODE, KCH, NST><<<ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const int *)d_tiles, S,
+                                                                   kp8, seg_pairs, xa);
     return cudaGetLastError();
 }
 
@@ -578,11 +741,20 @@ cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *m
                           cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
+    const OzAtomArgs none{};
     switch (cfg) {
-    case 0: return launch_cfg<2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
-    case 1: return launch_cfg<1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
+    case 0: return launch_cfg<OZ_HO, 2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, s);
+    case 1: return launch_cfg<OZ_HO, 1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_oz_atom(const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p, const KDesc *d_k,
+                           const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
+                           cudaStream_t s)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, xa, s);
 }
 
 // TMA views of the slices of all slots (int8, 4D):
@@ -621,6 +793,46 @@ bool make_oz_tensor_maps(void *base, size_t groups, int kp8, int kch, CUtensorMa
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
+    return true;
+}
+
+// TMA views for the per-atom products:
+//   mapArow: the slices as [group][128 rows][kp8 bytes] (3D), box {128, 32, 4}:
+//     one array of 4 G blocks, one 128-byte K chunk starting at any multiple
+//     of 16 bytes (the atom windows are not chunk aligned);
+//   mapX: the X slices as [group][128 rows][lw bytes] viewed like the B tiles
+//     (4D, K chunked), box {128, 128, 1, 1}.
+bool make_oz_atom_maps(void *base, size_t groups, int kp8, void *xbase, size_t xgroups, int lw, CUtensorMap *mapArow,
+                       CUtensorMap *mapX)
+{
+    typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+        return false;
+    EncodeFn encode = (EncodeFn)fn;
+    if (kp8 % OZ_CHUNK != 0 || lw % OZ_CHUNK != 0) return false;
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    {
+        const cuuint64_t dims[3] = {(cuuint64_t)kp8, 128, (cuuint64_t)groups};
+        const cuuint64_t strides[2] = {(cuuint64_t)kp8, (cuuint64_t)128 * kp8};
+        const cuuint32_t box[3] = {OZ_CHUNK, 32, 4};
+        if (encode(mapArow, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    {
+        const cuuint64_t dims[4] = {(cuuint64_t)OZ_CHUNK, 128, (cuuint64_t)xgroups, (cuuint64_t)(lw / OZ_CHUNK)};
+        const cuuint64_t strides[3] = {(cuuint64_t)lw, (cuuint64_t)128 * lw, (cuuint64_t)OZ_CHUNK};
+        const cuuint32_t box[4] = {OZ_CHUNK, 128, 1, 1};
+        if (encode(mapX, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, xbase, dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
     return true;
 }
 
