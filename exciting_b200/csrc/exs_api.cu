@@ -725,8 +725,8 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     if (oz) {
         // slices of A; B = h_a A and the APW-lo rows of H from the slices of h_a and loa
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 2, s));
-        EXS_CUDA(exs::launch_oz_atom(&c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles, u.nozatiles, c->slices,
-                                     c->kp8, c->oz_xseg, c->oz_atom_args(), s));
+        EXS_CUDA(exs::launch_oz_atom(c->oz_cfg, &c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles, u.nozatiles,
+                                     c->slices, c->kp8, c->oz_xseg, c->oz_atom_args(), s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
                                        u.nwork[exs::EPI_PLANAR], u.d_k, s));

@@ -22,7 +22,7 @@ enum : int {
 };
 
 // Pipeline configurations of the split-precision kernel.
-constexpr int OZ_NCFG = 2;
+constexpr int OZ_NCFG = 4;
 // Modes of the split-precision kernel: H/O tiles, per-atom products (h_a A, loa A).
 enum : int { OZ_HO = 0, OZ_ATOM = 1 };
 
@@ -240,9 +240,9 @@ cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, 
 // Split-precision contraction (ozaki.cu)
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s);
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStream_t s);
-cudaError_t launch_oz_atom(const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p, const KDesc *d_k,
-                           const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
-                           cudaStream_t s);
+cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
+                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                           const OzAtomArgs &xa, cudaStream_t s);
 bool make_oz_atom_maps(void *base, size_t groups, int kp8, void *xbase, size_t xgroups, int lw, CUtensorMap *mapArow,
                        CUtensorMap *mapX);
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,

@@ -30,9 +30,9 @@
 // descriptors use the matching SWIZZLE_128B K-major layout (8-row x 128-byte
 // atoms, 1024 B between 8-row groups, K advanced 32 bytes per MMA).
 //
-// Pipeline configurations (chosen per problem by the autotuner):
-//   KCH K chunks per stage (box = KCH x 16 KB) x NST stages, 192 KB in all:
-//   (2, 2) and (1, 4).
+// Configurations (chosen per problem by the autotuner): KCH K chunks per
+// stage (box = KCH x 16 KB) x NST stages, 192 KB in all: (2, 2) or (1, 4);
+// one CTA per tile or a persistent grid of one CTA per SM.
 //
 // Roles (one CTA per 128 x 32 output tile, 256 threads):
 //   warps 0-2  one TMA producer thread each (A_r, A_i and B box of a stage)
@@ -345,10 +345,39 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 // MODE OZ_ATOM: tiles {k, atom, ib, xb}: 128 G x 64 output rows n of one
 //   atom, B operand [X re | X im] (64 rows each), contraction over the
 //   atom's K window; writes B planes (xb < nfb) or the APW-lo rows of H.
+struct OzTileInfo {
+    int k, i0, j0, ias, xb, nst;
+};
+
+template <int MODE, int KCH>
+__device__ __forceinline__ OzTileInfo oz_tile(const DevParams &p, const int *tiles, int t, int kp8)
+{
+    OzTileInfo ti{};
+    if (MODE == OZ_HO) {
+        ti.k = tiles[3 * t];
+        ti.i0 = tiles[3 * t + 1] * OZ_BM;
+        ti.j0 = tiles[3 * t + 2] * OZ_BJ;
+        ti.nst = kp8 / (KCH * OZ_CHUNK);
+    } else {
+        ti.k = tiles[4 * t];
+        ti.ias = tiles[4 * t + 1];
+        ti.i0 = tiles[4 * t + 2] * OZ_BM;
+        ti.xb = tiles[4 * t + 3];
+        ti.nst = p.atoms[ti.ias].oz_nch / KCH;
+    }
+    return ti;
+}
+
+// Persistent: each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// and every role walks the same sequence (tile, diagonal d = 2..S+1, left
+// slice s = 1..d-1 with t = d - s on the right, K stages), so the mbarrier
+// phases simply continue from tile to tile.  The MMAs of a tile's first
+// segment overlap the final epilogue of the previous tile (the int32
+// accumulators are free once the last fold has read them).
 template <int MODE, int KCH, int NST>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
-              const KDesc *ks, const int *tiles, int S, int kp8, int seg_pairs, OzAtomArgs xa)
+              const KDesc *ks, const int *tiles, int ntiles, int S, int kp8, int seg_pairs, OzAtomArgs xa)
 {
     constexpr int BOX = KCH * OZ_TILE;          // one TMA box
     constexpr int STAGE = 3 * BOX;              // A_r, A_i, B
@@ -356,28 +385,11 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     __shared__ uint64_t full[NST], empty[NST], accf, acce;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
-    __shared__ int jiv[OZ_BJ][3];
-    __shared__ double jv[OZ_BJ][3];
     volatile int *abort = &abort_sh;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    int tk, ib, jb = 0, ias = 0, xb = 0;
-    if (MODE == OZ_HO) {
-        tk = tiles[3 * blockIdx.x];
-        ib = tiles[3 * blockIdx.x + 1];
-        jb = tiles[3 * blockIdx.x + 2];
-    } else {
-        tk = tiles[4 * blockIdx.x];
-        ias = tiles[4 * blockIdx.x + 1];
-        ib = tiles[4 * blockIdx.x + 2];
-        xb = tiles[4 * blockIdx.x + 3];
-    }
-    const KDesc kd = ks[tk];
-    const int i0 = ib * OZ_BM, j0 = jb * OZ_BJ;
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
     const int nblk = p.npad / 32;
-    // pipeline stages per slice pair
-    const int nst = (MODE == OZ_HO) ? kp8 / (KCH * OZ_CHUNK) : p.atoms[ias].oz_nch / KCH;
 
     if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
@@ -394,28 +406,11 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    if (MODE == OZ_HO && tid >= 128 && tid < 128 + OZ_BJ) {   // column data of the final epilogue
-        const int c = tid - 128, j = j0 + c;
-        if (j < kd.ngp) {
-            int g = kd.igpig[j] - 1;
-            if (g < 0 || g >= p.ngrtot) {
-                atomicOr(p.err, DEV_ERR_INDEX);
-                g = 0;
-            }
-            for (int x = 0; x < 3; x++) {
-                jiv[c][x] = p.ivg[3 * g + x];
-                jv[c][x] = kd.vgpc[3 * j + x];
-            }
-        }
-    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = tmem_sh;
 
-    // All roles walk the same sequence: diagonal d = 2..S+1, slice s of the
-    // left operand = 1 .. d-1 (t = d - s of the right one), segments of
-    // seg_pairs consecutive pairs within a diagonal.
     if (warp < 3) {
         // ------------------------------------------------ TMA producers: warp w loads box w
         if (lane == 0) {
@@ -425,34 +420,38 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             for (int q = 0; q < NST; q++) fills[q] = 0;
             int st = 0;
             bool bad = false;
-            const int x0 = (MODE == OZ_ATOM) ? p.atoms[ias].oz_x0 : 0;
-            for (int d = 2; d <= S + 1 && !bad; d++)
-                for (int s = 1; s <= d - 1 && !bad; s++) {
-                    const int t = d - s;
-                    for (int kb = 0; kb < nst; kb++) {
-                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
-                            bad = true;
-                            break;
+            for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
+                const OzTileInfo ti = oz_tile<MODE, KCH>(p, tiles, tile, kp8);
+                const int slot = ks[ti.k].oz_slot;
+                const int x0 = (MODE == OZ_ATOM) ? p.atoms[ti.ias].oz_x0 : 0;
+                for (int d = 2; d <= S + 1 && !bad; d++)
+                    for (int s = 1; s <= d - 1 && !bad; s++) {
+                        const int t = d - s;
+                        for (int kb = 0; kb < ti.nst; kb++) {
+                            if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
+                                bad = true;
+                                break;
+                            }
+                            mbar_expect_tx(&full[st], BOX);
+                            const uint32_t dst = sbase + st * STAGE + role * BOX;
+                            if (role < 2) {   // array Ar (2) or Ai (3) of G blocks i0/32 .. +3, slice s
+                                const int grp = (slot * S + (s - 1)) * nblk + (ti.i0 >> 5);
+                                if (MODE == OZ_HO)
+                                    tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * KCH, &full[st]);
+                                else
+                                    tma_load_3d(dst, &mapA, x0 + kb * OZ_CHUNK, (2 + role) * 32, grp, &full[st]);
+                            } else if (MODE == OZ_HO) {   // the four arrays of G block j0/32, slice t
+                                const int grp = (slot * S + (t - 1)) * nblk + (ti.j0 >> 5);
+                                tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
+                            } else {                      // X rows of block xb, slice t
+                                const int grp = (ti.ias * S + (t - 1)) * xa.nxb + ti.xb;
+                                tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
+                            }
+                            fills[st]++;
+                            st = (st + 1 == NST) ? 0 : st + 1;
                         }
-                        mbar_expect_tx(&full[st], BOX);
-                        const uint32_t dst = sbase + st * STAGE + role * BOX;
-                        if (role < 2) {   // array Ar (2) or Ai (3) of G blocks i0/32 .. +3, slice s
-                            const int grp = (kd.oz_slot * S + (s - 1)) * nblk + (i0 >> 5);
-                            if (MODE == OZ_HO)
-                                tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * KCH, &full[st]);
-                            else
-                                tma_load_3d(dst, &mapA, x0 + kb * OZ_CHUNK, (2 + role) * 32, grp, &full[st]);
-                        } else if (MODE == OZ_HO) {   // the four arrays of G block j0/32, slice t
-                            const int grp = (kd.oz_slot * S + (t - 1)) * nblk + (j0 >> 5);
-                            tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
-                        } else {                      // X rows of block xb, slice t
-                            const int grp = (ias * S + (t - 1)) * xa.nxb + xb;
-                            tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
-                        }
-                        fills[st]++;
-                        st = (st + 1 == NST) ? 0 : st + 1;
                     }
-                }
+            }
             if (bad)   // copies already issued must land before the CTA goes away
                 for (int q = 0; q < NST; q++)
                     if (fills[q] > 0) mbar_drain(&full[q], (fills[q] - 1) & 1);
@@ -466,44 +465,47 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             for (int q = 0; q < NST; q++) uses[q] = 0;
             int nseg = 0, st = 0;
             bool bad = false;
-            for (int d = 2; d <= S + 1 && !bad; d++)
-                for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
-                    const int s1 = min(d - 1, s0 + seg_pairs - 1);
-                    // the epilogue must have folded the previous segment
-                    if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
-                        bad = true;
-                        break;
-                    }
-                    tc_fence_after();
-                    bool first = true;
-                    for (int s = s0; s <= s1 && !bad; s++)
-                        for (int kb = 0; kb < nst; kb++) {
-                            if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
-                                bad = true;
-                                break;
-                            }
-                            tc_fence_after();
-                            const uint32_t sa = sbase + st * STAGE;
-#pragma unroll
-                            for (int c = 0; c < KCH; c++)
-#pragma unroll
-                                for (int q = 0; q < OZ_CHUNK / 32; q++) {
-                                    const uint32_t off = c * OZ_TILE + q * 32;
-                                    const uint64_t bd = umma_desc_sw128(sa + 2 * BOX + off);
-                                    const uint32_t acc = (first && c == 0 && q == 0) ? 0u : 1u;
-                                    umma_i8(tbase, umma_desc_sw128(sa + off), bd, idesc, acc);
-                                    umma_i8(tbase + 128, umma_desc_sw128(sa + BOX + off), bd, idesc, acc);
-                                }
-                            first = false;
-                            umma_commit(&empty[st]);
-                            uses[st]++;
-                            st = (st + 1 == NST) ? 0 : st + 1;
+            for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
+                const int nst = oz_tile<MODE, KCH>(p, tiles, tile, kp8).nst;
+                for (int d = 2; d <= S + 1 && !bad; d++)
+                    for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
+                        const int s1 = min(d - 1, s0 + seg_pairs - 1);
+                        // the epilogue must have folded the previous segment
+                        if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
+                            bad = true;
+                            break;
                         }
-                    if (!bad) {
-                        umma_commit(&accf);
-                        nseg++;
+                        tc_fence_after();
+                        bool first = true;
+                        for (int s = s0; s <= s1 && !bad; s++)
+                            for (int kb = 0; kb < nst; kb++) {
+                                if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
+                                    bad = true;
+                                    break;
+                                }
+                                tc_fence_after();
+                                const uint32_t sa = sbase + st * STAGE;
+#pragma unroll
+                                for (int c = 0; c < KCH; c++)
+#pragma unroll
+                                    for (int q = 0; q < OZ_CHUNK / 32; q++) {
+                                        const uint32_t off = c * OZ_TILE + q * 32;
+                                        const uint64_t bd = umma_desc_sw128(sa + 2 * BOX + off);
+                                        const uint32_t acc = (first && c == 0 && q == 0) ? 0u : 1u;
+                                        umma_i8(tbase, umma_desc_sw128(sa + off), bd, idesc, acc);
+                                        umma_i8(tbase + 128, umma_desc_sw128(sa + BOX + off), bd, idesc, acc);
+                                    }
+                                first = false;
+                                umma_commit(&empty[st]);
+                                uses[st]++;
+                                st = (st + 1 == NST) ? 0 : st + 1;
+                            }
+                        if (!bad) {
+                            umma_commit(&accf);
+                            nseg++;
+                        }
                     }
-                }
+            }
             if (bad)   // MMAs already issued must finish before tensor memory is freed
                 for (int q = 0; q < NST; q++)
                     if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
@@ -514,168 +516,185 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
         int nseg = 0;
         bool bad = false;
-        for (int d = 2; d <= S + 1 && !bad; d++) {
-            const double scale = ldexp(1.0, -7 * d);
-            for (int s0 = 1; s0 <= d - 1; s0 += seg_pairs) {
-                const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
-                if (!ok) {
-                    bad = true;
-                    break;
-                }
-                tc_fence_after();
-                const bool init = (nseg == 0);
-                // FP64 block o (32 values) = r block o +- i block (o ^ 1) (HO:
-                // Re H, Im H, Re O, Im O) or (o ^ 2) (ATOM: Re rows 0-63, Im rows 0-63)
+        for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
+            const OzTileInfo ti = oz_tile<MODE, KCH>(p, tiles, tile, kp8);
+            for (int d = 2; d <= S + 1 && !bad; d++) {
+                const double scale = ldexp(1.0, -7 * d);
+                for (int s0 = 1; s0 <= d - 1; s0 += seg_pairs) {
+                    const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
+                    if (!ok) {
+                        bad = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const bool init = (d == 2 && s0 == 1);      // first segment of the tile
+                    // FP64 block o (32 values) = r block o +- i block (o ^ 1) (HO:
+                    // Re H, Im H, Re O, Im O) or (o ^ 2) (ATOM: Re rows 0-63, Im rows 0-63)
 #pragma unroll 1
-                for (int o = 0; o < 4; o++) {
-                    const double sg = (MODE == OZ_HO) ? ((o & 1) ? -1.0 : 1.0) : ((o < 2) ? -1.0 : 1.0);
-                    const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
+                    for (int o = 0; o < 4; o++) {
+                        const double sg = (MODE == OZ_HO) ? ((o & 1) ? -1.0 : 1.0) : ((o < 2) ? -1.0 : 1.0);
+                        const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
 #pragma unroll 1
-                    for (int jc = 0; jc < 32; jc += 16) {
-                        uint32_t rv[16], iv[16], lo[16], hi[16];
-                        const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
-                        tm_ld16(t_lane + o * 32 + jc, rv);
-                        tm_ld16(t_lane + 128 + oi * 32 + jc, iv);
-                        if (!init) {
-                            tm_ld16(t_lane + fcol, lo);
-                            tm_ld16(t_lane + fcol + 16, hi);
-                        }
-                        tm_wait_ld();
-                        uint32_t o0[16], o1[16];
-#pragma unroll
-                        for (int e = 0; e < 16; e++) {
-                            double a = 0.0;
+                        for (int jc = 0; jc < 32; jc += 16) {
+                            uint32_t rv[16], iv[16], lo[16], hi[16];
+                            const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
+                            tm_ld16(t_lane + o * 32 + jc, rv);
+                            tm_ld16(t_lane + 128 + oi * 32 + jc, iv);
                             if (!init) {
-                                const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
-                                const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
-                                a = __hiloint2double((int)w1, (int)w0);
+                                tm_ld16(t_lane + fcol, lo);
+                                tm_ld16(t_lane + fcol + 16, hi);
                             }
-                            // r +- i is exact in FP64 (|int32| sums); one rounding per fold
-                            a += scale * ((double)(int)rv[e] + sg * (double)(int)iv[e]);
-                            const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
-                            if (e < 8) {
-                                o0[2 * e] = w0;
-                                o0[2 * e + 1] = w1;
-                            } else {
-                                o1[2 * (e - 8)] = w0;
-                                o1[2 * (e - 8) + 1] = w1;
+                            tm_wait_ld();
+                            uint32_t o0[16], o1[16];
+#pragma unroll
+                            for (int e = 0; e < 16; e++) {
+                                double a = 0.0;
+                                if (!init) {
+                                    const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
+                                    const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
+                                    a = __hiloint2double((int)w1, (int)w0);
+                                }
+                                // r +- i is exact in FP64 (|int32| sums); one rounding per fold
+                                a += scale * ((double)(int)rv[e] + sg * (double)(int)iv[e]);
+                                const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
+                                if (e < 8) {
+                                    o0[2 * e] = w0;
+                                    o0[2 * e + 1] = w1;
+                                } else {
+                                    o1[2 * (e - 8)] = w0;
+                                    o1[2 * (e - 8) + 1] = w1;
+                                }
                             }
+                            tm_st16(t_lane + fcol, o0);
+                            tm_st16(t_lane + fcol + 16, o1);
                         }
-                        tm_st16(t_lane + fcol, o0);
-                        tm_st16(t_lane + fcol + 16, o1);
+                    }
+                    tm_wait_st();
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acce);
+                    nseg++;
+                }
+            }
+            if (!__all_sync(0xffffffffu, !bad && !*abort)) {
+                bad = true;
+                break;
+            }
+            const KDesc kd = ks[ti.k];
+            if (MODE == OZ_HO) {
+                const int i = ti.i0 + qd * 32 + lane;
+                int ivi[3] = {0, 0, 0};
+                double vi[3] = {0.0, 0.0, 0.0};
+                const bool row_ok = i < kd.ngp;
+                if (row_ok) {
+                    int g = kd.igpig[i] - 1;
+                    if (g < 0 || g >= p.ngrtot) {
+                        atomicOr(p.err, DEV_ERR_INDEX);
+                        g = 0;
+                    }
+                    for (int x = 0; x < 3; x++) {
+                        ivi[x] = p.ivg[3 * g + x];
+                        vi[x] = kd.vgpc[3 * i + x];
                     }
                 }
-                tm_wait_st();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&acce);
-                nseg++;
-            }
-        }
-        if (MODE == OZ_HO && __all_sync(0xffffffffu, !bad && !*abort)) {
-            const int i = i0 + qd * 32 + lane;
-            int ivi[3] = {0, 0, 0};
-            double vi[3] = {0.0, 0.0, 0.0};
-            const bool row_ok = i < kd.ngp;
-            if (row_ok) {
-                int g = kd.igpig[i] - 1;
-                if (g < 0 || g >= p.ngrtot) {
-                    atomicOr(p.err, DEV_ERR_INDEX);
-                    g = 0;
-                }
-                for (int x = 0; x < 3; x++) {
-                    ivi[x] = p.ivg[3 * g + x];
-                    vi[x] = kd.vgpc[3 * i + x];
-                }
-            }
-            const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
+                const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
 #pragma unroll 1
-            for (int jc = 0; jc < OZ_BJ; jc += 8) {
-                double val[4][8];
+                for (int jc = 0; jc < OZ_BJ; jc += 8) {
+                    double val[4][8];
 #pragma unroll
-                for (int o = 0; o < 4; o++) {
-                    uint32_t w[16];
-                    tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
+                    for (int o = 0; o < 4; o++) {
+                        uint32_t w[16];
+                        tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
+                        tm_wait_ld();
+#pragma unroll
+                        for (int e = 0; e < 8; e++) val[o][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+                    }
+                    if (!row_ok) continue;
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        const int j = ti.j0 + jc + e;
+                        if (j >= kd.ngp || i > j) continue;
+                        // column data (the same for the whole warp: broadcast loads)
+                        int gj = kd.igpig[j] - 1;
+                        if (gj < 0 || gj >= p.ngrtot) {
+                            atomicOr(p.err, DEV_ERR_INDEX);
+                            gj = 0;
+                        }
+                        const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
+                        const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
+                        const double sbj = oz_sigma(kd.oz_scale[p.npad + j]), saj = oz_sigma(kd.oz_scale[j]);
+                        double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
+                        double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
+                        double ar, ai;
+                        if (interstitial(p, EPI_HAM, ivi, ivj, vi, vj, ar, ai)) {
+                            hr += ar;
+                            hi += ai;
+                        }
+                        if (interstitial(p, EPI_OVL, ivi, ivj, vi, vj, ar, ai)) {
+                            orr += ar;
+                            oi += ai;
+                        }
+                        exs_complex hv, ov;
+                        hv.re = hr;
+                        hv.im = hi;
+                        ov.re = orr;
+                        ov.im = oi;
+                        kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
+                        kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
+                        if (i < j) {
+                            hv.im = -hi;
+                            ov.im = -oi;
+                            kd.h[(size_t)j + (size_t)kd.nmat * i] = hv;
+                            kd.o[(size_t)j + (size_t)kd.nmat * i] = ov;
+                        }
+                    }
+                }
+            } else {
+                // row G of the tile; values v = 0..63 real, 64..127 imaginary parts of the 64 output rows
+                const int g = ti.i0 + qd * 32 + lane;
+                const bool g_ok = g < p.npad;
+                const AtomDesc at = p.atoms[ti.ias];
+                const bool lorows = ti.xb >= xa.nfb;
+                const double sa = g_ok ? oz_sigma(kd.oz_scale[g]) : 0.0;
+                const double *sig = xa.xsig + ((size_t)ti.ias * xa.nxb + ti.xb) * 64;
+                const size_t row0 = (size_t)kd.ngp + at.lo_off;
+                double bmax = 0.0;
+#pragma unroll 1
+                for (int jc = 0; jc < 64; jc += 8) {
+                    uint32_t wr[16], wi[16];
+                    tm_ld16(t_lane + OZ_FP64_COL + 2 * jc, wr);
+                    tm_ld16(t_lane + OZ_FP64_COL + 2 * (64 + jc), wi);
                     tm_wait_ld();
+                    if (!g_ok) continue;
 #pragma unroll
-                    for (int e = 0; e < 8; e++) val[o][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
-                }
-                if (!row_ok) continue;
-#pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const int jj = jc + e, j = j0 + jj;
-                    if (j >= kd.ngp || i > j) continue;
-                    const double sbj = oz_sigma(kd.oz_scale[p.npad + j]), saj = oz_sigma(kd.oz_scale[j]);
-                    double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
-                    double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
-                    double ar, ai;
-                    if (interstitial(p, EPI_HAM, ivi, jiv[jj], vi, jv[jj], ar, ai)) {
-                        hr += ar;
-                        hi += ai;
-                    }
-                    if (interstitial(p, EPI_OVL, ivi, jiv[jj], vi, jv[jj], ar, ai)) {
-                        orr += ar;
-                        oi += ai;
-                    }
-                    exs_complex hv, ov;
-                    hv.re = hr;
-                    hv.im = hi;
-                    ov.re = orr;
-                    ov.im = oi;
-                    kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
-                    kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
-                    if (i < j) {
-                        hv.im = -hi;
-                        ov.im = -oi;
-                        kd.h[(size_t)j + (size_t)kd.nmat * i] = hv;
-                        kd.o[(size_t)j + (size_t)kd.nmat * i] = ov;
+                    for (int e = 0; e < 8; e++) {
+                        const int n = jc + e;
+                        const double sc = sa * sig[n];
+                        const double re = __hiloint2double((int)wr[2 * e + 1], (int)wr[2 * e]) * sc;
+                        const double im = __hiloint2double((int)wi[2 * e + 1], (int)wi[2 * e]) * sc;
+                        if (!lorows) {
+                            const int f = ti.xb * 64 + n;
+                            if (f >= at.napw) continue;
+                            const size_t off = (size_t)(at.apw_off + f) * p.npad + g;
+                            kd.br[off] = re;
+                            kd.bi[off] = im;
+                            bmax = fmax(bmax, fmax(fabs(re), fabs(im)));
+                        } else {
+                            const int r = (ti.xb - xa.nfb) * 64 + n;
+                            if (r >= at.losize || g >= kd.ngp) continue;
+                            exs_complex v;
+                            v.re = re;
+                            v.im = im;
+                            kd.h[(row0 + r) + (size_t)kd.nmat * g] = v;
+                            v.im = -im;
+                            kd.h[(size_t)g + (size_t)kd.nmat * (row0 + r)] = v;
+                        }
                     }
                 }
+                if (!lorows && g_ok) atomic_max_nonneg(kd.oz_scale + p.npad + g, bmax);
             }
-        }
-        if (MODE == OZ_ATOM && __all_sync(0xffffffffu, !bad && !*abort)) {
-            // row G of the tile; values v = 0..63 real, 64..127 imaginary parts of the 64 output rows
-            const int g = i0 + qd * 32 + lane;
-            const bool g_ok = g < p.npad;
-            const AtomDesc at = p.atoms[ias];
-            const bool lorows = xb >= xa.nfb;
-            const double sa = g_ok ? oz_sigma(kd.oz_scale[g]) : 0.0;
-            const double *sig = xa.xsig + ((size_t)ias * xa.nxb + xb) * 64;
-            const size_t row0 = (size_t)kd.ngp + at.lo_off;
-            double bmax = 0.0;
-#pragma unroll 1
-            for (int jc = 0; jc < 64; jc += 8) {
-                uint32_t wr[16], wi[16];
-                tm_ld16(t_lane + OZ_FP64_COL + 2 * jc, wr);
-                tm_ld16(t_lane + OZ_FP64_COL + 2 * (64 + jc), wi);
-                tm_wait_ld();
-                if (!g_ok) continue;
-#pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const int n = jc + e;
-                    const double sc = sa * sig[n];
-                    const double re = __hiloint2double((int)wr[2 * e + 1], (int)wr[2 * e]) * sc;
-                    const double im = __hiloint2double((int)wi[2 * e + 1], (int)wi[2 * e]) * sc;
-                    if (!lorows) {
-                        const int f = xb * 64 + n;
-                        if (f >= at.napw) continue;
-                        const size_t off = (size_t)(at.apw_off + f) * p.npad + g;
-                        kd.br[off] = re;
-                        kd.bi[off] = im;
-                        bmax = fmax(bmax, fmax(fabs(re), fabs(im)));
-                    } else {
-                        const int r = (xb - xa.nfb) * 64 + n;
-                        if (r >= at.losize || g >= kd.ngp) continue;
-                        exs_complex v;
-                        v.re = re;
-                        v.im = im;
-                        kd.h[(row0 + r) + (size_t)kd.nmat * g] = v;
-                        v.im = -im;
-                        kd.h[(size_t)g + (size_t)kd.nmat * (row0 + r)] = v;
-                    }
-                }
-            }
-            if (!lorows && g_ok) atomic_max_nonneg(kd.oz_scale + p.npad + g, bmax);
+            // the FP64 region is read; the next tile's first fold may overwrite it
+            tc_fence_before();
         }
     }
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
@@ -700,8 +719,10 @@ int oz_seg_pairs(int S, int kp8)
     return (int)(n < 1 ? 0 : (n > S ? S : n));
 }
 
-const int OZ_CFG_KCH[OZ_NCFG] = {2, 1};
-const int OZ_CFG_NST[OZ_NCFG] = {2, 4};
+// configuration index: bit 0 = pipeline shape (KCH, NST) of the H/O tiles,
+// bit 1 = persistent launch (one CTA per SM) for both modes
+const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1};
+const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4};
 
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
 {
@@ -721,7 +742,7 @@ cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStr
 template <int MODE, int KCH, int NST>
 static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
                               const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
-                              cudaStream_t s)
+                              bool persistent, cudaStream_t s)
 {
     constexpr int smem = NST * 3 * KCH * OZ_TILE + 1024;
     static bool attr = false;
@@ -731,8 +752,13 @@ static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, 
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    oz_mma_kernel<MODE, KCH, NST><<<ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const int *)d_tiles, S,
-                                                                   kp8, seg_pairs, xa);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // persistent: one CTA per SM walking the tiles; else one CTA per tile
+    const int grid = (persistent && nsm < ntiles) ? nsm : ntiles;
+    oz_mma_kernel<MODE, KCH, NST><<<grid, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const int *)d_tiles, ntiles,
+                                                                 S, kp8, seg_pairs, xa);
     return cudaGetLastError();
 }
 
@@ -742,19 +768,20 @@ cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *m
 {
     if (ntiles <= 0) return cudaSuccess;
     const OzAtomArgs none{};
-    switch (cfg) {
-    case 0: return launch_cfg<OZ_HO, 2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, s);
-    case 1: return launch_cfg<OZ_HO, 1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, s);
-    default: return cudaErrorInvalidValue;
+    const bool persistent = (cfg & 2) != 0;
+    switch (cfg & 1) {
+    case 0: return launch_cfg<OZ_HO, 2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, persistent, s);
+    default: return launch_cfg<OZ_HO, 1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, persistent, s);
     }
 }
 
-cudaError_t launch_oz_atom(const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p, const KDesc *d_k,
-                           const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
-                           cudaStream_t s)
+cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
+                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                           const OzAtomArgs &xa, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
-    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, xa, s);
+    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, xa, (cfg & 2) != 0,
+                                     s);
 }
 
 // TMA views of the slices of all slots (int8, 4D):

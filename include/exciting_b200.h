@@ -145,9 +145,11 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
                  exs_complex *const *o_dev, int *choice);
 
 /* Selects the split-precision kernel configuration by index
- * (0 .. EXS_OZ_NCONFIG-1) instead of the autotuner's choice.  Every
- * configuration gives bit-identical results. */
-#define EXS_OZ_NCONFIG 2
+ * (0 .. EXS_OZ_NCONFIG-1) instead of the autotuner's choice: bit 0 picks the
+ * pipeline shape of the H/O tiles (two 96 KB stages or four 48 KB stages),
+ * bit 1 a persistent launch (one block per SM walking the tiles) instead of
+ * one block per tile.  Every configuration gives bit-identical results. */
+#define EXS_OZ_NCONFIG 4
 int exs_set_kernel_config(exs_ctx *ctx, int config);
 
 /* CUDA graph of one batched device setup (no counterpart in the reference):
