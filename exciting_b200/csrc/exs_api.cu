@@ -382,13 +382,14 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     c->kp8 = kp8;
     c->oz_seg = seg;
     c->oz_slot_bytes = slot;
-    // one tensor-map group = 128 rows (4 arrays x 32 G) of one slice of one slot
+    // the slices of all slots: (slot x slice) groups of 4 arrays x npad rows x kp8 bytes
+    const size_t nss = (size_t)slices * c->max_batch;
     bool maps_ok = true;
     for (int q = 0; q < exs::OZ_NCFG; q++)
-        maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8,
-                                                      exs::OZ_CFG_KCH[q], &c->oz_mapA[q], &c->oz_mapB[q]);
-    maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, (size_t)slices * (c->npad / 32) * c->max_batch, kp8,
-                                                c->d_xs, xgroups, c->oz_lw, &c->oz_mapArow, &c->oz_mapX);
+        maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, nss, c->npad, kp8, exs::OZ_CFG_KCH[q], &c->oz_mapA[q],
+                                                      &c->oz_mapB[q]);
+    maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, nss, c->npad, kp8, c->d_xs, xgroups, c->oz_lw,
+                                                &c->oz_mapArow, &c->oz_mapX);
     if (!maps_ok) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;

@@ -69,7 +69,7 @@ struct KDesc {
     double *ar, *ai;         // A planes  [Kpad][npad]
     double *br, *bi;         // B = blockdiag(h_a) A planes
     double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
-    int8_t *oz_slices;       // split-precision path: int8 slices of this slot [S][npad/32][4][32][kp8]
+    int8_t *oz_slices;       // split-precision path: int8 slices of this slot [S][4 arrays][npad][kp8]
     double *oz_scale;        // split-precision path: column maxima of |A| and |B| [2][npad] (null: FP64 path)
     int oz_slot;             // split-precision path: slot index in the slice tensor maps
 };
@@ -243,12 +243,12 @@ cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStr
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
                            const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
                            const OzAtomArgs &xa, cudaStream_t s);
-bool make_oz_atom_maps(void *base, size_t groups, int kp8, void *xbase, size_t xgroups, int lw, CUtensorMap *mapArow,
-                       CUtensorMap *mapX);
+bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, size_t xgroups, int lw,
+                       CUtensorMap *mapArow, CUtensorMap *mapX);
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
                           cudaStream_t s);
-bool make_oz_tensor_maps(void *base, size_t groups, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB);
+bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB);
 extern const int OZ_CFG_KCH[OZ_NCFG], OZ_CFG_NST[OZ_NCFG];
 int oz_kpad(int K);
 size_t oz_slot_bytes(int S, int npad, int kp8);

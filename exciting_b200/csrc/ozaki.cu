@@ -22,11 +22,12 @@
 // the upper triangle and its conjugate mirror, as the FP64 path does.
 //
 // Slice storage (int8, K contiguous, K padded to kp8 = multiple of 256):
-//   [slot][slice][32-row block of G][array: Br, Bi, Ar, Ai][32 rows][kp8]
-// so that a B tile (one G block, all four arrays) is 128 consecutive rows and
-// an A tile (one array of four consecutive G blocks) is a regular stride:
-// each operand tile of a pipeline stage (KCH 128-byte K chunks) is ONE TMA
-// box of KCH x 16 KB.  Boxes are written with 128-byte swizzling; the MMA
+//   [slot][slice][array: Br, Bi, Ar, Ai][G (npad rows)][kp8]
+// viewed by TMA as 5D (K byte in a 128-byte chunk, G, array, K chunk,
+// slot x slice), so that both A operands of a stage (Ar and Ai, 128 G rows
+// each) are ONE box and the B operand (32 G rows of all four arrays) is
+// another: two boxes per stage.  Rows past npad fall outside the view and
+// arrive as zeros.  Boxes are written with 128-byte swizzling; the MMA
 // descriptors use the matching SWIZZLE_128B K-major layout (8-row x 128-byte
 // atoms, 1024 B between 8-row groups, K advanced 32 bytes per MMA).
 //
@@ -35,7 +36,7 @@
 // one CTA per tile or a persistent grid of one CTA per SM.
 //
 // Roles (one CTA per 128 x 32 output tile, 256 threads):
-//   warps 0-2  one TMA producer thread each (A_r, A_i and B box of a stage)
+//   warps 0-1  one TMA producer thread each (the A box and the B box of a stage)
 //   warp 3     MMA issuer (one thread); allocates tensor memory
 //   warps 4-7  epilogue: segment folds and the final store
 // The same kernel (MODE OZ_ATOM) forms the per-atom products B_a = h_a A_a
@@ -129,6 +130,16 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            int c4, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];\n" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // K-major SWIZZLE_128B descriptor (8-row x 128-byte atoms, 1024 B between 8-row groups).
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
 {
@@ -198,9 +209,9 @@ __host__ __device__ __forceinline__ double oz_sigma(double m)
 }
 
 // Byte offset of (slice s, array a, row G, K index f) inside one slot.
-__device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int nblk, int kp8)
+__device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, int kp8)
 {
-    return ((((size_t)s * nblk + (g >> 5)) * OZ_NARR + a) * 32 + (g & 31)) * (size_t)kp8 + f;
+    return (((size_t)s * OZ_NARR + a) * npad + g) * (size_t)kp8 + f;
 }
 
 // The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
@@ -214,7 +225,6 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
     const KDesc k = ks[blockIdx.z];
     const int f0 = blockIdx.x * 32, g0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;      // 32 x 8
-    const int nblk = p.npad / 32;
     const double *pr = a0 == 0 ? k.br : k.ar, *pi = a0 == 0 ? k.bi : k.ai;
     for (int r = ty; r < 32; r += 8) {
         const int f = f0 + r, g = g0 + tx;
@@ -247,7 +257,7 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
                 x[a][e] -= tq;
                 w |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * e);
             }
-            *reinterpret_cast<uint32_t *>(k.oz_slices + oz_off(s, a0 + a, g, f, nblk, kp8)) = w;
+            *reinterpret_cast<uint32_t *>(k.oz_slices + oz_off(s, a0 + a, g, f, p.npad, kp8)) = w;
         }
 }
 
@@ -330,15 +340,6 @@ __global__ void oz_xsplit_kernel(DevParams p, OzAtomArgs xa, int S)
 }
 
 // ------------------------------------------------------------ main kernel
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2,
-                                            uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];\n" ::"r"(dst),
-        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-        : "memory");
-}
 
 // MODE OZ_HO: tiles {k, ib, jb}: H and O, 128 G_i x 32 G_j, B operand
 //   [Br | Bi | Ar | Ai] of one G block, contraction over all K.
@@ -379,8 +380,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
               const KDesc *ks, const int *tiles, int ntiles, int S, int kp8, int seg_pairs, OzAtomArgs xa)
 {
-    constexpr int BOX = KCH * OZ_TILE;          // one TMA box
-    constexpr int STAGE = 3 * BOX;              // A_r, A_i, B
+    constexpr int BOX = KCH * OZ_TILE;          // one operand of a stage
+    constexpr int STAGE = 3 * BOX;              // A box [chunk][Ar, Ai][128 rows], B box [chunk][128 rows]
     extern __shared__ __align__(1024) uint8_t oz_smem[];
     __shared__ uint64_t full[NST], empty[NST], accf, acce;
     __shared__ uint32_t tmem_sh;
@@ -389,7 +390,6 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
-    const int nblk = p.npad / 32;
 
     if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
@@ -398,7 +398,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     }
     if (tid == 0) {
         for (int s = 0; s < NST; s++) {
-            mbar_init(&full[s], 3);
+            mbar_init(&full[s], 2);
             mbar_init(&empty[s], 1);
         }
         mbar_init(&accf, 1);
@@ -412,9 +412,9 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     const uint32_t tbase = tmem_sh;
 
     if (warp < 3) {
-        // ------------------------------------------------ TMA producers: warp w loads box w
-        if (lane == 0) {
-            const int role = warp;                          // 0: A_r, 1: A_i, 2: B
+        // ------------------------------------------------ TMA producers: warp 0 the A box, warp 1 the B box
+        if (lane == 0 && warp < 2) {
+            const int role = warp;
             uint32_t fills[NST];
 #pragma unroll
             for (int q = 0; q < NST; q++) fills[q] = 0;
@@ -432,17 +432,15 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                                 bad = true;
                                 break;
                             }
-                            mbar_expect_tx(&full[st], BOX);
-                            const uint32_t dst = sbase + st * STAGE + role * BOX;
-                            if (role < 2) {   // array Ar (2) or Ai (3) of G blocks i0/32 .. +3, slice s
-                                const int grp = (slot * S + (s - 1)) * nblk + (ti.i0 >> 5);
+                            mbar_expect_tx(&full[st], role == 0 ? 2 * BOX : BOX);
+                            const uint32_t dst = sbase + st * STAGE + role * 2 * BOX;
+                            if (role == 0) {   // Ar and Ai (arrays 2, 3) of G rows i0 .. i0+127, slice s
                                 if (MODE == OZ_HO)
-                                    tma_load_4d(dst, &mapA, 0, (2 + role) * 32, grp, kb * KCH, &full[st]);
+                                    tma_load_5d(dst, &mapA, 0, ti.i0, 2, kb * KCH, slot * S + s - 1, &full[st]);
                                 else
-                                    tma_load_3d(dst, &mapA, x0 + kb * OZ_CHUNK, (2 + role) * 32, grp, &full[st]);
-                            } else if (MODE == OZ_HO) {   // the four arrays of G block j0/32, slice t
-                                const int grp = (slot * S + (t - 1)) * nblk + (ti.j0 >> 5);
-                                tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
+                                    tma_load_4d(dst, &mapA, x0 + kb * OZ_CHUNK, ti.i0, 2, slot * S + s - 1, &full[st]);
+                            } else if (MODE == OZ_HO) {   // the four arrays of G rows j0 .. j0+31, slice t
+                                tma_load_5d(dst, &mapB, 0, ti.j0, 0, kb * KCH, slot * S + t - 1, &full[st]);
                             } else {                      // X rows of block xb, slice t
                                 const int grp = (ti.ias * S + (t - 1)) * xa.nxb + ti.xb;
                                 tma_load_4d(dst, &mapB, 0, 0, grp, kb * KCH, &full[st]);
@@ -489,11 +487,11 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                                 for (int c = 0; c < KCH; c++)
 #pragma unroll
                                     for (int q = 0; q < OZ_CHUNK / 32; q++) {
-                                        const uint32_t off = c * OZ_TILE + q * 32;
-                                        const uint64_t bd = umma_desc_sw128(sa + 2 * BOX + off);
+                                        const uint32_t ao = c * 2 * OZ_TILE + q * 32;   // Ar; Ai one tile on
+                                        const uint64_t bd = umma_desc_sw128(sa + 2 * BOX + c * OZ_TILE + q * 32);
                                         const uint32_t acc = (first && c == 0 && q == 0) ? 0u : 1u;
-                                        umma_i8(tbase, umma_desc_sw128(sa + off), bd, idesc, acc);
-                                        umma_i8(tbase + 128, umma_desc_sw128(sa + BOX + off), bd, idesc, acc);
+                                        umma_i8(tbase, umma_desc_sw128(sa + ao), bd, idesc, acc);
+                                        umma_i8(tbase + 128, umma_desc_sw128(sa + ao + OZ_TILE), bd, idesc, acc);
                                     }
                                 first = false;
                                 umma_commit(&empty[st]);
@@ -784,39 +782,39 @@ cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMa
                                      s);
 }
 
-// TMA views of the slices of all slots (int8, 4D):
-//   d0: 128 bytes of K (one swizzle row)                     stride 1
-//   d1: the 128 rows of one (slot, slice, G block) group      stride kp8
-//       (4 arrays x 32 rows)
-//   d2: group index                                           stride 128 kp8
-//   d3: K chunk of 128 bytes                                  stride 128
-// A tile box {128, 32, 4, kch}: one array of 4 consecutive G blocks;
-// B tile box {128, 128, 1, kch}: all four arrays of one G block.
-// d3 is the outermost box dimension, so each K chunk lands in shared memory
-// as one contiguous 128-row x 128-byte tile.
-bool make_oz_tensor_maps(void *base, size_t groups, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB)
+// TMA views of the slices of all slots (int8, 5D):
+//   d0: K byte within a 128-byte chunk                       stride 1
+//   d1: G row (npad)                                         stride kp8
+//   d2: array (Br, Bi, Ar, Ai)                               stride npad kp8
+//   d3: K chunk                                              stride 128
+//   d4: slot x slice                                         stride 4 npad kp8
+// A box {128, 128, 2, kch, 1}: Ar and Ai of 128 G rows; B box
+// {128, 32, 4, kch, 1}: the four arrays of 32 G rows.  d3 is outside d1, d2
+// in the box, so each K chunk lands in shared memory as contiguous
+// 128-byte rows (A: 2 x 128 rows, B: 4 x 32 rows).
+bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-    static EncodeFn encode = nullptr;
-    if (!encode) {
-        void *fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
-            return false;
-        encode = (EncodeFn)fn;
-    }
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+        return false;
+    EncodeFn encode = (EncodeFn)fn;
     if (kch < 1 || kch > OZ_MAX_KCH || kp8 % (OZ_MAX_KCH * OZ_CHUNK) != 0) return false;
-    const cuuint64_t dims[4] = {(cuuint64_t)OZ_CHUNK, 128, (cuuint64_t)groups, (cuuint64_t)(kp8 / OZ_CHUNK)};
-    const cuuint64_t strides[3] = {(cuuint64_t)kp8, (cuuint64_t)128 * kp8, (cuuint64_t)OZ_CHUNK};
-    const cuuint32_t es[4] = {1, 1, 1, 1};
-    const cuuint32_t boxA[4] = {OZ_CHUNK, 32, 4, (cuuint32_t)kch}, boxB[4] = {OZ_CHUNK, 128, 1, (cuuint32_t)kch};
-    if (encode(mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    const cuuint64_t dims[5] = {(cuuint64_t)OZ_CHUNK, (cuuint64_t)npad, OZ_NARR, (cuuint64_t)(kp8 / OZ_CHUNK),
+                                (cuuint64_t)nss};
+    const cuuint64_t strides[4] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)OZ_CHUNK,
+                                   (cuuint64_t)OZ_NARR * npad * kp8};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    const cuuint32_t boxA[5] = {OZ_CHUNK, OZ_BM, 2, (cuuint32_t)kch, 1};
+    const cuuint32_t boxB[5] = {OZ_CHUNK, OZ_BJ, OZ_NARR, (cuuint32_t)kch, 1};
+    if (encode(mapA, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, boxA, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
-    if (encode(mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    if (encode(mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
@@ -824,13 +822,14 @@ bool make_oz_tensor_maps(void *base, size_t groups, int kp8, int kch, CUtensorMa
 }
 
 // TMA views for the per-atom products:
-//   mapArow: the slices as [group][128 rows][kp8 bytes] (3D), box {128, 32, 4}:
-//     one array of 4 G blocks, one 128-byte K chunk starting at any multiple
-//     of 16 bytes (the atom windows are not chunk aligned);
+//   mapArow: the slices as [slot x slice][array][G][kp8 bytes] (4D), box
+//     {128, 128, 2, 1}: Ar and Ai of 128 G rows, one 128-byte K chunk
+//     starting at any multiple of 16 bytes (the atom windows are not chunk
+//     aligned);
 //   mapX: the X slices as [group][128 rows][lw bytes] viewed like the B tiles
 //     (4D, K chunked), box {128, 128, 1, 1}.
-bool make_oz_atom_maps(void *base, size_t groups, int kp8, void *xbase, size_t xgroups, int lw, CUtensorMap *mapArow,
-                       CUtensorMap *mapX)
+bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, size_t xgroups, int lw,
+                       CUtensorMap *mapArow, CUtensorMap *mapX)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -843,10 +842,10 @@ bool make_oz_atom_maps(void *base, size_t groups, int kp8, void *xbase, size_t x
     if (kp8 % OZ_CHUNK != 0 || lw % OZ_CHUNK != 0) return false;
     const cuuint32_t es[4] = {1, 1, 1, 1};
     {
-        const cuuint64_t dims[3] = {(cuuint64_t)kp8, 128, (cuuint64_t)groups};
-        const cuuint64_t strides[2] = {(cuuint64_t)kp8, (cuuint64_t)128 * kp8};
-        const cuuint32_t box[3] = {OZ_CHUNK, 32, 4};
-        if (encode(mapArow, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, es,
+        const cuuint64_t dims[4] = {(cuuint64_t)kp8, (cuuint64_t)npad, OZ_NARR, (cuuint64_t)nss};
+        const cuuint64_t strides[3] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)OZ_NARR * npad * kp8};
+        const cuuint32_t box[4] = {OZ_CHUNK, OZ_BM, 2, 1};
+        if (encode(mapArow, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, box, es,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
