@@ -32,8 +32,9 @@
 // atoms, 1024 B between 8-row groups, K advanced 32 bytes per MMA).
 //
 // Configurations (chosen per problem by the autotuner): KCH K chunks per
-// stage (box = KCH x 16 KB) x NST stages, 192 KB in all: (2, 2) or (1, 4);
-// one CTA per tile or a persistent grid of one CTA per SM.
+// stage x NST stages, 192 KB in all: (2, 2) or (1, 4) for the H/O tiles;
+// one CTA per tile or a persistent grid of one CTA per SM, for the H/O tiles
+// and the per-atom tiles separately.
 //
 // Roles (one CTA per 128 x 32 output tile, 256 threads):
 //   warps 0-1  one TMA producer thread each (the A box and the B box of a stage)
@@ -718,9 +719,10 @@ int oz_seg_pairs(int S, int kp8)
 }
 
 // configuration index: bit 0 = pipeline shape (KCH, NST) of the H/O tiles,
-// bit 1 = persistent launch (one CTA per SM) for both modes
-const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1};
-const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4};
+// bit 1 = persistent launch (one CTA per SM) of the H/O tiles, bit 2 =
+// persistent launch of the per-atom tiles
+const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1};
+const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4};
 
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
 {
@@ -778,7 +780,7 @@ cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMa
                            const OzAtomArgs &xa, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
-    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, xa, (cfg & 2) != 0,
+    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, xa, (cfg & 4) != 0,
                                      s);
 }
 

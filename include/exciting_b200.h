@@ -147,9 +147,11 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
 /* Selects the split-precision kernel configuration by index
  * (0 .. EXS_OZ_NCONFIG-1) instead of the autotuner's choice: bit 0 picks the
  * pipeline shape of the H/O tiles (two 96 KB stages or four 48 KB stages),
- * bit 1 a persistent launch (one block per SM walking the tiles) instead of
- * one block per tile.  Every configuration gives bit-identical results. */
-#define EXS_OZ_NCONFIG 4
+ * bit 1 a persistent launch (one block per SM walking the tiles) of the H/O
+ * tiles instead of one block per tile, bit 2 the same for the per-atom
+ * products (h_a A, APW-lo rows).  Every configuration gives bit-identical
+ * results. */
+#define EXS_OZ_NCONFIG 8
 int exs_set_kernel_config(exs_ctx *ctx, int config);
 
 /* CUDA graph of one batched device setup (no counterpart in the reference):
