@@ -607,6 +607,107 @@ def run_large(args):
     return 0
 
 
+WORKLOAD_CELLS = ("si_fcc_random x256: independent 2-atom fcc Si cells, a ~ U[9.8, 10.8], rgkmax in {6,7,8,9} "
+                  "(seed 4+i), lmaxapw 8, Gamma point each; one context per cell, all cells in one CUDA graph")
+
+
+def run_cells(args):
+    """The uneven-size batch: 256 independent cells, one context each, set up
+    together by one multi-context CUDA graph per step."""
+    import torch
+    from exciting_b200 import workloads as W
+    from exciting_b200.fvsystem import Setup, multi_graph
+
+    ws, rank = _dist()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ncell = min(args.nk, 256) if args.nk != 27 else 256
+    cells = [W.si_fcc_random(i) for i in range(ncell)]
+    stream = torch.cuda.Stream()
+    setups, batches, keep, tuned = [], [], [], []
+    for s in cells:
+        gk = s.gkset(s.kpoints[0])
+        st = Setup(s, max_batch=1)
+        st.set_precision(args.precision, args.slices)
+        ig = np.zeros(st.ngkmax, dtype=np.int32)
+        ig[: gk.ngp] = gk.igpig
+        vg = np.zeros((st.ngkmax, 3))
+        vg[: gk.ngp] = gk.vgpc.T
+        m = gk.ngp + st.nlotot
+        t = (torch.from_numpy(ig).cuda(), torch.from_numpy(vg).cuda(),
+             torch.empty(2 * m * m, dtype=torch.float64, device="cuda"),
+             torch.empty(2 * m * m, dtype=torch.float64, device="cuda"), gk.ngp)
+        keep.append(t)
+        b = ([gk.ngp], t[0].data_ptr(), t[1].data_ptr(), [t[2].data_ptr()], [t[3].data_ptr()])
+        tuned.append(st.autotune(*b))
+        setups.append(st)
+        batches.append(b)
+    setups[0].set_stream(stream.cuda_stream)
+    g = multi_graph(setups, batches)
+    for _ in range(args.warmup):
+        g.launch()
+    g.synchronize()
+    rows, stop = [], threading.Event()
+    th = threading.Thread(target=_clock_sampler, args=(stop, rows), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            g.launch()
+        e1.record(stream)
+    g.synchronize()
+    torch.cuda.synchronize()
+    stop.set()
+    th.join(timeout=3)
+    ms = e0.elapsed_time(e1)
+    # the same cells one after another through the device entry point (no graph)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for st, b in zip(setups, batches):
+        st.setup_batched_device(*b)
+    for st in setups:
+        st.synchronize()
+    seq_ms = (time.perf_counter() - t0) * 1e3
+    g.close()
+    if rank == 0:
+        ngp = [t[4] for t in keep]
+        cpu_v, cpu_n, cpu_dt = (None, 0, 0.0)
+        if not args.skip_cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import lapw_oracle as O
+            t0 = time.perf_counter()
+            for s in cells:
+                O.hamiltonandoverlapsetup(s, s.gkset(s.kpoints[0]))
+                cpu_n += 1
+                if time.perf_counter() - t0 > 10.0:
+                    break
+            cpu_dt = time.perf_counter() - t0
+            cpu_v = cpu_n / cpu_dt
+        out = {
+            "metric": METRIC, "value": ncell * args.steps / (ms * 1e-3), "unit": "setups/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "i8 slices, f64 recombination" if args.precision == "ozaki" else "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_CELLS, "cells_per_step": ncell, "ngp": [min(ngp), max(ngp)],
+                       "precision": args.precision, "kernel_configs": sorted(set(tuned)),
+                       "l2": "all cells' working set ~3 GB > L2, no flush"},
+            "sequential_device_calls_ms": seq_ms,
+            "e2e": None,
+            "cpu_baseline": None if cpu_v is None else {
+                "value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": f"{cpu_n} cells by the FP64 CPU restatement in {cpu_dt:.1f} s"},
+            "clocks": _clock_summary(rows, 0),
+            "gpu_launches": 7 * ncell * args.steps,
+        }
+        print(json.dumps(out), flush=True)
+    for st in setups:
+        st.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -618,14 +719,17 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true", help="no host-pointer leg (profiling runs)")
     ap.add_argument("--precision", default="ozaki", choices=["fp64", "ozaki"],
                     help="MT contraction arithmetic (the native FP64 path is timed beside the split one)")
-    ap.add_argument("--workload", default="cube8", choices=["cube8", "cube216"],
-                    help="cube8: 8-atom cell, 27 k per step; cube216: 216-atom cell, 4 k per step")
+    ap.add_argument("--workload", default="cube8", choices=["cube8", "cube216", "cells256"],
+                    help="cube8: 8-atom cell, 27 k per step; cube216: 216-atom cell, 4 k per step; "
+                         "cells256: 256 independent 2-atom cells per step in one graph")
     ap.add_argument("--slices", type=int, default=7, help="int8 slices per operand (ozaki)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "cube216":
         return run_large(args)
+    if args.workload == "cells256":
+        return run_cells(args)
     return run_ours(args)
 
 

@@ -52,6 +52,8 @@ SIGNATURES = {
     "exs_graph_create": ([P, c_int, P, P, P, P, P, P], c_int),
     "exs_graph_launch": ([P], c_int),
     "exs_graph_destroy": ([P], None),
+    "exs_graph_create_multi": ([c_int, P, P, P, P, P, P, P, P], c_int),
+    "exs_graph_synchronize": ([P], c_int),
     "exs_forcek": ([P, c_int, P, P, c_int, P, c_int, P, P, c_double, P, P, P], c_int),
     "exs_adjoint": ([P, c_int, P, P, c_int, P, c_int, P, P, P, P, P, P, P], c_int),
     "exs_set_stream": ([P, P], c_int),

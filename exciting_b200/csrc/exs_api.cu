@@ -814,11 +814,13 @@ int device_batch(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
 }  // namespace
 
 struct exs_graph {
-    exs_ctx *c = nullptr;
-    unsigned gen = 0;
+    std::vector<exs_ctx *> cs;        // cs[0]'s stream is the one the graph is launched on
+    std::vector<unsigned> gens;
+    std::vector<void *> tables;       // per context, owned by the graph
+    std::vector<cudaStream_t> branches;
+    std::vector<cudaEvent_t> events;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    void *d_tables = nullptr;
 };
 
 extern "C" {
@@ -879,75 +881,169 @@ int exs_set_kernel_config(exs_ctx *c, int cfg)
     return EXS_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+void graph_free(exs_graph *G)
+{
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    for (void *t : G->tables)
+        if (t) cudaFree(t);
+    for (cudaStream_t b : G->branches) cudaStreamDestroy(b);
+    for (cudaEvent_t e : G->events) cudaEventDestroy(e);
+    delete G;
+}
+
+// Capture the batched setups of one or more contexts into one graph.  With
+// several contexts each one's launches go to one of up to 32 branch streams
+// forked from the first context's stream, so independent cells run
+// concurrently when the graph is replayed.
+int graph_capture(const std::vector<exs_ctx *> &cs, std::vector<std::vector<KDesc>> &kss, exs_graph **out)
+{
+    exs_ctx *c0 = cs[0];
+    exs_graph *G = new exs_graph;
+    G->cs = cs;
+    auto bail = [&](int code) {
+        graph_free(G);
+        return code;
+    };
+    std::vector<Uploaded> us(cs.size());
+    for (size_t i = 0; i < cs.size(); i++) {   // tables owned by the graph, then one plain run
+        exs_ctx *c = cs[i];
+        G->gens.push_back(c->gen);
+        std::vector<int> ozt;
+        TableLayout L;
+        pack_tables(c, kss[i], ozt, L);
+        std::vector<char> h(L.total);
+        write_tables(c, kss[i], ozt, L, h.data());
+        void *d = nullptr;
+        if (cudaMalloc(&d, L.total) != cudaSuccess) return bail(fail(c, EXS_ERR_NOMEM, "graph tables"));
+        G->tables.push_back(d);
+        if (cudaMemcpy(d, h.data(), L.total, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(c, EXS_ERR_CUDA, "graph tables upload"));
+        us[i] = device_view(L, (char *)d);
+        // kernel attributes are set on first launch, outside any capture
+        if (cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream) != cudaSuccess)
+            return bail(fail(c, EXS_ERR_CUDA, "memset"));
+        int rc = enqueue_setup(c, kss[i], us[i], false, false);
+        if (rc < 0) return bail(rc);
+        rc = exs_synchronize(c);
+        if (rc < 0) return bail(rc);
+    }
+    const int nb = cs.size() > 1 ? (int)std::min<size_t>(cs.size(), 32) : 0;
+    for (int b = 0; b < nb; b++) {
+        cudaStream_t st;
+        cudaEvent_t ev;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(c0, EXS_ERR_CUDA, "branch stream"));
+        G->branches.push_back(st);
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(c0, EXS_ERR_CUDA, "branch event"));
+        G->events.push_back(ev);
+    }
+    cudaEvent_t fork = nullptr;
+    if (nb > 0) {
+        if (cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(c0, EXS_ERR_CUDA, "fork event"));
+        G->events.push_back(fork);
+    }
+    cudaStream_t origin = c0->stream;
+    if (cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return bail(fail(c0, EXS_ERR_CUDA, "cudaStreamBeginCapture"));
+    int rc = EXS_OK;
+    if (nb > 0 && cudaEventRecord(fork, origin) != cudaSuccess) rc = EXS_ERR_CUDA;
+    for (int b = 0; b < nb && rc == EXS_OK; b++)
+        if (cudaStreamWaitEvent(G->branches[b], fork, 0) != cudaSuccess) rc = EXS_ERR_CUDA;
+    for (size_t i = 0; i < cs.size() && rc == EXS_OK; i++) {
+        exs_ctx *c = cs[i];
+        cudaStream_t own = c->stream;
+        if (nb > 0) c->stream = G->branches[i % nb];
+        if (cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream) != cudaSuccess) rc = EXS_ERR_CUDA;
+        if (rc == EXS_OK) rc = enqueue_setup(c, kss[i], us[i], false, false);
+        c->stream = own;
+    }
+    for (int b = 0; b < nb && rc == EXS_OK; b++)
+        if (cudaEventRecord(G->events[b], G->branches[b]) != cudaSuccess ||
+            cudaStreamWaitEvent(origin, G->events[b], 0) != cudaSuccess)
+            rc = EXS_ERR_CUDA;
+    cudaError_t ee = cudaStreamEndCapture(origin, &G->graph);
+    if (rc < 0 || ee != cudaSuccess) return bail(rc < 0 ? rc : fail(c0, EXS_ERR_CUDA, "cudaStreamEndCapture"));
+    if (cudaGraphInstantiate(&G->exec, G->graph, 0) != cudaSuccess)
+        return bail(fail(c0, EXS_ERR_CUDA, "cudaGraphInstantiate"));
+    *out = G;
+    return EXS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int exs_graph_create(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,
                      exs_complex *const *h_dev, exs_complex *const *o_dev, exs_graph **out)
 {
     if (!out) return fail(c, EXS_ERR_ARG, "exs_graph_create: null output");
     *out = nullptr;
-    std::vector<KDesc> ks;
-    int rc = device_batch(c, nk, ngp, igpig_dev, vgpc_dev, h_dev, o_dev, ks);
+    std::vector<std::vector<KDesc>> kss(1);
+    int rc = device_batch(c, nk, ngp, igpig_dev, vgpc_dev, h_dev, o_dev, kss[0]);
     if (rc != EXS_OK) return rc;
     if (nk == 0) return fail(c, EXS_ERR_SIZE, "exs_graph_create: empty batch");
     cudaSetDevice(c->device);
-    cudaStream_t s = c->stream;
     (void)cudaGetLastError();
-    // the graph owns its tables: pack them once, outside the capture
-    std::vector<int> ozt;
-    TableLayout L;
-    pack_tables(c, ks, ozt, L);
-    std::vector<char> h(L.total);
-    write_tables(c, ks, ozt, L, h.data());
-    exs_graph *G = new exs_graph;
-    G->c = c;
-    G->gen = c->gen;
-    auto bail = [&](int code) {
-        if (G->exec) cudaGraphExecDestroy(G->exec);
-        if (G->graph) cudaGraphDestroy(G->graph);
-        if (G->d_tables) cudaFree(G->d_tables);
-        delete G;
-        return code;
-    };
-    if (cudaMalloc(&G->d_tables, L.total) != cudaSuccess) return bail(fail(c, EXS_ERR_NOMEM, "graph tables"));
-    if (cudaMemcpy(G->d_tables, h.data(), L.total, cudaMemcpyHostToDevice) != cudaSuccess)
-        return bail(fail(c, EXS_ERR_CUDA, "graph tables upload"));
-    const Uploaded u = device_view(L, (char *)G->d_tables);
-    // one plain run first: kernel attributes are set on first launch, outside any capture
-    if (cudaMemsetAsync(c->d_err, 0, sizeof(int), s) != cudaSuccess) return bail(fail(c, EXS_ERR_CUDA, "memset"));
-    rc = enqueue_setup(c, ks, u, false, false);
-    if (rc < 0) return bail(rc);
-    rc = exs_synchronize(c);
-    if (rc < 0) return bail(rc);
-    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return bail(fail(c, EXS_ERR_CUDA, "cudaStreamBeginCapture"));
-    cudaError_t e = cudaMemsetAsync(c->d_err, 0, sizeof(int), s);
-    rc = e == cudaSuccess ? enqueue_setup(c, ks, u, false, false) : EXS_ERR_CUDA;
-    cudaError_t ee = cudaStreamEndCapture(s, &G->graph);
-    if (rc < 0 || ee != cudaSuccess) return bail(rc < 0 ? rc : fail(c, EXS_ERR_CUDA, "cudaStreamEndCapture"));
-    if (cudaGraphInstantiate(&G->exec, G->graph, 0) != cudaSuccess)
-        return bail(fail(c, EXS_ERR_CUDA, "cudaGraphInstantiate"));
-    *out = G;
-    return EXS_OK;
+    return graph_capture({c}, kss, out);
+}
+
+int exs_graph_create_multi(int nctx, exs_ctx *const *ctx, const int *nk, const int *const *ngp,
+                           const int *const *igpig_dev, const double *const *vgpc_dev,
+                           exs_complex *const *const *h_dev, exs_complex *const *const *o_dev, exs_graph **out)
+{
+    if (!out || nctx <= 0 || !ctx || !nk || !ngp || !igpig_dev || !vgpc_dev || !h_dev || !o_dev)
+        return EXS_ERR_ARG;
+    *out = nullptr;
+    std::vector<exs_ctx *> cs(ctx, ctx + nctx);
+    std::vector<std::vector<KDesc>> kss(nctx);
+    for (int i = 0; i < nctx; i++) {
+        if (!cs[i] || cs[i]->device != cs[0]->device) return EXS_ERR_ARG;
+        int rc = device_batch(cs[i], nk[i], ngp[i], igpig_dev[i], vgpc_dev[i], h_dev[i], o_dev[i], kss[i]);
+        if (rc != EXS_OK) return rc;
+        if (nk[i] == 0) return fail(cs[i], EXS_ERR_SIZE, "exs_graph_create_multi: empty batch");
+    }
+    cudaSetDevice(cs[0]->device);
+    (void)cudaGetLastError();
+    return graph_capture(cs, kss, out);
 }
 
 int exs_graph_launch(exs_graph *G)
 {
     if (!G) return EXS_ERR_ARG;
-    exs_ctx *c = G->c;
-    if (G->gen != c->gen) return fail(c, EXS_ERR_STATE, "graph captured before the last exs_set_precision");
+    for (size_t i = 0; i < G->cs.size(); i++)
+        if (G->gens[i] != G->cs[i]->gen)
+            return fail(G->cs[i], EXS_ERR_STATE, "graph captured before the last exs_set_precision");
+    exs_ctx *c = G->cs[0];
     cudaSetDevice(c->device);
     EXS_CUDA(cudaGraphLaunch(G->exec, c->stream));
-    c->timed = false;
+    for (exs_ctx *x : G->cs) x->timed = false;
     return EXS_OK;
+}
+
+int exs_graph_synchronize(exs_graph *G)
+{
+    if (!G) return EXS_ERR_ARG;
+    int worst = EXS_OK;
+    for (exs_ctx *c : G->cs) {   // the first waits for the graph; each reports its own device flags
+        const int rc = exs_synchronize(c);
+        if (rc < 0) return rc;
+        if (rc > worst) worst = rc;
+    }
+    return worst;
 }
 
 void exs_graph_destroy(exs_graph *G)
 {
     if (!G) return;
-    cudaSetDevice(G->c->device);
-    if (G->exec) cudaGraphExecDestroy(G->exec);
-    if (G->graph) cudaGraphDestroy(G->graph);
-    if (G->d_tables) cudaFree(G->d_tables);
-    delete G;
+    cudaSetDevice(G->cs[0]->device);
+    graph_free(G);
 }
 
 int exs_setup_batched_device(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,

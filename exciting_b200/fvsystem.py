@@ -245,14 +245,18 @@ class Setup:
 
 class SetupGraph:
     """A captured batched setup (exs_graph_*): launch() replays it on the
-    context's stream; Setup.synchronize() waits and reports device errors."""
+    (first) context's stream; synchronize() waits and reports device errors."""
 
-    def __init__(self, setup: Setup, handle):
+    def __init__(self, setup: Setup, handle, others=()):
         self.setup = setup
         self.handle = handle
+        self.others = list(others)          # further contexts of a multi-context graph
 
     def launch(self):
         return self.setup._check(self.setup.lib.exs_graph_launch(self.handle))
+
+    def synchronize(self):
+        return self.setup._check(self.setup.lib.exs_graph_synchronize(self.handle))
 
     def close(self):
         if self.handle:
@@ -264,3 +268,36 @@ class SetupGraph:
             self.close()
         except Exception:
             pass
+
+
+def multi_graph(setups, batches) -> SetupGraph:
+    """One CUDA graph over several contexts (exs_graph_create_multi).
+
+    ``batches[i]`` = (ngp list, igpig device pointer, vgpc device pointer,
+    h device pointers, o device pointers) for ``setups[i]``, as for
+    ``Setup.setup_batched_device``."""
+    n = len(setups)
+    P = ctypes.c_void_p
+    keep = []
+    ctxs = (P * n)(*[s.ctx for s in setups])
+    nk = np.array([len(b[0]) for b in batches], dtype=np.int32)
+    ngp_arrs = [np.asarray(b[0], dtype=np.int32) for b in batches]
+    keep += ngp_arrs
+    ngp_p = (P * n)(*[a.ctypes.data for a in ngp_arrs])
+    ig_p = (P * n)(*[b[1] for b in batches])
+    vg_p = (P * n)(*[b[2] for b in batches])
+    harr = [(P * len(b[3]))(*b[3]) for b in batches]
+    oarr = [(P * len(b[4]))(*b[4]) for b in batches]
+    keep += harr + oarr
+    h_p = (P * n)(*[ctypes.addressof(a) for a in harr])
+    o_p = (P * n)(*[ctypes.addressof(a) for a in oarr])
+    g = P()
+    lib = setups[0].lib
+    rc = lib.exs_graph_create_multi(n, ctxs, _ptr(nk), ngp_p, ig_p, vg_p, h_p, o_p, ctypes.byref(g))
+    if rc < 0:
+        for s in setups:
+            err = lib.exs_last_error(s.ctx)
+            if err:
+                raise abi.ExsError(rc, err.decode())
+        raise abi.ExsError(rc, "exs_graph_create_multi failed")
+    return SetupGraph(setups[0], g, setups[1:])

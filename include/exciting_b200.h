@@ -170,6 +170,20 @@ int exs_graph_create(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig
 int exs_graph_launch(exs_graph *graph);
 void exs_graph_destroy(exs_graph *graph);
 
+/* One graph over several contexts: the batched device setup of nk[i]
+ * k-points of context ctx[i] (arguments per context as for
+ * exs_setup_batched_device), for the uneven-size batch of independent cells
+ * (one context per cell).  The contexts' launches are captured on up to 32
+ * concurrent branches; the graph is launched on ctx[0]'s stream.
+ * exs_graph_synchronize waits for it and returns the worst status of all
+ * contexts (device error flags included); it also serves single-context
+ * graphs. */
+int exs_graph_create_multi(int nctx, exs_ctx *const *ctx, const int *nk, const int *const *ngp_host,
+                           const int *const *igpig_dev, const double *const *vgpc_dev,
+                           exs_complex *const *const *h_dev, exs_complex *const *const *o_dev,
+                           exs_graph **out);
+int exs_graph_synchronize(exs_graph *graph);
+
 /* Replaces the IBS part of  call forcek(ik, ffacg)  (src/forcek.f90:13) for
  * one k-point without second variation:
  *   igpig(ngkmax), vgpc(3, ngkmax), evecfv(nmatmax, nstfv) (leading dim ldv),
