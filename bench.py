@@ -126,6 +126,14 @@ def _measured_int8_peak(torch):
     return best
 
 
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0      # earlier measurement on this pool's B200s
+
+
 def ozaki_int8_ops(sys_, gks, slices):
     """int8 MMA operations the split-precision kernel issues: per 128 x 32 tile
     (B operand [Br|Bi|Ar|Ai] -> N = 128), S(S+1)/2 slice pairs x two A operands
@@ -350,6 +358,24 @@ def run_ours(args):
     graph_ms = float(t.item())
     graph.close()
 
+    # ---- the interstitial gather alone (hmlistln + olpistln on the 27 H/O pairs),
+    # HBM-bound: 32 N(N+1) bytes per k-point (read + write of the upper H and O)
+    def gather_step():
+        st.interstitial_batched_device(3, ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op, nmat)
+    for _ in range(args.warmup):
+        gather_step()
+    st.synchronize()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            gather_step()
+        e1.record(stream)
+    st.synchronize()
+    torch.cuda.synchronize()
+    gather_ms = e0.elapsed_time(e1) / args.steps
+    gather_bytes = sum(32.0 * n * (n + 1) for n in ngp)
+
     # ---- end to end through the host-pointer entry point
     if args.skip_e2e:
         e2e_value, h2d, d2h = None, 0, 0
@@ -441,6 +467,13 @@ def run_ours(args):
                              "ms_per_step": graph_ms / args.steps,
                              "note": "same batch captured once (exs_graph_create) and replayed"},
             "roofline": roof,
+            "interstitial_gather": {
+                "kernel": "interstitial_kernel (exs_interstitial_batched_device: hmlistln + olpistln, 27 k-points "
+                          "in one launch)",
+                "ms_per_step": gather_ms, "bytes_per_step": gather_bytes,
+                "achieved": gather_bytes / (gather_ms * 1e-3) / 1e9, "unit": "GB/s",
+                "peak": _hbm_peak(), "frac": gather_bytes / (gather_ms * 1e-3) / 1e9 / _hbm_peak(),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
             "cpu_baseline": None if cpu_v is None else {
                 "value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
                 "sample": f"{cpu_n} k-points of the 27-k set in {cpu_dt:.1f} s by the FP64 CPU "

@@ -48,6 +48,10 @@ SIGNATURES = {
     "exs_setup_batched_device": ([P, c_int, P, P, P, P, P], c_int),
     "exs_synchronize": ([P], c_int),
     "exs_autotune": ([P, c_int, P, P, P, P, P, P], c_int),
+    "exs_hmlistln": ([P, c_int, P, P, P, c_int], c_int),
+    "exs_olpistln": ([P, c_int, P, P, P, c_int], c_int),
+    "exs_interstitial_device": ([P, c_int, c_int, P, P, P, P, c_int], c_int),
+    "exs_interstitial_batched_device": ([P, c_int, c_int, P, P, P, P, P, P], c_int),
     "exs_set_kernel_config": ([P, c_int], c_int),
     "exs_graph_create": ([P, c_int, P, P, P, P, P, P], c_int),
     "exs_graph_launch": ([P], c_int),

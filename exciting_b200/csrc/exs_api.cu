@@ -692,6 +692,28 @@ int upload_tables(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
     return EXS_OK;
 }
 
+// Only the k descriptors, through the same staging buffer as upload_tables.
+int upload_kdesc(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
+{
+    const size_t need = ks.size() * sizeof(KDesc);
+    EXS_CUDA(cudaEventSynchronize(c->tables_free));
+    if (need > c->tables_bytes) {
+        if (c->h_tables) cudaFreeHost(c->h_tables);
+        if (c->d_tables) cudaFree(c->d_tables);
+        c->h_tables = c->d_tables = nullptr;
+        c->tables_bytes = 0;
+        EXS_CUDA(cudaMallocHost(&c->h_tables, need * 2));
+        EXS_CUDA(cudaMalloc(&c->d_tables, need * 2));
+        c->tables_bytes = need * 2;
+    }
+    std::memcpy(c->h_tables, ks.data(), need);
+    u = Uploaded{};
+    u.d_k = (const KDesc *)c->d_tables;
+    EXS_CUDA(cudaMemcpyAsync(c->d_tables, c->h_tables, need, cudaMemcpyHostToDevice, c->stream));
+    EXS_CUDA(cudaEventRecord(c->tables_free, c->stream));
+    return EXS_OK;
+}
+
 // Zero the column maxima that the A and B producers raise (split-precision
 // path only; the slots of one call are contiguous).
 cudaError_t oz_reset_maxima(exs_ctx *c, const std::vector<KDesc> &ks, cudaStream_t s)
@@ -1044,6 +1066,92 @@ void exs_graph_destroy(exs_graph *G)
     if (!G) return;
     cudaSetDevice(G->cs[0]->device);
     graph_free(G);
+}
+
+int exs_interstitial_batched_device(exs_ctx *c, int which, int nk, const int *ngp, const int *igpig_dev,
+                                    const double *vgpc_dev, exs_complex *const *h_dev, exs_complex *const *o_dev,
+                                    const int *ld)
+{
+    if (!c || which < 1 || which > 3 || nk < 0 || (nk > 0 && (!ngp || !igpig_dev || !vgpc_dev || !ld)) ||
+        ((which & 1) && nk > 0 && !h_dev) || ((which & 2) && nk > 0 && !o_dev))
+        return fail(c, EXS_ERR_ARG, "exs_interstitial_batched_device: bad argument");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    std::vector<KDesc> ks(nk);
+    int ngp_max = 0;
+    for (int k = 0; k < nk; k++) {
+        if (ngp[k] <= 0 || ngp[k] > c->ngkmax || ld[k] < ngp[k] || ((which & 1) && !h_dev[k]) ||
+            ((which & 2) && !o_dev[k]))
+            return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax, ld < ngp or null matrix");
+        KDesc &d = ks[k];
+        d = KDesc{};
+        d.ngp = ngp[k];
+        d.nmat = ld[k];
+        d.igpig = igpig_dev + (size_t)c->ngkmax * k;
+        d.vgpc = vgpc_dev + 3 * (size_t)c->ngkmax * k;
+        d.h = (which & 1) ? h_dev[k] : nullptr;
+        d.o = (which & 2) ? o_dev[k] : nullptr;
+        ngp_max = std::max(ngp_max, ngp[k]);
+    }
+    if (nk == 0) return EXS_OK;
+    cudaSetDevice(c->device);
+    (void)cudaGetLastError();
+    // the descriptors travel through the context's table buffer (same staging rules as the setup)
+    Uploaded u{};
+    int rc = upload_kdesc(c, ks, u);
+    if (rc != EXS_OK) return rc;
+    EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    EXS_CUDA(exs::launch_interstitial(c->params(), which, u.d_k, nk, ngp_max, c->stream));
+    c->timed = false;
+    return EXS_OK;
+}
+
+int exs_interstitial_device(exs_ctx *c, int which, int ngp, const int *igpig_dev, const double *vgpc_dev,
+                            exs_complex *h_dev, exs_complex *o_dev, int ld)
+{
+    exs_complex *hh[1] = {h_dev}, *oo[1] = {o_dev};
+    return exs_interstitial_batched_device(c, which, 1, &ngp, igpig_dev, vgpc_dev, hh, oo, &ld);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Host-array form: za(1:ngp, 1:ngp) (leading dimension ld) through the
+// context's H/O buffer of slot 0.
+int host_interstitial(exs_ctx *c, int which, int ngp, const int *igpig, const double *vgpc, exs_complex *z, int ld)
+{
+    if (!c || !igpig || !vgpc || !z) return fail(c, EXS_ERR_ARG, "hmlistln/olpistln: null argument");
+    if (ngp <= 0 || ngp > c->ngkmax || ld < ngp || ld > c->nmatmax)
+        return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax or ld outside ngp..nmatmax");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    for (int i = 0; i < ngp; i++)
+        if (igpig[i] < 1 || igpig[i] > c->ngrtot) return fail(c, EXS_ERR_INDEX, "igpig entry outside 1..ngrtot");
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    EXS_CUDA(cudaStreamSynchronize(s));
+    const size_t bytes = sizeof(exs_complex) * (size_t)ld * ngp;
+    EXS_CUDA(cudaMemcpyAsync(c->d_igpig, igpig, sizeof(int) * ngp, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaMemcpyAsync(c->d_vgpc, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyHostToDevice, s));
+    EXS_CUDA(cudaMemcpyAsync(c->d_ho, z, bytes, cudaMemcpyHostToDevice, s));
+    int rc = exs_interstitial_device(c, which, ngp, c->d_igpig, c->d_vgpc, which == 1 ? c->d_ho : nullptr,
+                                     which == 2 ? c->d_ho : nullptr, ld);
+    if (rc < 0) return rc;
+    EXS_CUDA(cudaMemcpyAsync(z, c->d_ho, bytes, cudaMemcpyDeviceToHost, s));
+    return exs_synchronize(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int exs_hmlistln(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, exs_complex *h, int ld)
+{
+    return host_interstitial(c, 1, ngp, igpig, vgpc, h, ld);
+}
+
+int exs_olpistln(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, exs_complex *o, int ld)
+{
+    return host_interstitial(c, 2, ngp, igpig, vgpc, o, ld);
 }
 
 int exs_setup_batched_device(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const double *vgpc_dev,

@@ -237,6 +237,8 @@ cudaError_t launch_olp_apwlo(const DevParams &p, const KDesc *d_k, int nk, int n
 void build_gemm_tables(const exs_ctx *c, const std::vector<KDesc> &ks, GemmTables &t);
 cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, const void *d_work, int nwork,
                              const KDesc *d_k, cudaStream_t s);
+// Stand-alone interstitial gather (interstitial.cu)
+cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s);
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStream_t s);

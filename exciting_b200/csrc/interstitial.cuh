@@ -6,7 +6,8 @@
 namespace exs {
 
 // Interstitial term of element (i, j), i <= j < ngp (hmlistln.f90:61-86,
-// olpistln.f90:53-82).  Returns false when nothing is added.
+// olpistln.f90:53-82).  Returns false when nothing is added.  The tables are
+// read-only during every kernel that calls this (read-only data path).
 __device__ __forceinline__ bool interstitial(const DevParams &p, int kind, const int *ivi, const int *ivj,
                                              const double *vi, const double *vj, double &zr, double &zi)
 {
@@ -18,16 +19,20 @@ __device__ __forceinline__ bool interstitial(const DevParams &p, int kind, const
         atomicOr(p.err, DEV_ERR_INDEX);
         return false;
     }
-    const int ig = p.ivgig[d0 + p.intgv_n[0] * (d1 + p.intgv_n[1] * d2)];
+    const int ig = __ldg(p.ivgig + d0 + p.intgv_n[0] * (d1 + p.intgv_n[1] * d2));
     if (ig <= 0 || ig > p.ngvec) return false;
     const double dp = vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2];
     if (kind == EPI_HAM) {
         const double t1 = 0.5 * dp;
-        const exs_complex v = p.veffig[ig - 1], w = p.kinw[ig - 1];
-        zr = v.re + t1 * w.re;
-        zi = v.im + t1 * w.im;
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p.veffig) + ig - 1);
+        const double2 w = __ldg(reinterpret_cast<const double2 *>(p.kinw) + ig - 1);
+        zr = v.x + t1 * w.x;
+        zi = v.y + t1 * w.y;
     } else {
-        const exs_complex c = p.cfunig[ig - 1];
+        const double2 cc = __ldg(reinterpret_cast<const double2 *>(p.cfunig) + ig - 1);
+        exs_complex c;
+        c.re = cc.x;
+        c.im = cc.y;
         if (p.relativity == EXS_REL_IORA) {
             const double alpha = 1.0 / 137.03599911, a2 = 0.5 * alpha * alpha;
             const double t1 = 0.5 * a2 * dp;

@@ -205,6 +205,35 @@ class Setup:
         self._check(self.lib.exs_autotune(*args, ctypes.byref(choice)))
         return choice.value
 
+    def hmlistln(self, gk, h):
+        """Add the interstitial H term to the upper triangle of h (Fortran-ordered, in place)."""
+        assert h.flags.f_contiguous and h.dtype == np.complex128
+        ig, vg = self._gk_arrays(gk)
+        return self._check(self.lib.exs_hmlistln(self.ctx, gk.ngp, _ptr(ig), _ptr(vg), _ptr(h), h.shape[0]))
+
+    def olpistln(self, gk, o):
+        """Add the interstitial O term to the upper triangle of o (Fortran-ordered, in place)."""
+        assert o.flags.f_contiguous and o.dtype == np.complex128
+        ig, vg = self._gk_arrays(gk)
+        return self._check(self.lib.exs_olpistln(self.ctx, gk.ngp, _ptr(ig), _ptr(vg), _ptr(o), o.shape[0]))
+
+    def interstitial_device(self, which, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptr, o_ptr, ld):
+        """Device form (which: 1 H, 2 O, 3 both); asynchronous on the context's stream."""
+        return self._check(self.lib.exs_interstitial_device(
+            self.ctx, int(which), int(ngp), ctypes.c_void_p(igpig_dev_ptr), ctypes.c_void_p(vgpc_dev_ptr),
+            ctypes.c_void_p(h_ptr) if h_ptr else None, ctypes.c_void_p(o_ptr) if o_ptr else None, int(ld)))
+
+    def interstitial_batched_device(self, which, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs, ld):
+        """All k-points of a batch in one launch (device pointers as for setup_batched_device)."""
+        nk = len(ngp)
+        ngp = np.asarray(ngp, dtype=np.int32)
+        ld = np.asarray(ld, dtype=np.int32)
+        hp = (ctypes.c_void_p * nk)(*h_ptrs)
+        op = (ctypes.c_void_p * nk)(*o_ptrs)
+        return self._check(self.lib.exs_interstitial_batched_device(
+            self.ctx, int(which), nk, _ptr(ngp), ctypes.c_void_p(igpig_dev_ptr), ctypes.c_void_p(vgpc_dev_ptr),
+            hp, op, _ptr(ld)))
+
     def set_kernel_config(self, cfg: int):
         """Force a split-precision kernel configuration (0 .. EXS_OZ_NCONFIG-1)."""
         return self._check(self.lib.exs_set_kernel_config(self.ctx, int(cfg)))

@@ -132,6 +132,29 @@ int exs_setup_batched_device(exs_ctx *ctx, int nk, const int *ngp_host,
                              exs_complex *const *h_dev, exs_complex *const *o_dev);
 int exs_synchronize(exs_ctx *ctx);
 
+/* The interstitial blocks alone: replaces
+ *   call hmlistln(hamilton, ngp, igpig, vgpc)  (src/src_eigensystem/hmlistln.f90:13)
+ *   call olpistln(overlap, ngp, igpig, vgpc)   (src/src_eigensystem/olpistln.f90:13)
+ * ADDING to the upper triangle za(i, j), i <= j < ngp, of za(ld, *) as the
+ * reference does (Hermitianmatrix_indexedupdate, modfvsystem.f90:126-143):
+ * V(ig) + 1/2 (k+G_i).(k+G_j) W(ig) for H, Theta(ig) (+ the iora* term) for
+ * O, ig = ivgig(ivg(:,igpig(i)) - ivg(:,igpig(j))).  Host arrays,
+ * synchronous; ld <= nmatmax.  (exs_hamiltonandoverlapsetup already
+ * includes these terms.) */
+int exs_hmlistln(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc, exs_complex *h, int ld);
+int exs_olpistln(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc, exs_complex *o, int ld);
+/* Same on device arrays: which = 1 (H), 2 (O) or 3 (both); asynchronous on
+ * the context's stream, exs_synchronize waits. */
+int exs_interstitial_device(exs_ctx *ctx, int which, int ngp, const int *igpig_dev,
+                            const double *vgpc_dev, exs_complex *h_dev, exs_complex *o_dev, int ld);
+/* nk k-points in one launch: igpig_dev(ngkmax, nk), vgpc_dev(3, ngkmax, nk),
+ * h_dev[k], o_dev[k] with leading dimensions ld[k] (host arrays of device
+ * pointers / sizes). */
+int exs_interstitial_batched_device(exs_ctx *ctx, int which, int nk, const int *ngp_host,
+                                    const int *igpig_dev, const double *vgpc_dev,
+                                    exs_complex *const *h_dev, exs_complex *const *o_dev,
+                                    const int *ld_host);
+
 /* Autotuner (no counterpart in the reference): runs the batch described as
  * for exs_setup_batched_device once per kernel configuration of the active
  * precision mode (for the split-precision contraction: K chunks per
