@@ -216,49 +216,60 @@ __device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, i
 }
 
 // The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
-// A 32(f) x 32(G) tile per block, transposed through shared memory: reads
-// G-contiguous planes (a warp reads 32 consecutive G), writes K-contiguous
-// int8 rows four bytes per thread (8 threads cover the tile's 32 K bytes of
-// one G row).
+// A 64(f) x 32(G) tile per block, transposed through shared memory: reads
+// G-contiguous planes (a warp reads 32 consecutive G; 16 loads per thread in
+// flight), writes K-contiguous int8 rows eight bytes per thread (8 threads
+// cover the tile's 64 K bytes of one G row).
+constexpr int SPLIT_F = 64;
+
 __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8, int a0)
 {
-    __shared__ double t[2][32][33];
+    __shared__ double t[2][SPLIT_F][33];
     const KDesc k = ks[blockIdx.z];
-    const int f0 = blockIdx.x * 32, g0 = blockIdx.y * 32;
+    const int f0 = blockIdx.x * SPLIT_F, g0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;      // 32 x 8
     const double *pr = a0 == 0 ? k.br : k.ar, *pi = a0 == 0 ? k.bi : k.ai;
-    for (int r = ty; r < 32; r += 8) {
-        const int f = f0 + r, g = g0 + tx;
-        const bool v = f < p.K && g < k.ngp;
-        const size_t i = (size_t)f * p.npad + g;
-        t[0][r][tx] = v ? pr[i] : 0.0;
-        t[1][r][tx] = v ? pi[i] : 0.0;
+    {
+        double vr[SPLIT_F / 8], vi[SPLIT_F / 8];
+#pragma unroll
+        for (int q = 0; q < SPLIT_F / 8; q++) {
+            const int f = f0 + ty + 8 * q, g = g0 + tx;
+            const bool v = f < p.K && g < k.ngp;
+            const size_t i = (size_t)f * p.npad + g;
+            vr[q] = v ? pr[i] : 0.0;
+            vi[q] = v ? pi[i] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < SPLIT_F / 8; q++) {
+            t[0][ty + 8 * q][tx] = vr[q];
+            t[1][ty + 8 * q][tx] = vi[q];
+        }
     }
     __syncthreads();
     const int tid = ty * 32 + tx;
-    const int gl = tid >> 3, fl = (tid & 7) * 4;
+    const int gl = tid >> 3, fl = (tid & 7) * 8;
     const int g = g0 + gl, f = f0 + fl;
     if (g >= p.npad || f >= kp8) return;
     // 1/sigma is a power of two: the scaling is exact
     const double rs = 1.0 / oz_sigma(k.oz_scale[(a0 == 0 ? p.npad : 0) + g]);
-    double x[2][4];
+    double x[2][8];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < 8; e++) {
         x[0][e] = t[0][fl + e][gl] * rs;
         x[1][e] = t[1][fl + e][gl] * rs;
     }
     for (int s = 0; s < S; s++)
 #pragma unroll
         for (int a = 0; a < 2; a++) {
-            uint32_t w = 0;
+            uint32_t w[2] = {0, 0};
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
+            for (int e = 0; e < 8; e++) {
                 x[a][e] *= 128.0;
                 const double tq = trunc(x[a][e]);
                 x[a][e] -= tq;
-                w |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * e);
+                w[e >> 2] |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * (e & 3));
             }
-            *reinterpret_cast<uint32_t *>(k.oz_slices + oz_off(s, a0 + a, g, f, p.npad, kp8)) = w;
+            *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(s, a0 + a, g, f, p.npad, kp8)) = make_uint2(w[0], w[1]);
         }
 }
 
@@ -726,7 +737,7 @@ const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4};
 
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
 {
-    oz_split_kernel<<<dim3(kp8 / 32, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8, a0);
+    oz_split_kernel<<<dim3(kp8 / SPLIT_F, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8, a0);
     return cudaGetLastError();
 }
 
