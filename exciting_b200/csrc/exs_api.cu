@@ -387,7 +387,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     bool maps_ok = true;
     for (int q = 0; q < exs::OZ_NCFG; q++)
         maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, nss, c->npad, kp8, exs::OZ_CFG_KCH[q], &c->oz_mapA[q],
-                                                      &c->oz_mapB[q]);
+                                                      &c->oz_mapB[q], &c->oz_mapB2[q]);
     maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, nss, c->npad, kp8, c->d_xs, xgroups, c->oz_lw,
                                                 &c->oz_mapArow, &c->oz_mapX);
     if (!maps_ok) {
@@ -573,15 +573,16 @@ struct Uploaded {
     int nozatiles;
 };
 
-// Upper tiles (128 rows x 32 columns) of the split-precision contraction.
-void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t)
+// Upper tiles (128 rows x 32 columns, or 256 x 32 for the two-SM tiles with
+// ib counting pairs of 128-row blocks) of the split-precision contraction.
+void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows)
 {
     t.clear();
     for (size_t k = 0; k < ks.size(); k++) {
         const int n = ks[k].ngp;
-        for (int ib = 0; ib < (n + 127) / 128; ib++)
+        for (int ib = 0; ib < (n + rows - 1) / rows; ib++)
             for (int jb = 0; jb < (n + 31) / 32; jb++)
-                if (jb * 32 + 31 >= ib * 128) { t.push_back((int)k); t.push_back(ib); t.push_back(jb); }
+                if (jb * 32 + 31 >= ib * rows) { t.push_back((int)k); t.push_back(ib); t.push_back(jb); }
     }
 }
 
@@ -616,7 +617,7 @@ void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt
     ozt.clear();
     std::vector<int> ozat;
     if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
-        oz_tiles(ks, ozt);
+        oz_tiles(ks, ozt, (c->oz_cfg & 8) ? 256 : 128);
         oz_atom_tiles(c, ks, ozat);
     }
     L.noz = (int)(ozt.size() / 3);
@@ -758,8 +759,8 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     if (oz) {
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 0, s));
         const int q = c->oz_cfg;
-        EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], &c->oz_mapB[q], p, u.d_k, u.d_oztiles, u.noztiles, c->slices,
-                                    c->kp8, c->oz_seg, s));
+        EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,
+                                    u.d_oztiles, u.noztiles, c->slices, c->kp8, c->oz_seg, s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
                                        u.nwork[exs::EPI_HAM], u.d_k, s));
@@ -863,14 +864,15 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
         return rc < 0 ? rc : exs_synchronize(c);
     }
     (void)cudaGetLastError();
-    Uploaded u{};
-    rc = upload_tables(c, ks, u);
-    if (rc != EXS_OK) return rc;
     constexpr int REPS = 3;
     float best = 0.f;
     int best_q = 0;
     for (int q = 0; q < exs::OZ_NCFG; q++) {
+        if ((q & 8) && (q & 2)) continue;   // the two-SM tiles have no persistent form
         c->oz_cfg = q;
+        Uploaded u{};                        // the tile list depends on the configuration
+        rc = upload_tables(c, ks, u);
+        if (rc != EXS_OK) return rc;
         EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
         rc = enqueue_setup(c, ks, u, false, false);      // warm-up
         if (rc < 0) return rc;

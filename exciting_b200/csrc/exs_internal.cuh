@@ -22,7 +22,7 @@ enum : int {
 };
 
 // Pipeline configurations of the split-precision kernel.
-constexpr int OZ_NCFG = 8;
+constexpr int OZ_NCFG = 16;
 // Modes of the split-precision kernel: H/O tiles, per-atom products (h_a A, loa A).
 enum : int { OZ_HO = 0, OZ_ATOM = 1 };
 
@@ -200,6 +200,7 @@ struct exs_ctx {
     double *d_ozscale = nullptr; // column scales of all slots
     size_t oz_slot_bytes = 0;
     CUtensorMap oz_mapA[exs::OZ_NCFG], oz_mapB[exs::OZ_NCFG];   // TMA views of d_oz per pipeline configuration
+    CUtensorMap oz_mapB2[exs::OZ_NCFG];                            // half-B views (two-SM tiles)
     int oz_cfg = 0;                   // pipeline configuration of the split-precision kernel
     // per-atom products of the split-precision path (h_a A, loa A)
     int8_t *d_xs = nullptr;           // slices of h_a and loa
@@ -250,7 +251,8 @@ bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, s
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
                           cudaStream_t s);
-bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB);
+bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB,
+                         CUtensorMap *mapB2);
 extern const int OZ_CFG_KCH[OZ_NCFG], OZ_CFG_NST[OZ_NCFG];
 int oz_kpad(int K);
 size_t oz_slot_bytes(int S, int npad, int kp8);

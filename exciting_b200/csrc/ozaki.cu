@@ -716,6 +716,340 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     }
 }
 
+// ------------------------------------------------------------ two-SM H/O tiles
+// A cluster of two CTAs computes a 256 (G_i) x 32 (G_j) tile with
+// tcgen05.mma.cta_group::2 (M = 256): each CTA holds its own 128 rows of the
+// A operands (Ar, Ai) and half of the B operand (CTA 0: Br, Bi; CTA 1: Ar,
+// Ai of the 32 G_j), so each SM fetches 320 instead of 384 operand rows per
+// K byte.  CTA 0 issues the MMAs; its full barriers count the bytes of both
+// CTAs' copies (the copies of CTA 1 signal CTA 0's barrier); MMA completion
+// is signalled to both CTAs (multicast commit); both CTAs' epilogues fold
+// their own 128 rows and report to CTA 0's barrier.  No TMA multicast.
+constexpr uint32_t OZ_PEER_BIT_MASK = 0xFEFFFFFFu;   // shared::cluster address of CTA 0's copy
+
+__device__ __forceinline__ uint32_t cluster_ctarank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t addr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d_2sm(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                                int c4, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3, %4, %5, %6}], [%7];\n" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar & OZ_PEER_BIT_MASK)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_i8_2sm(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+// Arrive on the barrier at this offset in both CTAs of the pair.
+__device__ __forceinline__ void umma_commit_2sm(uint64_t *bar)
+{
+    const uint16_t mask = 3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+            smem_u32(bar)),
+        "h"(mask)
+        : "memory");
+}
+
+template <int KCH, int NST>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
+oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB2, DevParams p,
+               const KDesc *ks, const int *tiles, int S, int kp8, int seg_pairs)
+{
+    constexpr int ABOX = 2 * KCH * OZ_TILE;          // Ar, Ai of this CTA's 128 rows
+    constexpr int BBOX = KCH * OZ_TILE / 2;          // this CTA's 64 rows of B
+    constexpr int STAGE = ABOX + BBOX;
+    extern __shared__ __align__(1024) uint8_t oz_smem[];
+    __shared__ uint64_t full[NST], empty[NST], accf, acce;
+    __shared__ uint32_t tmem_sh;
+    __shared__ int abort_sh;
+    volatile int *abort = &abort_sh;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_ctarank();
+    const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
+    const int t3 = 3 * (blockIdx.x >> 1);
+    const KDesc kd = ks[tiles[t3]];
+    const int i0 = (2 * tiles[t3 + 1] + (int)rank) * OZ_BM, j0 = tiles[t3 + 2] * OZ_BJ;
+    const int nst = kp8 / (KCH * OZ_CHUNK);
+
+    if (warp == 3) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(OZ_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < NST; s++) {
+            mbar_init(&full[s], 1);      // CTA 0: one arrive (with the bytes of both CTAs)
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accf, 1);
+        mbar_init(&acce, 8);             // CTA 0: four epilogue warps in each CTA
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync_all();                  // the peer's barriers are initialised before anyone signals them
+    tc_fence_after();
+    const uint32_t tbase = tmem_sh;
+
+    if (warp < 2) {
+        // ------------------------------------------------ TMA producers (both CTAs)
+        if (lane == 0) {
+            const int role = warp;       // 0: this CTA's A rows, 1: this CTA's half of B
+            uint32_t fills[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) fills[q] = 0;
+            int st = 0;
+            bool bad = false;
+            const int slot = kd.oz_slot;
+            for (int d = 2; d <= S + 1 && !bad; d++)
+                for (int s = 1; s <= d - 1 && !bad; s++) {
+                    const int t = d - s;
+                    for (int kb = 0; kb < nst; kb++) {
+                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
+                            bad = true;
+                            break;
+                        }
+                        if (rank == 0 && role == 0) mbar_expect_tx(&full[st], 2 * STAGE);
+                        const uint32_t bar = smem_u32(&full[st]);
+                        if (role == 0)
+                            tma_load_5d_2sm(sbase + st * STAGE, &mapA, 0, i0, 2, kb * KCH, slot * S + s - 1, bar);
+                        else
+                            tma_load_5d_2sm(sbase + st * STAGE + ABOX, &mapB2, 0, j0, 2 * (int)rank, kb * KCH,
+                                            slot * S + t - 1, bar);
+                        fills[st]++;
+                        st = (st + 1 == NST) ? 0 : st + 1;
+                    }
+                }
+            // CTA 0: copies already issued (both CTAs') must land before the pair goes away;
+            // CTA 1 stopped issuing at least one bounded wait ago
+            if (bad && rank == 0)
+                for (int q = 0; q < NST; q++)
+                    if (fills[q] > 0) mbar_drain(&full[q], (fills[q] - 1) & 1);
+        }
+    } else if (warp == 3) {
+        // ------------------------------------------------ MMA issuer (CTA 0)
+        if (lane == 0 && rank == 0) {
+            const uint32_t idesc = umma_idesc_i8(256, OZ_N);
+            uint32_t uses[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) uses[q] = 0;
+            int nseg = 0, st = 0;
+            bool bad = false;
+            for (int d = 2; d <= S + 1 && !bad; d++)
+                for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
+                    const int s1 = min(d - 1, s0 + seg_pairs - 1);
+                    if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
+                        bad = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    bool first = true;
+                    for (int s = s0; s <= s1 && !bad; s++)
+                        for (int kb = 0; kb < nst; kb++) {
+                            if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
+                                bad = true;
+                                break;
+                            }
+                            tc_fence_after();
+                            const uint32_t sa = sbase + st * STAGE;
+#pragma unroll
+                            for (int c = 0; c < KCH; c++)
+#pragma unroll
+                                for (int q = 0; q < OZ_CHUNK / 32; q++) {
+                                    const uint32_t ao = c * 2 * OZ_TILE + q * 32;
+                                    const uint64_t bd = umma_desc_sw128(sa + ABOX + c * (OZ_TILE / 2) + q * 32);
+                                    const uint32_t acc = (first && c == 0 && q == 0) ? 0u : 1u;
+                                    umma_i8_2sm(tbase, umma_desc_sw128(sa + ao), bd, idesc, acc);
+                                    umma_i8_2sm(tbase + 128, umma_desc_sw128(sa + ao + OZ_TILE), bd, idesc, acc);
+                                }
+                            first = false;
+                            umma_commit_2sm(&empty[st]);
+                            uses[st]++;
+                            st = (st + 1 == NST) ? 0 : st + 1;
+                        }
+                    if (!bad) {
+                        umma_commit_2sm(&accf);
+                        nseg++;
+                    }
+                }
+            if (bad)
+                for (int q = 0; q < NST; q++)
+                    if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
+        }
+    } else if (warp >= 4) {
+        // ------------------------------------------------ epilogue (both CTAs, warps 4..7)
+        const int qd = warp & 3;
+        const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
+        const uint32_t acce0 = mapa_shared(smem_u32(&acce), 0);
+        int nseg = 0;
+        bool bad = false;
+        for (int d = 2; d <= S + 1 && !bad; d++) {
+            const double scale = ldexp(1.0, -7 * d);
+            for (int s0 = 1; s0 <= d - 1; s0 += seg_pairs) {
+                const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
+                if (!ok) {
+                    bad = true;
+                    break;
+                }
+                tc_fence_after();
+                const bool init = (nseg == 0);
+#pragma unroll 1
+                for (int o = 0; o < 4; o++) {
+                    const double sg = (o & 1) ? -1.0 : 1.0;
+#pragma unroll 1
+                    for (int jc = 0; jc < 32; jc += 16) {
+                        uint32_t rv[16], iv[16], lo[16], hi[16];
+                        const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
+                        tm_ld16(t_lane + o * 32 + jc, rv);
+                        tm_ld16(t_lane + 128 + (o ^ 1) * 32 + jc, iv);
+                        if (!init) {
+                            tm_ld16(t_lane + fcol, lo);
+                            tm_ld16(t_lane + fcol + 16, hi);
+                        }
+                        tm_wait_ld();
+                        uint32_t o0[16], o1[16];
+#pragma unroll
+                        for (int e = 0; e < 16; e++) {
+                            double a = 0.0;
+                            if (!init) {
+                                const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
+                                const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
+                                a = __hiloint2double((int)w1, (int)w0);
+                            }
+                            a += scale * ((double)(int)rv[e] + sg * (double)(int)iv[e]);
+                            const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
+                            if (e < 8) {
+                                o0[2 * e] = w0;
+                                o0[2 * e + 1] = w1;
+                            } else {
+                                o1[2 * (e - 8)] = w0;
+                                o1[2 * (e - 8) + 1] = w1;
+                            }
+                        }
+                        tm_st16(t_lane + fcol, o0);
+                        tm_st16(t_lane + fcol + 16, o1);
+                    }
+                }
+                tm_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_remote(acce0);      // CTA 0's barrier (also from CTA 0)
+                nseg++;
+            }
+        }
+        if (__all_sync(0xffffffffu, !bad && !*abort)) {
+            const int i = i0 + qd * 32 + lane;
+            int ivi[3] = {0, 0, 0};
+            double vi[3] = {0.0, 0.0, 0.0};
+            const bool row_ok = i < kd.ngp;
+            if (row_ok) {
+                int g = kd.igpig[i] - 1;
+                if (g < 0 || g >= p.ngrtot) {
+                    atomicOr(p.err, DEV_ERR_INDEX);
+                    g = 0;
+                }
+                for (int x = 0; x < 3; x++) {
+                    ivi[x] = p.ivg[3 * g + x];
+                    vi[x] = kd.vgpc[3 * i + x];
+                }
+            }
+            const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
+#pragma unroll 1
+            for (int jc = 0; jc < OZ_BJ; jc += 8) {
+                double val[4][8];
+#pragma unroll
+                for (int o = 0; o < 4; o++) {
+                    uint32_t w[16];
+                    tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
+                    tm_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 8; e++) val[o][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+                }
+                if (!row_ok) continue;
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int j = j0 + jc + e;
+                    if (j >= kd.ngp || i > j) continue;
+                    int gj = kd.igpig[j] - 1;
+                    if (gj < 0 || gj >= p.ngrtot) {
+                        atomicOr(p.err, DEV_ERR_INDEX);
+                        gj = 0;
+                    }
+                    const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
+                    const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
+                    const double sbj = oz_sigma(kd.oz_scale[p.npad + j]), saj = oz_sigma(kd.oz_scale[j]);
+                    double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
+                    double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
+                    double ar, ai;
+                    if (interstitial(p, EPI_HAM, ivi, ivj, vi, vj, ar, ai)) {
+                        hr += ar;
+                        hi += ai;
+                    }
+                    if (interstitial(p, EPI_OVL, ivi, ivj, vi, vj, ar, ai)) {
+                        orr += ar;
+                        oi += ai;
+                    }
+                    exs_complex hv, ov;
+                    hv.re = hr;
+                    hv.im = hi;
+                    ov.re = orr;
+                    ov.im = oi;
+                    kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
+                    kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
+                    if (i < j) {
+                        hv.im = -hi;
+                        ov.im = -oi;
+                        kd.h[(size_t)j + (size_t)kd.nmat * i] = hv;
+                        kd.o[(size_t)j + (size_t)kd.nmat * i] = ov;
+                    }
+                }
+            }
+        }
+    }
+    if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync_all();                  // neither CTA leaves while the pair still uses its memory
+    if (warp == 3) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(OZ_TMEM_COLS));
+    }
+}
+
 // ------------------------------------------------------------ host side
 int oz_kpad(int K) { return (K + OZ_MAX_KCH * OZ_CHUNK - 1) / (OZ_MAX_KCH * OZ_CHUNK) * (OZ_MAX_KCH * OZ_CHUNK); }
 
@@ -731,9 +1065,10 @@ int oz_seg_pairs(int S, int kp8)
 
 // configuration index: bit 0 = pipeline shape (KCH, NST) of the H/O tiles,
 // bit 1 = persistent launch (one CTA per SM) of the H/O tiles, bit 2 =
-// persistent launch of the per-atom tiles
-const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1};
-const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4};
+// persistent launch of the per-atom tiles, bit 3 = two-SM H/O tiles (256 x 32
+// per CTA pair; bit 1 unused then)
+const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1};
+const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4};
 
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
 {
@@ -773,11 +1108,31 @@ static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, 
     return cudaGetLastError();
 }
 
+template <int KCH, int NST>
+static cudaError_t launch_2sm(const CUtensorMap *mapA, const CUtensorMap *mapB2, const DevParams &p, const KDesc *d_k,
+                              const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s)
+{
+    constexpr int smem = NST * (2 * KCH * OZ_TILE + KCH * OZ_TILE / 2) + 1024;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(oz_mma2_kernel<KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    oz_mma2_kernel<KCH, NST><<<2 * ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB2, p, d_k, (const int *)d_tiles, S, kp8,
+                                                                  seg_pairs);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
                           cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
+    if (cfg & 8) {   // two-SM tiles: mapB is the half-B view
+        if (cfg & 1) return launch_2sm<1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
+        return launch_2sm<2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
+    }
     const OzAtomArgs none{};
     const bool persistent = (cfg & 2) != 0;
     switch (cfg & 1) {
@@ -805,7 +1160,8 @@ cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMa
 // {128, 32, 4, kch, 1}: the four arrays of 32 G rows.  d3 is outside d1, d2
 // in the box, so each K chunk lands in shared memory as contiguous
 // 128-byte rows (A: 2 x 128 rows, B: 4 x 32 rows).
-bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB)
+bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB,
+                         CUtensorMap *mapB2)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -828,6 +1184,12 @@ bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUt
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
     if (encode(mapB, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, boxB, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    // half of B (two of the four arrays) for the two-SM tiles
+    const cuuint32_t boxB2[5] = {OZ_CHUNK, OZ_BJ, 2, (cuuint32_t)kch, 1};
+    if (encode(mapB2, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, boxB2, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;

@@ -172,9 +172,10 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
  * pipeline shape of the H/O tiles (two 96 KB stages or four 48 KB stages),
  * bit 1 a persistent launch (one block per SM walking the tiles) of the H/O
  * tiles instead of one block per tile, bit 2 the same for the per-atom
- * products (h_a A, APW-lo rows).  Every configuration gives bit-identical
- * results. */
-#define EXS_OZ_NCONFIG 8
+ * products (h_a A, APW-lo rows), bit 3 two-SM H/O tiles (a pair of blocks
+ * computes 256 x 32 with the B operand split between them; bit 1 is then
+ * ignored).  Every configuration gives bit-identical results. */
+#define EXS_OZ_NCONFIG 16
 int exs_set_kernel_config(exs_ctx *ctx, int config);
 
 /* CUDA graph of one batched device setup (no counterpart in the reference):

@@ -70,13 +70,13 @@ def test_ozaki_configurations_bit_identical():
     st.set_precision("ozaki", 7)
     b = DeviceBatch(st, gks)
     outs = []
-    for cfg in range(8):
+    for cfg in range(16):
         st.set_kernel_config(cfg)
         b.clear()
         st.setup_batched_device(*b.args())
         st.synchronize()
         outs.append([b.result(k) for k in range(NK)])
-    for cfg in range(1, 8):
+    for cfg in range(1, 16):
         for k in range(NK):
             assert np.array_equal(outs[0][k][0], outs[cfg][k][0])
             assert np.array_equal(outs[0][k][1], outs[cfg][k][1])
@@ -84,7 +84,7 @@ def test_ozaki_configurations_bit_identical():
     assert rel_fro(outs[1][1][0], hr) <= TOL_FRO
     assert rel_fro(outs[1][1][1], orf) <= TOL_FRO
     with pytest.raises(Exception):
-        st.set_kernel_config(8)
+        st.set_kernel_config(16)
 
 
 @pytest.mark.parametrize("prec", ["fp64", "ozaki"])
@@ -95,7 +95,7 @@ def test_autotune_keeps_results_correct(prec):
     st.set_precision(prec, 7)
     b = DeviceBatch(st, gks)
     choice = st.autotune(*b.args())
-    assert choice in ((0,) if prec == "fp64" else tuple(range(8)))
+    assert choice in ((0,) if prec == "fp64" else tuple(range(16)))
     h, o = b.result(2)
     hr, orf = O.hamiltonandoverlapsetup(s, gks[2])
     assert rel_fro(h, hr) <= TOL_FRO and rel_fro(o, orf) <= TOL_FRO
