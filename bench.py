@@ -219,17 +219,23 @@ def run_reference(args):
     return 0
 
 
-def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier):
-    """Setups/s through exs_setup_batched: pinned host igpig/vgpc in, pinned host H/O out."""
+def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, mode="auto", pinned=True):
+    """Setups/s through exs_setup_batched: pinned host igpig/vgpc in, host H/O out
+    (pinned or pageable), H/O brought back in the given copy mode."""
     import ctypes
 
     import torch
     import torch.distributed as dist
     nk = len(ngp)
+    st.set_host_copy_mode(mode)
     h_ig = torch.from_numpy(np.ascontiguousarray(ig)).pin_memory()      # (nk, ngkmax) == Fortran (ngkmax, nk)
     h_vg = torch.from_numpy(np.ascontiguousarray(vg)).pin_memory()      # (nk, ngkmax, 3) == Fortran (3, ngkmax, nk)
-    h_out = [(torch.empty(2 * m * m, dtype=torch.float64).pin_memory(),
-              torch.empty(2 * m * m, dtype=torch.float64).pin_memory()) for m in nmat]
+    if pinned:
+        h_out = [(torch.empty(2 * m * m, dtype=torch.float64).pin_memory(),
+                  torch.empty(2 * m * m, dtype=torch.float64).pin_memory()) for m in nmat]
+    else:
+        h_out = [(torch.empty(2 * m * m, dtype=torch.float64), torch.empty(2 * m * m, dtype=torch.float64))
+                 for m in nmat]
     ngp_np = np.array(ngp, dtype=np.int32)
     hpp = (ctypes.c_void_p * nk)(*[a.data_ptr() for a, _ in h_out])
     opp = (ctypes.c_void_p * nk)(*[b.data_ptr() for _, b in h_out])
@@ -256,7 +262,9 @@ def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     value = ws * nk * args.steps / (float(t.item()) * 1e-3)
     h2d = ig.nbytes + vg.nbytes
-    d2h = sum(2 * 16 * m * m for m in nmat)
+    packed = mode == "packed" or (mode == "auto" and not pinned)
+    d2h = sum(2 * 16 * (m * (m + 1) // 2 if packed else m * m) for m in nmat)
+    st.set_host_copy_mode("auto")
     return value, h2d, d2h
 
 
@@ -377,10 +385,17 @@ def run_ours(args):
     gather_bytes = sum(32.0 * n * (n + 1) for n in ngp)
 
     # ---- end to end through the host-pointer entry point
+    e2e_modes = None
     if args.skip_e2e:
         e2e_value, h2d, d2h = None, 0, 0
     else:
         e2e_value, h2d, d2h = _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier)
+        e2e_modes = {
+            "pinned_direct": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "direct")[0],
+            "pinned_packed": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "packed")[0],
+            "pageable_direct": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "direct", False)[0],
+            "pageable_packed": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "packed", False)[0],
+        }
 
     # ---- split precision: its error against the native FP64 path (k-point 0)
     # and the FP64 path's own device-resident rate for comparison
@@ -460,7 +475,8 @@ def run_ours(args):
                        "l2": "working set > 126 MB L2 (A/B planes 63 MB and H/O 48 MB per k-point), no flush"},
             "e2e": None if e2e_value is None else {
                 "value": e2e_value, "unit": "setups/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "host_copy_mode": "auto (pinned outputs)",
+                "by_copy_mode": e2e_modes},
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
             "graph_replay": {"value": ws * nk * args.steps / (graph_ms * 1e-3), "unit": "setups/s",

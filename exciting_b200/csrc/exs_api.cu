@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "exs_internal.cuh"
@@ -166,6 +167,14 @@ int exs_ctx_destroy(exs_ctx *c)
     if (c->tables_free) cudaEventDestroy(c->tables_free);
     for (auto &e : c->ev_group)
         if (e) cudaEventDestroy(e);
+    for (int q = 0; q < 2; q++) {
+        if (c->ev_d2h[q]) cudaEventDestroy(c->ev_d2h[q]);
+        if (c->d_pack[q]) cudaFree(c->d_pack[q]);
+        if (c->h_pack[q]) cudaFreeHost(c->h_pack[q]);
+        if (c->d_packdesc[q]) cudaFree(c->d_packdesc[q]);
+        if (c->h_packdesc[q]) cudaFreeHost(c->h_packdesc[q]);
+    }
+    delete c->pool;
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -312,6 +321,8 @@ int exs_ctx_create(const exs_config *cfg, exs_ctx **out)
     }
     cudaEventCreateWithFlags(&c->ev_group[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->ev_group[1], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_d2h[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_d2h[1], cudaEventDisableTiming);
     for (auto &ev : c->ev) cudaEventCreate(&ev);
     cudaEventCreateWithFlags(&c->tables_free, cudaEventDisableTiming);
     cudaStream_t s = c->stream;
@@ -1168,6 +1179,107 @@ int exs_setup_batched_device(exs_ctx *c, int nk, const int *ngp, const int *igpi
     return run_setup(c, ks, false);
 }
 
+int exs_set_host_copy_mode(exs_ctx *c, int mode)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (mode < EXS_COPY_AUTO || mode > EXS_COPY_PACKED) return fail(c, EXS_ERR_ARG, "unknown host copy mode");
+    c->host_copy_mode = mode;
+    return EXS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One matrix of a packed transfer: the upper triangle (i <= j) of the
+// column-major n x n matrix src, column after column, at element offset off.
+struct PackDesc {
+    const exs_complex *src;
+    long n;
+    size_t off;
+};
+
+__global__ void pack_upper_kernel(const PackDesc *pd, exs_complex *out)
+{
+    const PackDesc d = pd[blockIdx.y];
+    for (long j = blockIdx.x; j < d.n; j += gridDim.x) {
+        exs_complex *o = out + d.off + (size_t)j * (j + 1) / 2;
+        const exs_complex *z = d.src + (size_t)d.n * j;
+        for (long i = threadIdx.x; i <= j; i += blockDim.x) o[i] = z[i];
+    }
+}
+
+// Full Hermitian z (n x n, column-major) from its packed upper triangle p,
+// columns [c0, c1): the upper part is a copy per column, the lower part
+// (rows r > c) the conjugate of p read row by row in 64-row blocks.
+void unpack_columns(const exs_complex *p, exs_complex *z, long n, long c0, long c1)
+{
+    for (long j = c0; j < c1; j++) std::memcpy(z + n * j, p + (size_t)j * (j + 1) / 2, sizeof(exs_complex) * (j + 1));
+    for (long r0 = c0 + 1; r0 < n; r0 += 64) {
+        const long r1 = std::min(n, r0 + 64);
+        for (long r = r0; r < r1; r++) {
+            const exs_complex *pr = p + (size_t)r * (r + 1) / 2;     // row r of the upper part: p[.. + c], c <= r
+            const long ce = std::min(c1, r);
+            for (long cc = c0; cc < ce; cc++) {
+                exs_complex v = pr[cc];
+                v.im = -v.im;
+                z[r + n * cc] = v;
+            }
+        }
+    }
+}
+
+bool host_pinned(const void *ptr)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Grow the two packed-transfer slots to hold `elems` elements and `ndesc`
+// descriptors each.
+int pack_reserve(exs_ctx *c, size_t elems, size_t ndesc)
+{
+    if (elems > c->pack_elems) {
+        for (int q = 0; q < 2; q++) {
+            if (c->d_pack[q]) cudaFree(c->d_pack[q]);
+            if (c->h_pack[q]) cudaFreeHost(c->h_pack[q]);
+            c->d_pack[q] = c->h_pack[q] = nullptr;
+        }
+        c->pack_elems = 0;
+        for (int q = 0; q < 2; q++) {
+            EXS_CUDA(cudaMalloc((void **)&c->d_pack[q], sizeof(exs_complex) * elems));
+            EXS_CUDA(cudaMallocHost((void **)&c->h_pack[q], sizeof(exs_complex) * elems));
+        }
+        c->pack_elems = elems;
+    }
+    if (ndesc > c->packdesc_cap) {
+        for (int q = 0; q < 2; q++) {
+            if (c->d_packdesc[q]) cudaFree(c->d_packdesc[q]);
+            if (c->h_packdesc[q]) cudaFreeHost(c->h_packdesc[q]);
+            c->d_packdesc[q] = c->h_packdesc[q] = nullptr;
+        }
+        c->packdesc_cap = 0;
+        for (int q = 0; q < 2; q++) {
+            EXS_CUDA(cudaMalloc(&c->d_packdesc[q], sizeof(PackDesc) * ndesc));
+            EXS_CUDA(cudaMallocHost(&c->h_packdesc[q], sizeof(PackDesc) * ndesc));
+        }
+        c->packdesc_cap = ndesc;
+    }
+    if (!c->pool) {
+        const unsigned hc = std::thread::hardware_concurrency();
+        c->pool = new exs::HostPool((int)std::max(1u, std::min(hc, 32u)) - 1);
+    }
+    return EXS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, const double *vgpc,
                       exs_complex *const *h, exs_complex *const *o)
 {
@@ -1183,6 +1295,11 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
         }
     }
     cudaSetDevice(c->device);
+    bool packed = c->host_copy_mode == EXS_COPY_PACKED;
+    if (c->host_copy_mode == EXS_COPY_AUTO) {
+        packed = false;
+        for (int k = 0; k < nk && !packed; k++) packed = !host_pinned(h[k]) || !host_pinned(o[k]);
+    }
     cudaStream_t s = c->stream;
     int worst = EXS_OK;
     for (int k0 = 0; k0 < nk; k0 += c->max_batch) {
@@ -1207,29 +1324,109 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
         // copy stream while group g+1 is set up on the compute stream.
         const int ngroups = nb >= 8 ? 4 : (nb >= 2 ? 2 : 1);
         const int per = (nb + ngroups - 1) / ngroups;
+        const int G = (nb + per - 1) / per;
         auto group = [&](int g) {
             const int a = g * per, e = std::min(nb, a + per);
             return std::vector<KDesc>(all.begin() + a, all.begin() + e);
         };
-        int rc = EXS_OK;
-        std::vector<KDesc> cur = group(0);
-        rc = run_setup(c, cur, false);
-        if (rc < 0) return rc;
-        for (int g = 0; g < ngroups && g * per < nb; g++) {
+        if (packed) {   // room for the largest group (2 matrices per k)
+            size_t need = 0;
+            for (int g = 0; g < G; g++) {
+                size_t el = 0;
+                for (const KDesc &k : group(g)) el += 2 * ((size_t)k.nmat * (k.nmat + 1) / 2);
+                need = std::max(need, el);
+            }
+            int rc = pack_reserve(c, need, 2 * (size_t)per);
+            if (rc < 0) return rc;
+        }
+        // enqueue group g: its setup, and for the packed transfer its pack
+        // kernel; then the event that the copy stream waits for
+        auto enqueue = [&](int g) -> int {
+            std::vector<KDesc> cur = group(g);
+            int rc = run_setup(c, cur, false);
+            if (rc < 0) return rc;
+            if (packed) {
+                PackDesc *pd = (PackDesc *)c->h_packdesc[g & 1];
+                size_t off = 0;
+                for (size_t q = 0; q < cur.size(); q++) {
+                    const size_t t = (size_t)cur[q].nmat * (cur[q].nmat + 1) / 2;
+                    pd[2 * q] = PackDesc{cur[q].h, cur[q].nmat, off};
+                    pd[2 * q + 1] = PackDesc{cur[q].o, cur[q].nmat, off + t};
+                    off += 2 * t;
+                }
+                EXS_CUDA(cudaMemcpyAsync(c->d_packdesc[g & 1], pd, sizeof(PackDesc) * 2 * cur.size(),
+                                         cudaMemcpyHostToDevice, s));
+                pack_upper_kernel<<<dim3(512, (unsigned)(2 * cur.size())), 256, 0, s>>>(
+                    (const PackDesc *)c->d_packdesc[g & 1], c->d_pack[g & 1]);
+                EXS_CUDA(cudaGetLastError());
+            }
             EXS_CUDA(cudaEventRecord(c->ev_group[g & 1], s));
-            if ((g + 1) * per < nb) {           // enqueue the next group before copying this one
-                std::vector<KDesc> nxt = group(g + 1);
-                rc = run_setup(c, nxt, false);
+            return EXS_OK;
+        };
+        // the device-to-host copies of group g on the copy stream
+        auto copy_out = [&](int g) -> int {
+            std::vector<KDesc> cur = group(g);
+            EXS_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_group[g & 1], 0));
+            if (packed) {
+                size_t el = 0;
+                for (const KDesc &k : cur) el += 2 * ((size_t)k.nmat * (k.nmat + 1) / 2);
+                EXS_CUDA(cudaMemcpyAsync(c->h_pack[g & 1], c->d_pack[g & 1], sizeof(exs_complex) * el,
+                                         cudaMemcpyDeviceToHost, c->copy_stream));
+            } else {
+                for (size_t q = 0; q < cur.size(); q++) {
+                    const int kk = k0 + g * per + (int)q;
+                    const size_t bytes = sizeof(exs_complex) * (size_t)cur[q].nmat * cur[q].nmat;
+                    EXS_CUDA(cudaMemcpyAsync(h[kk], cur[q].h, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+                    EXS_CUDA(cudaMemcpyAsync(o[kk], cur[q].o, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+                }
+            }
+            EXS_CUDA(cudaEventRecord(c->ev_d2h[g & 1], c->copy_stream));
+            return EXS_OK;
+        };
+        // the full matrices of group g rebuilt on the host threads
+        auto unpack = [&](int g) -> int {
+            EXS_CUDA(cudaEventSynchronize(c->ev_d2h[g & 1]));
+            std::vector<KDesc> cur = group(g);
+            struct Task {
+                const exs_complex *p;
+                exs_complex *z;
+                long n, c0, c1;
+            };
+            std::vector<Task> tasks;
+            size_t off = 0;
+            for (size_t q = 0; q < cur.size(); q++) {
+                const int kk = k0 + g * per + (int)q;
+                const long n = cur[q].nmat;
+                const size_t t = (size_t)n * (n + 1) / 2;
+                for (int w = 0; w < 2; w++) {
+                    const exs_complex *pm = c->h_pack[g & 1] + off + w * t;
+                    exs_complex *z = w == 0 ? h[kk] : o[kk];
+                    for (long c0 = 0; c0 < n; c0 += 64) tasks.push_back(Task{pm, z, n, c0, std::min(n, c0 + 64)});
+                }
+                off += 2 * t;
+            }
+            c->pool->parallel_for((int)tasks.size(), [&](int i) {
+                const Task &t = tasks[i];
+                unpack_columns(t.p, t.z, t.n, t.c0, t.c1);
+            });
+            return EXS_OK;
+        };
+        int rc = enqueue(0);
+        if (rc < 0) return rc;
+        rc = copy_out(0);
+        if (rc < 0) return rc;
+        for (int g = 0; g < G; g++) {
+            if (g + 1 < G) {   // the next group's setup goes ahead of this group's host work
+                rc = enqueue(g + 1);
                 if (rc < 0) return rc;
             }
-            EXS_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_group[g & 1], 0));
-            for (const KDesc &k : cur) {
-                const int kk = k0 + (int)(&k - &cur[0]) + g * per;
-                const size_t bytes = sizeof(exs_complex) * (size_t)k.nmat * k.nmat;
-                EXS_CUDA(cudaMemcpyAsync(h[kk], k.h, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
-                EXS_CUDA(cudaMemcpyAsync(o[kk], k.o, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+            if (packed) {
+                // slot (g+1)&1 was last unpacked in iteration g-1: its copy may start now
+                if (g + 1 < G && (rc = copy_out(g + 1)) < 0) return rc;
+                if ((rc = unpack(g)) < 0) return rc;
+            } else if (g + 1 < G && (rc = copy_out(g + 1)) < 0) {
+                return rc;
             }
-            if ((g + 1) * per < nb) cur = group(g + 1);
         }
         EXS_CUDA(cudaStreamSynchronize(c->copy_stream));
         rc = exs_synchronize(c);

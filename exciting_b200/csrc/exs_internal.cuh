@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/exciting_b200.h"
+#include "host_pool.h"
 #include "special.cuh"
 
 namespace exs {
@@ -182,6 +183,14 @@ struct exs_ctx {
     // pinned staging for host-facing calls
     int *h_igpig_pinned = nullptr;
     double *h_vgpc_pinned = nullptr;
+    // host-pointer batched path: packed upper triangles, two group slots
+    int host_copy_mode = EXS_COPY_AUTO;
+    exs_complex *d_pack[2] = {nullptr, nullptr}, *h_pack[2] = {nullptr, nullptr};
+    size_t pack_elems = 0;               // capacity of each slot
+    void *h_packdesc[2] = {nullptr, nullptr}, *d_packdesc[2] = {nullptr, nullptr};
+    size_t packdesc_cap = 0;             // descriptors per slot
+    cudaEvent_t ev_d2h[2] = {};
+    exs::HostPool *pool = nullptr;
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)

@@ -245,6 +245,12 @@ class Setup:
         self._check(self.lib.exs_graph_create(*args, ctypes.byref(g)))
         return SetupGraph(self, g)
 
+    COPY_MODES = {"auto": 0, "direct": 1, "packed": 2}
+
+    def set_host_copy_mode(self, mode: str):
+        """How the host-pointer calls bring H and O back: "auto", "direct" or "packed"."""
+        return self._check(self.lib.exs_set_host_copy_mode(self.ctx, self.COPY_MODES[mode]))
+
     def set_stream(self, stream_ptr: int | None):
         """Run on a caller-owned cudaStream_t (its integer handle); None = own stream."""
         return self._check(self.lib.exs_set_stream(self.ctx, None if not stream_ptr else ctypes.c_void_p(stream_ptr)))

@@ -132,6 +132,20 @@ int exs_setup_batched_device(exs_ctx *ctx, int nk, const int *ngp_host,
                              exs_complex *const *h_dev, exs_complex *const *o_dev);
 int exs_synchronize(exs_ctx *ctx);
 
+/* How exs_setup_batched / exs_hamiltonandoverlapsetup bring H and O to the
+ * host (no counterpart in the reference; results are identical):
+ *   EXS_COPY_DIRECT  full matrices copied into the caller's arrays (fast
+ *                    when those are pinned, e.g. cudaHostRegister'ed);
+ *   EXS_COPY_PACKED  upper triangles packed on the device, half the bytes
+ *                    over PCIe into pinned staging, full matrices rebuilt on
+ *                    host threads (any caller memory);
+ *   EXS_COPY_AUTO    DIRECT when every output array is pinned, else PACKED
+ *                    (default). */
+#define EXS_COPY_AUTO 0
+#define EXS_COPY_DIRECT 1
+#define EXS_COPY_PACKED 2
+int exs_set_host_copy_mode(exs_ctx *ctx, int mode);
+
 /* The interstitial blocks alone: replaces
  *   call hmlistln(hamilton, ngp, igpig, vgpc)  (src/src_eigensystem/hmlistln.f90:13)
  *   call olpistln(overlap, ngp, igpig, vgpc)   (src/src_eigensystem/olpistln.f90:13)

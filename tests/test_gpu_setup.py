@@ -141,3 +141,29 @@ def test_singular_matching_system_warns_and_keeps_rhs():
     ar, nsing = O.match(s, gk, ngkmax=st.ngkmax)
     assert nsing > 0 and rc == 1
     assert np.abs(a[: gk.ngp] - ar[: gk.ngp]).max() <= 1e-12 * np.abs(ar).max()
+
+
+def test_host_copy_modes_identical():
+    """Direct and packed transfers of H/O (pinned and pageable outputs) give the same bits."""
+    import torch
+    s = W.si_cube8()
+    gks = s.gksets()[:9]
+    st = _setup(s, max_batch=9)
+    outs = {}
+    for mode in ("direct", "packed", "auto"):
+        st.set_host_copy_mode(mode)
+        outs[mode] = st.setup_batched(gks)
+    for k in range(9):
+        for w in range(2):
+            assert np.array_equal(outs["direct"][k][w], outs["packed"][k][w])
+            assert np.array_equal(outs["direct"][k][w], outs["auto"][k][w])
+    hr, orf = O.hamiltonandoverlapsetup(s, gks[4])
+    _check_pair(outs["packed"][4][0], outs["packed"][4][1], hr, orf, eig=False)
+    # pinned outputs through the packed path
+    nmat = [g.ngp + st.nlotot for g in gks]
+    pin = [(torch.empty((m, m), dtype=torch.complex128).pin_memory(),
+            torch.empty((m, m), dtype=torch.complex128).pin_memory()) for m in nmat]
+    st.set_host_copy_mode("packed")
+    got = st.setup_batched(gks, out=[(a.numpy().T, b.numpy().T) for a, b in pin])
+    for k in range(9):
+        assert np.array_equal(got[k][0], outs["direct"][k][0])
