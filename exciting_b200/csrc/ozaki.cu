@@ -252,25 +252,34 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
     if (g >= p.npad || f >= kp8) return;
     // 1/sigma is a power of two: the scaling is exact
     const double rs = 1.0 / oz_sigma(k.oz_scale[(a0 == 0 ? p.npad : 0) + g]);
-    double x[2][8];
+    // The slices are the base-128 digits of |x| 2^(7S) truncated, with the
+    // sign of x: the same digits as S steps of (x *= 128, q = trunc(x),
+    // x -= q) in exact FP64, taken from one integer (7S <= 63 bits).
+    const double two7s = ldexp(1.0, 7 * S);
+    unsigned long long mag[2][8];
+    uint32_t neg[2] = {0, 0};
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-        x[0][e] = t[0][fl + e][gl] * rs;
-        x[1][e] = t[1][fl + e][gl] * rs;
-    }
-    for (int s = 0; s < S; s++)
+    for (int e = 0; e < 8; e++)
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            const long long X = (long long)(t[a][fl + e][gl] * rs * two7s);   // |.| < 2^63, truncated
+            neg[a] |= (X < 0 ? 1u : 0u) << e;
+            mag[a][e] = (unsigned long long)(X < 0 ? -X : X);
+        }
+    for (int s = 0; s < S; s++) {
+        const int sh = 7 * (S - 1 - s);
 #pragma unroll
         for (int a = 0; a < 2; a++) {
             uint32_t w[2] = {0, 0};
 #pragma unroll
             for (int e = 0; e < 8; e++) {
-                x[a][e] *= 128.0;
-                const double tq = trunc(x[a][e]);
-                x[a][e] -= tq;
-                w[e >> 2] |= ((uint32_t)(uint8_t)(int8_t)tq) << (8 * (e & 3));
+                int q = (int)((mag[a][e] >> sh) & 127u);
+                if ((neg[a] >> e) & 1u) q = -q;
+                w[e >> 2] |= ((uint32_t)(uint8_t)(int8_t)q) << (8 * (e & 3));
             }
             *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(s, a0 + a, g, f, p.npad, kp8)) = make_uint2(w[0], w[1]);
         }
+    }
 }
 
 // ------------------------------------------------------------ per-atom operands
