@@ -48,6 +48,8 @@ SIGNATURES = {
     "exs_setup_batched_device": ([P, c_int, P, P, P, P, P], c_int),
     "exs_synchronize": ([P], c_int),
     "exs_set_host_copy_mode": ([P, c_int], c_int),
+    "exs_solve_batched_device": ([P, c_int, P, P, P, c_int, P, P, c_int], c_int),
+    "exs_setup_and_solve_batched": ([P, c_int, P, P, P, c_int, P, P, c_int], c_int),
     "exs_autotune": ([P, c_int, P, P, P, P, P, P], c_int),
     "exs_hmlistln": ([P, c_int, P, P, P, c_int], c_int),
     "exs_olpistln": ([P, c_int, P, P, P, c_int], c_int),

@@ -175,6 +175,9 @@ int exs_ctx_destroy(exs_ctx *c)
         if (c->h_packdesc[q]) cudaFreeHost(c->h_packdesc[q]);
     }
     delete c->pool;
+    exs::solver_release(c);
+    if (c->d_eval) cudaFree(c->d_eval);
+    if (c->d_evec) cudaFree(c->d_evec);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -1432,6 +1435,78 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
         rc = exs_synchronize(c);
         if (rc < 0) return rc;
         if (rc > worst) worst = rc;
+    }
+    return worst;
+}
+
+int exs_setup_and_solve_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, const double *vgpc, int nstfv,
+                                double *evalfv, exs_complex *evecfv, int ldv)
+{
+    if (!c || nk < 0 || nstfv <= 0 || (nk > 0 && (!ngp || !igpig || !vgpc || !evalfv || !evecfv)))
+        return fail(c, EXS_ERR_ARG, "exs_setup_and_solve_batched: bad argument");
+    if (!c->have_inputs) return fail(c, EXS_ERR_STATE, "exs_set_scf_inputs has not been called");
+    for (int k = 0; k < nk; k++) {
+        if (ngp[k] <= 0 || ngp[k] > c->ngkmax) return fail(c, EXS_ERR_SIZE, "ngp outside 1..ngkmax");
+        if (ldv < ngp[k] + c->nlotot || nstfv > ngp[k] + c->nlotot)
+            return fail(c, EXS_ERR_SIZE, "ldv < nmat or nstfv > nmat");
+        for (int i = 0; i < ngp[k]; i++) {
+            const int g = igpig[(size_t)c->ngkmax * k + i];
+            if (g < 1 || g > c->ngrtot) return fail(c, EXS_ERR_INDEX, "igpig entry outside 1..ngrtot");
+        }
+    }
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    const size_t nev = (size_t)nstfv * c->max_batch, nvec = (size_t)ldv * nstfv * c->max_batch;
+    if (nev > c->eval_cap) {
+        if (c->d_eval) cudaFree(c->d_eval);
+        c->d_eval = nullptr;
+        c->eval_cap = 0;
+        EXS_CUDA(cudaMalloc((void **)&c->d_eval, sizeof(double) * nev));
+        c->eval_cap = nev;
+    }
+    if (nvec > c->evec_cap) {
+        if (c->d_evec) cudaFree(c->d_evec);
+        c->d_evec = nullptr;
+        c->evec_cap = 0;
+        EXS_CUDA(cudaMalloc((void **)&c->d_evec, sizeof(exs_complex) * nvec));
+        c->evec_cap = nvec;
+    }
+    int worst = EXS_OK;
+    for (int k0 = 0; k0 < nk; k0 += c->max_batch) {
+        const int nb = std::min(c->max_batch, nk - k0);
+        EXS_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(c->h_igpig_pinned, igpig + (size_t)c->ngkmax * k0, sizeof(int) * (size_t)c->ngkmax * nb);
+        std::memcpy(c->h_vgpc_pinned, vgpc + 3 * (size_t)c->ngkmax * k0, sizeof(double) * 3 * (size_t)c->ngkmax * nb);
+        EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+        EXS_CUDA(cudaMemcpyAsync(c->d_igpig, c->h_igpig_pinned, sizeof(int) * (size_t)c->ngkmax * nb,
+                                 cudaMemcpyHostToDevice, s));
+        EXS_CUDA(cudaMemcpyAsync(c->d_vgpc, c->h_vgpc_pinned, sizeof(double) * 3 * (size_t)c->ngkmax * nb,
+                                 cudaMemcpyHostToDevice, s));
+        std::vector<KDesc> ks;
+        std::vector<int> nmat(nb);
+        std::vector<exs_complex *> hp(nb), op(nb), vp(nb);
+        for (int k = 0; k < nb; k++) {
+            exs_complex *dh = c->d_ho + (size_t)2 * k * c->nmatmax * c->nmatmax;
+            exs_complex *dob = dh + (size_t)c->nmatmax * c->nmatmax;
+            ks.push_back(slot_desc(c, k, ngp[k0 + k], c->d_igpig + (size_t)c->ngkmax * k,
+                                   c->d_vgpc + 3 * (size_t)c->ngkmax * k, dh, dob));
+            nmat[k] = ks.back().nmat;
+            hp[k] = dh;
+            op[k] = dob;
+            vp[k] = c->d_evec + (size_t)ldv * nstfv * k;
+        }
+        int rc = run_setup(c, ks, false);
+        if (rc < 0) return rc;
+        rc = exs_synchronize(c);
+        if (rc < 0) return rc;
+        if (rc > worst) worst = rc;
+        rc = exs_solve_batched_device(c, nb, nmat.data(), hp.data(), op.data(), nstfv, c->d_eval, vp.data(), ldv);
+        if (rc < 0) return rc;
+        EXS_CUDA(cudaMemcpyAsync(evalfv + (size_t)nstfv * k0, c->d_eval, sizeof(double) * nstfv * nb,
+                                 cudaMemcpyDeviceToHost, s));
+        EXS_CUDA(cudaMemcpyAsync(evecfv + (size_t)ldv * nstfv * k0, c->d_evec, sizeof(exs_complex) * ldv * nstfv * nb,
+                                 cudaMemcpyDeviceToHost, s));
+        EXS_CUDA(cudaStreamSynchronize(s));
     }
     return worst;
 }

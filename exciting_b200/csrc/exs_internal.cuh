@@ -191,6 +191,16 @@ struct exs_ctx {
     size_t packdesc_cap = 0;             // descriptors per slot
     cudaEvent_t ev_d2h[2] = {};
     exs::HostPool *pool = nullptr;
+    // device eigen-solve (cuSOLVER handle and work space, grown on demand)
+    void *solver = nullptr;
+    void *d_solve_work = nullptr;
+    size_t solve_lwork = 0;
+    double *d_solve_w = nullptr;
+    size_t solve_n = 0;
+    int *d_solve_info = nullptr;
+    double *d_eval = nullptr;            // eigenpairs of the host-pointer solve call
+    exs_complex *d_evec = nullptr;
+    size_t eval_cap = 0, evec_cap = 0;
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
@@ -247,6 +257,8 @@ cudaError_t launch_olp_apwlo(const DevParams &p, const KDesc *d_k, int nk, int n
 void build_gemm_tables(const exs_ctx *c, const std::vector<KDesc> &ks, GemmTables &t);
 cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, const void *d_work, int nwork,
                              const KDesc *d_k, cudaStream_t s);
+// Device eigen-solve (solve.cu)
+void solver_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)

@@ -180,6 +180,24 @@ class Setup:
         self._check(self.lib.exs_setup_batched(self.ctx, nk, _ptr(ngp), _ptr(ig), _ptr(vg), hp, op))
         return out
 
+    def setup_and_solve(self, gks, nstfv):
+        """Lowest nstfv eigenpairs of H x = e O x for every k-point in gks (H, O stay on the device).
+
+        Returns (evalfv (nstfv, nk), evecfv (ldv, nstfv, nk)), ldv = nmatmax, Fortran order."""
+        nk = len(gks)
+        ngp = np.array([g.ngp for g in gks], dtype=np.int32)
+        ig = np.zeros((self.ngkmax, nk), dtype=np.int32, order="F")
+        vg = np.zeros((3, self.ngkmax, nk), order="F")
+        for k, g in enumerate(gks):
+            ig[: g.ngp, k] = g.igpig
+            vg[:, : g.ngp, k] = g.vgpc
+        ldv = self.ngkmax + self.nlotot
+        ev = np.zeros((nstfv, nk), order="F")
+        vec = np.zeros((ldv, nstfv, nk), dtype=np.complex128, order="F")
+        self._check(self.lib.exs_setup_and_solve_batched(self.ctx, nk, _ptr(ngp), _ptr(ig), _ptr(vg), int(nstfv),
+                                                         _ptr(ev), _ptr(vec), ldv))
+        return ev, vec
+
     def setup_batched_device(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs):
         """Device-resident batched setup: pointers are device addresses (ints)."""
         nk = len(ngp)

@@ -169,6 +169,26 @@ int exs_interstitial_batched_device(exs_ctx *ctx, int which, int nk, const int *
                                     exs_complex *const *h_dev, exs_complex *const *o_dev,
                                     const int *ld_host);
 
+/* The consumer of the setup on the device: replaces
+ *   call solvewithlapack(system, nstfv, evecfv, evalfv)
+ *   (src/src_eigensystem/modfvsystem.f90:585-720, LAPACK zhegvx for the
+ *   eigenvalues IL = 1 .. IU = nstfv of H x = e O x and their vectors)
+ * by cuSOLVER zhegvdx with the same index range on the upper triangles.
+ * Device form: h_dev[k], o_dev[k] (nmat_k x nmat_k, destroyed),
+ * evalfv_dev(nstfv, nk), evecfv_dev[k] (ldv, nstfv).  Synchronous.
+ * EXS_ERR_ARG if O is not positive definite or the solver does not
+ * converge. */
+int exs_solve_batched_device(exs_ctx *ctx, int nk, const int *nmat_host, exs_complex *const *h_dev,
+                             exs_complex *const *o_dev, int nstfv, double *evalfv_dev,
+                             exs_complex *const *evecfv_dev, int ldv);
+/* Setup and solve for host callers: H and O stay on the device, only the
+ * eigenpairs come back.  Arguments as exs_setup_batched; evalfv(nstfv, nk),
+ * evecfv(ldv, nstfv, nk) host arrays (the reference's evecfv(nmatmax, nstfv)
+ * per k-point with ldv = nmatmax).  Synchronous. */
+int exs_setup_and_solve_batched(exs_ctx *ctx, int nk, const int *ngp, const int *igpig,
+                                const double *vgpc, int nstfv, double *evalfv, exs_complex *evecfv,
+                                int ldv);
+
 /* Autotuner (no counterpart in the reference): runs the batch described as
  * for exs_setup_batched_device once per kernel configuration of the active
  * precision mode (for the split-precision contraction: K chunks per
