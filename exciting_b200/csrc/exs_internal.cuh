@@ -191,13 +191,8 @@ struct exs_ctx {
     size_t packdesc_cap = 0;             // descriptors per slot
     cudaEvent_t ev_d2h[2] = {};
     exs::HostPool *pool = nullptr;
-    // device eigen-solve (cuSOLVER handle and work space, grown on demand)
+    // device eigen-solve: solver lanes (cuSOLVER handles, streams, work space)
     void *solver = nullptr;
-    void *d_solve_work = nullptr;
-    size_t solve_lwork = 0;
-    double *d_solve_w = nullptr;
-    size_t solve_n = 0;
-    int *d_solve_info = nullptr;
     double *d_eval = nullptr;            // eigenpairs of the host-pointer solve call
     exs_complex *d_evec = nullptr;
     size_t eval_cap = 0, evec_cap = 0;

@@ -51,6 +51,9 @@ __device__ inline void match_point(const DevParams &p, int ias, double gpc, doub
     const double fpso = 12.566370614359172954 / sqrt(p.omega);
     double sn, cs;
     sincos(theta, &sn, &cs);
+    // e^{i m phi}, m = 1..lmax_out, once per point (the same values for every l)
+    double cmt[EXS_LMAX_APW + 1], smt[EXS_LMAX_APW + 1];
+    for (int mm = 1; mm <= lmax_out; mm++) sincos((double)mm * phi, &smt[mm], &cmt[mm]);
     double xm[EXS_LMAX_APW + 1];
     for (int l = 0; l <= lmax_out; l++) {
         const int n = apw[l];
@@ -72,9 +75,7 @@ __device__ inline void match_point(const DevParams &p, int ias, double gpc, doub
             if (mm == 0) {
                 yr = xm[0]; yi = 0.0;
             } else {
-                double s, c;
-                sincos((double)mm * phi, &s, &c);
-                yr = xm[mm] * c; yi = xm[mm] * s;
+                yr = xm[mm] * cmt[mm]; yi = xm[mm] * smt[mm];
                 if (m < 0) { yi = -yi; if (mm & 1) { yr = -yr; yi = -yi; } }
             }
             // b_io = djl(l, io) * zt2 * conj(Y_lm)

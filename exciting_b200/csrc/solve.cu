@@ -8,6 +8,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "exs_internal.cuh"
 
@@ -19,63 +21,104 @@ int sfail(exs_ctx *c, int code, const char *msg)
     return code;
 }
 
-// Work space for one solve of order n (grown on demand, kept in the context).
-int solve_reserve(exs_ctx *c, int n, int nstfv, const exs_complex *a, const exs_complex *b)
+// One solver lane: a cuSOLVER handle on its own stream with its work space.
+// Solves of different k-points run on different lanes at the same time (a
+// single dense solve of order ~1000 leaves most of the GPU idle).
+struct SolveLane {
+    cusolverDnHandle_t h = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t done = nullptr;
+    void *work = nullptr;
+    size_t lwork = 0;
+    double *w = nullptr;
+    size_t wn = 0;
+    int *info = nullptr;
+};
+
+struct SolverState {
+    std::vector<SolveLane> lanes;
+};
+
+constexpr int SOLVE_LANES = 8;
+
+int lanes_reserve(exs_ctx *c, int nl)
 {
-    if (!c->solver) {
-        cusolverDnHandle_t h = nullptr;
-        if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return sfail(c, EXS_ERR_CUDA, "cusolverDnCreate failed");
-        c->solver = h;
+    SolverState *st = (SolverState *)c->solver;
+    if (!st) {
+        st = new SolverState;
+        c->solver = st;
     }
-    cusolverDnHandle_t h = (cusolverDnHandle_t)c->solver;
-    if (cusolverDnSetStream(h, c->stream) != CUSOLVER_STATUS_SUCCESS)
-        return sfail(c, EXS_ERR_CUDA, "cusolverDnSetStream failed");
-    int lwork = 0, meig = 0;
-    if (cusolverDnZhegvdx_bufferSize(h, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
-                                     CUBLAS_FILL_MODE_UPPER, n, (const cuDoubleComplex *)a, n,
-                                     (const cuDoubleComplex *)b, n, 0.0, 0.0, 1, nstfv, &meig, nullptr,
-                                     &lwork) != CUSOLVER_STATUS_SUCCESS)
-        return sfail(c, EXS_ERR_CUDA, "cusolverDnZhegvdx_bufferSize failed");
-    if ((size_t)lwork > c->solve_lwork) {
-        if (c->d_solve_work) cudaFree(c->d_solve_work);
-        c->d_solve_work = nullptr;
-        c->solve_lwork = 0;
-        if (cudaMalloc(&c->d_solve_work, sizeof(cuDoubleComplex) * (size_t)lwork) != cudaSuccess)
-            return sfail(c, EXS_ERR_NOMEM, "solver work space");
-        c->solve_lwork = (size_t)lwork;
+    while ((int)st->lanes.size() < nl) {
+        SolveLane l;
+        if (cusolverDnCreate(&l.h) != CUSOLVER_STATUS_SUCCESS) return sfail(c, EXS_ERR_CUDA, "cusolverDnCreate failed");
+        if (cudaStreamCreateWithFlags(&l.s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMalloc((void **)&l.info, sizeof(int)) != cudaSuccess) {
+            cusolverDnDestroy(l.h);
+            return sfail(c, EXS_ERR_CUDA, "solver lane");
+        }
+        if (cusolverDnSetStream(l.h, l.s) != CUSOLVER_STATUS_SUCCESS)
+            return sfail(c, EXS_ERR_CUDA, "cusolverDnSetStream failed");
+        st->lanes.push_back(l);
     }
-    if ((size_t)n > c->solve_n) {
-        if (c->d_solve_w) cudaFree(c->d_solve_w);
-        c->d_solve_w = nullptr;
-        c->solve_n = 0;
-        if (cudaMalloc((void **)&c->d_solve_w, sizeof(double) * (size_t)n) != cudaSuccess)
-            return sfail(c, EXS_ERR_NOMEM, "solver eigenvalue space");
-        c->solve_n = (size_t)n;
+    if (!c->pool) {
+        const unsigned hc = std::thread::hardware_concurrency();
+        c->pool = new exs::HostPool((int)std::max(1u, std::min(hc, 32u)) - 1);
     }
-    if (!c->d_solve_info && cudaMalloc((void **)&c->d_solve_info, sizeof(int)) != cudaSuccess)
-        return sfail(c, EXS_ERR_NOMEM, "solver info");
     return EXS_OK;
 }
 
-// Solve one problem in place: on return the first nstfv columns of a hold
-// the eigenvectors (leading dimension n), d_solve_w[0 .. nstfv) the values.
-int solve_one(exs_ctx *c, int n, exs_complex *a, exs_complex *b, int nstfv)
+// Work space of a lane for one solve of order n (grown on demand).  Returns
+// EXS_OK or an error code; no context state is written (lanes run on
+// several host threads).
+int lane_reserve(SolveLane &l, int n, int nstfv, const exs_complex *a, const exs_complex *b)
 {
-    int rc = solve_reserve(c, n, nstfv, a, b);
+    int lwork = 0, meig = 0;
+    if (cusolverDnZhegvdx_bufferSize(l.h, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                                     CUBLAS_FILL_MODE_UPPER, n, (const cuDoubleComplex *)a, n,
+                                     (const cuDoubleComplex *)b, n, 0.0, 0.0, 1, nstfv, &meig, nullptr,
+                                     &lwork) != CUSOLVER_STATUS_SUCCESS)
+        return EXS_ERR_CUDA;
+    if ((size_t)lwork > l.lwork) {
+        if (l.work) cudaFree(l.work);
+        l.work = nullptr;
+        l.lwork = 0;
+        if (cudaMalloc(&l.work, sizeof(cuDoubleComplex) * (size_t)lwork) != cudaSuccess) return EXS_ERR_NOMEM;
+        l.lwork = (size_t)lwork;
+    }
+    if ((size_t)n > l.wn) {
+        if (l.w) cudaFree(l.w);
+        l.w = nullptr;
+        l.wn = 0;
+        if (cudaMalloc((void **)&l.w, sizeof(double) * (size_t)n) != cudaSuccess) return EXS_ERR_NOMEM;
+        l.wn = (size_t)n;
+    }
+    return EXS_OK;
+}
+
+// Solve one problem in place on a lane: the first nstfv columns of a become
+// the eigenvectors (leading dimension n), l.w[0 .. nstfv) the values; then
+// copy them to the caller's arrays on the lane's stream.
+int lane_solve(SolveLane &l, int n, exs_complex *a, exs_complex *b, int nstfv, double *eval, exs_complex *evec,
+               int ldv)
+{
+    int rc = lane_reserve(l, n, nstfv, a, b);
     if (rc != EXS_OK) return rc;
-    cusolverDnHandle_t h = (cusolverDnHandle_t)c->solver;
     int meig = 0;
-    const cusolverStatus_t st = cusolverDnZhegvdx(
-        h, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, n,
-        (cuDoubleComplex *)a, n, (cuDoubleComplex *)b, n, 0.0, 0.0, 1, nstfv, &meig, c->d_solve_w,
-        (cuDoubleComplex *)c->d_solve_work, (int)c->solve_lwork, c->d_solve_info);
-    if (st != CUSOLVER_STATUS_SUCCESS) return sfail(c, EXS_ERR_CUDA, "cusolverDnZhegvdx failed");
+    if (cusolverDnZhegvdx(l.h, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                          CUBLAS_FILL_MODE_UPPER, n, (cuDoubleComplex *)a, n, (cuDoubleComplex *)b, n, 0.0, 0.0, 1,
+                          nstfv, &meig, l.w, (cuDoubleComplex *)l.work, (int)l.lwork,
+                          l.info) != CUSOLVER_STATUS_SUCCESS)
+        return EXS_ERR_CUDA;
     int info = 0;
-    if (cudaMemcpyAsync(&info, c->d_solve_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
-        cudaStreamSynchronize(c->stream) != cudaSuccess)
-        return sfail(c, EXS_ERR_CUDA, "solver status read");
-    if (info != 0 || meig < nstfv)
-        return sfail(c, EXS_ERR_ARG, "zhegvdx did not converge or O is not positive definite");
+    if (cudaMemcpyAsync(&info, l.info, sizeof(int), cudaMemcpyDeviceToHost, l.s) != cudaSuccess ||
+        cudaStreamSynchronize(l.s) != cudaSuccess)
+        return EXS_ERR_CUDA;
+    if (info != 0 || meig < nstfv) return EXS_ERR_ARG;
+    if (cudaMemcpyAsync(eval, l.w, sizeof(double) * nstfv, cudaMemcpyDeviceToDevice, l.s) != cudaSuccess ||
+        cudaMemcpy2DAsync(evec, sizeof(exs_complex) * ldv, a, sizeof(exs_complex) * n, sizeof(exs_complex) * n,
+                          nstfv, cudaMemcpyDeviceToDevice, l.s) != cudaSuccess)
+        return EXS_ERR_CUDA;
     return EXS_OK;
 }
 
@@ -85,14 +128,18 @@ namespace exs {
 
 void solver_release(exs_ctx *c)
 {
-    if (c->solver) cusolverDnDestroy((cusolverDnHandle_t)c->solver);
-    if (c->d_solve_work) cudaFree(c->d_solve_work);
-    if (c->d_solve_w) cudaFree(c->d_solve_w);
-    if (c->d_solve_info) cudaFree(c->d_solve_info);
+    SolverState *st = (SolverState *)c->solver;
+    if (!st) return;
+    for (SolveLane &l : st->lanes) {
+        if (l.h) cusolverDnDestroy(l.h);
+        if (l.s) cudaStreamDestroy(l.s);
+        if (l.done) cudaEventDestroy(l.done);
+        if (l.work) cudaFree(l.work);
+        if (l.w) cudaFree(l.w);
+        if (l.info) cudaFree(l.info);
+    }
+    delete st;
     c->solver = nullptr;
-    c->d_solve_work = nullptr;
-    c->d_solve_w = nullptr;
-    c->d_solve_info = nullptr;
 }
 
 }  // namespace exs
@@ -105,18 +152,38 @@ int exs_solve_batched_device(exs_ctx *c, int nk, const int *nmat, exs_complex *c
 {
     if (!c || nk < 0 || (nk > 0 && (!nmat || !h_dev || !o_dev || !evalfv_dev || !evecfv_dev)) || nstfv <= 0)
         return sfail(c, EXS_ERR_ARG, "exs_solve_batched_device: bad argument");
-    cudaSetDevice(c->device);
-    for (int k = 0; k < nk; k++) {
-        const int n = nmat[k];
-        if (n <= 0 || nstfv > n || ldv < n || !h_dev[k] || !o_dev[k] || !evecfv_dev[k])
+    for (int k = 0; k < nk; k++)
+        if (nmat[k] <= 0 || nstfv > nmat[k] || ldv < nmat[k] || !h_dev[k] || !o_dev[k] || !evecfv_dev[k])
             return sfail(c, EXS_ERR_SIZE, "nmat, nstfv or ldv out of range");
-        int rc = solve_one(c, n, h_dev[k], o_dev[k], nstfv);
-        if (rc != EXS_OK) return rc;
-        if (cudaMemcpyAsync(evalfv_dev + (size_t)nstfv * k, c->d_solve_w, sizeof(double) * nstfv,
-                            cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess ||
-            cudaMemcpy2DAsync(evecfv_dev[k], sizeof(exs_complex) * ldv, h_dev[k], sizeof(exs_complex) * n,
-                              sizeof(exs_complex) * n, nstfv, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
-            return sfail(c, EXS_ERR_CUDA, "eigenpair copy");
+    if (nk == 0) return EXS_OK;
+    cudaSetDevice(c->device);
+    const int nl = std::min(nk, SOLVE_LANES);
+    int rc = lanes_reserve(c, nl);
+    if (rc != EXS_OK) return rc;
+    SolverState *st = (SolverState *)c->solver;
+    // the lanes start after the work already queued on the context's stream
+    if (cudaEventRecord(c->ev[7], c->stream) != cudaSuccess) return sfail(c, EXS_ERR_CUDA, "event record");
+    for (int l = 0; l < nl; l++)
+        if (cudaStreamWaitEvent(st->lanes[l].s, c->ev[7], 0) != cudaSuccess)
+            return sfail(c, EXS_ERR_CUDA, "stream wait");
+    std::vector<int> lrc(nl, EXS_OK);
+    c->pool->parallel_for(nl, [&](int l) {
+        cudaSetDevice(c->device);
+        SolveLane &ln = st->lanes[l];
+        for (int k = l; k < nk && lrc[l] == EXS_OK; k += nl)
+            lrc[l] = lane_solve(ln, nmat[k], h_dev[k], o_dev[k], nstfv, evalfv_dev + (size_t)nstfv * k,
+                                evecfv_dev[k], ldv);
+        if (cudaEventRecord(ln.done, ln.s) != cudaSuccess && lrc[l] == EXS_OK) lrc[l] = EXS_ERR_CUDA;
+    });
+    for (int l = 0; l < nl; l++) {   // the context's stream continues after every lane
+        if (lrc[l] == EXS_OK && cudaStreamWaitEvent(c->stream, st->lanes[l].done, 0) != cudaSuccess)
+            lrc[l] = EXS_ERR_CUDA;
+    }
+    for (int l = 0; l < nl; l++) cudaStreamSynchronize(st->lanes[l].s);
+    for (int l = 0; l < nl; l++) {
+        if (lrc[l] == EXS_ERR_ARG) return sfail(c, EXS_ERR_ARG, "zhegvdx did not converge or O is not positive definite");
+        if (lrc[l] == EXS_ERR_NOMEM) return sfail(c, EXS_ERR_NOMEM, "solver work space");
+        if (lrc[l] != EXS_OK) return sfail(c, EXS_ERR_CUDA, "cuSOLVER call failed");
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return sfail(c, EXS_ERR_CUDA, "synchronize");
     return EXS_OK;
