@@ -151,6 +151,34 @@ def ozaki_int8_ops(sys_, gks, slices):
     return tiles * pairs * 2.0 * 128 * 128 * 2 * kp8
 
 
+# DRAM bytes per k-point of the dominant kernel from one ncu capture of a
+# small case (traffic grows with the k-points: the operands are read once per
+# k-point and H/O written once), scaled to a launch by the k-points it covers:
+#   split precision: oz_mma_kernel<OZ_HO,2,2>, 2 k-points: 131.6 MB read +
+#     35.2 MB written (profiles/oz_mma_si_cube8_nk2.md);
+#   FP64: zgemm_dmma_kernel<1> + <2>, 6 k-points: 673.5 MB read + 143.1 MB
+#     written (profiles/zgemm_dmma_si_cube8_nk6.md).
+PROFILED_DRAM_BYTES_PER_K = {"ozaki": (131.6e6 + 35.2e6) / 2, "fp64": (673.5e6 + 143.1e6) / 6}
+
+
+def main_bytes(sys_, gks, precision, slices):
+    """Algorithmic DRAM bytes of the MT contraction launch(es): operands read
+    once (int8 slices of Ar, Ai, Br, Bi; or the FP64 A and B planes) and the
+    N x N block of H and O written once."""
+    K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
+    total = 0.0
+    for g in gks:
+        n = g.ngp
+        npad = (n + 63) // 64 * 64
+        if precision == "ozaki":
+            kp8 = (K + 255) // 256 * 256
+            total += 4.0 * slices * npad * kp8
+        else:
+            total += 4.0 * 8 * K * npad
+        total += 2.0 * 16 * n * n
+    return total
+
+
 def main_flops(sys_, gks):
     """Algorithmic flops of the MT contraction stage (upper triangles of A^H B and A^H A):
     sum over k of 8 N (N+1) K, K = sum_a m_a."""
@@ -464,7 +492,9 @@ def run_ours(args):
             roof = {"bound": "tensor", "kernel": "oz_mma_kernel (tcgen05.mma kind::i8, MT contraction)",
                     "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                     "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
-                    "int8_ops_per_step": ops, "traffic": None,
+                    "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_PER_K["ozaki"] * nk,
+                    "traffic_note": "bytes per launch: ncu dram__bytes_read+write of a 2 k-point capture scaled "
+                                    "by k-points; algorithmic %.3g" % main_bytes(s, gks, "ozaki", args.slices),
                     "fp64_equivalent": {"achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                                         "frac": achieved / peak64,
                                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}}
@@ -473,7 +503,9 @@ def run_ours(args):
                     "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in "
                                    "MEASURED_PEAKS.json)",
-                    "algorithmic_flops_per_step": fl, "traffic": None}
+                    "algorithmic_flops_per_step": fl, "traffic": PROFILED_DRAM_BYTES_PER_K["fp64"] * nk,
+                    "traffic_note": "bytes per step of <1>+<2>: ncu dram__bytes_read+write of a 6 k-point "
+                                    "capture scaled by k-points; algorithmic %.3g" % main_bytes(s, gks, "fp64", 0)}
         clocks = _clock_summary(rows, local)
         cpu_v, cpu_n, cpu_dt = (None, 0, 0.0) if args.skip_cpu else cpu_sample(s, gks, budget_s=12.0)
         out = {
