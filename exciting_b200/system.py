@@ -91,3 +91,26 @@ class LapwSystem:
     def nmat(self, gk: GkSet) -> int:
         """nmat = ngk + nlotot (src/init1.f90:474)."""
         return gk.ngp + self.basis.nlotot
+
+
+@dataclass
+class MtRadial:
+    """Inputs of the muffin-tin integral generation ``hmlint``
+    (src/src_eigensystem/hmlint.f90:52-55): full radial functions on the
+    muffin-tin meshes and the effective potential in real spherical
+    harmonics, as the reference keeps them in ``apwfr``, ``lofr``,
+    ``veffmt`` and ``spr``."""
+    lmaxvr: int                       # potential expanded to l <= lmaxvr
+    nrmt: np.ndarray                  # (nspecies,) int32, radial points per species
+    spr: np.ndarray                   # (nrmtmax, nspecies)
+    apwfr: np.ndarray                 # (nrmtmax, 2, apwordmax, lmaxapw+1, natmtot): u, du/dr
+    lofr: np.ndarray                  # (nrmtmax, 2, nlomax, natmtot): v, dv/dr
+    veffmt: np.ndarray                # (lmmaxvr, nrmtmax, natmtot)
+
+    @property
+    def nrmtmax(self) -> int:
+        return self.spr.shape[0]
+
+    @property
+    def lmmaxvr(self) -> int:
+        return (self.lmaxvr + 1) ** 2

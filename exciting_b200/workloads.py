@@ -232,3 +232,64 @@ def si_cube216(*, relativity: str = "none", seed: int = 5) -> LapwSystem:
     kpts = np.array([[0, 0, 0], [0.5, 0, 0], [0.5, 0.5, 0], [0.5, 0.5, 0.5]])
     return build_system(crystal, basis, rgkmax=8.0, relativity=relativity,
                         kpoints=kpts, seed=seed, name="si_cube216")
+
+
+Y00 = 0.28209479177387814347
+
+
+def _pow_exp(r, p, a):
+    """r^p exp(-r/a) and its derivative."""
+    f = r ** p * np.exp(-r / a)
+    d = (p * r ** (p - 1) if p > 0 else 0.0) * np.exp(-r / a) - f / a
+    return f, d
+
+
+def mt_radial(sys: LapwSystem, *, lmaxvr: int = 8, seed: int = 11, nrmt: int = 300,
+              rmin: float = 1e-5):
+    """Seeded full radial functions and potential for ``hmlint``.
+
+    The APW functions continue the tails of ``sys`` (same analytic forms
+    r^l e^{-r/2} and r^{l+1} e^{-r/3}, same per-(l, atom) scale), so that the
+    matching coefficients and the muffin-tin integrals describe one basis.
+    Local orbitals (r/R)^{l+1} (1 - r/R) e^{-r/(2+i)} vanish at the sphere
+    boundary.  Potential: V_00 = (-14 e^{-2r}/r - 1)/Y00, and for l >= 1
+    V_lm = 0.3 N(0,1) (r/R)^l e^{-r/R}.  lmaxvr = 8 is the reference's
+    default (xml/schema/groundstate.xsd, attribute lmaxvr)."""
+    from .system import MtRadial
+    rng = np.random.default_rng(seed)
+    b, cr = sys.basis, sys.crystal
+    nsp, nat = cr.nspecies, cr.natmtot
+    spr = np.zeros((nrmt, nsp), order="F")
+    for is_ in range(nsp):
+        spr[:, is_] = radial_mesh_cubic(sys.rmt[is_], nrmt, rmin)
+        if abs(spr[-1, is_] - sys.spr_tail[-1, is_]) > 1e-12:
+            raise ValueError("radial mesh does not end on the tail mesh")
+    apwfr = np.zeros((nrmt, 2, b.apwordmax, b.lmaxapw + 1, nat), order="F")
+    lofr = np.zeros((nrmt, 2, b.nlomax, nat), order="F")
+    lmmaxvr = (lmaxvr + 1) ** 2
+    veffmt = np.zeros((lmmaxvr, nrmt, nat), order="F")
+    for ias in range(nat):
+        is_ = cr.atom_species[ias]
+        R = sys.rmt[is_]
+        r = spr[:, is_]
+        for l in range(b.lmaxapw + 1):
+            for io in range(b.apword[is_][l]):
+                p, a = l + io, 2.0 + io
+                f, d = _pow_exp(r, p, a)
+                # scale so that the tail points are reproduced
+                scale = sys.apwfr_tail[-1, io, l, ias] / f[-1]
+                apwfr[:, 0, io, l, ias] = scale * f
+                apwfr[:, 1, io, l, ias] = scale * d
+        for ilo, l in enumerate(b.lorbl[is_]):
+            x = r / R
+            e = np.exp(-r / (2.0 + ilo))
+            v = x ** (l + 1) * (1.0 - x) * e
+            dv = ((l + 1) * x ** l * (1.0 - x) / R - x ** (l + 1) / R) * e - v / (2.0 + ilo)
+            lofr[:, 0, ilo, ias] = v
+            lofr[:, 1, ilo, ias] = dv
+        veffmt[0, :, ias] = (-14.0 * np.exp(-2.0 * r) / r - 1.0) / Y00
+        for l in range(1, lmaxvr + 1):
+            for m in range(-l, l + 1):
+                veffmt[l * (l + 1) + m, :, ias] = 0.3 * rng.standard_normal() * (r / R) ** l * np.exp(-r / R)
+    return MtRadial(lmaxvr=lmaxvr, nrmt=np.full(nsp, nrmt, dtype=np.int32), spr=spr,
+                    apwfr=apwfr, lofr=lofr, veffmt=veffmt)

@@ -59,6 +59,16 @@ def lib():
         L.orc_hmlistln_olpistln.restype = None
         L.orc_copy_ul.argtypes = [i, i, P]
         L.orc_copy_ul.restype = None
+        L.orc_fint.argtypes = [i, P, P]
+        L.orc_fint.restype = d
+        L.orc_wigner3j.argtypes = [i] * 6
+        L.orc_wigner3j.restype = d
+        L.orc_gaunt.argtypes = [i] * 6
+        L.orc_gaunt.restype = d
+        L.orc_gauntyry_re_im.argtypes = [i] * 6 + [P]
+        L.orc_gauntyry_re_im.restype = None
+        L.orc_hmlint.argtypes = [i, P, i, i, i, i, P, i, P, P, i, P, P, P, P, P, i, i, i, P, P, P]
+        L.orc_hmlint.restype = None
         _LIB = L
     return _LIB
 
@@ -343,3 +353,57 @@ def overlapsetup_atom_aa(sys, apwalm, ngp, ias, o):
                 zm[:, f + io2] += apwi2[:, f + io2]
             f += n_io
     o[:ngp, :ngp] += apwi.conj().T @ zm.conj().T
+
+
+# ---------------------------------------------------------------- muffin-tin integrals
+def fint(x, f):
+    """Integral of the cubic spline through (x_i, f_i) from x_1 to x_n
+    (src/src_lib/fderiv.f90 with m = -1, gr(nr))."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    return lib().orc_fint(len(x), _p(x), _p(f))
+
+
+def wigner3j(j1, j2, j3, m1, m2, m3):
+    """src/src_lib/wigner3j.f90."""
+    return lib().orc_wigner3j(j1, j2, j3, m1, m2, m3)
+
+
+def gaunt(l1, l2, l3, m1, m2, m3):
+    """src/src_lib/gaunt.f90: integral of conj(Y_l1m1) Y_l2m2 Y_l3m3."""
+    return lib().orc_gaunt(l1, l2, l3, m1, m2, m3)
+
+
+def gauntyry(l1, l2, l3, m1, m2, m3):
+    """src/src_lib/gauntyry.f90: integral of conj(Y_l1m1) R_l2m2 Y_l3m3."""
+    out = np.zeros(2)
+    lib().orc_gauntyry_re_im(l1, l2, l3, m1, m2, m3, _p(out))
+    return complex(out[0], out[1])
+
+
+def hmlint(sys, rad):
+    """mt_hscf%main after hmlint = mt_kin + mt_pot on zeroed arrays
+    (src/src_eigensystem/hmlint.f90:53-55, mt_kin.f90:98-225,
+    mt_pot.f90:113-306).  Returns (aa, loa, lolo) in the reference's
+    (maxaa, maxaa, natmtot), (maxnlo, maxaa, natmtot), (maxnlo, maxnlo,
+    natmtot) layouts."""
+    b, cr = sys.basis, sys.crystal
+    nat, nsp = cr.natmtot, cr.nspecies
+    maxaa, maxnlo = b.maxaa, max(b.maxnlo, 1)
+    aa = np.zeros((maxaa, maxaa, nat), dtype=np.complex128, order="F")
+    loa = np.zeros((maxnlo, maxaa, nat), dtype=np.complex128, order="F")
+    lolo = np.zeros((maxnlo, maxnlo, nat), dtype=np.complex128, order="F")
+    species = np.asarray(cr.atom_species, dtype=np.int32)
+    apword = _f(np.array(b.apword, dtype=np.int32).T, np.int32)           # (lmaxapw+1, nsp)
+    nlorb = np.array([len(x) for x in b.lorbl], dtype=np.int32)
+    lorbl = np.zeros((b.nlomax, nsp), dtype=np.int32, order="F")
+    for is_ in range(nsp):
+        lorbl[:len(b.lorbl[is_]), is_] = b.lorbl[is_]
+    nrmt = np.asarray(rad.nrmt, dtype=np.int32)
+    spr, apwfr = _f(rad.spr, np.float64), _f(rad.apwfr, np.float64)
+    lofr, veffmt = _f(rad.lofr, np.float64), _f(rad.veffmt, np.float64)
+    lib().orc_hmlint(nat, _p(species), b.lmaxapw, b.lmaxmat, rad.lmaxvr, b.apwordmax, _p(apword),
+                     b.nlomax, _p(nlorb), _p(lorbl), rad.nrmtmax, _p(nrmt), _p(spr), _p(apwfr),
+                     _p(lofr), _p(veffmt), 0 if sys.relativity == "none" else 1, maxaa, maxnlo,
+                     _p(aa), _p(loa), _p(lolo))
+    return aa, loa, lolo

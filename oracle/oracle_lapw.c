@@ -482,3 +482,388 @@ void orc_copy_ul(int n, int ld, zdouble *a)
     for (int i = 0; i < n - 1; i++)
         for (int j = i + 1; j < n; j++) a[j + (size_t)ld * i] = conj(a[i + (size_t)ld * j]);
 }
+
+/* ======================================================================
+ * Muffin-tin integrals: hmlint = mt_kin + mt_pot (spin-unpolarised main
+ * Hamiltonian), src/src_eigensystem/hmlint.f90:55-57.
+ * ==================================================================== */
+
+#define ORC_Y00 0.28209479177387814347
+
+/* ---- src/src_lib/spline.f90:1-80: cubic spline coefficients cf(3, n) ---- */
+static void orc_spline(int n, const double *x, const double *f, double *cf, double *w)
+{
+#define CF(j, i) cf[(j) + 3 * (i)]
+    double t1, t2, t3, t4;
+    for (int i = 0; i < n - 1; i++) {
+        w[i] = 1.0 / (x[i + 1] - x[i]);
+        CF(0, i) = w[i] * (f[i + 1] - f[i]);
+    }
+    CF(1, 0) = 1.0;
+    CF(2, 0) = (CF(0, 1) - CF(0, 0)) / (x[2] - x[0]);
+    t1 = (x[1] - x[0]) * w[1];
+    t2 = t1 * CF(1, 0);
+    t3 = 1.0 / (2.0 * (t1 + 1.0));
+    CF(1, 1) = t3;
+    t4 = 3.0 * (CF(0, 1) - CF(0, 0)) * w[1] - t2 * CF(2, 0);
+    CF(2, 1) = t4;
+    for (int i = 2; i < n - 1; i++) {
+        t1 = (x[i] - x[i - 1]) * w[i];
+        t2 = t1 * t3;
+        t3 = 1.0 / (2.0 * t1 + 2.0 - t2);
+        CF(1, i) = t3;
+        t4 = 3.0 * (CF(0, i) - CF(0, i - 1)) * w[i] - t2 * t4;
+        CF(2, i) = t4;
+    }
+    CF(1, n - 1) = 1.0;
+    t1 = (CF(0, n - 2) - CF(0, n - 3)) / (x[n - 1] - x[n - 3]);
+    CF(2, n - 1) = t1;
+    for (int i = n - 2; i >= 1; i--) {
+        t1 = CF(2, i) - t1 * CF(1, i + 1);
+        CF(2, i) = t1;
+    }
+    for (int i = 0; i < n; i++) CF(1, i) = CF(1, i) * CF(2, i);
+    for (int i = 0; i < n - 1; i++) {
+        t1 = 0.3333333333333333333 * (CF(1, i + 1) - CF(1, i)) * w[i];
+        CF(2, i) = t1;
+        t2 = x[i + 1] - x[i];
+        CF(0, i) = CF(0, i) - (CF(1, i) + t1 * t2) * t2;
+    }
+    t1 = x[n - 1] - x[n - 2];
+    CF(0, n - 1) = CF(0, n - 2) + (2.0 * CF(1, n - 2) + 3.0 * CF(2, n - 2) * t1) * t1;
+    CF(2, n - 1) = CF(2, n - 2);
+#undef CF
+}
+
+/* ---- src/src_lib/fderiv.f90, m = -1: the integral from x(1) to x(n) ---- */
+double orc_fint(int n, const double *x, const double *f)
+{
+    double *cf = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+    double *w = (double *)malloc(sizeof(double) * (size_t)n);
+    orc_spline(n, x, f, cf, w);
+    double g = 0.0;
+    for (int i = 0; i < n - 1; i++) {
+        const double dx = x[i + 1] - x[i];
+        g = g + (((0.25 * cf[2 + 3 * i] * dx + 0.3333333333333333333 * cf[1 + 3 * i]) * dx + 0.5 * cf[3 * i]) * dx +
+                 f[i]) * dx;
+    }
+    free(cf);
+    free(w);
+    return g;
+}
+
+/* ---- src/src_lib/wigner3j.f90 --------------------------------------- */
+double orc_wigner3j(int j1, int j2, int j3, int m1, int m2, int m3)
+{
+    if (j1 == 0 && j2 == 0 && j3 == 0) return 1.0;
+    const int l1 = j2 - j1 + j3, l2 = j1 - j2 + j3, l3 = j1 + j2 - j3;
+    if (m1 + m2 + m3 != 0 || l1 < 0 || l2 < 0 || l3 < 0) return 0.0;
+    const int n1 = j1 - m1, n2 = j2 + m2;
+    int k1 = 0;
+    if (j2 - j3 - m1 > k1) k1 = j2 - j3 - m1;
+    if (j1 - j3 + m2 > k1) k1 = j1 - j3 + m2;
+    int k2 = l3;
+    if (n1 < k2) k2 = n1;
+    if (n2 < k2) k2 = n2;
+    double sgn = ((k1 + j1 + j2 + m3) % 2 != 0) ? -1.0 : 1.0;
+    double sum = 0.0;
+    for (int k = k1; k <= k2; k++) {
+        const double t1 = sgn * orc_factr(l1, l1 - n2 + k) * orc_factr(l2, l2 - n1 + k) * orc_factr(l3, l3 - k);
+        sum = sum + t1 / (orc_factnm(k, 1) * orc_factnm(n1 - k, 1) * orc_factnm(n2 - k, 1));
+        sgn = -sgn;
+    }
+    double t1 = orc_factr(j1 + m1, l1) * orc_factr(j2 + m2, l2) * orc_factr(j3 + m3, l3);
+    t1 = t1 * orc_factr(j3 - m3, 1 + j1 + j2 + j3) * orc_factnm(j1 - m1, 1) * orc_factnm(j2 - m2, 1);
+    return sum * sqrt(t1);
+}
+
+/* ---- src/src_lib/gaunt.f90: integral of conj(Y_l1m1) Y_l2m2 Y_l3m3 ------ */
+double orc_gaunt(int l1, int l2, int l3, int m1, int m2, int m3)
+{
+    if (m1 - m2 - m3 != 0) return 0.0;
+    const int j1 = l2 - l1 + l3, j2 = l1 - l2 + l3, j3 = l1 + l2 - l3;
+    if (j1 < 0 || j2 < 0 || j3 < 0) return 0.0;
+    const int j = l1 + l2 + l3;
+    if (j % 2 != 0) return 0.0;
+    const int jh = j / 2;
+    double t1 = sqrt((double)((2 * l1 + 1) * (2 * l2 + 1) * (2 * l3 + 1)) * orc_factr(j1, j + 1) *
+                     orc_factnm(j2, 1) * orc_factnm(j3, 1));
+    t1 = t1 * orc_factr(jh, jh - l1) / (orc_factnm(jh - l2, 1) * orc_factnm(jh - l3, 1));
+    double g = t1 * ORC_Y00 * orc_wigner3j(l1, l2, l3, -m1, m2, m3);
+    if ((m1 + jh) % 2 != 0) g = -g;
+    return g;
+}
+
+/* ---- src/src_lib/gauntyry.f90: conj(Y_l1m1) R_l2m2 Y_l3m3, R real harmonic */
+zdouble orc_gauntyry(int l1, int l2, int l3, int m1, int m2, int m3)
+{
+    const double c1 = 0.7071067811865475244;
+    if (m2 > 0) {
+        const double t1 = (m2 % 2 == 0) ? 1.0 : -1.0;
+        const double t2 = c1 * (orc_gaunt(l1, l2, l3, m1, m2, m3) + t1 * orc_gaunt(l1, l2, l3, m1, -m2, m3));
+        return t2;
+    } else if (m2 < 0) {
+        const double t1 = ((-m2) % 2 == 0) ? 1.0 : -1.0;
+        const double t2 = c1 * (orc_gaunt(l1, l2, l3, m1, m2, m3) - t1 * orc_gaunt(l1, l2, l3, m1, -m2, m3));
+        return -t2 * I;
+    }
+    return orc_gaunt(l1, l2, l3, m1, m2, m3);
+}
+
+void orc_gauntyry_re_im(int l1, int l2, int l3, int m1, int m2, int m3, double *re_im)
+{
+    const zdouble z = orc_gauntyry(l1, l2, l3, m1, m2, m3);
+    re_im[0] = creal(z);
+    re_im[1] = cimag(z);
+}
+
+static int orc_idxlm(int l, int m) { return l * (l + 1) + m; }   /* 0-based */
+
+/* ---- hmlint's main Hamiltonian: mt_kin.f90:70-195 then mt_pot.f90:114-306 ----
+ * apwfr(nrmtmax, 2, apwordmax, 0:lmaxapw, natmtot): u and du/dr;
+ * lofr(nrmtmax, 2, nlomax, natmtot); veffmt(lmmaxvr, nrmtmax, natmtot) in
+ * real spherical harmonics; spr(nrmtmax, nspecies); apword(0:lmaxapw, nspecies);
+ * lorbl(nlomax, nspecies).  aa(maxaa, maxaa, natmtot), loa(maxnlo, maxaa,
+ * natmtot), lolo(maxnlo, maxnlo, natmtot) are ADDED to (the reference adds
+ * to mt_hscf%main, zeroed beforehand by MTInit). */
+void orc_hmlint(int natmtot, const int *atom_species, int lmaxapw, int lmaxmat, int lmaxvr, int apwordmax,
+                const int *apword, int nlomax, const int *nlorb, const int *lorbl, int nrmtmax, const int *nrmt,
+                const double *spr, const double *apwfr, const double *lofr, const double *veffmt, int relativistic,
+                int maxaa, int maxnlo, zdouble *aa, zdouble *loa, zdouble *lolo)
+{
+    const int lmmaxvr = (lmaxvr + 1) * (lmaxvr + 1);
+    const double alpha = 1.0 / 137.03599911;
+    const double a = relativistic ? 0.5 * alpha * alpha : 0.0;
+#define APWFR(ir, d, io, l, ias) \
+    apwfr[(ir) + (size_t)nrmtmax * ((d) + 2 * ((io) + (size_t)apwordmax * ((l) + (size_t)(lmaxapw + 1) * (ias))))]
+#define LOFR(ir, d, ilo, ias) lofr[(ir) + (size_t)nrmtmax * ((d) + 2 * ((ilo) + (size_t)nlomax * (ias)))]
+#define POT(lm, ir, ias) veffmt[(lm) + (size_t)lmmaxvr * ((ir) + (size_t)nrmtmax * (ias))]
+#define AA(i, j, ias) aa[(i) + (size_t)maxaa * ((j) + (size_t)maxaa * (ias))]
+#define LOA(i, j, ias) loa[(i) + (size_t)maxnlo * ((j) + (size_t)maxaa * (ias))]
+#define LOLO(i, j, ias) lolo[(i) + (size_t)maxnlo * ((j) + (size_t)maxnlo * (ias))]
+    double *fr = (double *)malloc(sizeof(double) * nrmtmax);
+    double *r2 = (double *)malloc(sizeof(double) * nrmtmax);
+    double *r2inv = (double *)malloc(sizeof(double) * nrmtmax);
+    double *rmtable = (double *)malloc(sizeof(double) * nrmtmax);
+    /* Gaunt table gntryy(lm2, lm3, lm1) for lm1, lm3 <= lmmaxmat */
+    const int lmmaxmat = (lmaxmat + 1) * (lmaxmat + 1);
+    zdouble *gnt = (zdouble *)malloc(sizeof(zdouble) * (size_t)lmmaxvr * lmmaxmat * lmmaxmat);
+    for (int l1 = 0; l1 <= lmaxmat; l1++)
+        for (int m1 = -l1; m1 <= l1; m1++)
+            for (int l3 = 0; l3 <= lmaxmat; l3++)
+                for (int m3 = -l3; m3 <= l3; m3++)
+                    for (int l2 = 0; l2 <= lmaxvr; l2++)
+                        for (int m2 = -l2; m2 <= l2; m2++)
+                            gnt[orc_idxlm(l2, m2) + (size_t)lmmaxvr * (orc_idxlm(l3, m3) + (size_t)lmmaxmat * orc_idxlm(l1, m1))] =
+                                orc_gauntyry(l1, l2, l3, m1, m2, m3);
+#define GNT(lm2, lm3, lm1) gnt[(lm2) + (size_t)lmmaxvr * ((lm3) + (size_t)lmmaxmat * (lm1))]
+    /* radial integrals I(lm2, io2, l3, io1, l1) of mt_pot and K(io2, io1, l1) of mt_kin */
+    const size_t nint = (size_t)lmmaxvr * apwordmax * (lmaxmat + 1) * apwordmax * (lmaxmat + 1);
+    double *hint = (double *)malloc(sizeof(double) * nint);
+    double *hkin = (double *)malloc(sizeof(double) * apwordmax * apwordmax * (lmaxmat + 1));
+    double *hlo = (double *)malloc(sizeof(double) * (size_t)lmmaxvr * apwordmax * (lmaxmat + 1) * (nlomax > 0 ? nlomax : 1));
+    double *hlokin = (double *)malloc(sizeof(double) * apwordmax * (nlomax > 0 ? nlomax : 1));
+    double *hll = (double *)malloc(sizeof(double) * (size_t)lmmaxvr * (nlomax > 0 ? nlomax * nlomax : 1));
+    double *hllkin = (double *)malloc(sizeof(double) * (nlomax > 0 ? nlomax * nlomax : 1));
+#define HINT(lm2, io2, l3, io1, l1) \
+    hint[(lm2) + (size_t)lmmaxvr * ((io2) + (size_t)apwordmax * ((l3) + (size_t)(lmaxmat + 1) * ((io1) + (size_t)apwordmax * (l1))))]
+#define HLO(lm2, io, l3, ilo) hlo[(lm2) + (size_t)lmmaxvr * ((io) + (size_t)apwordmax * ((l3) + (size_t)(lmaxmat + 1) * (ilo)))]
+#define HLL(lm2, i1, i2) hll[(lm2) + (size_t)lmmaxvr * ((i1) + (size_t)nlomax * (i2))]
+    for (int ias = 0; ias < natmtot; ias++) {
+        const int is = atom_species[ias];
+        const int nr = nrmt[is];
+        const double *x = spr + (size_t)nrmtmax * is;
+        const int *apw = apword + (size_t)(lmaxapw + 1) * is;
+        const int nlo = nlorb[is];
+        const int *lol = lorbl + (size_t)nlomax * is;
+        for (int ir = 0; ir < nr; ir++) {
+            r2[ir] = x[ir] * x[ir];
+            r2inv[ir] = 1.0 / r2[ir];
+            rmtable[ir] = 1.0 / (1.0 - a * POT(0, ir, ias) * ORC_Y00);
+        }
+        /* ---- mt_kin: radial integrals (mt_kin.f90:71-121) */
+        for (int l1 = 0; l1 <= lmaxmat; l1++)
+            for (int io1 = 0; io1 < apw[l1]; io1++)
+                for (int io2 = 0; io2 < apw[l1]; io2++) {
+                    const double ang = (double)(l1 * (l1 + 1));
+                    for (int ir = 0; ir < nr; ir++) {
+                        const double t1 = APWFR(ir, 0, io1, l1, ias) * APWFR(ir, 0, io2, l1, ias);
+                        const double t2 = APWFR(ir, 1, io1, l1, ias) * APWFR(ir, 1, io2, l1, ias);
+                        fr[ir] = (0.5 * t2 * rmtable[ir] + 0.5 * ang * t1 * rmtable[ir] * r2inv[ir]) * r2[ir];
+                    }
+                    hkin[io2 + apwordmax * (io1 + apwordmax * l1)] = orc_fint(nr, x, fr) / ORC_Y00;
+                }
+        for (int ilo = 0; ilo < nlo; ilo++) {
+            const int l1 = lol[ilo];
+            for (int io = 0; io < apw[l1]; io++) {
+                const double ang = (double)(l1 * (l1 + 1));
+                for (int ir = 0; ir < nr; ir++) {
+                    const double t1 = APWFR(ir, 0, io, l1, ias) * LOFR(ir, 0, ilo, ias);
+                    const double t2 = APWFR(ir, 1, io, l1, ias) * LOFR(ir, 1, ilo, ias);
+                    fr[ir] = (0.5 * t2 * rmtable[ir] + 0.5 * ang * t1 * rmtable[ir] * r2inv[ir]) * r2[ir];
+                }
+                hlokin[io + apwordmax * ilo] = orc_fint(nr, x, fr) / ORC_Y00;
+            }
+        }
+        for (int ilo1 = 0; ilo1 < nlo; ilo1++)
+            for (int ilo2 = 0; ilo2 < nlo; ilo2++) {
+                if (lol[ilo1] != lol[ilo2]) continue;
+                const double ang = (double)(lol[ilo1] * (lol[ilo1] + 1));
+                for (int ir = 0; ir < nr; ir++) {
+                    const double t1 = LOFR(ir, 0, ilo1, ias) * LOFR(ir, 0, ilo2, ias);
+                    const double t2 = LOFR(ir, 1, ilo1, ias) * LOFR(ir, 1, ilo2, ias);
+                    fr[ir] = (0.5 * t2 * rmtable[ir] + 0.5 * ang * t1 * rmtable[ir] * r2inv[ir]) * r2[ir];
+                }
+                hllkin[ilo1 + nlomax * ilo2] = orc_fint(nr, x, fr) / ORC_Y00;
+            }
+        /* ---- mt_kin: diagonal lm blocks (mt_kin.f90:150-195) */
+        {
+            int if1 = 0;
+            for (int l1 = 0; l1 <= lmaxmat; l1++)
+                for (int m1 = -l1; m1 <= l1; m1++) {
+                    for (int io1 = 0; io1 < apw[l1]; io1++)
+                        for (int io2 = 0; io2 < apw[l1]; io2++)
+                            AA(if1 + io1, if1 + io2, ias) += hkin[io2 + apwordmax * (io1 + apwordmax * l1)] * ORC_Y00;
+                    if1 += apw[l1];
+                }
+            if1 = 0;
+            for (int ilo = 0; ilo < nlo; ilo++) {
+                const int l1 = lol[ilo];
+                for (int m1 = -l1; m1 <= l1; m1++) {
+                    const int lm1 = orc_idxlm(l1, m1);
+                    int if3 = 0;
+                    for (int l3 = 0; l3 <= lmaxmat; l3++)
+                        for (int m3 = -l3; m3 <= l3; m3++)
+                            for (int io = 0; io < apw[l3]; io++) {
+                                if (lm1 == orc_idxlm(l3, m3))
+                                    LOA(if1, if3, ias) += hlokin[io + apwordmax * ilo] * ORC_Y00;
+                                if3++;
+                            }
+                    if1++;
+                }
+            }
+            if1 = 0;
+            for (int ilo1 = 0; ilo1 < nlo; ilo1++)
+                for (int m1 = -lol[ilo1]; m1 <= lol[ilo1]; m1++) {
+                    const int lm1 = orc_idxlm(lol[ilo1], m1);
+                    int if3 = 0;
+                    for (int ilo2 = 0; ilo2 < nlo; ilo2++)
+                        for (int m3 = -lol[ilo2]; m3 <= lol[ilo2]; m3++) {
+                            if (lm1 == orc_idxlm(lol[ilo2], m3))
+                                LOLO(if1, if3, ias) += hllkin[ilo1 + nlomax * ilo2] * ORC_Y00;
+                            if3++;
+                        }
+                    if1++;
+                }
+        }
+        /* ---- mt_pot: radial integrals (mt_pot.f90:130-222) */
+        for (int l1 = 0; l1 <= lmaxmat; l1++)
+            for (int io1 = 0; io1 < apw[l1]; io1++)
+                for (int l3 = 0; l3 <= lmaxmat; l3++)
+                    for (int io2 = 0; io2 < apw[l3]; io2++)
+                        for (int lm2 = 0; lm2 < lmmaxvr; lm2++) {
+                            for (int ir = 0; ir < nr; ir++) {
+                                const double t1 = APWFR(ir, 0, io1, l1, ias) * APWFR(ir, 0, io2, l3, ias) * r2[ir];
+                                fr[ir] = t1 * POT(lm2, ir, ias);
+                            }
+                            HINT(lm2, io2, l3, io1, l1) = orc_fint(nr, x, fr);
+                        }
+        for (int ilo = 0; ilo < nlo; ilo++)
+            for (int l3 = 0; l3 <= lmaxmat; l3++)
+                for (int io = 0; io < apw[l3]; io++)
+                    for (int lm2 = 0; lm2 < lmmaxvr; lm2++) {
+                        for (int ir = 0; ir < nr; ir++) {
+                            const double t1 = LOFR(ir, 0, ilo, ias) * APWFR(ir, 0, io, l3, ias) * r2[ir];
+                            fr[ir] = t1 * POT(lm2, ir, ias);
+                        }
+                        HLO(lm2, io, l3, ilo) = orc_fint(nr, x, fr);
+                    }
+        for (int ilo1 = 0; ilo1 < nlo; ilo1++)
+            for (int ilo2 = 0; ilo2 < nlo; ilo2++)
+                for (int lm2 = 0; lm2 < lmmaxvr; lm2++) {
+                    for (int ir = 0; ir < nr; ir++) {
+                        const double t1 = LOFR(ir, 0, ilo1, ias) * LOFR(ir, 0, ilo2, ias) * r2[ir];
+                        fr[ir] = t1 * POT(lm2, ir, ias);
+                    }
+                    HLL(lm2, ilo1, ilo2) = orc_fint(nr, x, fr);
+                }
+        /* ---- mt_pot: angular sums over the nonzero Gaunt coefficients, lm2 ascending
+         * (mt_pot.f90:232-306, the gntnonz list of init1.f90:575-595) */
+        {
+            int if1 = 0;
+            for (int l1 = 0; l1 <= lmaxmat; l1++)
+                for (int m1 = -l1; m1 <= l1; m1++) {
+                    const int lm1 = orc_idxlm(l1, m1);
+                    for (int io1 = 0; io1 < apw[l1]; io1++) {
+                        int if3 = 0;
+                        for (int l3 = 0; l3 <= lmaxmat; l3++)
+                            for (int m3 = -l3; m3 <= l3; m3++) {
+                                const int lm3 = orc_idxlm(l3, m3);
+                                for (int io2 = 0; io2 < apw[l3]; io2++) {
+                                    zdouble zsum = 0.0;
+                                    for (int lm2 = 0; lm2 < lmmaxvr; lm2++) {
+                                        const zdouble g = GNT(lm2, lm3, lm1);
+                                        if (cabs(g) > 1e-20) zsum = zsum + g * HINT(lm2, io2, l3, io1, l1);
+                                    }
+                                    AA(if1, if3, ias) += zsum;
+                                    if3++;
+                                }
+                            }
+                        if1++;
+                    }
+                }
+            if1 = 0;
+            for (int ilo = 0; ilo < nlo; ilo++) {
+                const int l1 = lol[ilo];
+                for (int m1 = -l1; m1 <= l1; m1++) {
+                    const int lm1 = orc_idxlm(l1, m1);
+                    int if3 = 0;
+                    for (int l3 = 0; l3 <= lmaxmat; l3++)
+                        for (int m3 = -l3; m3 <= l3; m3++) {
+                            const int lm3 = orc_idxlm(l3, m3);
+                            for (int io = 0; io < apw[l3]; io++) {
+                                zdouble zsum = 0.0;
+                                for (int lm2 = 0; lm2 < lmmaxvr; lm2++) {
+                                    const zdouble g = GNT(lm2, lm3, lm1);
+                                    if (cabs(g) > 1e-20) zsum = zsum + g * HLO(lm2, io, l3, ilo);
+                                }
+                                LOA(if1, if3, ias) += zsum;
+                                if3++;
+                            }
+                        }
+                    if1++;
+                }
+            }
+            if1 = 0;
+            for (int ilo1 = 0; ilo1 < nlo; ilo1++)
+                for (int m1 = -lol[ilo1]; m1 <= lol[ilo1]; m1++) {
+                    const int lm1 = orc_idxlm(lol[ilo1], m1);
+                    int if3 = 0;
+                    for (int ilo2 = 0; ilo2 < nlo; ilo2++)
+                        for (int m3 = -lol[ilo2]; m3 <= lol[ilo2]; m3++) {
+                            const int lm3 = orc_idxlm(lol[ilo2], m3);
+                            zdouble zsum = 0.0;
+                            for (int lm2 = 0; lm2 < lmmaxvr; lm2++) {
+                                const zdouble g = GNT(lm2, lm3, lm1);
+                                if (cabs(g) > 1e-20) zsum = zsum + g * HLL(lm2, ilo1, ilo2);
+                            }
+                            LOLO(if1, if3, ias) += zsum;
+                            if3++;
+                        }
+                    if1++;
+                }
+        }
+    }
+    free(fr); free(r2); free(r2inv); free(rmtable); free(gnt); free(hint); free(hkin);
+    free(hlo); free(hlokin); free(hll); free(hllkin);
+#undef APWFR
+#undef LOFR
+#undef POT
+#undef AA
+#undef LOA
+#undef LOLO
+#undef GNT
+#undef HINT
+#undef HLO
+#undef HLL
+}
