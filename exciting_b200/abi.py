@@ -34,6 +34,13 @@ class exs_scf_inputs(ctypes.Structure):
     ]
 
 
+class exs_mt_radial(ctypes.Structure):
+    _fields_ = [
+        ("lmaxvr", c_int), ("nrmtmax", c_int), ("nrmt", P), ("spr", P), ("apwfr", P),
+        ("lofr", P), ("veffmt", P),
+    ]
+
+
 # entry point -> (argtypes, restype); the list mirrors include/exciting_b200.h
 SIGNATURES = {
     "exs_ctx_create": ([P, P], c_int),
@@ -66,6 +73,10 @@ SIGNATURES = {
     "exs_set_stream": ([P, P], c_int),
     "exs_last_timings": ([P, P, c_int], c_int),
     "exs_mt_contract_noalloc": ([c_int, c_int, P, c_int, P, P, P, P, c_int, P], c_int),
+    "exs_hmlint": ([P, P, P, P, P], c_int),
+    "exs_hmlint_device": ([P, P], c_int),
+    "exs_gauntyry": ([c_int] * 6 + [P], c_int),
+    "exs_fderiv_int": ([c_int, P, P, P], c_int),
 }
 
 _LIB = None

@@ -176,6 +176,7 @@ int exs_ctx_destroy(exs_ctx *c)
     }
     delete c->pool;
     exs::solver_release(c);
+    exs::mt_release(c);
     if (c->d_eval) cudaFree(c->d_eval);
     if (c->d_evec) cudaFree(c->d_evec);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -425,10 +426,13 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
 
 int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
 {
-    if (!c || !in || !in->mt_aa || !in->veffig || !in->cfunig || !in->spr_tail || !in->apwfr_tail || !in->oalo ||
-        !in->ololo)
+    if (!c || !in || !in->veffig || !in->cfunig || !in->spr_tail || !in->apwfr_tail || !in->oalo || !in->ololo)
         return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: missing input array");
-    if (c->nlotot > 0 && (!in->mt_loa || !in->mt_lolo)) return fail(c, EXS_ERR_ARG, "missing loa/lolo");
+    // mt_aa = NULL keeps the muffin-tin integrals exs_hmlint left on the device
+    const bool keep_mt = !in->mt_aa;
+    if (keep_mt && !c->have_mt)
+        return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: mt_aa is NULL and exs_hmlint has not run");
+    if (!keep_mt && c->nlotot > 0 && (!in->mt_loa || !in->mt_lolo)) return fail(c, EXS_ERR_ARG, "missing loa/lolo");
     if (c->relativity != EXS_REL_NONE && !in->meffig) return fail(c, EXS_ERR_ARG, "missing meffig");
     if (c->relativity == EXS_REL_IORA && (!in->m2effig || !in->h1aa || !in->h1loa || !in->h1lolo))
         return fail(c, EXS_ERR_ARG, "missing iora* inputs");
@@ -439,7 +443,7 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
     c->have_inputs = false;
     const int nat = c->natmtot, maxaa = c->maxaa, maxnlo = std::max(c->maxnlo, 1);
     // h_a: aa(f, f', ias) -> planar [ias][f'][f] with leading dim ldh
-    {
+    if (!keep_mt) {
         std::vector<double> re((size_t)nat * c->ldh * c->ldh, 0.0), im(re.size(), 0.0);
         for (int ias = 0; ias < nat; ias++)
             for (int f2 = 0; f2 < maxaa; f2++)
@@ -453,7 +457,7 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
         EXS_CUDA(cudaStreamSynchronize(s));
     }
     // loa(r, f, ias) -> planar [ias][f][r] with leading dim ldlo
-    {
+    if (!keep_mt) {
         std::vector<double> re((size_t)nat * c->ldlo * maxaa, 0.0), im(re.size(), 0.0);
         if (in->mt_loa)
             for (int ias = 0; ias < nat; ias++)
@@ -467,10 +471,14 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
         EXS_CUDA(upload(&c->d_loa_i, im.data(), im.size(), s));
         EXS_CUDA(cudaStreamSynchronize(s));
     }
-    std::vector<exs_complex> zero_lolo;
-    const exs_complex *lolo = in->mt_lolo;
-    if (!lolo) { zero_lolo.assign((size_t)maxnlo * maxnlo * nat, exs_complex{0, 0}); lolo = zero_lolo.data(); }
-    EXS_CUDA(upload(&c->d_lolo, lolo, (size_t)maxnlo * maxnlo * nat, s));
+    if (!keep_mt) {
+        std::vector<exs_complex> zero_lolo;
+        const exs_complex *lolo = in->mt_lolo;
+        if (!lolo) { zero_lolo.assign((size_t)maxnlo * maxnlo * nat, exs_complex{0, 0}); lolo = zero_lolo.data(); }
+        EXS_CUDA(upload(&c->d_lolo, lolo, (size_t)maxnlo * maxnlo * nat, s));
+        EXS_CUDA(cudaStreamSynchronize(s));
+        c->have_mt = false;
+    }
     EXS_CUDA(upload(&c->d_oalo, in->oalo, (size_t)c->apwordmax * c->nlomax * nat, s));
     EXS_CUDA(upload(&c->d_ololo, in->ololo, (size_t)c->nlomax * c->nlomax * nat, s));
     if (c->relativity == EXS_REL_IORA) {

@@ -196,6 +196,9 @@ struct exs_ctx {
     double *d_eval = nullptr;            // eigenpairs of the host-pointer solve call
     exs_complex *d_evec = nullptr;
     size_t eval_cap = 0, evec_cap = 0;
+    // muffin-tin integral generation (mtint.cu): tables, Gaunt list, work space
+    void *mt = nullptr;
+    bool have_mt = false;                // h_a, loa, lolo on the device came from exs_hmlint
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
@@ -254,6 +257,8 @@ cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, 
                              const KDesc *d_k, cudaStream_t s);
 // Device eigen-solve (solve.cu)
 void solver_release(exs_ctx *c);
+// Muffin-tin integral generation (mtint.cu)
+void mt_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)

@@ -109,11 +109,14 @@ class Setup:
         except Exception:
             pass
 
-    def set_scf_inputs(self, sys: LapwSystem | None = None):
+    def set_scf_inputs(self, sys: LapwSystem | None = None, *, keep_mt: bool = False):
+        """Upload the per-SCF inputs; keep_mt keeps the muffin-tin integrals
+        that :meth:`hmlint` left on the device instead of sys.mt_*."""
         s = sys or self.sys
         keep = dict(
-            mt_aa=_f(s.mt_aa, np.complex128), mt_loa=_f(s.mt_loa, np.complex128),
-            mt_lolo=_f(s.mt_lolo, np.complex128), oalo=_f(s.oalo, np.float64),
+            mt_aa=None if keep_mt else _f(s.mt_aa, np.complex128),
+            mt_loa=None if keep_mt else _f(s.mt_loa, np.complex128),
+            mt_lolo=None if keep_mt else _f(s.mt_lolo, np.complex128), oalo=_f(s.oalo, np.float64),
             ololo=_f(s.ololo, np.float64), veffig=_f(s.veffig, np.complex128),
             cfunig=_f(s.cfunig, np.complex128), spr_tail=_f(s.spr_tail, np.float64),
             apwfr_tail=_f(s.apwfr_tail, np.float64),
@@ -127,6 +130,37 @@ class Setup:
         for k, v in keep.items():
             setattr(inp, k, None if v is None else v.ctypes.data)
         self._check(self.lib.exs_set_scf_inputs(self.ctx, ctypes.byref(inp)))
+
+    def _mt_radial(self, rad, apwfr, lofr, veffmt):
+        keep = dict(nrmt=np.ascontiguousarray(rad.nrmt, dtype=np.int32), spr=_f(rad.spr, np.float64))
+        r = abi.exs_mt_radial()
+        r.lmaxvr, r.nrmtmax = int(rad.lmaxvr), int(rad.nrmtmax)
+        r.nrmt, r.spr = keep["nrmt"].ctypes.data, keep["spr"].ctypes.data
+        r.apwfr, r.lofr, r.veffmt = apwfr, lofr, veffmt
+        return r, keep
+
+    def hmlint(self, rad, *, outputs: bool = True):
+        """Muffin-tin integrals (aa, loa, lolo) of the radial inputs ``rad``
+        (system.MtRadial), installed on the device as this context's h_a;
+        returned in the reference's layouts when ``outputs``."""
+        b, nat = self.sys.basis, self.sys.natmtot
+        maxaa, maxnlo = b.maxaa, max(b.maxnlo, 1)
+        apwfr, lofr, veffmt = _f(rad.apwfr, np.float64), _f(rad.lofr, np.float64), _f(rad.veffmt, np.float64)
+        r, keep = self._mt_radial(rad, apwfr.ctypes.data, lofr.ctypes.data if lofr.size else None,
+                                  veffmt.ctypes.data)
+        aa = loa = lolo = None
+        if outputs:
+            aa = np.zeros((maxaa, maxaa, nat), dtype=np.complex128, order="F")
+            loa = np.zeros((maxnlo, maxaa, nat), dtype=np.complex128, order="F")
+            lolo = np.zeros((maxnlo, maxnlo, nat), dtype=np.complex128, order="F")
+        self._check(self.lib.exs_hmlint(self.ctx, ctypes.byref(r), _ptr(aa), _ptr(loa), _ptr(lolo)))
+        return aa, loa, lolo
+
+    def hmlint_device(self, rad, apwfr_ptr: int, lofr_ptr: int | None, veffmt_ptr: int):
+        """exs_hmlint_device: radial functions and potential already on the
+        device (their layouts as in system.MtRadial); enqueued, no outputs."""
+        r, keep = self._mt_radial(rad, apwfr_ptr, lofr_ptr, veffmt_ptr)
+        return self._check(self.lib.exs_hmlint_device(self.ctx, ctypes.byref(r)))
 
     def set_precision(self, mode: str = "fp64", slices: int = 7):
         m = {"fp64": 0, "ozaki": 1}[mode]

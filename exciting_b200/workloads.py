@@ -244,8 +244,8 @@ def _pow_exp(r, p, a):
     return f, d
 
 
-def mt_radial(sys: LapwSystem, *, lmaxvr: int = 8, seed: int = 11, nrmt: int = 300,
-              rmin: float = 1e-5):
+def mt_radial(sys: LapwSystem, *, lmaxvr: int = 8, seed: int = 11, nrmt=300,
+              rmin: float = 1e-5, nrmtmax: int | None = None):
     """Seeded full radial functions and potential for ``hmlint``.
 
     The APW functions continue the tails of ``sys`` (same analytic forms
@@ -254,42 +254,62 @@ def mt_radial(sys: LapwSystem, *, lmaxvr: int = 8, seed: int = 11, nrmt: int = 3
     Local orbitals (r/R)^{l+1} (1 - r/R) e^{-r/(2+i)} vanish at the sphere
     boundary.  Potential: V_00 = (-14 e^{-2r}/r - 1)/Y00, and for l >= 1
     V_lm = 0.3 N(0,1) (r/R)^l e^{-r/R}.  lmaxvr = 8 is the reference's
-    default (xml/schema/groundstate.xsd, attribute lmaxvr)."""
+    default (xml/schema/groundstate.xsd, attribute lmaxvr).  ``nrmt`` is one
+    count for every species or a list per species; the arrays are padded
+    with zeros to ``nrmtmax`` radial points (default: the largest nrmt)."""
     from .system import MtRadial
     rng = np.random.default_rng(seed)
     b, cr = sys.basis, sys.crystal
     nsp, nat = cr.nspecies, cr.natmtot
-    spr = np.zeros((nrmt, nsp), order="F")
+    nr_s = [int(nrmt)] * nsp if np.isscalar(nrmt) else [int(x) for x in nrmt]
+    nrmax = int(nrmtmax or max(nr_s))
+    spr = np.zeros((nrmax, nsp), order="F")
     for is_ in range(nsp):
-        spr[:, is_] = radial_mesh_cubic(sys.rmt[is_], nrmt, rmin)
-        if abs(spr[-1, is_] - sys.spr_tail[-1, is_]) > 1e-12:
+        spr[:nr_s[is_], is_] = radial_mesh_cubic(sys.rmt[is_], nr_s[is_], rmin)
+        if abs(spr[nr_s[is_] - 1, is_] - sys.spr_tail[-1, is_]) > 1e-12:
             raise ValueError("radial mesh does not end on the tail mesh")
-    apwfr = np.zeros((nrmt, 2, b.apwordmax, b.lmaxapw + 1, nat), order="F")
-    lofr = np.zeros((nrmt, 2, b.nlomax, nat), order="F")
+    apwfr = np.zeros((nrmax, 2, b.apwordmax, b.lmaxapw + 1, nat), order="F")
+    lofr = np.zeros((nrmax, 2, b.nlomax, nat), order="F")
     lmmaxvr = (lmaxvr + 1) ** 2
-    veffmt = np.zeros((lmmaxvr, nrmt, nat), order="F")
+    veffmt = np.zeros((lmmaxvr, nrmax, nat), order="F")
     for ias in range(nat):
         is_ = cr.atom_species[ias]
         R = sys.rmt[is_]
-        r = spr[:, is_]
+        n = nr_s[is_]
+        r = spr[:n, is_]
         for l in range(b.lmaxapw + 1):
             for io in range(b.apword[is_][l]):
                 p, a = l + io, 2.0 + io
                 f, d = _pow_exp(r, p, a)
                 # scale so that the tail points are reproduced
                 scale = sys.apwfr_tail[-1, io, l, ias] / f[-1]
-                apwfr[:, 0, io, l, ias] = scale * f
-                apwfr[:, 1, io, l, ias] = scale * d
+                apwfr[:n, 0, io, l, ias] = scale * f
+                apwfr[:n, 1, io, l, ias] = scale * d
         for ilo, l in enumerate(b.lorbl[is_]):
             x = r / R
             e = np.exp(-r / (2.0 + ilo))
             v = x ** (l + 1) * (1.0 - x) * e
             dv = ((l + 1) * x ** l * (1.0 - x) / R - x ** (l + 1) / R) * e - v / (2.0 + ilo)
-            lofr[:, 0, ilo, ias] = v
-            lofr[:, 1, ilo, ias] = dv
-        veffmt[0, :, ias] = (-14.0 * np.exp(-2.0 * r) / r - 1.0) / Y00
+            lofr[:n, 0, ilo, ias] = v
+            lofr[:n, 1, ilo, ias] = dv
+        veffmt[0, :n, ias] = (-14.0 * np.exp(-2.0 * r) / r - 1.0) / Y00
         for l in range(1, lmaxvr + 1):
             for m in range(-l, l + 1):
-                veffmt[l * (l + 1) + m, :, ias] = 0.3 * rng.standard_normal() * (r / R) ** l * np.exp(-r / R)
-    return MtRadial(lmaxvr=lmaxvr, nrmt=np.full(nsp, nrmt, dtype=np.int32), spr=spr,
+                veffmt[l * (l + 1) + m, :n, ias] = 0.3 * rng.standard_normal() * (r / R) ** l * np.exp(-r / R)
+    return MtRadial(lmaxvr=lmaxvr, nrmt=np.array(nr_s, dtype=np.int32), spr=spr,
                     apwfr=apwfr, lofr=lofr, veffmt=veffmt)
+
+
+
+def sic_two_species(*, relativity: str = "none", seed: int = 3) -> LapwSystem:
+    """Zincblende two-species cell (a = 8.24 Bohr) with different bases per
+    species: rmt 1.9 / 1.6, lmaxapw 8 with lmaxmat 7, apword 1 for l <= 1
+    and 2 above with lo l = 0, 1, 2 on species 0; apword 2 with one lo
+    (l = 0) on species 1.  Two k-points."""
+    h = 8.24 / 2.0
+    avec = np.array([[h, h, 0.0], [h, 0.0, h], [0.0, h, h]]).T
+    crystal = Crystal(avec, [1.9, 1.6], [0, 1], np.array([[0, 0, 0], [0.25, 0.25, 0.25]]).T)
+    basis = Basis(lmaxapw=8, lmaxmat=7, apword=[[1, 1] + [2] * 7, [2] * 9], lorbl=[[0, 1, 2], [0]],
+                  atom_species=[0, 1])
+    return build_system(crystal, basis, rgkmax=6.0, relativity=relativity,
+                        kpoints=np.array([[0.0, 0.0, 0.0], [0.25, 0.125, 0.0]]), seed=seed, name="sic_two_species")

@@ -78,6 +78,19 @@ typedef struct exs_scf_inputs {
     const double *apwfr_tail;    /* apwfr(nrmt-np+1:nrmt, 1, 1:apwordmax, 0:lmaxapw, natmtot) */
 } exs_scf_inputs;
 
+/* Inputs of the muffin-tin integral generation (exs_hmlint): the full
+ * radial functions and the effective potential of the current SCF
+ * iteration, in the reference's layouts. */
+typedef struct exs_mt_radial {
+    int lmaxvr;                  /* potential expanded in real harmonics up to lmaxvr */
+    int nrmtmax;                 /* leading dimension of the radial arrays */
+    const int *nrmt;             /* nrmt(nspecies): radial points per species (HOST, >= 4) */
+    const double *spr;           /* spr(nrmtmax, nspecies): radial meshes (HOST) */
+    const double *apwfr;         /* apwfr(nrmtmax, 2, apwordmax, 0:lmaxapw, natmtot): u and du/dr */
+    const double *lofr;          /* lofr(nrmtmax, 2, nlomax, natmtot): v and dv/dr (NULL if no lo) */
+    const double *veffmt;        /* veffmt(lmmaxvr, nrmtmax, natmtot), lmmaxvr = (lmaxvr+1)^2 */
+} exs_mt_radial;
+
 /* Create a context on the current CUDA device: validates the basis, builds
  * maxaa (MaxAPWs, mod_eigensystem.F90:151-184), losize/maxnlo (MTInitAll,
  * :194-235) and idxlo (genidxlo.f90), uploads the G-vector tables and sizes
@@ -89,8 +102,34 @@ const char *exs_last_error(const exs_ctx *ctx);
 /* Sizes the context derived: maxaa, maxnlo, nlotot (so a caller can size za). */
 int exs_ctx_sizes(const exs_ctx *ctx, int *maxaa, int *maxnlo, int *nlotot);
 
-/* Upload the per-SCF-iteration inputs (copied; the caller may free them). */
+/* Upload the per-SCF-iteration inputs (copied; the caller may free them).
+ * mt_aa = NULL (with mt_loa, mt_lolo ignored) keeps the muffin-tin integrals
+ * that exs_hmlint left on the device; EXS_ERR_ARG if it has not run. */
 int exs_set_scf_inputs(exs_ctx *ctx, const exs_scf_inputs *in);
+
+/* Replaces  call hmlint  (src/src_eigensystem/hmlint.f90:53-55: mt_kin then
+ * mt_pot, the spin-unpolarised mt_hscf%main): the muffin-tin Hamiltonian
+ * integrals of every atom,
+ *   aa(maxaa, maxaa, natmtot), loa(maxnlo, maxaa, natmtot),
+ *   lolo(maxnlo, maxnlo, natmtot)
+ * (as the reference leaves them in arrays MTInit zeroed; alo is the plain
+ * transpose of loa, mt_pot.f90:285), computed on the device from the radial
+ * functions and potential in *in (host arrays) and installed as the
+ * context's h_a for the following setups.  aa, loa, lolo: optional HOST
+ * outputs (NULL: not copied).  The scalar-relativistic kinetic factor
+ * 1/(1 - a V_00 Y00), a = alpha^2/2, applies when the context's relativity
+ * is not "none" (ValenceRelativity /= 'none', mt_kin.f90:55-59).
+ * Synchronous. */
+int exs_hmlint(exs_ctx *ctx, const exs_mt_radial *in, exs_complex *aa, exs_complex *loa,
+               exs_complex *lolo);
+/* The same with apwfr, lofr, veffmt DEVICE arrays (nrmt, spr stay on the
+ * host); enqueued on the context's stream, no host outputs. */
+int exs_hmlint_device(exs_ctx *ctx, const exs_mt_radial *in);
+/* Host utilities of the integral generation, callable without a GPU:
+ * gauntyry (src/src_lib/gauntyry.f90) -> re_im[2]; the spline integral
+ * fderiv(-1, n, x, f, g, cf) g(n) (src/src_lib/fderiv.f90), n >= 4. */
+int exs_gauntyry(int l1, int l2, int l3, int m1, int m2, int m3, double *re_im);
+int exs_fderiv_int(int n, const double *x, const double *f, double *result);
 
 /* Select the MT contraction arithmetic: EXS_PREC_FP64 (native FP64) or
  * EXS_PREC_OZAKI_INT8 with `slices` int8 slices per operand (3..9). */
