@@ -296,6 +296,80 @@ def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, mode="auto", pinned=T
     return value, h2d, d2h
 
 
+def hmlint_flops(sys_, rad):
+    """FP64 flops of the radial integrals of hmlint: per atom, lmmaxvr
+    potential channels x nrad^2 function pairs x nrmt points x 2 (one FMA),
+    plus the kinetic channel (two FMAs per point)."""
+    b, cr = sys_.basis, sys_.crystal
+    fl = 0.0
+    for ias in range(cr.natmtot):
+        is_ = cr.atom_species[ias]
+        nrad = sum(b.apword[is_][l] for l in range(b.lmaxmat + 1)) + len(b.lorbl[is_])
+        fl += (rad.lmmaxvr * 2.0 + 4.0) * nrad * nrad * float(rad.nrmt[is_])
+    return fl
+
+
+def hmlint_leg(args, st, sys_, stream, torch):
+    """exs_hmlint_device timed with CUDA events on the context's stream,
+    exs_hmlint (host arrays in, integrals out) by wall clock, and on cube8 the
+    oracle's CPU restatement of hmlint beside them.  Restores the synthetic
+    integrals of the setup afterwards."""
+    from exciting_b200 import workloads as W
+    rad = W.mt_radial(sys_)
+    dev = {k: torch.from_numpy(np.asfortranarray(getattr(rad, k)).ravel(order="F")).cuda()
+           for k in ("apwfr", "lofr", "veffmt")}
+    torch.cuda.synchronize()
+
+    def call():
+        st.hmlint_device(rad, dev["apwfr"].data_ptr(), dev["lofr"].data_ptr(), dev["veffmt"].data_ptr())
+
+    for _ in range(max(3, args.warmup)):
+        call()
+    st.synchronize()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 20
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(n):
+            call()
+        e1.record(stream)
+    st.synchronize()
+    torch.cuda.synchronize()
+    dev_ms = e0.elapsed_time(e1) / n
+    st.hmlint(rad)
+    t0 = time.perf_counter()
+    nrep = 5
+    for _ in range(nrep):
+        st.hmlint(rad)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / nrep
+    cpu = None
+    if not args.skip_cpu and sys_.natmtot <= 8:
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle"))
+        import lapw_oracle as O
+        t0 = time.perf_counter()
+        O.hmlint(sys_, rad)
+        dt = time.perf_counter() - t0
+        cpu = {"value": sys_.natmtot / dt, "unit": "atoms/s", "cores": 1, "kind": "port",
+               "sample": f"all {sys_.natmtot} atoms in {dt:.2f} s by the oracle's C restatement of "
+                         "mt_kin + mt_pot (one fderiv spline per radial product, as the reference)"}
+    st.set_scf_inputs()
+    fl = hmlint_flops(sys_, rad)
+    peak64 = _measured_fp64_peak(torch)
+    nin = sum(getattr(rad, k).size for k in ("apwfr", "lofr", "veffmt")) * 8
+    return {
+        "kernels": "mt_radial_kernel + mt_angular_kernel (exs_hmlint_device)",
+        "value": sys_.natmtot / (dev_ms * 1e-3), "unit": "atoms/s", "ms": dev_ms,
+        "e2e": {"value": sys_.natmtot / (e2e_ms * 1e-3), "unit": "atoms/s", "ms": e2e_ms,
+                "h2d_bytes": int(nin), "note": "exs_hmlint: pageable host inputs, integrals copied back"},
+        "lmaxvr": rad.lmaxvr, "nrmt": int(rad.nrmt[0]),
+        "roofline": {"bound": "fp64", "achieved": fl / (dev_ms * 1e-3) / 1e12, "peak": peak64,
+                     "unit": "TFLOP/s", "frac": fl / (dev_ms * 1e-3) / 1e12 / peak64,
+                     "flops": fl, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"},
+        "cpu_baseline": cpu,
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -411,6 +485,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     gather_ms = e0.elapsed_time(e1) / args.steps
     gather_bytes = sum(32.0 * n * (n + 1) for n in ngp)
+
+    # ---- muffin-tin integral generation (hmlint), once per SCF iteration
+    hml = None if args.skip_hmlint else hmlint_leg(args, st, s, stream, torch)
 
     # ---- setup + device eigen-solve through the host entry point (only the
     # lowest 40 eigenpairs come back; the consumer solvewithlapack replaced)
@@ -549,6 +626,7 @@ def run_ours(args):
             "setup_flops_per_step": setup_flops(s, gks),
             "accuracy": accuracy,
             "fp64_path_value": fp64_value,
+            "hmlint": hml,
         }
         print(json.dumps(out), flush=True)
     st.set_stream(None)
@@ -816,6 +894,7 @@ def main():
     ap.add_argument("--nk", type=int, default=27, help="k-points per step (profiling runs use fewer)")
     ap.add_argument("--skip-cpu", action="store_true", help="no CPU-baseline leg (profiling runs)")
     ap.add_argument("--skip-e2e", action="store_true", help="no host-pointer leg (profiling runs)")
+    ap.add_argument("--skip-hmlint", action="store_true", help="no muffin-tin integral leg (profiling runs)")
     ap.add_argument("--precision", default="ozaki", choices=["fp64", "ozaki"],
                     help="MT contraction arithmetic (the native FP64 path is timed beside the split one)")
     ap.add_argument("--workload", default="cube8", choices=["cube8", "cube216", "cells256"],

@@ -253,13 +253,19 @@ __device__ __forceinline__ const double *radfun(const MtArgs &a, int4 f, int ias
     return a.lofr + (size_t)a.nrmtmax * 2 * (f.z + (size_t)a.nlomax * ias);
 }
 
-// grid (tile pairs tp <= tq, nslot, natmtot), 256 threads.  Slot lm2 <
-// lmmaxvr: I[lm2][p][q] = sum_r w_r r^2 V_lm2(r) phi_p phi_q.  Slot lmmaxvr
-// (kinetic, mt_kin.f90:98-150): sum_r w_r rm_r (phi'_p phi'_q r^2 + l(l+1)
-// phi_p phi_q) / 2 with rm = 1 / (1 - a V_00 Y00), meaningful for equal l.
+constexpr int SG = 8;    // potential channels per block of mt_radial_kernel
+
+// grid (tile pairs tp <= tq, channel groups + 1, natmtot), 256 threads.
+// Group g < ngroup: channels lm2 = SG g .. SG g + SG - 1 (< lmmaxvr),
+//   I[lm2][p][q] = sum_r phi_p (phi_q w_r r^2) V_lm2(r);
+// the staged radial functions serve all SG channels of the block.  Group
+// ngroup: the kinetic channel (mt_kin.f90:98-150)
+//   sum_r w_r rm_r (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2,
+// rm = 1 / (1 - a V_00 Y00), meaningful for equal l.  Tiles are 32 x 32
+// function pairs; thread (tx, ty) owns q = tx and p = ty + 8 k, k < 4.
 __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
 {
-    const int ias = blockIdx.z, slot = blockIdx.y;
+    const int ias = blockIdx.z, grp = blockIdx.y;
     const int is = a.species[ias];
     const int nrad = a.nrad[is], nr = a.nrmt[is];
     const int ntile = (a.nradmax + RT - 1) / RT;
@@ -268,12 +274,19 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
     if (tp >= ntile) return;
     const int tq = tp + t;
     if (tp * RT >= nrad || tq * RT >= nrad) return;
-    const bool kin = slot == a.lmmaxvr;
+    const int ngroup = (a.lmmaxvr + SG - 1) / SG;
+    const bool kin = grp == ngroup;
+    const int lm0 = grp * SG;
     __shared__ double sA[RC][RT + 1], sB[RC][RT + 1], sAd[RC][RT + 1], sBd[RC][RT + 1];
+    __shared__ double sV[SG][RC];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const double *w = a.wr + (size_t)is * 2 * a.nrmtmax, *rr = w + a.nrmtmax;
     const double *vat = a.veffmt + (size_t)a.lmmaxvr * a.nrmtmax * ias;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double acc[4][SG];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int c = 0; c < SG; c++) acc[k][c] = 0.0;
     for (int r0 = 0; r0 < nr; r0 += RC) {
 #pragma unroll
         for (int k = 0; k < (RC * RT) / 256; k++) {
@@ -292,7 +305,7 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
                     const int4 fq = a.rfun[is * a.nradmax + q];
                     const double *f = radfun(a, fq, ias);
                     if (!kin) {
-                        fb = f[r] * (wt * x * x * vat[slot + (size_t)a.lmmaxvr * r]);
+                        fb = f[r] * (wt * x * x);
                     } else {
                         const double rm = 1.0 / (1.0 - a.a * vat[(size_t)a.lmmaxvr * r] * Y00);
                         fb = f[r] * (wt * rm * 0.5 * (double)(fq.y * (fq.y + 1)));
@@ -305,32 +318,50 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
             sAd[rl][col] = fad;
             sBd[rl][col] = fbd;
         }
+        if (!kin) {   // V_lm2(r) of the block's channels: 8 consecutive lm2 per r
+            const int c = threadIdx.x % SG, rl = threadIdx.x / SG, r = r0 + rl;
+            sV[c][rl] = (r < nr && lm0 + c < a.lmmaxvr) ? vat[lm0 + c + (size_t)a.lmmaxvr * r] : 0.0;
+        }
         __syncthreads();
         if (kin) {
 #pragma unroll 4
             for (int rl = 0; rl < RC; rl++) {
                 const double b = sB[rl][tx], bd = sBd[rl][tx];
 #pragma unroll
-                for (int k = 0; k < 4; k++) acc[k] += sA[rl][ty + 8 * k] * b + sAd[rl][ty + 8 * k] * bd;
+                for (int k = 0; k < 4; k++) acc[k][0] += sA[rl][ty + 8 * k] * b + sAd[rl][ty + 8 * k] * bd;
             }
         } else {
-#pragma unroll 8
+#pragma unroll 2
             for (int rl = 0; rl < RC; rl++) {
                 const double b = sB[rl][tx];
+                double bv[SG];
 #pragma unroll
-                for (int k = 0; k < 4; k++) acc[k] += sA[rl][ty + 8 * k] * b;
+                for (int c = 0; c < SG; c++) bv[c] = b * sV[c][rl];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double av = sA[rl][ty + 8 * k];
+#pragma unroll
+                    for (int c = 0; c < SG; c++) acc[k][c] += av * bv[c];
+                }
             }
         }
         __syncthreads();
     }
-    double *out = a.rint + ((size_t)ias * a.nslot + slot) * a.nradmax * a.nradmax;
+    const size_t nr2 = (size_t)a.nradmax * a.nradmax;
+    double *out = a.rint + (size_t)ias * a.nslot * nr2;
     const int q = tq * RT + tx;
+    const int nch = kin ? 1 : (a.lmmaxvr - lm0 < SG ? a.lmmaxvr - lm0 : SG);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const int p = tp * RT + ty + 8 * k;
         if (p < nrad && q < nrad) {
-            out[(size_t)p * a.nradmax + q] = acc[k];
-            if (tp != tq) out[(size_t)q * a.nradmax + p] = acc[k];
+#pragma unroll
+            for (int c = 0; c < SG; c++) {
+                if (c >= nch) break;
+                double *o = out + (size_t)(kin ? a.lmmaxvr : lm0 + c) * nr2;
+                o[(size_t)p * a.nradmax + q] = acc[k][c];
+                if (tp != tq) o[(size_t)q * a.nradmax + p] = acc[k][c];
+            }
         }
     }
 }
@@ -654,7 +685,8 @@ int enqueue(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const doubl
     a.out_aa = want_out ? m.d_out : nullptr;
     a.out_loa = want_out ? m.d_out + naa : nullptr;
     const int ntile = (m.nradmax + RT - 1) / RT;
-    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, (unsigned)nslot, nat), 256, 0, s>>>(a);
+    const int ngroup = (lmmaxvr + SG - 1) / SG;
+    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, ngroup + 1, nat), 256, 0, s>>>(a);
     MT_CUDA(cudaGetLastError());
     mt_angular_kernel<<<dim3((m.maxrows + 31) / 32, (m.maxrows + 7) / 8, nat), 256, 0, s>>>(a);
     MT_CUDA(cudaGetLastError());
