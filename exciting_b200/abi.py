@@ -75,6 +75,8 @@ SIGNATURES = {
     "exs_mt_contract_noalloc": ([c_int, c_int, P, c_int, P, P, P, P, c_int, P], c_int),
     "exs_hmlint": ([P, P, P, P, P], c_int),
     "exs_hmlint_device": ([P, P], c_int),
+    "exs_olprad": ([P, P, P, P, P, P, P], c_int),
+    "exs_olprad_device": ([P, P], c_int),
     "exs_gauntyry": ([c_int] * 6 + [P], c_int),
     "exs_fderiv_int": ([c_int, P, P, P], c_int),
 }

@@ -426,15 +426,20 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
 
 int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
 {
-    if (!c || !in || !in->veffig || !in->cfunig || !in->spr_tail || !in->apwfr_tail || !in->oalo || !in->ololo)
+    if (!c || !in || !in->veffig || !in->cfunig || !in->spr_tail || !in->apwfr_tail)
         return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: missing input array");
+    // oalo = NULL keeps the overlap radial integrals (and h1*) exs_olprad left on the device
+    const bool keep_olp = !in->oalo;
+    if (keep_olp && !c->have_olp)
+        return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: oalo is NULL and exs_olprad has not run");
+    if (!keep_olp && !in->ololo) return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: missing ololo");
     // mt_aa = NULL keeps the muffin-tin integrals exs_hmlint left on the device
     const bool keep_mt = !in->mt_aa;
     if (keep_mt && !c->have_mt)
         return fail(c, EXS_ERR_ARG, "exs_set_scf_inputs: mt_aa is NULL and exs_hmlint has not run");
     if (!keep_mt && c->nlotot > 0 && (!in->mt_loa || !in->mt_lolo)) return fail(c, EXS_ERR_ARG, "missing loa/lolo");
     if (c->relativity != EXS_REL_NONE && !in->meffig) return fail(c, EXS_ERR_ARG, "missing meffig");
-    if (c->relativity == EXS_REL_IORA && (!in->m2effig || !in->h1aa || !in->h1loa || !in->h1lolo))
+    if (c->relativity == EXS_REL_IORA && (!in->m2effig || (!keep_olp && (!in->h1aa || !in->h1loa || !in->h1lolo))))
         return fail(c, EXS_ERR_ARG, "missing iora* inputs");
     cudaSetDevice(c->device);
     cudaStream_t s = c->stream;
@@ -479,14 +484,18 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
         EXS_CUDA(cudaStreamSynchronize(s));
         c->have_mt = false;
     }
-    EXS_CUDA(upload(&c->d_oalo, in->oalo, (size_t)c->apwordmax * c->nlomax * nat, s));
-    EXS_CUDA(upload(&c->d_ololo, in->ololo, (size_t)c->nlomax * c->nlomax * nat, s));
-    if (c->relativity == EXS_REL_IORA) {
-        EXS_CUDA(upload(&c->d_h1aa, in->h1aa, (size_t)c->apwordmax * c->apwordmax * (c->lmaxapw + 1) * nat, s));
-        EXS_CUDA(upload(&c->d_h1loa, in->h1loa, (size_t)c->apwordmax * c->nlomax * nat, s));
-        EXS_CUDA(upload(&c->d_h1lolo, in->h1lolo, (size_t)c->nlomax * c->nlomax * nat, s));
-        EXS_CUDA(upload(&c->d_m2effig, in->m2effig, (size_t)c->ngvec, s));
+    if (!keep_olp) {
+        EXS_CUDA(upload(&c->d_oalo, in->oalo, (size_t)c->apwordmax * c->nlomax * nat, s));
+        EXS_CUDA(upload(&c->d_ololo, in->ololo, (size_t)c->nlomax * c->nlomax * nat, s));
+        if (c->relativity == EXS_REL_IORA) {
+            EXS_CUDA(upload(&c->d_h1aa, in->h1aa, (size_t)c->apwordmax * c->apwordmax * (c->lmaxapw + 1) * nat, s));
+            EXS_CUDA(upload(&c->d_h1loa, in->h1loa, (size_t)c->apwordmax * c->nlomax * nat, s));
+            EXS_CUDA(upload(&c->d_h1lolo, in->h1lolo, (size_t)c->nlomax * c->nlomax * nat, s));
+        }
+        EXS_CUDA(cudaStreamSynchronize(s));
+        c->have_olp = false;
     }
+    if (c->relativity == EXS_REL_IORA) EXS_CUDA(upload(&c->d_m2effig, in->m2effig, (size_t)c->ngvec, s));
     EXS_CUDA(upload(&c->d_veffig, in->veffig, (size_t)c->ngvec, s));
     EXS_CUDA(upload(&c->d_cfunig, in->cfunig, (size_t)c->ngvec, s));
     EXS_CUDA(upload(&c->d_kinw, c->relativity == EXS_REL_NONE ? in->cfunig : in->meffig, (size_t)c->ngvec, s));

@@ -199,6 +199,7 @@ struct exs_ctx {
     // muffin-tin integral generation (mtint.cu): tables, Gaunt list, work space
     void *mt = nullptr;
     bool have_mt = false;                // h_a, loa, lolo on the device came from exs_hmlint
+    bool have_olp = false;               // oalo, ololo (h1*) on the device came from exs_olprad
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)

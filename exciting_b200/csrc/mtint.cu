@@ -221,6 +221,7 @@ struct RadFun {      // one radial function of a species
 
 struct MtArgs {
     int natmtot, lmmaxvr, nslot, nradmax, nrmtmax, apwordmax, lmaxapw, nlomax, lmmaxmat;
+    int g0;                        // first channel group of the launch (mt_radial_kernel)
     double a;                      // 0.5 alpha^2 for a relativistic valence, else 0
     const int *species;            // [natmtot]
     const int *nrmt;               // [nspecies]
@@ -241,7 +242,12 @@ struct MtArgs {
     int ldlo, maxaa, maxnlo;
     exs_complex *lolo;             // (maxnlo, maxnlo, natmtot)
     exs_complex *out_aa, *out_loa; // optional copies in the reference layouts
+    double *oalo, *ololo;          // olprad outputs, reference layouts
+    double *h1aa, *h1loa, *h1lolo; // iora* only (else null)
 };
+
+// Channels after the lmmaxvr potential channels of the radial integrals.
+constexpr int CH_KIN = 0, CH_OVL = 1, CH_H1 = 2, NSPECIAL = 3;
 
 constexpr int RT = 32;   // radial functions per tile side
 constexpr int RC = 32;   // radial points per chunk
@@ -255,17 +261,21 @@ __device__ __forceinline__ const double *radfun(const MtArgs &a, int4 f, int ias
 
 constexpr int SG = 8;    // potential channels per block of mt_radial_kernel
 
-// grid (tile pairs tp <= tq, channel groups + 1, natmtot), 256 threads.
-// Group g < ngroup: channels lm2 = SG g .. SG g + SG - 1 (< lmmaxvr),
+// grid (tile pairs tp <= tq, channel groups of the launch, natmtot), 256
+// threads; group g = g0 + blockIdx.y.  Group g < ngroup: channels lm2 =
+// SG g .. SG g + SG - 1 (< lmmaxvr),
 //   I[lm2][p][q] = sum_r phi_p (phi_q w_r r^2) V_lm2(r);
-// the staged radial functions serve all SG channels of the block.  Group
-// ngroup: the kinetic channel (mt_kin.f90:98-150)
-//   sum_r w_r rm_r (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2,
-// rm = 1 / (1 - a V_00 Y00), meaningful for equal l.  Tiles are 32 x 32
-// function pairs; thread (tx, ty) owns q = tx and p = ty + 8 k, k < 4.
+// the staged radial functions serve all SG channels of the block.  Groups
+// ngroup + CH_*: one channel each, stored at slot lmmaxvr + CH_*, with
+// rm = 1 / (1 - a V_00 Y00):
+//   CH_KIN (mt_kin.f90:98-150)  sum_r w_r rm (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2
+//   CH_OVL (olprad.f90:52-56)   sum_r w_r r^2 phi_p phi_q
+//   CH_H1  (olprad.f90:30-44)   sum_r w_r a rm^2 (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2
+// the l(l+1) terms meaningful for equal l.  Tiles are 32 x 32 function
+// pairs; thread (tx, ty) owns q = tx and p = ty + 8 k, k < 4.
 __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
 {
-    const int ias = blockIdx.z, grp = blockIdx.y;
+    const int ias = blockIdx.z, grp = blockIdx.y + a.g0;
     const int is = a.species[ias];
     const int nrad = a.nrad[is], nr = a.nrmt[is];
     const int ntile = (a.nradmax + RT - 1) / RT;
@@ -275,7 +285,8 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
     const int tq = tp + t;
     if (tp * RT >= nrad || tq * RT >= nrad) return;
     const int ngroup = (a.lmmaxvr + SG - 1) / SG;
-    const bool kin = grp == ngroup;
+    const bool kin = grp >= ngroup;             // one of the single-channel groups
+    const int special = grp - ngroup;
     const int lm0 = grp * SG;
     __shared__ double sA[RC][RT + 1], sB[RC][RT + 1], sAd[RC][RT + 1], sBd[RC][RT + 1];
     __shared__ double sV[SG][RC];
@@ -304,12 +315,13 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
                 if (q < nrad) {
                     const int4 fq = a.rfun[is * a.nradmax + q];
                     const double *f = radfun(a, fq, ias);
-                    if (!kin) {
+                    if (!kin || special == CH_OVL) {
                         fb = f[r] * (wt * x * x);
                     } else {
                         const double rm = 1.0 / (1.0 - a.a * vat[(size_t)a.lmmaxvr * r] * Y00);
-                        fb = f[r] * (wt * rm * 0.5 * (double)(fq.y * (fq.y + 1)));
-                        fbd = f[r + a.nrmtmax] * (wt * rm * 0.5 * x * x);
+                        const double g = special == CH_KIN ? wt * rm * 0.5 : wt * a.a * rm * rm * 0.5;
+                        fb = f[r] * (g * (double)(fq.y * (fq.y + 1)));
+                        fbd = f[r + a.nrmtmax] * (g * x * x);
                     }
                 }
             }
@@ -358,7 +370,7 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
 #pragma unroll
             for (int c = 0; c < SG; c++) {
                 if (c >= nch) break;
-                double *o = out + (size_t)(kin ? a.lmmaxvr : lm0 + c) * nr2;
+                double *o = out + (size_t)(kin ? a.lmmaxvr + special : lm0 + c) * nr2;
                 o[(size_t)p * a.nradmax + q] = acc[k][c];
                 if (tp != tq) o[(size_t)q * a.nradmax + p] = acc[k][c];
             }
@@ -403,6 +415,51 @@ __global__ void __launch_bounds__(256) mt_angular_kernel(MtArgs a)
     } else {                         // lolo(i - napw, j - napw)
         a.lolo[(i - napw) + (size_t)a.maxnlo * ((j - napw) + (size_t)a.maxnlo * ias)] = exs_complex{re, im};
     }
+}
+
+__device__ __forceinline__ int find_radfun(const MtArgs &a, int is, int kind, int l, int idx)
+{
+    const int n = a.nrad[is];
+    for (int p = 0; p < n; p++) {
+        const int4 f = a.rfun[is * a.nradmax + p];
+        if (f.x == kind && f.z == idx && (kind == 1 || f.y == l)) return p;
+    }
+    return -1;
+}
+
+// grid (natmtot), 256 threads: the olprad arrays of one atom from the
+// overlap (and, for iora*, h1) channels; entries the reference does not
+// visit (l > lmaxmat, io >= apword, lo pairs of different l) are zero.
+__global__ void __launch_bounds__(256) mt_olprad_kernel(MtArgs a)
+{
+    const int ias = blockIdx.x, is = a.species[ias];
+    const size_t nr2 = (size_t)a.nradmax * a.nradmax;
+    const double *I = a.rint + (size_t)ias * a.nslot * nr2;
+    const double *Io = I + (size_t)(a.lmmaxvr + CH_OVL) * nr2, *Ih = I + (size_t)(a.lmmaxvr + CH_H1) * nr2;
+    const int ao = a.apwordmax, nlo = a.nlomax;
+    for (int t = threadIdx.x; t < ao * nlo; t += blockDim.x) {        // oalo, h1loa (io, ilo)
+        const int io = t % ao, ilo = t / ao;
+        const int q = find_radfun(a, is, 1, 0, ilo);
+        const int p = q < 0 ? -1 : find_radfun(a, is, 0, a.rfun[is * a.nradmax + q].y, io);
+        const size_t o = (size_t)t + (size_t)ao * nlo * ias;
+        a.oalo[o] = p < 0 ? 0.0 : Io[(size_t)p * a.nradmax + q];
+        if (a.h1loa) a.h1loa[o] = p < 0 ? 0.0 : Ih[(size_t)p * a.nradmax + q];
+    }
+    for (int t = threadIdx.x; t < nlo * nlo; t += blockDim.x) {       // ololo, h1lolo (ilo1, ilo2)
+        const int i1 = t % nlo, i2 = t / nlo;
+        const int p = find_radfun(a, is, 1, 0, i1), q = find_radfun(a, is, 1, 0, i2);
+        const bool ok = p >= 0 && q >= 0 && a.rfun[is * a.nradmax + p].y == a.rfun[is * a.nradmax + q].y;
+        const size_t o = (size_t)t + (size_t)nlo * nlo * ias;
+        a.ololo[o] = ok ? Io[(size_t)p * a.nradmax + q] : 0.0;
+        if (a.h1lolo) a.h1lolo[o] = ok ? Ih[(size_t)p * a.nradmax + q] : 0.0;
+    }
+    if (a.h1aa)                                                        // h1aa (io1, io2, l)
+        for (int t = threadIdx.x; t < ao * ao * (a.lmaxapw + 1); t += blockDim.x) {
+            const int io1 = t % ao, io2 = (t / ao) % ao, l = t / (ao * ao);
+            const int p = find_radfun(a, is, 0, l, io1), q = find_radfun(a, is, 0, l, io2);
+            a.h1aa[(size_t)t + (size_t)ao * ao * (a.lmaxapw + 1) * ias] =
+                (p < 0 || q < 0) ? 0.0 : Ih[(size_t)p * a.nradmax + q];
+        }
 }
 
 // ------------------------------------------------------------------ context state
@@ -619,33 +676,16 @@ int prepare(exs_ctx *c, const exs_mt_radial *in, MtState **out)
     return EXS_OK;
 }
 
-// Device work of one call: radial integrals, angular sums into the context's
-// h_a / loa / lolo, then the split-precision slices of the new h_a.
-int enqueue(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const double *lofr, const double *veffmt,
-            bool want_out, cudaStream_t s)
+// Arguments every launch of a call shares: tables, inputs, radial integrals.
+int common_args(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const double *lofr, const double *veffmt,
+                MtArgs &a, cudaStream_t s)
 {
-    const int nat = c->natmtot, maxaa = c->maxaa, maxnlo = std::max(c->maxnlo, 1);
-    const int lmmaxvr = (lmaxvr + 1) * (lmaxvr + 1);
+    const int nat = c->natmtot, lmmaxvr = (lmaxvr + 1) * (lmaxvr + 1);
     int rc = upload_tables(c, m, s);
     if (rc != EXS_OK) return rc;
-    MT_CUDA(ensure_dev(&c->d_haa_r, (size_t)nat * c->ldh * c->ldh));
-    MT_CUDA(ensure_dev(&c->d_haa_i, (size_t)nat * c->ldh * c->ldh));
-    MT_CUDA(ensure_dev(&c->d_loa_r, (size_t)nat * c->ldlo * maxaa));
-    MT_CUDA(ensure_dev(&c->d_loa_i, (size_t)nat * c->ldlo * maxaa));
-    MT_CUDA(ensure_dev(&c->d_lolo, (size_t)nat * maxnlo * maxnlo));
-    const size_t nslot = (size_t)lmmaxvr + 1;
+    const size_t nslot = (size_t)lmmaxvr + NSPECIAL;
     MT_CUDA(grow(&m.d_rint, &m.rint_cap, (size_t)nat * nslot * m.nradmax * m.nradmax));
-    const size_t naa = (size_t)maxaa * maxaa * nat, nloa = (size_t)maxnlo * maxaa * nat;
-    if (want_out) MT_CUDA(grow(&m.d_out, &m.out_cap, naa + nloa));
-    // rows and columns past a species' own block stay zero
-    MT_CUDA(cudaMemsetAsync(c->d_haa_r, 0, sizeof(double) * nat * c->ldh * c->ldh, s));
-    MT_CUDA(cudaMemsetAsync(c->d_haa_i, 0, sizeof(double) * nat * c->ldh * c->ldh, s));
-    MT_CUDA(cudaMemsetAsync(c->d_loa_r, 0, sizeof(double) * nat * c->ldlo * maxaa, s));
-    MT_CUDA(cudaMemsetAsync(c->d_loa_i, 0, sizeof(double) * nat * c->ldlo * maxaa, s));
-    MT_CUDA(cudaMemsetAsync(c->d_lolo, 0, sizeof(exs_complex) * nat * maxnlo * maxnlo, s));
-    if (want_out) MT_CUDA(cudaMemsetAsync(m.d_out, 0, sizeof(exs_complex) * (naa + nloa), s));
-
-    MtArgs a{};
+    a = MtArgs{};
     const char *tab = (const char *)m.d_tab;
     a.natmtot = nat;
     a.lmmaxvr = lmmaxvr;
@@ -673,6 +713,41 @@ int enqueue(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const doubl
     a.gnt_off = (const int *)(tab + m.off_goff);
     a.gnt_lm2 = (const int *)(tab + m.off_glm2);
     a.gnt_val = (const double2 *)(tab + m.off_gval);
+    return EXS_OK;
+}
+
+void launch_radial(const MtArgs &a, const MtState &m, int g0, int ngroups, cudaStream_t s)
+{
+    MtArgs b = a;
+    b.g0 = g0;
+    const int ntile = (m.nradmax + RT - 1) / RT;
+    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, ngroups, a.natmtot), 256, 0, s>>>(b);
+}
+
+// hmlint: radial integrals (potential and kinetic channels), angular sums
+// into the context's h_a / loa / lolo, then the split-precision slices of
+// the new h_a.
+int enqueue_hmlint(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const double *lofr,
+                   const double *veffmt, bool want_out, cudaStream_t s)
+{
+    const int nat = c->natmtot, maxaa = c->maxaa, maxnlo = std::max(c->maxnlo, 1);
+    MtArgs a;
+    int rc = common_args(c, m, lmaxvr, apwfr, lofr, veffmt, a, s);
+    if (rc != EXS_OK) return rc;
+    MT_CUDA(ensure_dev(&c->d_haa_r, (size_t)nat * c->ldh * c->ldh));
+    MT_CUDA(ensure_dev(&c->d_haa_i, (size_t)nat * c->ldh * c->ldh));
+    MT_CUDA(ensure_dev(&c->d_loa_r, (size_t)nat * c->ldlo * maxaa));
+    MT_CUDA(ensure_dev(&c->d_loa_i, (size_t)nat * c->ldlo * maxaa));
+    MT_CUDA(ensure_dev(&c->d_lolo, (size_t)nat * maxnlo * maxnlo));
+    const size_t naa = (size_t)maxaa * maxaa * nat, nloa = (size_t)maxnlo * maxaa * nat;
+    if (want_out) MT_CUDA(grow(&m.d_out, &m.out_cap, naa + nloa));
+    // rows and columns past a species' own block stay zero
+    MT_CUDA(cudaMemsetAsync(c->d_haa_r, 0, sizeof(double) * nat * c->ldh * c->ldh, s));
+    MT_CUDA(cudaMemsetAsync(c->d_haa_i, 0, sizeof(double) * nat * c->ldh * c->ldh, s));
+    MT_CUDA(cudaMemsetAsync(c->d_loa_r, 0, sizeof(double) * nat * c->ldlo * maxaa, s));
+    MT_CUDA(cudaMemsetAsync(c->d_loa_i, 0, sizeof(double) * nat * c->ldlo * maxaa, s));
+    MT_CUDA(cudaMemsetAsync(c->d_lolo, 0, sizeof(exs_complex) * nat * maxnlo * maxnlo, s));
+    if (want_out) MT_CUDA(cudaMemsetAsync(m.d_out, 0, sizeof(exs_complex) * (naa + nloa), s));
     a.haa_r = c->d_haa_r;
     a.haa_i = c->d_haa_i;
     a.ldh = c->ldh;
@@ -684,14 +759,62 @@ int enqueue(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const doubl
     a.lolo = c->d_lolo;
     a.out_aa = want_out ? m.d_out : nullptr;
     a.out_loa = want_out ? m.d_out + naa : nullptr;
-    const int ntile = (m.nradmax + RT - 1) / RT;
-    const int ngroup = (lmmaxvr + SG - 1) / SG;
-    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, ngroup + 1, nat), 256, 0, s>>>(a);
+    const int ngroup = (a.lmmaxvr + SG - 1) / SG;
+    launch_radial(a, m, 0, ngroup + 1, s);            // potential groups + CH_KIN
     MT_CUDA(cudaGetLastError());
     mt_angular_kernel<<<dim3((m.maxrows + 31) / 32, (m.maxrows + 7) / 8, nat), 256, 0, s>>>(a);
     MT_CUDA(cudaGetLastError());
     if (c->prec_mode == EXS_PREC_OZAKI_INT8 && c->d_xs)
         MT_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->slices, s));
+    return EXS_OK;
+}
+
+// olprad: overlap (and for iora* the h1) channels, then the small arrays
+// oalo, ololo (h1aa, h1loa, h1lolo) written into the context's copies.
+int enqueue_olprad(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const double *lofr,
+                   const double *veffmt, cudaStream_t s)
+{
+    const int nat = c->natmtot, ao = c->apwordmax, nlo = c->nlomax;
+    const bool iora = c->relativity == EXS_REL_IORA;
+    MtArgs a;
+    int rc = common_args(c, m, lmaxvr, apwfr, lofr, veffmt, a, s);
+    if (rc != EXS_OK) return rc;
+    MT_CUDA(ensure_dev(&c->d_oalo, (size_t)ao * nlo * nat));
+    MT_CUDA(ensure_dev(&c->d_ololo, (size_t)nlo * nlo * nat));
+    a.oalo = c->d_oalo;
+    a.ololo = c->d_ololo;
+    if (iora) {
+        MT_CUDA(ensure_dev(&c->d_h1aa, (size_t)ao * ao * (c->lmaxapw + 1) * nat));
+        MT_CUDA(ensure_dev(&c->d_h1loa, (size_t)ao * nlo * nat));
+        MT_CUDA(ensure_dev(&c->d_h1lolo, (size_t)nlo * nlo * nat));
+        a.h1aa = c->d_h1aa;
+        a.h1loa = c->d_h1loa;
+        a.h1lolo = c->d_h1lolo;
+    }
+    const int ngroup = (a.lmmaxvr + SG - 1) / SG;
+    launch_radial(a, m, ngroup + CH_OVL, iora ? 2 : 1, s);   // CH_OVL (+ CH_H1)
+    MT_CUDA(cudaGetLastError());
+    mt_olprad_kernel<<<nat, 256, 0, s>>>(a);
+    MT_CUDA(cudaGetLastError());
+    return EXS_OK;
+}
+
+// Radial inputs of a host-pointer call copied into the state's device buffer.
+int upload_inputs(exs_ctx *c, MtState &m, const exs_mt_radial *in, const double **apwfr, const double **lofr,
+                  const double **veffmt, cudaStream_t s)
+{
+    const int nat = c->natmtot, lmmaxvr = (in->lmaxvr + 1) * (in->lmaxvr + 1);
+    const size_t n_apw = (size_t)in->nrmtmax * 2 * c->apwordmax * (c->lmaxapw + 1) * nat;
+    const size_t n_lo = in->lofr ? (size_t)in->nrmtmax * 2 * c->nlomax * nat : 0;
+    const size_t n_v = (size_t)lmmaxvr * in->nrmtmax * nat;
+    MT_CUDA(cudaStreamSynchronize(s));   // the previous call's inputs may still be read
+    MT_CUDA(grow(&m.d_in, &m.in_cap, n_apw + n_lo + n_v));
+    MT_CUDA(cudaMemcpyAsync(m.d_in, in->apwfr, sizeof(double) * n_apw, cudaMemcpyHostToDevice, s));
+    if (n_lo) MT_CUDA(cudaMemcpyAsync(m.d_in + n_apw, in->lofr, sizeof(double) * n_lo, cudaMemcpyHostToDevice, s));
+    MT_CUDA(cudaMemcpyAsync(m.d_in + n_apw + n_lo, in->veffmt, sizeof(double) * n_v, cudaMemcpyHostToDevice, s));
+    *apwfr = m.d_in;
+    *lofr = n_lo ? m.d_in + n_apw : m.d_in;
+    *veffmt = m.d_in + n_apw + n_lo;
     return EXS_OK;
 }
 
@@ -732,17 +855,10 @@ int exs_hmlint(exs_ctx *c, const exs_mt_radial *in, exs_complex *aa, exs_complex
     if (rc != EXS_OK) return rc;
     cudaSetDevice(c->device);
     cudaStream_t s = c->stream;
-    const int nat = c->natmtot, lmmaxvr = (in->lmaxvr + 1) * (in->lmaxvr + 1);
-    const size_t n_apw = (size_t)in->nrmtmax * 2 * c->apwordmax * (c->lmaxapw + 1) * nat;
-    const size_t n_lo = in->lofr ? (size_t)in->nrmtmax * 2 * c->nlomax * nat : 0;
-    const size_t n_v = (size_t)lmmaxvr * in->nrmtmax * nat;
-    MT_CUDA(cudaStreamSynchronize(s));   // the previous call's inputs may still be read
-    MT_CUDA(grow(&m->d_in, &m->in_cap, n_apw + n_lo + n_v));
-    MT_CUDA(cudaMemcpyAsync(m->d_in, in->apwfr, sizeof(double) * n_apw, cudaMemcpyHostToDevice, s));
-    if (n_lo) MT_CUDA(cudaMemcpyAsync(m->d_in + n_apw, in->lofr, sizeof(double) * n_lo, cudaMemcpyHostToDevice, s));
-    MT_CUDA(cudaMemcpyAsync(m->d_in + n_apw + n_lo, in->veffmt, sizeof(double) * n_v, cudaMemcpyHostToDevice, s));
-    const bool want = aa || loa;
-    rc = enqueue(c, *m, in->lmaxvr, m->d_in, n_lo ? m->d_in + n_apw : m->d_in, m->d_in + n_apw + n_lo, want, s);
+    const double *apwfr, *lofr, *veffmt;
+    rc = upload_inputs(c, *m, in, &apwfr, &lofr, &veffmt, s);
+    if (rc != EXS_OK) return rc;
+    rc = enqueue_hmlint(c, *m, in->lmaxvr, apwfr, lofr, veffmt, aa || loa, s);
     if (rc != EXS_OK) return rc;
     rc = copy_out(c, *m, aa, loa, lolo, s);
     if (rc != EXS_OK) return rc;
@@ -757,9 +873,50 @@ int exs_hmlint_device(exs_ctx *c, const exs_mt_radial *in)
     int rc = prepare(c, in, &m);
     if (rc != EXS_OK) return rc;
     cudaSetDevice(c->device);
-    rc = enqueue(c, *m, in->lmaxvr, in->apwfr, in->lofr ? in->lofr : in->apwfr, in->veffmt, false, c->stream);
+    rc = enqueue_hmlint(c, *m, in->lmaxvr, in->apwfr, in->lofr ? in->lofr : in->apwfr, in->veffmt, false, c->stream);
     if (rc != EXS_OK) return rc;
     c->have_mt = true;
+    return EXS_OK;
+}
+
+int exs_olprad(exs_ctx *c, const exs_mt_radial *in, double *oalo, double *ololo, double *h1aa, double *h1loa,
+               double *h1lolo)
+{
+    MtState *m = nullptr;
+    int rc = prepare(c, in, &m);
+    if (rc != EXS_OK) return rc;
+    cudaSetDevice(c->device);
+    cudaStream_t s = c->stream;
+    const double *apwfr, *lofr, *veffmt;
+    rc = upload_inputs(c, *m, in, &apwfr, &lofr, &veffmt, s);
+    if (rc != EXS_OK) return rc;
+    rc = enqueue_olprad(c, *m, in->lmaxvr, apwfr, lofr, veffmt, s);
+    if (rc != EXS_OK) return rc;
+    const int nat = c->natmtot, ao = c->apwordmax, nlo = c->nlomax;
+    const bool iora = c->relativity == EXS_REL_IORA;
+    if (oalo) MT_CUDA(cudaMemcpyAsync(oalo, c->d_oalo, sizeof(double) * ao * nlo * nat, cudaMemcpyDeviceToHost, s));
+    if (ololo) MT_CUDA(cudaMemcpyAsync(ololo, c->d_ololo, sizeof(double) * nlo * nlo * nat, cudaMemcpyDeviceToHost, s));
+    if (iora && h1aa)
+        MT_CUDA(cudaMemcpyAsync(h1aa, c->d_h1aa, sizeof(double) * ao * ao * (c->lmaxapw + 1) * nat,
+                                cudaMemcpyDeviceToHost, s));
+    if (iora && h1loa)
+        MT_CUDA(cudaMemcpyAsync(h1loa, c->d_h1loa, sizeof(double) * ao * nlo * nat, cudaMemcpyDeviceToHost, s));
+    if (iora && h1lolo)
+        MT_CUDA(cudaMemcpyAsync(h1lolo, c->d_h1lolo, sizeof(double) * nlo * nlo * nat, cudaMemcpyDeviceToHost, s));
+    MT_CUDA(cudaStreamSynchronize(s));
+    c->have_olp = true;
+    return EXS_OK;
+}
+
+int exs_olprad_device(exs_ctx *c, const exs_mt_radial *in)
+{
+    MtState *m = nullptr;
+    int rc = prepare(c, in, &m);
+    if (rc != EXS_OK) return rc;
+    cudaSetDevice(c->device);
+    rc = enqueue_olprad(c, *m, in->lmaxvr, in->apwfr, in->lofr ? in->lofr : in->apwfr, in->veffmt, c->stream);
+    if (rc != EXS_OK) return rc;
+    c->have_olp = true;
     return EXS_OK;
 }
 

@@ -109,9 +109,10 @@ class Setup:
         except Exception:
             pass
 
-    def set_scf_inputs(self, sys: LapwSystem | None = None, *, keep_mt: bool = False):
+    def set_scf_inputs(self, sys: LapwSystem | None = None, *, keep_mt: bool = False, keep_olp: bool = False):
         """Upload the per-SCF inputs; keep_mt keeps the muffin-tin integrals
-        that :meth:`hmlint` left on the device instead of sys.mt_*."""
+        that :meth:`hmlint` left on the device instead of sys.mt_*, keep_olp
+        the overlap integrals of :meth:`olprad` instead of sys.oalo, ololo, h1*."""
         s = sys or self.sys
         keep = dict(
             mt_aa=None if keep_mt else _f(s.mt_aa, np.complex128),
@@ -126,6 +127,9 @@ class Setup:
             h1loa=None if s.h1loa is None else _f(s.h1loa, np.float64),
             h1lolo=None if s.h1lolo is None else _f(s.h1lolo, np.float64),
         )
+        if keep_olp:
+            for k in ("oalo", "ololo", "h1aa", "h1loa", "h1lolo"):
+                keep[k] = None
         inp = abi.exs_scf_inputs()
         for k, v in keep.items():
             setattr(inp, k, None if v is None else v.ctypes.data)
@@ -155,6 +159,29 @@ class Setup:
             lolo = np.zeros((maxnlo, maxnlo, nat), dtype=np.complex128, order="F")
         self._check(self.lib.exs_hmlint(self.ctx, ctypes.byref(r), _ptr(aa), _ptr(loa), _ptr(lolo)))
         return aa, loa, lolo
+
+    def olprad(self, rad, *, outputs: bool = True):
+        """Overlap radial integrals (oalo, ololo, h1aa, h1loa, h1lolo) of ``rad``,
+        installed on the device; the h1 arrays are None unless relativity is iora*."""
+        b, nat = self.sys.basis, self.sys.natmtot
+        nlo = max(b.nlomax, 1)
+        apwfr, lofr, veffmt = _f(rad.apwfr, np.float64), _f(rad.lofr, np.float64), _f(rad.veffmt, np.float64)
+        r, keep = self._mt_radial(rad, apwfr.ctypes.data, lofr.ctypes.data if lofr.size else None,
+                                  veffmt.ctypes.data)
+        iora = self.sys.relativity == "iora*"
+        out = [None] * 5
+        if outputs:
+            out = [np.zeros((b.apwordmax, nlo, nat), order="F"), np.zeros((nlo, nlo, nat), order="F"),
+                   np.zeros((b.apwordmax, b.apwordmax, b.lmaxapw + 1, nat), order="F") if iora else None,
+                   np.zeros((b.apwordmax, nlo, nat), order="F") if iora else None,
+                   np.zeros((nlo, nlo, nat), order="F") if iora else None]
+        self._check(self.lib.exs_olprad(self.ctx, ctypes.byref(r), *[_ptr(a) for a in out]))
+        return tuple(out)
+
+    def olprad_device(self, rad, apwfr_ptr: int, lofr_ptr: int | None, veffmt_ptr: int):
+        """exs_olprad_device: inputs already on the device; enqueued, no outputs."""
+        r, keep = self._mt_radial(rad, apwfr_ptr, lofr_ptr, veffmt_ptr)
+        return self._check(self.lib.exs_olprad_device(self.ctx, ctypes.byref(r)))
 
     def hmlint_device(self, rad, apwfr_ptr: int, lofr_ptr: int | None, veffmt_ptr: int):
         """exs_hmlint_device: radial functions and potential already on the

@@ -104,7 +104,9 @@ int exs_ctx_sizes(const exs_ctx *ctx, int *maxaa, int *maxnlo, int *nlotot);
 
 /* Upload the per-SCF-iteration inputs (copied; the caller may free them).
  * mt_aa = NULL (with mt_loa, mt_lolo ignored) keeps the muffin-tin integrals
- * that exs_hmlint left on the device; EXS_ERR_ARG if it has not run. */
+ * that exs_hmlint left on the device, oalo = NULL (with ololo and h1*
+ * ignored) the overlap integrals of exs_olprad; EXS_ERR_ARG if that call
+ * has not run. */
 int exs_set_scf_inputs(exs_ctx *ctx, const exs_scf_inputs *in);
 
 /* Replaces  call hmlint  (src/src_eigensystem/hmlint.f90:53-55: mt_kin then
@@ -125,6 +127,18 @@ int exs_hmlint(exs_ctx *ctx, const exs_mt_radial *in, exs_complex *aa, exs_compl
 /* The same with apwfr, lofr, veffmt DEVICE arrays (nrmt, spr stay on the
  * host); enqueued on the context's stream, no host outputs. */
 int exs_hmlint_device(exs_ctx *ctx, const exs_mt_radial *in);
+/* Replaces  call olprad  (src/src_eigensystem/olprad.f90, called before
+ * hmlint in scf_cycle.f90:207): the overlap radial integrals
+ *   oalo(apwordmax, nlomax, natmtot) = int u_{l,io} v_ilo r^2 (l = lorbl(ilo)),
+ *   ololo(nlomax, nlomax, natmtot)   = int v_ilo1 v_ilo2 r^2 (equal l, else 0),
+ * and for iora* h1aa(apwordmax, apwordmax, 0:lmaxapw, natmtot), h1loa,
+ * h1lolo (olprad.f90:30-44, :58-69, :78-90), computed on the device from
+ * *in and installed for the following setups.  Host outputs optional (NULL:
+ * not copied; the h1 arrays are written only for iora*).  Synchronous. */
+int exs_olprad(exs_ctx *ctx, const exs_mt_radial *in, double *oalo, double *ololo, double *h1aa,
+               double *h1loa, double *h1lolo);
+/* The same with apwfr, lofr, veffmt DEVICE arrays; enqueued, no outputs. */
+int exs_olprad_device(exs_ctx *ctx, const exs_mt_radial *in);
 /* Host utilities of the integral generation, callable without a GPU:
  * gauntyry (src/src_lib/gauntyry.f90) -> re_im[2]; the spline integral
  * fderiv(-1, n, x, f, g, cf) g(n) (src/src_lib/fderiv.f90), n >= 4. */

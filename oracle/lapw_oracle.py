@@ -69,6 +69,8 @@ def lib():
         L.orc_gauntyry_re_im.restype = None
         L.orc_hmlint.argtypes = [i, P, i, i, i, i, P, i, P, P, i, P, P, P, P, P, i, i, i, P, P, P]
         L.orc_hmlint.restype = None
+        L.orc_olprad.argtypes = [i, P, i, i, i, i, P, i, P, P, i, P, P, P, P, P, i, i, P, P, P, P, P]
+        L.orc_olprad.restype = None
         _LIB = L
     return _LIB
 
@@ -407,3 +409,37 @@ def hmlint(sys, rad):
                      _p(lofr), _p(veffmt), 0 if sys.relativity == "none" else 1, maxaa, maxnlo,
                      _p(aa), _p(loa), _p(lolo))
     return aa, loa, lolo
+
+
+def _radial_args(sys, rad):
+    b, cr = sys.basis, sys.crystal
+    nsp = cr.nspecies
+    species = np.asarray(cr.atom_species, dtype=np.int32)
+    apword = _f(np.array(b.apword, dtype=np.int32).T, np.int32)
+    nlorb = np.array([len(x) for x in b.lorbl], dtype=np.int32)
+    lorbl = np.zeros((b.nlomax, nsp), dtype=np.int32, order="F")
+    for is_ in range(nsp):
+        lorbl[:len(b.lorbl[is_]), is_] = b.lorbl[is_]
+    return [species, apword, nlorb, lorbl, np.asarray(rad.nrmt, dtype=np.int32), _f(rad.spr, np.float64),
+            _f(rad.apwfr, np.float64), _f(rad.lofr, np.float64), _f(rad.veffmt, np.float64)]
+
+
+def olprad(sys, rad):
+    """src/src_eigensystem/olprad.f90 on zeroed arrays: (oalo, ololo, h1aa,
+    h1loa, h1lolo); the h1 arrays are None unless the relativity is iora*."""
+    b, cr = sys.basis, sys.crystal
+    nat = cr.natmtot
+    A = _radial_args(sys, rad)
+    oalo = np.zeros((b.apwordmax, b.nlomax, nat), order="F")
+    ololo = np.zeros((b.nlomax, b.nlomax, nat), order="F")
+    iora = sys.relativity == "iora*"
+    h1aa = np.zeros((b.apwordmax, b.apwordmax, b.lmaxapw + 1, nat), order="F")
+    h1loa = np.zeros((b.apwordmax, b.nlomax, nat), order="F")
+    h1lolo = np.zeros((b.nlomax, b.nlomax, nat), order="F")
+    lib().orc_olprad(nat, _p(A[0]), b.lmaxapw, b.lmaxmat, rad.lmaxvr, b.apwordmax, _p(A[1]), b.nlomax,
+                     _p(A[2]), _p(A[3]), rad.nrmtmax, _p(A[4]), _p(A[5]), _p(A[6]), _p(A[7]), _p(A[8]),
+                     0 if sys.relativity == "none" else 1, 1 if iora else 0,
+                     _p(oalo), _p(ololo), _p(h1aa), _p(h1loa), _p(h1lolo))
+    if not iora:
+        h1aa = h1loa = h1lolo = None
+    return oalo, ololo, h1aa, h1loa, h1lolo

@@ -867,3 +867,92 @@ void orc_hmlint(int natmtot, const int *atom_species, int lmaxapw, int lmaxmat, 
 #undef HLO
 #undef HLL
 }
+
+/* ---- src/src_eigensystem/olprad.f90: overlap radial integrals -------------
+ * oalo(apwordmax, nlomax, natmtot), ololo(nlomax, nlomax, natmtot) and, for
+ * iora* (iora != 0), h1aa(apwordmax, apwordmax, 0:lmaxapw, natmtot),
+ * h1loa(apwordmax, nlomax, natmtot), h1lolo(nlomax, nlomax, natmtot).  The
+ * h1 arrays are zeroed first (olprad.f90:11-13); oalo/ololo entries the
+ * reference does not visit are left as passed in. */
+void orc_olprad(int natmtot, const int *atom_species, int lmaxapw, int lmaxmat, int lmaxvr, int apwordmax,
+                const int *apword, int nlomax, const int *nlorb, const int *lorbl, int nrmtmax, const int *nrmt,
+                const double *spr, const double *apwfr, const double *lofr, const double *veffmt, int relativistic,
+                int iora, double *oalo, double *ololo, double *h1aa, double *h1loa, double *h1lolo)
+{
+    const int lmmaxvr = (lmaxvr + 1) * (lmaxvr + 1);
+    const double alpha = 1.0 / 137.03599911;
+    const double a = relativistic ? 0.5 * alpha * alpha : 0.0;
+#define APWFR(ir, d, io, l, ias) \
+    apwfr[(ir) + (size_t)nrmtmax * ((d) + 2 * ((io) + (size_t)apwordmax * ((l) + (size_t)(lmaxapw + 1) * (ias))))]
+#define LOFR(ir, d, ilo, ias) lofr[(ir) + (size_t)nrmtmax * ((d) + 2 * ((ilo) + (size_t)nlomax * (ias)))]
+#define POT0(ir, ias) veffmt[(size_t)lmmaxvr * ((ir) + (size_t)nrmtmax * (ias))]
+    if (iora) {
+        memset(h1aa, 0, sizeof(double) * apwordmax * apwordmax * (lmaxapw + 1) * (size_t)natmtot);
+        memset(h1loa, 0, sizeof(double) * apwordmax * nlomax * (size_t)natmtot);
+        memset(h1lolo, 0, sizeof(double) * nlomax * nlomax * (size_t)natmtot);
+    }
+    double *fr = (double *)malloc(sizeof(double) * nrmtmax);
+    for (int ias = 0; ias < natmtot; ias++) {
+        const int is = atom_species[ias];
+        const int nr = nrmt[is];
+        const double *x = spr + (size_t)nrmtmax * is;
+        const int *apw = apword + (size_t)(lmaxapw + 1) * is;
+        const int *lol = lorbl + (size_t)nlomax * is;
+        if (iora)
+            for (int l = 0; l <= lmaxmat; l++) {
+                const double ang = (double)(l * (l + 1));
+                for (int io1 = 0; io1 < apw[l]; io1++)
+                    for (int io2 = 0; io2 < apw[l]; io2++) {
+                        for (int ir = 0; ir < nr; ir++) {
+                            const double rm = 1.0 / (1.0 - a * POT0(ir, ias) * ORC_Y00);
+                            const double t1 = APWFR(ir, 0, io1, l, ias) * APWFR(ir, 0, io2, l, ias);
+                            const double t2 = APWFR(ir, 1, io1, l, ias) * APWFR(ir, 1, io2, l, ias);
+                            fr[ir] = a * (0.5 * t2 * rm * rm + 0.5 * ang * t1 * rm * rm / (x[ir] * x[ir])) *
+                                     (x[ir] * x[ir]);
+                        }
+                        h1aa[io1 + (size_t)apwordmax * (io2 + (size_t)apwordmax * (l + (size_t)(lmaxapw + 1) * ias))] =
+                            orc_fint(nr, x, fr);
+                    }
+            }
+        for (int ilo = 0; ilo < nlorb[is]; ilo++) {
+            const int l = lol[ilo];
+            for (int io = 0; io < apw[l]; io++) {
+                for (int ir = 0; ir < nr; ir++) fr[ir] = APWFR(ir, 0, io, l, ias) * LOFR(ir, 0, ilo, ias) * (x[ir] * x[ir]);
+                oalo[io + (size_t)apwordmax * (ilo + (size_t)nlomax * ias)] = orc_fint(nr, x, fr);
+                if (iora) {
+                    const double ang = (double)(l * (l + 1));
+                    for (int ir = 0; ir < nr; ir++) {
+                        const double rm = 1.0 / (1.0 - a * POT0(ir, ias) * ORC_Y00);
+                        const double t1 = APWFR(ir, 0, io, l, ias) * LOFR(ir, 0, ilo, ias);
+                        const double t2 = APWFR(ir, 1, io, l, ias) * LOFR(ir, 1, ilo, ias);
+                        fr[ir] = (a * (0.5 * t2 * rm * rm + 0.5 * ang * t1 * rm * rm / (x[ir] * x[ir]))) * (x[ir] * x[ir]);
+                    }
+                    h1loa[io + (size_t)apwordmax * (ilo + (size_t)nlomax * ias)] = orc_fint(nr, x, fr);
+                }
+            }
+        }
+        for (int ilo1 = 0; ilo1 < nlorb[is]; ilo1++) {
+            const int l = lol[ilo1];
+            for (int ilo2 = 0; ilo2 < nlorb[is]; ilo2++) {
+                if (lol[ilo2] != l) continue;
+                for (int ir = 0; ir < nr; ir++)
+                    fr[ir] = LOFR(ir, 0, ilo1, ias) * LOFR(ir, 0, ilo2, ias) * (x[ir] * x[ir]);
+                ololo[ilo1 + (size_t)nlomax * (ilo2 + (size_t)nlomax * ias)] = orc_fint(nr, x, fr);
+                if (iora) {
+                    const double ang = (double)(l * (l + 1));
+                    for (int ir = 0; ir < nr; ir++) {
+                        const double rm = 1.0 / (1.0 - a * POT0(ir, ias) * ORC_Y00);
+                        const double t1 = LOFR(ir, 0, ilo1, ias) * LOFR(ir, 0, ilo2, ias);
+                        const double t2 = LOFR(ir, 1, ilo1, ias) * LOFR(ir, 1, ilo2, ias);
+                        fr[ir] = (a * (0.5 * t2 * rm * rm + 0.5 * ang * t1 * rm * rm / (x[ir] * x[ir]))) * (x[ir] * x[ir]);
+                    }
+                    h1lolo[ilo1 + (size_t)nlomax * (ilo2 + (size_t)nlomax * ias)] = orc_fint(nr, x, fr);
+                }
+            }
+        }
+    }
+    free(fr);
+#undef APWFR
+#undef LOFR
+#undef POT0
+}

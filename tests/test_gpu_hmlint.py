@@ -119,3 +119,54 @@ def test_keep_mt_without_hmlint_is_an_error():
     st = _setup(s)
     with pytest.raises(ExsError):
         st.set_scf_inputs(keep_mt=True)
+
+
+# ---------------------------------------------------------------- olprad
+def _check_olp(got, ref):
+    for g, r in zip(got, ref):
+        if r is None:
+            assert g is None
+            continue
+        scale = max(np.abs(r).max(), 1e-300)
+        assert np.abs(g - r).max() <= TOL * scale, np.abs(g - r).max() / scale
+
+
+@pytest.mark.parametrize("make", [lambda: W.si_fcc("shipped"), lambda: W.si_fcc("text", relativity="iora*"),
+                                  lambda: W.sic_two_species(relativity="iora*")])
+def test_olprad_vs_oracle(make):
+    s = make()
+    rad = W.mt_radial(s, nrmt=[300] * s.crystal.nspecies)
+    st = _setup(s)
+    _check_olp(st.olprad(rad), O.olprad(s, rad))
+
+
+def test_generated_integrals_drive_the_iora_setup():
+    """olprad + hmlint installed, then set_scf_inputs(keep_mt, keep_olp): H and
+    O equal those from uploading the same arrays, and the oracle's setup."""
+    s = W.si_fcc("text", relativity="iora*")
+    rad = W.mt_radial(s)
+    st = _setup(s)
+    oalo, ololo, h1aa, h1loa, h1lolo = st.olprad(rad)
+    aa, loa, lolo = st.hmlint(rad)
+    st.set_scf_inputs(keep_mt=True, keep_olp=True)
+    gks = s.gksets()[:2]
+    got = st.setup_batched(gks)
+    s2 = copy.copy(s)
+    s2.mt_aa, s2.mt_loa, s2.mt_lolo = aa, loa, lolo
+    s2.oalo, s2.ololo, s2.h1aa, s2.h1loa, s2.h1lolo = oalo, ololo, h1aa, h1loa, h1lolo
+    st.set_scf_inputs(s2)
+    ref = st.setup_batched(gks)
+    for (h, o), (hr, orf) in zip(got, ref):
+        assert np.array_equal(h, hr) and np.array_equal(o, orf)
+    ho = O.hamiltonandoverlapsetup(s2, gks[1])
+    h, o = got[1]
+    assert np.linalg.norm(h - ho[0]) / np.linalg.norm(ho[0]) <= 1e-12
+    assert np.linalg.norm(o - ho[1]) / np.linalg.norm(ho[1]) <= 1e-12
+
+
+def test_keep_olp_without_olprad_is_an_error():
+    from exciting_b200.abi import ExsError
+    s = W.si_fcc("shipped")
+    st = _setup(s)
+    with pytest.raises(ExsError):
+        st.set_scf_inputs(keep_olp=True)

@@ -237,3 +237,39 @@ def test_hmlint_relativistic_mass_enters_kinetic_only():
         for j, (l3, m3, _b) in enumerate(rows):
             if (l1, m1) != (l3, m3):
                 assert d[i, j, 0] == 0.0
+
+
+# ---------------------------------------------------------------- olprad
+def test_olprad_definitions():
+    s = W.si_fcc("text", relativity="iora*")
+    rad = W.mt_radial(s, lmaxvr=2)
+    oalo, ololo, h1aa, h1loa, h1lolo = O.olprad(s, rad)
+    b = s.basis
+    r = rad.spr[:, 0]
+    A2 = 0.5 * (1.0 / 137.03599911) ** 2
+    rm = 1.0 / (1.0 - A2 * rad.veffmt[0, :, 1] * Y00)
+    for ilo, l in enumerate(b.lorbl[0]):
+        v = rad.lofr[:, 0, ilo, 1]
+        for io in range(b.apword[0][l]):
+            u = rad.apwfr[:, 0, io, l, 1]
+            assert abs(oalo[io, ilo, 1] - O.fint(r, u * v * r * r)) < 1e-15
+        for ilo2, l2 in enumerate(b.lorbl[0]):
+            if l2 != l:
+                assert ololo[ilo, ilo2, 1] == 0.0 and h1lolo[ilo, ilo2, 1] == 0.0
+    # one lo per l in this basis: ololo is diagonal and positive
+    assert np.all(np.diag(ololo[:, :, 1]) > 0)
+    # h1aa(io1, io2, l) = a int (u1' u2' + l(l+1) u1 u2 / r^2) rm^2 r^2 / 2
+    l = 3
+    u1, u2 = rad.apwfr[:, 0, 0, l, 1], rad.apwfr[:, 0, 1, l, 1]
+    d1, d2 = rad.apwfr[:, 1, 0, l, 1], rad.apwfr[:, 1, 1, l, 1]
+    want = O.fint(r, A2 * (0.5 * d1 * d2 * rm * rm + 0.5 * l * (l + 1) * u1 * u2 * rm * rm / (r * r)) * r * r)
+    assert abs(h1aa[0, 1, l, 1] - want) < 1e-14 * abs(want) + 1e-20
+    assert abs(h1aa[0, 1, l, 1] - h1aa[1, 0, l, 1]) < 1e-14 * abs(want) + 1e-20
+
+
+def test_olprad_without_iora_has_no_h1():
+    s = W.si_fcc("shipped")
+    rad = W.mt_radial(s)
+    oalo, ololo, h1aa, h1loa, h1lolo = O.olprad(s, rad)
+    assert h1aa is None and h1loa is None and h1lolo is None
+    assert np.abs(oalo).max() > 0 and np.abs(ololo).max() > 0
