@@ -77,6 +77,9 @@ SIGNATURES = {
     "exs_hmlint_device": ([P, P], c_int),
     "exs_olprad": ([P, P, P, P, P, P, P], c_int),
     "exs_olprad_device": ([P, P], c_int),
+    "exs_rttddft_set_pmat": ([P, c_int, P, P, c_int], c_int),
+    "exs_rttddft_updateham": ([P, c_int, P, P, P, P, c_int, P, P, c_int], c_int),
+    "exs_rttddft_updateham_device": ([P, c_int, P, P, P, P, c_int, P, P, P], c_int),
     "exs_gauntyry": ([c_int] * 6 + [P], c_int),
     "exs_fderiv_int": ([c_int, P, P, P], c_int),
 }

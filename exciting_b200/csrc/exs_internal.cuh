@@ -200,6 +200,8 @@ struct exs_ctx {
     void *mt = nullptr;
     bool have_mt = false;                // h_a, loa, lolo on the device came from exs_hmlint
     bool have_olp = false;               // oalo, ololo (h1*) on the device came from exs_olprad
+    // real-time TDDFT Hamiltonian update (rttddft.cu): momentum matrices, work space
+    void *rt = nullptr;
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
@@ -260,6 +262,8 @@ cudaError_t launch_gemm_kind(int kind, const DevParams &p, const void *d_probs, 
 void solver_release(exs_ctx *c);
 // Muffin-tin integral generation (mtint.cu)
 void mt_release(exs_ctx *c);
+// Real-time TDDFT Hamiltonian update (rttddft.cu)
+void rt_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)

@@ -259,6 +259,62 @@ class Setup:
                                                          _ptr(ev), _ptr(vec), ldv))
         return ev, vec
 
+    def _k_arrays(self, gks):
+        nk = len(gks)
+        ngp = np.array([g.ngp for g in gks], dtype=np.int32)
+        ig = np.zeros((self.ngkmax, nk), dtype=np.int32, order="F")
+        vg = np.zeros((3, self.ngkmax, nk), order="F")
+        for k, g in enumerate(gks):
+            ig[: g.ngp, k] = g.igpig
+            vg[:, : g.ngp, k] = g.vgpc
+        return ngp, ig, vg
+
+    def rttddft_set_pmat(self, pmats):
+        """Register the momentum matrix elements, one (nmat, nmat, 3) complex
+        array per k-point (exs_rttddft_set_pmat)."""
+        ps = [np.asfortranarray(p, dtype=np.complex128) for p in pmats]
+        nmat = np.array([p.shape[0] for p in ps], dtype=np.int32)
+        ld = int(max(nmat)) if len(ps) else 1
+        blocks = []
+        for p in ps:
+            b = np.zeros((ld, ld, 3), dtype=np.complex128, order="F")
+            b[: p.shape[0], : p.shape[1], :] = p
+            blocks.append(b)
+        ptrs = (ctypes.c_void_p * len(blocks))(*[b.ctypes.data for b in blocks])
+        self._check(self.lib.exs_rttddft_set_pmat(self.ctx, len(blocks), _ptr(nmat), ptrs, ld))
+
+    def rttddft_updateham(self, gks, atot, calculate_overlap=True, overlap=None):
+        """UpdateHam's k-loop: returns (ham_time, overlap) lists of (nmat, nmat)
+        arrays; with calculate_overlap False, ``overlap`` (one array per
+        k-point) is the overlap that enters the sum."""
+        nk = len(gks)
+        ngp, ig, vg = self._k_arrays(gks)
+        nmat = [g.ngp + self.nlotot for g in gks]
+        ld = max(nmat)
+        ham = [np.zeros((ld, ld), dtype=np.complex128, order="F") for _ in gks]
+        ovl = [np.zeros((ld, ld), dtype=np.complex128, order="F") for _ in gks]
+        if not calculate_overlap:
+            for k, o in enumerate(overlap):
+                ovl[k][: nmat[k], : nmat[k]] = o
+        at = np.ascontiguousarray(atot, dtype=np.float64)
+        hp = (ctypes.c_void_p * nk)(*[h.ctypes.data for h in ham])
+        op = (ctypes.c_void_p * nk)(*[o.ctypes.data for o in ovl])
+        self._check(self.lib.exs_rttddft_updateham(self.ctx, nk, _ptr(ngp), _ptr(ig), _ptr(vg), _ptr(at),
+                                                   1 if calculate_overlap else 0, hp, op, ld))
+        return ([h[: n, : n] for h, n in zip(ham, nmat)], [o[: n, : n] for o, n in zip(ovl, nmat)])
+
+    def rttddft_updateham_device(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, atot, calculate_overlap, p_ptrs, h_ptrs,
+                                 o_ptrs):
+        nk = len(ngp)
+        ngp = np.asarray(ngp, dtype=np.int32)
+        at = np.ascontiguousarray(atot, dtype=np.float64)
+        pp = (ctypes.c_void_p * nk)(*p_ptrs)
+        hp = (ctypes.c_void_p * nk)(*h_ptrs)
+        op = (ctypes.c_void_p * nk)(*o_ptrs)
+        return self._check(self.lib.exs_rttddft_updateham_device(
+            self.ctx, nk, _ptr(ngp), ctypes.c_void_p(igpig_dev_ptr), ctypes.c_void_p(vgpc_dev_ptr), _ptr(at),
+            1 if calculate_overlap else 0, pp, hp, op))
+
     def setup_batched_device(self, ngp, igpig_dev_ptr, vgpc_dev_ptr, h_ptrs, o_ptrs):
         """Device-resident batched setup: pointers are device addresses (ints)."""
         nk = len(ngp)

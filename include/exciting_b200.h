@@ -242,6 +242,33 @@ int exs_setup_and_solve_batched(exs_ctx *ctx, int nk, const int *ngp, const int 
                                 const double *vgpc, int nstfv, double *evalfv, exs_complex *evecfv,
                                 int ldv);
 
+/* Real-time TDDFT (src/src_xs/src_rttddft/rttddft_hamiltonianoverlap.f90,
+ * UpdateHam :40-106).  exs_rttddft_set_pmat registers the momentum matrix
+ * elements pmat(1:nmat, 1:nmat, 1:3, ik) of nk k-points (host arrays of
+ * leading dimension ld, each the start of an (ld, ld, 3) block) and keeps a
+ * device copy for the whole propagation.  exs_rttddft_updateham then
+ * replaces the k-loop of UpdateHam (:80-101): per k-point H and O of the
+ * current SCF inputs (its hamsetup / overlapsetup, the ground-state
+ * blocks), and
+ *   ham[ik] = H + (|atot|^2 / (2 c^2)) O + sum_i (atot(i) / c) pmat(:,:,i)
+ * with c the speed of light in atomic units (physical_constants.f90:50).
+ * calculate_overlap /= 0: overlap[ik] receives the new O, which enters the
+ * sum; = 0: overlap[ik] is read as the overlap to use (the reference keeps
+ * the array of an earlier step).  ham, overlap: nk host pointers to
+ * (ld, ld) arrays (the reference's ham_time(:,:,ik), overlap(:,:,ik) with
+ * ld = nmatmax); ngp, igpig, vgpc as exs_setup_batched.  Synchronous. */
+int exs_rttddft_set_pmat(exs_ctx *ctx, int nk, const int *nmat, const exs_complex *const *pmat, int ld);
+int exs_rttddft_updateham(exs_ctx *ctx, int nk, const int *ngp, const int *igpig, const double *vgpc,
+                          const double *atot, int calculate_overlap, exs_complex *const *ham,
+                          exs_complex *const *overlap, int ld);
+/* The same on device arrays: pmat_dev[ik] (nmat, nmat, 3), h_dev[ik],
+ * o_dev[ik] (nmat, nmat); igpig_dev, vgpc_dev as exs_setup_batched_device.
+ * Asynchronous on the context's stream. */
+int exs_rttddft_updateham_device(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev,
+                                 const double *vgpc_dev, const double *atot, int calculate_overlap,
+                                 exs_complex *const *pmat_dev, exs_complex *const *h_dev,
+                                 exs_complex *const *o_dev);
+
 /* Autotuner (no counterpart in the reference): runs the batch described as
  * for exs_setup_batched_device once per kernel configuration of the active
  * precision mode (for the split-precision contraction: K chunks per

@@ -443,3 +443,28 @@ def olprad(sys, rad):
     if not iora:
         h1aa = h1loa = h1lolo = None
     return oalo, ololo, h1aa, h1loa, h1lolo
+
+
+# speed of light in atomic units (src/constants/physical_constants.f90:41-50)
+C_AU = 299792458.0 * 2.418884326509e-17 / 0.52917721067e-10
+
+
+def rttddft_updateham(sys, gk, atot, pmat, overlap=None):
+    """One k-point of UpdateHam (src/src_xs/src_rttddft/rttddft_hamiltonianoverlap.f90:40-106).
+
+    H and O are its hamsetup/overlapsetup (:108-330), which build the same
+    blocks as the ground-state hamiltonsetup/overlapsetup; the module's
+    interstitial loop mirrors each updated (i, j), i <= j, to (j, i) by
+    conjugation (:156-185), which agrees with the ground-state mirror to
+    rounding.  Then ham_time = H + (|A|^2/2c^2) O + sum_i (A_i/c) P_i (:95-100),
+    with O the new overlap, or ``overlap`` when the call skips it.
+    Returns (ham_time, O)."""
+    h, o = hamiltonandoverlapsetup(sys, gk)
+    if overlap is not None:
+        o = np.asarray(overlap)
+    a = np.asarray(atot, dtype=np.float64)
+    fact = float(np.dot(a, a)) / (2.0 * C_AU ** 2)
+    ham = h + fact * o
+    for i in range(3):
+        ham = ham + (a[i] / C_AU) * pmat[:, :, i]
+    return ham, o
