@@ -232,7 +232,9 @@ struct MtArgs {
     int maxrows;
     const double *wr;              // [nspecies][2][nrmtmax]: spline weights, radii
     const double *apwfr, *lofr, *veffmt;
-    double *rint;                  // [natmtot][nslot][nradmax][nradmax]
+    double *rint;                  // [natmtot][nradmax (p)][nradmax (q)][nslot]
+    int nsplit;                    // radial ranges per integral (mt_radial_kernel)
+    double *rpart;                 // nsplit > 1: partial sums [split][natmtot][p][q][nslot]
     const int *gnt_off;            // [lmmaxmat^2 + 1]
     const int *gnt_lm2;            // [nnz]
     const double2 *gnt_val;        // [nnz]
@@ -272,10 +274,13 @@ constexpr int SG = 8;    // potential channels per block of mt_radial_kernel
 //   CH_OVL (olprad.f90:52-56)   sum_r w_r r^2 phi_p phi_q
 //   CH_H1  (olprad.f90:30-44)   sum_r w_r a rm^2 (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2
 // the l(l+1) terms meaningful for equal l.  Tiles are 32 x 32 function
-// pairs; thread (tx, ty) owns q = tx and p = ty + 8 k, k < 4.
+// pairs; thread (tx, ty) owns q = tx and p = ty + 8 k, k < 4.  With
+// nsplit > 1 (few atoms), blockIdx.y also selects one of nsplit contiguous
+// ranges of 32-point chunks, and the block writes its partial sums to rpart
+// (mt_reduce_kernel adds them in a fixed order).
 __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
 {
-    const int ias = blockIdx.z, grp = blockIdx.y + a.g0;
+    const int ias = blockIdx.z, grp = blockIdx.y / a.nsplit + a.g0, split = blockIdx.y % a.nsplit;
     const int is = a.species[ias];
     const int nrad = a.nrad[is], nr = a.nrmt[is];
     const int ntile = (a.nradmax + RT - 1) / RT;
@@ -298,7 +303,9 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
     for (int k = 0; k < 4; k++)
 #pragma unroll
         for (int c = 0; c < SG; c++) acc[k][c] = 0.0;
-    for (int r0 = 0; r0 < nr; r0 += RC) {
+    const int nchunk = (nr + RC - 1) / RC;
+    const int c_end = (split + 1) * nchunk / a.nsplit;
+    for (int r0 = split * nchunk / a.nsplit * RC; r0 < c_end * RC; r0 += RC) {
 #pragma unroll
         for (int k = 0; k < (RC * RT) / 256; k++) {
             const int i = threadIdx.x + 256 * k;
@@ -360,7 +367,8 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
         __syncthreads();
     }
     const size_t nr2 = (size_t)a.nradmax * a.nradmax;
-    double *out = a.rint + (size_t)ias * a.nslot * nr2;
+    double *out = (a.nsplit > 1 ? a.rpart + (size_t)split * a.natmtot * nr2 * a.nslot : a.rint) +
+                  (size_t)ias * nr2 * a.nslot;
     const int q = tq * RT + tx;
     const int nch = kin ? 1 : (a.lmmaxvr - lm0 < SG ? a.lmmaxvr - lm0 : SG);
 #pragma unroll
@@ -370,11 +378,25 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
 #pragma unroll
             for (int c = 0; c < SG; c++) {
                 if (c >= nch) break;
-                double *o = out + (size_t)(kin ? a.lmmaxvr + special : lm0 + c) * nr2;
-                o[(size_t)p * a.nradmax + q] = acc[k][c];
-                if (tp != tq) o[(size_t)q * a.nradmax + p] = acc[k][c];
+                const int slot = kin ? a.lmmaxvr + special : lm0 + c;
+                out[((size_t)p * a.nradmax + q) * a.nslot + slot] = acc[k][c];
+                if (tp != tq) out[((size_t)q * a.nradmax + p) * a.nslot + slot] = acc[k][c];
             }
         }
+    }
+}
+
+// rint[x][s] = sum over the splits of rpart[split][x][s] for the channels
+// s0 <= s < s1 of a launch, splits added in order.
+__global__ void __launch_bounds__(256) mt_reduce_kernel(MtArgs a, int s0, int s1)
+{
+    const int ns = s1 - s0;
+    const size_t nx = (size_t)a.natmtot * a.nradmax * a.nradmax, stride = nx * a.nslot;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nx * ns; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t o = (i / ns) * a.nslot + s0 + i % ns;
+        double v = a.rpart[o];
+        for (int sp = 1; sp < a.nsplit; sp++) v += a.rpart[sp * stride + o];
+        a.rint[o] = v;
     }
 }
 
@@ -391,16 +413,16 @@ __global__ void __launch_bounds__(256) mt_angular_kernel(MtArgs a)
     if (i >= nrow || j >= nrow || (i < napw && j >= napw)) return;
     const int2 ri = a.rows[is * a.maxrows + i], rj = a.rows[is * a.maxrows + j];
     const size_t nr2 = (size_t)a.nradmax * a.nradmax;
-    const double *I = a.rint + (size_t)ias * a.nslot * nr2 + (size_t)ri.y * a.nradmax + rj.y;
+    const double *I = a.rint + ((size_t)ias * nr2 + (size_t)ri.y * a.nradmax + rj.y) * a.nslot;
     const int e0 = a.gnt_off[ri.x * a.lmmaxmat + rj.x], e1 = a.gnt_off[ri.x * a.lmmaxmat + rj.x + 1];
     double re = 0.0, im = 0.0;
     for (int e = e0; e < e1; e++) {
-        const double v = I[(size_t)a.gnt_lm2[e] * nr2];
+        const double v = I[a.gnt_lm2[e]];
         const double2 g = a.gnt_val[e];
         re += g.x * v;
         im += g.y * v;
     }
-    if (ri.x == rj.x) re += I[(size_t)a.lmmaxvr * nr2];
+    if (ri.x == rj.x) re += I[a.lmmaxvr];
     if (i < napw) {                  // aa(i, j)
         const size_t o = (size_t)i + (size_t)a.ldh * (j + (size_t)a.ldh * ias);
         a.haa_r[o] = re;
@@ -434,31 +456,31 @@ __global__ void __launch_bounds__(256) mt_olprad_kernel(MtArgs a)
 {
     const int ias = blockIdx.x, is = a.species[ias];
     const size_t nr2 = (size_t)a.nradmax * a.nradmax;
-    const double *I = a.rint + (size_t)ias * a.nslot * nr2;
-    const double *Io = I + (size_t)(a.lmmaxvr + CH_OVL) * nr2, *Ih = I + (size_t)(a.lmmaxvr + CH_H1) * nr2;
+    const double *I = a.rint + (size_t)ias * nr2 * a.nslot;
+    const double *Io = I + a.lmmaxvr + CH_OVL, *Ih = I + a.lmmaxvr + CH_H1;   // stride nslot per (p, q)
     const int ao = a.apwordmax, nlo = a.nlomax;
     for (int t = threadIdx.x; t < ao * nlo; t += blockDim.x) {        // oalo, h1loa (io, ilo)
         const int io = t % ao, ilo = t / ao;
         const int q = find_radfun(a, is, 1, 0, ilo);
         const int p = q < 0 ? -1 : find_radfun(a, is, 0, a.rfun[is * a.nradmax + q].y, io);
         const size_t o = (size_t)t + (size_t)ao * nlo * ias;
-        a.oalo[o] = p < 0 ? 0.0 : Io[(size_t)p * a.nradmax + q];
-        if (a.h1loa) a.h1loa[o] = p < 0 ? 0.0 : Ih[(size_t)p * a.nradmax + q];
+        a.oalo[o] = p < 0 ? 0.0 : Io[((size_t)p * a.nradmax + q) * a.nslot];
+        if (a.h1loa) a.h1loa[o] = p < 0 ? 0.0 : Ih[((size_t)p * a.nradmax + q) * a.nslot];
     }
     for (int t = threadIdx.x; t < nlo * nlo; t += blockDim.x) {       // ololo, h1lolo (ilo1, ilo2)
         const int i1 = t % nlo, i2 = t / nlo;
         const int p = find_radfun(a, is, 1, 0, i1), q = find_radfun(a, is, 1, 0, i2);
         const bool ok = p >= 0 && q >= 0 && a.rfun[is * a.nradmax + p].y == a.rfun[is * a.nradmax + q].y;
         const size_t o = (size_t)t + (size_t)nlo * nlo * ias;
-        a.ololo[o] = ok ? Io[(size_t)p * a.nradmax + q] : 0.0;
-        if (a.h1lolo) a.h1lolo[o] = ok ? Ih[(size_t)p * a.nradmax + q] : 0.0;
+        a.ololo[o] = ok ? Io[((size_t)p * a.nradmax + q) * a.nslot] : 0.0;
+        if (a.h1lolo) a.h1lolo[o] = ok ? Ih[((size_t)p * a.nradmax + q) * a.nslot] : 0.0;
     }
     if (a.h1aa)                                                        // h1aa (io1, io2, l)
         for (int t = threadIdx.x; t < ao * ao * (a.lmaxapw + 1); t += blockDim.x) {
             const int io1 = t % ao, io2 = (t / ao) % ao, l = t / (ao * ao);
             const int p = find_radfun(a, is, 0, l, io1), q = find_radfun(a, is, 0, l, io2);
             a.h1aa[(size_t)t + (size_t)ao * ao * (a.lmaxapw + 1) * ias] =
-                (p < 0 || q < 0) ? 0.0 : Ih[(size_t)p * a.nradmax + q];
+                (p < 0 || q < 0) ? 0.0 : Ih[((size_t)p * a.nradmax + q) * a.nslot];
         }
 }
 
@@ -487,6 +509,8 @@ struct MtState {
            off_wr = 0, off_goff = 0, off_glm2 = 0, off_gval = 0;
     double *d_rint = nullptr;
     size_t rint_cap = 0;
+    double *d_rpart = nullptr;     // partial sums of split radial ranges
+    size_t rpart_cap = 0;
     double *d_in = nullptr;        // uploaded apwfr | lofr | veffmt of the host-pointer call
     size_t in_cap = 0;
     exs_complex *d_out = nullptr;  // aa | loa in the reference layouts
@@ -716,12 +740,37 @@ int common_args(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, const d
     return EXS_OK;
 }
 
-void launch_radial(const MtArgs &a, const MtState &m, int g0, int ngroups, cudaStream_t s)
+// Radial integrals of channel groups g0 .. g0 + ngroups - 1, which fill the
+// slots s0 .. s1 - 1.  When the grid would not cover the GPU twice (few
+// atoms), the radial range is split over up to 4 blocks per integral and the
+// partial sums are added by mt_reduce_kernel.
+cudaError_t launch_radial(const MtArgs &a, MtState &m, int g0, int ngroups, int s0, int s1, cudaStream_t s)
 {
     MtArgs b = a;
     b.g0 = g0;
     const int ntile = (m.nradmax + RT - 1) / RT;
-    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, ngroups, a.natmtot), 256, 0, s>>>(b);
+    const long blocks = (long)ntile * (ntile + 1) / 2 * ngroups * a.natmtot;
+    int nsplit = 1;
+    int nsm = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    while (nsplit < 4 && blocks * nsplit < 2L * nsm) nsplit++;
+    b.nsplit = nsplit;
+    if (nsplit > 1) {
+        const size_t n = (size_t)nsplit * a.natmtot * m.nradmax * m.nradmax * a.nslot;
+        if (n > m.rpart_cap) {
+            cudaError_t e = cudaStreamSynchronize(s);   // the old buffer may still be in use
+            if (e == cudaSuccess) e = grow(&m.d_rpart, &m.rpart_cap, n);
+            if (e != cudaSuccess) return e;
+        }
+        b.rpart = m.d_rpart;
+    }
+    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, ngroups * nsplit, a.natmtot), 256, 0, s>>>(b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || nsplit == 1) return e;
+    const size_t total = (size_t)a.natmtot * m.nradmax * m.nradmax * (s1 - s0);
+    mt_reduce_kernel<<<(unsigned)std::min<size_t>((total + 255) / 256, 4 * (size_t)nsm), 256, 0, s>>>(b, s0, s1);
+    return cudaGetLastError();
 }
 
 // hmlint: radial integrals (potential and kinetic channels), angular sums
@@ -760,8 +809,7 @@ int enqueue_hmlint(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, cons
     a.out_aa = want_out ? m.d_out : nullptr;
     a.out_loa = want_out ? m.d_out + naa : nullptr;
     const int ngroup = (a.lmmaxvr + SG - 1) / SG;
-    launch_radial(a, m, 0, ngroup + 1, s);            // potential groups + CH_KIN
-    MT_CUDA(cudaGetLastError());
+    MT_CUDA(launch_radial(a, m, 0, ngroup + 1, 0, a.lmmaxvr + 1, s));   // potential groups + CH_KIN
     mt_angular_kernel<<<dim3((m.maxrows + 31) / 32, (m.maxrows + 7) / 8, nat), 256, 0, s>>>(a);
     MT_CUDA(cudaGetLastError());
     if (c->prec_mode == EXS_PREC_OZAKI_INT8 && c->d_xs)
@@ -792,8 +840,8 @@ int enqueue_olprad(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, cons
         a.h1lolo = c->d_h1lolo;
     }
     const int ngroup = (a.lmmaxvr + SG - 1) / SG;
-    launch_radial(a, m, ngroup + CH_OVL, iora ? 2 : 1, s);   // CH_OVL (+ CH_H1)
-    MT_CUDA(cudaGetLastError());
+    MT_CUDA(launch_radial(a, m, ngroup + CH_OVL, iora ? 2 : 1, a.lmmaxvr + CH_OVL,
+                          a.lmmaxvr + CH_OVL + (iora ? 2 : 1), s));   // CH_OVL (+ CH_H1)
     mt_olprad_kernel<<<nat, 256, 0, s>>>(a);
     MT_CUDA(cudaGetLastError());
     return EXS_OK;
@@ -839,6 +887,7 @@ void mt_release(exs_ctx *c)
     if (!m) return;
     if (m->d_tab) cudaFree(m->d_tab);
     if (m->d_rint) cudaFree(m->d_rint);
+    if (m->d_rpart) cudaFree(m->d_rpart);
     if (m->d_in) cudaFree(m->d_in);
     if (m->d_out) cudaFree(m->d_out);
     delete m;
