@@ -251,7 +251,6 @@ struct MtArgs {
 // Channels after the lmmaxvr potential channels of the radial integrals.
 constexpr int CH_KIN = 0, CH_OVL = 1, CH_H1 = 2, NSPECIAL = 3;
 
-constexpr int RT = 32;   // radial functions per tile side
 constexpr int RC = 32;   // radial points per chunk
 
 __device__ __forceinline__ const double *radfun(const MtArgs &a, int4 f, int ias)
@@ -263,7 +262,7 @@ __device__ __forceinline__ const double *radfun(const MtArgs &a, int4 f, int ias
 
 constexpr int SG = 8;    // potential channels per block of mt_radial_kernel
 
-// grid (tile pairs tp <= tq, channel groups of the launch, natmtot), 256
+// grid (tile pairs tp <= tq, channel groups of the launch, natmtot), 8 T
 // threads; group g = g0 + blockIdx.y.  Group g < ngroup: channels lm2 =
 // SG g .. SG g + SG - 1 (< lmmaxvr),
 //   I[lm2][p][q] = sum_r phi_p (phi_q w_r r^2) V_lm2(r);
@@ -273,44 +272,48 @@ constexpr int SG = 8;    // potential channels per block of mt_radial_kernel
 //   CH_KIN (mt_kin.f90:98-150)  sum_r w_r rm (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2
 //   CH_OVL (olprad.f90:52-56)   sum_r w_r r^2 phi_p phi_q
 //   CH_H1  (olprad.f90:30-44)   sum_r w_r a rm^2 (phi'_p phi'_q r^2 + l(l+1) phi_p phi_q) / 2
-// the l(l+1) terms meaningful for equal l.  Tiles are 32 x 32 function
-// pairs; thread (tx, ty) owns q = tx and p = ty + 8 k, k < 4.  With
+// the l(l+1) terms meaningful for equal l.  Tiles are T x T function
+// pairs, T = 16, 24 or 32 chosen to fit the basis (the 21 radial functions
+// of an lmaxmat 8 atom fill a 24 tile to 77 %, a 32 tile to 43 %); thread
+// (tx, ty) = (i % T, i / T) owns q = tx and p = ty + 8 k, k < T / 8.  With
 // nsplit > 1 (few atoms), blockIdx.y also selects one of nsplit contiguous
 // ranges of 32-point chunks, and the block writes its partial sums to rpart
 // (mt_reduce_kernel adds them in a fixed order).
-__global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
+template <int T>
+__global__ void __launch_bounds__(8 * T) mt_radial_kernel(MtArgs a)
 {
+    constexpr int KP = T / 8, NT = 8 * T;
     const int ias = blockIdx.z, grp = blockIdx.y / a.nsplit + a.g0, split = blockIdx.y % a.nsplit;
     const int is = a.species[ias];
     const int nrad = a.nrad[is], nr = a.nrmt[is];
-    const int ntile = (a.nradmax + RT - 1) / RT;
+    const int ntile = (a.nradmax + T - 1) / T;
     int t = blockIdx.x, tp = 0;
     while (tp < ntile && t >= ntile - tp) { t -= ntile - tp; tp++; }
     if (tp >= ntile) return;
     const int tq = tp + t;
-    if (tp * RT >= nrad || tq * RT >= nrad) return;
+    if (tp * T >= nrad || tq * T >= nrad) return;
     const int ngroup = (a.lmmaxvr + SG - 1) / SG;
     const bool kin = grp >= ngroup;             // one of the single-channel groups
     const int special = grp - ngroup;
     const int lm0 = grp * SG;
-    __shared__ double sA[RC][RT + 1], sB[RC][RT + 1], sAd[RC][RT + 1], sBd[RC][RT + 1];
+    __shared__ double sA[RC][T + 1], sB[RC][T + 1], sAd[RC][T + 1], sBd[RC][T + 1];
     __shared__ double sV[SG][RC];
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int tx = threadIdx.x % T, ty = threadIdx.x / T;
     const double *w = a.wr + (size_t)is * 2 * a.nrmtmax, *rr = w + a.nrmtmax;
     const double *vat = a.veffmt + (size_t)a.lmmaxvr * a.nrmtmax * ias;
-    double acc[4][SG];
+    double acc[KP][SG];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
+    for (int k = 0; k < KP; k++)
 #pragma unroll
         for (int c = 0; c < SG; c++) acc[k][c] = 0.0;
     const int nchunk = (nr + RC - 1) / RC;
     const int c_end = (split + 1) * nchunk / a.nsplit;
     for (int r0 = split * nchunk / a.nsplit * RC; r0 < c_end * RC; r0 += RC) {
 #pragma unroll
-        for (int k = 0; k < (RC * RT) / 256; k++) {
-            const int i = threadIdx.x + 256 * k;
+        for (int k = 0; k < (RC * T) / NT; k++) {
+            const int i = threadIdx.x + NT * k;
             const int rl = i % RC, col = i / RC, r = r0 + rl;
-            const int p = tp * RT + col, q = tq * RT + col;
+            const int p = tp * T + col, q = tq * T + col;
             double fa = 0.0, fad = 0.0, fb = 0.0, fbd = 0.0;
             if (r < nr) {
                 const double wt = w[r], x = rr[r];
@@ -337,17 +340,18 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
             sAd[rl][col] = fad;
             sBd[rl][col] = fbd;
         }
-        if (!kin) {   // V_lm2(r) of the block's channels: 8 consecutive lm2 per r
-            const int c = threadIdx.x % SG, rl = threadIdx.x / SG, r = r0 + rl;
-            sV[c][rl] = (r < nr && lm0 + c < a.lmmaxvr) ? vat[lm0 + c + (size_t)a.lmmaxvr * r] : 0.0;
-        }
+        if (!kin)   // V_lm2(r) of the block's channels: 8 consecutive lm2 per r
+            for (int i = threadIdx.x; i < SG * RC; i += NT) {
+                const int c = i % SG, rl = i / SG, r = r0 + rl;
+                sV[c][rl] = (r < nr && lm0 + c < a.lmmaxvr) ? vat[lm0 + c + (size_t)a.lmmaxvr * r] : 0.0;
+            }
         __syncthreads();
         if (kin) {
 #pragma unroll 4
             for (int rl = 0; rl < RC; rl++) {
                 const double b = sB[rl][tx], bd = sBd[rl][tx];
 #pragma unroll
-                for (int k = 0; k < 4; k++) acc[k][0] += sA[rl][ty + 8 * k] * b + sAd[rl][ty + 8 * k] * bd;
+                for (int k = 0; k < KP; k++) acc[k][0] += sA[rl][ty + 8 * k] * b + sAd[rl][ty + 8 * k] * bd;
             }
         } else {
 #pragma unroll 2
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
 #pragma unroll
                 for (int c = 0; c < SG; c++) bv[c] = b * sV[c][rl];
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
+                for (int k = 0; k < KP; k++) {
                     const double av = sA[rl][ty + 8 * k];
 #pragma unroll
                     for (int c = 0; c < SG; c++) acc[k][c] += av * bv[c];
@@ -369,11 +373,11 @@ __global__ void __launch_bounds__(256) mt_radial_kernel(MtArgs a)
     const size_t nr2 = (size_t)a.nradmax * a.nradmax;
     double *out = (a.nsplit > 1 ? a.rpart + (size_t)split * a.natmtot * nr2 * a.nslot : a.rint) +
                   (size_t)ias * nr2 * a.nslot;
-    const int q = tq * RT + tx;
+    const int q = tq * T + tx;
     const int nch = kin ? 1 : (a.lmmaxvr - lm0 < SG ? a.lmmaxvr - lm0 : SG);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int p = tp * RT + ty + 8 * k;
+    for (int k = 0; k < KP; k++) {
+        const int p = tp * T + ty + 8 * k;
         if (p < nrad && q < nrad) {
 #pragma unroll
             for (int c = 0; c < SG; c++) {
@@ -748,7 +752,8 @@ cudaError_t launch_radial(const MtArgs &a, MtState &m, int g0, int ngroups, int 
 {
     MtArgs b = a;
     b.g0 = g0;
-    const int ntile = (m.nradmax + RT - 1) / RT;
+    const int T = m.nradmax <= 16 ? 16 : (m.nradmax <= 24 ? 24 : 32);
+    const int ntile = (m.nradmax + T - 1) / T;
     const long blocks = (long)ntile * (ntile + 1) / 2 * ngroups * a.natmtot;
     int nsplit = 1;
     int nsm = 148;
@@ -765,7 +770,13 @@ cudaError_t launch_radial(const MtArgs &a, MtState &m, int g0, int ngroups, int 
         }
         b.rpart = m.d_rpart;
     }
-    mt_radial_kernel<<<dim3(ntile * (ntile + 1) / 2, ngroups * nsplit, a.natmtot), 256, 0, s>>>(b);
+    const dim3 grid(ntile * (ntile + 1) / 2, ngroups * nsplit, a.natmtot);
+    if (T == 16)
+        mt_radial_kernel<16><<<grid, 8 * 16, 0, s>>>(b);
+    else if (T == 24)
+        mt_radial_kernel<24><<<grid, 8 * 24, 0, s>>>(b);
+    else
+        mt_radial_kernel<32><<<grid, 8 * 32, 0, s>>>(b);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || nsplit == 1) return e;
     const size_t total = (size_t)a.natmtot * m.nradmax * m.nradmax * (s1 - s0);
