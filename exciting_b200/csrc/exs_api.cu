@@ -778,12 +778,17 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     if (c->relativity == EXS_REL_IORA) EXS_CUDA(exs::launch_iora_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_EV(1);
     const bool oz = c->prec_mode == EXS_PREC_OZAKI_INT8;
+    // configuration bit 4: B = h_a A and the APW-lo rows in native FP64 even
+    // when the H/O contraction is split
+    const bool b64 = !oz || (c->oz_cfg & 16);
     if (oz) {
         // slices of A; B = h_a A and the APW-lo rows of H from the slices of h_a and loa
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 2, s));
-        EXS_CUDA(exs::launch_oz_atom(c->oz_cfg, &c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles, u.nozatiles,
-                                     c->slices, c->kp8, c->oz_xseg, c->oz_atom_args(), s));
-    } else {
+        if (!b64)
+            EXS_CUDA(exs::launch_oz_atom(c->oz_cfg, &c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles,
+                                         u.nozatiles, c->slices, c->kp8, c->oz_xseg, c->oz_atom_args(), s));
+    }
+    if (b64) {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
                                        u.nwork[exs::EPI_PLANAR], u.d_k, s));
     }
@@ -800,7 +805,7 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
                                        u.nwork[exs::EPI_OVL], u.d_k, s));
     }
     EXS_EV(3);
-    if (!oz)
+    if (b64)
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_LOROWS, p, u.d_probs[exs::EPI_LOROWS], u.d_work[exs::EPI_LOROWS],
                                        u.nwork[exs::EPI_LOROWS], u.d_k, s));
     EXS_CUDA(exs::launch_olp_apwlo(p, u.d_k, (int)ks.size(), ngp_max, s));
@@ -901,6 +906,7 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
     int best_q = 0;
     for (int q = 0; q < exs::OZ_NCFG; q++) {
         if ((q & 8) && (q & 2)) continue;   // the two-SM tiles have no persistent form
+        if ((q & 16) && (q & 4)) continue;  // no per-atom int8 kernel to make persistent
         c->oz_cfg = q;
         Uploaded u{};                        // the tile list depends on the configuration
         rc = upload_tables(c, ks, u);
@@ -926,7 +932,10 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
     c->oz_cfg = best_q;
     c->oz_tuned[std::make_tuple((int)c->prec_mode, c->npad, c->K, c->slices)] = best_q;
     if (choice) *choice = best_q;
-    return EXS_OK;
+    // the outputs hold the last configuration's results: leave the chosen one's
+    EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
+    rc = run_setup(c, ks, false);
+    return rc < 0 ? rc : exs_synchronize(c);
 }
 
 int exs_set_kernel_config(exs_ctx *c, int cfg)

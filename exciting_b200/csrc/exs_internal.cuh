@@ -23,7 +23,7 @@ enum : int {
 };
 
 // Pipeline configurations of the split-precision kernel.
-constexpr int OZ_NCFG = 16;
+constexpr int OZ_NCFG = 32;
 // Modes of the split-precision kernel: H/O tiles, per-atom products (h_a A, loa A).
 enum : int { OZ_HO = 0, OZ_ATOM = 1 };
 

@@ -1076,8 +1076,11 @@ int oz_seg_pairs(int S, int kp8)
 // bit 1 = persistent launch (one CTA per SM) of the H/O tiles, bit 2 =
 // persistent launch of the per-atom tiles, bit 3 = two-SM H/O tiles (256 x 32
 // per CTA pair; bit 1 unused then)
-const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1};
-const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4};
+// bit 0 of a configuration: two 96 KB stages of 2 K chunks, or four 48 KB stages of 1
+const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1,
+                                 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1};
+const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4,
+                                 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4};
 
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
 {

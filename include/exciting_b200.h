@@ -288,8 +288,12 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
  * tiles instead of one block per tile, bit 2 the same for the per-atom
  * products (h_a A, APW-lo rows), bit 3 two-SM H/O tiles (a pair of blocks
  * computes 256 x 32 with the B operand split between them; bit 1 is then
- * ignored).  Every configuration gives bit-identical results. */
-#define EXS_OZ_NCONFIG 16
+ * ignored), bit 4 the products h_a A and the APW-lo rows of H in native
+ * FP64 (DMMA) instead of int8 slices (bit 2 is then ignored; only the H/O
+ * contraction stays split).  Configurations with the same bit 4 give
+ * bit-identical results; the two arithmetics for h_a A agree to FP64
+ * rounding. */
+#define EXS_OZ_NCONFIG 32
 int exs_set_kernel_config(exs_ctx *ctx, int config);
 
 /* CUDA graph of one batched device setup (no counterpart in the reference):
