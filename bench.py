@@ -291,7 +291,12 @@ def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, mode="auto", pinned=T
     value = ws * nk * args.steps / (float(t.item()) * 1e-3)
     h2d = ig.nbytes + vg.nbytes
     packed = mode == "packed" or (mode == "auto" and not pinned)
-    d2h = sum(2 * 16 * (m * (m + 1) // 2 if packed else m * m) for m in nmat)
+
+    def upper_bytes(m):   # rows 0 .. j0+63 of each block of 64 columns
+        return sum(16 * min(m, j0 + 64) * (min(m, j0 + 64) - j0) for j0 in range(0, m, 64))
+
+    d2h = sum(2 * (upper_bytes(m) if mode == "upper" else 16 * (m * (m + 1) // 2 if packed else m * m))
+              for m in nmat)
     st.set_host_copy_mode("auto")
     return value, h2d, d2h
 
@@ -558,6 +563,7 @@ def run_ours(args):
         e2e_modes = {
             "pinned_direct": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "direct")[0],
             "pinned_packed": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "packed")[0],
+            "pinned_upper": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "upper")[0],
             "pageable_direct": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "direct", False)[0],
             "pageable_packed": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "packed", False)[0],
         }

@@ -1212,7 +1212,7 @@ int exs_setup_batched_device(exs_ctx *c, int nk, const int *ngp, const int *igpi
 int exs_set_host_copy_mode(exs_ctx *c, int mode)
 {
     if (!c) return EXS_ERR_ARG;
-    if (mode < EXS_COPY_AUTO || mode > EXS_COPY_PACKED) return fail(c, EXS_ERR_ARG, "unknown host copy mode");
+    if (mode < EXS_COPY_AUTO || mode > EXS_COPY_UPPER) return fail(c, EXS_ERR_ARG, "unknown host copy mode");
     c->host_copy_mode = mode;
     return EXS_OK;
 }
@@ -1254,6 +1254,25 @@ void unpack_columns(const exs_complex *p, exs_complex *z, long n, long c0, long 
                 exs_complex v = pr[cc];
                 v.im = -v.im;
                 z[r + n * cc] = v;
+            }
+        }
+    }
+}
+
+// Rows c0+64 .. n-1 of columns c0 .. c0+63 of the Hermitian z (n x n,
+// column-major) from its upper part: z(r, c) = conj(z(c, r)), in 64 x 64
+// tiles (each source column segment z(c0 .. c0+63, r) is contiguous).
+void fill_lower_block(exs_complex *z, long n, long c0)
+{
+    const long c1 = std::min(n, c0 + 64);
+    for (long r0 = c0 + 64; r0 < n; r0 += 64) {
+        const long r1 = std::min(n, r0 + 64);
+        for (long c = c0; c < c1; c++) {
+            exs_complex *dst = z + n * c;
+            for (long r = r0; r < r1; r++) {
+                exs_complex v = z[c + n * r];
+                v.im = -v.im;
+                dst[r] = v;
             }
         }
     }
@@ -1326,6 +1345,7 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
     }
     cudaSetDevice(c->device);
     bool packed = c->host_copy_mode == EXS_COPY_PACKED;
+    const bool upper = c->host_copy_mode == EXS_COPY_UPPER;
     if (c->host_copy_mode == EXS_COPY_AUTO) {
         packed = false;
         for (int k = 0; k < nk && !packed; k++) packed = !host_pinned(h[k]) || !host_pinned(o[k]);
@@ -1359,6 +1379,10 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
             const int a = g * per, e = std::min(nb, a + per);
             return std::vector<KDesc>(all.begin() + a, all.begin() + e);
         };
+        if (upper && !c->pool) {
+            const unsigned hc = std::thread::hardware_concurrency();
+            c->pool = new exs::HostPool((int)std::max(1u, std::min(hc, 32u)) - 1);
+        }
         if (packed) {   // room for the largest group (2 matrices per k)
             size_t need = 0;
             for (int g = 0; g < G; g++) {
@@ -1402,6 +1426,22 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
                 for (const KDesc &k : cur) el += 2 * ((size_t)k.nmat * (k.nmat + 1) / 2);
                 EXS_CUDA(cudaMemcpyAsync(c->h_pack[g & 1], c->d_pack[g & 1], sizeof(exs_complex) * el,
                                          cudaMemcpyDeviceToHost, c->copy_stream));
+            } else if (upper) {   // rows 0 .. j0+63 of each block of 64 columns
+                for (size_t q = 0; q < cur.size(); q++) {
+                    const int kk = k0 + g * per + (int)q;
+                    const long n = cur[q].nmat;
+                    const size_t pitch = sizeof(exs_complex) * n;
+                    for (int w = 0; w < 2; w++) {
+                        const exs_complex *src = w == 0 ? cur[q].h : cur[q].o;
+                        exs_complex *dst = w == 0 ? h[kk] : o[kk];
+                        for (long j0 = 0; j0 < n; j0 += 64) {
+                            const long rows = std::min(n, j0 + 64), cols = std::min(n, j0 + 64) - j0;
+                            EXS_CUDA(cudaMemcpy2DAsync(dst + n * j0, pitch, src + n * j0, pitch,
+                                                       sizeof(exs_complex) * rows, cols, cudaMemcpyDeviceToHost,
+                                                       c->copy_stream));
+                        }
+                    }
+                }
             } else {
                 for (size_t q = 0; q < cur.size(); q++) {
                     const int kk = k0 + g * per + (int)q;
@@ -1411,6 +1451,24 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
                 }
             }
             EXS_CUDA(cudaEventRecord(c->ev_d2h[g & 1], c->copy_stream));
+            return EXS_OK;
+        };
+        // the lower parts of group g filled from the copied upper parts
+        auto fill = [&](int g) -> int {
+            EXS_CUDA(cudaEventSynchronize(c->ev_d2h[g & 1]));
+            std::vector<KDesc> cur = group(g);
+            struct Task {
+                exs_complex *z;
+                long n, c0;
+            };
+            std::vector<Task> tasks;
+            for (size_t q = 0; q < cur.size(); q++) {
+                const int kk = k0 + g * per + (int)q;
+                for (int w = 0; w < 2; w++)
+                    for (long c0 = 0; c0 + 64 < cur[q].nmat; c0 += 64)
+                        tasks.push_back(Task{w == 0 ? h[kk] : o[kk], cur[q].nmat, c0});
+            }
+            c->pool->parallel_for((int)tasks.size(), [&](int i) { fill_lower_block(tasks[i].z, tasks[i].n, tasks[i].c0); });
             return EXS_OK;
         };
         // the full matrices of group g rebuilt on the host threads
@@ -1454,6 +1512,9 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
                 // slot (g+1)&1 was last unpacked in iteration g-1: its copy may start now
                 if (g + 1 < G && (rc = copy_out(g + 1)) < 0) return rc;
                 if ((rc = unpack(g)) < 0) return rc;
+            } else if (upper) {
+                if (g + 1 < G && (rc = copy_out(g + 1)) < 0) return rc;
+                if ((rc = fill(g)) < 0) return rc;
             } else if (g + 1 < G && (rc = copy_out(g + 1)) < 0) {
                 return rc;
             }

@@ -380,10 +380,10 @@ class Setup:
         self._check(self.lib.exs_graph_create(*args, ctypes.byref(g)))
         return SetupGraph(self, g)
 
-    COPY_MODES = {"auto": 0, "direct": 1, "packed": 2}
+    COPY_MODES = {"auto": 0, "direct": 1, "packed": 2, "upper": 3}
 
     def set_host_copy_mode(self, mode: str):
-        """How the host-pointer calls bring H and O back: "auto", "direct" or "packed"."""
+        """How the host-pointer calls bring H and O back: "auto", "direct", "packed" or "upper"."""
         return self._check(self.lib.exs_set_host_copy_mode(self.ctx, self.COPY_MODES[mode]))
 
     def set_stream(self, stream_ptr: int | None):

@@ -192,11 +192,18 @@ int exs_synchronize(exs_ctx *ctx);
  *   EXS_COPY_PACKED  upper triangles packed on the device, half the bytes
  *                    over PCIe into pinned staging, full matrices rebuilt on
  *                    host threads (any caller memory);
+ *   EXS_COPY_UPPER   per block of 64 columns only the rows down to the
+ *                    block's last column copied into the caller's arrays
+ *                    (the upper triangle and the diagonal blocks, ~55 % of
+ *                    the bytes), the rest filled on host threads by
+ *                    conjugate transposes inside the same array (pinned
+ *                    caller memory);
  *   EXS_COPY_AUTO    DIRECT when every output array is pinned, else PACKED
  *                    (default). */
 #define EXS_COPY_AUTO 0
 #define EXS_COPY_DIRECT 1
 #define EXS_COPY_PACKED 2
+#define EXS_COPY_UPPER 3
 int exs_set_host_copy_mode(exs_ctx *ctx, int mode);
 
 /* The interstitial blocks alone: replaces

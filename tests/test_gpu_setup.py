@@ -144,7 +144,7 @@ def test_singular_matching_system_warns_and_keeps_rhs():
 
 
 def test_host_copy_modes_identical():
-    """Direct and packed transfers of H/O (pinned and pageable outputs) give the same bits."""
+    """Direct, packed and upper-part transfers of H/O (pinned and pageable outputs) give the same bits."""
     import torch
     s = W.si_cube8()
     gks = s.gksets()[:9]
@@ -163,7 +163,18 @@ def test_host_copy_modes_identical():
     nmat = [g.ngp + st.nlotot for g in gks]
     pin = [(torch.empty((m, m), dtype=torch.complex128).pin_memory(),
             torch.empty((m, m), dtype=torch.complex128).pin_memory()) for m in nmat]
-    st.set_host_copy_mode("packed")
-    got = st.setup_batched(gks, out=[(a.numpy().T, b.numpy().T) for a, b in pin])
+    for mode in ("packed", "upper"):
+        st.set_host_copy_mode(mode)
+        for a, b in pin:
+            a.fill_(float("nan"))
+            b.fill_(float("nan"))
+        got = st.setup_batched(gks, out=[(a.numpy().T, b.numpy().T) for a, b in pin])
+        for k in range(9):
+            assert np.array_equal(got[k][0], outs["direct"][k][0]), mode
+            assert np.array_equal(got[k][1], outs["direct"][k][1]), mode
+    # the upper-part transfer into pageable memory as well
+    st.set_host_copy_mode("upper")
+    up = st.setup_batched(gks)
     for k in range(9):
-        assert np.array_equal(got[k][0], outs["direct"][k][0])
+        for w in range(2):
+            assert np.array_equal(up[k][w], outs["direct"][k][w])
