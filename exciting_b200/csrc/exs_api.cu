@@ -181,6 +181,8 @@ int exs_ctx_destroy(exs_ctx *c)
     if (c->d_eval) cudaFree(c->d_eval);
     if (c->d_evec) cudaFree(c->d_evec);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->copy_stream2) cudaStreamDestroy(c->copy_stream2);
+    if (c->ev_copy2) cudaEventDestroy(c->ev_copy2);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return EXS_OK;
@@ -320,7 +322,9 @@ int exs_ctx_create(const exs_config *cfg, exs_ctx **out)
         return EXS_ERR_CUDA;
     }
     c->stream = c->own_stream;
-    if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    if ((e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->copy_stream2, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_copy2, cudaEventDisableTiming)) != cudaSuccess) {
         exs_ctx_destroy(c);
         return EXS_ERR_CUDA;
     }
@@ -1443,12 +1447,16 @@ int exs_setup_batched(exs_ctx *c, int nk, const int *ngp, const int *igpig, cons
                     }
                 }
             } else {
+                // H on one copy stream, O on a second one (two copy engines)
+                EXS_CUDA(cudaStreamWaitEvent(c->copy_stream2, c->ev_group[g & 1], 0));
                 for (size_t q = 0; q < cur.size(); q++) {
                     const int kk = k0 + g * per + (int)q;
                     const size_t bytes = sizeof(exs_complex) * (size_t)cur[q].nmat * cur[q].nmat;
                     EXS_CUDA(cudaMemcpyAsync(h[kk], cur[q].h, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
-                    EXS_CUDA(cudaMemcpyAsync(o[kk], cur[q].o, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+                    EXS_CUDA(cudaMemcpyAsync(o[kk], cur[q].o, bytes, cudaMemcpyDeviceToHost, c->copy_stream2));
                 }
+                EXS_CUDA(cudaEventRecord(c->ev_copy2, c->copy_stream2));
+                EXS_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_copy2, 0));
             }
             EXS_CUDA(cudaEventRecord(c->ev_d2h[g & 1], c->copy_stream));
             return EXS_OK;

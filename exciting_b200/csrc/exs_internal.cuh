@@ -235,6 +235,8 @@ struct exs_ctx {
     cudaStream_t stream = nullptr;      // stream the work runs on
     cudaStream_t own_stream = nullptr;  // the context's own stream
     cudaStream_t copy_stream = nullptr; // device-to-host copies of the host-facing calls
+    cudaStream_t copy_stream2 = nullptr; // a second copy engine's share (the overlaps of direct copies)
+    cudaEvent_t ev_copy2 = nullptr;
     cudaEvent_t ev_group[2] = {};
     cudaEvent_t ev[8] = {};
     double last_t[5] = {0, 0, 0, 0, 0};
