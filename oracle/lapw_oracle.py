@@ -71,6 +71,14 @@ def lib():
         L.orc_hmlint.restype = None
         L.orc_olprad.argtypes = [i, P, i, i, i, i, P, i, P, P, i, P, P, P, P, P, i, i, P, P, P, P, P]
         L.orc_olprad.restype = None
+        L.orc_clebgor.argtypes = [i] * 6
+        L.orc_clebgor.restype = d
+        L.orc_fderiv1.argtypes = [i, P, P, P]
+        L.orc_fderiv1.restype = None
+        L.orc_gradzfmtr.argtypes = [i, i, P, i, i, i, i, P, P]
+        L.orc_gradzfmtr.restype = None
+        L.orc_pmatrad.argtypes = [i, P, i, i, P, i, P, P, i, i, P, P, P, P, P, P, P, P]
+        L.orc_pmatrad.restype = None
         _LIB = L
     return _LIB
 
@@ -468,3 +476,107 @@ def rttddft_updateham(sys, gk, atot, pmat, overlap=None):
     for i in range(3):
         ham = ham + (a[i] / C_AU) * pmat[:, :, i]
     return ham, o
+
+
+# ---------------------------------------------------------------- momentum matrix elements
+def clebgor(j1, j2, j3, m1, m2, m3):
+    """src/src_lib/clebgor.f90: <j1 m1; j2 m2 | j3 m3>."""
+    return lib().orc_clebgor(j1, j2, j3, m1, m2, m3)
+
+
+def fderiv1(x, f):
+    """src/src_lib/fderiv.f90 with m = 1: the spline's first derivative at the points."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    g = np.zeros_like(f)
+    lib().orc_fderiv1(len(x), _p(x), _p(f), _p(g))
+    return g
+
+
+def gradzfmtr(lmax, r, l1, m1, fmt):
+    """src/src_xs/gradzfmtr.F90: gfmt(lmmax, nr, 3), the gradient of
+    fmt(r) Y_l1m1 expanded in Y_lm2 (x, y, z; the y entry is -i d/dy)."""
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    f = np.ascontiguousarray(fmt, dtype=np.float64)
+    lmmax = (lmax + 1) ** 2
+    g = np.zeros((lmmax, len(r), 3), order="F")
+    lib().orc_gradzfmtr(lmax, len(r), _p(r), l1, m1, lmmax, len(r), _p(f), _p(g))
+    return g
+
+
+def pmatrad(sys, rad):
+    """src/src_xs/pmatrad.F90: the radial-angular integrals <phi_1 | d/dx_j | phi_2>
+    of the APW and local-orbital functions (ripaa, ripalo, riploa, riplolo,
+    shapes as src/src_xs/src_rttddft/rttddft_pmat.f90:29-39 allocates them;
+    the m index of a local orbital stored at m + lolmax)."""
+    b, cr = sys.basis, sys.crystal
+    nat = cr.natmtot
+    A = _radial_args(sys, rad)
+    lmmax = (b.lmaxapw + 1) ** 2
+    nm = 2 * b.lolmax + 1
+    ao, nlo = b.apwordmax, b.nlomax
+    ripaa = np.zeros((ao, lmmax, ao, lmmax, nat, 3), order="F")
+    ripalo = np.zeros((ao, lmmax, nlo, nm, nat, 3), order="F")
+    riploa = np.zeros((nlo, nm, ao, lmmax, nat, 3), order="F")
+    riplolo = np.zeros((nlo, nm, nlo, nm, nat, 3), order="F")
+    lib().orc_pmatrad(nat, _p(A[0]), b.lmaxapw, ao, _p(A[1]), nlo, _p(A[2]), _p(A[3]), b.lolmax, rad.nrmtmax,
+                      _p(A[4]), _p(A[5]), _p(A[6]), _p(A[7]), _p(ripaa), _p(ripalo), _p(riploa), _p(riplolo))
+    return ripaa, ripalo, riploa, riplolo
+
+
+def _apw_cols(basis, is_):
+    """(io, lm) of the APW functions of a species, l <= lmaxapw, in the order
+    l, m, io of genpmatbasisik's loops."""
+    out = []
+    for l in range(basis.lmaxapw + 1):
+        for m in range(-l, l + 1):
+            for io in range(basis.apword[is_][l]):
+                out.append((io, l * (l + 1) + m))
+    return out
+
+
+def genpmatbasisik(sys, gk, apwalm, rip):
+    """pmat(nmat, nmat, 3) of one k-point, src/src_xs/src_rttddft/rttddft_pmat.f90:66-188:
+    per atom and direction the APW block conj(A) R A^T (zoutpr, :85-104), the
+    APW-lo columns, the lo-APW rows and the lo-lo block (:105-166); -i times
+    the x and z components (:170-171); then (k+G_j)_x Theta(G_i - G_j) on the
+    whole G+k block (:173-184)."""
+    ripaa, ripalo, riploa, riplolo = rip
+    b, cr = sys.basis, sys.crystal
+    ng = gk.ngp
+    nmat = sys.nmat(gk)
+    lol = b.lolmax
+    pm = np.zeros((nmat, nmat, 3), dtype=np.complex128, order="F")
+    for ias in range(cr.natmtot):
+        is_ = cr.atom_species[ias]
+        cols = _apw_cols(b, is_)
+        Am = np.stack([apwalm[:ng, io, lm, ias] for io, lm in cols], axis=1)        # (ng, F)
+        for j in range(3):
+            R = np.array([[ripaa[io1, lm1, io2, lm2, ias, j] for io2, lm2 in cols] for io1, lm1 in cols])
+            pm[:ng, :ng, j] += np.conj(Am) @ (R @ Am.T)
+        for ilo, l2 in enumerate(b.lorbl[is_]):
+            for m2 in range(-l2, l2 + 1):
+                c = ng + b.idxlo[l2 * (l2 + 1) + m2, ilo, ias] - 1
+                for j in range(3):
+                    rl = np.array([ripalo[io, lm, ilo, m2 + lol, ias, j] for io, lm in cols])
+                    pm[:ng, c, j] += np.conj(Am) @ rl
+                    rla = np.array([riploa[ilo, m2 + lol, io, lm, ias, j] for io, lm in cols])
+                    pm[c, :ng, j] += Am @ rla
+        for i1, l1 in enumerate(b.lorbl[is_]):
+            for m1 in range(-l1, l1 + 1):
+                r1 = ng + b.idxlo[l1 * (l1 + 1) + m1, i1, ias] - 1
+                for i2, l2 in enumerate(b.lorbl[is_]):
+                    for m2 in range(-l2, l2 + 1):
+                        r2 = ng + b.idxlo[l2 * (l2 + 1) + m2, i2, ias] - 1
+                        for j in range(3):
+                            pm[r1, r2, j] = riplolo[i1, m1 + lol, i2, m2 + lol, ias, j]
+    pm[:, :, 0] *= -1j
+    pm[:, :, 2] *= -1j
+    gv = sys.gv
+    iv = gv.ivg[:, gk.igpig - 1]                          # (3, ng)
+    diff = iv[:, :, None] - iv[:, None, :]                # (3, ng_i, ng_j)
+    ig = gv.ivgig_lookup(diff.reshape(3, -1)).reshape(ng, ng) - 1
+    th = np.asarray(sys.cfunig)[ig]
+    for j in range(3):
+        pm[:ng, :ng, j] += gk.vgpc[j][None, :] * th
+    return pm

@@ -956,3 +956,181 @@ void orc_olprad(int natmtot, const int *atom_species, int lmaxapw, int lmaxmat, 
 #undef LOFR
 #undef POT0
 }
+
+/* ======================================================================
+ * Momentum matrix elements of the LAPW+lo basis for real-time TDDFT:
+ * pmatrad (src/src_xs/pmatrad.F90) with gradzfmtr (src/src_xs/gradzfmtr.F90)
+ * and clebgor (src/src_lib/clebgor.f90).  The basis contraction
+ * (genpmatbasisik, src/src_xs/src_rttddft/rttddft_pmat.f90:66-188) is in
+ * lapw_oracle.py.
+ * ==================================================================== */
+
+/* src/src_lib/clebgor.f90 */
+double orc_clebgor(int j1, int j2, int j3, int m1, int m2, int m3)
+{
+    if (j1 == 0 && j2 == 0 && j3 == 0) return 1.0;
+    if (m1 + m2 - m3 != 0 || j2 + j3 < j1 || j1 + j3 < j2 || j1 + j2 < j3) return 0.0;
+    double c = sqrt((double)(2 * j3 + 1)) * orc_wigner3j(j1, j2, j3, m1, m2, -m3);
+    if ((j1 - j2 + m3) % 2 != 0) c = -c;
+    return c;
+}
+
+/* src/src_lib/fderiv.f90, m = 1: the first derivative of the spline at the points */
+void orc_fderiv1(int n, const double *x, const double *f, double *g)
+{
+    double *cf = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+    double *w = (double *)malloc(sizeof(double) * (size_t)n);
+    orc_spline(n, x, f, cf, w);
+    for (int i = 0; i < n; i++) g[i] = cf[3 * i];
+    free(cf);
+    free(w);
+}
+
+/* src/src_xs/gradzfmtr.F90: the gradient of f(r) Y_l1m1, expanded in Y_lm2
+ * (l2 = l1 +- 1 <= lmax): gfmt(ld1, nr, 3) (x, y, z) */
+void orc_gradzfmtr(int lmax, int nr, const double *r, int l1, int m1, int ld1, int ld2, const double *fmt,
+                          double *gfmt)
+{
+    const double s2 = sqrt(2.0);
+    double *g1 = (double *)malloc(sizeof(double) * nr);
+    for (size_t i = 0; i < (size_t)ld1 * ld2 * 3; i++) gfmt[i] = 0.0;
+    orc_fderiv1(nr, r, fmt, g1);
+    const double t1 = sqrt((double)(l1 + 1) / (double)(2 * l1 + 1));
+    const double t2 = sqrt((double)l1 / (double)(2 * l1 + 1));
+#define G(lm, ir, j) gfmt[(lm) + (size_t)ld1 * ((ir) + (size_t)ld2 * (j))]
+    int l2 = l1 + 1;
+    if (l2 <= lmax)
+        for (int m2 = -l2; m2 <= l2; m2++) {
+            const int lm2 = l2 * (l2 + 1) + m2;
+            const double t3 = orc_clebgor(l2, 1, l1, m2, -1, m1), t4 = orc_clebgor(l2, 1, l1, m2, 0, m1),
+                         t5 = orc_clebgor(l2, 1, l1, m2, 1, m1);
+            for (int ir = 0; ir < nr; ir++) {
+                const double tt2 = t1 * (fmt[ir] * (double)l1 / r[ir] - g1[ir]);
+                G(lm2, ir, 0) += ((t3 - t5) / s2) * tt2;
+                G(lm2, ir, 1) += ((-t3 - t5) / s2) * tt2;
+                G(lm2, ir, 2) += t4 * tt2;
+            }
+        }
+    l2 = l1 - 1;
+    if (l2 >= 0)
+        for (int m2 = -l2; m2 <= l2; m2++) {
+            const int lm2 = l2 * (l2 + 1) + m2;
+            const double t3 = orc_clebgor(l2, 1, l1, m2, -1, m1), t4 = orc_clebgor(l2, 1, l1, m2, 0, m1),
+                         t5 = orc_clebgor(l2, 1, l1, m2, 1, m1);
+            for (int ir = 0; ir < nr; ir++) {
+                const double tt2 = t2 * (fmt[ir] * (double)(l1 + 1) / r[ir] + g1[ir]);
+                G(lm2, ir, 0) += ((t3 - t5) / s2) * tt2;
+                G(lm2, ir, 1) += ((-t3 - t5) / s2) * tt2;
+                G(lm2, ir, 2) += t4 * tt2;
+            }
+        }
+#undef G
+    free(g1);
+}
+
+/* src/src_xs/pmatrad.F90: ripaa(apwordmax, lmmaxapw, apwordmax, lmmaxapw, natmtot, 3),
+ * ripalo(apwordmax, lmmaxapw, nlomax, 2 lolmax + 1, natmtot, 3),
+ * riploa(nlomax, 2 lolmax + 1, apwordmax, lmmaxapw, natmtot, 3),
+ * riplolo(nlomax, 2 lolmax + 1, nlomax, 2 lolmax + 1, natmtot, 3); the m index
+ * of a local orbital is stored at m + lolmax.  All outputs are overwritten. */
+void orc_pmatrad(int natmtot, const int *atom_species, int lmaxapw, int apwordmax, const int *apword, int nlomax,
+                 const int *nlorb, const int *lorbl, int lolmax, int nrmtmax, const int *nrmt, const double *spr,
+                 const double *apwfr, const double *lofr, double *ripaa, double *ripalo, double *riploa,
+                 double *riplolo)
+{
+    const int lmmax = (lmaxapw + 1) * (lmaxapw + 1), nm = 2 * lolmax + 1, ao = apwordmax;
+    const size_t naa = (size_t)ao * lmmax * ao * lmmax * natmtot, nal = (size_t)ao * lmmax * nlomax * nm * natmtot,
+                 nll = (size_t)nlomax * nm * nlomax * nm * natmtot;
+    memset(ripaa, 0, sizeof(double) * naa * 3);
+    memset(ripalo, 0, sizeof(double) * nal * 3);
+    memset(riploa, 0, sizeof(double) * nal * 3);
+    memset(riplolo, 0, sizeof(double) * nll * 3);
+#define APWFR(ir, io, l, ias) apwfr[(ir) + (size_t)nrmtmax * (2 * ((io) + (size_t)ao * ((l) + (size_t)(lmaxapw + 1) * (ias))))]
+#define LOFR(ir, ilo, ias) lofr[(ir) + (size_t)nrmtmax * (2 * ((ilo) + (size_t)nlomax * (ias)))]
+    /* dapwfr(lmmax, nrmtmax, 3, apwordmax, lmmax), dlofr(lmmax, nrmtmax, 3, nlomax, nm) */
+    const size_t gsz = (size_t)lmmax * nrmtmax * 3;
+    double *dapw = (double *)calloc(gsz * ao * lmmax, sizeof(double));
+    double *dlo = (double *)calloc(gsz * nlomax * nm, sizeof(double));
+    double *fr = (double *)malloc(sizeof(double) * nrmtmax);
+#define DAPW(lm1, ir, j, io, lm) dapw[(lm1) + (size_t)lmmax * ((ir) + (size_t)nrmtmax * ((j) + 3 * ((io) + (size_t)ao * (lm))))]
+#define DLO(lm1, ir, j, ilo, m) dlo[(lm1) + (size_t)lmmax * ((ir) + (size_t)nrmtmax * ((j) + 3 * ((ilo) + (size_t)nlomax * (m))))]
+#define RAA(io1, lm1, io2, lm3, ias, j) \
+    ripaa[(io1) + (size_t)ao * ((lm1) + (size_t)lmmax * ((io2) + (size_t)ao * ((lm3) + (size_t)lmmax * ((ias) + (size_t)natmtot * (j)))))]
+#define RAL(io1, lm1, ilo, m, ias, j) \
+    ripalo[(io1) + (size_t)ao * ((lm1) + (size_t)lmmax * ((ilo) + (size_t)nlomax * ((m) + (size_t)nm * ((ias) + (size_t)natmtot * (j)))))]
+#define RLA(ilo, m, io2, lm3, ias, j) \
+    riploa[(ilo) + (size_t)nlomax * ((m) + (size_t)nm * ((io2) + (size_t)ao * ((lm3) + (size_t)lmmax * ((ias) + (size_t)natmtot * (j)))))]
+#define RLL(i1, m1, i2, m2, ias, j) \
+    riplolo[(i1) + (size_t)nlomax * ((m1) + (size_t)nm * ((i2) + (size_t)nlomax * ((m2) + (size_t)nm * ((ias) + (size_t)natmtot * (j)))))]
+    for (int ias = 0; ias < natmtot; ias++) {
+        const int is = atom_species[ias], nr = nrmt[is];
+        const double *r = spr + (size_t)nrmtmax * is;
+        const int *apw = apword + (size_t)(lmaxapw + 1) * is;
+        const int *lol = lorbl + (size_t)nlomax * is;
+        memset(dapw, 0, sizeof(double) * gsz * ao * lmmax);
+        memset(dlo, 0, sizeof(double) * gsz * nlomax * nm);
+        for (int l1 = 0; l1 <= lmaxapw; l1++)
+            for (int m1 = -l1; m1 <= l1; m1++)
+                for (int io = 0; io < apw[l1]; io++)
+                    orc_gradzfmtr(lmaxapw, nr, r, l1, m1, lmmax, nrmtmax, &APWFR(0, io, l1, ias),
+                                  &DAPW(0, 0, 0, io, l1 * (l1 + 1) + m1));
+        for (int ilo = 0; ilo < nlorb[is]; ilo++)
+            for (int m1 = -lol[ilo]; m1 <= lol[ilo]; m1++)
+                orc_gradzfmtr(lmaxapw, nr, r, lol[ilo], m1, lmmax, nrmtmax, &LOFR(0, ilo, ias),
+                              &DLO(0, 0, 0, ilo, m1 + lolmax));
+        for (int l1 = 0; l1 <= lmaxapw; l1++)
+            for (int m1 = -l1; m1 <= l1; m1++) {
+                const int lm1 = l1 * (l1 + 1) + m1;
+                for (int io1 = 0; io1 < apw[l1]; io1++) {
+                    for (int l3 = 0; l3 <= lmaxapw; l3++)
+                        for (int m3 = -l3; m3 <= l3; m3++)
+                            for (int io2 = 0; io2 < apw[l3]; io2++)
+                                for (int j = 0; j < 3; j++) {
+                                    const int lm3 = l3 * (l3 + 1) + m3;
+                                    for (int ir = 0; ir < nr; ir++)
+                                        fr[ir] = r[ir] * r[ir] * APWFR(ir, io1, l1, ias) * DAPW(lm1, ir, j, io2, lm3);
+                                    RAA(io1, lm1, io2, lm3, ias, j) = orc_fint(nr, r, fr);
+                                }
+                    for (int ilo = 0; ilo < nlorb[is]; ilo++)
+                        for (int m3 = -lol[ilo]; m3 <= lol[ilo]; m3++)
+                            for (int j = 0; j < 3; j++) {
+                                for (int ir = 0; ir < nr; ir++)
+                                    fr[ir] = r[ir] * r[ir] * APWFR(ir, io1, l1, ias) * DLO(lm1, ir, j, ilo, m3 + lolmax);
+                                RAL(io1, lm1, ilo, m3 + lolmax, ias, j) = orc_fint(nr, r, fr);
+                            }
+                }
+            }
+        for (int ilo = 0; ilo < nlorb[is]; ilo++) {
+            const int l1 = lol[ilo];
+            for (int m1 = -l1; m1 <= l1; m1++) {
+                const int lm1 = l1 * (l1 + 1) + m1;
+                for (int l3 = 0; l3 <= lmaxapw; l3++)
+                    for (int m3 = -l3; m3 <= l3; m3++)
+                        for (int io2 = 0; io2 < apw[l3]; io2++)
+                            for (int j = 0; j < 3; j++) {
+                                for (int ir = 0; ir < nr; ir++)
+                                    fr[ir] = r[ir] * r[ir] * LOFR(ir, ilo, ias) * DAPW(lm1, ir, j, io2, l3 * (l3 + 1) + m3);
+                                RLA(ilo, m1 + lolmax, io2, l3 * (l3 + 1) + m3, ias, j) = orc_fint(nr, r, fr);
+                            }
+                for (int ilo2 = 0; ilo2 < nlorb[is]; ilo2++)
+                    for (int m3 = -lol[ilo2]; m3 <= lol[ilo2]; m3++)
+                        for (int j = 0; j < 3; j++) {
+                            for (int ir = 0; ir < nr; ir++)
+                                fr[ir] = r[ir] * r[ir] * LOFR(ir, ilo, ias) * DLO(lm1, ir, j, ilo2, m3 + lolmax);
+                            RLL(ilo, m1 + lolmax, ilo2, m3 + lolmax, ias, j) = orc_fint(nr, r, fr);
+                        }
+            }
+        }
+    }
+    free(dapw);
+    free(dlo);
+    free(fr);
+#undef APWFR
+#undef LOFR
+#undef DAPW
+#undef DLO
+#undef RAA
+#undef RAL
+#undef RLA
+#undef RLL
+}
