@@ -421,7 +421,22 @@ def rttddft_leg(args, st, stream, torch, ngp, nmat, d_ig, d_vg, hp, op, step_dev
         dt = time.perf_counter() - t0
         cpu = {"value": 2 / dt, "unit": "k-points/s", "cores": os.cpu_count(), "kind": "port",
                "sample": f"2 k-points in {dt:.2f} s by the oracle (setup restatement + the combination)"}
+    # momentum matrices generated on the device (once per propagation), 9 k-points
+    gen = None
+    if gks is not None:
+        from exciting_b200 import workloads as W
+        rad = W.mt_radial(sys_)
+        sub = gks[:9]
+        al = [st.match(g)[0] for g in sub]
+        st.rttddft_genpmat(sub, al, rad, outputs=False)          # warm-up (cuBLAS handle, buffers)
+        t0 = time.perf_counter()
+        st.rttddft_genpmat(sub, al, rad, outputs=False)
+        dt = time.perf_counter() - t0
+        gen = {"value": len(sub) / dt, "unit": "k-points/s", "ms": dt * 1e3, "k_points": len(sub),
+               "note": "exs_rttddft_genpmat (pmatrad + genpmatbasisik), host matching coefficients in, "
+                       "wall clock of the synchronous call"}
     return {"value": len(nmat) / (t_rt * 1e-3), "unit": "k-points/s", "ms_per_step": t_rt, "cpu_baseline": cpu,
+            "genpmat": gen,
             "setup_ms_per_step": t_setup,
             "combine": {"kernel": "rt_combine_kernel", "ms_per_step": comb_ms, "bytes_per_step": nbytes,
                         "achieved": nbytes / (comb_ms * 1e-3) / 1e9, "unit": "GB/s", "peak": _hbm_peak(),

@@ -80,6 +80,8 @@ SIGNATURES = {
     "exs_rttddft_set_pmat": ([P, c_int, P, P, c_int], c_int),
     "exs_rttddft_updateham": ([P, c_int, P, P, P, P, c_int, P, P, c_int], c_int),
     "exs_rttddft_updateham_device": ([P, c_int, P, P, P, P, c_int, P, P, P], c_int),
+    "exs_rttddft_genpmat": ([P, c_int, P, P, P, P, P, P, c_int], c_int),
+    "exs_clebgor_unit": ([c_int] * 5 + [P], c_int),
     "exs_gauntyry": ([c_int] * 6 + [P], c_int),
     "exs_fderiv_int": ([c_int, P, P, P], c_int),
 }

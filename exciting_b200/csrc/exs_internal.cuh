@@ -202,6 +202,7 @@ struct exs_ctx {
     bool have_olp = false;               // oalo, ololo (h1*) on the device came from exs_olprad
     // real-time TDDFT Hamiltonian update (rttddft.cu): momentum matrices, work space
     void *rt = nullptr;
+    void *pm = nullptr;                  // momentum-matrix generation (pmat.cu)
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
@@ -266,6 +267,9 @@ void solver_release(exs_ctx *c);
 void mt_release(exs_ctx *c);
 // Real-time TDDFT Hamiltonian update (rttddft.cu)
 void rt_release(exs_ctx *c);
+int rt_reserve_pmat(exs_ctx *c, int nk, const int *nmat, exs_complex **d_p, size_t *off);
+// Momentum-matrix generation (pmat.cu)
+void pm_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)

@@ -131,6 +131,25 @@ int launch_combine(exs_ctx *c, int nk, const int *nmat, exs_complex *const *h, c
 }  // namespace
 
 namespace exs {
+// Storage for the momentum matrices of nk k-points, (nmat_k, nmat_k, 3)
+// each, registered as exs_rttddft_set_pmat registers them; returns the
+// device base and the per-k-point element offsets.
+int rt_reserve_pmat(exs_ctx *c, int nk, const int *nmat, exs_complex **d_p, size_t *off)
+{
+    RtState *r = state(c);
+    RT_CUDA(cudaStreamSynchronize(c->stream));
+    r->p_off.assign(nk, 0);
+    r->p_nmat.assign(nmat, nmat + nk);
+    size_t tot = 0;
+    for (int k = 0; k < nk; k++) {
+        r->p_off[k] = off[k] = tot;
+        tot += 3 * (size_t)nmat[k] * nmat[k];
+    }
+    RT_CUDA(grow(&r->d_p, &r->p_cap, tot));
+    *d_p = r->d_p;
+    return EXS_OK;
+}
+
 void rt_release(exs_ctx *c)
 {
     RtState *r = (RtState *)c->rt;

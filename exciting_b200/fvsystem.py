@@ -283,6 +283,27 @@ class Setup:
         ptrs = (ctypes.c_void_p * len(blocks))(*[b.ctypes.data for b in blocks])
         self._check(self.lib.exs_rttddft_set_pmat(self.ctx, len(blocks), _ptr(nmat), ptrs, ld))
 
+    def rttddft_genpmat(self, gks, apwalms, rad, *, outputs: bool = True):
+        """Momentum matrices of the k-points in gks on the device
+        (exs_rttddft_genpmat), registered for rttddft_updateham; apwalms: one
+        (ngkmax, apwordmax, lmmaxapw, natmtot) array per k-point (as match
+        returns them).  Returns the (nmat, nmat, 3) arrays when ``outputs``."""
+        nk = len(gks)
+        ngp, ig, vg = self._k_arrays(gks)
+        al = [np.asfortranarray(a, dtype=np.complex128) for a in apwalms]
+        apwfr, lofr = _f(rad.apwfr, np.float64), _f(rad.lofr, np.float64)
+        r, keep = self._mt_radial(rad, apwfr.ctypes.data, lofr.ctypes.data if lofr.size else None, None)
+        nmat = [g.ngp + self.nlotot for g in gks]
+        ld = max(nmat)
+        outs = [np.zeros((ld, ld, 3), dtype=np.complex128, order="F") for _ in gks] if outputs else None
+        ap = (ctypes.c_void_p * nk)(*[a.ctypes.data for a in al])
+        op = (ctypes.c_void_p * nk)(*[o.ctypes.data for o in outs]) if outputs else None
+        self._check(self.lib.exs_rttddft_genpmat(self.ctx, nk, _ptr(ngp), _ptr(ig), _ptr(vg), ap, ctypes.byref(r),
+                                                 op, ld))
+        if not outputs:
+            return None
+        return [o[: n, : n, :] for o, n in zip(outs, nmat)]
+
     def rttddft_updateham(self, gks, atot, calculate_overlap=True, overlap=None):
         """UpdateHam's k-loop: returns (ham_time, overlap) lists of (nmat, nmat)
         arrays; with calculate_overlap False, ``overlap`` (one array per

@@ -276,6 +276,25 @@ int exs_rttddft_updateham_device(exs_ctx *ctx, int nk, const int *ngp_host, cons
                                  exs_complex *const *pmat_dev, exs_complex *const *h_dev,
                                  exs_complex *const *o_dev);
 
+/* Replaces Obtain_Pmat_LAPWLOBasis (src/src_xs/src_rttddft/rttddft_pmat.f90:
+ * 22-64: pmatrad, then genpmatbasisik per k-point): the momentum matrix
+ * elements pmat(1:nmat, 1:nmat, 1:3) of nk k-points, -i<phi|d/dx_j|phi'> in
+ * the LAPW+lo basis with the interstitial (k+G')_j Theta(G - G') term,
+ * computed on the device and registered for exs_rttddft_updateham as
+ * exs_rttddft_set_pmat registers them.  apwalm[ik]: HOST matching
+ * coefficients (ngkmax, apwordmax, lmmaxapw, natmtot) of the k-point (as
+ * exs_match returns them); *in: the radial functions apwfr, lofr on the
+ * meshes spr, nrmt (host; lmaxvr and veffmt unused); ngp, igpig, vgpc as
+ * exs_setup_batched.  pmat: NULL, or nk HOST pointers (entries may be NULL)
+ * to (ld, ld, 3) arrays that receive a copy.  Synchronous. */
+int exs_rttddft_genpmat(exs_ctx *ctx, int nk, const int *ngp, const int *igpig, const double *vgpc,
+                        const exs_complex *const *apwalm, const exs_mt_radial *in,
+                        exs_complex *const *pmat, int ld);
+/* Host utility of the above, callable without a GPU: the vector-coupling
+ * coefficient <l2 m2; 1 q | l m> for l = l2 +- 1 (clebgor(l2, 1, l, m2, q, m),
+ * src/src_lib/clebgor.f90, as gradzfmtr uses it), else 0. */
+int exs_clebgor_unit(int l2, int m2, int q, int l, int m, double *value);
+
 /* Autotuner (no counterpart in the reference): runs the batch described as
  * for exs_setup_batched_device once per kernel configuration of the active
  * precision mode (for the split-precision contraction: K chunks per

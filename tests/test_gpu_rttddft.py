@@ -104,3 +104,26 @@ def test_device_entry_equals_host_entry():
         h = d_h[k].cpu().numpy().view(np.complex128).reshape(n, n, order="F")
         o = d_o[k].cpu().numpy().view(np.complex128).reshape(n, n, order="F")
         assert np.array_equal(h, ham[k]) and np.array_equal(o, ovl[k])
+
+
+@pytest.mark.parametrize("variant", ["shipped", "text"])
+def test_genpmat_vs_oracle(variant):
+    """Momentum matrices on the device (exs_rttddft_genpmat) against the
+    oracle's pmatrad + genpmatbasisik, same matching coefficients."""
+    s = W.si_fcc(variant)
+    rad = W.mt_radial(s, lmaxvr=2)
+    gks = s.gksets()[:2]
+    st = _setup(s, max_batch=len(gks))
+    al = [st.match(g)[0] for g in gks]
+    pm = st.rttddft_genpmat(gks, al, rad)
+    rip = O.pmatrad(s, rad)
+    for k, g in enumerate(gks):
+        ref = O.genpmatbasisik(s, g, al[k], rip)
+        for j in range(3):
+            assert rel(pm[k][:, :, j], ref[:, :, j]) <= 1e-12, (k, j, rel(pm[k][:, :, j], ref[:, :, j]))
+    # the registered matrices drive the update
+    atot = np.array([0.4, -1.1, 0.9])
+    ham, _ = st.rttddft_updateham(gks, atot)
+    for k, g in enumerate(gks):
+        hr, _ = O.rttddft_updateham(s, g, atot, O.genpmatbasisik(s, g, al[k], rip))
+        assert rel(ham[k], hr) <= 1e-12

@@ -70,3 +70,22 @@ def test_fderiv_int_rejects_short_meshes():
     rc = _lib().exs_fderiv_int(3, x.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p),
                                ctypes.byref(out))
     assert rc != 0
+
+
+def test_unit_coupling_coefficients_match_oracle():
+    """The closed forms behind exs_rttddft_genpmat's gradient coefficients
+    against the oracle's clebgor (Racah formula), l <= 9."""
+    out = ctypes.c_double()
+    worst = 0.0
+    for l2 in range(0, 10):
+        for l in (l2 - 1, l2 + 1):
+            if l < 0:
+                continue
+            for m2 in range(-l2, l2 + 1):
+                for q in (-1, 0, 1):
+                    m = m2 + q
+                    if abs(m) > l:
+                        continue
+                    assert _lib().exs_clebgor_unit(l2, m2, q, l, m, ctypes.byref(out)) == 0
+                    worst = max(worst, abs(out.value - O.clebgor(l2, 1, l, m2, q, m)))
+    assert worst < 1e-15
