@@ -556,6 +556,7 @@ int exs_last_timings(exs_ctx *c, double *t, int n)
 {
     if (!c || !t) return EXS_ERR_ARG;
     for (int i = 0; i < n && i < 5; i++) t[i] = c->last_t[i];
+    if (n > 5) t[5] = exs::rt_combine_ms(c);
     return EXS_OK;
 }
 

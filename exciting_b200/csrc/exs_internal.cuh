@@ -268,6 +268,7 @@ void mt_release(exs_ctx *c);
 // Real-time TDDFT Hamiltonian update (rttddft.cu)
 void rt_release(exs_ctx *c);
 int rt_reserve_pmat(exs_ctx *c, int nk, const int *nmat, exs_complex **d_p, size_t *off);
+double rt_combine_ms(exs_ctx *c);
 // Momentum-matrix generation (pmat.cu)
 void pm_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)

@@ -82,6 +82,9 @@ struct RtState {
     int *d_ig = nullptr;
     double *d_vg = nullptr;
     size_t kv_cap = 0;
+    // device time of the last combination (CUDA events around its launches)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
 };
 
 template <class T>
@@ -150,10 +153,25 @@ int rt_reserve_pmat(exs_ctx *c, int nk, const int *nmat, exs_complex **d_p, size
     return EXS_OK;
 }
 
+// Device milliseconds of the last combination (0 if none); waits for it.
+double rt_combine_ms(exs_ctx *c)
+{
+    RtState *r = (RtState *)c->rt;
+    if (!r || !r->timed) return 0.0;
+    float ms = 0.f;
+    if (cudaEventSynchronize(r->ev1) != cudaSuccess || cudaEventElapsedTime(&ms, r->ev0, r->ev1) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0.0;
+    }
+    return ms;
+}
+
 void rt_release(exs_ctx *c)
 {
     RtState *r = (RtState *)c->rt;
     if (!r) return;
+    if (r->ev0) cudaEventDestroy(r->ev0);
+    if (r->ev1) cudaEventDestroy(r->ev1);
     void *ps[] = {r->d_p, r->d_h, r->d_o, r->d_o2, r->d_ig, r->d_vg};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -221,7 +239,16 @@ int exs_rttddft_updateham_device(exs_ctx *c, int nk, const int *ngp_host, const 
     int rc = exs_setup_batched_device(c, nk, ngp_host, igpig_dev, vgpc_dev, h_dev, o_setup.data());
     if (rc != EXS_OK) return rc;
     std::vector<const exs_complex *> oc(o_dev, o_dev + nk), pc(pmat_dev, pmat_dev + nk);
-    return launch_combine(c, nk, nmat.data(), h_dev, oc.data(), pc.data(), atot, c->stream);
+    if (!r->ev0) {
+        RT_CUDA(cudaEventCreate(&r->ev0));
+        RT_CUDA(cudaEventCreate(&r->ev1));
+    }
+    RT_CUDA(cudaEventRecord(r->ev0, c->stream));
+    rc = launch_combine(c, nk, nmat.data(), h_dev, oc.data(), pc.data(), atot, c->stream);
+    if (rc != EXS_OK) return rc;
+    RT_CUDA(cudaEventRecord(r->ev1, c->stream));
+    r->timed = true;
+    return EXS_OK;
 }
 
 int exs_rttddft_updateham(exs_ctx *c, int nk, const int *ngp, const int *igpig, const double *vgpc,

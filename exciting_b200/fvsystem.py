@@ -415,8 +415,10 @@ class Setup:
         return self._check(self.lib.exs_synchronize(self.ctx))
 
     def last_timings(self):
-        t = np.zeros(5)
-        self.lib.exs_last_timings(self.ctx, _ptr(t), 5)
+        """Device ms of the last setup's phases (match, h_a A, MT + interstitial,
+        lo blocks, total) and of the last RT-TDDFT combination."""
+        t = np.zeros(6)
+        self.lib.exs_last_timings(self.ctx, _ptr(t), 6)
         return t
 
     def forcek(self, gk, evecfv, evalfv, occsv, wkpt, forceibs=None):

@@ -382,7 +382,8 @@ int exs_adjoint(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc, int
 int exs_set_stream(exs_ctx *ctx, void *stream);
 
 /* Device time of the phases of the last setup call, milliseconds:
- * t[0] match, t[1] h_a A, t[2] MT contraction + interstitial, t[3] lo blocks, t[4] total. */
+ * t[0] match, t[1] h_a A, t[2] MT contraction + interstitial, t[3] lo blocks, t[4] total;
+ * with n > 5, t[5] the field/momentum combination of the last RT-TDDFT update. */
 int exs_last_timings(exs_ctx *ctx, double *t, int n);
 
 /* For callers that cannot allocate device memory (no exs_ctx: creating one
