@@ -106,12 +106,18 @@ def test_device_entry_equals_host_entry():
         assert np.array_equal(h, ham[k]) and np.array_equal(o, ovl[k])
 
 
-@pytest.mark.parametrize("variant", ["shipped", "text"])
+@pytest.mark.parametrize("variant", ["shipped", "text", "two_species"])
 def test_genpmat_vs_oracle(variant):
     """Momentum matrices on the device (exs_rttddft_genpmat) against the
-    oracle's pmatrad + genpmatbasisik, same matching coefficients."""
-    s = W.si_fcc(variant)
-    rad = W.mt_radial(s, lmaxvr=2)
+    oracle's pmatrad + genpmatbasisik, same matching coefficients; the
+    two-species cell has different bases per species, lmaxmat < lmaxapw and
+    radial meshes of 300 and 250 points."""
+    if variant == "two_species":
+        s = W.sic_two_species()
+        rad = W.mt_radial(s, lmaxvr=2, nrmt=[300, 250])
+    else:
+        s = W.si_fcc(variant)
+        rad = W.mt_radial(s, lmaxvr=2)
     gks = s.gksets()[:2]
     st = _setup(s, max_batch=len(gks))
     al = [st.match(g)[0] for g in gks]
