@@ -733,7 +733,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
 // K byte.  CTA 0 issues the MMAs; its full barriers count the bytes of both
 // CTAs' copies (the copies of CTA 1 signal CTA 0's barrier); MMA completion
 // is signalled to both CTAs (multicast commit); both CTAs' epilogues fold
-// their own 128 rows and report to CTA 0's barrier.  No TMA multicast.
+// their own 128 rows and report to CTA 0's barrier.  Each CTA loads its own operands.
 constexpr uint32_t OZ_PEER_BIT_MASK = 0xFEFFFFFFu;   // shared::cluster address of CTA 0's copy
 
 __device__ __forceinline__ uint32_t cluster_ctarank()
