@@ -223,7 +223,7 @@ constexpr int SG = 8;    // potential channels per block of mt_radial_kernel
 // ranges of 32-point chunks, and the block writes its partial sums to rpart
 // (mt_reduce_kernel adds them in a fixed order).
 template <int T>
-__global__ void __launch_bounds__(8 * T) mt_radial_kernel(MtArgs a)
+__global__ void __launch_bounds__(8 * T, T == 16 ? 4 : (T == 24 ? 3 : 2)) mt_radial_kernel(MtArgs a)
 {
     constexpr int KP = T / 8, NT = 8 * T;
     const int ias = blockIdx.z, grp = blockIdx.y / a.nsplit + a.g0, split = blockIdx.y % a.nsplit;
