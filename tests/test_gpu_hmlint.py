@@ -170,3 +170,22 @@ def test_keep_olp_without_olprad_is_an_error():
     st = _setup(s)
     with pytest.raises(ExsError):
         st.set_scf_inputs(keep_olp=True)
+
+
+def test_hmlint_argument_errors():
+    """Sizes outside the documented ranges are rejected with EXS_ERR_SIZE and
+    leave the context usable."""
+    from exciting_b200.abi import ExsError
+    s = W.si_fcc("text")
+    st = _setup(s)
+    rad = W.mt_radial(s, lmaxvr=2)
+    bad = copy.copy(rad)
+    bad.nrmt = np.array([rad.nrmtmax + 1], dtype=np.int32)
+    with pytest.raises(ExsError) as e:
+        st.hmlint(bad)
+    assert e.value.code == -3 or "nrmt" in str(e.value)
+    bad = copy.copy(rad)
+    bad.lmaxvr = -1
+    with pytest.raises(ExsError):
+        st.olprad(bad)
+    _check(st.hmlint(rad), O.hmlint(s, rad))                 # still works afterwards

@@ -133,3 +133,22 @@ def test_genpmat_vs_oracle(variant):
     for k, g in enumerate(gks):
         hr, _ = O.rttddft_updateham(s, g, atot, O.genpmatbasisik(s, g, al[k], rip))
         assert rel(ham[k], hr) <= 1e-12
+
+
+def test_rttddft_argument_errors():
+    """The update without registered momentum matrices, a batch above
+    max_batch and mismatched sizes are rejected; the context stays usable."""
+    from exciting_b200.abi import ExsError
+    s = W.si_fcc("shipped")
+    gks = s.gksets()[:3]
+    st = _setup(s, max_batch=2)
+    with pytest.raises(ExsError):
+        st.rttddft_updateham(gks[:2], np.zeros(3))           # nothing registered yet
+    with pytest.raises(ExsError):
+        st.rttddft_set_pmat([_pmat(g.ngp + st.nlotot, 0) for g in gks])   # 3 > max_batch
+    st.rttddft_set_pmat([_pmat(g.ngp + st.nlotot, 0) for g in gks[:2]])
+    with pytest.raises(ExsError):
+        st.rttddft_updateham([gks[1], gks[0]], np.zeros(3))  # nmat differs from the registered one
+    ham, _ = st.rttddft_updateham(gks[:2], np.zeros(3))
+    ref = st.setup_batched(gks[:2])
+    assert np.array_equal(ham[0], ref[0][0])
