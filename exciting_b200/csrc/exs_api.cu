@@ -123,6 +123,7 @@ exs::DevParams exs_ctx::params() const
     p.idxlo = d_idxlo;
     p.lorbl = d_lorbl;
     p.nlorb = d_nlorb;
+    p.dlu = d_dlu;
     p.err = d_err;
     return p;
 }
@@ -148,7 +149,7 @@ int exs_ctx_destroy(exs_ctx *c)
     void *dev[] = {c->d_atoms, c->d_apword, c->d_ivg, c->d_ivgig, c->d_idxlo, c->d_lorbl, c->d_nlorb, c->d_rmt,
                    c->d_haa_r, c->d_haa_i, c->d_loa_r, c->d_loa_i, c->d_lolo, c->d_oalo, c->d_ololo, c->d_h1aa,
                    c->d_h1loa, c->d_h1lolo, c->d_veffig, c->d_kinw, c->d_cfunig, c->d_m2effig, c->d_spr_tail,
-                   c->d_apwfr_tail, c->d_work, c->d_ho, c->d_igpig, c->d_vgpc, c->d_err, c->d_tables,
+                   c->d_apwfr_tail, c->d_dlu, c->d_work, c->d_ho, c->d_igpig, c->d_vgpc, c->d_err, c->d_tables,
                    c->d_match_in, c->d_match_sf, c->d_apwalm};
     for (void *p : dev)
         if (p) cudaFree(p);
@@ -508,6 +509,9 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
     EXS_CUDA(upload(&c->d_spr_tail, in->spr_tail, (size_t)c->np_tail * c->nspecies, s));
     EXS_CUDA(upload(&c->d_apwfr_tail, in->apwfr_tail,
                     (size_t)c->np_tail * c->apwordmax * (c->lmaxapw + 1) * nat, s));
+    // the matching systems D_l depend only on the tails: factorised once here
+    if (!c->d_dlu) EXS_CUDA(dalloc(&c->d_dlu, (size_t)nat * (c->lmaxapw + 1) * exs::DLU_STRIDE));
+    EXS_CUDA(exs::launch_match_dlu(c->params(), c->d_dlu, s));
     if (c->prec_mode == EXS_PREC_OZAKI_INT8)   // slices of the new h_a and loa, in place
         EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->slices, s));
     EXS_CUDA(cudaStreamSynchronize(s));

@@ -76,6 +76,10 @@ struct KDesc {
 };
 
 // Constant per-context device parameters passed by value to kernels.
+// Per (atom, l) entry of DevParams::dlu: the n x n LU factors of D_l
+// (n <= EXS_APWORD_MAX = 3), the pivots and the factorisation's info.
+constexpr int DLU_STRIDE = 13;
+
 struct DevParams {
     int natmtot, lmaxapw, lmaxmat, apwordmax, lmmaxapw, np_tail;
     int ngkmax, npad, K, Kpad;
@@ -104,6 +108,7 @@ struct DevParams {
     const int *idxlo;            // (lolmmax, nlomax, natmtot), 1-based values
     const int *lorbl;            // (nlomax, nspecies)
     const int *nlorb;            // nspecies
+    const double *dlu;           // LU factors of D_l per (atom, l): [ias][l][DLU_STRIDE]
     int *err;                    // device error flags
 };
 
@@ -166,6 +171,7 @@ struct exs_ctx {
     double *d_oalo = nullptr, *d_ololo = nullptr, *d_h1aa = nullptr, *d_h1loa = nullptr, *d_h1lolo = nullptr;
     exs_complex *d_veffig = nullptr, *d_kinw = nullptr, *d_cfunig = nullptr, *d_m2effig = nullptr;
     double *d_spr_tail = nullptr, *d_apwfr_tail = nullptr;
+    double *d_dlu = nullptr;         // LU factors of the matching systems D_l (from the tails)
     // work space (max_batch slots)
     size_t plane = 0;            // Kpad * npad doubles per plane
     double *d_work = nullptr;    // A, B (and C) planes for all slots
@@ -250,6 +256,7 @@ struct exs_ctx {
 // Launch helpers implemented in the .cu files.
 namespace exs {
 cudaError_t launch_match_planes(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
+cudaError_t launch_match_dlu(const DevParams &p, double *dlu, cudaStream_t s);
 cudaError_t launch_match_ref(const DevParams &p, int ngp, int ngkmax, const double *gpc, const double *tpgpc,
                              const exs_complex *sfacgp, exs_complex *apwalm, cudaStream_t s);
 cudaError_t launch_apwalm_to_planes(const DevParams &p, int ngp, const exs_complex *apwalm, double *ar,

@@ -57,9 +57,13 @@ __device__ inline void match_point(const DevParams &p, int ias, double gpc, doub
     double xm[EXS_LMAX_APW + 1];
     for (int l = 0; l <= lmax_out; l++) {
         const int n = apw[l];
+        // D_l of this atom, factorised once per set of SCF inputs (match_dlu_kernel)
         double d[EXS_APWORD_MAX * EXS_APWORD_MAX];
         int ipiv[EXS_APWORD_MAX];
-        const int info = match_dmat(p, ias, is, l, n, d, ipiv);
+        const double *lu = p.dlu + ((size_t)ias * (p.lmaxapw + 1) + l) * DLU_STRIDE;
+        for (int i = 0; i < n * n; i++) d[i] = lu[i];
+        for (int i = 0; i < n; i++) ipiv[i] = (int)lu[9 + i];
+        const int info = (int)lu[12];
         if (info != 0) atomicOr(p.err, DEV_WARN_SINGULAR);
         // zt2 = fpso * i^l * sfacgp
         double z1r = 0.0, z1i = 0.0;
@@ -200,6 +204,29 @@ __global__ void iora_planes_kernel(DevParams p, const KDesc *ks)
 }
 
 static const int MATCH_THREADS = 64;
+
+// LU factors of D_l for every (atom, l <= lmaxapw) (match.f90:136-163):
+// one thread per l, one block per atom.
+__global__ void match_dlu_kernel(DevParams p, double *dlu)
+{
+    const int ias = blockIdx.x, l = threadIdx.x;
+    if (l > p.lmaxapw) return;
+    const int is = p.atoms[ias].species;
+    const int n = p.apword[l + (size_t)(p.lmaxapw + 1) * is];
+    double d[EXS_APWORD_MAX * EXS_APWORD_MAX];
+    int ipiv[EXS_APWORD_MAX];
+    const int info = match_dmat(p, ias, is, l, n, d, ipiv);
+    double *out = dlu + ((size_t)ias * (p.lmaxapw + 1) + l) * DLU_STRIDE;
+    for (int i = 0; i < 9; i++) out[i] = i < n * n ? d[i] : 0.0;
+    for (int i = 0; i < 3; i++) out[9 + i] = i < n ? (double)ipiv[i] : 0.0;
+    out[12] = (double)info;
+}
+
+cudaError_t launch_match_dlu(const DevParams &p, double *dlu, cudaStream_t s)
+{
+    match_dlu_kernel<<<p.natmtot, 32 * ((p.lmaxapw + 32) / 32), 0, s>>>(p, dlu);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_match_planes(const DevParams &p, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s)
 {
