@@ -83,6 +83,7 @@ SIGNATURES = {
     "exs_rttddft_genpmat": ([P, c_int, P, P, P, P, P, P, c_int], c_int),
     "exs_clebgor_unit": ([c_int] * 5 + [P], c_int),
     "exs_gauntyry": ([c_int] * 6 + [P], c_int),
+    "exs_ozaki_moduli": ([c_int, c_int, c_int, P, P, P, P, P], c_int),
     "exs_fderiv_int": ([c_int, P, P, P], c_int),
 }
 

@@ -371,13 +371,26 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         c->prec_mode = mode;
         return EXS_OK;
     }
-    if (mode != EXS_PREC_OZAKI_INT8) return fail(c, EXS_ERR_ARG, "unknown precision mode");
-    if (slices < 3 || slices > 9) return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
+    if (mode != EXS_PREC_OZAKI_INT8 && mode != EXS_PREC_OZAKI_MOD)
+        return fail(c, EXS_ERR_ARG, "unknown precision mode");
+    if (mode == EXS_PREC_OZAKI_INT8 && (slices < 3 || slices > 9))
+        return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
+    if (mode == EXS_PREC_OZAKI_MOD && slices != 0 && (slices < 6 || slices > exs::OZ_MAX_MODULI))
+        return fail(c, EXS_ERR_ARG, "moduli must be 0 (automatic) or in 6..16");
     if (c->relativity == EXS_REL_IORA)
         return fail(c, EXS_ERR_ARG, "the split-precision contraction does not take the iora* overlap term");
     const int kp8 = exs::oz_kpad(c->K);
-    const int seg = exs::oz_seg_pairs(slices, kp8);
-    if (seg < 1) return fail(c, EXS_ERR_SIZE, "K too large for exact int32 accumulation of one slice pair");
+    exs::OzScheme sch{};
+    if (mode == EXS_PREC_OZAKI_MOD) {
+        if (exs::oz_mod_plan(slices, c->K, std::max(1, c->maxaa), &sch) != 0)
+            return fail(c, EXS_ERR_SIZE, "no modular plan for this K (K <= 65536, at least 8 bits per operand)");
+        slices = sch.n;
+    } else {
+        sch.n = slices;
+        sch.seg = exs::oz_seg_pairs(slices, kp8);
+        if (sch.seg < 1) return fail(c, EXS_ERR_SIZE, "K too large for exact int32 accumulation of one slice pair");
+    }
+    const int seg = sch.seg;
     cudaSetDevice(c->device);
     EXS_CUDA(cudaStreamSynchronize(c->stream));
     const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8);
@@ -391,7 +404,8 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     c->oz_lw = 128 * nch;
     c->oz_nfb = (c->maxaa + 63) / 64;
     c->oz_nxb = c->oz_nfb + (c->maxnlo + 63) / 64;
-    c->oz_xseg = exs::oz_seg_pairs(slices, c->oz_lw);
+    c->oz_xseg = mode == EXS_PREC_OZAKI_MOD ? 1 : exs::oz_seg_pairs(slices, c->oz_lw);
+    sch.segx = c->oz_xseg;
     const size_t xgroups = (size_t)c->natmtot * slices * c->oz_nxb;
     cudaError_t e = cudaMalloc((void **)&c->d_oz, slot * c->max_batch);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 2 * c->npad * c->max_batch);
@@ -419,9 +433,10 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         return fail(c, EXS_ERR_CUDA, "cuTensorMapEncodeTiled failed for the slice array");
     }
     c->slices = slices;
+    c->oz_sch = sch;
     c->prec_mode = mode;
     if (c->have_inputs) {   // slices of the current h_a and loa
-        EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), slices, c->stream));
+        EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->oz_sch, c->stream));
         EXS_CUDA(cudaStreamSynchronize(c->stream));
     }
     {   // a configuration the autotuner chose earlier for this shape
@@ -512,8 +527,8 @@ int exs_set_scf_inputs(exs_ctx *c, const exs_scf_inputs *in)
     // the matching systems D_l depend only on the tails: factorised once here
     if (!c->d_dlu) EXS_CUDA(dalloc(&c->d_dlu, (size_t)nat * (c->lmaxapw + 1) * exs::DLU_STRIDE));
     EXS_CUDA(exs::launch_match_dlu(c->params(), c->d_dlu, s));
-    if (c->prec_mode == EXS_PREC_OZAKI_INT8)   // slices of the new h_a and loa, in place
-        EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->slices, s));
+    if (c->oz_on())   // slices of the new h_a and loa, in place
+        EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->oz_sch, s));
     EXS_CUDA(cudaStreamSynchronize(s));
     c->have_inputs = true;
     return EXS_OK;
@@ -658,7 +673,7 @@ void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt
     exs::build_gemm_tables(c, ks, c->gt);
     ozt.clear();
     std::vector<int> ozat;
-    if (c->prec_mode == EXS_PREC_OZAKI_INT8) {
+    if (c->oz_on()) {
         oz_tiles(ks, ozt, (c->oz_cfg & 8) ? 256 : 128);
         oz_atom_tiles(c, ks, ozat);
     }
@@ -761,7 +776,7 @@ int upload_kdesc(exs_ctx *c, const std::vector<KDesc> &ks, Uploaded &u)
 // path only; the slots of one call are contiguous).
 cudaError_t oz_reset_maxima(exs_ctx *c, const std::vector<KDesc> &ks, cudaStream_t s)
 {
-    if (c->prec_mode != EXS_PREC_OZAKI_INT8 || ks.empty()) return cudaSuccess;
+    if (!c->oz_on() || ks.empty()) return cudaSuccess;
     double *lo = ks[0].oz_scale, *hi = ks[0].oz_scale;
     for (const KDesc &k : ks) {
         lo = std::min(lo, k.oz_scale);
@@ -787,16 +802,16 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     if (!have_planes) EXS_CUDA(exs::launch_match_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     if (c->relativity == EXS_REL_IORA) EXS_CUDA(exs::launch_iora_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_EV(1);
-    const bool oz = c->prec_mode == EXS_PREC_OZAKI_INT8;
+    const bool oz = c->oz_on();
     // configuration bit 4: B = h_a A and the APW-lo rows in native FP64 even
     // when the H/O contraction is split
     const bool b64 = !oz || (c->oz_cfg & 16);
     if (oz) {
         // slices of A; B = h_a A and the APW-lo rows of H from the slices of h_a and loa
-        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 2, s));
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 2, s));
         if (!b64)
             EXS_CUDA(exs::launch_oz_atom(c->oz_cfg, &c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles,
-                                         u.nozatiles, c->slices, c->kp8, c->oz_xseg, c->oz_atom_args(), s));
+                                         u.nozatiles, c->oz_sch, c->kp8, c->oz_atom_args(), s));
     }
     if (b64) {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, u.d_probs[exs::EPI_PLANAR], u.d_work[exs::EPI_PLANAR],
@@ -804,10 +819,10 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     }
     EXS_EV(2);
     if (oz) {
-        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->slices, c->kp8, 0, s));
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 0, s));
         const int q = c->oz_cfg;
         EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,
-                                    u.d_oztiles, u.noztiles, c->slices, c->kp8, c->oz_seg, s));
+                                    u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
                                        u.nwork[exs::EPI_HAM], u.d_k, s));
@@ -857,7 +872,7 @@ KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double 
         k.ci = k.ai;
     }
     k.oz_slices = c->d_oz ? c->d_oz + (size_t)slot * c->oz_slot_bytes : nullptr;
-    const bool oz = c->prec_mode == EXS_PREC_OZAKI_INT8 && c->d_ozscale;
+    const bool oz = c->oz_on() && c->d_ozscale;
     k.oz_scale = oz ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
     k.oz_slot = slot;
     return k;
@@ -905,7 +920,7 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
     if (nk == 0) return EXS_OK;
     cudaSetDevice(c->device);
     cudaStream_t s = c->stream;
-    if (c->prec_mode != EXS_PREC_OZAKI_INT8) {   // one configuration only: just run it
+    if (!c->oz_on()) {   // one configuration only: just run it
         EXS_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), s));
         rc = run_setup(c, ks, false);
         return rc < 0 ? rc : exs_synchronize(c);

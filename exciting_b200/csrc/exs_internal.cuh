@@ -40,6 +40,26 @@ struct OzAtomArgs {
 };
 static_assert(OZ_NCFG == EXS_OZ_NCONFIG, "public configuration count");
 
+// The arithmetic of the split-precision contraction.
+//   slices (mod = 0): n int8 slices of 7 bits per operand, pairs s + t <= n + 1,
+//     folded diagonal by diagonal in FP64 (seg / segx pairs per exact int32
+//     segment for the H/O and the per-atom tiles);
+//   moduli (mod = 1): every operand scaled to integers of b bits (bx for the
+//     h_a / loa rows) and stored as its residues modulo n pairwise coprime odd
+//     moduli p[m] (int8 in [-127, 127]); one int8 product per modulus, each
+//     folded into a 64-bit sum t += (v mod p[m]) c[m] (mod 2^64), so that
+//     t / 2^64 = X / M (mod 1) for the integer product X, |X| < M / 2; the
+//     value is t (as a signed integer) times fin (H/O) or finx (per-atom).
+constexpr int OZ_MAX_MODULI = 16;
+struct OzScheme {
+    int mod, n, seg, segx, b, bx;
+    double fin, finx;
+    int p[OZ_MAX_MODULI];
+    int mg[OZ_MAX_MODULI];             // round(2^32 / p): quotient estimate by a multiply-high
+    int c32[OZ_MAX_MODULI], c16[OZ_MAX_MODULI];   // 2^32 mod p, 2^16 mod p
+    unsigned long long c[OZ_MAX_MODULI];
+};
+
 // atomicMax for non-negative doubles: their IEEE bit patterns order like
 // unsigned integers.
 __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
@@ -220,7 +240,9 @@ struct exs_ctx {
     size_t fk_tab_hbytes = 0, fk_tab_dbytes = 0;
     // precision
     int prec_mode = EXS_PREC_FP64;
-    int slices = 7;
+    int slices = 7;              // slices or moduli of the split-precision modes
+    exs::OzScheme oz_sch{};      // their arithmetic
+    bool oz_on() const { return prec_mode == EXS_PREC_OZAKI_INT8 || prec_mode == EXS_PREC_OZAKI_MOD; }
     int kp8 = 0;                 // K rounded up to 256 (int8 slice rows)
     int oz_seg = 0;              // slice pairs per exact int32 segment
     int8_t *d_oz = nullptr;      // int8 slices of all slots
@@ -281,15 +303,16 @@ void pm_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)
-cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s);
-cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStream_t s);
+cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int a0,
+                            cudaStream_t s);
+cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s);
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
-                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                           const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s);
 bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, size_t xgroups, int lw,
                        CUtensorMap *mapArow, CUtensorMap *mapX);
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
-                          const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                          const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                           cudaStream_t s);
 bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB,
                          CUtensorMap *mapB2);
@@ -297,4 +320,5 @@ extern const int OZ_CFG_KCH[OZ_NCFG], OZ_CFG_NST[OZ_NCFG];
 int oz_kpad(int K);
 size_t oz_slot_bytes(int S, int npad, int kp8);
 int oz_seg_pairs(int S, int kp8);
+int oz_mod_plan(int n, int K, int kx, OzScheme *sch);
 }  // namespace exs

@@ -766,8 +766,8 @@ int enqueue_hmlint(exs_ctx *c, MtState &m, int lmaxvr, const double *apwfr, cons
     MT_CUDA(launch_radial(a, m, 0, ngroup + 1, 0, a.lmmaxvr + 1, s));   // potential groups + CH_KIN
     mt_angular_kernel<<<dim3((m.maxrows + 31) / 32, (m.maxrows + 7) / 8, nat), 256, 0, s>>>(a);
     MT_CUDA(cudaGetLastError());
-    if (c->prec_mode == EXS_PREC_OZAKI_INT8 && c->d_xs)
-        MT_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->slices, s));
+    if (c->oz_on() && c->d_xs)
+        MT_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->oz_sch, s));
     return EXS_OK;
 }
 

@@ -21,6 +21,19 @@
 // multiplies by sigma_A(i) sigma_B(j), adds the interstitial term and writes
 // the upper triangle and its conjugate mirror, as the FP64 path does.
 //
+// Modular arithmetic (OzScheme.mod = 1) replaces the slices by residues:
+// every column is scaled to integers of b bits, x' = rint(x 2^b / sigma)
+// (|x'| <= 2^b, exact in FP64), and stored as n int8 planes x' mod p_m in
+// [-127, 127] for pairwise coprime odd moduli p_m.  One int8 product per
+// modulus gives r +- i = X (mod p_m) for the integer product X; with M =
+// prod p_m > 2 * 2K * 2^(2b) > 2|X|, X / M is the signed fraction of
+// sum_m (X mod p_m) y_m / p_m, y_m = (M / p_m)^-1 mod p_m (the Chinese
+// remainder theorem).  The kernel keeps that fraction as a 64-bit fixed-point
+// sum t += r c_m (mod 2^64), c_m = round(2^64 y_m / p_m), in the tensor-memory
+// columns of the FP64 sums; the error of the rounded constants is at most
+// sum |r| / 2 units of 2^-64 M.  n products replace the n(n+1)/2 slice pairs
+// (14 moduli keep 48 bits per operand at K = 1936, where 7 slices keep 49).
+//
 // Slice storage (int8, K contiguous, K padded to kp8 = multiple of 256):
 //   [slot][slice][array: Br, Bi, Ar, Ai][G (npad rows)][kp8]
 // viewed by TMA as 5D (K byte in a 128-byte chunk, G, array, K chunk,
@@ -49,6 +62,8 @@
 // (bounded), frees tensor memory and returns.
 #include <cuda.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 
 #include "exs_internal.cuh"
@@ -215,6 +230,138 @@ __device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, i
     return (((size_t)s * OZ_NARR + a) * npad + g) * (size_t)kp8 + f;
 }
 
+// Residue of the integer x (|x| <= 2^52) modulo p_m in [-127, 127], in
+// 32-bit integer arithmetic: x = xh 2^32 + xm 2^16 + xl (xh signed,
+// |xh| <= 2^20; xm, xl in [0, 2^16)) gives v = xh (2^32 mod p) + xm (2^16
+// mod p) + xl = x (mod p), |v| < 2^29; v - floor(v mg / 2^32) p lies in
+// [-p/4, 5p/4] (mg = round(2^32 / p)), and one subtraction of p above 127
+// brings it into [-127, 127] (p <= 255).
+__device__ __forceinline__ int oz_residue(long long x, const OzScheme &sch, int m)
+{
+    const int p = sch.p[m];
+    const int xh = (int)(x >> 32);
+    const uint32_t lo = (uint32_t)x;
+    const int v = xh * sch.c32[m] + (int)(lo >> 16) * sch.c16[m] + (int)(lo & 0xffffu);
+    int r = v - __mulhi(v, sch.mg[m]) * p;
+    if (r > 127) r -= p;
+    return r;
+}
+
+__device__ __forceinline__ void oz_put(uint32_t (&o0)[16], uint32_t (&o1)[16], int e, uint32_t w0, uint32_t w1)
+{
+    if (e < 8) {
+        o0[2 * e] = w0;
+        o0[2 * e + 1] = w1;
+    } else {
+        o1[2 * (e - 8)] = w0;
+        o1[2 * (e - 8) + 1] = w1;
+    }
+}
+
+// Fold 16 finished int32 sums of diagonal g (slices) into the FP64 running
+// sums (two 32-bit tensor-memory words each, low word first; lo / hi hold
+// the previous values unless init): a += 2^{-7(g+2)} (r + sg i), r + sg i
+// exact in FP64, one rounding per fold.
+__device__ __forceinline__ void oz_fold16(int g, bool init, int sg, const uint32_t (&rv)[16], const uint32_t (&iv)[16],
+                                          const uint32_t (&lo)[16], const uint32_t (&hi)[16], uint32_t (&o0)[16],
+                                          uint32_t (&o1)[16])
+{
+    const double scale = ldexp(1.0, -7 * (g + 2));
+    const double sgd = (double)sg;
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+        double a = 0.0;
+        if (!init) {
+            const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
+            const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
+            a = __hiloint2double((int)w1, (int)w0);
+        }
+        a += scale * ((double)(int)rv[e] + sgd * (double)(int)iv[e]);
+        oz_put(o0, o1, e, (uint32_t)__double2loint(a), (uint32_t)__double2hiint(a));
+    }
+}
+
+// Modular fold of modulus g in two phases, so that the MMAs of the next
+// modulus need wait only for the first.
+// Phase 1 reads the int32 sums (r at columns [0, 128), i at [128, 256)) of
+// the 128 values of this lane, v = r +- i (exact: |v| <= 2 K 127^2 < 2^31),
+// and keeps v - q p_g, q = floor(v mg / 2^32), mg = round(2^32 / p_g):
+// |v (mg - 2^32 / p_g)| / 2^32 <= 1/4, so the residue lies in
+// [-p_g / 4, 5 p_g / 4], 16 bits, packed two per word (value q at half
+// q & 1 of word q >> 1).  Value block o (32 values) = r block o +- i block
+// (o ^ 1) for the H/O tiles (Re H, Im H, Re O, Im O), (o ^ 2) for the
+// per-atom tiles (Re rows 0-63, Im rows 0-63).
+template <int MODE>
+__device__ __forceinline__ void oz_mod_read(uint32_t t_lane, const OzScheme &sch, int g, uint32_t (&rp)[64])
+{
+    const int pm = sch.p[g], mg = sch.mg[g];
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+        const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
+        const bool minus = (MODE == OZ_HO) ? (o & 1) != 0 : o < 2;
+        uint32_t r0[16], r1[16], i0[16], i1[16];
+        tm_ld16(t_lane + o * 32, r0);
+        tm_ld16(t_lane + o * 32 + 16, r1);
+        tm_ld16(t_lane + 128 + oi * 32, i0);
+        tm_ld16(t_lane + 128 + oi * 32 + 16, i1);
+        tm_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; e += 2) {
+            int res[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int q = e + h;
+                const int rv = (int)(q < 16 ? r0[q] : r1[q - 16]), iv = (int)(q < 16 ? i0[q] : i1[q - 16]);
+                const int v = minus ? rv - iv : rv + iv;
+                res[h] = v - __mulhi(v, mg) * pm;
+            }
+            rp[o * 16 + e / 2] = ((uint32_t)res[0] & 0xffffu) | ((uint32_t)res[1] << 16);
+        }
+    }
+}
+
+// Phase 2: the 64-bit running sums t += r c_g (mod 2^64) in the FP64
+// columns, two 32-bit words per value (low first); t = r c_g for g = 0.
+__device__ __forceinline__ void oz_mod_accumulate(uint32_t t_lane, const OzScheme &sch, int g, const uint32_t (&rp)[64])
+{
+    const unsigned long long cm = sch.c[g];
+    const bool init = g == 0;
+#pragma unroll
+    for (int o = 0; o < 4; o++)
+#pragma unroll
+        for (int jc = 0; jc < 32; jc += 16) {
+            const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
+            uint32_t lo[16], hi[16];            // updated in place
+            if (!init) {
+                tm_ld16(t_lane + fcol, lo);
+                tm_ld16(t_lane + fcol + 16, hi);
+                tm_wait_ld();
+            }
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const int q = o * 32 + jc + e;
+                const int r = (int)(int16_t)(uint16_t)(rp[q >> 1] >> (16 * (q & 1)));
+                uint32_t &w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
+                uint32_t &w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
+                unsigned long long t = init ? 0ull : (((unsigned long long)w1 << 32) | w0);
+                t += (unsigned long long)(long long)r * cm;
+                w0 = (uint32_t)t;
+                w1 = (uint32_t)(t >> 32);
+            }
+            tm_st16(t_lane + fcol, lo);
+            tm_st16(t_lane + fcol + 16, hi);
+        }
+    tm_wait_st();
+}
+
+// A finished running sum as a value: the FP64 sum of the slices, or the
+// signed 64-bit fraction t / 2^64 = X / M times fin = M 2^-64 2^-(bits).
+__device__ __forceinline__ double oz_final(const OzScheme &sch, double fin, uint32_t w0, uint32_t w1)
+{
+    if (!sch.mod) return __hiloint2double((int)w1, (int)w0);
+    return (double)(long long)(((unsigned long long)w1 << 32) | w0) * fin;
+}
+
 // The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
 // A 64(f) x 32(G) tile per block, transposed through shared memory: reads
 // G-contiguous planes (a warp reads 32 consecutive G; 16 loads per thread in
@@ -222,8 +369,10 @@ __device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, i
 // cover the tile's 64 K bytes of one G row).
 constexpr int SPLIT_F = 64;
 
-__global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks, int S, int kp8, int a0)
+__global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks,
+                                                       const __grid_constant__ OzScheme sch, int kp8, int a0)
 {
+    const int S = sch.n;
     __shared__ double t[2][SPLIT_F][33];
     const KDesc k = ks[blockIdx.z];
     const int f0 = blockIdx.x * SPLIT_F, g0 = blockIdx.y * 32;
@@ -252,6 +401,26 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
     if (g >= p.npad || f >= kp8) return;
     // 1/sigma is a power of two: the scaling is exact
     const double rs = 1.0 / oz_sigma(k.oz_scale[(a0 == 0 ? p.npad : 0) + g]);
+    if (sch.mod) {
+        // x' = rint(x 2^b / sigma) (power-of-two scaling: exact), then its residues
+        const double sc = rs * ldexp(1.0, sch.b);
+        long long xq[2][8];
+#pragma unroll
+        for (int e = 0; e < 8; e++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) xq[a][e] = __double2ll_rn(t[a][fl + e][gl] * sc);
+        for (int m = 0; m < S; m++) {
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                uint32_t w[2] = {0, 0};
+#pragma unroll
+                for (int e = 0; e < 8; e++)
+                    w[e >> 2] |= ((uint32_t)(uint8_t)(int8_t)oz_residue(xq[a][e], sch, m)) << (8 * (e & 3));
+                *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(m, a0 + a, g, f, p.npad, kp8)) = make_uint2(w[0], w[1]);
+            }
+        }
+        return;
+    }
     // The slices are the base-128 digits of |x| 2^(7S) truncated, with the
     // sign of x: the same digits as S steps of (x *= 128, q = trunc(x),
     // x -= q) in exact FP64, taken from one integer (7S <= 63 bits).
@@ -327,8 +496,9 @@ __global__ void oz_xsig_kernel(DevParams p, OzAtomArgs xa)
 }
 
 // The slices of X: one thread per (atom, block, row, 4 window bytes).
-__global__ void oz_xsplit_kernel(DevParams p, OzAtomArgs xa, int S)
+__global__ void oz_xsplit_kernel(DevParams p, OzAtomArgs xa, const __grid_constant__ OzScheme sch)
 {
+    const int S = sch.n;
     const int ias = blockIdx.z, xb = blockIdx.y;
     const int n = threadIdx.y + blockIdx.x * blockDim.y;        // row 0..63
     const int k4 = threadIdx.x * 4;                             // window byte
@@ -343,6 +513,26 @@ __global__ void oz_xsplit_kernel(DevParams p, OzAtomArgs xa, int S)
         x_value(p, xa, ias, xb, n, k4 + e - delta, re, im);
         x[0][e] = re * r;
         x[1][e] = im * r;
+    }
+    if (sch.mod) {
+        const double sc = ldexp(1.0, sch.bx);
+        long long xq[2][4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            xq[0][e] = __double2ll_rn(x[0][e] * sc);
+            xq[1][e] = __double2ll_rn(x[1][e] * sc);
+        }
+        for (int m = 0; m < S; m++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                uint32_t w = 0;
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    w |= ((uint32_t)(uint8_t)(int8_t)oz_residue(xq[a][e], sch, m)) << (8 * e);
+                const size_t row = ((((size_t)ias * S + m) * xa.nxb + xb) * 2 + a) * 64 + n;
+                *reinterpret_cast<uint32_t *>(xa.xs + row * xa.lw + k4) = w;
+            }
+        return;
     }
     for (int s = 0; s < S; s++)
 #pragma unroll
@@ -399,8 +589,12 @@ __device__ __forceinline__ OzTileInfo oz_tile(const DevParams &p, const int *til
 template <int MODE, int KCH, int NST>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
-              const KDesc *ks, const int *tiles, int ntiles, int S, int kp8, int seg_pairs, OzAtomArgs xa)
+              const KDesc *ks, const int *tiles, int ntiles, const __grid_constant__ OzScheme sch, int kp8,
+              OzAtomArgs xa)
 {
+    const int S = sch.n;
+    const bool mod = sch.mod != 0;
+    const int seg_pairs = mod ? 1 : (MODE == OZ_HO ? sch.seg : sch.segx);
     constexpr int BOX = KCH * OZ_TILE;          // one operand of a stage
     constexpr int STAGE = 3 * BOX;              // A box [chunk][Ar, Ai][128 rows], B box [chunk][128 rows]
     extern __shared__ __align__(1024) uint8_t oz_smem[];
@@ -445,9 +639,10 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 const OzTileInfo ti = oz_tile<MODE, KCH>(p, tiles, tile, kp8);
                 const int slot = ks[ti.k].oz_slot;
                 const int x0 = (MODE == OZ_ATOM) ? p.atoms[ti.ias].oz_x0 : 0;
-                for (int d = 2; d <= S + 1 && !bad; d++)
-                    for (int s = 1; s <= d - 1 && !bad; s++) {
-                        const int t = d - s;
+                // group g: slices, the pairs (s, t) of diagonal s + t = g + 2; moduli, plane g with itself
+                for (int g = 0; g < S && !bad; g++)
+                    for (int j = 0; j < (mod ? 1 : g + 1) && !bad; j++) {
+                        const int s = mod ? g + 1 : j + 1, t = mod ? g + 1 : g + 1 - j;
                         for (int kb = 0; kb < ti.nst; kb++) {
                             if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
                                 bad = true;
@@ -486,9 +681,9 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             bool bad = false;
             for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
                 const int nst = oz_tile<MODE, KCH>(p, tiles, tile, kp8).nst;
-                for (int d = 2; d <= S + 1 && !bad; d++)
-                    for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
-                        const int s1 = min(d - 1, s0 + seg_pairs - 1);
+                for (int g = 0; g < S && !bad; g++)
+                    for (int s0 = 1; s0 <= (mod ? 1 : g + 1) && !bad; s0 += seg_pairs) {
+                        const int s1 = min(mod ? 1 : g + 1, s0 + seg_pairs - 1);
                         // the epilogue must have folded the previous segment
                         if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
                             bad = true;
@@ -537,21 +732,30 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         bool bad = false;
         for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
             const OzTileInfo ti = oz_tile<MODE, KCH>(p, tiles, tile, kp8);
-            for (int d = 2; d <= S + 1 && !bad; d++) {
-                const double scale = ldexp(1.0, -7 * d);
-                for (int s0 = 1; s0 <= d - 1; s0 += seg_pairs) {
+            for (int g = 0; g < S && !bad; g++) {
+                for (int s0 = 1; s0 <= (mod ? 1 : g + 1); s0 += seg_pairs) {
                     const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
                     if (!ok) {
                         bad = true;
                         break;
                     }
                     tc_fence_after();
-                    const bool init = (d == 2 && s0 == 1);      // first segment of the tile
-                    // FP64 block o (32 values) = r block o +- i block (o ^ 1) (HO:
+                    if (mod) {
+                        uint32_t rp[64];
+                        oz_mod_read<MODE>(t_lane, sch, g, rp);
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&acce);          // the accumulators are free
+                        nseg++;
+                        oz_mod_accumulate(t_lane, sch, g, rp);
+                        continue;
+                    }
+                    const bool init = (g == 0 && s0 == 1);      // first segment of the tile
+                    // running-sum block o (32 values) = r block o +- i block (o ^ 1) (HO:
                     // Re H, Im H, Re O, Im O) or (o ^ 2) (ATOM: Re rows 0-63, Im rows 0-63)
 #pragma unroll 1
                     for (int o = 0; o < 4; o++) {
-                        const double sg = (MODE == OZ_HO) ? ((o & 1) ? -1.0 : 1.0) : ((o < 2) ? -1.0 : 1.0);
+                        const int sg = (MODE == OZ_HO) ? ((o & 1) ? -1 : 1) : ((o < 2) ? -1 : 1);
                         const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
 #pragma unroll 1
                         for (int jc = 0; jc < 32; jc += 16) {
@@ -565,25 +769,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                             }
                             tm_wait_ld();
                             uint32_t o0[16], o1[16];
-#pragma unroll
-                            for (int e = 0; e < 16; e++) {
-                                double a = 0.0;
-                                if (!init) {
-                                    const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
-                                    const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
-                                    a = __hiloint2double((int)w1, (int)w0);
-                                }
-                                // r +- i is exact in FP64 (|int32| sums); one rounding per fold
-                                a += scale * ((double)(int)rv[e] + sg * (double)(int)iv[e]);
-                                const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
-                                if (e < 8) {
-                                    o0[2 * e] = w0;
-                                    o0[2 * e + 1] = w1;
-                                } else {
-                                    o1[2 * (e - 8)] = w0;
-                                    o1[2 * (e - 8) + 1] = w1;
-                                }
-                            }
+                            oz_fold16(g, init, sg, rv, iv, lo, hi, o0, o1);
                             tm_st16(t_lane + fcol, o0);
                             tm_st16(t_lane + fcol + 16, o1);
                         }
@@ -626,7 +812,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                         tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
                         tm_wait_ld();
 #pragma unroll
-                        for (int e = 0; e < 8; e++) val[o][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+                        for (int e = 0; e < 8; e++) val[o][e] = oz_final(sch, sch.fin, w[2 * e], w[2 * e + 1]);
                     }
                     if (!row_ok) continue;
 #pragma unroll
@@ -689,8 +875,8 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     for (int e = 0; e < 8; e++) {
                         const int n = jc + e;
                         const double sc = sa * sig[n];
-                        const double re = __hiloint2double((int)wr[2 * e + 1], (int)wr[2 * e]) * sc;
-                        const double im = __hiloint2double((int)wi[2 * e + 1], (int)wi[2 * e]) * sc;
+                        const double re = oz_final(sch, sch.finx, wr[2 * e], wr[2 * e + 1]) * sc;
+                        const double im = oz_final(sch, sch.finx, wi[2 * e], wi[2 * e + 1]) * sc;
                         if (!lorows) {
                             const int f = ti.xb * 64 + n;
                             if (f >= at.napw) continue;
@@ -794,8 +980,11 @@ __device__ __forceinline__ void umma_commit_2sm(uint64_t *bar)
 template <int KCH, int NST>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
 oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB2, DevParams p,
-               const KDesc *ks, const int *tiles, int S, int kp8, int seg_pairs)
+               const KDesc *ks, const int *tiles, const __grid_constant__ OzScheme sch, int kp8)
 {
+    const int S = sch.n;
+    const bool mod = sch.mod != 0;
+    const int seg_pairs = mod ? 1 : sch.seg;
     constexpr int ABOX = 2 * KCH * OZ_TILE;          // Ar, Ai of this CTA's 128 rows
     constexpr int BBOX = KCH * OZ_TILE / 2;          // this CTA's 64 rows of B
     constexpr int STAGE = ABOX + BBOX;
@@ -844,9 +1033,9 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             int st = 0;
             bool bad = false;
             const int slot = kd.oz_slot;
-            for (int d = 2; d <= S + 1 && !bad; d++)
-                for (int s = 1; s <= d - 1 && !bad; s++) {
-                    const int t = d - s;
+            for (int g = 0; g < S && !bad; g++)
+                for (int j = 0; j < (mod ? 1 : g + 1) && !bad; j++) {
+                    const int s = mod ? g + 1 : j + 1, t = mod ? g + 1 : g + 1 - j;
                     for (int kb = 0; kb < nst; kb++) {
                         if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
                             bad = true;
@@ -878,9 +1067,9 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             for (int q = 0; q < NST; q++) uses[q] = 0;
             int nseg = 0, st = 0;
             bool bad = false;
-            for (int d = 2; d <= S + 1 && !bad; d++)
-                for (int s0 = 1; s0 <= d - 1 && !bad; s0 += seg_pairs) {
-                    const int s1 = min(d - 1, s0 + seg_pairs - 1);
+            for (int g = 0; g < S && !bad; g++)
+                for (int s0 = 1; s0 <= (mod ? 1 : g + 1) && !bad; s0 += seg_pairs) {
+                    const int s1 = min(mod ? 1 : g + 1, s0 + seg_pairs - 1);
                     if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
                         bad = true;
                         break;
@@ -926,19 +1115,28 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
         const uint32_t acce0 = mapa_shared(smem_u32(&acce), 0);
         int nseg = 0;
         bool bad = false;
-        for (int d = 2; d <= S + 1 && !bad; d++) {
-            const double scale = ldexp(1.0, -7 * d);
-            for (int s0 = 1; s0 <= d - 1; s0 += seg_pairs) {
+        for (int g = 0; g < S && !bad; g++) {
+            for (int s0 = 1; s0 <= (mod ? 1 : g + 1); s0 += seg_pairs) {
                 const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
                 if (!ok) {
                     bad = true;
                     break;
                 }
                 tc_fence_after();
+                if (mod) {
+                    uint32_t rp[64];
+                    oz_mod_read<OZ_HO>(t_lane, sch, g, rp);
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_remote(acce0);      // the accumulators are free
+                    nseg++;
+                    oz_mod_accumulate(t_lane, sch, g, rp);
+                    continue;
+                }
                 const bool init = (nseg == 0);
 #pragma unroll 1
                 for (int o = 0; o < 4; o++) {
-                    const double sg = (o & 1) ? -1.0 : 1.0;
+                    const int sg = (o & 1) ? -1 : 1;
 #pragma unroll 1
                     for (int jc = 0; jc < 32; jc += 16) {
                         uint32_t rv[16], iv[16], lo[16], hi[16];
@@ -951,24 +1149,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                         }
                         tm_wait_ld();
                         uint32_t o0[16], o1[16];
-#pragma unroll
-                        for (int e = 0; e < 16; e++) {
-                            double a = 0.0;
-                            if (!init) {
-                                const uint32_t w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
-                                const uint32_t w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
-                                a = __hiloint2double((int)w1, (int)w0);
-                            }
-                            a += scale * ((double)(int)rv[e] + sg * (double)(int)iv[e]);
-                            const uint32_t w0 = (uint32_t)__double2loint(a), w1 = (uint32_t)__double2hiint(a);
-                            if (e < 8) {
-                                o0[2 * e] = w0;
-                                o0[2 * e + 1] = w1;
-                            } else {
-                                o1[2 * (e - 8)] = w0;
-                                o1[2 * (e - 8) + 1] = w1;
-                            }
-                        }
+                        oz_fold16(g, init, sg, rv, iv, lo, hi, o0, o1);
                         tm_st16(t_lane + fcol, o0);
                         tm_st16(t_lane + fcol + 16, o1);
                     }
@@ -1006,7 +1187,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                     tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
                     tm_wait_ld();
 #pragma unroll
-                    for (int e = 0; e < 8; e++) val[o][e] = __hiloint2double((int)w[2 * e + 1], (int)w[2 * e]);
+                    for (int e = 0; e < 8; e++) val[o][e] = oz_final(sch, sch.fin, w[2 * e], w[2 * e + 1]);
                 }
                 if (!row_ok) continue;
 #pragma unroll
@@ -1072,6 +1253,80 @@ int oz_seg_pairs(int S, int kp8)
     return (int)(n < 1 ? 0 : (n > S ? S : n));
 }
 
+// Pairwise coprime odd moduli below 256, largest first (247 = 13 * 19,
+// 217 = 7 * 31; the others are primes or 255 = 3 * 5 * 17, 253 = 11 * 23).
+static const int OZ_MODULI[OZ_MAX_MODULI] = {255, 253, 251, 247, 241, 239, 233, 229,
+                                             227, 223, 217, 211, 199, 197, 193, 191};
+
+// Bits per operand so that |X| <= 2K 2^(b + b') < M / 2 for a product of
+// 2K int terms; log2 M is a sum of logarithms, taken with a margin.
+static int oz_mod_bits(int n, int K)
+{
+    double lm = 0.0;
+    for (int m = 0; m < n; m++) lm += std::log2((double)OZ_MODULI[m]);
+    return (int)std::floor(lm - 1.0 - std::log2(2.0 * K) - 1e-9);
+}
+
+static int oz_inverse_mod(long long a, long long p)
+{
+    // extended Euclid on (a mod p, p); gcd is 1 for coprime moduli
+    long long r0 = p, r1 = ((a % p) + p) % p, t0 = 0, t1 = 1;
+    while (r1 != 0) {
+        const long long q = r0 / r1, r2 = r0 - q * r1, t2 = t0 - q * t1;
+        r0 = r1; r1 = r2; t0 = t1; t1 = t2;
+    }
+    return r0 == 1 ? (int)(((t0 % p) + p) % p) : -1;
+}
+
+// The modular scheme for n moduli (0: the fewest in 6..16 that keep b >= 48),
+// contraction length K (H/O tiles) and per-atom window kx.  Returns 0, or
+// -1 if no valid plan exists (n out of range, b or bx below 8, or K past
+// the exact int32 range of one product: 2 K 127^2 < 2^31).
+int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
+{
+    if (K < 1 || kx < 1 || K > 65536 || kx > 65536) return -1;
+    if (n == 0) {
+        n = OZ_MAX_MODULI;
+        for (int q = 6; q <= OZ_MAX_MODULI; q++)
+            if (oz_mod_bits(q, K) >= 2 * 48) {
+                n = q;
+                break;
+            }
+    }
+    if (n < 6 || n > OZ_MAX_MODULI) return -1;
+    const int two_b = oz_mod_bits(n, K);
+    const int b = std::min(52, two_b / 2);
+    const int bx = std::min(52, oz_mod_bits(n, kx) - b);
+    if (b < 8 || bx < 8) return -1;
+    OzScheme s{};
+    s.mod = 1;
+    s.n = n;
+    s.seg = s.segx = 1;
+    s.b = b;
+    s.bx = bx;
+    double M = 1.0;
+    for (int m = 0; m < n; m++) M *= (double)OZ_MODULI[m];
+    s.fin = std::ldexp(M, -64 - 2 * b);
+    s.finx = std::ldexp(M, -64 - b - bx);
+    for (int m = 0; m < n; m++) {
+        const int p = OZ_MODULI[m];
+        long long mm = 1;   // (M / p) mod p
+        for (int q = 0; q < n; q++)
+            if (q != m) mm = mm * OZ_MODULI[q] % p;
+        const int y = oz_inverse_mod(mm, p);
+        if (y < 0) return -1;
+        s.p[m] = p;
+        s.mg[m] = (int)((((long long)1 << 32) + p / 2) / p);
+        s.c32[m] = (int)((((long long)1 << 32)) % p);
+        s.c16[m] = (1 << 16) % p;
+        // round(2^64 y / p); y < p, so the quotient is below 2^64
+        const unsigned __int128 num = ((unsigned __int128)y << 64) + (unsigned)(p / 2);
+        s.c[m] = (unsigned long long)(num / (unsigned)p);
+    }
+    *sch = s;
+    return 0;
+}
+
 // configuration index: bit 0 = pipeline shape (KCH, NST) of the H/O tiles,
 // bit 1 = persistent launch (one CTA per SM) of the H/O tiles, bit 2 =
 // persistent launch of the per-atom tiles, bit 3 = two-SM H/O tiles (256 x 32
@@ -1082,24 +1337,25 @@ const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1,
 const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4,
                                  2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4};
 
-cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, int S, int kp8, int a0, cudaStream_t s)
+cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int a0,
+                            cudaStream_t s)
 {
-    oz_split_kernel<<<dim3(kp8 / SPLIT_F, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, S, kp8, a0);
+    oz_split_kernel<<<dim3(kp8 / SPLIT_F, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, sch, kp8, a0);
     return cudaGetLastError();
 }
 
-cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, int S, cudaStream_t s)
+cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s)
 {
     oz_xsig_kernel<<<dim3(xa.nxb, p.natmtot), 64, 0, s>>>(p, xa);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    oz_xsplit_kernel<<<dim3(8, xa.nxb, p.natmtot), dim3(xa.lw / 4, 8), 0, s>>>(p, xa, S);
+    oz_xsplit_kernel<<<dim3(8, xa.nxb, p.natmtot), dim3(xa.lw / 4, 8), 0, s>>>(p, xa, sch);
     return cudaGetLastError();
 }
 
 template <int MODE, int KCH, int NST>
 static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p, const KDesc *d_k,
-                              const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, const OzAtomArgs &xa,
+                              const void *d_tiles, int ntiles, const OzScheme &sch, int kp8, const OzAtomArgs &xa,
                               bool persistent, cudaStream_t s)
 {
     constexpr int smem = NST * 3 * KCH * OZ_TILE + 1024;
@@ -1116,13 +1372,13 @@ static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, 
     // persistent: one CTA per SM walking the tiles; else one CTA per tile
     const int grid = (persistent && nsm < ntiles) ? nsm : ntiles;
     oz_mma_kernel<MODE, KCH, NST><<<grid, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const int *)d_tiles, ntiles,
-                                                                 S, kp8, seg_pairs, xa);
+                                                                 sch, kp8, xa);
     return cudaGetLastError();
 }
 
 template <int KCH, int NST>
 static cudaError_t launch_2sm(const CUtensorMap *mapA, const CUtensorMap *mapB2, const DevParams &p, const KDesc *d_k,
-                              const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs, cudaStream_t s)
+                              const void *d_tiles, int ntiles, const OzScheme &sch, int kp8, cudaStream_t s)
 {
     constexpr int smem = NST * (2 * KCH * OZ_TILE + KCH * OZ_TILE / 2) + 1024;
     static bool attr = false;
@@ -1131,35 +1387,34 @@ static cudaError_t launch_2sm(const CUtensorMap *mapA, const CUtensorMap *mapB2,
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    oz_mma2_kernel<KCH, NST><<<2 * ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB2, p, d_k, (const int *)d_tiles, S, kp8,
-                                                                  seg_pairs);
+    oz_mma2_kernel<KCH, NST><<<2 * ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB2, p, d_k, (const int *)d_tiles, sch,
+                                                                  kp8);
     return cudaGetLastError();
 }
 
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
-                          const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                          const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                           cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
     if (cfg & 8) {   // two-SM tiles: mapB is the half-B view
-        if (cfg & 1) return launch_2sm<1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
-        return launch_2sm<2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, s);
+        if (cfg & 1) return launch_2sm<1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, sch, kp8, s);
+        return launch_2sm<2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, sch, kp8, s);
     }
     const OzAtomArgs none{};
     const bool persistent = (cfg & 2) != 0;
     switch (cfg & 1) {
-    case 0: return launch_cfg<OZ_HO, 2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, persistent, s);
-    default: return launch_cfg<OZ_HO, 1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, none, persistent, s);
+    case 0: return launch_cfg<OZ_HO, 2, 2>(mapA, mapB, p, d_k, d_tiles, ntiles, sch, kp8, none, persistent, s);
+    default: return launch_cfg<OZ_HO, 1, 4>(mapA, mapB, p, d_k, d_tiles, ntiles, sch, kp8, none, persistent, s);
     }
 }
 
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
-                           const KDesc *d_k, const void *d_tiles, int ntiles, int S, int kp8, int seg_pairs,
+                           const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
-    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, S, kp8, seg_pairs, xa, (cfg & 4) != 0,
-                                     s);
+    return launch_cfg<OZ_ATOM, 1, 4>(mapArow, mapX, p, d_k, d_tiles, ntiles, sch, kp8, xa, (cfg & 4) != 0, s);
 }
 
 // TMA views of the slices of all slots (int8, 5D):
@@ -1250,3 +1505,17 @@ bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, s
 }
 
 }  // namespace exs
+
+extern "C" int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsigned long long *c, int *b, int *bx)
+{
+    exs::OzScheme s{};
+    if (exs::oz_mod_plan(n, K, kx, &s) != 0) return EXS_ERR_ARG;
+    if (n_out) *n_out = s.n;
+    for (int m = 0; m < s.n; m++) {
+        if (p) p[m] = s.p[m];
+        if (c) c[m] = s.c[m];
+    }
+    if (b) *b = s.b;
+    if (bx) *bx = s.bx;
+    return EXS_OK;
+}

@@ -190,7 +190,8 @@ class Setup:
         return self._check(self.lib.exs_hmlint_device(self.ctx, ctypes.byref(r)))
 
     def set_precision(self, mode: str = "fp64", slices: int = 7):
-        m = {"fp64": 0, "ozaki": 1}[mode]
+        """fp64; ozaki (``slices`` int8 slices); ozaki_mod (``slices`` moduli, 0 = automatic)."""
+        m = {"fp64": 0, "ozaki": 1, "ozaki_mod": 2}[mode]
         self._check(self.lib.exs_set_precision(self.ctx, m, slices))
 
     # ------------------------------------------------------------------

@@ -34,7 +34,7 @@ enum {
 };
 
 enum { EXS_REL_NONE = 0, EXS_REL_ZORA = 1, EXS_REL_IORA = 2 };   /* ValenceRelativity */
-enum { EXS_PREC_FP64 = 0, EXS_PREC_OZAKI_INT8 = 1 };             /* MT contraction path */
+enum { EXS_PREC_FP64 = 0, EXS_PREC_OZAKI_INT8 = 1, EXS_PREC_OZAKI_MOD = 2 };   /* MT contraction path */
 
 /* Per-run description: what init0/init1 leave in the reference's modules. */
 typedef struct exs_config {
@@ -145,9 +145,22 @@ int exs_olprad_device(exs_ctx *ctx, const exs_mt_radial *in);
 int exs_gauntyry(int l1, int l2, int l3, int m1, int m2, int m3, double *re_im);
 int exs_fderiv_int(int n, const double *x, const double *f, double *result);
 
-/* Select the MT contraction arithmetic: EXS_PREC_FP64 (native FP64) or
- * EXS_PREC_OZAKI_INT8 with `slices` int8 slices per operand (3..9). */
+/* Select the MT contraction arithmetic: EXS_PREC_FP64 (native FP64),
+ * EXS_PREC_OZAKI_INT8 with `slices` int8 slices per operand (3..9), or
+ * EXS_PREC_OZAKI_MOD: the operands as integers modulo `slices` pairwise
+ * coprime odd moduli (6..16; 0 = the fewest that keep 48 bits per operand
+ * for this context's K), one int8 product per modulus, recombined by the
+ * Chinese remainder theorem.  No reference counterpart (the reference's
+ * contraction is zgemm in FP64). */
 int exs_set_precision(exs_ctx *ctx, int mode, int slices);
+
+/* The modular plan exs_set_precision(EXS_PREC_OZAKI_MOD, n) would use for a
+ * contraction length K (2K products per real sum) and per-atom windows of
+ * kx rows: the moduli p[0..n-1], the constants c[m] = round(2^64 y_m / p_m)
+ * mod 2^64 with y_m = (M / p_m)^-1 mod p_m, M = prod p, and the bits b of
+ * the scaled A and B columns and bx of the scaled h_a / loa rows.  n = 0
+ * picks n as exs_set_precision does; *n_out receives it.  Host only. */
+int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsigned long long *c, int *b, int *bx);
 
 /* Replaces  call match(ngp, gpc, tpgpc, sfacgp, apwalm)   (src/match.f90:13).
  *   gpc(ngkmax), tpgpc(2, ngkmax), sfacgp(ngkmax, natmtot)  in;

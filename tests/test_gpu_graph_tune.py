@@ -63,11 +63,12 @@ def _system():
     return s, s.gksets()[:NK]
 
 
-def test_ozaki_configurations_bit_identical():
+@pytest.mark.parametrize("mode,n", [("ozaki", 7), ("ozaki_mod", 0)])
+def test_ozaki_configurations_bit_identical(mode, n):
     from exciting_b200.fvsystem import Setup
     s, gks = _system()
     st = Setup(s, max_batch=NK)
-    st.set_precision("ozaki", 7)
+    st.set_precision(mode, n)
     b = DeviceBatch(st, gks)
     outs = []
     for cfg in range(32):
@@ -90,12 +91,13 @@ def test_ozaki_configurations_bit_identical():
         st.set_kernel_config(32)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "ozaki"])
+@pytest.mark.parametrize("prec", ["fp64", "ozaki", "ozaki_mod"])
 def test_autotune_keeps_results_correct(prec):
     from exciting_b200.fvsystem import Setup
     s, gks = _system()
     st = Setup(s, max_batch=NK)
-    st.set_precision(prec, 7)
+    n = 0 if prec == "ozaki_mod" else 7
+    st.set_precision(prec, n)
     b = DeviceBatch(st, gks)
     choice = st.autotune(*b.args())
     assert choice in ((0,) if prec == "fp64" else tuple(range(32)))
@@ -104,7 +106,7 @@ def test_autotune_keeps_results_correct(prec):
     assert rel_fro(h, hr) <= TOL_FRO and rel_fro(o, orf) <= TOL_FRO
     # the choice sticks for this shape after switching precision back and forth
     st.set_precision("fp64")
-    st.set_precision(prec, 7)
+    st.set_precision(prec, n)
     b.clear()
     st.setup_batched_device(*b.args())
     st.synchronize()
@@ -112,13 +114,13 @@ def test_autotune_keeps_results_correct(prec):
     assert np.array_equal(h, h2) and np.array_equal(o, o2)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "ozaki"])
+@pytest.mark.parametrize("prec", ["fp64", "ozaki", "ozaki_mod"])
 def test_graph_replay(prec):
     from exciting_b200.abi import ExsError
     from exciting_b200.fvsystem import Setup
     s, gks = _system()
     st = Setup(s, max_batch=NK)
-    st.set_precision(prec, 7)
+    st.set_precision(prec, 0 if prec == "ozaki_mod" else 7)
     b = DeviceBatch(st, gks)
     st.setup_batched_device(*b.args())
     st.synchronize()

@@ -9,6 +9,10 @@ solver asks zhegvx for the range IL = 1 .. IU = nstfv only
 |e| <= 1 Ha and 1e-8 |e| above: the seeded synthetic MT integrals put some
 of the lowest generalized eigenvalues near -1000 Ha, where an absolute 1e-8
 would ask for 17 significant digits of an FP64 result.
+
+The modular mode (ozaki_mod: residues modulo pairwise coprime moduli, one
+int8 product per modulus) is held to the same bars; its error must fall as
+moduli are added.
 """
 import numpy as np
 import pytest
@@ -33,17 +37,21 @@ def eig_dev(w, wr):
     return np.max(np.abs(w - wr) / (TOL_EIG * np.maximum(1.0, np.abs(wr))))
 
 
-def _setup(s, slices=7, **kw):
+def _setup(s, slices=7, mode="ozaki", **kw):
     from exciting_b200.fvsystem import Setup
     st = Setup(s, **kw)
-    st.set_precision("ozaki", slices)
+    st.set_precision(mode, slices if mode == "ozaki" else 0)
     return st
 
 
+MODES = ["ozaki", "ozaki_mod"]
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("variant,rel", [("text", "none"), ("shipped", "zora")])
-def test_ozaki_si_fcc_vs_oracle(variant, rel):
+def test_ozaki_si_fcc_vs_oracle(variant, rel, mode):
     s = W.si_fcc(variant, relativity=rel)
-    st = _setup(s)
+    st = _setup(s, mode=mode)
     for ik in (0, 5):
         gk = s.gkset(s.kpoints[ik])
         h, o = st.hamiltonandoverlapsetup(gk)
@@ -57,10 +65,11 @@ def test_ozaki_si_fcc_vs_oracle(variant, rel):
         assert eig_dev(w, wr) <= 1.0
 
 
-def test_ozaki_cube8_batched_vs_oracle():
+@pytest.mark.parametrize("mode", MODES)
+def test_ozaki_cube8_batched_vs_oracle(mode):
     s = W.si_cube8()
     gks = s.gksets()
-    st = _setup(s, max_batch=len(gks))
+    st = _setup(s, mode=mode, max_batch=len(gks))
     out = st.setup_batched(gks)
     for ik in (0, 13):
         hr, orf = O.hamiltonandoverlapsetup(s, gks[ik])
@@ -82,6 +91,36 @@ def test_ozaki_error_falls_with_slices():
         errs.append(rel_fro(h, hr))
     assert errs[0] > errs[1] > errs[2] > errs[3], errs
     assert errs[0] < 1e-5 and errs[3] < TOL_FRO
+
+
+def test_ozaki_mod_error_falls_with_moduli():
+    from exciting_b200.fvsystem import Setup
+    s = W.si_fcc("text")
+    gk = s.gkset(s.kpoints[3])
+    hr, orf = O.hamiltonandoverlapsetup(s, gk)
+    st = Setup(s)
+    errs = []
+    for n in (6, 8, 10, 12):
+        st.set_precision("ozaki_mod", n)
+        h, o = st.hamiltonandoverlapsetup(gk)
+        errs.append(rel_fro(h, hr))
+    assert errs[0] > errs[1] > errs[2] > errs[3], errs
+    assert errs[3] < TOL_FRO
+
+
+def test_ozaki_mod_argument_errors():
+    from exciting_b200.abi import ExsError
+    from exciting_b200.fvsystem import Setup
+    s = W.si_fcc("text")
+    st = Setup(s)
+    for n in (5, 17):
+        with pytest.raises(ExsError):
+            st.set_precision("ozaki_mod", n)
+    st.set_precision("ozaki_mod", 0)                  # still usable afterwards
+    gk = s.gkset(s.kpoints[0])
+    h, o = st.hamiltonandoverlapsetup(gk)
+    hr, orf = O.hamiltonandoverlapsetup(s, gk)
+    assert rel_fro(h, hr) <= TOL_FRO
 
 
 def test_ozaki_rejects_iora():
