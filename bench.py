@@ -134,13 +134,30 @@ def _hbm_peak():
         return 6650.0      # earlier measurement on this pool's B200s
 
 
-def ozaki_int8_ops(sys_, gks, slices):
+def split_scheme(args, sys_):
+    """(int8 planes per operand, int8 products per output tile, dtype text,
+    precision text) of the split-precision mode args.precision."""
+    if args.precision == "ozaki":
+        S = args.slices
+        return (S, S * (S + 1) // 2, "i8 slices, f64 recombination",
+                "split int8 x%d slices (tcgen05), FP64 recombination" % S)
+    from exciting_b200.fvsystem import ozaki_moduli
+    K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
+    ps, _, b, bx = ozaki_moduli(args.moduli, K, sys_.basis.maxaa)
+    n = len(ps)
+    return (n, n, "i8 residues mod %d coprime moduli, CRT in 64-bit fixed point, f64 scaling" % n,
+            "split int8, residues modulo %d moduli (%d-bit operands; tcgen05), Chinese-remainder recombination"
+            % (n, b))
+
+
+def ozaki_int8_ops(sys_, gks, products):
     """int8 MMA operations the split-precision kernel issues: per 128 x 32 tile
-    (B operand [Br|Bi|Ar|Ai] -> N = 128), S(S+1)/2 slice pairs x two A operands
-    (Ar, Ai) x 2 x 128 x 128 x kp8 (K padded to 256)."""
+    (B operand [Br|Bi|Ar|Ai] -> N = 128), `products` int8 products (S(S+1)/2
+    slice pairs, or one per modulus) x two A operands (Ar, Ai) x 2 x 128 x 128
+    x kp8 (K padded to 256)."""
     K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
     kp8 = (K + 255) // 256 * 256
-    pairs = slices * (slices + 1) // 2
+    pairs = products
     tiles = 0
     for g in gks:
         n = g.ngp
@@ -155,22 +172,24 @@ def ozaki_int8_ops(sys_, gks, slices):
 # small case (traffic grows with the k-points: the operands are read once per
 # k-point and H/O written once), scaled to a launch by the k-points it covers:
 #   split precision: oz_mma_kernel<OZ_HO,2,2>, 2 k-points: 131.6 MB read +
-#     35.2 MB written (profiles/oz_mma_si_cube8_nk2.md);
+#     35.2 MB written with 7 slices (profiles/oz_mma_si_cube8_nk2.md), 118.6 MB
+#     read + 5.5 MB written with 14 moduli (profiles/oz_mma_mod_si_cube8_nk2.md);
 #   FP64: zgemm_dmma_kernel<1> + <2>, 6 k-points: 673.5 MB read + 143.1 MB
 #     written (profiles/zgemm_dmma_si_cube8_nk6.md).
-PROFILED_DRAM_BYTES_PER_K = {"ozaki": (131.6e6 + 35.2e6) / 2, "fp64": (673.5e6 + 143.1e6) / 6}
+PROFILED_DRAM_BYTES_PER_K = {"ozaki": (131.6e6 + 35.2e6) / 2, "fp64": (673.5e6 + 143.1e6) / 6,
+                             "ozaki_mod": (118.6e6 + 5.5e6) / 2}
 
 
 def main_bytes(sys_, gks, precision, slices):
     """Algorithmic DRAM bytes of the MT contraction launch(es): operands read
-    once (int8 slices of Ar, Ai, Br, Bi; or the FP64 A and B planes) and the
-    N x N block of H and O written once."""
+    once (int8 slices or residues of Ar, Ai, Br, Bi, `slices` planes each; or
+    the FP64 A and B planes) and the N x N block of H and O written once."""
     K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
     total = 0.0
     for g in gks:
         n = g.ngp
         npad = (n + 63) // 64 * 64
-        if precision == "ozaki":
+        if precision != "fp64":
             kp8 = (K + 255) // 256 * 256
             total += 4.0 * slices * npad * kp8
         else:
@@ -466,8 +485,9 @@ def run_ours(args):
     gks = s.gksets()[: args.nk]
     nk = len(gks)
     st = Setup(s, max_batch=nk)
-    if args.precision == "ozaki":
-        st.set_precision("ozaki", args.slices)
+    if args.precision != "fp64":
+        st.set_precision(args.precision, args.slices if args.precision == "ozaki" else args.moduli)
+        planes, products, dtype_text, prec_text = split_scheme(args, s)
     stream = torch.cuda.Stream()
     st.set_stream(stream.cuda_stream)
     ngkmax, nlotot = st.ngkmax, st.nlotot
@@ -599,7 +619,7 @@ def run_ours(args):
     # ---- split precision: its error against the native FP64 path (k-point 0)
     # and the FP64 path's own device-resident rate for comparison
     accuracy, fp64_value = None, None
-    if args.precision == "ozaki":
+    if args.precision != "fp64":
         st.setup_batched_device(ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op)
         st.synchronize()
         h_oz = d_h[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
@@ -642,16 +662,16 @@ def run_ours(args):
         main_ms = phase[2]
         peak64 = _measured_fp64_peak(torch)
         achieved = fl / (main_ms * 1e-3) / 1e12
-        if args.precision == "ozaki":
-            ops = ozaki_int8_ops(s, gks, args.slices)
+        if args.precision != "fp64":
+            ops = ozaki_int8_ops(s, gks, products)
             peak8 = _measured_int8_peak(torch)
             a8 = ops / (main_ms * 1e-3) / 1e12
             roof = {"bound": "tensor", "kernel": "oz_mma_kernel (tcgen05.mma kind::i8, MT contraction)",
                     "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                     "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
-                    "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_PER_K["ozaki"] * nk,
+                    "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_PER_K[args.precision] * nk,
                     "traffic_note": "bytes per launch: ncu dram__bytes_read+write of a 2 k-point capture scaled "
-                                    "by k-points; algorithmic %.3g" % main_bytes(s, gks, "ozaki", args.slices),
+                                    "by k-points; algorithmic %.3g" % main_bytes(s, gks, args.precision, planes),
                     "fp64_equivalent": {"achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                                         "frac": achieved / peak64,
                                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}}
@@ -669,12 +689,11 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "i8 slices, f64 recombination" if args.precision == "ozaki" else "f64", "data": "synthetic",
+            "dtype": dtype_text if args.precision != "fp64" else "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "k_per_step": nk, "ngp": [min(ngp), max(ngp)],
                        "nmat": [min(nmat), max(nmat)],
                        "kernel_config": tuned,
-                       "precision": ("split int8 x%d slices (tcgen05), FP64 recombination" % args.slices
-                                     if args.precision == "ozaki" else "fp64 (DMMA)"),
+                       "precision": prec_text if args.precision != "fp64" else "fp64 (DMMA)",
                        "l2": "working set > 126 MB L2 (A/B planes 63 MB and H/O 48 MB per k-point), no flush"},
             "e2e": None if e2e_value is None else {
                 "value": e2e_value, "unit": "setups/s", "h2d_bytes_per_step": int(h2d),
@@ -801,7 +820,10 @@ def run_large(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item()), phase / max(nsteps, 1), rows
 
-    st.set_precision("ozaki", args.slices)
+    prec = args.precision if args.precision != "fp64" else "ozaki_mod"
+    st.set_precision(prec, args.slices if prec == "ozaki" else args.moduli)
+    args.precision = prec
+    planes, products, dtype_text, prec_text = split_scheme(args, s)
     ms, phase, rows = timed(args.steps, args.warmup, True)
     value = len(gks_all) * args.steps / (ms * 1e-3)
     # accuracy of the split precision against the native FP64 path, k-point 0, whole matrices
@@ -819,7 +841,7 @@ def run_large(args):
            "rel_fro_H": _rel_fro_dev(h8, d_h[: 2 * m0 * m0]), "rel_fro_O": _rel_fro_dev(o8, d_o[: 2 * m0 * m0])}
     del h8, o8
     if rank == 0:
-        ops = ozaki_int8_ops(s, gks_all, args.slices)
+        ops = ozaki_int8_ops(s, gks_all, products)
         fl = main_flops(s, gks_all)
         peak8 = _measured_int8_peak(torch)
         peak64 = _measured_fp64_peak(torch)
@@ -828,13 +850,14 @@ def run_large(args):
         out = {
             "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "i8 slices, f64 recombination",
+            "scaling": "strong", "vs_baseline": None, "dtype": dtype_text,
             "data": "synthetic",
             "config": {"workload": WORKLOAD_216, "k_per_step": len(gks_all),
                        "ngp": [min(g.ngp for g in gks_all), max(g.ngp for g in gks_all)],
                        "nmat": [min(g.ngp for g in gks_all) + nlotot, max(g.ngp for g in gks_all) + nlotot],
-                       "precision": "split int8 x%d slices (tcgen05), FP64 recombination" % args.slices,
-                       "l2": "working set (A/B planes 30 GB, slices 27 GB, H/O 27 GB) far above L2, no flush"},
+                       "precision": prec_text,
+                       "l2": "working set (A/B planes 30 GB, %d int8 planes of 4 arrays, H/O 27 GB) far above "
+                             "L2, no flush" % planes},
             "e2e": None,
             "e2e_note": "H and O are 13.7 GB each per k-point; host staging of that size is not measured",
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
@@ -885,7 +908,7 @@ def run_cells(args):
     for s in cells:
         gk = s.gkset(s.kpoints[0])
         st = Setup(s, max_batch=1)
-        st.set_precision(args.precision, args.slices)
+        st.set_precision(args.precision, args.slices if args.precision != "ozaki_mod" else args.moduli)
         ig = np.zeros(st.ngkmax, dtype=np.int32)
         ig[: gk.ngp] = gk.igpig
         vg = np.zeros((st.ngkmax, 3))
@@ -947,7 +970,8 @@ def run_cells(args):
             "metric": METRIC, "value": ncell * args.steps / (ms * 1e-3), "unit": "setups/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "i8 slices, f64 recombination" if args.precision == "ozaki" else "f64",
+            "dtype": {"ozaki": "i8 slices, f64 recombination", "fp64": "f64"}.get(
+                args.precision, "i8 residues modulo coprime moduli (per-cell count), CRT recombination"),
             "data": "synthetic",
             "config": {"workload": WORKLOAD_CELLS, "cells_per_step": ncell, "ngp": [min(ngp), max(ngp)],
                        "precision": args.precision, "kernel_configs": sorted(set(tuned)),
@@ -1005,12 +1029,15 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true", help="no host-pointer leg (profiling runs)")
     ap.add_argument("--skip-hmlint", action="store_true", help="no muffin-tin integral leg (profiling runs)")
     ap.add_argument("--skip-rttddft", action="store_true", help="no RT-TDDFT update leg (profiling runs)")
-    ap.add_argument("--precision", default="ozaki", choices=["fp64", "ozaki"],
-                    help="MT contraction arithmetic (the native FP64 path is timed beside the split one)")
+    ap.add_argument("--precision", default="ozaki_mod", choices=["fp64", "ozaki", "ozaki_mod"],
+                    help="MT contraction arithmetic: ozaki_mod = int8 residues modulo coprime moduli, "
+                         "ozaki = int8 slices (the native FP64 path is timed beside either)")
     ap.add_argument("--workload", default="cube8", choices=["cube8", "cube216", "cells256"],
                     help="cube8: 8-atom cell, 27 k per step; cube216: 216-atom cell, 4 k per step; "
                          "cells256: 256 independent 2-atom cells per step in one graph")
     ap.add_argument("--slices", type=int, default=7, help="int8 slices per operand (ozaki)")
+    ap.add_argument("--moduli", type=int, default=0,
+                    help="moduli of ozaki_mod (0: the fewest that keep 44 bits per operand)")
     ap.add_argument("--leg", default="setup", choices=["setup", "hmlint"],
                     help="hmlint: only the muffin-tin integral generation of --workload (cube8 or cube216)")
     args = ap.parse_args()

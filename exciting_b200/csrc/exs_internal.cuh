@@ -56,7 +56,8 @@ struct OzScheme {
     double fin, finx;
     int p[OZ_MAX_MODULI];
     int mg[OZ_MAX_MODULI];             // round(2^32 / p): quotient estimate by a multiply-high
-    int c32[OZ_MAX_MODULI], c16[OZ_MAX_MODULI];   // 2^32 mod p, 2^16 mod p
+    float fp[OZ_MAX_MODULI], finv[OZ_MAX_MODULI];  // p and 1/p in FP32 (the split kernels)
+    float fc[3][OZ_MAX_MODULI];        // 2^13, 2^26, 2^39 mod p
     unsigned long long c[OZ_MAX_MODULI];
 };
 

@@ -230,21 +230,35 @@ __device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, i
     return (((size_t)s * OZ_NARR + a) * npad + g) * (size_t)kp8 + f;
 }
 
-// Residue of the integer x (|x| <= 2^52) modulo p_m in [-127, 127], in
-// 32-bit integer arithmetic: x = xh 2^32 + xm 2^16 + xl (xh signed,
-// |xh| <= 2^20; xm, xl in [0, 2^16)) gives v = xh (2^32 mod p) + xm (2^16
-// mod p) + xl = x (mod p), |v| < 2^29; v - floor(v mg / 2^32) p lies in
-// [-p/4, 5p/4] (mg = round(2^32 / p)), and one subtraction of p above 127
-// brings it into [-127, 127] (p <= 255).
-__device__ __forceinline__ int oz_residue(long long x, const OzScheme &sch, int m)
+// Residues of an integer x (|x| <= 2^52) in exact FP32 arithmetic: with
+// 13-bit limbs x = x3 2^39 + x2 2^26 + x1 2^13 + x0 (x3 signed, |x3| <=
+// 2^13; the others in [0, 2^13)), v = x3 (2^39 mod p) + x2 (2^26 mod p) +
+// x1 (2^13 mod p) + x0 = x (mod p) has every partial sum an integer below
+// 2^23, so each FMA is exact.  q = round(v / p) by one FMA with 1.5 * 2^23
+// (|v / p| < 2^15; the error of 1/p in FP32 moves v/p by under 2^-9), and
+// r = v - q p is exact with |r| <= (p + 1) / 2 <= 127 for odd p <= 253.
+// The byte of r is the low byte of the FP32 bits of 1.5 * 2^23 + r.
+struct OzLimbs {
+    float l[4];
+};
+
+__device__ __forceinline__ OzLimbs oz_limbs(long long x)
 {
-    const int p = sch.p[m];
-    const int xh = (int)(x >> 32);
-    const uint32_t lo = (uint32_t)x;
-    const int v = xh * sch.c32[m] + (int)(lo >> 16) * sch.c16[m] + (int)(lo & 0xffffu);
-    int r = v - __mulhi(v, sch.mg[m]) * p;
-    if (r > 127) r -= p;
-    return r;
+    OzLimbs t;
+    t.l[0] = (float)(int)(x & 0x1fff);
+    t.l[1] = (float)(int)((x >> 13) & 0x1fff);
+    t.l[2] = (float)(int)((x >> 26) & 0x1fff);
+    t.l[3] = (float)(int)(x >> 39);
+    return t;
+}
+
+__device__ __forceinline__ uint32_t oz_residue_byte(const OzLimbs &x, const OzScheme &sch, int m)
+{
+    constexpr float MAGIC = 12582912.0f;           // 1.5 * 2^23
+    const float v = fmaf(x.l[3], sch.fc[2][m], fmaf(x.l[2], sch.fc[1][m], fmaf(x.l[1], sch.fc[0][m], x.l[0])));
+    const float q = fmaf(v, sch.finv[m], MAGIC) - MAGIC;
+    const float r = fmaf(-q, sch.fp[m], v);
+    return __float_as_uint(r + MAGIC) & 0xffu;
 }
 
 __device__ __forceinline__ void oz_put(uint32_t (&o0)[16], uint32_t (&o1)[16], int e, uint32_t w0, uint32_t w1)
@@ -404,18 +418,17 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
     if (sch.mod) {
         // x' = rint(x 2^b / sigma) (power-of-two scaling: exact), then its residues
         const double sc = rs * ldexp(1.0, sch.b);
-        long long xq[2][8];
+        OzLimbs xq[2][8];
 #pragma unroll
         for (int e = 0; e < 8; e++)
 #pragma unroll
-            for (int a = 0; a < 2; a++) xq[a][e] = __double2ll_rn(t[a][fl + e][gl] * sc);
+            for (int a = 0; a < 2; a++) xq[a][e] = oz_limbs(__double2ll_rn(t[a][fl + e][gl] * sc));
         for (int m = 0; m < S; m++) {
 #pragma unroll
             for (int a = 0; a < 2; a++) {
                 uint32_t w[2] = {0, 0};
 #pragma unroll
-                for (int e = 0; e < 8; e++)
-                    w[e >> 2] |= ((uint32_t)(uint8_t)(int8_t)oz_residue(xq[a][e], sch, m)) << (8 * (e & 3));
+                for (int e = 0; e < 8; e++) w[e >> 2] |= oz_residue_byte(xq[a][e], sch, m) << (8 * (e & 3));
                 *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(m, a0 + a, g, f, p.npad, kp8)) = make_uint2(w[0], w[1]);
             }
         }
@@ -516,19 +529,18 @@ __global__ void oz_xsplit_kernel(DevParams p, OzAtomArgs xa, const __grid_consta
     }
     if (sch.mod) {
         const double sc = ldexp(1.0, sch.bx);
-        long long xq[2][4];
+        OzLimbs xq[2][4];
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-            xq[0][e] = __double2ll_rn(x[0][e] * sc);
-            xq[1][e] = __double2ll_rn(x[1][e] * sc);
+            xq[0][e] = oz_limbs(__double2ll_rn(x[0][e] * sc));
+            xq[1][e] = oz_limbs(__double2ll_rn(x[1][e] * sc));
         }
         for (int m = 0; m < S; m++)
 #pragma unroll
             for (int a = 0; a < 2; a++) {
                 uint32_t w = 0;
 #pragma unroll
-                for (int e = 0; e < 4; e++)
-                    w |= ((uint32_t)(uint8_t)(int8_t)oz_residue(xq[a][e], sch, m)) << (8 * e);
+                for (int e = 0; e < 4; e++) w |= oz_residue_byte(xq[a][e], sch, m) << (8 * e);
                 const size_t row = ((((size_t)ias * S + m) * xa.nxb + xb) * 2 + a) * 64 + n;
                 *reinterpret_cast<uint32_t *>(xa.xs + row * xa.lw + k4) = w;
             }
@@ -1253,10 +1265,11 @@ int oz_seg_pairs(int S, int kp8)
     return (int)(n < 1 ? 0 : (n > S ? S : n));
 }
 
-// Pairwise coprime odd moduli below 256, largest first (247 = 13 * 19,
-// 217 = 7 * 31; the others are primes or 255 = 3 * 5 * 17, 253 = 11 * 23).
-static const int OZ_MODULI[OZ_MAX_MODULI] = {255, 253, 251, 247, 241, 239, 233, 229,
-                                             227, 223, 217, 211, 199, 197, 193, 191};
+// Pairwise coprime odd moduli up to 253, largest first (253 = 11 * 23,
+// 247 = 13 * 19, 217 = 7 * 31, 185 = 5 * 37; the others are primes).  At
+// most 253 so that a rounded residue |r| <= (p + 1) / 2 fits int8.
+static const int OZ_MODULI[OZ_MAX_MODULI] = {253, 251, 247, 241, 239, 233, 229, 227,
+                                             223, 217, 211, 199, 197, 193, 191, 185};
 
 // Bits per operand so that |X| <= 2K 2^(b + b') < M / 2 for a product of
 // 2K int terms; log2 M is a sum of logarithms, taken with a margin.
@@ -1278,7 +1291,9 @@ static int oz_inverse_mod(long long a, long long p)
     return r0 == 1 ? (int)(((t0 % p) + p) % p) : -1;
 }
 
-// The modular scheme for n moduli (0: the fewest in 6..16 that keep b >= 48),
+// The modular scheme for n moduli (0: the fewest in 6..16 that keep b >= 44;
+// at 44 bits the quantisation error is already below the floor of the
+// 64-bit recombination, sum |r| / 2 units of 2^-64 M),
 // contraction length K (H/O tiles) and per-atom window kx.  Returns 0, or
 // -1 if no valid plan exists (n out of range, b or bx below 8, or K past
 // the exact int32 range of one product: 2 K 127^2 < 2^31).
@@ -1288,7 +1303,7 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
     if (n == 0) {
         n = OZ_MAX_MODULI;
         for (int q = 6; q <= OZ_MAX_MODULI; q++)
-            if (oz_mod_bits(q, K) >= 2 * 48) {
+            if (oz_mod_bits(q, K) >= 2 * 44) {
                 n = q;
                 break;
             }
@@ -1317,8 +1332,9 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
         if (y < 0) return -1;
         s.p[m] = p;
         s.mg[m] = (int)((((long long)1 << 32) + p / 2) / p);
-        s.c32[m] = (int)((((long long)1 << 32)) % p);
-        s.c16[m] = (1 << 16) % p;
+        s.fp[m] = (float)p;
+        s.finv[m] = 1.0f / (float)p;
+        for (int j = 0; j < 3; j++) s.fc[j][m] = (float)((1LL << (13 * (j + 1))) % p);
         // round(2^64 y / p); y < p, so the quotient is below 2^64
         const unsigned __int128 num = ((unsigned __int128)y << 64) + (unsigned)(p / 2);
         s.c[m] = (unsigned long long)(num / (unsigned)p);

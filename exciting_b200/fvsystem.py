@@ -464,6 +464,21 @@ class SetupGraph:
             pass
 
 
+def ozaki_moduli(n: int, K: int, kx: int):
+    """The modular plan of exs_set_precision(EXS_PREC_OZAKI_MOD, n) for contraction
+    length K and per-atom windows of kx rows: (moduli, CRT constants, b, bx)."""
+    lib = abi.load()
+    n_out, b, bx = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    p = np.zeros(16, dtype=np.int32)
+    c = np.zeros(16, dtype=np.uint64)
+    rc = lib.exs_ozaki_moduli(int(n), int(K), int(kx), ctypes.byref(n_out), _ptr(p), _ptr(c), ctypes.byref(b),
+                              ctypes.byref(bx))
+    if rc != 0:
+        raise abi.ExsError(rc, "no modular plan for n=%d K=%d kx=%d" % (n, K, kx))
+    m = n_out.value
+    return [int(x) for x in p[:m]], [int(x) for x in c[:m]], b.value, bx.value
+
+
 def multi_graph(setups, batches) -> SetupGraph:
     """One CUDA graph over several contexts (exs_graph_create_multi).
 

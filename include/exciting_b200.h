@@ -148,7 +148,7 @@ int exs_fderiv_int(int n, const double *x, const double *f, double *result);
 /* Select the MT contraction arithmetic: EXS_PREC_FP64 (native FP64),
  * EXS_PREC_OZAKI_INT8 with `slices` int8 slices per operand (3..9), or
  * EXS_PREC_OZAKI_MOD: the operands as integers modulo `slices` pairwise
- * coprime odd moduli (6..16; 0 = the fewest that keep 48 bits per operand
+ * coprime odd moduli (6..16; 0 = the fewest that keep 44 bits per operand
  * for this context's K), one int8 product per modulus, recombined by the
  * Chinese remainder theorem.  No reference counterpart (the reference's
  * contraction is zgemm in FP64). */

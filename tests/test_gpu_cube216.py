@@ -6,8 +6,8 @@ through properties that do not depend on size:
 * a 192 x 192 APW block of H and O (random rows/columns) against the oracle
   evaluated on that G+k subset (exact for APW-APW entries);
 * the conjugate mirror is exact on whole rows/columns;
-* the split-precision result within 1e-12 (Frobenius, relative) of the
-  native FP64 result over the whole matrices.
+* the split-precision results (slices and moduli) within 1e-12
+  (Frobenius, relative) of the native FP64 result over the whole matrices.
 Device memory: about 140 GB (context 85 GB, two H/O pairs 55 GB).
 """
 import numpy as np
@@ -90,4 +90,14 @@ def test_cube216_fp64_and_split_precision():
         assert _strips_hermitian(t, m, idx)
     eh, eo = _rel_fro_dev(h8, h64), _rel_fro_dev(o8, o64)
     print(f"216-atom split precision vs FP64: dH {eh:.3e}  dO {eo:.3e}")
+    assert eh <= TOL_FRO and eo <= TOL_FRO
+    # the modular mode (more int8 planes: the slice buffers are replaced, H8/O8 reused)
+    st.set_precision("ozaki_mod", 0)
+    run(h8, o8)
+    for t, ref in ((h8, hb), (o8, ob)):
+        got = _block(t, m, idx)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= TOL_FRO
+        assert _strips_hermitian(t, m, idx)
+    eh, eo = _rel_fro_dev(h8, h64), _rel_fro_dev(o8, o64)
+    print(f"216-atom modular split precision vs FP64: dH {eh:.3e}  dO {eo:.3e}")
     assert eh <= TOL_FRO and eo <= TOL_FRO

@@ -100,7 +100,7 @@ def test_ozaki_mod_error_falls_with_moduli():
     hr, orf = O.hamiltonandoverlapsetup(s, gk)
     st = Setup(s)
     errs = []
-    for n in (6, 8, 10, 12):
+    for n in (6, 8, 10, 13):
         st.set_precision("ozaki_mod", n)
         h, o = st.hamiltonandoverlapsetup(gk)
         errs.append(rel_fro(h, hr))

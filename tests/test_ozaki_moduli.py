@@ -53,10 +53,10 @@ def test_plan_constants_and_bounds(n, K, kx):
     # b is the largest that fits (unless capped at 52)
     assert b == 52 or 2 * K * 2 ** (2 * (b + 1)) >= M // 2
     if n == 0:
-        assert b >= 48
-        if len(ps) > 6:    # one modulus fewer would not keep 48 bits
+        assert b >= 44
+        if len(ps) > 6:    # one modulus fewer would not keep 44 bits
             Mf = math.prod(ps[:-1])
-            assert 2 * K * 2 ** 96 >= Mf // 2
+            assert 2 * K * 2 ** 88 >= Mf // 2
 
 
 def test_plan_rejects_bad_arguments():
@@ -147,21 +147,24 @@ def test_emulated_contraction_meets_the_bar():
 
 
 def test_split_residue_formula():
-    """The split kernels' integer residue: x = xh 2^32 + xm 2^16 + xl, v = xh (2^32 mod p)
-    + xm (2^16 mod p) + xl, r = v - floor(v round(2^32/p) / 2^32) p, minus p once above
-    127: r = x (mod p) and |r| <= 127 for |x| <= 2^52 and every modulus of the table."""
+    """The split kernels' FP32 residue: 13-bit limbs, v = x3 (2^39 mod p) + x2 (2^26 mod p)
+    + x1 (2^13 mod p) + x0 with integer partial sums below 2^24 (exact in FP32), q =
+    round(v / p) as one FMA v * fl(1/p) + 1.5 2^23 rounded once to FP32, r = v - q p:
+    r = x (mod p) and |r| <= 127 for |x| <= 2^52 and every modulus of the table."""
     ps, _, _, _ = plan(16, 1000, 100)
     rng = np.random.default_rng(7)
-    xs = np.concatenate([rng.integers(-2 ** 52, 2 ** 52, size=4000, dtype=np.int64),
-                         np.array([0, 1, -1, 2 ** 52, -2 ** 52, 2 ** 32 - 1, -2 ** 32, 2 ** 48 + 12345],
+    xs = np.concatenate([rng.integers(-2 ** 52, 2 ** 52, size=20000, dtype=np.int64),
+                         np.array([0, 1, -1, 2 ** 52, -2 ** 52, 2 ** 39 - 1, -2 ** 39, 2 ** 48 + 12345],
                                   dtype=np.int64)])
+    limbs = [(xs & 0x1fff), (xs >> 13) & 0x1fff, (xs >> 26) & 0x1fff, xs >> 39]
+    magic = np.float64(1.5 * 2 ** 23)
     for p in ps:
-        mg, c32, c16 = ((1 << 32) + p // 2) // p, (1 << 32) % p, (1 << 16) % p
-        xh = xs >> 32
-        lo = xs & 0xffffffff
-        v = xh * c32 + (lo >> 16) * c16 + (lo & 0xffff)
-        assert np.abs(v).max() < 2 ** 31
-        r = v - ((v * mg) >> 32) * p
-        r = np.where(r > 127, r - p, r)
+        assert p <= 253
+        c = [(1 << 13) % p, (1 << 26) % p, (1 << 39) % p]
+        v = limbs[0] + limbs[1] * c[0] + limbs[2] * c[1] + limbs[3] * c[2]
+        assert np.abs(v).max() < 2 ** 23
+        inv = np.float64(np.float32(1.0 / p))
+        q = (v * inv + magic).astype(np.float32).astype(np.float64) - magic   # exact product, one rounding
+        r = (v - q * p).astype(np.int64)
         assert np.abs(r).max() <= 127
         assert np.all(np.mod(r - xs, p) == 0)
