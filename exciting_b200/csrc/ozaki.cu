@@ -49,10 +49,13 @@
 // one CTA per tile or a persistent grid of one CTA per SM, for the H/O tiles
 // and the per-atom tiles separately.
 //
-// Roles (one CTA per 128 x 32 output tile, 256 threads):
+// Roles (one CTA per 128 x 32 output tile, 384 threads):
 //   warps 0-1  one TMA producer thread each (the A box and the B box of a stage)
 //   warp 3     MMA issuer (one thread); allocates tensor memory
-//   warps 4-7  epilogue: segment folds and the final store
+//   warps 4-11 epilogue: segment folds and the final store, two warps per
+//              tensor-memory lane quadrant, each with two of the four value
+//              blocks (H/O tiles: half 0 Re H, Im H, half 1 Re O, Im O;
+//              per-atom tiles: half h the re and im blocks of rows 32h..32h+31)
 // The same kernel (MODE OZ_ATOM) forms the per-atom products B_a = h_a A_a
 // and the APW-lo rows loa_a A_a from int8 slices of h_a and loa.
 // Tensor memory (512 columns): r at [0,128), i at [128,256), FP64 sums (two
@@ -77,7 +80,7 @@ constexpr int OZ_N = 4 * OZ_BJ;
 constexpr int OZ_NARR = 4;                       // Br, Bi, Ar, Ai
 constexpr int OZ_CHUNK = 128;                    // bytes of K in one swizzle row
 constexpr int OZ_TILE = 128 * OZ_CHUNK;          // 16 KB: one K chunk of a 128-row operand
-constexpr int OZ_THREADS = 256;
+constexpr int OZ_THREADS = 384;                  // 12 warps: see the roles below
 constexpr int OZ_MAX_KCH = 2;                    // K chunks per stage of the widest configuration
 constexpr int OZ_TMEM_COLS = 512;
 constexpr int OZ_FP64_COL = 256;
@@ -305,12 +308,21 @@ __device__ __forceinline__ void oz_fold16(int g, bool init, int sg, const uint32
 // q & 1 of word q >> 1).  Value block o (32 values) = r block o +- i block
 // (o ^ 1) for the H/O tiles (Re H, Im H, Re O, Im O), (o ^ 2) for the
 // per-atom tiles (Re rows 0-63, Im rows 0-63).
+// Value blocks of an epilogue half: H/O tiles {2h, 2h + 1} (Re H, Im H or
+// Re O, Im O); per-atom tiles {h, h + 2} (re and im of rows 32h..32h+31).
 template <int MODE>
-__device__ __forceinline__ void oz_mod_read(uint32_t t_lane, const OzScheme &sch, int g, uint32_t (&rp)[64])
+__device__ __forceinline__ int oz_block(int half, int k)
+{
+    return MODE == OZ_HO ? 2 * half + k : half + 2 * k;
+}
+
+template <int MODE>
+__device__ __forceinline__ void oz_mod_read(uint32_t t_lane, const OzScheme &sch, int g, int half, uint32_t (&rp)[32])
 {
     const int pm = sch.p[g], mg = sch.mg[g];
 #pragma unroll
-    for (int o = 0; o < 4; o++) {
+    for (int k = 0; k < 2; k++) {
+        const int o = oz_block<MODE>(half, k);
         const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
         const bool minus = (MODE == OZ_HO) ? (o & 1) != 0 : o < 2;
         uint32_t r0[16], r1[16], i0[16], i1[16];
@@ -329,22 +341,25 @@ __device__ __forceinline__ void oz_mod_read(uint32_t t_lane, const OzScheme &sch
                 const int v = minus ? rv - iv : rv + iv;
                 res[h] = v - __mulhi(v, mg) * pm;
             }
-            rp[o * 16 + e / 2] = ((uint32_t)res[0] & 0xffffu) | ((uint32_t)res[1] << 16);
+            rp[k * 16 + e / 2] = ((uint32_t)res[0] & 0xffffu) | ((uint32_t)res[1] << 16);
         }
     }
 }
 
 // Phase 2: the 64-bit running sums t += r c_g (mod 2^64) in the FP64
-// columns, two 32-bit words per value (low first); t = r c_g for g = 0.
-__device__ __forceinline__ void oz_mod_accumulate(uint32_t t_lane, const OzScheme &sch, int g, const uint32_t (&rp)[64])
+// columns of this half's blocks, two 32-bit words per value (low first);
+// t = r c_g for g = 0.
+template <int MODE>
+__device__ __forceinline__ void oz_mod_accumulate(uint32_t t_lane, const OzScheme &sch, int g, int half,
+                                                  const uint32_t (&rp)[32])
 {
     const unsigned long long cm = sch.c[g];
     const bool init = g == 0;
 #pragma unroll
-    for (int o = 0; o < 4; o++)
+    for (int k = 0; k < 2; k++)
 #pragma unroll
         for (int jc = 0; jc < 32; jc += 16) {
-            const uint32_t fcol = OZ_FP64_COL + 2 * (o * 32 + jc);
+            const uint32_t fcol = OZ_FP64_COL + 2 * (oz_block<MODE>(half, k) * 32 + jc);
             uint32_t lo[16], hi[16];            // updated in place
             if (!init) {
                 tm_ld16(t_lane + fcol, lo);
@@ -353,7 +368,7 @@ __device__ __forceinline__ void oz_mod_accumulate(uint32_t t_lane, const OzSchem
             }
 #pragma unroll
             for (int e = 0; e < 16; e++) {
-                const int q = o * 32 + jc + e;
+                const int q = k * 32 + jc + e;
                 const int r = (int)(int16_t)(uint16_t)(rp[q >> 1] >> (16 * (q & 1)));
                 uint32_t &w0 = e < 8 ? lo[2 * e] : hi[2 * (e - 8)];
                 uint32_t &w1 = e < 8 ? lo[2 * e + 1] : hi[2 * (e - 8) + 1];
@@ -374,6 +389,76 @@ __device__ __forceinline__ double oz_final(const OzScheme &sch, double fin, uint
 {
     if (!sch.mod) return __hiloint2double((int)w1, (int)w0);
     return (double)(long long)(((unsigned long long)w1 << 32) | w0) * fin;
+}
+
+
+// Final store of one row of a 128 x 32 H/O tile by epilogue half `half`:
+// half 0 writes H (Re H, Im H scaled by sigma_A(i) sigma_B(j), plus the
+// hmlistln term), half 1 writes O (sigma_A(i) sigma_A(j), plus olpistln);
+// the upper triangle and its conjugate mirror, like the FP64 path.
+__device__ __forceinline__ void oz_store_ho(const DevParams &p, const KDesc &kd, const OzScheme &sch, int i0, int j0,
+                                            uint32_t t_lane, int row, int half)
+{
+    const int i = i0 + row;
+    int ivi[3] = {0, 0, 0};
+    double vi[3] = {0.0, 0.0, 0.0};
+    const bool row_ok = i < kd.ngp;
+    if (row_ok) {
+        int g = kd.igpig[i] - 1;
+        if (g < 0 || g >= p.ngrtot) {
+            atomicOr(p.err, DEV_ERR_INDEX);
+            g = 0;
+        }
+        for (int x = 0; x < 3; x++) {
+            ivi[x] = p.ivg[3 * g + x];
+            vi[x] = kd.vgpc[3 * i + x];
+        }
+    }
+    const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
+    const int kind = half == 0 ? EPI_HAM : EPI_OVL;
+    exs_complex *out = half == 0 ? kd.h : kd.o;
+    const double *scol = kd.oz_scale + (half == 0 ? p.npad : 0);
+#pragma unroll 1
+    for (int jc = 0; jc < OZ_BJ; jc += 8) {
+        double val[2][8];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            uint32_t w[16];
+            tm_ld16(t_lane + OZ_FP64_COL + 2 * ((2 * half + k) * 32 + jc), w);
+            tm_wait_ld();
+#pragma unroll
+            for (int e = 0; e < 8; e++) val[k][e] = oz_final(sch, sch.fin, w[2 * e], w[2 * e + 1]);
+        }
+        if (!row_ok) continue;
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int j = j0 + jc + e;
+            if (j >= kd.ngp || i > j) continue;
+            // column data (the same for the whole warp: broadcast loads)
+            int gj = kd.igpig[j] - 1;
+            if (gj < 0 || gj >= p.ngrtot) {
+                atomicOr(p.err, DEV_ERR_INDEX);
+                gj = 0;
+            }
+            const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
+            const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
+            const double sj = oz_sigma(scol[j]);
+            double re = val[0][e] * sai * sj, im = val[1][e] * sai * sj;
+            double ar, ai;
+            if (interstitial(p, kind, ivi, ivj, vi, vj, ar, ai)) {
+                re += ar;
+                im += ai;
+            }
+            exs_complex v;
+            v.re = re;
+            v.im = im;
+            out[(size_t)i + (size_t)kd.nmat * j] = v;
+            if (i < j) {
+                v.im = -im;
+                out[(size_t)j + (size_t)kd.nmat * i] = v;
+            }
+        }
+    }
 }
 
 // The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
@@ -629,7 +714,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             mbar_init(&empty[s], 1);
         }
         mbar_init(&accf, 1);
-        mbar_init(&acce, 4);
+        mbar_init(&acce, 8);                  // the eight epilogue warps
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -737,8 +822,9 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
         }
     } else {
-        // ------------------------------------------------ epilogue (warps 4..7)
+        // ------------------------------------------------ epilogue (warps 4..11)
         const int qd = warp & 3;                                    // tensor-memory lane quadrant
+        const int half = (warp - 4) >> 2;                           // which two value blocks
         const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
         int nseg = 0;
         bool bad = false;
@@ -753,20 +839,21 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     }
                     tc_fence_after();
                     if (mod) {
-                        uint32_t rp[64];
-                        oz_mod_read<MODE>(t_lane, sch, g, rp);
+                        uint32_t rp[32];
+                        oz_mod_read<MODE>(t_lane, sch, g, half, rp);
                         tc_fence_before();
                         __syncwarp();
                         if (lane == 0) mbar_arrive(&acce);          // the accumulators are free
                         nseg++;
-                        oz_mod_accumulate(t_lane, sch, g, rp);
+                        oz_mod_accumulate<MODE>(t_lane, sch, g, half, rp);
                         continue;
                     }
                     const bool init = (g == 0 && s0 == 1);      // first segment of the tile
                     // running-sum block o (32 values) = r block o +- i block (o ^ 1) (HO:
                     // Re H, Im H, Re O, Im O) or (o ^ 2) (ATOM: Re rows 0-63, Im rows 0-63)
 #pragma unroll 1
-                    for (int o = 0; o < 4; o++) {
+                    for (int k = 0; k < 2; k++) {
+                        const int o = oz_block<MODE>(half, k);
                         const int sg = (MODE == OZ_HO) ? ((o & 1) ? -1 : 1) : ((o < 2) ? -1 : 1);
                         const int oi = (MODE == OZ_HO) ? (o ^ 1) : (o ^ 2);
 #pragma unroll 1
@@ -799,75 +886,10 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             }
             const KDesc kd = ks[ti.k];
             if (MODE == OZ_HO) {
-                const int i = ti.i0 + qd * 32 + lane;
-                int ivi[3] = {0, 0, 0};
-                double vi[3] = {0.0, 0.0, 0.0};
-                const bool row_ok = i < kd.ngp;
-                if (row_ok) {
-                    int g = kd.igpig[i] - 1;
-                    if (g < 0 || g >= p.ngrtot) {
-                        atomicOr(p.err, DEV_ERR_INDEX);
-                        g = 0;
-                    }
-                    for (int x = 0; x < 3; x++) {
-                        ivi[x] = p.ivg[3 * g + x];
-                        vi[x] = kd.vgpc[3 * i + x];
-                    }
-                }
-                const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
-#pragma unroll 1
-                for (int jc = 0; jc < OZ_BJ; jc += 8) {
-                    double val[4][8];
-#pragma unroll
-                    for (int o = 0; o < 4; o++) {
-                        uint32_t w[16];
-                        tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
-                        tm_wait_ld();
-#pragma unroll
-                        for (int e = 0; e < 8; e++) val[o][e] = oz_final(sch, sch.fin, w[2 * e], w[2 * e + 1]);
-                    }
-                    if (!row_ok) continue;
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const int j = ti.j0 + jc + e;
-                        if (j >= kd.ngp || i > j) continue;
-                        // column data (the same for the whole warp: broadcast loads)
-                        int gj = kd.igpig[j] - 1;
-                        if (gj < 0 || gj >= p.ngrtot) {
-                            atomicOr(p.err, DEV_ERR_INDEX);
-                            gj = 0;
-                        }
-                        const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
-                        const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
-                        const double sbj = oz_sigma(kd.oz_scale[p.npad + j]), saj = oz_sigma(kd.oz_scale[j]);
-                        double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
-                        double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
-                        double ar, ai;
-                        if (interstitial(p, EPI_HAM, ivi, ivj, vi, vj, ar, ai)) {
-                            hr += ar;
-                            hi += ai;
-                        }
-                        if (interstitial(p, EPI_OVL, ivi, ivj, vi, vj, ar, ai)) {
-                            orr += ar;
-                            oi += ai;
-                        }
-                        exs_complex hv, ov;
-                        hv.re = hr;
-                        hv.im = hi;
-                        ov.re = orr;
-                        ov.im = oi;
-                        kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
-                        kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
-                        if (i < j) {
-                            hv.im = -hi;
-                            ov.im = -oi;
-                            kd.h[(size_t)j + (size_t)kd.nmat * i] = hv;
-                            kd.o[(size_t)j + (size_t)kd.nmat * i] = ov;
-                        }
-                    }
-                }
+                oz_store_ho(p, kd, sch, ti.i0, ti.j0, t_lane, qd * 32 + lane, half);
             } else {
-                // row G of the tile; values v = 0..63 real, 64..127 imaginary parts of the 64 output rows
+                // row G of the tile; values v = 0..63 real, 64..127 imaginary parts of the 64 output
+                // rows, of which this half holds rows 32 half .. 32 half + 31
                 const int g = ti.i0 + qd * 32 + lane;
                 const bool g_ok = g < p.npad;
                 const AtomDesc at = p.atoms[ti.ias];
@@ -877,7 +899,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 const size_t row0 = (size_t)kd.ngp + at.lo_off;
                 double bmax = 0.0;
 #pragma unroll 1
-                for (int jc = 0; jc < 64; jc += 8) {
+                for (int jc = 32 * half; jc < 32 * half + 32; jc += 8) {
                     uint32_t wr[16], wi[16];
                     tm_ld16(t_lane + OZ_FP64_COL + 2 * jc, wr);
                     tm_ld16(t_lane + OZ_FP64_COL + 2 * (64 + jc), wi);
@@ -1025,7 +1047,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             mbar_init(&empty[s], 1);
         }
         mbar_init(&accf, 1);
-        mbar_init(&acce, 8);             // CTA 0: four epilogue warps in each CTA
+        mbar_init(&acce, 16);            // CTA 0: eight epilogue warps in each CTA
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -1121,8 +1143,9 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                     if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
         }
     } else if (warp >= 4) {
-        // ------------------------------------------------ epilogue (both CTAs, warps 4..7)
+        // ------------------------------------------------ epilogue (both CTAs, warps 4..11)
         const int qd = warp & 3;
+        const int half = (warp - 4) >> 2;
         const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
         const uint32_t acce0 = mapa_shared(smem_u32(&acce), 0);
         int nseg = 0;
@@ -1136,18 +1159,19 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                 }
                 tc_fence_after();
                 if (mod) {
-                    uint32_t rp[64];
-                    oz_mod_read<OZ_HO>(t_lane, sch, g, rp);
+                    uint32_t rp[32];
+                    oz_mod_read<OZ_HO>(t_lane, sch, g, half, rp);
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive_remote(acce0);      // the accumulators are free
                     nseg++;
-                    oz_mod_accumulate(t_lane, sch, g, rp);
+                    oz_mod_accumulate<OZ_HO>(t_lane, sch, g, half, rp);
                     continue;
                 }
                 const bool init = (nseg == 0);
 #pragma unroll 1
-                for (int o = 0; o < 4; o++) {
+                for (int k = 0; k < 2; k++) {
+                    const int o = oz_block<OZ_HO>(half, k);
                     const int sg = (o & 1) ? -1 : 1;
 #pragma unroll 1
                     for (int jc = 0; jc < 32; jc += 16) {
@@ -1173,74 +1197,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                 nseg++;
             }
         }
-        if (__all_sync(0xffffffffu, !bad && !*abort)) {
-            const int i = i0 + qd * 32 + lane;
-            int ivi[3] = {0, 0, 0};
-            double vi[3] = {0.0, 0.0, 0.0};
-            const bool row_ok = i < kd.ngp;
-            if (row_ok) {
-                int g = kd.igpig[i] - 1;
-                if (g < 0 || g >= p.ngrtot) {
-                    atomicOr(p.err, DEV_ERR_INDEX);
-                    g = 0;
-                }
-                for (int x = 0; x < 3; x++) {
-                    ivi[x] = p.ivg[3 * g + x];
-                    vi[x] = kd.vgpc[3 * i + x];
-                }
-            }
-            const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
-#pragma unroll 1
-            for (int jc = 0; jc < OZ_BJ; jc += 8) {
-                double val[4][8];
-#pragma unroll
-                for (int o = 0; o < 4; o++) {
-                    uint32_t w[16];
-                    tm_ld16(t_lane + OZ_FP64_COL + 2 * (o * 32 + jc), w);
-                    tm_wait_ld();
-#pragma unroll
-                    for (int e = 0; e < 8; e++) val[o][e] = oz_final(sch, sch.fin, w[2 * e], w[2 * e + 1]);
-                }
-                if (!row_ok) continue;
-#pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const int j = j0 + jc + e;
-                    if (j >= kd.ngp || i > j) continue;
-                    int gj = kd.igpig[j] - 1;
-                    if (gj < 0 || gj >= p.ngrtot) {
-                        atomicOr(p.err, DEV_ERR_INDEX);
-                        gj = 0;
-                    }
-                    const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
-                    const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
-                    const double sbj = oz_sigma(kd.oz_scale[p.npad + j]), saj = oz_sigma(kd.oz_scale[j]);
-                    double hr = val[0][e] * sai * sbj, hi = val[1][e] * sai * sbj;
-                    double orr = val[2][e] * sai * saj, oi = val[3][e] * sai * saj;
-                    double ar, ai;
-                    if (interstitial(p, EPI_HAM, ivi, ivj, vi, vj, ar, ai)) {
-                        hr += ar;
-                        hi += ai;
-                    }
-                    if (interstitial(p, EPI_OVL, ivi, ivj, vi, vj, ar, ai)) {
-                        orr += ar;
-                        oi += ai;
-                    }
-                    exs_complex hv, ov;
-                    hv.re = hr;
-                    hv.im = hi;
-                    ov.re = orr;
-                    ov.im = oi;
-                    kd.h[(size_t)i + (size_t)kd.nmat * j] = hv;
-                    kd.o[(size_t)i + (size_t)kd.nmat * j] = ov;
-                    if (i < j) {
-                        hv.im = -hi;
-                        ov.im = -oi;
-                        kd.h[(size_t)j + (size_t)kd.nmat * i] = hv;
-                        kd.o[(size_t)j + (size_t)kd.nmat * i] = ov;
-                    }
-                }
-            }
-        }
+        if (__all_sync(0xffffffffu, !bad && !*abort)) oz_store_ho(p, kd, sch, i0, j0, t_lane, qd * 32 + lane, half);
     }
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
     tc_fence_before();
