@@ -395,9 +395,13 @@ __device__ __forceinline__ double oz_final(const OzScheme &sch, double fin, uint
 // Final store of one row of a 128 x 32 H/O tile by epilogue half `half`:
 // half 0 writes H (Re H, Im H scaled by sigma_A(i) sigma_B(j), plus the
 // hmlistln term), half 1 writes O (sigma_A(i) sigma_A(j), plus olpistln);
-// the upper triangle and its conjugate mirror, like the FP64 path.
+// the upper triangle and its conjugate mirror, like the FP64 path.  With
+// T (shared memory, OZ_MIRROR_LD x 64 values) the mirror values go to
+// T[(half * 32 + j - j0) * OZ_MIRROR_LD + row] instead, for oz_store_mirror.
+constexpr int OZ_MIRROR_LD = 129;                 // 16-byte values; odd stride: no bank conflicts
+
 __device__ __forceinline__ void oz_store_ho(const DevParams &p, const KDesc &kd, const OzScheme &sch, int i0, int j0,
-                                            uint32_t t_lane, int row, int half)
+                                            uint32_t t_lane, int row, int half, exs_complex *T)
 {
     const int i = i0 + row;
     int ivi[3] = {0, 0, 0};
@@ -455,9 +459,28 @@ __device__ __forceinline__ void oz_store_ho(const DevParams &p, const KDesc &kd,
             out[(size_t)i + (size_t)kd.nmat * j] = v;
             if (i < j) {
                 v.im = -im;
-                out[(size_t)j + (size_t)kd.nmat * i] = v;
+                if (T)
+                    T[(half * 32 + jc + e) * OZ_MIRROR_LD + row] = v;
+                else
+                    out[(size_t)j + (size_t)kd.nmat * i] = v;
             }
         }
+    }
+}
+
+// The staged mirror of a 128 x 32 H/O tile, written as whole columns: the
+// 256 (matrix, row i) pairs are split over the eight epilogue warps (ew =
+// 0..7); lane l writes element (j0 + l, i), so each warp store covers 32
+// consecutive rows of one column (512 contiguous bytes).
+__device__ __forceinline__ void oz_store_mirror(const KDesc &kd, int i0, int j0, const exs_complex *T, int ew, int lane)
+{
+    const int j = j0 + lane;
+#pragma unroll 4
+    for (int q = 0; q < 32; q++) {
+        const int pr = ew * 32 + q, h = pr >> 7, il = pr & 127;
+        const int i = i0 + il;
+        if (i < kd.ngp && j < kd.ngp && i < j)
+            (h ? kd.o : kd.h)[(size_t)j + (size_t)kd.nmat * i] = T[(h * 32 + lane) * OZ_MIRROR_LD + il];
     }
 }
 
@@ -695,13 +718,18 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     constexpr int BOX = KCH * OZ_TILE;          // one operand of a stage
     constexpr int STAGE = 3 * BOX;              // A box [chunk][Ar, Ai][128 rows], B box [chunk][128 rows]
     extern __shared__ __align__(1024) uint8_t oz_smem[];
-    __shared__ uint64_t full[NST], empty[NST], accf, acce;
+    __shared__ uint64_t full[NST], empty[NST], accf, acce, stg;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
     volatile int *abort = &abort_sh;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
+    // one tile per CTA: at the final store the stage buffers are idle and
+    // hold the H/O mirror (2 x 32 x OZ_MIRROR_LD values, below the stages' size)
+    static_assert(2 * 32 * OZ_MIRROR_LD * 16 <= NST * 3 * KCH * OZ_TILE, "mirror staging fits the stages");
+    const bool staged = MODE == OZ_HO && (int)gridDim.x >= ntiles;
+    exs_complex *mirror = reinterpret_cast<exs_complex *>(oz_smem + (sbase - smem_u32(oz_smem)));
 
     if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
@@ -715,6 +743,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
         }
         mbar_init(&accf, 1);
         mbar_init(&acce, 8);                  // the eight epilogue warps
+        mbar_init(&stg, 8);                   // the mirror is staged (one tile per CTA only)
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -886,7 +915,13 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             }
             const KDesc kd = ks[ti.k];
             if (MODE == OZ_HO) {
-                oz_store_ho(p, kd, sch, ti.i0, ti.j0, t_lane, qd * 32 + lane, half);
+                oz_store_ho(p, kd, sch, ti.i0, ti.j0, t_lane, qd * 32 + lane, half, staged ? mirror : nullptr);
+                if (staged) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&stg);
+                    if (__all_sync(0xffffffffu, mbar_wait_ab(&stg, 0, abort)))
+                        oz_store_mirror(kd, ti.i0, ti.j0, mirror, warp - 4, lane);
+                }
             } else {
                 // row G of the tile; values v = 0..63 real, 64..127 imaginary parts of the 64 output
                 // rows, of which this half holds rows 32 half .. 32 half + 31
@@ -1023,13 +1058,14 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
     constexpr int BBOX = KCH * OZ_TILE / 2;          // this CTA's 64 rows of B
     constexpr int STAGE = ABOX + BBOX;
     extern __shared__ __align__(1024) uint8_t oz_smem[];
-    __shared__ uint64_t full[NST], empty[NST], accf, acce;
+    __shared__ uint64_t full[NST], empty[NST], accf, acce, stg;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
     volatile int *abort = &abort_sh;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t rank = cluster_ctarank();
+    static_assert(2 * 32 * OZ_MIRROR_LD * 16 <= NST * STAGE, "mirror staging fits the stages");
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
     const int t3 = 3 * (blockIdx.x >> 1);
     const KDesc kd = ks[tiles[t3]];
@@ -1048,6 +1084,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
         }
         mbar_init(&accf, 1);
         mbar_init(&acce, 16);            // CTA 0: eight epilogue warps in each CTA
+        mbar_init(&stg, 8);              // this CTA's epilogue warps: the mirror is staged
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -1197,7 +1234,13 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                 nseg++;
             }
         }
-        if (__all_sync(0xffffffffu, !bad && !*abort)) oz_store_ho(p, kd, sch, i0, j0, t_lane, qd * 32 + lane, half);
+        exs_complex *mirror = reinterpret_cast<exs_complex *>(oz_smem + (sbase - smem_u32(oz_smem)));
+        if (__all_sync(0xffffffffu, !bad && !*abort))
+            oz_store_ho(p, kd, sch, i0, j0, t_lane, qd * 32 + lane, half, mirror);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&stg);
+        if (__all_sync(0xffffffffu, mbar_wait_ab(&stg, 0, abort) && !*abort))
+            oz_store_mirror(kd, i0, j0, mirror, warp - 4, lane);
     }
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
     tc_fence_before();
