@@ -172,12 +172,12 @@ def ozaki_int8_ops(sys_, gks, products):
 # small case (traffic grows with the k-points: the operands are read once per
 # k-point and H/O written once), scaled to a launch by the k-points it covers:
 #   split precision: oz_mma_kernel<OZ_HO,2,2>, 2 k-points: 131.6 MB read +
-#     35.2 MB written with 7 slices (profiles/oz_mma_si_cube8_nk2.md), 118.6 MB
-#     read + 5.5 MB written with 14 moduli (profiles/oz_mma_mod_si_cube8_nk2.md);
+#     35.2 MB written with 7 slices (profiles/oz_mma_si_cube8_nk2.md), 227.2 MB
+#     read + 37.4 MB written with 13 moduli (profiles/oz_mma_mod_si_cube8_nk2.md);
 #   FP64: zgemm_dmma_kernel<1> + <2>, 6 k-points: 673.5 MB read + 143.1 MB
 #     written (profiles/zgemm_dmma_si_cube8_nk6.md).
 PROFILED_DRAM_BYTES_PER_K = {"ozaki": (131.6e6 + 35.2e6) / 2, "fp64": (673.5e6 + 143.1e6) / 6,
-                             "ozaki_mod": (118.6e6 + 5.5e6) / 2}
+                             "ozaki_mod": (227.2e6 + 37.4e6) / 2}
 
 
 def main_bytes(sys_, gks, precision, slices):
