@@ -81,6 +81,24 @@ def test_ozaki_cube8_batched_vs_oracle(mode):
     assert eig_dev(w, wr) <= 1.0
 
 
+@pytest.mark.parametrize("mode", MODES)
+def test_ozaki_two_species_vs_oracle(mode):
+    """Different bases per species (apword 1 and 2, lmaxmat < lmaxapw, lo on
+    one species only): per-atom windows of different widths in the int8
+    per-atom products, batched over both k-points."""
+    s = W.sic_two_species()
+    gks = s.gksets()
+    st = _setup(s, mode=mode, max_batch=len(gks))
+    out = st.setup_batched(gks)
+    for gk, (h, o) in zip(gks, out):
+        hr, orf = O.hamiltonandoverlapsetup(s, gk)
+        assert rel_fro(h, hr) <= TOL_FRO, rel_fro(h, hr)
+        assert rel_fro(o, orf) <= TOL_FRO, rel_fro(o, orf)
+        w = sl.eigh(h, o, eigvals_only=True, subset_by_index=[0, 19])
+        wr = sl.eigh(hr, orf, eigvals_only=True, subset_by_index=[0, 19])
+        assert eig_dev(w, wr) <= 1.0
+
+
 def test_ozaki_error_falls_with_slices():
     s = W.si_fcc("text")
     gk = s.gkset(s.kpoints[3])
