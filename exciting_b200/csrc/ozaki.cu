@@ -1,5 +1,7 @@
-// Split-precision (Ozaki scheme, int8 slices) MT contraction on the 5th-gen
-// tensor cores (tcgen05.mma kind::i8, int32 accumulators in tensor memory).
+// Split-precision MT contraction on the 5th-gen tensor cores (tcgen05.mma
+// kind::i8, int32 accumulators in tensor memory): int8 slices (Ozaki scheme)
+// or int8 residues modulo coprime moduli (the modular scheme, the default
+// of the benchmark).
 //
 // H = A^H B and O = A^H A in real arithmetic: with the real and imaginary
 // planes of A and B,
@@ -32,7 +34,10 @@
 // sum t += r c_m (mod 2^64), c_m = round(2^64 y_m / p_m), in the tensor-memory
 // columns of the FP64 sums; the error of the rounded constants is at most
 // sum |r| / 2 units of 2^-64 M.  n products replace the n(n+1)/2 slice pairs
-// (14 moduli keep 48 bits per operand at K = 1936, where 7 slices keep 49).
+// (13 moduli keep 44 bits per operand at K = 1936, 14 keep 46 at K = 34,992;
+// 7 slices cost 28 products).  The fold runs in two phases: phase 1 reads r
+// and i, reduces v = r +- i below 16 bits and releases the accumulators to
+// the next modulus's MMAs; phase 2 updates the 64-bit sums meanwhile.
 //
 // Slice storage (int8, K contiguous, K padded to kp8 = multiple of 256):
 //   [slot][slice][array: Br, Bi, Ar, Ai][G (npad rows)][kp8]
@@ -57,9 +62,12 @@
 //              blocks (H/O tiles: half 0 Re H, Im H, half 1 Re O, Im O;
 //              per-atom tiles: half h the re and im blocks of rows 32h..32h+31)
 // The same kernel (MODE OZ_ATOM) forms the per-atom products B_a = h_a A_a
-// and the APW-lo rows loa_a A_a from int8 slices of h_a and loa.
-// Tensor memory (512 columns): r at [0,128), i at [128,256), FP64 sums (two
-// 32-bit columns per value) at [256,512).  Every wait on an mbarrier is
+// and the APW-lo rows loa_a A_a from int8 slices (or residues) of h_a and loa.
+// Tensor memory (512 columns): r at [0,128), i at [128,256), the running sums
+// (FP64 for slices, 64-bit fixed point for moduli; two 32-bit columns per
+// value) at [256,512).  With one tile per CTA the H/O tile's conjugate
+// mirror is staged in the stage buffers (idle by then) and written as whole
+// columns.  Every wait on an mbarrier is
 // bounded (about one second) and gives up early once another role has given
 // up; the kernel then records an error, lets its own copies and MMAs drain
 // (bounded), frees tensor memory and returns.
