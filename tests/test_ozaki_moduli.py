@@ -168,3 +168,35 @@ def test_split_residue_formula():
         r = (v - q * p).astype(np.int64)
         assert np.abs(r).max() <= 127
         assert np.all(np.mod(r - xs, p) == 0)
+
+
+def test_emulated_per_atom_product_meets_the_bar():
+    """B_a = h_a A_a as the per-atom kernel forms it: rows of h_a scaled to bx
+    bits (a power of two above each row's maximum), A to b bits by its column
+    maxima over all atoms, the same moduli; |X| <= 2 maxaa 2^(b + bx) < M / 2."""
+    import lapw_oracle as O
+    from exciting_b200 import workloads as W
+    s = W.si_fcc("text")
+    gk = s.gkset(s.kpoints[3])
+    apwalm, _ = O.match(s, gk)
+    N = gk.ngp
+    apwi = [O._apwi(s, apwalm, N, a) for a in range(s.natmtot)]
+    A = np.concatenate(apwi)
+    K, kx = A.shape[0], s.basis.maxaa
+    ps, cs, b, bx = plan(0, K, kx)
+    M = float(math.prod(ps))
+    _, _, sa = _split_scaled(A, b)
+    for a in range(s.natmtot):
+        h = s.mt_aa[:, :, a]
+        Aa = apwi[a]
+        ar, ai = np.rint(Aa.real / sa * 2.0 ** b), np.rint(Aa.imag / sa * 2.0 ** b)
+        hm = np.maximum(np.abs(h.real).max(1), np.abs(h.imag).max(1))
+        sx = np.ldexp(1.0, np.frexp(np.where(hm > 0, hm, 1.0))[1])
+        hr = np.rint(h.real / sx[:, None] * 2.0 ** bx).T           # (f', f)
+        hi = np.rint(h.imag / sx[:, None] * 2.0 ** bx).T
+        X = np.concatenate([hr, hi])
+        re = emulate(X, np.concatenate([ar, -ai]), ps, cs)[0].astype(np.float64)
+        im = emulate(X, np.concatenate([ai, ar]), ps, cs)[0].astype(np.float64)
+        got = (re + 1j * im) * (M * 2.0 ** (-64 - b - bx)) * np.outer(sx, sa)
+        ref = h @ Aa
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-13
