@@ -143,11 +143,11 @@ def split_scheme(args, sys_):
                 "split int8 x%d slices (tcgen05), FP64 recombination" % S)
     from exciting_b200.fvsystem import ozaki_moduli
     K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
-    ps, _, b, bx = ozaki_moduli(args.moduli, K, sys_.basis.maxaa)
+    ps, _, b, bx, h = ozaki_moduli(args.moduli, K, sys_.basis.maxaa)
     n = len(ps)
     return (n, n, "i8 residues mod %d coprime moduli, CRT in 64-bit fixed point, f64 scaling" % n,
-            "split int8, residues modulo %d moduli (%d-bit operands; tcgen05), Chinese-remainder recombination"
-            % (n, b))
+            "split int8, residues modulo %d moduli (columns scaled by their 2-norms to %d bits, %d headroom bits "
+            "in the 64-bit recombination; tcgen05), Chinese-remainder recombination" % (n, b, h))
 
 
 def ozaki_int8_ops(sys_, gks, products):
@@ -264,6 +264,14 @@ def run_reference(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def launches_per_setup(precision):
+    """Kernel launches of one batched setup call: match, (modular: the A column
+    norms), the A split, the per-atom products, (modular: the B column norms),
+    the B split, the H/O tiles, the O APW-lo block and the lo-lo blocks; the
+    FP64 path: match, four grouped DMMA products, APW-lo and lo-lo."""
+    return 9 if precision == "ozaki_mod" else 7
 
 
 def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, mode="auto", pinned=True):
@@ -464,7 +472,10 @@ def rttddft_leg(args, st, stream, torch, ngp, nmat, d_ig, d_vg, hp, op, step_dev
             "note": "exs_rttddft_updateham_device: UpdateHam's k-loop, calculate_overlap = .true."}
 
 
-def run_ours(args):
+def run_ours(args, emit=True):
+    """The 8-atom batch (27 k-points per step); with emit=False the JSON
+    object is returned instead of printed (the secondary leg of the
+    216-atom run, one process)."""
     import torch
     import torch.distributed as dist
     from exciting_b200 import workloads as W
@@ -608,6 +619,7 @@ def run_ours(args):
         e2e_value, h2d, d2h = None, 0, 0
     else:
         e2e_value, h2d, d2h = _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier)
+    if not args.skip_e2e and getattr(args, "e2e_modes", True):
         e2e_modes = {
             "pinned_direct": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "direct")[0],
             "pinned_packed": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "packed")[0],
@@ -616,14 +628,17 @@ def run_ours(args):
             "pageable_packed": _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, "packed", False)[0],
         }
 
-    # ---- split precision: its error against the native FP64 path (k-point 0)
-    # and the FP64 path's own device-resident rate for comparison
+    # ---- split precision: its error against the native FP64 path on every
+    # k-point of the batch (H and O on the device, Frobenius), the lowest 40
+    # generalized eigenvalues of each by the device eigen-solve of both
+    # paths, and the FP64 path's own device-resident rate for comparison
     accuracy, fp64_value = None, None
     if args.precision != "fp64":
         st.setup_batched_device(ngp, d_ig.data_ptr(), d_vg.data_ptr(), hp, op)
         st.synchronize()
-        h_oz = d_h[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
-        o_oz = d_o[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
+        h_oz = [t.clone() for t in d_h]
+        o_oz = [t.clone() for t in d_o]
+        ev_oz, _ = st.setup_and_solve(gks, 40)
         st.set_precision("fp64")
         for _ in range(2):
             step_device()
@@ -641,21 +656,24 @@ def run_ours(args):
         if ws > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         fp64_value = ws * nk * args.steps / (float(t.item()) * 1e-3)
-        h64 = d_h[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
-        o64 = d_o[0].cpu().numpy().view(np.complex128).reshape(nmat[0], nmat[0]).T
-        if rank == 0:
-            import scipy.linalg as sl
-            w = sl.eigh(h_oz, o_oz, eigvals_only=True, subset_by_index=[0, 39])
-            wr = sl.eigh(h64, o64, eigvals_only=True, subset_by_index=[0, 39])
-            small = np.abs(wr) <= 1.0
-            accuracy = {
-                "against": "native FP64 GPU path (itself within 1e-14 of the CPU oracle), k-point 0",
-                "rel_fro_H": float(np.linalg.norm(h_oz - h64) / np.linalg.norm(h64)),
-                "rel_fro_O": float(np.linalg.norm(o_oz - o64) / np.linalg.norm(o64)),
-                "max_abs_eig_dev_lowest40_Ha": float(np.max(np.abs(w - wr))),
-                "max_rel_eig_dev_lowest40": float(np.max(np.abs(w - wr) / np.maximum(1.0, np.abs(wr)))),
-                "max_abs_eig_dev_abs_le_1Ha": float(np.max(np.abs(w - wr)[small])) if small.any() else None,
-            }
+        fro_h = [_rel_fro_dev(a, b) for a, b in zip(h_oz, d_h)]
+        fro_o = [_rel_fro_dev(a, b) for a, b in zip(o_oz, d_o)]
+        del h_oz, o_oz
+        ev_64, _ = st.setup_and_solve(gks, 40)
+        dev = np.abs(ev_oz - ev_64)                        # (40, nk)
+        accuracy = {
+            "against": "native FP64 GPU path (itself within 1e-14 of the CPU oracle), all %d k-points" % nk,
+            "eigen_solver": "exs_setup_and_solve_batched (cuSOLVER zhegvdx, lowest 40) on both paths",
+            "rel_fro_H_max": float(max(fro_h)), "rel_fro_O_max": float(max(fro_o)),
+            "max_abs_eig_dev_lowest40_Ha": float(dev.max()),
+            "max_abs_eig_dev_per_k_Ha": [float(x) for x in dev.max(axis=0)],
+            "max_rel_eig_dev_lowest40": float(np.max(dev / np.maximum(1.0, np.abs(ev_64)))),
+            "lowest_eigenvalue_Ha": float(ev_64.min()),
+            "gate_abs_1e-8_Ha": bool(dev.max() <= 1e-8),
+        }
+
+    # ---- the adjoint of one k-point (FP64 in either mode)
+    adj = None if getattr(args, "skip_adjoint", False) else adjoint_leg(st, s, gks[0], torch)
 
     if rank == 0:
         fl = main_flops(s, gks)
@@ -721,20 +739,22 @@ def run_ours(args):
                 "sample": f"{cpu_n} k-points of the 27-k set in {cpu_dt:.1f} s by the FP64 CPU "
                           "restatement (C + OpenMP + OpenBLAS zgemm)"},
             "clocks": clocks,
-            "gpu_launches": 7 * args.steps,
+            "gpu_launches": launches_per_setup(args.precision) * args.steps,
             "setup_flops_per_step": setup_flops(s, gks),
             "accuracy": accuracy,
             "fp64_path_value": fp64_value,
+            "adjoint": adj,
             "hmlint": hml,
             "rttddft_updateham": rtl,
         }
-        print(json.dumps(out), flush=True)
+        if emit:
+            print(json.dumps(out), flush=True)
     st.set_stream(None)
     st.close()
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return 0 if emit else (out if rank == 0 else None)
 
 
 WORKLOAD_216 = ("si_cube216 216-atom Si (3x3x3 supercell of the 8-atom cube, a = 30.78), Gamma + 3 k, "
@@ -750,9 +770,140 @@ def _rel_fro_dev(a, b, chunk=1 << 27):
     return (num / den) ** 0.5
 
 
+def _host(t, n):
+    """The first n doubles of a device tensor, on the host (pageable)."""
+    return t[:n].cpu()
+
+
+def _rel_fro_host(h, d, chunk=1 << 27):
+    """||h - d|| / ||d|| for a host tensor h and a device tensor d of the same length."""
+    num = den = 0.0
+    for i in range(0, h.numel(), chunk):
+        x = h[i:i + chunk].cuda(non_blocking=False)
+        y = d[i:i + chunk]
+        num += float(((x - y) ** 2).sum())
+        den += float((y ** 2).sum())
+    return (num / den) ** 0.5
+
+
+def _lowest_generalized(h, o, m, nev, torch):
+    """The lowest nev eigenvalues of H x = e O x for za(m, m) matrices held as
+    host tensors of 2 m^2 doubles (column-major, so the tensors read as the
+    transposes: conj(H), conj(O), which have the same eigenvalues), by a
+    Cholesky reduction and a dense Hermitian eigen-solve on the device
+    (cuSOLVER, through torch)."""
+    H = h.cuda().view(torch.complex128).view(m, m)
+    L = torch.linalg.cholesky(o.cuda().view(torch.complex128).view(m, m))
+    X = torch.linalg.solve_triangular(L, H, upper=False)               # L^-1 H
+    del H
+    C = torch.linalg.solve_triangular(L, X.mH.contiguous(), upper=False)   # L^-1 H L^-H
+    del X, L
+    w = torch.linalg.eigvalsh(C)[:nev].cpu().numpy()
+    del C
+    torch.cuda.empty_cache()
+    return w
+
+
+def adjoint_recipe(nmat, seed=3, nst=40):
+    """The force-check states: nst orthonormal complex vectors (QR of a
+    Gaussian, seed 3), w = 2, eps ~ U[-0.5, 0.5] Ha."""
+    rng = np.random.default_rng(seed)
+    c, _ = np.linalg.qr(rng.standard_normal((nmat, nst)) + 1j * rng.standard_normal((nmat, nst)))
+    eps = rng.uniform(-0.5, 0.5, nst)
+    return np.asfortranarray(c), np.full(nst, 2.0), eps
+
+
+def adjoint_flops(sys_, gk, nst):
+    """Algorithmic flops of the factored adjoint: U_q = A_a C (q = 0..3), h_a U_q,
+    and the two N x N rank-nst products P and Q (8 flops per complex MAC)."""
+    b = sys_.basis
+    K = sum(b.napw_atom(a) for a in range(sys_.natmtot))
+    m2 = sum(b.napw_atom(a) ** 2 for a in range(sys_.natmtot))
+    n = gk.ngp
+    return 4 * 8.0 * K * n * nst + 4 * 8.0 * m2 * nst + 2 * 8.0 * n * n * nst
+
+
+def adjoint_leg(st, sys_, gk, torch, reps=3):
+    """exs_adjoint (dL/dtau, dL/dV, dL/dh_a) on one k-point with the force-check
+    states, wall clock of the synchronous call (uploads of the states included)."""
+    c, w, eps = adjoint_recipe(sys_.nmat(gk))
+    st.adjoint(gk, c, w, eps, dveffig=True, dh=True)             # warm-up (work space)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        dtau, _, _ = st.adjoint(gk, c, w, eps, dveffig=True, dh=True)
+    dt = (time.perf_counter() - t0) / reps
+    fl = adjoint_flops(sys_, gk, c.shape[1])
+    return {"ms": dt * 1e3, "k_points_per_s": 1.0 / dt, "states": int(c.shape[1]),
+            "flops": fl, "achieved_tflops": fl / dt / 1e12,
+            "max_abs_dL_dtau": float(np.max(np.abs(dtau))),
+            "note": "exs_adjoint: dL/dtau (= -F_IBS), dL/dV(G), dL/dh_a for 40 orthonormal states, w = 2, "
+                    "eps ~ U[-0.5, 0.5] (seed 3); FP64 in either precision mode; wall clock of the call"}
+
+
+def cpu_sample_216(sys_, gk, m_atoms=1, n_sub=3000):
+    """The FP64 CPU restatement on a bounded sample of one 216-atom k-point:
+    match and the H and O zgemm pairs (hamiltonsetup.f90:75-103,
+    overlapsetup.f90:88-101) of m_atoms atoms, and hmlistln/olpistln over the
+    first n_sub G+k; extrapolated linearly in atoms and by N(N+1) in G+k.
+    Returns (extrapolated seconds per k-point, sample seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lapw_oracle as O
+    from exciting_b200.crystal import gensfacgp
+    lib = O.lib()
+    b = sys_.basis
+    n = gk.ngp
+    t0 = time.perf_counter()
+    # match for the sample atoms
+    gpc = np.ascontiguousarray(gk.gpc)
+    tpgpc = np.asfortranarray(gk.tpgpc)
+    sf = np.asfortranarray(gensfacgp(gk.vgpc, sys_.crystal.atposc[:, :m_atoms]))
+    apword = O._f(np.array(b.apword).T, np.int32)
+    species = np.asarray(b.atom_species[:m_atoms], dtype=np.int32)
+    apwalm = np.zeros((n, b.apwordmax, b.lmmaxapw, m_atoms), dtype=np.complex128, order="F")
+    tail = np.asfortranarray(sys_.apwfr_tail[..., :m_atoms])
+    lib.orc_match(n, n, O._p(gpc), O._p(tpgpc), O._p(sf), m_atoms, O._p(species), b.lmaxapw, b.apwordmax,
+                  O._p(apword), O._p(O._f(sys_.rmt, np.float64)), sys_.crystal.omega, sys_.np_tail,
+                  O._p(O._f(sys_.spr_tail, np.float64)), O._p(tail), O._p(apwalm))
+    t_match = time.perf_counter() - t0
+    # the zgemm pairs into full N x N accumulators, as the reference (beta = 1)
+    import scipy.linalg.blas as blas
+    h = np.zeros((n, n), dtype=np.complex128, order="F")
+    t1 = time.perf_counter()
+    for ias in range(m_atoms):
+        apwi = np.asfortranarray(O._apwi(sys_, apwalm, n, ias))
+        zm = blas.zgemm(1.0, np.asfortranarray(sys_.mt_aa[:, :, ias]), apwi)
+        h = blas.zgemm(1.0, apwi, zm, beta=1.0, c=h, trans_a=2, overwrite_c=1)
+        h = blas.zgemm(1.0, apwi, apwi, beta=1.0, c=h, trans_a=2, overwrite_c=1)    # the O pair, same cost
+    t_pairs = time.perf_counter() - t1
+    del h
+    # hmlistln + olpistln over the first n_sub G+k
+    ns = min(n_sub, n)
+    gv = sys_.gv
+    hs = np.zeros((ns, ns), dtype=np.complex128, order="F")
+    os_ = np.zeros((ns, ns), dtype=np.complex128, order="F")
+    ivg = O._f(gv.ivg, np.int32)
+    ivgig = np.asfortranarray(gv.ivgig, dtype=np.int32)
+    intgv = O._f(gv.intgv, np.int32)
+    vgpc = O._f(gk.vgpc[:, :ns], np.float64)
+    igpig = O._f(gk.igpig[:ns], np.int32)
+    kinw = O._f(sys_.kinetic_weight, np.complex128)
+    t2 = time.perf_counter()
+    lib.orc_hmlistln_olpistln(ns, O._p(igpig), O._p(vgpc), ns, O._p(ivg), O._p(ivgig), O._p(intgv), gv.ngvec,
+                              O._p(sys_.veffig), O._p(kinw), O._p(sys_.cfunig), None, 0, O._p(hs), O._p(os_))
+    t_int = time.perf_counter() - t2
+    scale_a = sys_.natmtot / m_atoms
+    full = (t_match + t_pairs) * scale_a + t_int * (n * (n + 1.0)) / (ns * (ns + 1.0))
+    return full, time.perf_counter() - t0
+
+
 def run_large(args):
-    """The 216-atom cell: one k-point per call (H and O are ~13.7 GB each),
-    the step is the 4 k-points; split precision and native FP64 both timed."""
+    """The 216-atom cell, the north-star workload: one k-point per step (H and
+    O are ~13.6 GB each), Gamma and the three other k-points in turn.  Timed:
+    the split-precision setup (value), the native FP64 path, the adjoint, and
+    the host-pointer entry point; accuracy at Gamma (Frobenius and the lowest
+    40 generalized eigenvalues of both paths); the CPU restatement on a bounded
+    sample; the 8-atom batch as a secondary leg."""
     import torch
     import torch.distributed as dist
     from exciting_b200 import workloads as W
@@ -784,17 +935,14 @@ def run_large(args):
     d_h = torch.empty(2 * mmax * mmax, dtype=torch.float64, device="cuda")
     d_o = torch.empty_like(d_h)
 
-    def step(phase):
-        for k, g in enumerate(gks):
-            st.setup_batched_device([g.ngp], ig[k].data_ptr(), vg[k].data_ptr(), [d_h.data_ptr()],
-                                    [d_o.data_ptr()])
-            st.synchronize()
-            phase += st.last_timings()[:5]
+    def one(k):
+        st.setup_batched_device([gks[k].ngp], ig[k].data_ptr(), vg[k].data_ptr(), [d_h.data_ptr()],
+                                [d_o.data_ptr()])
 
     def timed(nsteps, nwarm, sample_clocks):
-        junk = np.zeros(5)
-        for _ in range(nwarm):
-            step(junk)
+        for i in range(nwarm):
+            one(i % len(gks))
+            st.synchronize()
         rows, stop = [], threading.Event()
         th = None
         if sample_clocks:
@@ -808,8 +956,10 @@ def run_large(args):
         phase = np.zeros(5)
         with torch.cuda.stream(stream):
             e0.record(stream)
-            for _ in range(nsteps):
-                step(phase)
+            for i in range(nsteps):
+                one(i % len(gks))
+                st.synchronize()
+                phase += st.last_timings()[:5]
             e1.record(stream)
         torch.cuda.synchronize()
         stop.set()
@@ -825,63 +975,127 @@ def run_large(args):
     args.precision = prec
     planes, products, dtype_text, prec_text = split_scheme(args, s)
     ms, phase, rows = timed(args.steps, args.warmup, True)
-    value = len(gks_all) * args.steps / (ms * 1e-3)
-    # accuracy of the split precision against the native FP64 path, k-point 0, whole matrices
-    st.setup_batched_device([gks[0].ngp], ig[0].data_ptr(), vg[0].data_ptr(), [d_h.data_ptr()], [d_o.data_ptr()])
-    st.synchronize()
+    value = ws * args.steps / (ms * 1e-3)
+    # ---- Gamma in split precision, kept on the host for the comparison
     m0 = gks[0].ngp + nlotot
-    h8 = d_h[: 2 * m0 * m0].clone()
-    o8 = d_o[: 2 * m0 * m0].clone()
-    st.set_precision("fp64")
-    ms64, phase64, _ = timed(max(1, args.steps // 3), 1, False)
-    fp64_value = len(gks_all) * max(1, args.steps // 3) / (ms64 * 1e-3)
-    st.setup_batched_device([gks[0].ngp], ig[0].data_ptr(), vg[0].data_ptr(), [d_h.data_ptr()], [d_o.data_ptr()])
+    one(0)
     st.synchronize()
-    acc = {"against": "native FP64 GPU path, k-point 0 (Gamma), whole H and O",
-           "rel_fro_H": _rel_fro_dev(h8, d_h[: 2 * m0 * m0]), "rel_fro_O": _rel_fro_dev(o8, d_o[: 2 * m0 * m0])}
-    del h8, o8
+    h8, o8 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
+    # ---- the native FP64 path: a few stated steps (one per k-point)
+    nf = len(gks)
+    st.set_precision("fp64")
+    ms64, phase64, _ = timed(nf, 1, False)
+    fp64_value = ws * nf / (ms64 * 1e-3)
+    one(0)
+    st.synchronize()
+    acc = {"against": "native FP64 GPU path, Gamma, whole H and O",
+           "rel_fro_H": _rel_fro_host(h8, d_h[: 2 * m0 * m0]), "rel_fro_O": _rel_fro_host(o8, d_o[: 2 * m0 * m0])}
+    h64, o64 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
+    del d_h, d_o
+    torch.cuda.empty_cache()
+    # ---- end to end through the host-pointer entry point (pinned H and O, 13.6 GB each per k-point)
+    e2e = None
+    if not args.skip_e2e and rank == 0:
+        st.set_precision(prec, args.slices if prec == "ozaki" else args.moduli)
+        hp = torch.empty(2 * mmax * mmax, dtype=torch.float64, pin_memory=True)
+        op = torch.empty_like(hp, pin_memory=True)
+
+        def views(g):     # za(nmat, nmat) of this k-point at the start of the pinned buffers
+            m = g.ngp + nlotot
+            return [(hp.numpy()[: 2 * m * m].view(np.complex128).reshape(m, m, order="F"),
+                     op.numpy()[: 2 * m * m].view(np.complex128).reshape(m, m, order="F"))]
+        ne = 2
+        st.setup_batched([gks[0]], out=views(gks[0]))          # warm-up
+        t0 = time.perf_counter()
+        for i in range(ne):
+            g = gks[i % len(gks)]
+            st.setup_batched([g], out=views(g))
+        dt = time.perf_counter() - t0
+        e2e = {"value": ne / dt, "unit": "setups/s", "h2d_bytes_per_step": int(gks[0].ngp * 16),
+               "d2h_bytes_per_step": int(2 * 16 * m0 * m0), "host_copy_mode": "auto (pinned outputs)",
+               "steps": ne, "note": "exs_setup_batched, one k-point per call: igpig/vgpc in, H and O (13.6 GB "
+                                    "each) to pinned host memory; wall clock"}
+        del hp, op
+    # ---- the adjoint at Gamma (FP64 in either mode)
+    adj = None if args.skip_adjoint else adjoint_leg(st, s, gks[0], torch)
+    clocks = _clock_summary(rows, local)
+    st.set_stream(None)
+    st.close()
+    torch.cuda.empty_cache()
+    # ---- eigenvalues of both Gamma pairs
+    if not args.skip_eig and rank == 0:
+        t0 = time.perf_counter()
+        w8 = _lowest_generalized(h8, o8, m0, 40, torch)
+        w64 = _lowest_generalized(h64, o64, m0, 40, torch)
+        acc.update({"eigen_solver": "Cholesky reduction + dense eigen-solve on the device (torch / cuSOLVER), "
+                                    "lowest 40 of each path", "eig_solve_s": time.perf_counter() - t0,
+                    "max_abs_eig_dev_lowest40_Ha": float(np.max(np.abs(w8 - w64))),
+                    "lowest_eigenvalue_Ha": float(w64[0]),
+                    "gate_abs_1e-8_Ha": bool(np.max(np.abs(w8 - w64)) <= 1e-8)})
+    del h8, o8, h64, o64
+    if ws > 1:
+        dist.barrier()
     if rank == 0:
-        ops = ozaki_int8_ops(s, gks_all, products)
-        fl = main_flops(s, gks_all)
+        ops = ozaki_int8_ops(s, gks_all, products) / len(gks_all)      # per k-point (one per step)
+        fl = main_flops(s, gks_all) / len(gks_all)
         peak8 = _measured_int8_peak(torch)
         peak64 = _measured_fp64_peak(torch)
-        mt_ms = phase[2]                                      # MT phase per step (all k)
+        mt_ms = phase[2]
         a8 = ops / (mt_ms * 1e-3) / 1e12
+        cpu = None
+        if not args.skip_cpu:
+            cpu_sample_216(s, gks_all[0], 1, 1000)                          # warm-up (libraries, pages)
+            full, dt = cpu_sample_216(s, gks_all[0], 2, 3000)
+            cpu = {"value": 1.0 / full, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": "Gamma: match and the H and O zgemm pairs of 2 of 216 atoms plus hmlistln/olpistln "
+                             "over 3000 of %d G+k by the FP64 CPU restatement (C + OpenBLAS zgemm, %.1f s), "
+                             "extrapolated linearly in atoms and by N(N+1) in G+k" % (gks_all[0].ngp, dt)}
+        sub = None
+        if not args.skip_cube8 and ws == 1:
+            sub = run_ours(argparse.Namespace(**{**vars(args), "steps": 10, "warmup": 3, "nk": 27, "skip_cpu": True,
+                                                 "skip_hmlint": True, "skip_rttddft": True, "skip_e2e": True,
+                                                 "e2e_modes": False}), emit=False)
         out = {
             "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": dtype_text,
             "data": "synthetic",
-            "config": {"workload": WORKLOAD_216, "k_per_step": len(gks_all),
+            "config": {"workload": WORKLOAD_216, "k_per_step": 1,
+                       "kpoints": "Gamma, (1/2,0,0), (1/2,1/2,0), (1/2,1/2,1/2) in turn, one per step",
                        "ngp": [min(g.ngp for g in gks_all), max(g.ngp for g in gks_all)],
                        "nmat": [min(g.ngp for g in gks_all) + nlotot, max(g.ngp for g in gks_all) + nlotot],
                        "precision": prec_text,
                        "l2": "working set (A/B planes 30 GB, %d int8 planes of 4 arrays, H/O 27 GB) far above "
                              "L2, no flush" % planes},
-            "e2e": None,
-            "e2e_note": "H and O are 13.7 GB each per k-point; host staging of that size is not measured",
+            "e2e": e2e,
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
-            "roofline": {"bound": "tensor", "kernel": "oz_mma_kernel (tcgen05.mma kind::i8, MT contraction)",
+            "roofline": {"bound": "tensor", "kernel": "oz_mma_kernel<OZ_HO> (tcgen05.mma kind::i8, MT contraction)",
                          "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                          "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
                          "int8_ops_per_step": ops, "traffic": None,
+                         "traffic_note": "not captured at this size (an ncu replay of a multi-second launch); "
+                                         "the 8-atom leg's capture is in the profiles",
                          "fp64_equivalent": {"achieved": fl / (mt_ms * 1e-3) / 1e12, "peak": peak64,
                                              "unit": "TFLOP/s", "frac": fl / (mt_ms * 1e-3) / 1e12 / peak64}},
-            "cpu_baseline": None,
-            "cpu_baseline_note": "the CPU restatement needs ~2e14 flops per k-point here (hours on the host)",
-            "clocks": _clock_summary(rows, local),
-            "gpu_launches": 7 * len(gks_all) * args.steps,
-            "setup_flops_per_step": setup_flops(s, gks_all),
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches_per_setup(prec) * args.steps,
+            "setup_flops_per_step": setup_flops(s, gks_all) / len(gks_all),
             "accuracy": acc,
             "fp64_path_value": fp64_value,
+            "fp64_steps": nf,
             "fp64_phases_ms_per_step": {"match": phase64[0], "h_a_A": phase64[1], "mt_contraction": phase64[2],
                                         "lo_blocks": phase64[3], "total": phase64[4]},
             "speedup_split_vs_fp64": value / fp64_value,
+            "adjoint": adj,
+            "with_adjoint": None if adj is None else {
+                "split_setups_per_s": 1.0 / (1.0 / value + adj["ms"] * 1e-3),
+                "fp64_setups_per_s": 1.0 / (1.0 / fp64_value + adj["ms"] * 1e-3),
+                "note": "setup + adjoint per k-point, both paths (the adjoint runs in FP64 in either)"},
+            "cube8": sub,
         }
         print(json.dumps(out), flush=True)
-    st.set_stream(None)
-    st.close()
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -982,7 +1196,7 @@ def run_cells(args):
                 "value": cpu_v, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
                 "sample": f"{cpu_n} cells by the FP64 CPU restatement in {cpu_dt:.1f} s"},
             "clocks": _clock_summary(rows, 0),
-            "gpu_launches": 7 * ncell * args.steps,
+            "gpu_launches": launches_per_setup(args.precision) * ncell * args.steps,
         }
         print(json.dumps(out), flush=True)
     for st in setups:
@@ -1032,12 +1246,16 @@ def main():
     ap.add_argument("--precision", default="ozaki_mod", choices=["fp64", "ozaki", "ozaki_mod"],
                     help="MT contraction arithmetic: ozaki_mod = int8 residues modulo coprime moduli, "
                          "ozaki = int8 slices (the native FP64 path is timed beside either)")
-    ap.add_argument("--workload", default="cube8", choices=["cube8", "cube216", "cells256"],
-                    help="cube8: 8-atom cell, 27 k per step; cube216: 216-atom cell, 4 k per step; "
-                         "cells256: 256 independent 2-atom cells per step in one graph")
+    ap.add_argument("--workload", default="cube216", choices=["cube8", "cube216", "cells256"],
+                    help="cube216: 216-atom cell, one of its 4 k-points per step (the 8-atom batch runs as a "
+                         "secondary leg); cube8: 8-atom cell, 27 k per step; cells256: 256 independent 2-atom "
+                         "cells per step in one graph")
+    ap.add_argument("--skip-adjoint", action="store_true", help="no adjoint leg")
+    ap.add_argument("--skip-eig", action="store_true", help="cube216: no eigenvalue comparison at Gamma")
+    ap.add_argument("--skip-cube8", action="store_true", help="cube216: no 8-atom secondary leg")
     ap.add_argument("--slices", type=int, default=7, help="int8 slices per operand (ozaki)")
     ap.add_argument("--moduli", type=int, default=0,
-                    help="moduli of ozaki_mod (0: the fewest that keep 44 bits per operand)")
+                    help="moduli of ozaki_mod (0: the fewest that keep 41 + log2(K)/2 bits per operand)")
     ap.add_argument("--leg", default="setup", choices=["setup", "hmlint"],
                     help="hmlint: only the muffin-tin integral generation of --workload (cube8 or cube216)")
     args = ap.parse_args()

@@ -49,6 +49,7 @@ SIGNATURES = {
     "exs_ctx_sizes": ([P, P, P, P], c_int),
     "exs_set_scf_inputs": ([P, P], c_int),
     "exs_set_precision": ([P, c_int, c_int], c_int),
+    "exs_set_wait_limit": ([P, ctypes.c_longlong], c_int),
     "exs_match": ([P, c_int, P, P, P, P], c_int),
     "exs_hamiltonandoverlapsetup": ([P, c_int, P, P, P, P, P], c_int),
     "exs_setup_batched": ([P, c_int, P, P, P, P, P], c_int),
@@ -83,7 +84,7 @@ SIGNATURES = {
     "exs_rttddft_genpmat": ([P, c_int, P, P, P, P, P, P, c_int], c_int),
     "exs_clebgor_unit": ([c_int] * 5 + [P], c_int),
     "exs_gauntyry": ([c_int] * 6 + [P], c_int),
-    "exs_ozaki_moduli": ([c_int, c_int, c_int, P, P, P, P, P], c_int),
+    "exs_ozaki_moduli": ([c_int, c_int, c_int, P, P, P, P, P, P], c_int),
     "exs_fderiv_int": ([c_int, P, P, P], c_int),
 }
 

@@ -433,6 +433,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         return fail(c, EXS_ERR_CUDA, "cuTensorMapEncodeTiled failed for the slice array");
     }
     c->slices = slices;
+    sch.wait = c->oz_wait;
     c->oz_sch = sch;
     c->prec_mode = mode;
     if (c->have_inputs) {   // slices of the current h_a and loa
@@ -554,11 +555,21 @@ int exs_synchronize(exs_ctx *c)
     if (err & exs::DEV_ERR_INDEX)
         return fail(c, EXS_ERR_INDEX, "a G-G' difference fell outside the ivgig box");
     if (err & exs::DEV_ERR_TIMEOUT)
-        return fail(c, EXS_ERR_CUDA, "a tensor-core pipeline wait expired (kernel gave up)");
+        return fail(c, EXS_ERR_TIMEOUT, "a tensor-core pipeline wait expired (the kernel gave up and drained)");
     if (err & exs::DEV_WARN_SINGULAR) {
         c->last_error = "a matching system D_l was singular (match.f90:166-175)";
         return EXS_WARN_SINGULAR;
     }
+    return EXS_OK;
+}
+
+int exs_set_wait_limit(exs_ctx *c, long long cycles)
+{
+    if (!c) return EXS_ERR_ARG;
+    if (cycles < 0) return fail(c, EXS_ERR_ARG, "negative wait limit");
+    c->gen++;   // captured graphs carry the old limit
+    c->oz_wait = cycles;
+    c->oz_sch.wait = cycles;
     return EXS_OK;
 }
 
@@ -806,8 +817,11 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     // configuration bit 4: B = h_a A and the APW-lo rows in native FP64 even
     // when the H/O contraction is split
     const bool b64 = !oz || (c->oz_cfg & 16);
+    // moduli: the columns are scaled by their 2-norms (over the maxima the producers raised)
+    const bool norms = oz && c->oz_sch.mod;
     if (oz) {
         // slices of A; B = h_a A and the APW-lo rows of H from the slices of h_a and loa
+        if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 0, s));
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 2, s));
         if (!b64)
             EXS_CUDA(exs::launch_oz_atom(c->oz_cfg, &c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles,
@@ -819,6 +833,7 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     }
     EXS_EV(2);
     if (oz) {
+        if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 1, s));
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 0, s));
         const int q = c->oz_cfg;
         EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <map>
 #include <string>
 #include <tuple>
@@ -21,6 +22,23 @@ enum : int {
     DEV_WARN_SINGULAR = 2,
     DEV_ERR_TIMEOUT = 4,  // a bounded wait in a kernel expired
 };
+
+// A kernel attribute (such as the dynamic shared memory size) is a setting of
+// the current device: set it once per device, bit d of `done` recording
+// device d (devices past 63 set it on every call).  Host threads that race
+// both set it, which is harmless.
+template <class F>
+inline cudaError_t once_per_device(std::atomic<unsigned long long> &done, F set)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // Pipeline configurations of the split-precision kernel.
 constexpr int OZ_NCFG = 32;
@@ -44,15 +62,22 @@ static_assert(OZ_NCFG == EXS_OZ_NCONFIG, "public configuration count");
 //   slices (mod = 0): n int8 slices of 7 bits per operand, pairs s + t <= n + 1,
 //     folded diagonal by diagonal in FP64 (seg / segx pairs per exact int32
 //     segment for the H/O and the per-atom tiles);
-//   moduli (mod = 1): every operand scaled to integers of b bits (bx for the
-//     h_a / loa rows) and stored as its residues modulo n pairwise coprime odd
-//     moduli p[m] (int8 in [-127, 127]); one int8 product per modulus, each
-//     folded into a 64-bit sum t += (v mod p[m]) c[m] (mod 2^64), so that
-//     t / 2^64 = X / M (mod 1) for the integer product X, |X| < M / 2; the
-//     value is t (as a signed integer) times fin (H/O) or finx (per-atom).
+//   moduli (mod = 1): every column of A and B scaled by a power of two above
+//     its 2-norm and rounded to integers (b bits: the scaled column has norm
+//     <= 2^b; bx for the h_a / loa rows, scaled by their row norms), stored
+//     as residues modulo n pairwise coprime odd moduli p[m] (int8 in
+//     [-127, 127]); one int8 product per modulus, each folded into a 64-bit
+//     sum t += (v mod p[m]) c[m] (mod 2^64) with c[m] = round(2^(64+h) y_m /
+//     p[m]) mod 2^64, so that t / 2^64 = 2^h X / M (mod 1) for the integer
+//     product X; by the Cauchy-Schwarz inequality |X| <= 2^(2b) (1 + eps)^2 and
+//     2^(2b + h + 2) <= M, so 2^h |X| / M < 1/2 and t read as a signed integer
+//     is exact but for the rounding of the constants; the value is t times fin
+//     (H/O) or finx (per-atom).  The h headroom bits divide that rounding
+//     error by 2^h.
 constexpr int OZ_MAX_MODULI = 16;
 struct OzScheme {
-    int mod, n, seg, segx, b, bx;
+    int mod, n, seg, segx, b, bx, h;
+    long long wait;                    // limit of the pipeline waits in cycles (0: OZ_WAIT_CYCLES)
     double fin, finx;
     int p[OZ_MAX_MODULI];
     int mg[OZ_MAX_MODULI];             // round(2^32 / p): quotient estimate by a multiply-high
@@ -92,7 +117,8 @@ struct KDesc {
     double *br, *bi;         // B = blockdiag(h_a) A planes
     double *cr, *ci;         // (I + h1) A planes (iora* only) else == ar/ai
     int8_t *oz_slices;       // split-precision path: int8 slices of this slot [S][4 arrays][npad][kp8]
-    double *oz_scale;        // split-precision path: column maxima of |A| and |B| [2][npad] (null: FP64 path)
+    double *oz_scale;        // split-precision path: column bounds of A and B [2][npad] (maxima with slices,
+                             // 2-norms with moduli; the scale is the power of two above; null: FP64 path)
     int oz_slot;             // split-precision path: slot index in the slice tensor maps
 };
 
@@ -243,6 +269,7 @@ struct exs_ctx {
     int prec_mode = EXS_PREC_FP64;
     int slices = 7;              // slices or moduli of the split-precision modes
     exs::OzScheme oz_sch{};      // their arithmetic
+    long long oz_wait = 0;       // limit of their pipeline waits in cycles (0: the default)
     bool oz_on() const { return prec_mode == EXS_PREC_OZAKI_INT8 || prec_mode == EXS_PREC_OZAKI_MOD; }
     int kp8 = 0;                 // K rounded up to 256 (int8 slice rows)
     int oz_seg = 0;              // slice pairs per exact int32 segment
@@ -307,6 +334,7 @@ cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k,
 cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int a0,
                             cudaStream_t s);
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s);
+cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, cudaStream_t s);
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
                            const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s);

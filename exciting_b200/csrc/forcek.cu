@@ -36,7 +36,7 @@ struct ForceWork {
     double *u[4][2];                 // U_q [f][n]
     double *hu[4][2];                // h_a U_q
     double *mu[4][2];                // M U_q (iora*) or == u
-    double *pt[2], *qt[2];           // P^T, Q^T [i][j], ld npad
+    double *pt[2], *qt[2];           // one band of rows of P^T, Q^T [i - i0][j], ld npad
     exs_complex *evec;               // (nmat, nst) dense
     const double *w, *eps;           // (nst)
     exs_complex *rh, *ro, *rv;       // (ngvec)
@@ -223,12 +223,13 @@ __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, cons
     if (threadIdx.x == 0) atomicAdd(&fw.force[x + 3 * ias], s);
 }
 
-// Scatter of P(j,i), dp_ij P(j,i) and Q(j,i) onto G_i - G_j (all i, j < ngp).
-__global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd)
+// Scatter of P(j,i), dp_ij P(j,i) and Q(j,i) onto G_i - G_j for the rows
+// i0 <= i < i1 of one band of P^T and Q^T (held from row i0 on) and all j < ngp.
+__global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd, int i0, int i1)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
-    if (i >= fw.ngp) return;
+    if (i >= i1 || i >= fw.ngp) return;
     const int gi = kd->igpig[i] - 1, gj = kd->igpig[j] - 1;
     if (gi < 0 || gi >= p.ngrtot || gj < 0 || gj >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); return; }
     const int d0 = p.ivg[3 * gi] - p.ivg[3 * gj] - p.intgv_lo[0];
@@ -243,7 +244,7 @@ __global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd)
     if (ig <= 0 || ig > p.ngvec) return;
     const double *vi = kd->vgpc + 3 * i, *vj = kd->vgpc + 3 * j;
     const double dp = 0.5 * (vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2]);
-    const size_t e = (size_t)i * p.npad + j;
+    const size_t e = (size_t)(i - i0) * p.npad + j;
     const double pr = fw.pt[0][e], pi = fw.pt[1][e], qr = fw.qt[0][e], qi = fw.qt[1][e];
     double *rh = reinterpret_cast<double *>(fw.rh + (ig - 1));
     double *ro = reinterpret_cast<double *>(fw.ro + (ig - 1));
@@ -368,7 +369,9 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     const size_t o_hu = take(8 * sizeof(double) * (size_t)Kp * nstp);
     const bool iora = c->relativity == EXS_REL_IORA;
     const size_t o_mu = take(iora ? 8 * sizeof(double) * (size_t)Kp * nstp : 0);
-    const size_t o_pq = take(4 * sizeof(double) * (size_t)npad * npad);
+    // P^T and Q^T in bands of rows of at most ~1 GiB (one band below ~5,800 G+k)
+    const int band = std::max(64, std::min(npad, (int)((((size_t)1 << 30) / (4 * sizeof(double) * (size_t)npad)) / 64 * 64)));
+    const size_t o_pq = take(4 * sizeof(double) * (size_t)band * npad);
     const size_t o_ev = take(sizeof(exs_complex) * (size_t)nmat * nst);
     const size_t o_we = take(2 * sizeof(double) * (size_t)nst);
     const size_t o_r = take(3 * sizeof(exs_complex) * (size_t)c->ngvec);
@@ -393,8 +396,8 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
             fw.mu[q][r] = iora ? (double *)(b + o_mu) + (size_t)(2 * q + r) * Kp * nstp : fw.u[q][r];
         }
     double *pq = (double *)(b + o_pq);
-    fw.pt[0] = pq; fw.pt[1] = pq + (size_t)npad * npad;
-    fw.qt[0] = pq + 2 * (size_t)npad * npad; fw.qt[1] = pq + 3 * (size_t)npad * npad;
+    fw.pt[0] = pq; fw.pt[1] = pq + (size_t)band * npad;
+    fw.qt[0] = pq + 2 * (size_t)band * npad; fw.qt[1] = pq + 3 * (size_t)band * npad;
     fw.evec = (exs_complex *)(b + o_ev);
     double *we = (double *)(b + o_we);
     fw.w = we;
@@ -431,7 +434,8 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     kd.ar = wk; kd.ai = wk + c->plane; kd.br = wk + 2 * c->plane; kd.bi = wk + 3 * c->plane;
     kd.cr = kd.ar; kd.ci = kd.ai;
     std::vector<GemmProb> probs;
-    std::vector<TileWork> w1, w2;
+    std::vector<TileWork> w1, w2, wb;
+    std::vector<size_t> wb_off;
     for (int q = 0; q < 4; q++) {              // U_q = A C_q   (contraction over G)
         GemmProb P{};
         P.xr = fw.atr; P.xi = fw.ati; P.ldx = Kp;
@@ -441,15 +445,19 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
         add_tiles(w1, (int)probs.size(), P.M, P.N, false);
         probs.push_back(P);
     }
-    for (int which = 0; which < 2; which++) {  // P^T = conj(C)^T (w C), Q^T = conj(C)^T (w eps C)
-        GemmProb P{};
-        P.xr = fw.cn[0]; P.xi = fw.cn[1]; P.ldx = npad;
-        P.yr = which == 0 ? fw.wc[0] : fw.wec[0]; P.yi = which == 0 ? fw.wc[1] : fw.wec[1]; P.ldy = npad;
-        P.M = ngp; P.N = ngp; P.K = nst; P.conjx = 1;
-        P.outr = which == 0 ? fw.pt[0] : fw.qt[0]; P.outi = which == 0 ? fw.pt[1] : fw.qt[1]; P.ldo = npad;
-        add_tiles(w1, (int)probs.size(), P.M, P.N, false);
-        probs.push_back(P);
+    for (int i0 = 0; i0 < ngp; i0 += band) {   // P^T = conj(C)^T (w C), Q^T = conj(C)^T (w eps C), rows i0..
+        wb_off.push_back(wb.size());
+        for (int which = 0; which < 2; which++) {
+            GemmProb P{};
+            P.xr = fw.cn[0] + i0; P.xi = fw.cn[1] + i0; P.ldx = npad;
+            P.yr = which == 0 ? fw.wc[0] : fw.wec[0]; P.yi = which == 0 ? fw.wc[1] : fw.wec[1]; P.ldy = npad;
+            P.M = std::min(band, ngp - i0); P.N = ngp; P.K = nst; P.conjx = 1;
+            P.outr = which == 0 ? fw.pt[0] : fw.qt[0]; P.outi = which == 0 ? fw.pt[1] : fw.qt[1]; P.ldo = npad;
+            add_tiles(wb, (int)probs.size(), P.M, P.N, false);
+            probs.push_back(P);
+        }
     }
+    wb_off.push_back(wb.size());
     for (int q = 0; q < 4; q++)                // h_a U_q per atom
         for (int ias = 0; ias < c->natmtot; ias++) {
             const exs::AtomDesc &a = c->atoms[ias];
@@ -464,8 +472,8 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
             probs.push_back(P);
         }
     const size_t kb = al256(sizeof(KDesc)), pb = al256(sizeof(GemmProb) * probs.size());
-    const size_t wb = sizeof(TileWork) * (w1.size() + w2.size());
-    const size_t tb = kb + pb + wb;
+    const size_t wbytes = sizeof(TileWork) * (w1.size() + w2.size() + wb.size());
+    const size_t tb = kb + pb + wbytes;
     FK_CUDA(grow(&c->fk_tab_h, &c->fk_tab_hbytes, tb, true));
     FK_CUDA(grow(&c->fk_tab_d, &c->fk_tab_dbytes, tb, false));
     char *th = (char *)c->fk_tab_h;
@@ -473,12 +481,14 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     std::memcpy(th + kb, probs.data(), sizeof(GemmProb) * probs.size());
     std::memcpy(th + kb + pb, w1.data(), sizeof(TileWork) * w1.size());
     std::memcpy(th + kb + pb + sizeof(TileWork) * w1.size(), w2.data(), sizeof(TileWork) * w2.size());
+    std::memcpy(th + kb + pb + sizeof(TileWork) * (w1.size() + w2.size()), wb.data(), sizeof(TileWork) * wb.size());
     FK_CUDA(cudaMemcpyAsync(c->fk_tab_d, th, tb, cudaMemcpyHostToDevice, s));
     char *td = (char *)c->fk_tab_d;
     const KDesc *d_k = (const KDesc *)td;
     const GemmProb *d_p = (const GemmProb *)(td + kb);
     const TileWork *d_w1 = (const TileWork *)(td + kb + pb);
     const TileWork *d_w2 = d_w1 + w1.size();
+    const TileWork *d_wb = d_w2 + w2.size();
 
     // ---- launches
     (void)cudaGetLastError();   // launch checks below read the last error: start clean
@@ -496,7 +506,13 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     exs::fk_terms_mt<<<dim3(c->natmtot, 3), 128, 0, s>>>(p, fw);
     if (c->nlotot > 0)
         exs::fk_terms_lo<<<dim3(c->natmtot, 3), 256, 0, s>>>(p, fw, c->d_loa_r, c->d_loa_i, c->ldlo, c->maxaa);
-    exs::fk_scatter<<<dim3((ngp + 127) / 128, ngp), 128, 0, s>>>(p, fw, d_k);
+    for (size_t b = 0; b + 1 < wb_off.size(); b++) {   // one band of P^T, Q^T, then its scatter
+        const int i0 = (int)b * band, i1 = std::min(ngp, i0 + band);
+        FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_wb + wb_off[b], (int)(wb_off[b + 1] - wb_off[b]),
+                                      d_k, s));
+        exs::fk_scatter<<<dim3((i1 - i0 + 127) / 128, ngp), 128, 0, s>>>(p, fw, d_k, i0, i1);
+        FK_CUDA(cudaGetLastError());
+    }
     exs::fk_terms_theta<<<c->natmtot, 256, 0, s>>>(p, fw, c->ngvec);
     FK_CUDA(cudaGetLastError());
     return EXS_OK;

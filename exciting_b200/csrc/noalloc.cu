@@ -16,14 +16,19 @@
 // Problems whose work space does not fit are rejected with EXS_ERR_SIZE.
 //
 // The array is shared by all calls and keeps the previous call's contents;
-// each call rewrites every part it reads (padding included).  Two calls
-// whose work overlaps on the GPU (different streams, or different host
-// threads) race on the array and give wrong results: serialise them.
+// each call rewrites every part it reads (padding included), its tables
+// included: they are written on the device by kernels that receive the
+// per-atom sizes as launch arguments, so no host buffer is copied.  Two
+// calls whose work overlaps on the GPU (different streams, or different
+// host threads) race on the array and give wrong results: serialise them.
 //
 // Host code cannot use the array's name as a device address; on the first
 // call on each device (with that device current) the address is looked up
 // with cudaGetSymbolAddress and cached.  That first call should therefore
-// come before any stream capture.
+// come before any stream capture.  cudaDeviceReset destroys the array with
+// the context, so the cached address is stale afterwards: this entry point
+// is not for processes that reset a device and go on using it.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -34,6 +39,9 @@
 #define EXS_NOALLOC_MAX_DEVICES 64
 
 namespace {
+
+using exs::GemmProb;
+using exs::TileWork;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[EXS_NOALLOC_SCRATCH_BYTES];
 
@@ -58,8 +66,87 @@ cudaError_t noalloc_scratch(unsigned char **out)
     return cudaSuccess;
 }
 
+// The grouped-product tables on the device.  Per-atom entries come in
+// chunks of NA_CHUNK atoms whose sizes, row offsets and first work entries
+// travel as launch arguments: problem a is B_a = h_a A_a with tiles
+// (a, tm, tn), tm < ceil(napw / 64), tn < ntile, from entry wbase on.
+constexpr int NA_CHUNK = 256;
+
+struct NaBase {
+    double *ar, *ai, *br, *bi, *hr, *hi, *Hr, *Hi, *Or, *Oi;
+    int natmtot, ldh, np, ngp, K, ntile;
+};
+
+struct NaChunk {
+    int a0, count;
+    int off[NA_CHUNK], napw[NA_CHUNK], wbase[NA_CHUNK];
+};
+
+__global__ void na_atom_tables(const __grid_constant__ NaBase b, const __grid_constant__ NaChunk c, int *d_off,
+                               int *d_napw, GemmProb *probs, TileWork *work)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c.count) return;
+    const int a = c.a0 + t, na = c.napw[t], off = c.off[t];
+    d_off[a] = off;
+    d_napw[a] = na;
+    GemmProb P{};
+    P.xr = b.hr + (size_t)a * b.ldh * b.ldh;
+    P.xi = b.hi + (size_t)a * b.ldh * b.ldh;
+    P.ldx = b.ldh;
+    P.yr = b.ar + (size_t)off * b.np;
+    P.yi = b.ai + (size_t)off * b.np;
+    P.ldy = b.np;
+    P.M = na;
+    P.N = b.np;
+    P.K = na;
+    P.conjx = 0;
+    P.outr = b.br + (size_t)off * b.np;
+    P.outi = b.bi + (size_t)off * b.np;
+    P.ldo = b.np;
+    probs[a] = P;
+    int w = c.wbase[t];
+    for (int tm = 0; tm < (na + 63) / 64; tm++)
+        for (int tn = 0; tn < b.ntile; tn++) work[w++] = TileWork{a, tm, tn};
+}
+
+// The two main problems (H = A^H B, O = A^H A) and their upper tiles, from
+// entry nwork_ha on: entry q < T = ntile (ntile + 1) / 2 of problem `which`
+// is the q-th (tm, tn >= tm) pair in row order.
+__global__ void na_main_tables(const __grid_constant__ NaBase b, int nwork_ha, GemmProb *probs, TileWork *work)
+{
+    const int T = b.ntile * (b.ntile + 1) / 2;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < 2) {
+        GemmProb P{};
+        P.xr = b.ar;
+        P.xi = b.ai;
+        P.ldx = b.np;
+        P.yr = q == 0 ? b.br : b.ar;
+        P.yi = q == 0 ? b.bi : b.ai;
+        P.ldy = b.np;
+        P.M = b.ngp;
+        P.N = b.ngp;
+        P.K = b.K;
+        P.conjx = 1;
+        P.outr = q == 0 ? b.Hr : b.Or;
+        P.outi = q == 0 ? b.Hi : b.Oi;
+        P.ldo = b.np;
+        probs[b.natmtot + q] = P;
+    }
+    if (q >= 2 * T) return;
+    const int which = q / T;
+    int r = q - which * T, tm = 0;
+    while (r >= b.ntile - tm) {
+        r -= b.ntile - tm;
+        tm++;
+    }
+    work[nwork_ha + q] = TileWork{b.natmtot + which, tm, tm + r};
+}
+
 // apwi(maxaa, ngp, natmtot) -> A planes [K][np]; rows beyond K and columns
-// beyond ngp are written as zero.
+// beyond ngp are written as zero.  The atom of row f is found by a binary
+// search of the row offsets (the same for the whole block).
 __global__ void na_pack_a(int natmtot, int maxaa, const int *off, const int *napw, int K, int Kp, int ngp, int np,
                           const exs_complex *apwi, double *ar, double *ai)
 {
@@ -68,8 +155,15 @@ __global__ void na_pack_a(int natmtot, int maxaa, const int *off, const int *nap
     if (g >= np || f >= Kp) return;
     double re = 0.0, im = 0.0;
     if (f < K && g < ngp) {
-        int ias = 0;
-        while (ias + 1 < natmtot && f >= off[ias + 1]) ias++;
+        int lo = 0, hi = natmtot - 1;         // the last atom with off <= f
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (off[mid] <= f)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int ias = lo;
         const int fl = f - off[ias];
         if (fl < napw[ias]) {
             const exs_complex z = apwi[fl + (size_t)maxaa * (g + (size_t)ngp * ias)];
@@ -139,8 +233,6 @@ extern "C" int exs_mt_contract_noalloc(int natmtot, int maxaa, const int *napw, 
     const int np = (ngp + 63) / 64 * 64;
     const int ldh = (maxaa + 7) / 8 * 8;
     const int ntile = np / 64;
-    std::vector<GemmProb> probs;
-    std::vector<TileWork> work_ha, work_main;
     const size_t plane = (size_t)Kp * np;
     size_t o_ints = 0;
     size_t o_tab = al256(o_ints + sizeof(int) * 2 * (size_t)natmtot);
@@ -148,7 +240,7 @@ extern "C" int exs_mt_contract_noalloc(int natmtot, int maxaa, const int *napw, 
     const size_t nprob = (size_t)natmtot + 2;
     size_t nwork_ha = 0;
     for (int a = 0; a < natmtot; a++) nwork_ha += (size_t)((na[a] + 63) / 64) * ntile;
-    const size_t nwork_main = 2 * (size_t)ntile * ntile;
+    const size_t nwork_main = (size_t)ntile * (ntile + 1);      // the upper tiles of H and of O
     const size_t o_work = al256(o_tab + sizeof(GemmProb) * nprob);
     const size_t o_planes = al256(o_work + sizeof(TileWork) * (nwork_ha + nwork_main));
     const size_t n_doubles = 4 * plane + 2 * (size_t)natmtot * ldh * ldh + 4 * (size_t)ngp * np;
@@ -172,39 +264,30 @@ extern "C" int exs_mt_contract_noalloc(int natmtot, int maxaa, const int *napw, 
     double *Or = Hi + (size_t)ngp * np;
     double *Oi = Or + (size_t)ngp * np;
 
-    // ---- grouped-product tables (the same kernel as the context path)
-    for (int a = 0; a < natmtot; a++) {           // B_a = h_a A_a
-        GemmProb P{};
-        P.xr = hr + (size_t)a * ldh * ldh; P.xi = hi + (size_t)a * ldh * ldh; P.ldx = ldh;
-        P.yr = ar + (size_t)off[a] * np; P.yi = ai + (size_t)off[a] * np; P.ldy = np;
-        P.M = na[a]; P.N = np; P.K = na[a]; P.conjx = 0;
-        P.outr = br + (size_t)off[a] * np; P.outi = bi + (size_t)off[a] * np; P.ldo = np;
-        const int pi = (int)probs.size();
-        probs.push_back(P);
-        for (int tm = 0; tm < (na[a] + 63) / 64; tm++)
-            for (int tn = 0; tn < ntile; tn++) work_ha.push_back({pi, tm, tn});
+    // ---- grouped-product tables (the same kernel as the context path), written on the device
+    NaBase nb{};
+    nb.ar = ar; nb.ai = ai; nb.br = br; nb.bi = bi; nb.hr = hr; nb.hi = hi;
+    nb.Hr = Hr; nb.Hi = Hi; nb.Or = Or; nb.Oi = Oi;
+    nb.natmtot = natmtot; nb.ldh = ldh; nb.np = np; nb.ngp = ngp; nb.K = K; nb.ntile = ntile;
+    cudaError_t e = cudaSuccess;
+    size_t wnext = 0;
+    for (int a0 = 0; a0 < natmtot && e == cudaSuccess; a0 += NA_CHUNK) {
+        NaChunk ch{};
+        ch.a0 = a0;
+        ch.count = std::min(NA_CHUNK, natmtot - a0);
+        for (int t = 0; t < ch.count; t++) {
+            ch.off[t] = off[a0 + t];
+            ch.napw[t] = na[a0 + t];
+            ch.wbase[t] = (int)wnext;
+            wnext += (size_t)((na[a0 + t] + 63) / 64) * ntile;
+        }
+        na_atom_tables<<<(ch.count + 127) / 128, 128, 0, s>>>(nb, ch, d_off, d_napw, d_probs, d_work);
+        e = cudaGetLastError();
     }
-    for (int which = 0; which < 2; which++) {    // H = A^H B, O = A^H A
-        GemmProb P{};
-        P.xr = ar; P.xi = ai; P.ldx = np;
-        P.yr = which == 0 ? br : ar; P.yi = which == 0 ? bi : ai; P.ldy = np;
-        P.M = ngp; P.N = ngp; P.K = K; P.conjx = 1;
-        P.outr = which == 0 ? Hr : Or; P.outi = which == 0 ? Hi : Oi; P.ldo = np;
-        const int pi = (int)probs.size();
-        probs.push_back(P);
-        for (int tm = 0; tm < ntile; tm++)
-            for (int tn = tm; tn < ntile; tn++) work_main.push_back({pi, tm, tn});
+    if (e == cudaSuccess) {
+        na_main_tables<<<(unsigned)((nwork_main + 127) / 128), 128, 0, s>>>(nb, (int)nwork_ha, d_probs, d_work);
+        e = cudaGetLastError();
     }
-    std::vector<int> ints(2 * (size_t)natmtot);
-    for (int a = 0; a < natmtot; a++) { ints[a] = off[a]; ints[natmtot + a] = na[a]; }
-    cudaError_t e = cudaMemcpyAsync(d_off, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_probs, probs.data(), sizeof(GemmProb) * probs.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_work, work_ha.data(), sizeof(TileWork) * work_ha.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_work + work_ha.size(), work_main.data(), sizeof(TileWork) * work_main.size(),
-                            cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return EXS_ERR_CUDA;
 
     // ---- pack, contract, store
@@ -212,9 +295,9 @@ extern "C" int exs_mt_contract_noalloc(int natmtot, int maxaa, const int *napw, 
     na_pack_h<<<dim3((ldh + 63) / 64, ldh, natmtot), 64, 0, s>>>(natmtot, maxaa, ldh, aa, hr, hi);
     if ((e = cudaGetLastError()) != cudaSuccess) return EXS_ERR_CUDA;
     const DevParams none{};
-    e = launch_gemm_kind(EPI_PLANAR, none, d_probs, d_work, (int)work_ha.size(), nullptr, s);
+    e = launch_gemm_kind(EPI_PLANAR, none, d_probs, d_work, (int)nwork_ha, nullptr, s);
     if (e == cudaSuccess)
-        e = launch_gemm_kind(EPI_PLANAR, none, d_probs, d_work + work_ha.size(), (int)work_main.size(), nullptr, s);
+        e = launch_gemm_kind(EPI_PLANAR, none, d_probs, d_work + nwork_ha, (int)nwork_main, nullptr, s);
     if (e != cudaSuccess) return EXS_ERR_CUDA;
     na_store_hermitian<<<dim3((ngp + 127) / 128, ngp), 128, 0, s>>>(ngp, np, Hr, Hi, h, ld);
     na_store_hermitian<<<dim3((ngp + 127) / 128, ngp), 128, 0, s>>>(ngp, np, Or, Oi, o, ld);

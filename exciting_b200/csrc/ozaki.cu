@@ -24,20 +24,26 @@
 // the upper triangle and its conjugate mirror, as the FP64 path does.
 //
 // Modular arithmetic (OzScheme.mod = 1) replaces the slices by residues:
-// every column is scaled to integers of b bits, x' = rint(x 2^b / sigma)
-// (|x'| <= 2^b, exact in FP64), and stored as n int8 planes x' mod p_m in
-// [-127, 127] for pairwise coprime odd moduli p_m.  One int8 product per
-// modulus gives r +- i = X (mod p_m) for the integer product X; with M =
-// prod p_m > 2 * 2K * 2^(2b) > 2|X|, X / M is the signed fraction of
-// sum_m (X mod p_m) y_m / p_m, y_m = (M / p_m)^-1 mod p_m (the Chinese
+// every column is scaled by sigma = a power of two above its 2-norm and
+// rounded to integers of b bits, x' = rint(x 2^b / sigma) (exact in FP64;
+// the scaled column has norm <= 2^b (1 + eps)), and stored as n int8 planes
+// x' mod p_m in [-127, 127] for pairwise coprime odd moduli p_m.  One int8
+// product per modulus gives r +- i = X (mod p_m) for the integer product X,
+// and |X| <= 2^(2b) (1 + eps)^2 by the Cauchy-Schwarz inequality.  With M =
+// prod p_m >= 2^(2b + h + 2), 2^h X / M is the signed fraction of
+// sum_m (X mod p_m) 2^h y_m / p_m, y_m = (M / p_m)^-1 mod p_m (the Chinese
 // remainder theorem).  The kernel keeps that fraction as a 64-bit fixed-point
-// sum t += r c_m (mod 2^64), c_m = round(2^64 y_m / p_m), in the tensor-memory
-// columns of the FP64 sums; the error of the rounded constants is at most
-// sum |r| / 2 units of 2^-64 M.  n products replace the n(n+1)/2 slice pairs
-// (13 moduli keep 44 bits per operand at K = 1936, 14 keep 46 at K = 34,992;
-// 7 slices cost 28 products).  The fold runs in two phases: phase 1 reads r
-// and i, reduces v = r +- i below 16 bits and releases the accumulators to
-// the next modulus's MMAs; phase 2 updates the 64-bit sums meanwhile.
+// sum t += r c_m (mod 2^64), c_m = round(2^(64+h) y_m / p_m) mod 2^64, in the
+// tensor-memory columns of the FP64 sums; the rounded constants err by at
+// most sum |r| / 2 units of 2^-(64+h) M, so the h headroom bits (at least 5)
+// divide the recombination error by 2^h.  That error adds to H and O like
+// noise, which the generalized eigenvalues feel far more than the rounding
+// of the operands (a perturbation of A itself), hence the headroom.  n
+// products replace the n(n+1)/2 slice pairs (13 moduli keep 47 bits per
+// operand at K = 1936, 14 keep 51 at K = 34,992; 7 slices cost 28
+// products).  The fold runs in two phases: phase 1 reads r and i, reduces
+// v = r +- i below 16 bits and releases the accumulators to the next
+// modulus's MMAs; phase 2 updates the 64-bit sums meanwhile.
 //
 // Slice storage (int8, K contiguous, K padded to kp8 = multiple of 256):
 //   [slot][slice][array: Br, Bi, Ar, Ai][G (npad rows)][kp8]
@@ -115,14 +121,16 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait that also gives up as soon as another role raised `abort`.
-__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort)
+// Bounded wait (limit cycles; 0: OZ_WAIT_CYCLES) that also gives up as soon
+// as another role raised `abort`.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t *bar, uint32_t parity, volatile int *abort, long long limit)
 {
     const long long t0 = clock64();
+    const long long lim = limit > 0 ? limit : OZ_WAIT_CYCLES;
     while (true) {
         if (mbar_try(bar, parity)) return true;
         if (*abort) return false;
-        if (clock64() - t0 > OZ_WAIT_CYCLES) {
+        if (clock64() - t0 > lim) {
             *abort = 1;
             return false;
         }
@@ -224,10 +232,11 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
 // ------------------------------------------------------------ preparation
-// Column scale sigma(G) = 2^e with max|column| < 2^e (frexp) from the column
-// maximum m that the producers of the A and B planes left in oz_scale (the
-// matching kernels for A, the h_a A epilogue for B).  An all-zero column
-// gets sigma = 1.
+// Column scale sigma(G) = 2^e with m < 2^e (frexp) for the column bound m in
+// oz_scale: with slices the column maximum that the producers of the A and B
+// planes raise (the matching kernels for A, the h_a A epilogue for B), with
+// moduli the column 2-norm (oz_colnorm_kernel).  An all-zero column gets
+// sigma = 1.
 __host__ __device__ __forceinline__ double oz_sigma(double m)
 {
     int e = 0;
@@ -492,6 +501,37 @@ __device__ __forceinline__ void oz_store_mirror(const KDesc &kd, int i0, int j0,
     }
 }
 
+// Column 2-norms of the A planes (which = 0) or the B planes (which = 1) for
+// the modular scheme, written over the maxima in oz_scale: one column per
+// thread column of a 32 x 8 block, the eight rows of threads summing the
+// squares of interleaved rows f (stride 8) and the eight partial sums added
+// in a fixed order, so that the scales, and every result, are the same from
+// run to run.  The factor 1 + 2^-30 covers the rounding of the sum.
+__global__ void __launch_bounds__(256) oz_colnorm_kernel(DevParams p, const KDesc *ks, int which)
+{
+    __shared__ double part[8][33];
+    const KDesc k = ks[blockIdx.y];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int g = blockIdx.x * 32 + tx;
+    const double *pr = which ? k.br : k.ar, *pi = which ? k.bi : k.ai;
+    double s = 0.0;
+    if (g < k.ngp) {
+#pragma unroll 4
+        for (int f = ty; f < p.K; f += 8) {
+            const size_t i = (size_t)f * p.npad + g;
+            const double xr = pr[i], xi = pi[i];
+            s = fma(xr, xr, fma(xi, xi, s));
+        }
+    }
+    part[ty][tx] = s;
+    __syncthreads();
+    if (ty == 0 && g < p.npad) {
+        double t = 0.0;
+        for (int q = 0; q < 8; q++) t += part[q][tx];
+        k.oz_scale[(which ? p.npad : 0) + g] = sqrt(t) * (1.0 + 0x1p-30);
+    }
+}
+
 // The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
 // A 64(f) x 32(G) tile per block, transposed through shared memory: reads
 // G-contiguous planes (a warp reads 32 consecutive G; 16 loads per thread in
@@ -589,7 +629,8 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
 //   at oz_x0 (apw_off rounded down to 16) so that X(n, k) = 0 unless
 //   0 <= k - (apw_off - oz_x0) < napw.
 // Layout [atom][slice][block xb][array re, im][64 rows][lw bytes], one scale
-// sigma per row (power of two above the row maximum).
+// sigma per row (power of two above the row maximum with slices, above the
+// row 2-norm with moduli).
 __device__ __forceinline__ void x_value(const DevParams &p, const OzAtomArgs &xa, int ias, int xb, int n, int fp,
                                         double &re, double &im)
 {
@@ -611,17 +652,19 @@ __device__ __forceinline__ void x_value(const DevParams &p, const OzAtomArgs &xa
     }
 }
 
-// sigma of every X row: one thread per (atom, block, row).
-__global__ void oz_xsig_kernel(DevParams p, OzAtomArgs xa)
+// sigma of every X row: one thread per (atom, block, row); the row maximum
+// (slices) or the row 2-norm (moduli, norm != 0).
+__global__ void oz_xsig_kernel(DevParams p, OzAtomArgs xa, int norm)
 {
     const int n = threadIdx.x, xb = blockIdx.x, ias = blockIdx.y;
-    double m = 0.0;
+    double m = 0.0, s = 0.0;
     for (int fp = 0; fp < p.atoms[ias].napw; fp++) {
         double re, im;
         x_value(p, xa, ias, xb, n, fp, re, im);
         m = fmax(m, fmax(fabs(re), fabs(im)));
+        s = fma(re, re, fma(im, im, s));
     }
-    xa.xsig[((size_t)ias * xa.nxb + xb) * 64 + n] = oz_sigma(m);
+    xa.xsig[((size_t)ias * xa.nxb + xb) * 64 + n] = oz_sigma(norm ? sqrt(s) * (1.0 + 0x1p-30) : m);
 }
 
 // The slices of X: one thread per (atom, block, row, 4 window bytes).
@@ -778,7 +821,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     for (int j = 0; j < (mod ? 1 : g + 1) && !bad; j++) {
                         const int s = mod ? g + 1 : j + 1, t = mod ? g + 1 : g + 1 - j;
                         for (int kb = 0; kb < ti.nst; kb++) {
-                            if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
+                            if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
                                 bad = true;
                                 break;
                             }
@@ -819,7 +862,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                     for (int s0 = 1; s0 <= (mod ? 1 : g + 1) && !bad; s0 += seg_pairs) {
                         const int s1 = min(mod ? 1 : g + 1, s0 + seg_pairs - 1);
                         // the epilogue must have folded the previous segment
-                        if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
+                        if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort, sch.wait)) {
                             bad = true;
                             break;
                         }
@@ -827,7 +870,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                         bool first = true;
                         for (int s = s0; s <= s1 && !bad; s++)
                             for (int kb = 0; kb < nst; kb++) {
-                                if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
+                                if (!mbar_wait_ab(&full[st], uses[st] & 1, abort, sch.wait)) {
                                     bad = true;
                                     break;
                                 }
@@ -869,7 +912,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
             const OzTileInfo ti = oz_tile<MODE, KCH>(p, tiles, tile, kp8);
             for (int g = 0; g < S && !bad; g++) {
                 for (int s0 = 1; s0 <= (mod ? 1 : g + 1); s0 += seg_pairs) {
-                    const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
+                    const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort, sch.wait));
                     if (!ok) {
                         bad = true;
                         break;
@@ -927,7 +970,7 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                 if (staged) {
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&stg);
-                    if (__all_sync(0xffffffffu, mbar_wait_ab(&stg, 0, abort)))
+                    if (__all_sync(0xffffffffu, mbar_wait_ab(&stg, 0, abort, sch.wait)))
                         oz_store_mirror(kd, ti.i0, ti.j0, mirror, warp - 4, lane);
                 }
             } else {
@@ -1116,7 +1159,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                 for (int j = 0; j < (mod ? 1 : g + 1) && !bad; j++) {
                     const int s = mod ? g + 1 : j + 1, t = mod ? g + 1 : g + 1 - j;
                     for (int kb = 0; kb < nst; kb++) {
-                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort)) {
+                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
                             bad = true;
                             break;
                         }
@@ -1149,7 +1192,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             for (int g = 0; g < S && !bad; g++)
                 for (int s0 = 1; s0 <= (mod ? 1 : g + 1) && !bad; s0 += seg_pairs) {
                     const int s1 = min(mod ? 1 : g + 1, s0 + seg_pairs - 1);
-                    if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort)) {
+                    if (nseg > 0 && !mbar_wait_ab(&acce, (nseg - 1) & 1, abort, sch.wait)) {
                         bad = true;
                         break;
                     }
@@ -1157,7 +1200,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                     bool first = true;
                     for (int s = s0; s <= s1 && !bad; s++)
                         for (int kb = 0; kb < nst; kb++) {
-                            if (!mbar_wait_ab(&full[st], uses[st] & 1, abort)) {
+                            if (!mbar_wait_ab(&full[st], uses[st] & 1, abort, sch.wait)) {
                                 bad = true;
                                 break;
                             }
@@ -1197,7 +1240,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
         bool bad = false;
         for (int g = 0; g < S && !bad; g++) {
             for (int s0 = 1; s0 <= (mod ? 1 : g + 1); s0 += seg_pairs) {
-                const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort));
+                const bool ok = __all_sync(0xffffffffu, mbar_wait_ab(&accf, nseg & 1, abort, sch.wait));
                 if (!ok) {
                     bad = true;
                     break;
@@ -1247,7 +1290,7 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             oz_store_ho(p, kd, sch, i0, j0, t_lane, qd * 32 + lane, half, mirror);
         __syncwarp();
         if (lane == 0) mbar_arrive(&stg);
-        if (__all_sync(0xffffffffu, mbar_wait_ab(&stg, 0, abort) && !*abort))
+        if (__all_sync(0xffffffffu, mbar_wait_ab(&stg, 0, abort, sch.wait) && !*abort))
             oz_store_mirror(kd, i0, j0, mirror, warp - 4, lane);
     }
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
@@ -1279,13 +1322,13 @@ int oz_seg_pairs(int S, int kp8)
 static const int OZ_MODULI[OZ_MAX_MODULI] = {253, 251, 247, 241, 239, 233, 229, 227,
                                              223, 217, 211, 199, 197, 193, 191, 185};
 
-// Bits per operand so that |X| <= 2K 2^(b + b') < M / 2 for a product of
-// 2K int terms; log2 M is a sum of logarithms, taken with a margin.
-static int oz_mod_bits(int n, int K)
+// log2 M for the first n moduli (a sum of logarithms: the plan keeps a
+// margin of one bit beyond it).
+static double oz_log2_modulus(int n)
 {
     double lm = 0.0;
     for (int m = 0; m < n; m++) lm += std::log2((double)OZ_MODULI[m]);
-    return (int)std::floor(lm - 1.0 - std::log2(2.0 * K) - 1e-9);
+    return lm;
 }
 
 static int oz_inverse_mod(long long a, long long p)
@@ -1299,38 +1342,54 @@ static int oz_inverse_mod(long long a, long long p)
     return r0 == 1 ? (int)(((t0 % p) + p) % p) : -1;
 }
 
-// The modular scheme for n moduli (0: the fewest in 6..16 that keep b >= 44;
-// at 44 bits the quantisation error is already below the floor of the
-// 64-bit recombination, sum |r| / 2 units of 2^-64 M),
-// contraction length K (H/O tiles) and per-atom window kx.  Returns 0, or
-// -1 if no valid plan exists (n out of range, b or bx below 8, or K past
-// the exact int32 range of one product: 2 K 127^2 < 2^31).
+// The modular scheme for n moduli, contraction length K (H/O tiles) and
+// per-atom window kx.  Columns are scaled by their 2-norms, so the integer
+// products obey |X| <= 2^(2b) (1 + eps)^2 (H/O) and 2^(b + bx) (1 + eps)^2
+// (per-atom) whatever K; the plan keeps h >= 5 headroom bits and one bit of
+// margin: b = min(52, floor((log2 M - 7) / 2)), h = floor(log2 M - 2 - 2b),
+// bx = min(52, floor(log2 M - 2 - h - b)).  The quantisation error of the
+// operands grows like 2^-b sqrt(K), so n = 0 takes the fewest moduli in
+// 6..16 with b >= 41 + log2(K) / 2 (47 bits and 13 moduli at K = 1936, 51
+// bits and 14 moduli at K = 34,992).  Returns 0, or -1 if no valid plan
+// exists (n out of range, b or bx below 8, or K past the exact int32 range
+// of one product: 2 K 127^2 < 2^31).
+static void oz_mod_bits(int n, int *b, int *h, int *bx)
+{
+    const double lm = oz_log2_modulus(n) - 1e-9;
+    *b = std::min(52, (int)std::floor((lm - 7.0) / 2.0));
+    *h = (int)std::floor(lm - 2.0 - 2.0 * *b);
+    *bx = std::min(52, (int)std::floor(lm - 2.0 - *h - *b));
+}
+
 int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
 {
     if (K < 1 || kx < 1 || K > 65536 || kx > 65536) return -1;
+    int b = 0, h = 0, bx = 0;
     if (n == 0) {
+        const int want = (int)std::ceil(41.0 + 0.5 * std::log2((double)K) - 1e-9);
         n = OZ_MAX_MODULI;
-        for (int q = 6; q <= OZ_MAX_MODULI; q++)
-            if (oz_mod_bits(q, K) >= 2 * 44) {
+        for (int q = 6; q <= OZ_MAX_MODULI; q++) {
+            oz_mod_bits(q, &b, &h, &bx);
+            if (b >= want) {
                 n = q;
                 break;
             }
+        }
     }
     if (n < 6 || n > OZ_MAX_MODULI) return -1;
-    const int two_b = oz_mod_bits(n, K);
-    const int b = std::min(52, two_b / 2);
-    const int bx = std::min(52, oz_mod_bits(n, kx) - b);
-    if (b < 8 || bx < 8) return -1;
+    oz_mod_bits(n, &b, &h, &bx);
+    if (b < 8 || bx < 8 || h < 5) return -1;
     OzScheme s{};
     s.mod = 1;
     s.n = n;
     s.seg = s.segx = 1;
     s.b = b;
     s.bx = bx;
+    s.h = h;
     double M = 1.0;
     for (int m = 0; m < n; m++) M *= (double)OZ_MODULI[m];
-    s.fin = std::ldexp(M, -64 - 2 * b);
-    s.finx = std::ldexp(M, -64 - b - bx);
+    s.fin = std::ldexp(M, -64 - h - 2 * b);
+    s.finx = std::ldexp(M, -64 - h - b - bx);
     for (int m = 0; m < n; m++) {
         const int p = OZ_MODULI[m];
         long long mm = 1;   // (M / p) mod p
@@ -1343,8 +1402,8 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
         s.fp[m] = (float)p;
         s.finv[m] = 1.0f / (float)p;
         for (int j = 0; j < 3; j++) s.fc[j][m] = (float)((1LL << (13 * (j + 1))) % p);
-        // round(2^64 y / p); y < p, so the quotient is below 2^64
-        const unsigned __int128 num = ((unsigned __int128)y << 64) + (unsigned)(p / 2);
+        // round(2^(64+h) y / p) mod 2^64 (y < p < 2^8 and h <= 18: the numerator fits 128 bits)
+        const unsigned __int128 num = ((unsigned __int128)y << (64 + h)) + (unsigned)(p / 2);
         s.c[m] = (unsigned long long)(num / (unsigned)p);
     }
     *sch = s;
@@ -1368,9 +1427,15 @@ cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const 
     return cudaGetLastError();
 }
 
+cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, cudaStream_t s)
+{
+    oz_colnorm_kernel<<<dim3(p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, which);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s)
 {
-    oz_xsig_kernel<<<dim3(xa.nxb, p.natmtot), 64, 0, s>>>(p, xa);
+    oz_xsig_kernel<<<dim3(xa.nxb, p.natmtot), 64, 0, s>>>(p, xa, sch.mod);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     oz_xsplit_kernel<<<dim3(8, xa.nxb, p.natmtot), dim3(xa.lw / 4, 8), 0, s>>>(p, xa, sch);
@@ -1383,13 +1448,11 @@ static cudaError_t launch_cfg(const CUtensorMap *mapA, const CUtensorMap *mapB, 
                               bool persistent, cudaStream_t s)
 {
     constexpr int smem = NST * 3 * KCH * OZ_TILE + 1024;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e =
-            cudaFuncSetAttribute(oz_mma_kernel<MODE, KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(oz_mma_kernel<MODE, KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    });
+    if (e != cudaSuccess) return e;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1405,12 +1468,11 @@ static cudaError_t launch_2sm(const CUtensorMap *mapA, const CUtensorMap *mapB2,
                               const void *d_tiles, int ntiles, const OzScheme &sch, int kp8, cudaStream_t s)
 {
     constexpr int smem = NST * (2 * KCH * OZ_TILE + KCH * OZ_TILE / 2) + 1024;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz_mma2_kernel<KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(oz_mma2_kernel<KCH, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    });
+    if (e != cudaSuccess) return e;
     oz_mma2_kernel<KCH, NST><<<2 * ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapB2, p, d_k, (const int *)d_tiles, sch,
                                                                   kp8);
     return cudaGetLastError();
@@ -1530,7 +1592,8 @@ bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, s
 
 }  // namespace exs
 
-extern "C" int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsigned long long *c, int *b, int *bx)
+extern "C" int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsigned long long *c, int *b, int *bx,
+                                int *h)
 {
     exs::OzScheme s{};
     if (exs::oz_mod_plan(n, K, kx, &s) != 0) return EXS_ERR_ARG;
@@ -1541,5 +1604,6 @@ extern "C" int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsign
     }
     if (b) *b = s.b;
     if (bx) *bx = s.bx;
+    if (h) *h = s.h;
     return EXS_OK;
 }

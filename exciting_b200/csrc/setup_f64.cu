@@ -254,12 +254,11 @@ static cudaError_t launch_kind(const DevParams &p, const GemmProb *d_probs, cons
                                const KDesc *d_k, cudaStream_t s)
 {
     if (nwork <= 0) return cudaSuccess;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(zgemm_dmma_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GB_SMEM);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(zgemm_dmma_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GB_SMEM);
+    });
+    if (e != cudaSuccess) return e;
     zgemm_dmma_kernel<KIND><<<(unsigned)nwork, GB_THREADS, GB_SMEM, s>>>(p, d_probs, d_work, d_k);
     return cudaGetLastError();
 }

@@ -195,6 +195,10 @@ class Setup:
         self._check(self.lib.exs_set_precision(self.ctx, m, slices))
 
     # ------------------------------------------------------------------
+    def set_wait_limit(self, cycles: int = 0):
+        """Limit (SM cycles) of the split-precision kernels' pipeline waits; 0 = the default (~1 s)."""
+        self._check(self.lib.exs_set_wait_limit(self.ctx, int(cycles)))
+
     def match(self, gk):
         """apwalm(ngkmax, apwordmax, lmmaxapw, natmtot) from the reference's match inputs."""
         b = self.sys.basis
@@ -437,6 +441,26 @@ class Setup:
         return f
 
 
+    def adjoint(self, gk, c, w, eps, *, dveffig: bool = False, dh: bool = False):
+        """Adjoint of the setup for L = sum_n w_n c_n^H (H - eps_n O) c_n
+        (exs_adjoint): (dL/dtau (3, natmtot), dL/dV (ngvec) or None,
+        dL/dh_a (maxaa, maxaa, natmtot) or None)."""
+        s = self.sys
+        ig, vg = self._gk_arrays(gk)
+        cv = _f(c, np.complex128)
+        ffacg = _f(np.stack([ffacg_species(s.gv.gc[: s.gv.ngvec], r, s.crystal.omega) for r in s.rmt], axis=1),
+                   np.float64)
+        vgc = _f(s.gv.vgc[:, : s.gv.ngvec], np.float64)
+        dtau = np.zeros((3, s.natmtot), order="F")
+        dv = np.zeros(s.gv.ngvec, dtype=np.complex128) if dveffig else None
+        dhv = np.zeros((self.maxaa, self.maxaa, s.natmtot), dtype=np.complex128, order="F") if dh else None
+        self._check(self.lib.exs_adjoint(self.ctx, gk.ngp, _ptr(ig), _ptr(vg), cv.shape[1], _ptr(cv), cv.shape[0],
+                                         _ptr(_f(w, np.float64)), _ptr(_f(eps, np.float64)), _ptr(ffacg),
+                                         _ptr(vgc), _ptr(dtau), None if dv is None else _ptr(dv),
+                                         None if dhv is None else _ptr(dhv)))
+        return dtau, dv, dhv
+
+
 class SetupGraph:
     """A captured batched setup (exs_graph_*): launch() replays it on the
     (first) context's stream; synchronize() waits and reports device errors."""
@@ -466,17 +490,17 @@ class SetupGraph:
 
 def ozaki_moduli(n: int, K: int, kx: int):
     """The modular plan of exs_set_precision(EXS_PREC_OZAKI_MOD, n) for contraction
-    length K and per-atom windows of kx rows: (moduli, CRT constants, b, bx)."""
+    length K and per-atom windows of kx rows: (moduli, CRT constants, b, bx, h)."""
     lib = abi.load()
-    n_out, b, bx = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    n_out, b, bx, h = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     p = np.zeros(16, dtype=np.int32)
     c = np.zeros(16, dtype=np.uint64)
     rc = lib.exs_ozaki_moduli(int(n), int(K), int(kx), ctypes.byref(n_out), _ptr(p), _ptr(c), ctypes.byref(b),
-                              ctypes.byref(bx))
+                              ctypes.byref(bx), ctypes.byref(h))
     if rc != 0:
         raise abi.ExsError(rc, "no modular plan for n=%d K=%d kx=%d" % (n, K, kx))
     m = n_out.value
-    return [int(x) for x in p[:m]], [int(x) for x in c[:m]], b.value, bx.value
+    return [int(x) for x in p[:m]], [int(x) for x in c[:m]], b.value, bx.value, h.value
 
 
 def multi_graph(setups, batches) -> SetupGraph:

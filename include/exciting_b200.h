@@ -30,7 +30,9 @@ enum {
     EXS_ERR_SIZE = -3,       /* a size above the compiled limits or the context's maxima */
     EXS_ERR_INDEX = -4,      /* a G-G' difference fell outside the ivgig box */
     EXS_ERR_STATE = -5,      /* exs_set_scf_inputs has not been called */
-    EXS_ERR_NOMEM = -6       /* a device allocation failed */
+    EXS_ERR_NOMEM = -6,      /* a device allocation failed */
+    EXS_ERR_TIMEOUT = -7     /* a bounded wait inside a tensor-core kernel expired; the kernel gave up
+                                cleanly (its copies and products drained) and the context stays usable */
 };
 
 enum { EXS_REL_NONE = 0, EXS_REL_ZORA = 1, EXS_REL_IORA = 2 };   /* ValenceRelativity */
@@ -148,19 +150,23 @@ int exs_fderiv_int(int n, const double *x, const double *f, double *result);
 /* Select the MT contraction arithmetic: EXS_PREC_FP64 (native FP64),
  * EXS_PREC_OZAKI_INT8 with `slices` int8 slices per operand (3..9), or
  * EXS_PREC_OZAKI_MOD: the operands as integers modulo `slices` pairwise
- * coprime odd moduli (6..16; 0 = the fewest that keep 44 bits per operand
- * for this context's K), one int8 product per modulus, recombined by the
- * Chinese remainder theorem.  No reference counterpart (the reference's
+ * coprime odd moduli (6..16; 0 = the fewest that keep 41 + log2(K)/2 bits
+ * per 2-norm-scaled operand column for this context's K), one int8 product
+ * per modulus, recombined by the Chinese remainder theorem.  No reference counterpart (the reference's
  * contraction is zgemm in FP64). */
 int exs_set_precision(exs_ctx *ctx, int mode, int slices);
 
 /* The modular plan exs_set_precision(EXS_PREC_OZAKI_MOD, n) would use for a
  * contraction length K (2K products per real sum) and per-atom windows of
- * kx rows: the moduli p[0..n-1], the constants c[m] = round(2^64 y_m / p_m)
- * mod 2^64 with y_m = (M / p_m)^-1 mod p_m, M = prod p, and the bits b of
- * the scaled A and B columns and bx of the scaled h_a / loa rows.  n = 0
- * picks n as exs_set_precision does; *n_out receives it.  Host only. */
-int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsigned long long *c, int *b, int *bx);
+ * kx rows: the moduli p[0..n-1], the constants
+ * c[m] = round(2^(64+h) y_m / p_m) mod 2^64 with y_m = (M / p_m)^-1 mod p_m,
+ * M = prod p, the bits b of the A and B columns (scaled to 2-norm <= 2^b),
+ * bx of the h_a / loa rows (likewise) and the headroom h of the 64-bit
+ * recombination (2^(2b + h + 2) <= M and 2^(b + bx + h + 2) <= M).  n = 0
+ * picks n as exs_set_precision does; *n_out receives it.  Any output pointer
+ * may be NULL.  Host only. */
+int exs_ozaki_moduli(int n, int K, int kx, int *n_out, int *p, unsigned long long *c, int *b, int *bx,
+                     int *h);
 
 /* Replaces  call match(ngp, gpc, tpgpc, sfacgp, apwalm)   (src/match.f90:13).
  *   gpc(ngkmax), tpgpc(2, ngkmax), sfacgp(ngkmax, natmtot)  in;
@@ -390,6 +396,16 @@ int exs_adjoint(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc, int
                 const double *ffacg, const double *vgc, double *dtau,
                 exs_complex *dveffig, exs_complex *dh);
 
+/* Limit, in SM clock cycles, of every wait of the split-precision
+ * kernels' pipelines (a producer on a free stage, the tensor core on a
+ * filled one, the epilogue on finished products); 0 restores the default
+ * of 2e9 (about one second).  A wait that runs out makes the kernel give up
+ * cleanly and the call return EXS_ERR_TIMEOUT; the context stays usable.
+ * Graphs captured before the call keep their old limit (they are
+ * invalidated: exs_graph_launch returns EXS_ERR_STATE).  No counterpart in
+ * the reference (failure detection of the device pipeline). */
+int exs_set_wait_limit(exs_ctx *ctx, long long cycles);
+
 /* Run the context's work on a caller-owned CUDA stream (a cudaStream_t
  * passed as void*); NULL returns to the context's own stream. */
 int exs_set_stream(exs_ctx *ctx, void *stream);
@@ -412,8 +428,10 @@ int exs_last_timings(exs_ctx *ctx, double *t, int n);
  *     apwi^H apwi as full Hermitian matrices (lower = conjugate of upper).
  * Allocates nothing; EXS_ERR_SIZE when the work space exceeds 32 MiB.  The
  * first call on a device looks up the array's device address (make it
- * before any stream capture).  Calls share the array: calls that overlap on
- * the GPU race, so serialise them.  stream: a cudaStream_t, or NULL. */
+ * before any stream capture); cudaDeviceReset destroys the array, so do not
+ * call it again on a device after resetting it.  Calls share the array:
+ * calls that overlap on the GPU race, so serialise them.  stream: a
+ * cudaStream_t, or NULL. */
 int exs_mt_contract_noalloc(int natmtot, int maxaa, const int *napw, int ngp,
                             const exs_complex *apwi, const exs_complex *aa,
                             exs_complex *h, exs_complex *o, int ld, void *stream);

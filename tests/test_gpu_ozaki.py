@@ -1,18 +1,22 @@
-"""Split-precision (int8 slices on tcgen05) MT contraction against the FP64 oracle.
-
-Tolerances (the benchmark's stated bar): ||dH||_F/||H||_F <= 1e-12,
-||dO||_F/||O||_F <= 1e-12 and eigenvalues within 1e-8 Ha with 7 slices; the
-error must fall as slices are added; the conjugate mirror stays exact.
-The eigenvalues compared are the lowest NSTFV of H x = e O x: the reference's
-solver asks zhegvx for the range IL = 1 .. IU = nstfv only
-(src/src_eigensystem/modfvsystem.f90:691-693).  The bar is 1e-8 Ha for
-|e| <= 1 Ha and 1e-8 |e| above: the seeded synthetic MT integrals put some
-of the lowest generalized eigenvalues near -1000 Ha, where an absolute 1e-8
-would ask for 17 significant digits of an FP64 result.
+"""Split-precision MT contraction on tcgen05 against the FP64 oracle.
 
 The modular mode (ozaki_mod: residues modulo pairwise coprime moduli, one
-int8 product per modulus) is held to the same bars; its error must fall as
-moduli are added.
+int8 product per modulus, the mode the benchmark times) is held to the
+metric's bars: ||dH||_F/||H||_F <= 1e-12, ||dO||_F/||O||_F <= 1e-12 and the
+lowest NSTFV generalized eigenvalues within an absolute 1e-8 Ha (the
+reference's own tolerance, test/test_farm/groundstate-GGA_PBE-properties-Si/
+init.xml:27 tolEigval 1e-8).  The eigenvalues compared are the lowest NSTFV
+of H x = e O x: the reference's solver asks zhegvx for the range IL = 1 ..
+IU = nstfv only (src/src_eigensystem/modfvsystem.f90:691-693).  The seeded
+synthetic MT integrals of the 8-atom cell put the lowest of them near
+-1600 Ha with O conditioned ~2.5e4, which makes that bar a relative 6e-12.
+
+The slice mode (ozaki: 7 int8 slices, pairs s + t <= 8) meets the Frobenius
+bars and the absolute eigenvalue bar on the 2-atom cells; on the 8-atom
+cell the pairs it drops add noise to H and O like an inexact recombination,
+and its eigenvalues are held to 1e-8 relative there (SLICE_EIG_REL), a bar
+of the slice mode only.  The error of each mode must fall as slices or
+moduli are added; the conjugate mirror stays exact.
 """
 import numpy as np
 import pytest
@@ -24,8 +28,9 @@ from exciting_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 TOL_FRO = 1e-12
-TOL_EIG = 1e-8
-NSTFV = 40          # lowest eigenvalues compared (a superset of the Si cells' nstfv)
+TOL_EIG = 1e-8          # Ha, absolute
+SLICE_EIG_REL = 1e-8    # the slice mode on the 8-atom cell: relative to |e| above 1 Ha
+NSTFV = 40              # lowest eigenvalues compared (a superset of the Si cells' nstfv)
 
 
 def rel_fro(a, b):
@@ -33,8 +38,12 @@ def rel_fro(a, b):
 
 
 def eig_dev(w, wr):
-    """Eigenvalue deviation in units of the bar: |dw| / (1e-8 max(1, |w|))."""
-    return np.max(np.abs(w - wr) / (TOL_EIG * np.maximum(1.0, np.abs(wr))))
+    """Eigenvalue deviation in units of the absolute bar: max |dw| / 1e-8 Ha."""
+    return np.max(np.abs(w - wr)) / TOL_EIG
+
+
+def eig_dev_slices(w, wr):
+    return np.max(np.abs(w - wr) / (SLICE_EIG_REL * np.maximum(1.0, np.abs(wr))))
 
 
 def _setup(s, slices=7, mode="ozaki", **kw):
@@ -78,7 +87,25 @@ def test_ozaki_cube8_batched_vs_oracle(mode):
         assert rel_fro(o, orf) <= TOL_FRO, rel_fro(o, orf)
     w = sl.eigh(out[13][0], out[13][1], eigvals_only=True, subset_by_index=[0, NSTFV - 1])
     wr = sl.eigh(hr, orf, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
-    assert eig_dev(w, wr) <= 1.0
+    assert (eig_dev(w, wr) if mode == "ozaki_mod" else eig_dev_slices(w, wr)) <= 1.0, np.max(np.abs(w - wr))
+
+
+def test_ozaki_mod_cube8_all_kpoints_eigenvalues():
+    """All 27 k-points of the 8-atom batch in the modular mode with the
+    default plan: the lowest 40 eigenvalues of every k-point within 1e-8 Ha
+    of those of the oracle's FP64 H and O."""
+    s = W.si_cube8()
+    gks = s.gksets()
+    st = _setup(s, mode="ozaki_mod", max_batch=len(gks))
+    out = st.setup_batched(gks)
+    worst = 0.0
+    for gk, (h, o) in zip(gks, out):
+        hr, orf = O.hamiltonandoverlapsetup(s, gk)
+        assert rel_fro(h, hr) <= TOL_FRO and rel_fro(o, orf) <= TOL_FRO
+        w = sl.eigh(h, o, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
+        wr = sl.eigh(hr, orf, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
+        worst = max(worst, float(np.max(np.abs(w - wr))))
+    assert worst <= TOL_EIG, worst
 
 
 @pytest.mark.parametrize("mode", MODES)

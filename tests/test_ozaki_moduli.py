@@ -1,14 +1,16 @@
 """The modular split-precision scheme (EXS_PREC_OZAKI_MOD), checked on the CPU.
 
 The library's plan (exs_ozaki_moduli: moduli, Chinese-remainder constants,
-bits per operand) is checked against exact integer arithmetic, and the
-device arithmetic is emulated in numpy with that plan: residues in
+bits per operand, headroom bits) is checked against exact integer
+arithmetic, and the device arithmetic is emulated in numpy with that plan:
+columns scaled by a power of two above their 2-norms, residues in
 [-127, 127], one exact integer product per modulus, the multiply-high
-quotient of the fold, the 64-bit wrapping sum t += r c_m and the final
-t / 2^64 * M.  The emulated products must reconstruct the exact integer
-product within the stated bound (sum |r| / 2 + 1 units of 2^-64 M), and an
-emulated H = A^H B on a Si k-point must meet the 1e-12 bar.  No GPU is
-touched.
+quotient of the fold, the 64-bit wrapping sum t += r c_m with c_m =
+round(2^(64+h) y_m / p_m) and the final t / 2^(64+h) * M.  The emulated
+products must reconstruct the exact integer product within the stated bound
+(sum |r| / 2 + 1 units of 2^-(64+h) M), and an emulated setup on a Si
+k-point must meet the 1e-12 Frobenius bar and keep the lowest generalized
+eigenvalues within 1e-8 Ha.  No GPU is touched.
 """
 import ctypes
 import math
@@ -24,19 +26,19 @@ def plan(n, K, kx):
     n_out = ctypes.c_int()
     p = np.zeros(16, dtype=np.int32)
     c = np.zeros(16, dtype=np.uint64)
-    b, bx = ctypes.c_int(), ctypes.c_int()
+    b, bx, h = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     rc = lib.exs_ozaki_moduli(n, K, kx, ctypes.byref(n_out), p.ctypes.data_as(ctypes.c_void_p),
-                              c.ctypes.data_as(ctypes.c_void_p), ctypes.byref(b), ctypes.byref(bx))
+                              c.ctypes.data_as(ctypes.c_void_p), ctypes.byref(b), ctypes.byref(bx), ctypes.byref(h))
     if rc != 0:
         return None
     m = n_out.value
-    return [int(x) for x in p[:m]], [int(x) for x in c[:m]], b.value, bx.value
+    return [int(x) for x in p[:m]], [int(x) for x in c[:m]], b.value, bx.value, h.value
 
 
 @pytest.mark.parametrize("n,K,kx", [(14, 1936, 242), (12, 1936, 242), (0, 1936, 242), (0, 34992, 162),
-                                    (16, 65536, 512), (6, 200, 50)])
+                                    (16, 65536, 512), (6, 200, 50), (0, 324, 162)])
 def test_plan_constants_and_bounds(n, K, kx):
-    ps, cs, b, bx = plan(n, K, kx)
+    ps, cs, b, bx, h = plan(n, K, kx)
     if n:
         assert len(ps) == n
     for i in range(len(ps)):
@@ -46,17 +48,26 @@ def test_plan_constants_and_bounds(n, K, kx):
     M = math.prod(ps)
     for p, c in zip(ps, cs):
         y = pow(M // p, -1, p)
-        assert c == ((y << 64) + p // 2) // p          # round(2^64 y / p)
-    # |X| <= 2K 2^(2b) < M / 2 for the H/O products, 2 kx 2^(b + bx) for the per-atom ones
-    assert 2 * K * 2 ** (2 * b) < M // 2 and 2 * kx * 2 ** (b + bx) < M // 2
-    assert b <= 52 and bx <= 52
-    # b is the largest that fits (unless capped at 52)
-    assert b == 52 or 2 * K * 2 ** (2 * (b + 1)) >= M // 2
+        assert c == (((y << (64 + h)) + p // 2) // p) % 2 ** 64      # round(2^(64+h) y / p) mod 2^64
+    # |X| <= 2^(2b) (1 + eps)^2 for 2-norm-scaled columns: one bit of margin beyond 2^h |X| < M / 2
+    assert 2 ** (2 * b + h + 2) <= M and 2 ** (b + bx + h + 2) <= M
+    assert h >= 5 and b <= 52 and bx <= 52
+    # b is the largest that keeps 5 headroom bits (unless capped at 52), h and bx the largest after it
+    assert b == 52 or 2 ** (2 * (b + 1) + 5 + 2) > M
+    assert 2 ** (2 * b + (h + 1) + 2) > M
+    assert bx == 52 or 2 ** (b + bx + 1 + h + 2) > M
     if n == 0:
-        assert b >= 44
-        if len(ps) > 6:    # one modulus fewer would not keep 44 bits
-            Mf = math.prod(ps[:-1])
-            assert 2 * K * 2 ** 88 >= Mf // 2
+        want = math.ceil(41 + 0.5 * math.log2(K) - 1e-9)
+        assert b >= want
+        if len(ps) > 6:    # one modulus fewer would not keep the bits
+            assert plan(len(ps) - 1, K, kx)[2] < want
+
+
+def test_plan_counts_of_the_benchmark_cells():
+    """13 moduli at 47 bits for the 8-atom cell (K = 1936), 14 at 51 for the
+    216-atom cell (K = 34,992), both with 5 headroom bits."""
+    assert [plan(0, 1936, 242)[k] for k in (2, 4)] == [47, 5] and len(plan(0, 1936, 242)[0]) == 13
+    assert [plan(0, 34992, 162)[k] for k in (2, 4)] == [51, 5] and len(plan(0, 34992, 162)[0]) == 14
 
 
 def test_plan_rejects_bad_arguments():
@@ -83,7 +94,7 @@ def emulate(X, Y, ps, cs):
     t = np.zeros((X.shape[1], Y.shape[1]), dtype=np.uint64)
     rsum = np.zeros(t.shape)
     for p, c in zip(ps, cs):
-        v = (_residues(X, p).T @ _residues(Y, p)).astype(np.int64)     # exact: |v| < 2^31
+        v = np.rint(_residues(X, p).T @ _residues(Y, p)).astype(np.int64)     # exact: |v| < 2^31
         assert np.abs(v).max() < 2 ** 31
         r = _fold_reduce(v, p)
         assert r.min() >= -p / 4 and r.max() <= 5 * p / 4
@@ -93,57 +104,102 @@ def emulate(X, Y, ps, cs):
     return t.view(np.int64), rsum
 
 
+def _norm_columns(rng, K, ncol, b):
+    """Integer columns of 2-norm <= 2^b (random directions, rounded)."""
+    Z = rng.standard_normal((K, ncol))
+    Z *= (2.0 ** b) * (1 - 1e-9) / np.linalg.norm(Z, axis=0)
+    return np.trunc(Z)
+
+
 @pytest.mark.parametrize("n", [8, 12, 14])
 def test_emulated_fold_reconstructs_integer_products(n):
     rng = np.random.default_rng(n)
     K = 300
-    ps, cs, b, _ = plan(n, K // 2, 8)
-    lim = 2 ** b
-    X = rng.integers(-lim, lim + 1, size=(K, 5), dtype=np.int64)
-    Y = rng.integers(-lim, lim + 1, size=(K, 4), dtype=np.int64)
-    X[:, 0] = lim                      # the bound's extreme: one column pair at +-2^b everywhere
-    Y[:, 0] = -lim
-    t, rsum = emulate(X.astype(np.float64), Y.astype(np.float64), ps, cs)
+    ps, cs, b, _, h = plan(n, K // 2, 8)
+    X = _norm_columns(rng, K, 5, b)
+    Y = _norm_columns(rng, K, 4, b)
+    Y[:, 0] = -X[:, 0]                 # the bound's extreme: a column pair with |X| = |x|^2 ~ 2^(2b)
+    t, rsum = emulate(X, Y, ps, cs)
     M = math.prod(ps)
     for i in range(X.shape[1]):
         for j in range(Y.shape[1]):
             exact = sum(int(a) * int(bb) for a, bb in zip(X[:, i], Y[:, j]))
-            assert abs(exact) < M // 2
-            # t = 2^64 X / M + e, |e| <= sum |r| / 2 (rounded constants) + 1 (the exact quotient's fraction)
-            err = int(t[i, j]) * M - exact * 2 ** 64
+            assert 2 ** (h + 1) * abs(exact) < M
+            # t = 2^(64+h) X / M + e, |e| <= sum |r| / 2 (rounded constants) + 1 (the exact quotient's fraction)
+            err = int(t[i, j]) * M - exact * 2 ** (64 + h)
             assert abs(err) <= (rsum[i, j] / 2 + 1) * M, (i, j)
 
 
 def _split_scaled(Z, b):
-    """Columns scaled by a power of two above their maximum, then to b-bit integers."""
-    m = np.maximum(np.abs(Z.real).max(0), np.abs(Z.imag).max(0))
+    """Columns scaled by a power of two above their 2-norm, then to integers (norm <= 2^b)."""
+    m = np.sqrt((np.abs(Z) ** 2).sum(0)) * (1 + 2.0 ** -30)
     sig = np.ldexp(1.0, np.frexp(np.where(m > 0, m, 1.0))[1])
     return np.rint(Z.real / sig * 2.0 ** b), np.rint(Z.imag / sig * 2.0 ** b), sig
 
 
-def test_emulated_contraction_meets_the_bar():
-    """H = A^H B and O = A^H A for one Si k-point (2 atoms, K = 2 x 81 x 2)."""
+def _rows_scaled(X, b):
+    m = np.sqrt((np.abs(X) ** 2).sum(1)) * (1 + 2.0 ** -30)
+    sx = np.ldexp(1.0, np.frexp(np.where(m > 0, m, 1.0))[1])
+    return np.rint(X.real / sx[:, None] * 2.0 ** b), np.rint(X.imag / sx[:, None] * 2.0 ** b), sx
+
+
+def _emulated_setup(s, gk, apwalm):
+    """H and O of one k-point with the APW-APW block (and B = h_a A) taken
+    through the emulated integer path of the default plan."""
+    import lapw_oracle as O
+    N = gk.ngp
+    apwi = [O._apwi(s, apwalm, N, a) for a in range(s.natmtot)]
+    A = np.concatenate(apwi)
+    K, kx = A.shape[0], s.basis.maxaa
+    ps, cs, b, bx, h = plan(0, K, kx)
+    M = float(math.prod(ps))
+    ar, ai, sa = _split_scaled(A, b)
+    Bs = []
+    for a in range(s.natmtot):      # the per-atom products B_a = h_a A_a (A residues over the atom's rows)
+        f0 = sum(x.shape[0] for x in apwi[:a])
+        war, wai = ar[f0:f0 + apwi[a].shape[0]], ai[f0:f0 + apwi[a].shape[0]]
+        hr, hi, sx = _rows_scaled(s.mt_aa[:, :, a], bx)
+        X = np.concatenate([hr.T, hi.T])
+        re = emulate(X, np.concatenate([war, -wai]), ps, cs)[0].astype(np.float64)
+        im = emulate(X, np.concatenate([wai, war]), ps, cs)[0].astype(np.float64)
+        Bs.append((re + 1j * im) * (M * 2.0 ** (-64 - h - b - bx)) * np.outer(sx, sa))
+    B = np.concatenate(Bs)
+    br, bi, sb = _split_scaled(B, b)
+    XA = np.concatenate([ar, ai])                   # [Ar; Ai]
+    YH = [np.concatenate([br, bi]), np.concatenate([bi, -br])]    # Re H, Im H
+    YO = [np.concatenate([ar, ai]), np.concatenate([ai, -ar])]    # Re O, Im O
+    scale = M * 2.0 ** (-64 - h - 2 * b)
+    out = []
+    for Ys, sy in ((YH, sb), (YO, sa)):
+        parts = [emulate(XA, Y, ps, cs)[0].astype(np.float64) * scale for Y in Ys]
+        out.append((parts[0] + 1j * parts[1]) * np.outer(sa, sy))
+    Bx = np.concatenate([s.mt_aa[:, :, a] @ apwi[a] for a in range(s.natmtot)])
+    return out[0], out[1], A.conj().T @ Bx, A.conj().T @ A, B, Bx
+
+
+def test_emulated_setup_meets_the_bars():
+    """One Si k-point (2 atoms, K = 2 x 81 x 2): the emulated integer path
+    (B = h_a A included) within 1e-12 of the FP64 products in Frobenius norm,
+    and the lowest 20 generalized eigenvalues of the whole H, O within
+    1e-8 Ha of the FP64 ones (the metric's absolute bar)."""
+    import scipy.linalg as sl
     import lapw_oracle as O
     from exciting_b200 import workloads as W
     s = W.si_fcc("text")
     gk = s.gkset(s.kpoints[3])
     apwalm, _ = O.match(s, gk)
+    Hm, Om, Href, Oref, B, Bx = _emulated_setup(s, gk, apwalm)
+    assert np.linalg.norm(B - Bx) / np.linalg.norm(Bx) <= 1e-13
+    assert np.linalg.norm(Hm - Href) / np.linalg.norm(Href) <= 1e-12
+    assert np.linalg.norm(Om - Oref) / np.linalg.norm(Oref) <= 1e-12
+    H, Ov = O.hamiltonandoverlapsetup(s, gk, apwalm)
     N = gk.ngp
-    A = np.concatenate([O._apwi(s, apwalm, N, a) for a in range(s.natmtot)])
-    B = np.concatenate([s.mt_aa[:, :, a] @ O._apwi(s, apwalm, N, a) for a in range(s.natmtot)])
-    K = A.shape[0]
-    ps, cs, b, _ = plan(0, K, 8)
-    M = float(math.prod(ps))
-    ar, ai, sa = _split_scaled(A, b)
-    br, bi, sb = _split_scaled(B, b)
-    XA = np.concatenate([ar, ai])                   # [Ar; Ai]
-    YH = [np.concatenate([br, bi]), np.concatenate([bi, -br])]    # Re H, Im H
-    YO = [np.concatenate([ar, ai]), np.concatenate([ai, -ar])]    # Re O, Im O
-    scale = M * 2.0 ** (-64 - 2 * b)
-    for Ys, ref, sy in ((YH, A.conj().T @ B, sb), (YO, A.conj().T @ A, sa)):
-        parts = [emulate(XA, Y, ps, cs)[0].astype(np.float64) * scale for Y in Ys]
-        got = (parts[0] + 1j * parts[1]) * np.outer(sa, sy)
-        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-12
+    H2, O2 = H.copy(), Ov.copy()
+    H2[:N, :N] += Hm - Href
+    O2[:N, :N] += Om - Oref
+    w0 = sl.eigh(H, Ov, eigvals_only=True, subset_by_index=[0, 19])
+    w = sl.eigh(H2, O2, eigvals_only=True, subset_by_index=[0, 19])
+    assert np.abs(w - w0).max() <= 1e-8
 
 
 def test_split_residue_formula():
@@ -151,7 +207,7 @@ def test_split_residue_formula():
     + x1 (2^13 mod p) + x0 with integer partial sums below 2^24 (exact in FP32), q =
     round(v / p) as one FMA v * fl(1/p) + 1.5 2^23 rounded once to FP32, r = v - q p:
     r = x (mod p) and |r| <= 127 for |x| <= 2^52 and every modulus of the table."""
-    ps, _, _, _ = plan(16, 1000, 100)
+    ps = plan(16, 1000, 100)[0]
     rng = np.random.default_rng(7)
     xs = np.concatenate([rng.integers(-2 ** 52, 2 ** 52, size=20000, dtype=np.int64),
                          np.array([0, 1, -1, 2 ** 52, -2 ** 52, 2 ** 39 - 1, -2 ** 39, 2 ** 48 + 12345],
@@ -170,33 +226,43 @@ def test_split_residue_formula():
         assert np.all(np.mod(r - xs, p) == 0)
 
 
-def test_emulated_per_atom_product_meets_the_bar():
-    """B_a = h_a A_a as the per-atom kernel forms it: rows of h_a scaled to bx
-    bits (a power of two above each row's maximum), A to b bits by its column
-    maxima over all atoms, the same moduli; |X| <= 2 maxaa 2^(b + bx) < M / 2."""
+def test_emulated_eight_atom_eigenvalues():
+    """The 8-atom cell (K = 1936, O conditioned ~2.5e4, eigenvalues down to
+    about -1600 Ha), k-point 0: H/O products through the emulated integer
+    path of the default plan (13 moduli, 47 bits, 5 headroom bits), the
+    lowest 40 generalized eigenvalues within the absolute 1e-8 Ha of FP64.
+    With the constants at 2^64 and column-maximum scaling (no headroom) the
+    same emulation is 4.3e-8 Ha off: the recombination error, not the
+    operand bits, limits the eigenvalues."""
+    import scipy.linalg as sl
     import lapw_oracle as O
     from exciting_b200 import workloads as W
-    s = W.si_fcc("text")
-    gk = s.gkset(s.kpoints[3])
+    s = W.si_cube8()
+    gk = s.gkset(s.kpoints[0])
     apwalm, _ = O.match(s, gk)
+    H, Ov = O.hamiltonandoverlapsetup(s, gk, apwalm)
     N = gk.ngp
     apwi = [O._apwi(s, apwalm, N, a) for a in range(s.natmtot)]
     A = np.concatenate(apwi)
-    K, kx = A.shape[0], s.basis.maxaa
-    ps, cs, b, bx = plan(0, K, kx)
+    B = np.concatenate([s.mt_aa[:, :, a] @ apwi[a] for a in range(s.natmtot)])
+    ps, cs, b, _, h = plan(0, A.shape[0], s.basis.maxaa)
+    assert (len(ps), b, h) == (13, 47, 5)
     M = float(math.prod(ps))
-    _, _, sa = _split_scaled(A, b)
-    for a in range(s.natmtot):
-        h = s.mt_aa[:, :, a]
-        Aa = apwi[a]
-        ar, ai = np.rint(Aa.real / sa * 2.0 ** b), np.rint(Aa.imag / sa * 2.0 ** b)
-        hm = np.maximum(np.abs(h.real).max(1), np.abs(h.imag).max(1))
-        sx = np.ldexp(1.0, np.frexp(np.where(hm > 0, hm, 1.0))[1])
-        hr = np.rint(h.real / sx[:, None] * 2.0 ** bx).T           # (f', f)
-        hi = np.rint(h.imag / sx[:, None] * 2.0 ** bx).T
-        X = np.concatenate([hr, hi])
-        re = emulate(X, np.concatenate([ar, -ai]), ps, cs)[0].astype(np.float64)
-        im = emulate(X, np.concatenate([ai, ar]), ps, cs)[0].astype(np.float64)
-        got = (re + 1j * im) * (M * 2.0 ** (-64 - b - bx)) * np.outer(sx, sa)
-        ref = h @ Aa
-        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-13
+    ar, ai, sa = _split_scaled(A, b)
+    br, bi, sb = _split_scaled(B, b)
+    XA = np.concatenate([ar, ai])
+    scale = M * 2.0 ** (-64 - h - 2 * b)
+    got = []
+    for Ys, sy in (([np.concatenate([br, bi]), np.concatenate([bi, -br])], sb),
+                   ([np.concatenate([ar, ai]), np.concatenate([ai, -ar])], sa)):
+        parts = [emulate(XA, Y, ps, cs)[0].astype(np.float64) * scale for Y in Ys]
+        got.append((parts[0] + 1j * parts[1]) * np.outer(sa, sy))
+    Href, Oref = A.conj().T @ B, A.conj().T @ A
+    assert np.linalg.norm(got[0] - Href) / np.linalg.norm(Href) <= 1e-12
+    assert np.linalg.norm(got[1] - Oref) / np.linalg.norm(Oref) <= 1e-12
+    H2, O2 = H.copy(), Ov.copy()
+    H2[:N, :N] += got[0] - Href
+    O2[:N, :N] += got[1] - Oref
+    w0 = sl.eigh(H, Ov, eigvals_only=True, subset_by_index=[0, 39])
+    w = sl.eigh(H2, O2, eigvals_only=True, subset_by_index=[0, 39])
+    assert np.abs(w - w0).max() <= 1e-8

@@ -8,8 +8,11 @@ that keeps its work space in a static device array instead of allocating.
 Checked against the existing context entry point: on a system without local
 orbitals and with the interstitial tables set to zero, the APW-APW block of
 exs_hamiltonandoverlapsetup is exactly the muffin-tin sum this entry point
-computes.  Two calls in a row must both agree (the shared array keeps the
-previous call's contents).  Same tolerance as the other parity tests.
+computes.  Two checked calls must both agree (the shared array keeps the
+previous call's contents); between them a call with another layout (one
+atom, fewer G+k, so other offsets, padding and tile tables) runs and its
+outputs are discarded, and the second checked call runs on a non-default
+stream.  Same tolerance as the other parity tests.
 """
 import ctypes
 
@@ -64,14 +67,30 @@ def test_noalloc_matches_context_entry_point_twice():
     d_apwi = torch.from_numpy(np.ascontiguousarray(apwi.transpose(2, 1, 0)).view(np.float64)).to(dev)
     d_aa = torch.from_numpy(np.ascontiguousarray(s.mt_aa.transpose(2, 1, 0)).view(np.float64)).to(dev)
     lib = st.lib
+    side = torch.cuda.Stream(device=dev)
     for call in range(2):
+        if call == 1:
+            # another layout in between: atom 0 only, 100 G+k (the first 100 columns of its apwi)
+            n2 = 100
+            d_a2 = torch.from_numpy(np.ascontiguousarray(apwi[:, :n2, 0].T).view(np.float64)).to(dev)
+            d_h2 = torch.empty((n2, n2, 2), dtype=torch.float64, device=dev)
+            d_o2 = torch.empty_like(d_h2)
+            rc = lib.exs_mt_contract_noalloc(1, maxaa, napw.ctypes.data_as(ctypes.c_void_p), n2,
+                                             ctypes.c_void_p(d_a2.data_ptr()), ctypes.c_void_p(d_aa.data_ptr()),
+                                             ctypes.c_void_p(d_h2.data_ptr()), ctypes.c_void_p(d_o2.data_ptr()),
+                                             n2, None)
+            assert rc == 0
+            torch.cuda.synchronize()
         d_h = torch.full((ngp, ngp, 2), float("nan"), dtype=torch.float64, device=dev)
         d_o = torch.full((ngp, ngp, 2), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        stream = None if call == 0 else ctypes.c_void_p(side.cuda_stream)
         rc = lib.exs_mt_contract_noalloc(s.natmtot, maxaa, napw.ctypes.data_as(ctypes.c_void_p), ngp,
                                          ctypes.c_void_p(d_apwi.data_ptr()), ctypes.c_void_p(d_aa.data_ptr()),
                                          ctypes.c_void_p(d_h.data_ptr()), ctypes.c_void_p(d_o.data_ptr()),
-                                         ngp, None)
+                                         ngp, stream)
         assert rc == 0
+        side.synchronize()
         torch.cuda.synchronize()
         # device arrays are za(ld, ngp) column-major: [col][row][re/im]
         h = d_h.cpu().numpy().view(np.complex128)[..., 0].T
