@@ -20,11 +20,15 @@ All arrays follow the reference's Fortran layout when handed to the C-ABI
 ``ivg`` has shape (3, ngrtot) and ``vgpc`` (3, ngp).
 
 G-vector numbering: the reference sorts the box by |G| with a heapsort
-(src/sorting.f90 ``sort_index_1d``), which is not stable.  Here a stable sort
-is used, so G-vectors of exactly equal length may be numbered in a different
-order inside a shell.  Every count (``ngvec``, ``ngk``, ``nmat``) and every
-H/O element is independent of that order, because the same ``ivg``/``ivgig``
-pair is used consistently by all consumers.
+(src/sorting.f90 ``sort_index_1d``), which is not stable, so the order of
+G-vectors of equal length follows from the heapsort's steps and from the last
+bits of each computed length.  Both are reproduced: the lengths with the
+reference's operation order (``reciplat`` for bvec, then the same sums and
+square root, no fused multiply-add), the order with the library's
+``exs_sort_index_1d``, the heapsort of src/sorting.f90:74-117 step for step.
+``ivg``, ``ivgig``, ``igpig`` and with them the place of every H/O element
+are then the reference's (given a reference build without fused
+multiply-add contraction in gengvec).
 """
 from __future__ import annotations
 
@@ -51,9 +55,39 @@ def nfftifc(n: int) -> int:
         n += 1
 
 
+def reciplat(avec: np.ndarray):
+    """bvec and omega as src/reciplat.f90:33-53 computes them: b1 = a2 x a3,
+    b2 = a3 x a1, b3 = a1 x a2 (r3cross), t1 = a1 . b1, omega = |t1|, then
+    bvec = (twopi / t1) bvec, in the same floating-point order."""
+    a = [avec[:, j].astype(np.float64) for j in range(3)]
+
+    def cross(x, y):
+        return [x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]]
+
+    b = [cross(a[1], a[2]), cross(a[2], a[0]), cross(a[0], a[1])]
+    t1 = float(a[0][0] * b[0][0] + a[0][1] * b[0][1] + a[0][2] * b[0][2])
+    f = TWOPI / t1
+    bvec = np.array([[f * b[j][i] for j in range(3)] for i in range(3)], dtype=np.float64)
+    return bvec, abs(t1)
+
+
 def reciprocal(avec: np.ndarray) -> np.ndarray:
-    """Reciprocal lattice vectors bvec(:, j) with a_i . b_j = 2 pi delta_ij."""
-    return TWOPI * np.linalg.inv(avec).T
+    """Reciprocal lattice vectors bvec(:, j) with a_i . b_j = 2 pi delta_ij (reciplat)."""
+    return reciplat(avec)[0]
+
+
+def sort_index_1d(a: np.ndarray) -> np.ndarray:
+    """0-based index map sorting a ascending with the reference's heapsort
+    (src/sorting.f90:74-117; exs_sort_index_1d in the library)."""
+    import ctypes
+    from . import abi
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    idx = np.zeros(a.size, dtype=np.int32)
+    rc = abi.load().exs_sort_index_1d(a.size, a.ctypes.data_as(ctypes.c_void_p), 1,
+                                      idx.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise abi.ExsError(rc, "exs_sort_index_1d")
+    return idx.astype(np.int64) - 1
 
 
 def gridsize(avec: np.ndarray, gmaxvr: float):
@@ -104,8 +138,8 @@ def gengvec(avec: np.ndarray, gmaxvr: float) -> GVectors:
     i1 = i1.ravel(); i2 = i2.ravel(); i3 = i3.ravel()
     v = (i1[None, :] * bvec[:, 0:1] + i2[None, :] * bvec[:, 1:2]
          + i3[None, :] * bvec[:, 2:3])
-    gc = np.sqrt(v[0] ** 2 + v[1] ** 2 + v[2] ** 2)
-    idx = np.argsort(gc, kind="stable")
+    gc = np.sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    idx = sort_index_1d(gc)                     # gengvec.f90:74, the reference's heapsort
     gc = gc[idx]
     ivg = np.stack([i1[idx], i2[idx], i3[idx]]).astype(np.int32)
     ngrtot = ivg.shape[1]
@@ -223,8 +257,7 @@ class Crystal:
     def __post_init__(self):
         self.avec = np.asarray(self.avec, dtype=np.float64)
         self.atposl = np.asarray(self.atposl, dtype=np.float64)
-        self.bvec = reciprocal(self.avec)
-        self.omega = abs(float(np.linalg.det(self.avec)))
+        self.bvec, self.omega = reciplat(self.avec)
         self.atposc = self.avec @ self.atposl
 
     @property

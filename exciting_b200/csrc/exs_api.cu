@@ -1687,4 +1687,46 @@ int exs_hamiltonandoverlapsetup(exs_ctx *c, int ngp, const exs_complex *apwalm, 
     return exs_synchronize(c);
 }
 
+// sort_index_1d_real (src/sorting.f90:74-117): the heapsort's sift-down
+// with 1-based positions l (heap build) and k (extraction), comparing
+// a(inc (idx - 1) + 1) with strict "<" as the reference does.
+int exs_sort_index_1d(int n, const double *a, int inc, int *idx)
+{
+    if (n < 0 || (n > 0 && (!a || !idx)) || inc < 1) return EXS_ERR_ARG;
+    if (n == 0) return EXS_OK;
+    auto key = [&](int m) { return a[(size_t)inc * (m - 1)]; };
+    int *ix = idx - 1;                         // ix[1..n]
+    for (int i = 1; i <= n; i++) ix[i] = i;
+    if (n == 1) return EXS_OK;
+    int l = n / 2 + 1, k = n;
+    while (true) {
+        int m;
+        if (l > 1) {
+            l = l - 1;
+            m = ix[l];
+        } else {
+            m = ix[k];
+            ix[k] = ix[1];
+            k = k - 1;
+            if (k == 1) {
+                ix[1] = m;
+                break;
+            }
+        }
+        int i = l, j = l + l;
+        while (j <= k) {
+            if (j < k && key(ix[j]) < key(ix[j + 1])) j = j + 1;
+            if (key(m) < key(ix[j])) {
+                ix[i] = ix[j];
+                i = j;
+                j = j + j;
+            } else {
+                j = k + 1;
+            }
+        }
+        ix[i] = m;
+    }
+    return EXS_OK;
+}
+
 }  // extern "C"

@@ -396,6 +396,13 @@ int exs_adjoint(exs_ctx *ctx, int ngp, const int *igpig, const double *vgpc, int
                 const double *ffacg, const double *vgc, double *dtau,
                 exs_complex *dveffig, exs_complex *dh);
 
+/* Index map that sorts a(1 + inc*(i-1)), i = 1..n, ascending: the heapsort
+ * of sort_index_1d_real (src/sorting.f90:74-117) step for step, so that
+ * elements of equal value come out in the reference's order (the heapsort is
+ * not stable).  idx(n) receives 1-based indices.  Host only; used to number
+ * the G-vectors by length as gengvec does (src/gengvec.f90:73-74). */
+int exs_sort_index_1d(int n, const double *a, int inc, int *idx);
+
 /* Limit, in SM clock cycles, of every wait of the split-precision
  * kernels' pipelines (a producer on a free stage, the tensor core on a
  * filled one, the epilogue on finished products); 0 restores the default
