@@ -150,32 +150,47 @@ def split_scheme(args, sys_):
             "in the 64-bit recombination; tcgen05), Chinese-remainder recombination" % (n, b, h))
 
 
-def ozaki_int8_ops(sys_, gks, products):
-    """int8 MMA operations the split-precision kernel issues: per 128 x 32 tile
-    (B operand [Br|Bi|Ar|Ai] -> N = 128), `products` int8 products (S(S+1)/2
-    slice pairs, or one per modulus) x two A operands (Ar, Ai) x 2 x 128 x 128
-    x kp8 (K padded to 256)."""
+def ozaki_int8_ops(sys_, gks, products, cols=32):
+    """int8 MMA operations the split-precision H/O kernel issues: per 128 x
+    cols tile (B operand [Br|Bi|Ar|Ai] -> N = 4 cols), `products` int8
+    products (S(S+1)/2 slice pairs, or one per modulus) x two A operands
+    (Ar, Ai) x 2 x 128 x N x kp8 (K padded to 256)."""
     K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
     kp8 = (K + 255) // 256 * 256
-    pairs = products
     tiles = 0
     for g in gks:
         n = g.ngp
         for ib in range((n + 127) // 128):
-            for jb in range((n + 31) // 32):
-                if jb * 32 + 31 >= ib * 128:
+            for jb in range((n + cols - 1) // cols):
+                if jb * cols + cols - 1 >= ib * 128:
                     tiles += 1
-    return tiles * pairs * 2.0 * 128 * 128 * 2 * kp8
+    return tiles * products * 2.0 * 2 * 128 * (4 * cols) * kp8
 
 
-# DRAM bytes per k-point of the dominant kernel from one ncu capture of a
-# small case (traffic grows with the k-points: the operands are read once per
-# k-point and H/O written once), scaled to a launch by the k-points it covers:
-#   split precision: oz_mma_kernel<OZ_HO,2,2>, 2 k-points: 131.6 MB read +
-#     35.2 MB written with 7 slices (profiles/oz_mma_si_cube8_nk2.md), 227.2 MB
-#     read + 37.4 MB written with 13 moduli (profiles/oz_mma_mod_si_cube8_nk2.md);
-#   FP64: zgemm_dmma_kernel<1> + <2>, 6 k-points: 673.5 MB read + 143.1 MB
-#     written (profiles/zgemm_dmma_si_cube8_nk6.md).
+HO_KERNEL = {"ozaki_mod": "oz_res_kernel (residue tiles, tcgen05.mma kind::i8) + oz_crt_kernel (96-bit CRT), "
+                          "MT contraction phase",
+             "ozaki": "oz_mma_kernel (tcgen05.mma kind::i8, FP64 fold), MT contraction phase"}
+
+
+def ho_tile_cols(precision, kernel_config):
+    """Columns of the H/O tiles: 64 or 32 for the modular residue tiles
+    (configuration bit 0), 32 for the slice kernel."""
+    if precision == "ozaki_mod":
+        return 32 if (kernel_config & 1) else 64
+    return 32
+
+
+# DRAM bytes per k-point of the dominant kernel, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the 8-atom batch cut to a
+# few k-points; the traffic grows with the k-points (each k-point's operands
+# are read once and its H/O written once), so a launch's traffic is this
+# figure times its k-points:
+#   split precision, oz_mma_kernel<OZ_HO,2,2>, 2 k-points: 131.6 MB read +
+#     35.2 MB written with 7 slices, 227.2 MB read + 37.4 MB written with 13
+#     moduli;
+#   FP64, zgemm_dmma_kernel<1> + <2>, 6 k-points: 673.5 MB read + 143.1 MB written.
+# The figures are reported with the capture they come from; a kernel change
+# needs a new capture.
 PROFILED_DRAM_BYTES_PER_K = {"ozaki": (131.6e6 + 35.2e6) / 2, "fp64": (673.5e6 + 143.1e6) / 6,
                              "ozaki_mod": (227.2e6 + 37.4e6) / 2}
 
@@ -237,29 +252,52 @@ def cpu_sample(sys_, gks, budget_s=12.0):
 
 
 def run_reference(args):
+    """The CPU arm: the FP64 restatement of the path (the Fortran reference
+    has no compiler on either machine) on the host cores, on the same
+    workload, metric and unit as the GPU arm; each step a bounded sample of
+    one k-point, extrapolated to the whole k-point.  Rank 0 only."""
     ws, rank = _dist()
     if rank != 0:
         return 0
     from exciting_b200 import workloads as W
-    s = W.si_cube8()
-    gks = s.gksets()
-    for _ in range(args.warmup):
-        cpu_sample(s, gks, budget_s=1.0)
-    vals = []
-    for _ in range(args.steps):
-        v, n, dt = cpu_sample(s, gks, budget_s=6.0)
-        vals.append(v)
-    value = float(np.median(vals))
     cores = os.cpu_count()
+    if args.workload == "cube216":
+        s = W.si_cube216()
+        gks = s.gksets()
+        for i in range(args.warmup):
+            cpu_sample_216(s, gks[i % len(gks)], 1, 1000)
+        vals = []
+        for i in range(args.steps):
+            full, _ = cpu_sample_216(s, gks[i % len(gks)], 1, 1000)
+            vals.append(1.0 / full)
+        value = float(np.median(vals))
+        config = {"workload": WORKLOAD_216, "k_per_step": 1,
+                  "kpoints": "Gamma, (1/2,0,0), (1/2,1/2,0), (1/2,1/2,1/2) in turn, one per step"}
+        sample = ("per step one k-point in turn: match and the H and O zgemm pairs of 1 of 216 atoms plus "
+                  "hmlistln/olpistln over 1000 G+k by the FP64 CPU restatement (C + OpenBLAS zgemm), "
+                  "extrapolated linearly in atoms and by N(N+1) in G+k; the value is the median over steps; "
+                  "the Fortran reference has no compiler here")
+        ms = 1e3 / value
+    else:
+        s = W.si_cube8()
+        gks = s.gksets()
+        for _ in range(args.warmup):
+            cpu_sample(s, gks, budget_s=1.0)
+        vals = []
+        for _ in range(args.steps):
+            v, n, dt = cpu_sample(s, gks, budget_s=6.0)
+            vals.append(v)
+        value = float(np.median(vals))
+        config = {"workload": WORKLOAD, "k_per_step": 27}
+        sample = ("k-points of the 27-k set set up by the FP64 CPU restatement (C + OpenMP + OpenBLAS zgemm) "
+                  "until 6 s elapse, per step; the Fortran reference has no compiler here")
+        ms = 27.0 / value * 1e3
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 27.0 / value * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "k_per_step": 27},
-        "cpu_baseline": {"value": value, "unit": "setups/s", "cores": cores, "kind": "port",
-                         "sample": "k-points of the 27-k set set up by the FP64 CPU restatement (C + OpenMP + "
-                                   "OpenBLAS zgemm) until 6 s elapse, per step; the Fortran reference has no "
-                                   "compiler here"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "strong" if args.workload == "cube216" else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+        "cpu_baseline": {"value": value, "unit": "setups/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "setups/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -269,9 +307,10 @@ def run_reference(args):
 def launches_per_setup(precision):
     """Kernel launches of one batched setup call: match, (modular: the A column
     norms), the A split, the per-atom products, (modular: the B column norms),
-    the B split, the H/O tiles, the O APW-lo block and the lo-lo blocks; the
-    FP64 path: match, four grouped DMMA products, APW-lo and lo-lo."""
-    return 9 if precision == "ozaki_mod" else 7
+    the B split, the H/O tiles (modular: residue tiles, then their
+    recombination), the O APW-lo block and the lo-lo blocks; the FP64 path:
+    match, four grouped DMMA products, APW-lo and lo-lo."""
+    return 10 if precision == "ozaki_mod" else 7
 
 
 def _e2e(args, st, stream, ig, vg, ngp, nmat, ws, barrier, mode="auto", pinned=True):
@@ -681,10 +720,10 @@ def run_ours(args, emit=True):
         peak64 = _measured_fp64_peak(torch)
         achieved = fl / (main_ms * 1e-3) / 1e12
         if args.precision != "fp64":
-            ops = ozaki_int8_ops(s, gks, products)
+            ops = ozaki_int8_ops(s, gks, products, ho_tile_cols(args.precision, tuned))
             peak8 = _measured_int8_peak(torch)
             a8 = ops / (main_ms * 1e-3) / 1e12
-            roof = {"bound": "tensor", "kernel": "oz_mma_kernel (tcgen05.mma kind::i8, MT contraction)",
+            roof = {"bound": "tensor", "kernel": HO_KERNEL[args.precision],
                     "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                     "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
                     "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_PER_K[args.precision] * nk,
@@ -786,22 +825,29 @@ def _rel_fro_host(h, d, chunk=1 << 27):
     return (num / den) ** 0.5
 
 
-def _lowest_generalized(h, o, m, nev, torch):
+def _lowest_generalized(solver, h, o, m, nev, torch):
     """The lowest nev eigenvalues of H x = e O x for za(m, m) matrices held as
-    host tensors of 2 m^2 doubles (column-major, so the tensors read as the
-    transposes: conj(H), conj(O), which have the same eigenvalues), by a
-    Cholesky reduction and a dense Hermitian eigen-solve on the device
-    (cuSOLVER, through torch)."""
-    H = h.cuda().view(torch.complex128).view(m, m)
-    L = torch.linalg.cholesky(o.cuda().view(torch.complex128).view(m, m))
-    X = torch.linalg.solve_triangular(L, H, upper=False)               # L^-1 H
-    del H
-    C = torch.linalg.solve_triangular(L, X.mH.contiguous(), upper=False)   # L^-1 H L^-H
-    del X, L
-    w = torch.linalg.eigvalsh(C)[:nev].cpu().numpy()
-    del C
+    host tensors of 2 m^2 doubles, by the library's device eigen-solve
+    (exs_solve_batched_device: cuSOLVER zhegvdx, index range 1..nev) on a
+    context `solver` that only lends its solver handles."""
+    import ctypes
+    H, O_ = h.cuda(), o.cuda()
+    ev = torch.zeros(nev, dtype=torch.float64, device="cuda")
+    vec = torch.zeros(2 * m * nev, dtype=torch.float64, device="cuda")
+    nmat = (ctypes.c_int * 1)(m)
+    hp = (ctypes.c_void_p * 1)(H.data_ptr())
+    op = (ctypes.c_void_p * 1)(O_.data_ptr())
+    vp = (ctypes.c_void_p * 1)(vec.data_ptr())
+    solver._check(solver.lib.exs_solve_batched_device(solver.ctx, 1, nmat, hp, op, nev,
+                                                      ctypes.c_void_p(ev.data_ptr()), vp, m))
+    w = ev.cpu().numpy()
+    del H, O_, vec
     torch.cuda.empty_cache()
     return w
+
+
+def _progress(msg):
+    print("[bench] %s" % msg, file=sys.stderr, flush=True)
 
 
 def adjoint_recipe(nmat, seed=3, nst=40):
@@ -897,6 +943,29 @@ def cpu_sample_216(sys_, gk, m_atoms=1, n_sub=3000):
     return full, time.perf_counter() - t0
 
 
+def e2e_large(st, gks, nlotot, mmax, torch, ne=2):
+    """Setups/s through exs_setup_batched, one k-point per call: igpig/vgpc in
+    from the host, H and O (13.6 GB each) back into pinned host memory."""
+    hp = torch.empty(2 * mmax * mmax, dtype=torch.float64, pin_memory=True)
+    op = torch.empty_like(hp, pin_memory=True)
+
+    def views(g):     # za(nmat, nmat) of this k-point at the start of the pinned buffers
+        m = g.ngp + nlotot
+        return [(hp.numpy()[: 2 * m * m].view(np.complex128).reshape(m, m, order="F"),
+                 op.numpy()[: 2 * m * m].view(np.complex128).reshape(m, m, order="F"))]
+    st.setup_batched([gks[0]], out=views(gks[0]))          # warm-up
+    t0 = time.perf_counter()
+    for i in range(ne):
+        g = gks[i % len(gks)]
+        st.setup_batched([g], out=views(g))
+    dt = time.perf_counter() - t0
+    m0 = gks[0].ngp + nlotot
+    return {"value": ne / dt, "unit": "setups/s", "h2d_bytes_per_step": int(gks[0].ngp * 16),
+            "d2h_bytes_per_step": int(2 * 16 * m0 * m0), "host_copy_mode": "auto (pinned outputs)",
+            "steps": ne, "note": "exs_setup_batched, one k-point per call: igpig/vgpc in, H and O (13.6 GB "
+                                 "each) to pinned host memory; wall clock"}
+
+
 def run_large(args):
     """The 216-atom cell, the north-star workload: one k-point per step (H and
     O are ~13.6 GB each), Gamma and the three other k-points in turn.  Timed:
@@ -908,7 +977,6 @@ def run_large(args):
     import torch.distributed as dist
     from exciting_b200 import workloads as W
     from exciting_b200.fvsystem import Setup
-    from exciting_b200.kdist import my_kpoints
 
     ws, rank = _dist()
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -918,7 +986,9 @@ def run_large(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     s = W.si_cube216()
     gks_all = s.gksets()[: min(args.nk, 4)]
-    gks = [gks_all[i] for i in my_kpoints(rank, len(gks_all), ws)] if ws > 1 else gks_all
+    # every rank sets up one k-point per step, starting at its own k-point (weak scaling)
+    r0 = rank % len(gks_all)
+    gks = gks_all[r0:] + gks_all[:r0]
     st = Setup(s, ngkmax=max(g.ngp for g in gks_all), max_batch=1)
     stream = torch.cuda.Stream()
     st.set_stream(stream.cuda_stream)
@@ -976,6 +1046,7 @@ def run_large(args):
     planes, products, dtype_text, prec_text = split_scheme(args, s)
     ms, phase, rows = timed(args.steps, args.warmup, True)
     value = ws * args.steps / (ms * 1e-3)
+    _progress("split: %.4f setups/s, phases %s" % (value, list(np.round(phase, 2))))
     # ---- Gamma in split precision, kept on the host for the comparison
     m0 = gks[0].ngp + nlotot
     one(0)
@@ -986,6 +1057,7 @@ def run_large(args):
     st.set_precision("fp64")
     ms64, phase64, _ = timed(nf, 1, False)
     fp64_value = ws * nf / (ms64 * 1e-3)
+    _progress("fp64: %.4f setups/s, phases %s" % (fp64_value, list(np.round(phase64, 2))))
     one(0)
     st.synchronize()
     acc = {"against": "native FP64 GPU path, Gamma, whole H and O",
@@ -994,30 +1066,23 @@ def run_large(args):
     del d_h, d_o
     torch.cuda.empty_cache()
     # ---- end to end through the host-pointer entry point (pinned H and O, 13.6 GB each per k-point)
+    _progress("accuracy: %s" % json.dumps(acc))
     e2e = None
     if not args.skip_e2e and rank == 0:
-        st.set_precision(prec, args.slices if prec == "ozaki" else args.moduli)
-        hp = torch.empty(2 * mmax * mmax, dtype=torch.float64, pin_memory=True)
-        op = torch.empty_like(hp, pin_memory=True)
-
-        def views(g):     # za(nmat, nmat) of this k-point at the start of the pinned buffers
-            m = g.ngp + nlotot
-            return [(hp.numpy()[: 2 * m * m].view(np.complex128).reshape(m, m, order="F"),
-                     op.numpy()[: 2 * m * m].view(np.complex128).reshape(m, m, order="F"))]
-        ne = 2
-        st.setup_batched([gks[0]], out=views(gks[0]))          # warm-up
-        t0 = time.perf_counter()
-        for i in range(ne):
-            g = gks[i % len(gks)]
-            st.setup_batched([g], out=views(g))
-        dt = time.perf_counter() - t0
-        e2e = {"value": ne / dt, "unit": "setups/s", "h2d_bytes_per_step": int(gks[0].ngp * 16),
-               "d2h_bytes_per_step": int(2 * 16 * m0 * m0), "host_copy_mode": "auto (pinned outputs)",
-               "steps": ne, "note": "exs_setup_batched, one k-point per call: igpig/vgpc in, H and O (13.6 GB "
-                                    "each) to pinned host memory; wall clock"}
-        del hp, op
+        try:
+            st.set_precision(prec, args.slices if prec == "ozaki" else args.moduli)
+            e2e = e2e_large(st, gks, nlotot, mmax, torch)
+        except Exception as e:      # reported, not fatal
+            e2e = {"error": str(e)[:300]}
+        _progress("e2e: %s" % json.dumps(e2e))
     # ---- the adjoint at Gamma (FP64 in either mode)
-    adj = None if args.skip_adjoint else adjoint_leg(st, s, gks[0], torch)
+    adj = None
+    if not args.skip_adjoint:
+        try:
+            adj = adjoint_leg(st, s, gks[0], torch)
+        except Exception as e:      # reported, not fatal
+            adj = {"error": str(e)[:300]}
+        _progress("adjoint: %s" % json.dumps(adj))
     clocks = _clock_summary(rows, local)
     st.set_stream(None)
     st.close()
@@ -1025,18 +1090,24 @@ def run_large(args):
     # ---- eigenvalues of both Gamma pairs
     if not args.skip_eig and rank == 0:
         t0 = time.perf_counter()
-        w8 = _lowest_generalized(h8, o8, m0, 40, torch)
-        w64 = _lowest_generalized(h64, o64, m0, 40, torch)
-        acc.update({"eigen_solver": "Cholesky reduction + dense eigen-solve on the device (torch / cuSOLVER), "
-                                    "lowest 40 of each path", "eig_solve_s": time.perf_counter() - t0,
-                    "max_abs_eig_dev_lowest40_Ha": float(np.max(np.abs(w8 - w64))),
-                    "lowest_eigenvalue_Ha": float(w64[0]),
-                    "gate_abs_1e-8_Ha": bool(np.max(np.abs(w8 - w64)) <= 1e-8)})
+        try:
+            solver = Setup(W.si_fcc("text"))
+            w8 = _lowest_generalized(solver, h8, o8, m0, 40, torch)
+            w64 = _lowest_generalized(solver, h64, o64, m0, 40, torch)
+            solver.close()
+            acc.update({"eigen_solver": "exs_solve_batched_device (cuSOLVER zhegvdx, lowest 40) on each path's "
+                                        "H and O", "eig_solve_s": time.perf_counter() - t0,
+                        "max_abs_eig_dev_lowest40_Ha": float(np.max(np.abs(w8 - w64))),
+                        "lowest_eigenvalue_Ha": float(w64[0]),
+                        "gate_abs_1e-8_Ha": bool(np.max(np.abs(w8 - w64)) <= 1e-8)})
+        except Exception as e:      # reported, not fatal: the timing legs stand
+            acc.update({"eigen_solver_error": str(e)[:300]})
+        _progress("eigenvalues: %s" % json.dumps({k: v for k, v in acc.items() if "eig" in k}))
     del h8, o8, h64, o64
     if ws > 1:
         dist.barrier()
     if rank == 0:
-        ops = ozaki_int8_ops(s, gks_all, products) / len(gks_all)      # per k-point (one per step)
+        ops = ozaki_int8_ops(s, gks_all, products, ho_tile_cols(prec, 0)) / len(gks_all)   # per k-point
         fl = main_flops(s, gks_all) / len(gks_all)
         peak8 = _measured_int8_peak(torch)
         peak64 = _measured_fp64_peak(torch)
@@ -1044,21 +1115,29 @@ def run_large(args):
         a8 = ops / (mt_ms * 1e-3) / 1e12
         cpu = None
         if not args.skip_cpu:
-            cpu_sample_216(s, gks_all[0], 1, 1000)                          # warm-up (libraries, pages)
-            full, dt = cpu_sample_216(s, gks_all[0], 2, 3000)
-            cpu = {"value": 1.0 / full, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": "Gamma: match and the H and O zgemm pairs of 2 of 216 atoms plus hmlistln/olpistln "
-                             "over 3000 of %d G+k by the FP64 CPU restatement (C + OpenBLAS zgemm, %.1f s), "
-                             "extrapolated linearly in atoms and by N(N+1) in G+k" % (gks_all[0].ngp, dt)}
+            try:
+                cpu_sample_216(s, gks_all[0], 1, 1000)                      # warm-up (libraries, pages)
+                full, dt = cpu_sample_216(s, gks_all[0], 2, 3000)
+                cpu = {"value": 1.0 / full, "unit": "setups/s", "cores": os.cpu_count(), "kind": "port",
+                       "sample": "Gamma: match and the H and O zgemm pairs of 2 of 216 atoms plus "
+                                 "hmlistln/olpistln over 3000 of %d G+k by the FP64 CPU restatement (C + "
+                                 "OpenBLAS zgemm, %.1f s), extrapolated linearly in atoms and by N(N+1) in G+k"
+                                 % (gks_all[0].ngp, dt)}
+            except Exception as e:      # reported, not fatal
+                cpu = {"error": str(e)[:300]}
+            _progress("cpu: %s" % json.dumps(cpu))
         sub = None
         if not args.skip_cube8 and ws == 1:
-            sub = run_ours(argparse.Namespace(**{**vars(args), "steps": 10, "warmup": 3, "nk": 27, "skip_cpu": True,
-                                                 "skip_hmlint": True, "skip_rttddft": True, "skip_e2e": True,
-                                                 "e2e_modes": False}), emit=False)
+            try:
+                sub = run_ours(argparse.Namespace(**{**vars(args), "steps": 10, "warmup": 3, "nk": 27,
+                                                     "skip_cpu": True, "skip_hmlint": True, "skip_rttddft": True,
+                                                     "skip_e2e": True, "e2e_modes": False}), emit=False)
+            except Exception as e:      # reported, not fatal
+                sub = {"error": str(e)[:300]}
         out = {
             "metric": METRIC, "value": value, "unit": "setups/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": dtype_text,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype_text,
             "data": "synthetic",
             "config": {"workload": WORKLOAD_216, "k_per_step": 1,
                        "kpoints": "Gamma, (1/2,0,0), (1/2,1/2,0), (1/2,1/2,1/2) in turn, one per step",
@@ -1070,7 +1149,7 @@ def run_large(args):
             "e2e": e2e,
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
-            "roofline": {"bound": "tensor", "kernel": "oz_mma_kernel<OZ_HO> (tcgen05.mma kind::i8, MT contraction)",
+            "roofline": {"bound": "tensor", "kernel": HO_KERNEL[prec],
                          "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                          "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
                          "int8_ops_per_step": ops, "traffic": None,

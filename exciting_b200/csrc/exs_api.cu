@@ -154,6 +154,7 @@ int exs_ctx_destroy(exs_ctx *c)
     for (void *p : dev)
         if (p) cudaFree(p);
     if (c->d_oz) cudaFree(c->d_oz);
+    if (c->d_res) cudaFree(c->d_res);
     if (c->d_ozscale) cudaFree(c->d_ozscale);
     if (c->d_xs) cudaFree(c->d_xs);
     if (c->d_xsig) cudaFree(c->d_xsig);
@@ -395,6 +396,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     EXS_CUDA(cudaStreamSynchronize(c->stream));
     const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8);
     if (c->d_oz) { cudaFree(c->d_oz); c->d_oz = nullptr; }
+    if (c->d_res) { cudaFree(c->d_res); c->d_res = nullptr; c->res_bytes = 0; }
     if (c->d_ozscale) { cudaFree(c->d_ozscale); c->d_ozscale = nullptr; }
     if (c->d_xs) { cudaFree(c->d_xs); c->d_xs = nullptr; }
     if (c->d_xsig) { cudaFree(c->d_xsig); c->d_xsig = nullptr; }
@@ -407,7 +409,23 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     c->oz_xseg = mode == EXS_PREC_OZAKI_MOD ? 1 : exs::oz_seg_pairs(slices, c->oz_lw);
     sch.segx = c->oz_xseg;
     const size_t xgroups = (size_t)c->natmtot * slices * c->oz_nxb;
+    // moduli: the residue tiles of the H/O products of a whole batch, for
+    // either tile width (the upper tiles of ngkmax G+k per k-point)
+    size_t res = 0;
+    if (mode == EXS_PREC_OZAKI_MOD)
+        for (int q = 0; q < 2; q++) {
+            const int bj = exs::oz_res_cols(q);
+            size_t tiles = 0;
+            for (int ib = 0; ib < (c->ngkmax + 127) / 128; ib++)
+                for (int jb = 0; jb < (c->ngkmax + bj - 1) / bj; jb++)
+                    if (jb * bj + bj - 1 >= ib * 128) tiles++;
+            res = std::max(res, tiles * exs::oz_res_tile_bytes(slices, q) * c->max_batch);
+        }
     cudaError_t e = cudaMalloc((void **)&c->d_oz, slot * c->max_batch);
+    if (e == cudaSuccess && res > 0) {
+        e = cudaMalloc((void **)&c->d_res, res);
+        if (e == cudaSuccess) c->res_bytes = res;
+    }
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 2 * c->npad * c->max_batch);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xs, xgroups * 128 * c->oz_lw);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xsig, sizeof(double) * c->natmtot * c->oz_nxb * 64);
@@ -426,6 +444,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
                                                       &c->oz_mapB[q], &c->oz_mapB2[q]);
     maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, nss, c->npad, kp8, c->d_xs, xgroups, c->oz_lw,
                                                 &c->oz_mapArow, &c->oz_mapX);
+    maps_ok = maps_ok && exs::make_oz_b64_map(c->d_oz, nss, c->npad, kp8, &c->oz_mapB64);
     if (!maps_ok) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
@@ -641,16 +660,17 @@ struct Uploaded {
     int nozatiles;
 };
 
-// Upper tiles (128 rows x 32 columns, or 256 x 32 for the two-SM tiles with
-// ib counting pairs of 128-row blocks) of the split-precision contraction.
-void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows)
+// Upper tiles (128 rows x 32 columns, 256 x 32 for the two-SM tiles with ib
+// counting pairs of 128-row blocks, 128 x 32 or 128 x 64 for the residue
+// tiles of the modular mode) of the split-precision contraction.
+void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows, int cols)
 {
     t.clear();
     for (size_t k = 0; k < ks.size(); k++) {
         const int n = ks[k].ngp;
         for (int ib = 0; ib < (n + rows - 1) / rows; ib++)
-            for (int jb = 0; jb < (n + 31) / 32; jb++)
-                if (jb * 32 + 31 >= ib * rows) { t.push_back((int)k); t.push_back(ib); t.push_back(jb); }
+            for (int jb = 0; jb < (n + cols - 1) / cols; jb++)
+                if (jb * cols + cols - 1 >= ib * rows) { t.push_back((int)k); t.push_back(ib); t.push_back(jb); }
     }
 }
 
@@ -685,7 +705,10 @@ void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt
     ozt.clear();
     std::vector<int> ozat;
     if (c->oz_on()) {
-        oz_tiles(ks, ozt, (c->oz_cfg & 8) ? 256 : 128);
+        if (c->oz_sch.mod)
+            oz_tiles(ks, ozt, 128, exs::oz_res_cols(c->oz_cfg));
+        else
+            oz_tiles(ks, ozt, (c->oz_cfg & 8) ? 256 : 128, 32);
         oz_atom_tiles(c, ks, ozat);
     }
     L.noz = (int)(ozt.size() / 3);
@@ -836,8 +859,12 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
         if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 1, s));
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 0, s));
         const int q = c->oz_cfg;
-        EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,
-                                    u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, s));
+        if (c->oz_sch.mod)   // residue tiles (one K chunk per stage: the maps of configuration 1), then the CRT
+            EXS_CUDA(exs::launch_oz_res(q, &c->oz_mapA[1], &c->oz_mapB[1], &c->oz_mapB64, p, u.d_k, u.d_oztiles,
+                                        u.noztiles, c->oz_sch, c->kp8, c->d_res, s));
+        else
+            EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,
+                                        u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, s));
     } else {
         EXS_CUDA(exs::launch_gemm_kind(exs::EPI_HAM, p, u.d_probs[exs::EPI_HAM], u.d_work[exs::EPI_HAM],
                                        u.nwork[exs::EPI_HAM], u.d_k, s));
@@ -946,6 +973,7 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
     int best_q = 0;
     for (int q = 0; q < exs::OZ_NCFG; q++) {
         if ((q & 8) && (q & 2)) continue;   // the two-SM tiles have no persistent form
+        if ((q & 8) && c->oz_sch.mod) continue;   // moduli: residue tiles, no two-SM form
         if ((q & 16) && (q & 4)) continue;  // no per-atom int8 kernel to make persistent
         c->oz_cfg = q;
         Uploaded u{};                        // the tile list depends on the configuration

@@ -66,14 +66,19 @@ static_assert(OZ_NCFG == EXS_OZ_NCONFIG, "public configuration count");
 //     its 2-norm and rounded to integers (b bits: the scaled column has norm
 //     <= 2^b; bx for the h_a / loa rows, scaled by their row norms), stored
 //     as residues modulo n pairwise coprime odd moduli p[m] (int8 in
-//     [-127, 127]); one int8 product per modulus, each folded into a 64-bit
-//     sum t += (v mod p[m]) c[m] (mod 2^64) with c[m] = round(2^(64+h) y_m /
-//     p[m]) mod 2^64, so that t / 2^64 = 2^h X / M (mod 1) for the integer
-//     product X; by the Cauchy-Schwarz inequality |X| <= 2^(2b) (1 + eps)^2 and
-//     2^(2b + h + 2) <= M, so 2^h |X| / M < 1/2 and t read as a signed integer
-//     is exact but for the rounding of the constants; the value is t times fin
-//     (H/O) or finx (per-atom).  The h headroom bits divide that rounding
-//     error by 2^h.
+//     [-127, 127]); one int8 product per modulus.  By the Cauchy-Schwarz
+//     inequality an H/O product obeys |X| <= 2^(2b) (1 + eps)^2 with
+//     2^(2b + 2) <= M, and its residues are recombined by 96-bit constants
+//     c96 (residue tiles, oz_res_kernel / oz_crt_kernel): exact but for
+//     2^-64 M.  A per-atom product (|X| <= 2^(b + bx) (1 + eps)^2) is folded in
+//     the kernel into a 64-bit sum t += (v mod p[m]) c[m] (mod 2^64) with
+//     c[m] = round(2^(64+h) y_m / p[m]) mod 2^64 and 2^(b + bx + h + 2) <= M,
+//     so that t / 2^64 = 2^h X / M (mod 1) and t read as a signed integer is
+//     exact but for the rounding of the constants (sum |r| / 2 units of
+//     2^-(64+h) M; the h >= 5 headroom bits divide it by 2^h); the value is t
+//     times finx.  fin is the same factor for the H/O products folded in the
+//     64-bit form (2^(2b + h + 2) <= M does not hold for the plan's b: only
+//     the per-atom products use the fold).
 constexpr int OZ_MAX_MODULI = 16;
 struct OzScheme {
     int mod, n, seg, segx, b, bx, h;
@@ -84,6 +89,10 @@ struct OzScheme {
     float fp[OZ_MAX_MODULI], finv[OZ_MAX_MODULI];  // p and 1/p in FP32 (the split kernels)
     float fc[3][OZ_MAX_MODULI];        // 2^13, 2^26, 2^39 mod p
     unsigned long long c[OZ_MAX_MODULI];
+    // the H/O products (residue tiles): C_m = round(2^96 y_m / p_m) in 32-bit
+    // words (low first), recombined exactly but for 2^-64 M; fin96 = M 2^-64 2^-2b
+    unsigned c96[3][OZ_MAX_MODULI];
+    double fin96;
 };
 
 // atomicMax for non-negative doubles: their IEEE bit patterns order like
@@ -278,6 +287,9 @@ struct exs_ctx {
     size_t oz_slot_bytes = 0;
     CUtensorMap oz_mapA[exs::OZ_NCFG], oz_mapB[exs::OZ_NCFG];   // TMA views of d_oz per pipeline configuration
     CUtensorMap oz_mapB2[exs::OZ_NCFG];                            // half-B views (two-SM tiles)
+    CUtensorMap oz_mapB64;                                         // B operand of the 128 x 64 residue tiles
+    uint8_t *d_res = nullptr;                                      // residue tiles of the modular H/O products
+    size_t res_bytes = 0;
     int oz_cfg = 0;                   // pipeline configuration of the split-precision kernel
     // per-atom products of the split-precision path (h_a A, loa A)
     int8_t *d_xs = nullptr;           // slices of h_a and loa
@@ -335,6 +347,12 @@ cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const 
                             cudaStream_t s);
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s);
 cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, cudaStream_t s);
+cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
+                          const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch,
+                          int kp8, uint8_t *res, cudaStream_t s);
+int oz_res_cols(int cfg);
+size_t oz_res_tile_bytes(int n, int cfg);
+bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, CUtensorMap *mapB64);
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
                            const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s);

@@ -1303,6 +1303,323 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
     }
 }
 
+// ------------------------------------------------------------ residue tiles (modular H/O)
+// The modular H/O contraction in two kernels.  oz_res_kernel forms, per
+// 128 (G_i) x BJ (G_j) tile and per modulus, the int32 products
+// r = Ar^T [Br|Bi|Ar|Ai] and i = Ai^T [Br|Bi|Ar|Ai] (MMA N = 4 BJ) and writes
+// the residues x = v mod p in [0, p) of the four values
+// v = Re H (r0 + i1), Im H (r1 - i0), Re O (r2 + i3), Im O (r3 - i2) as bytes.
+// oz_crt_kernel recombines the n residues of each value by the Chinese
+// remainder theorem with 96-bit constants (exact but for 2^-64 M; no
+// headroom bits needed), scales by sigma_A(i) sigma_B(j) (sigma_A(j) for O),
+// adds the interstitial term and writes the upper triangle and its mirror.
+// With no running sums in tensor memory the tile is 128 x 64 (N = 256: r and
+// i fill the 512 columns) or 128 x 32 with two accumulator pairs, so that
+// the MMAs of one modulus run while the epilogue reduces the previous one.
+//
+// Residues of a tile (n * 4 * 128 * BJ bytes): [modulus g][value o]
+// [16-column chunk][row 0..127][16 bytes]: an epilogue warp (32 rows) stores
+// 512 contiguous bytes, a thread of oz_crt_kernel reads 8 of the 16 bytes of
+// one vector per (g, o).
+template <int BJ>
+struct ResCfg {
+    static constexpr int N = 4 * BJ;                     // MMA N
+    static constexpr int NACC = BJ == 32 ? 2 : 1;        // accumulator pairs (r, i) in tensor memory
+    static constexpr int ABOX = 2 * OZ_TILE;             // Ar, Ai of 128 G rows, one K chunk
+    static constexpr int BBOX = 4 * BJ * OZ_CHUNK;       // four arrays of BJ G rows, one K chunk
+    static constexpr int STAGE = ABOX + BBOX;
+    static constexpr int NST = (192 * 1024) / STAGE;     // 4 stages (BJ 32) or 3 (BJ 64)
+    static constexpr int NCH = BJ / 16;                  // 16-column chunks of a value block
+    static constexpr int MOD_BYTES = 4 * 128 * BJ;       // residues of one modulus of a tile
+    static constexpr int SMEM = NST * STAGE + 1024;
+};
+
+__device__ __forceinline__ uint32_t oz_res4(const uint32_t (&rv)[16], const uint32_t (&iv)[16], int e0, bool minus,
+                                            int pm, int mg)
+{
+    uint32_t w = 0;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int v = minus ? (int)rv[e0 + e] - (int)iv[e0 + e] : (int)rv[e0 + e] + (int)iv[e0 + e];
+        int x = v - __mulhi(v, mg) * pm;          // in [-p/4, 5p/4]
+        x += x < 0 ? pm : 0;
+        x -= x >= pm ? pm : 0;                    // in [0, p)
+        w |= (uint32_t)x << (8 * e);
+    }
+    return w;
+}
+
+template <int BJ>
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+oz_res_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, DevParams p,
+              const KDesc *ks, const int *tiles, int ntiles, const __grid_constant__ OzScheme sch, int kp8,
+              uint8_t *res)
+{
+    using C = ResCfg<BJ>;
+    constexpr int NST = C::NST, NACC = C::NACC, N = C::N;
+    const int S = sch.n;
+    const int nch = kp8 / OZ_CHUNK;
+    extern __shared__ __align__(1024) uint8_t oz_smem[];
+    __shared__ uint64_t full[NST], empty[NST], accf[NACC], acce[NACC];
+    __shared__ uint32_t tmem_sh;
+    __shared__ int abort_sh;
+    volatile int *abort = &abort_sh;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
+
+    if (warp == 3) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(OZ_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int q = 0; q < NST; q++) {
+            mbar_init(&full[q], 2);
+            mbar_init(&empty[q], 1);
+        }
+        for (int a = 0; a < NACC; a++) {
+            mbar_init(&accf[a], 1);
+            mbar_init(&acce[a], 8);              // the eight epilogue warps
+        }
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = tmem_sh;
+
+    if (warp < 3) {
+        // ------------------------------------------------ TMA producers: warp 0 the A box, warp 1 the B box
+        if (lane == 0 && warp < 2) {
+            const int role = warp;
+            uint32_t fills[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) fills[q] = 0;
+            int st = 0;
+            bool bad = false;
+            for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
+                const int slot = ks[tiles[3 * tile]].oz_slot;
+                const int i0 = tiles[3 * tile + 1] * OZ_BM, j0 = tiles[3 * tile + 2] * BJ;
+                for (int g = 0; g < S && !bad; g++)
+                    for (int kb = 0; kb < nch; kb++) {
+                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
+                            bad = true;
+                            break;
+                        }
+                        mbar_expect_tx(&full[st], role == 0 ? C::ABOX : C::BBOX);
+                        const uint32_t dst = sbase + st * C::STAGE + (role == 0 ? 0 : C::ABOX);
+                        if (role == 0)          // Ar and Ai (arrays 2, 3) of G rows i0 .. i0+127, modulus g
+                            tma_load_5d(dst, &mapA, 0, i0, 2, kb, slot * S + g, &full[st]);
+                        else                    // the four arrays of G rows j0 .. j0+BJ-1
+                            tma_load_5d(dst, &mapB, 0, j0, 0, kb, slot * S + g, &full[st]);
+                        fills[st]++;
+                        st = (st + 1 == NST) ? 0 : st + 1;
+                    }
+            }
+            if (bad)   // copies already issued must land before the CTA goes away
+                for (int q = 0; q < NST; q++)
+                    if (fills[q] > 0) mbar_drain(&full[q], (fills[q] - 1) & 1);
+        }
+    } else if (warp == 3) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_i8(128, N);
+            uint32_t uses[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) uses[q] = 0;
+            int st = 0, u = 0;
+            bool bad = false;
+            for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x)
+                for (int g = 0; g < S && !bad; g++, u++) {
+                    const int buf = u % NACC, use = u / NACC;
+                    // the epilogue must have read this accumulator pair's previous modulus
+                    if (use > 0 && !mbar_wait_ab(&acce[buf], (use - 1) & 1, abort, sch.wait)) {
+                        bad = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t tacc = tbase + (uint32_t)(buf * 2 * N);
+                    for (int kb = 0; kb < nch; kb++) {
+                        if (!mbar_wait_ab(&full[st], uses[st] & 1, abort, sch.wait)) {
+                            bad = true;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sa = sbase + st * C::STAGE;
+#pragma unroll
+                        for (int q = 0; q < OZ_CHUNK / 32; q++) {
+                            const uint64_t bd = umma_desc_sw128(sa + C::ABOX + q * 32);
+                            const uint32_t acc = (kb == 0 && q == 0) ? 0u : 1u;
+                            umma_i8(tacc, umma_desc_sw128(sa + q * 32), bd, idesc, acc);
+                            umma_i8(tacc + N, umma_desc_sw128(sa + OZ_TILE + q * 32), bd, idesc, acc);
+                        }
+                        umma_commit(&empty[st]);
+                        uses[st]++;
+                        st = (st + 1 == NST) ? 0 : st + 1;
+                    }
+                    if (!bad) umma_commit(&accf[buf]);
+                }
+            if (bad)   // MMAs already issued must finish before tensor memory is freed
+                for (int q = 0; q < NST; q++)
+                    if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
+        }
+    } else {
+        // ------------------------------------------------ epilogue (warps 4..11): residues of two value blocks
+        const int qd = warp & 3;                                    // tensor-memory lane quadrant
+        const int half = (warp - 4) >> 2;                           // 0: Re H, Im H; 1: Re O, Im O
+        const int row = qd * 32 + lane;
+        const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
+        int u = 0;
+        bool bad = false;
+        for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
+            uint8_t *tres = res + (size_t)tile * S * C::MOD_BYTES;
+            for (int g = 0; g < S; g++, u++) {
+                const int buf = u % NACC, use = u / NACC;
+                if (!__all_sync(0xffffffffu, mbar_wait_ab(&accf[buf], use & 1, abort, sch.wait))) {
+                    bad = true;
+                    break;
+                }
+                tc_fence_after();
+                const int pm = sch.p[g], mg = sch.mg[g];
+                const uint32_t tacc = t_lane + (uint32_t)(buf * 2 * N);
+                uint4 out[2][C::NCH];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int o = 2 * half + k, oi = o ^ 1;
+                    const bool minus = (o & 1) != 0;
+#pragma unroll
+                    for (int c = 0; c < C::NCH; c++) {
+                        uint32_t rv[16], iv[16];
+                        tm_ld16(tacc + o * BJ + c * 16, rv);
+                        tm_ld16(tacc + N + oi * BJ + c * 16, iv);
+                        tm_wait_ld();
+                        out[k][c] = make_uint4(oz_res4(rv, iv, 0, minus, pm, mg), oz_res4(rv, iv, 4, minus, pm, mg),
+                                               oz_res4(rv, iv, 8, minus, pm, mg), oz_res4(rv, iv, 12, minus, pm, mg));
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[buf]);             // the accumulator pair is free
+                uint8_t *gres = tres + (size_t)g * C::MOD_BYTES;
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+#pragma unroll
+                    for (int c = 0; c < C::NCH; c++)
+                        *reinterpret_cast<uint4 *>(gres + ((size_t)((2 * half + k) * C::NCH + c) * 128 + row) * 16) =
+                            out[k][c];
+            }
+        }
+    }
+    if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 3) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(OZ_TMEM_COLS));
+    }
+}
+
+// Eight values from their n residues (8 bytes at r + m stride for modulus
+// m): per value the 96-bit fixed-point sum t = sum_m x_m C_m (mod 2^96),
+// C_m = round(2^96 y_m / p_m) in three 32-bit words (three 32 x 32 -> 64-bit
+// multiply-adds per term, the carries propagated once at the end), whose top
+// 64 bits read as a signed integer are 2^64 X / M (the constants' rounding
+// moves t by at most sum x_m / 2 units of 2^-96); X 2^-2b = that times
+// fin96 = M 2^-64 2^-2b.
+__device__ __forceinline__ void oz_crt8(const OzScheme &sch, const uint8_t *r, size_t stride, double (&v)[8])
+{
+    unsigned long long a[8][3];
+#pragma unroll
+    for (int e = 0; e < 8; e++) a[e][0] = a[e][1] = a[e][2] = 0ull;
+    for (int m = 0; m < sch.n; m++) {
+        const uint2 w = *reinterpret_cast<const uint2 *>(r + (size_t)m * stride);
+        const unsigned long long c0 = sch.c96[0][m], c1 = sch.c96[1][m], c2 = sch.c96[2][m];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const unsigned long long x = ((e < 4 ? w.x : w.y) >> (8 * (e & 3))) & 0xffu;
+            a[e][0] += x * c0;
+            a[e][1] += x * c1;
+            a[e][2] += x * c2;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        const unsigned long long a1 = a[e][1] + (a[e][0] >> 32);
+        const unsigned long long a2 = a[e][2] + (a1 >> 32);
+        const unsigned long long top = (a2 << 32) | (a1 & 0xffffffffull);
+        v[e] = (double)(long long)top * sch.fin96;
+    }
+}
+
+// Recombination, scaling, interstitial term and store of the residue tiles:
+// one thread per (row of the tile, 16-column chunk, matrix: 0 = H, 1 = O),
+// 256 threads per block, blockIdx.y covering 128 * NCH * 2 threads of a tile.
+template <int BJ>
+__global__ void __launch_bounds__(256) oz_crt_kernel(DevParams p, const KDesc *ks, const int *tiles,
+                                                     const __grid_constant__ OzScheme sch, const uint8_t *res)
+{
+    using C = ResCfg<BJ>;
+    const int tile = blockIdx.x;
+    const int t = blockIdx.y * blockDim.x + threadIdx.x;
+    const int row = t & 127, rest = t >> 7;
+    const int c = rest % C::NCH, half = rest / C::NCH;
+    if (half > 1) return;
+    const KDesc kd = ks[tiles[3 * tile]];
+    const int i = tiles[3 * tile + 1] * OZ_BM + row;
+    const int jb = tiles[3 * tile + 2] * BJ + c * 16;
+    if (i >= kd.ngp || jb >= kd.ngp || jb + 15 < i) return;    // no element i <= j < ngp here
+    const uint8_t *tres = res + (size_t)tile * sch.n * C::MOD_BYTES;
+    const size_t stride = C::MOD_BYTES;                          // between moduli
+    const uint8_t *re_p = tres + ((size_t)((2 * half) * C::NCH + c) * 128 + row) * 16;
+    const uint8_t *im_p = tres + ((size_t)((2 * half + 1) * C::NCH + c) * 128 + row) * 16;
+    // row data
+    int gi = kd.igpig[i] - 1;
+    if (gi < 0 || gi >= p.ngrtot) {
+        atomicOr(p.err, DEV_ERR_INDEX);
+        gi = 0;
+    }
+    const int ivi[3] = {p.ivg[3 * gi], p.ivg[3 * gi + 1], p.ivg[3 * gi + 2]};
+    const double vi[3] = {kd.vgpc[3 * i], kd.vgpc[3 * i + 1], kd.vgpc[3 * i + 2]};
+    const double sai = oz_sigma(kd.oz_scale[i]);
+    const double *scol = kd.oz_scale + (half == 0 ? p.npad : 0);
+    const int kind = half == 0 ? EPI_HAM : EPI_OVL;
+    exs_complex *out = half == 0 ? kd.h : kd.o;
+    double vre[2][8], vim[2][8];
+    oz_crt8(sch, re_p, stride, vre[0]);
+    oz_crt8(sch, re_p + 8, stride, vre[1]);
+    oz_crt8(sch, im_p, stride, vim[0]);
+    oz_crt8(sch, im_p + 8, stride, vim[1]);
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+        const int j = jb + e;
+        if (j >= kd.ngp || j < i) continue;
+        int gj = kd.igpig[j] - 1;
+        if (gj < 0 || gj >= p.ngrtot) {
+            atomicOr(p.err, DEV_ERR_INDEX);
+            gj = 0;
+        }
+        const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
+        const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
+        const double sc = sai * oz_sigma(scol[j]);
+        double re = vre[e >> 3][e & 7] * sc, im = vim[e >> 3][e & 7] * sc;
+        double ar, ai;
+        if (interstitial(p, kind, ivi, ivj, vi, vj, ar, ai)) {
+            re += ar;
+            im += ai;
+        }
+        exs_complex v;
+        v.re = re;
+        v.im = im;
+        out[(size_t)i + (size_t)kd.nmat * j] = v;
+        if (i < j) {
+            v.im = -im;
+            out[(size_t)j + (size_t)kd.nmat * i] = v;
+        }
+    }
+}
+
 // ------------------------------------------------------------ host side
 int oz_kpad(int K) { return (K + OZ_MAX_KCH * OZ_CHUNK - 1) / (OZ_MAX_KCH * OZ_CHUNK) * (OZ_MAX_KCH * OZ_CHUNK); }
 
@@ -1345,20 +1662,22 @@ static int oz_inverse_mod(long long a, long long p)
 // The modular scheme for n moduli, contraction length K (H/O tiles) and
 // per-atom window kx.  Columns are scaled by their 2-norms, so the integer
 // products obey |X| <= 2^(2b) (1 + eps)^2 (H/O) and 2^(b + bx) (1 + eps)^2
-// (per-atom) whatever K; the plan keeps h >= 5 headroom bits and one bit of
-// margin: b = min(52, floor((log2 M - 7) / 2)), h = floor(log2 M - 2 - 2b),
-// bx = min(52, floor(log2 M - 2 - h - b)).  The quantisation error of the
-// operands grows like 2^-b sqrt(K), so n = 0 takes the fewest moduli in
-// 6..16 with b >= 41 + log2(K) / 2 (47 bits and 13 moduli at K = 1936, 51
-// bits and 14 moduli at K = 34,992).  Returns 0, or -1 if no valid plan
-// exists (n out of range, b or bx below 8, or K past the exact int32 range
-// of one product: 2 K 127^2 < 2^31).
+// (per-atom) whatever K.  The H/O products are recombined exactly (96-bit
+// constants), so b = min(52, floor((log2 M - 2) / 2)) keeps one bit of
+// margin beyond 2|X| < M; the per-atom products are folded in 64 bits with
+// h >= 5 headroom bits: bx = min(52, floor(log2 M - 7 - b)),
+// h = floor(log2 M - 2 - b - bx).  The quantisation error of the operands
+// grows like 2^-b sqrt(K), so n = 0 takes the fewest moduli in 6..16 with
+// b >= 41 + log2(K) / 2 and bx >= 44 (13 moduli, b = 49 and bx = 45, at both
+// K = 1936 and K = 34,992).  Returns 0, or -1 if no valid plan exists (n out
+// of range, b or bx below 8, or K past the exact int32 range of one product:
+// 2 K 127^2 < 2^31).
 static void oz_mod_bits(int n, int *b, int *h, int *bx)
 {
     const double lm = oz_log2_modulus(n) - 1e-9;
-    *b = std::min(52, (int)std::floor((lm - 7.0) / 2.0));
-    *h = (int)std::floor(lm - 2.0 - 2.0 * *b);
-    *bx = std::min(52, (int)std::floor(lm - 2.0 - *h - *b));
+    *b = std::min(52, (int)std::floor((lm - 2.0) / 2.0));
+    *bx = std::min(52, (int)std::floor(lm - 7.0 - *b));
+    *h = (int)std::floor(lm - 2.0 - *b - *bx);
 }
 
 int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
@@ -1370,7 +1689,7 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
         n = OZ_MAX_MODULI;
         for (int q = 6; q <= OZ_MAX_MODULI; q++) {
             oz_mod_bits(q, &b, &h, &bx);
-            if (b >= want) {
+            if (b >= want && bx >= 44) {
                 n = q;
                 break;
             }
@@ -1390,6 +1709,7 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
     for (int m = 0; m < n; m++) M *= (double)OZ_MODULI[m];
     s.fin = std::ldexp(M, -64 - h - 2 * b);
     s.finx = std::ldexp(M, -64 - h - b - bx);
+    s.fin96 = std::ldexp(M, -64 - 2 * b);
     for (int m = 0; m < n; m++) {
         const int p = OZ_MODULI[m];
         long long mm = 1;   // (M / p) mod p
@@ -1405,6 +1725,9 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
         // round(2^(64+h) y / p) mod 2^64 (y < p < 2^8 and h <= 18: the numerator fits 128 bits)
         const unsigned __int128 num = ((unsigned __int128)y << (64 + h)) + (unsigned)(p / 2);
         s.c[m] = (unsigned long long)(num / (unsigned)p);
+        // round(2^96 y / p) < 2^96 in three 32-bit words
+        const unsigned __int128 c96 = (((unsigned __int128)y << 96) + (unsigned)(p / 2)) / (unsigned)p;
+        for (int w = 0; w < 3; w++) s.c96[w][m] = (unsigned)(c96 >> (32 * w));
     }
     *sch = s;
     return 0;
@@ -1495,6 +1818,46 @@ cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *m
     }
 }
 
+template <int BJ>
+static cudaError_t launch_res_bj(const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
+                                 const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
+                                 uint8_t *res, bool persistent, cudaStream_t s)
+{
+    constexpr int smem = ResCfg<BJ>::SMEM;
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(oz_res_kernel<BJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    });
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (persistent && nsm < ntiles) ? nsm : ntiles;
+    oz_res_kernel<BJ><<<grid, OZ_THREADS, smem, s>>>(*mapA, *mapB, p, d_k, (const int *)d_tiles, ntiles, sch, kp8,
+                                                     res);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    oz_crt_kernel<BJ><<<dim3(ntiles, ResCfg<BJ>::NCH), 256, 0, s>>>(p, d_k, (const int *)d_tiles, sch, res);
+    return cudaGetLastError();
+}
+
+// The modular H/O products: residue tiles then their recombination.
+// Configuration bit 0: 128 x 32 tiles (two accumulator pairs) instead of
+// 128 x 64; bit 1: persistent residue kernel (one CTA per SM).
+cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
+                          const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch,
+                          int kp8, uint8_t *res, cudaStream_t s)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    const bool persistent = (cfg & 2) != 0;
+    if (cfg & 1) return launch_res_bj<32>(mapA, mapB32, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
+    return launch_res_bj<64>(mapA, mapB64, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
+}
+
+int oz_res_cols(int cfg) { return (cfg & 1) ? 32 : 64; }
+
+size_t oz_res_tile_bytes(int n, int cfg) { return (size_t)n * 4 * 128 * oz_res_cols(cfg); }
+
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
                            const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s)
@@ -1547,6 +1910,30 @@ bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUt
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
     return true;
+}
+
+// The B operand of the 128 x 64 residue tiles: the four arrays of 64 G rows,
+// one 128-byte K chunk (the 5D view of make_oz_tensor_maps, box {128, 64, 4, 1, 1}).
+bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, CUtensorMap *mapB64)
+{
+    typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+        return false;
+    EncodeFn encode = (EncodeFn)fn;
+    if (kp8 % OZ_CHUNK != 0 || npad % 64 != 0) return false;
+    const cuuint64_t dims[5] = {(cuuint64_t)OZ_CHUNK, (cuuint64_t)npad, OZ_NARR, (cuuint64_t)(kp8 / OZ_CHUNK),
+                                (cuuint64_t)nss};
+    const cuuint64_t strides[4] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)OZ_CHUNK,
+                                   (cuuint64_t)OZ_NARR * npad * kp8};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    const cuuint32_t box[5] = {OZ_CHUNK, 64, OZ_NARR, 1, 1};
+    return encode(mapB64, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // TMA views for the per-atom products:

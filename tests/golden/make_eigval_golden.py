@@ -1,7 +1,7 @@
 """Collect the reference's own EIGVAL.OUT files as text fixtures.
 
 Reads ``test/test_farm/<case>/ref/EIGVAL.OUT`` of the exciting source tree
-(path given as argv[1], default /root/reference) and writes
+(its path is the required argument) and writes
 ``eigval_fixtures.json`` beside this script: {case: file text} for every
 case whose file is at most 20 kB.  They pin the EIGVAL.OUT writer
 (exciting_b200.fileio.write_eigval, the I6 / G18.10 layout of
@@ -29,4 +29,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_eigval_golden.py <exciting source tree>")
+    main(sys.argv[1])

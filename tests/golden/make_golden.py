@@ -1,7 +1,7 @@
 """Extract golden counts from the reference's own test-farm outputs.
 
 Reads ``test/test_farm/<case>/ref/{INFO.OUT,KPOINTS.OUT}`` of the exciting
-source tree (path given as argv[1], default /root/reference) and writes
+source tree (its path is the required argument) and writes
 ``reference_counts.json`` beside this script: per case the lattice, the muffin
 tin radii, the atomic positions, rgkmax, gmaxvr, the FFT box (``G-vector grid
 sizes``), the number of G-vectors, the unit-cell volume, the number of local
@@ -87,7 +87,9 @@ def parse_kpoints(path):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <exciting source tree>")
+    root = sys.argv[1]
     farm = os.path.join(root, "test", "test_farm")
     out = {}
     for case in CASES:

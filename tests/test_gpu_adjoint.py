@@ -153,7 +153,9 @@ def test_adjoint_autograd_function():
     st = setup(s)
     direct = adjoint(st, s, gk, c, w, eps)
     st.close()
-    assert np.array_equal(grad, direct)
+    # the same quantity up to the forward's rebuilt positions (lattice coordinates from Cartesian
+    # ones) and the order of the scatter's atomic additions
+    assert np.max(np.abs(grad - direct)) <= TOL_F
     # finite differences through the wrapped forward
     for ias, x in ((0, 0), (1, 2)):
         e = np.zeros(3 * s.natmtot)

@@ -1,16 +1,18 @@
 """The modular split-precision scheme (EXS_PREC_OZAKI_MOD), checked on the CPU.
 
-The library's plan (exs_ozaki_moduli: moduli, Chinese-remainder constants,
-bits per operand, headroom bits) is checked against exact integer
+The library's plan (exs_ozaki_moduli: moduli, bits per operand, the per-atom
+fold's constants and headroom bits) is checked against exact integer
 arithmetic, and the device arithmetic is emulated in numpy with that plan:
 columns scaled by a power of two above their 2-norms, residues in
-[-127, 127], one exact integer product per modulus, the multiply-high
-quotient of the fold, the 64-bit wrapping sum t += r c_m with c_m =
-round(2^(64+h) y_m / p_m) and the final t / 2^(64+h) * M.  The emulated
-products must reconstruct the exact integer product within the stated bound
-(sum |r| / 2 + 1 units of 2^-(64+h) M), and an emulated setup on a Si
-k-point must meet the 1e-12 Frobenius bar and keep the lowest generalized
-eigenvalues within 1e-8 Ha.  No GPU is touched.
+[-127, 127], one exact integer product per modulus; for the H/O products the
+residues x = v mod p in [0, p) recombined with 96-bit constants C_m =
+round(2^96 y_m / p_m) (the top 64 bits of sum x_m C_m mod 2^96 read as a
+signed integer times M 2^-64, oz_crt_kernel); for the per-atom products the
+kernel's multiply-high fold into the 64-bit wrapping sum t += r c_m with
+c_m = round(2^(64+h) y_m / p_m).  The emulated products must reconstruct the
+exact integer products within the stated bounds, and an emulated setup must
+meet the 1e-12 Frobenius bar and keep the lowest generalized eigenvalues
+within 1e-8 Ha.  No GPU is touched.
 """
 import ctypes
 import math
@@ -36,7 +38,7 @@ def plan(n, K, kx):
 
 
 @pytest.mark.parametrize("n,K,kx", [(14, 1936, 242), (12, 1936, 242), (0, 1936, 242), (0, 34992, 162),
-                                    (16, 65536, 512), (6, 200, 50), (0, 324, 162)])
+                                    (16, 65536, 512), (8, 200, 50), (0, 324, 162)])
 def test_plan_constants_and_bounds(n, K, kx):
     ps, cs, b, bx, h = plan(n, K, kx)
     if n:
@@ -49,25 +51,28 @@ def test_plan_constants_and_bounds(n, K, kx):
     for p, c in zip(ps, cs):
         y = pow(M // p, -1, p)
         assert c == (((y << (64 + h)) + p // 2) // p) % 2 ** 64      # round(2^(64+h) y / p) mod 2^64
-    # |X| <= 2^(2b) (1 + eps)^2 for 2-norm-scaled columns: one bit of margin beyond 2^h |X| < M / 2
-    assert 2 ** (2 * b + h + 2) <= M and 2 ** (b + bx + h + 2) <= M
+    # H/O: |X| <= 2^(2b) (1 + eps)^2, one bit of margin beyond 2|X| < M; per-atom fold: h headroom bits
+    assert 2 ** (2 * b + 2) <= M and 2 ** (b + bx + h + 2) <= M
     assert h >= 5 and b <= 52 and bx <= 52
-    # b is the largest that keeps 5 headroom bits (unless capped at 52), h and bx the largest after it
-    assert b == 52 or 2 ** (2 * (b + 1) + 5 + 2) > M
-    assert 2 ** (2 * b + (h + 1) + 2) > M
-    assert bx == 52 or 2 ** (b + bx + 1 + h + 2) > M
+    # b, bx and h are the largest that fit (unless capped at 52)
+    assert b == 52 or 2 ** (2 * (b + 1) + 2) > M
+    assert bx == 52 or 2 ** (b + (bx + 1) + 5 + 2) > M
+    assert 2 ** (b + bx + (h + 1) + 2) > M
     if n == 0:
         want = math.ceil(41 + 0.5 * math.log2(K) - 1e-9)
-        assert b >= want
+        assert b >= want and bx >= 44
         if len(ps) > 6:    # one modulus fewer would not keep the bits
-            assert plan(len(ps) - 1, K, kx)[2] < want
+            q = plan(len(ps) - 1, K, kx)
+            assert q[2] < want or q[3] < 44
 
 
 def test_plan_counts_of_the_benchmark_cells():
-    """13 moduli at 47 bits for the 8-atom cell (K = 1936), 14 at 51 for the
-    216-atom cell (K = 34,992), both with 5 headroom bits."""
-    assert [plan(0, 1936, 242)[k] for k in (2, 4)] == [47, 5] and len(plan(0, 1936, 242)[0]) == 13
-    assert [plan(0, 34992, 162)[k] for k in (2, 4)] == [51, 5] and len(plan(0, 34992, 162)[0]) == 14
+    """13 moduli at 49 bits (45 for the h_a rows, 5 headroom bits in the
+    per-atom fold) for both the 8-atom cell (K = 1936) and the 216-atom cell
+    (K = 34,992)."""
+    for K, kx in ((1936, 242), (34992, 162)):
+        ps, _, b, bx, h = plan(0, K, kx)
+        assert (len(ps), b, bx, h) == (13, 49, 45, 5)
 
 
 def test_plan_rejects_bad_arguments():
@@ -90,7 +95,7 @@ def _fold_reduce(v, p):
 
 
 def emulate(X, Y, ps, cs):
-    """Integer product X^T Y (entries of X, Y integers as float64) by the modular fold."""
+    """Integer product X^T Y by the per-atom kernel's 64-bit fold."""
     t = np.zeros((X.shape[1], Y.shape[1]), dtype=np.uint64)
     rsum = np.zeros(t.shape)
     for p, c in zip(ps, cs):
@@ -104,6 +109,40 @@ def emulate(X, Y, ps, cs):
     return t.view(np.int64), rsum
 
 
+def c96(ps):
+    """The H/O recombination constants C_m = round(2^96 y_m / p_m) as three 32-bit words."""
+    M = math.prod(ps)
+    out = []
+    for p in ps:
+        y = pow(M // p, -1, p)
+        c = ((y << 96) + p // 2) // p
+        out.append([(c >> (32 * w)) & 0xffffffff for w in range(3)])
+    return out
+
+
+def emulate_crt(X, Y, ps):
+    """Integer product X^T Y as the residue tiles give it: per modulus the
+    residue x = (X^T Y) mod p in [0, p) (the kernel's multiply-high reduction
+    of the exact int32 sum, then moved into [0, p)), recombined by the 96-bit
+    sum of oz_crt_kernel (three 64-bit accumulators, carries at the end); the
+    result is the signed top 64 bits (2^64 X / M)."""
+    C = c96(ps)
+    a = [np.zeros((X.shape[1], Y.shape[1]), dtype=np.uint64) for _ in range(3)]
+    for p, cw in zip(ps, C):
+        v = np.rint(_residues(X, p).T @ _residues(Y, p)).astype(np.int64)
+        x = _fold_reduce(v, p)
+        x = np.where(x < 0, x + p, x)
+        x = np.where(x >= p, x - p, x).astype(np.uint64)
+        with np.errstate(over="ignore"):
+            for w in range(3):
+                a[w] += x * np.uint64(cw[w])
+    with np.errstate(over="ignore"):
+        a1 = a[1] + (a[0] >> np.uint64(32))
+        a2 = a[2] + (a1 >> np.uint64(32))
+        top = (a2 << np.uint64(32)) | (a1 & np.uint64(0xffffffff))
+    return top.view(np.int64)
+
+
 def _norm_columns(rng, K, ncol, b):
     """Integer columns of 2-norm <= 2^b (random directions, rounded)."""
     Z = rng.standard_normal((K, ncol))
@@ -112,22 +151,43 @@ def _norm_columns(rng, K, ncol, b):
 
 
 @pytest.mark.parametrize("n", [8, 12, 14])
-def test_emulated_fold_reconstructs_integer_products(n):
+def test_emulated_fold_reconstructs_per_atom_products(n):
+    """The 64-bit fold of the per-atom products: |X| <= 2^(b + bx), t =
+    2^(64+h) X / M + e with |e| <= sum |r| / 2 + 1."""
     rng = np.random.default_rng(n)
     K = 300
-    ps, cs, b, _, h = plan(n, K // 2, 8)
+    ps, cs, b, bx, h = plan(n, K // 2, 8)
     X = _norm_columns(rng, K, 5, b)
-    Y = _norm_columns(rng, K, 4, b)
-    Y[:, 0] = -X[:, 0]                 # the bound's extreme: a column pair with |X| = |x|^2 ~ 2^(2b)
+    Y = _norm_columns(rng, K, 4, bx)
+    Y[:, 0] = -np.trunc(X[:, 0] * 2.0 ** (bx - b))    # the bound's extreme: a nearly parallel pair
     t, rsum = emulate(X, Y, ps, cs)
     M = math.prod(ps)
     for i in range(X.shape[1]):
         for j in range(Y.shape[1]):
             exact = sum(int(a) * int(bb) for a, bb in zip(X[:, i], Y[:, j]))
             assert 2 ** (h + 1) * abs(exact) < M
-            # t = 2^(64+h) X / M + e, |e| <= sum |r| / 2 (rounded constants) + 1 (the exact quotient's fraction)
             err = int(t[i, j]) * M - exact * 2 ** (64 + h)
             assert abs(err) <= (rsum[i, j] / 2 + 1) * M, (i, j)
+
+
+@pytest.mark.parametrize("n", [8, 12, 13, 16])
+def test_emulated_crt_reconstructs_ho_products(n):
+    """The residue tiles' recombination: |X| <= 2^(2b), the top 64 bits of the
+    96-bit sum equal floor(2^64 X / M) up to one unit (the constants' rounding
+    is below 2^-85 of M)."""
+    rng = np.random.default_rng(100 + n)
+    K = 300
+    ps, _, b, _, _ = plan(n, K // 2, 8)
+    X = _norm_columns(rng, K, 5, b)
+    Y = _norm_columns(rng, K, 4, b)
+    Y[:, 0] = -X[:, 0]
+    top = emulate_crt(X, Y, ps)
+    M = math.prod(ps)
+    for i in range(X.shape[1]):
+        for j in range(Y.shape[1]):
+            exact = sum(int(a) * int(bb) for a, bb in zip(X[:, i], Y[:, j]))
+            assert 2 * abs(exact) < M
+            assert abs(int(top[i, j]) * M - exact * 2 ** 64) <= 2 * M, (i, j)
 
 
 def _split_scaled(Z, b):
@@ -168,10 +228,10 @@ def _emulated_setup(s, gk, apwalm):
     XA = np.concatenate([ar, ai])                   # [Ar; Ai]
     YH = [np.concatenate([br, bi]), np.concatenate([bi, -br])]    # Re H, Im H
     YO = [np.concatenate([ar, ai]), np.concatenate([ai, -ar])]    # Re O, Im O
-    scale = M * 2.0 ** (-64 - h - 2 * b)
+    scale = M * 2.0 ** (-64 - 2 * b)
     out = []
     for Ys, sy in ((YH, sb), (YO, sa)):
-        parts = [emulate(XA, Y, ps, cs)[0].astype(np.float64) * scale for Y in Ys]
+        parts = [emulate_crt(XA, Y, ps).astype(np.float64) * scale for Y in Ys]
         out.append((parts[0] + 1j * parts[1]) * np.outer(sa, sy))
     Bx = np.concatenate([s.mt_aa[:, :, a] @ apwi[a] for a in range(s.natmtot)])
     return out[0], out[1], A.conj().T @ Bx, A.conj().T @ A, B, Bx
@@ -189,7 +249,7 @@ def test_emulated_setup_meets_the_bars():
     gk = s.gkset(s.kpoints[3])
     apwalm, _ = O.match(s, gk)
     Hm, Om, Href, Oref, B, Bx = _emulated_setup(s, gk, apwalm)
-    assert np.linalg.norm(B - Bx) / np.linalg.norm(Bx) <= 1e-13
+    assert np.linalg.norm(B - Bx) / np.linalg.norm(Bx) <= 1e-12
     assert np.linalg.norm(Hm - Href) / np.linalg.norm(Href) <= 1e-12
     assert np.linalg.norm(Om - Oref) / np.linalg.norm(Oref) <= 1e-12
     H, Ov = O.hamiltonandoverlapsetup(s, gk, apwalm)
@@ -228,12 +288,12 @@ def test_split_residue_formula():
 
 def test_emulated_eight_atom_eigenvalues():
     """The 8-atom cell (K = 1936, O conditioned ~2.5e4, eigenvalues down to
-    about -1600 Ha), k-point 0: H/O products through the emulated integer
-    path of the default plan (13 moduli, 47 bits, 5 headroom bits), the
+    about -1600 Ha), k-point 0: H/O products through the emulated residue
+    tiles of the default plan (13 moduli, 49 bits, 96-bit recombination), the
     lowest 40 generalized eigenvalues within the absolute 1e-8 Ha of FP64.
-    With the constants at 2^64 and column-maximum scaling (no headroom) the
-    same emulation is 4.3e-8 Ha off: the recombination error, not the
-    operand bits, limits the eigenvalues."""
+    A 64-bit recombination with column-maximum scaling and no headroom is
+    4.3e-8 Ha off on the same k-point: the recombination, not the operand
+    bits, limited the eigenvalues."""
     import scipy.linalg as sl
     import lapw_oracle as O
     from exciting_b200 import workloads as W
@@ -246,16 +306,16 @@ def test_emulated_eight_atom_eigenvalues():
     A = np.concatenate(apwi)
     B = np.concatenate([s.mt_aa[:, :, a] @ apwi[a] for a in range(s.natmtot)])
     ps, cs, b, _, h = plan(0, A.shape[0], s.basis.maxaa)
-    assert (len(ps), b, h) == (13, 47, 5)
+    assert (len(ps), b) == (13, 49)
     M = float(math.prod(ps))
     ar, ai, sa = _split_scaled(A, b)
     br, bi, sb = _split_scaled(B, b)
     XA = np.concatenate([ar, ai])
-    scale = M * 2.0 ** (-64 - h - 2 * b)
+    scale = M * 2.0 ** (-64 - 2 * b)
     got = []
     for Ys, sy in (([np.concatenate([br, bi]), np.concatenate([bi, -br])], sb),
                    ([np.concatenate([ar, ai]), np.concatenate([ai, -ar])], sa)):
-        parts = [emulate(XA, Y, ps, cs)[0].astype(np.float64) * scale for Y in Ys]
+        parts = [emulate_crt(XA, Y, ps).astype(np.float64) * scale for Y in Ys]
         got.append((parts[0] + 1j * parts[1]) * np.outer(sa, sy))
     Href, Oref = A.conj().T @ B, A.conj().T @ A
     assert np.linalg.norm(got[0] - Href) / np.linalg.norm(Href) <= 1e-12
