@@ -378,8 +378,6 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         return fail(c, EXS_ERR_ARG, "slices must be in 3..9");
     if (mode == EXS_PREC_OZAKI_MOD && slices != 0 && (slices < 6 || slices > exs::OZ_MAX_MODULI))
         return fail(c, EXS_ERR_ARG, "moduli must be 0 (automatic) or in 6..16");
-    if (c->relativity == EXS_REL_IORA)
-        return fail(c, EXS_ERR_ARG, "the split-precision contraction does not take the iora* overlap term");
     const int kp8 = exs::oz_kpad(c->K);
     exs::OzScheme sch{};
     if (mode == EXS_PREC_OZAKI_MOD) {
@@ -394,7 +392,8 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     const int seg = sch.seg;
     cudaSetDevice(c->device);
     EXS_CUDA(cudaStreamSynchronize(c->stream));
-    const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8);
+    const int narr = c->relativity == EXS_REL_IORA ? 6 : 4;    // + Cr, Ci: O = A^H (I + h1aa) A
+    const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8, narr);
     if (c->d_oz) { cudaFree(c->d_oz); c->d_oz = nullptr; }
     if (c->d_res) { cudaFree(c->d_res); c->d_res = nullptr; c->res_bytes = 0; }
     if (c->d_ozscale) { cudaFree(c->d_ozscale); c->d_ozscale = nullptr; }
@@ -426,7 +425,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         e = cudaMalloc((void **)&c->d_res, res);
         if (e == cudaSuccess) c->res_bytes = res;
     }
-    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 2 * c->npad * c->max_batch);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 3 * c->npad * c->max_batch);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xs, xgroups * 128 * c->oz_lw);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xsig, sizeof(double) * c->natmtot * c->oz_nxb * 64);
     if (e != cudaSuccess || c->oz_xseg < 1) {
@@ -440,11 +439,11 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     const size_t nss = (size_t)slices * c->max_batch;
     bool maps_ok = true;
     for (int q = 0; q < exs::OZ_NCFG; q++)
-        maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, nss, c->npad, kp8, exs::OZ_CFG_KCH[q], &c->oz_mapA[q],
-                                                      &c->oz_mapB[q], &c->oz_mapB2[q]);
-    maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, nss, c->npad, kp8, c->d_xs, xgroups, c->oz_lw,
+        maps_ok = maps_ok && exs::make_oz_tensor_maps(c->d_oz, nss, c->npad, kp8, exs::OZ_CFG_KCH[q], narr,
+                                                      &c->oz_mapA[q], &c->oz_mapB[q], &c->oz_mapB2[q]);
+    maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, nss, c->npad, kp8, narr, c->d_xs, xgroups, c->oz_lw,
                                                 &c->oz_mapArow, &c->oz_mapX);
-    maps_ok = maps_ok && exs::make_oz_b64_map(c->d_oz, nss, c->npad, kp8, &c->oz_mapB64);
+    maps_ok = maps_ok && exs::make_oz_b64_map(c->d_oz, nss, c->npad, kp8, narr, &c->oz_mapB64);
     if (!maps_ok) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
@@ -662,15 +661,29 @@ struct Uploaded {
 
 // Upper tiles (128 rows x 32 columns, 256 x 32 for the two-SM tiles with ib
 // counting pairs of 128-row blocks, 128 x 32 or 128 x 64 for the residue
-// tiles of the modular mode) of the split-precision contraction.
-void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows, int cols)
+// tiles of the modular mode) of the split-precision contraction, in groups of
+// `group` x `group` tiles (row blocks outer, then column blocks, inside a
+// group row blocks outer again): the tiles that run at the same time (one
+// CTA per SM) then read about `group` row blocks of A and `group` column
+// blocks of B instead of one row block and ~148 column blocks, so the L2
+// serves the shared operand chunks and HBM streams each block about
+// (number of groups in its row or column) times instead of once per tile
+// row.  group = 1 is the plain row-major order.
+void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows, int cols, int group = 1)
 {
     t.clear();
     for (size_t k = 0; k < ks.size(); k++) {
         const int n = ks[k].ngp;
-        for (int ib = 0; ib < (n + rows - 1) / rows; ib++)
-            for (int jb = 0; jb < (n + cols - 1) / cols; jb++)
-                if (jb * cols + cols - 1 >= ib * rows) { t.push_back((int)k); t.push_back(ib); t.push_back(jb); }
+        const int nib = (n + rows - 1) / rows, njb = (n + cols - 1) / cols;
+        for (int gi = 0; gi < nib; gi += group)
+            for (int gj = 0; gj < njb; gj += group)
+                for (int ib = gi; ib < std::min(nib, gi + group); ib++)
+                    for (int jb = gj; jb < std::min(njb, gj + group); jb++)
+                        if (jb * cols + cols - 1 >= ib * rows) {
+                            t.push_back((int)k);
+                            t.push_back(ib);
+                            t.push_back(jb);
+                        }
     }
 }
 
@@ -705,8 +718,8 @@ void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt
     ozt.clear();
     std::vector<int> ozat;
     if (c->oz_on()) {
-        if (c->oz_sch.mod)
-            oz_tiles(ks, ozt, 128, exs::oz_res_cols(c->oz_cfg));
+        if (c->oz_sch.mod)   // grouped 12 x 12 (about one wave of 148 CTAs)
+            oz_tiles(ks, ozt, 128, exs::oz_res_cols(c->oz_cfg), 12);
         else
             oz_tiles(ks, ozt, (c->oz_cfg & 8) ? 256 : 128, 32);
         oz_atom_tiles(c, ks, ozat);
@@ -816,7 +829,7 @@ cudaError_t oz_reset_maxima(exs_ctx *c, const std::vector<KDesc> &ks, cudaStream
         lo = std::min(lo, k.oz_scale);
         hi = std::max(hi, k.oz_scale);
     }
-    return cudaMemsetAsync(lo, 0, sizeof(double) * ((size_t)(hi - lo) + 2 * (size_t)c->npad), s);
+    return cudaMemsetAsync(lo, 0, sizeof(double) * ((size_t)(hi - lo) + 3 * (size_t)c->npad), s);
 }
 
 // Enqueue the whole setup for the k descriptors in ks (device arrays filled)
@@ -837,6 +850,11 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     if (c->relativity == EXS_REL_IORA) EXS_CUDA(exs::launch_iora_planes(p, u.d_k, (int)ks.size(), ngp_max, s));
     EXS_EV(1);
     const bool oz = c->oz_on();
+    if (oz && c->relativity == EXS_REL_IORA) {
+        // C = (I + h1aa) A, the right operand of O: its column bound (maximum or 2-norm), then its slices
+        EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 2, c->oz_sch.mod, s));
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 2, s));
+    }
     // configuration bit 4: B = h_a A and the APW-lo rows in native FP64 even
     // when the H/O contraction is split
     const bool b64 = !oz || (c->oz_cfg & 16);
@@ -844,8 +862,8 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     const bool norms = oz && c->oz_sch.mod;
     if (oz) {
         // slices of A; B = h_a A and the APW-lo rows of H from the slices of h_a and loa
-        if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 0, s));
-        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 2, s));
+        if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 0, 1, s));
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 0, s));
         if (!b64)
             EXS_CUDA(exs::launch_oz_atom(c->oz_cfg, &c->oz_mapArow, &c->oz_mapX, p, u.d_k, u.d_ozatiles,
                                          u.nozatiles, c->oz_sch, c->kp8, c->oz_atom_args(), s));
@@ -856,8 +874,8 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
     }
     EXS_EV(2);
     if (oz) {
-        if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 1, s));
-        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 0, s));
+        if (norms) EXS_CUDA(exs::launch_oz_colnorm(p, u.d_k, (int)ks.size(), 1, 1, s));
+        EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 1, s));
         const int q = c->oz_cfg;
         if (c->oz_sch.mod)   // residue tiles (one K chunk per stage: the maps of configuration 1), then the CRT
             EXS_CUDA(exs::launch_oz_res(q, &c->oz_mapA[1], &c->oz_mapB[1], &c->oz_mapB64, p, u.d_k, u.d_oztiles,
@@ -915,7 +933,7 @@ KDesc slot_desc(exs_ctx *c, int slot, int ngp, const int *d_igpig, const double 
     }
     k.oz_slices = c->d_oz ? c->d_oz + (size_t)slot * c->oz_slot_bytes : nullptr;
     const bool oz = c->oz_on() && c->d_ozscale;
-    k.oz_scale = oz ? c->d_ozscale + (size_t)slot * 2 * c->npad : nullptr;
+    k.oz_scale = oz ? c->d_ozscale + (size_t)slot * 3 * c->npad : nullptr;
     k.oz_slot = slot;
     return k;
 }

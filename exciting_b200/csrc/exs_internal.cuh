@@ -343,29 +343,29 @@ void pm_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)
-cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int a0,
+cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int which,
                             cudaStream_t s);
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s);
-cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, cudaStream_t s);
+cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, int norm, cudaStream_t s);
 cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
                           const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch,
                           int kp8, uint8_t *res, cudaStream_t s);
 int oz_res_cols(int cfg);
 size_t oz_res_tile_bytes(int n, int cfg);
-bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, CUtensorMap *mapB64);
+bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64);
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
                            const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s);
-bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, size_t xgroups, int lw,
+bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, int narr, void *xbase, size_t xgroups, int lw,
                        CUtensorMap *mapArow, CUtensorMap *mapX);
 cudaError_t launch_oz_mma(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB, const DevParams &p,
                           const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                           cudaStream_t s);
-bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB,
-                         CUtensorMap *mapB2);
+bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, int narr, CUtensorMap *mapA,
+                         CUtensorMap *mapB, CUtensorMap *mapB2);
 extern const int OZ_CFG_KCH[OZ_NCFG], OZ_CFG_NST[OZ_NCFG];
 int oz_kpad(int K);
-size_t oz_slot_bytes(int S, int npad, int kp8);
+size_t oz_slot_bytes(int S, int npad, int kp8, int narr);
 int oz_seg_pairs(int S, int kp8);
 int oz_mod_plan(int n, int K, int kx, OzScheme *sch);
 }  // namespace exs

@@ -91,7 +91,7 @@ namespace exs {
 constexpr int OZ_BM = 128;                       // tile rows (G_i)
 constexpr int OZ_BJ = 32;                        // tile columns (G_j); MMA N = 4 * OZ_BJ
 constexpr int OZ_N = 4 * OZ_BJ;
-constexpr int OZ_NARR = 4;                       // Br, Bi, Ar, Ai
+constexpr int OZ_NARR = 4;                       // Br, Bi, Ar, Ai (the B box: four arrays)
 constexpr int OZ_CHUNK = 128;                    // bytes of K in one swizzle row
 constexpr int OZ_TILE = 128 * OZ_CHUNK;          // 16 KB: one K chunk of a 128-row operand
 constexpr int OZ_THREADS = 384;                  // 12 warps: see the roles below
@@ -244,10 +244,15 @@ __host__ __device__ __forceinline__ double oz_sigma(double m)
     return ldexp(1.0, e);
 }
 
+// Arrays of one slice of a slot: Br, Bi, Ar, Ai, or with iora* (O = A^H C,
+// C = (I + h1aa) A) Br, Bi, Cr, Ci, Ar, Ai, so that the B box is always the
+// first four arrays and the A operand the last two.
+__host__ __device__ __forceinline__ int oz_narr(int relativity) { return relativity == EXS_REL_IORA ? 6 : 4; }
+
 // Byte offset of (slice s, array a, row G, K index f) inside one slot.
-__device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, int kp8)
+__device__ __forceinline__ size_t oz_off(int s, int a, int g, int f, int npad, int kp8, int narr)
 {
-    return (((size_t)s * OZ_NARR + a) * npad + g) * (size_t)kp8 + f;
+    return (((size_t)s * narr + a) * npad + g) * (size_t)kp8 + f;
 }
 
 // Residues of an integer x (|x| <= 2^52) in exact FP32 arithmetic: with
@@ -438,7 +443,8 @@ __device__ __forceinline__ void oz_store_ho(const DevParams &p, const KDesc &kd,
     const double sai = row_ok ? oz_sigma(kd.oz_scale[i]) : 0.0;
     const int kind = half == 0 ? EPI_HAM : EPI_OVL;
     exs_complex *out = half == 0 ? kd.h : kd.o;
-    const double *scol = kd.oz_scale + (half == 0 ? p.npad : 0);
+    // H: sigma_B(j); O: sigma_A(j), or sigma_C(j) with iora* (O = A^H C)
+    const double *scol = kd.oz_scale + (half == 0 ? p.npad : (p.relativity == EXS_REL_IORA ? 2 * p.npad : 0));
 #pragma unroll 1
     for (int jc = 0; jc < OZ_BJ; jc += 8) {
         double val[2][8];
@@ -501,38 +507,49 @@ __device__ __forceinline__ void oz_store_mirror(const KDesc &kd, int i0, int j0,
     }
 }
 
-// Column 2-norms of the A planes (which = 0) or the B planes (which = 1) for
-// the modular scheme, written over the maxima in oz_scale: one column per
-// thread column of a 32 x 8 block, the eight rows of threads summing the
-// squares of interleaved rows f (stride 8) and the eight partial sums added
-// in a fixed order, so that the scales, and every result, are the same from
-// run to run.  The factor 1 + 2^-30 covers the rounding of the sum.
-__global__ void __launch_bounds__(256) oz_colnorm_kernel(DevParams p, const KDesc *ks, int which)
+// Planes and scale block of operand `which` (0: A, 1: B, 2: C = (I + h1aa) A).
+__device__ __forceinline__ void oz_operand(const KDesc &k, int which, const double *&pr, const double *&pi)
+{
+    pr = which == 0 ? k.ar : (which == 1 ? k.br : k.cr);
+    pi = which == 0 ? k.ai : (which == 1 ? k.bi : k.ci);
+}
+
+// Column bounds of the A, B or C planes (which = 0, 1, 2) written into
+// oz_scale block `which`: 2-norms (norm != 0; the modular scheme, over the
+// maxima the producers raised) or maxima of |re|, |im| (the slices, for C
+// whose producer raises none).  One column per thread column of a 32 x 8
+// block, the eight rows of threads covering interleaved rows f (stride 8),
+// the eight partial results combined in a fixed order, so that the scales,
+// and every result, are the same from run to run.  The factor 1 + 2^-30
+// covers the rounding of a sum of squares.
+__global__ void __launch_bounds__(256) oz_colnorm_kernel(DevParams p, const KDesc *ks, int which, int norm)
 {
     __shared__ double part[8][33];
     const KDesc k = ks[blockIdx.y];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int g = blockIdx.x * 32 + tx;
-    const double *pr = which ? k.br : k.ar, *pi = which ? k.bi : k.ai;
+    const double *pr, *pi;
+    oz_operand(k, which, pr, pi);
     double s = 0.0;
     if (g < k.ngp) {
 #pragma unroll 4
         for (int f = ty; f < p.K; f += 8) {
             const size_t i = (size_t)f * p.npad + g;
             const double xr = pr[i], xi = pi[i];
-            s = fma(xr, xr, fma(xi, xi, s));
+            s = norm ? fma(xr, xr, fma(xi, xi, s)) : fmax(s, fmax(fabs(xr), fabs(xi)));
         }
     }
     part[ty][tx] = s;
     __syncthreads();
     if (ty == 0 && g < p.npad) {
         double t = 0.0;
-        for (int q = 0; q < 8; q++) t += part[q][tx];
-        k.oz_scale[(which ? p.npad : 0) + g] = sqrt(t) * (1.0 + 0x1p-30);
+        for (int q = 0; q < 8; q++) t = norm ? t + part[q][tx] : fmax(t, part[q][tx]);
+        k.oz_scale[(size_t)which * p.npad + g] = norm ? sqrt(t) * (1.0 + 0x1p-30) : t;
     }
 }
 
-// The S slices of two of the four arrays (a0 = 0: Br, Bi; a0 = 2: Ar, Ai).
+// The S slices of one operand (which = 0: A into the last two arrays of the
+// slot; 1: B into arrays 0, 1; 2: C into arrays 2, 3 (iora*)).
 // A 64(f) x 32(G) tile per block, transposed through shared memory: reads
 // G-contiguous planes (a warp reads 32 consecutive G; 16 loads per thread in
 // flight), writes K-contiguous int8 rows eight bytes per thread (8 threads
@@ -540,14 +557,17 @@ __global__ void __launch_bounds__(256) oz_colnorm_kernel(DevParams p, const KDes
 constexpr int SPLIT_F = 64;
 
 __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc *ks,
-                                                       const __grid_constant__ OzScheme sch, int kp8, int a0)
+                                                       const __grid_constant__ OzScheme sch, int kp8, int which)
 {
     const int S = sch.n;
     __shared__ double t[2][SPLIT_F][33];
     const KDesc k = ks[blockIdx.z];
     const int f0 = blockIdx.x * SPLIT_F, g0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;      // 32 x 8
-    const double *pr = a0 == 0 ? k.br : k.ar, *pi = a0 == 0 ? k.bi : k.ai;
+    const int narr = oz_narr(p.relativity);
+    const int a0 = which == 0 ? narr - 2 : (which == 1 ? 0 : 2);
+    const double *pr, *pi;
+    oz_operand(k, which, pr, pi);
     {
         double vr[SPLIT_F / 8], vi[SPLIT_F / 8];
 #pragma unroll
@@ -570,7 +590,7 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
     const int g = g0 + gl, f = f0 + fl;
     if (g >= p.npad || f >= kp8) return;
     // 1/sigma is a power of two: the scaling is exact
-    const double rs = 1.0 / oz_sigma(k.oz_scale[(a0 == 0 ? p.npad : 0) + g]);
+    const double rs = 1.0 / oz_sigma(k.oz_scale[(size_t)which * p.npad + g]);
     if (sch.mod) {
         // x' = rint(x 2^b / sigma) (power-of-two scaling: exact), then its residues
         const double sc = rs * ldexp(1.0, sch.b);
@@ -585,7 +605,7 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
                 uint32_t w[2] = {0, 0};
 #pragma unroll
                 for (int e = 0; e < 8; e++) w[e >> 2] |= oz_residue_byte(xq[a][e], sch, m) << (8 * (e & 3));
-                *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(m, a0 + a, g, f, p.npad, kp8)) = make_uint2(w[0], w[1]);
+                *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(m, a0 + a, g, f, p.npad, kp8, narr)) = make_uint2(w[0], w[1]);
             }
         }
         return;
@@ -615,7 +635,7 @@ __global__ void __launch_bounds__(256) oz_split_kernel(DevParams p, const KDesc 
                 if ((neg[a] >> e) & 1u) q = -q;
                 w[e >> 2] |= ((uint32_t)(uint8_t)(int8_t)q) << (8 * (e & 3));
             }
-            *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(s, a0 + a, g, f, p.npad, kp8)) = make_uint2(w[0], w[1]);
+            *reinterpret_cast<uint2 *>(k.oz_slices + oz_off(s, a0 + a, g, f, p.npad, kp8, narr)) = make_uint2(w[0], w[1]);
         }
     }
 }
@@ -827,11 +847,12 @@ oz_mma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                             }
                             mbar_expect_tx(&full[st], role == 0 ? 2 * BOX : BOX);
                             const uint32_t dst = sbase + st * STAGE + role * 2 * BOX;
-                            if (role == 0) {   // Ar and Ai (arrays 2, 3) of G rows i0 .. i0+127, slice s
+                            if (role == 0) {   // Ar and Ai (the slot's last two arrays) of G rows i0 .. i0+127, slice s
                                 if (MODE == OZ_HO)
-                                    tma_load_5d(dst, &mapA, 0, ti.i0, 2, kb * KCH, slot * S + s - 1, &full[st]);
+                                    tma_load_5d(dst, &mapA, 0, ti.i0, oz_narr(p.relativity) - 2, kb * KCH, slot * S + s - 1, &full[st]);
                                 else
-                                    tma_load_4d(dst, &mapA, x0 + kb * OZ_CHUNK, ti.i0, 2, slot * S + s - 1, &full[st]);
+                                    tma_load_4d(dst, &mapA, x0 + kb * OZ_CHUNK, ti.i0, oz_narr(p.relativity) - 2, slot * S + s - 1,
+                                                &full[st]);
                             } else if (MODE == OZ_HO) {   // the four arrays of G rows j0 .. j0+31, slice t
                                 tma_load_5d(dst, &mapB, 0, ti.j0, 0, kb * KCH, slot * S + t - 1, &full[st]);
                             } else {                      // X rows of block xb, slice t
@@ -1166,7 +1187,8 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                         if (rank == 0 && role == 0) mbar_expect_tx(&full[st], 2 * STAGE);
                         const uint32_t bar = smem_u32(&full[st]);
                         if (role == 0)
-                            tma_load_5d_2sm(sbase + st * STAGE, &mapA, 0, i0, 2, kb * KCH, slot * S + s - 1, bar);
+                            tma_load_5d_2sm(sbase + st * STAGE, &mapA, 0, i0, oz_narr(p.relativity) - 2, kb * KCH,
+                                            slot * S + s - 1, bar);
                         else
                             tma_load_5d_2sm(sbase + st * STAGE + ABOX, &mapB2, 0, j0, 2 * (int)rank, kb * KCH,
                                             slot * S + t - 1, bar);
@@ -1410,8 +1432,8 @@ oz_res_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
                         }
                         mbar_expect_tx(&full[st], role == 0 ? C::ABOX : C::BBOX);
                         const uint32_t dst = sbase + st * C::STAGE + (role == 0 ? 0 : C::ABOX);
-                        if (role == 0)          // Ar and Ai (arrays 2, 3) of G rows i0 .. i0+127, modulus g
-                            tma_load_5d(dst, &mapA, 0, i0, 2, kb, slot * S + g, &full[st]);
+                        if (role == 0)          // Ar and Ai (the slot's last two arrays) of G rows i0 .. i0+127, modulus g
+                            tma_load_5d(dst, &mapA, 0, i0, oz_narr(p.relativity) - 2, kb, slot * S + g, &full[st]);
                         else                    // the four arrays of G rows j0 .. j0+BJ-1
                             tma_load_5d(dst, &mapB, 0, j0, 0, kb, slot * S + g, &full[st]);
                         fills[st]++;
@@ -1521,24 +1543,25 @@ oz_res_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     }
 }
 
-// Eight values from their n residues (8 bytes at r + m stride for modulus
-// m): per value the 96-bit fixed-point sum t = sum_m x_m C_m (mod 2^96),
-// C_m = round(2^96 y_m / p_m) in three 32-bit words (three 32 x 32 -> 64-bit
+// Eight values from their n residues (w[m]: the 8 bytes of modulus m): per
+// value the 96-bit fixed-point sum t = sum_m x_m C_m (mod 2^96), C_m =
+// round(2^96 y_m / p_m) in three 32-bit words (three 32 x 32 -> 64-bit
 // multiply-adds per term, the carries propagated once at the end), whose top
 // 64 bits read as a signed integer are 2^64 X / M (the constants' rounding
 // moves t by at most sum x_m / 2 units of 2^-96); X 2^-2b = that times
 // fin96 = M 2^-64 2^-2b.
-__device__ __forceinline__ void oz_crt8(const OzScheme &sch, const uint8_t *r, size_t stride, double (&v)[8])
+__device__ __forceinline__ void oz_crt8(const OzScheme &sch, const uint2 (&w)[OZ_MAX_MODULI], double (&v)[8])
 {
     unsigned long long a[8][3];
 #pragma unroll
     for (int e = 0; e < 8; e++) a[e][0] = a[e][1] = a[e][2] = 0ull;
-    for (int m = 0; m < sch.n; m++) {
-        const uint2 w = *reinterpret_cast<const uint2 *>(r + (size_t)m * stride);
+#pragma unroll
+    for (int m = 0; m < OZ_MAX_MODULI; m++) {
+        if (m >= sch.n) break;
         const unsigned long long c0 = sch.c96[0][m], c1 = sch.c96[1][m], c2 = sch.c96[2][m];
 #pragma unroll
         for (int e = 0; e < 8; e++) {
-            const unsigned long long x = ((e < 4 ? w.x : w.y) >> (8 * (e & 3))) & 0xffu;
+            const unsigned long long x = ((e < 4 ? w[m].x : w[m].y) >> (8 * (e & 3))) & 0xffu;
             a[e][0] += x * c0;
             a[e][1] += x * c1;
             a[e][2] += x * c2;
@@ -1554,26 +1577,35 @@ __device__ __forceinline__ void oz_crt8(const OzScheme &sch, const uint8_t *r, s
 }
 
 // Recombination, scaling, interstitial term and store of the residue tiles:
-// one thread per (row of the tile, 16-column chunk, matrix: 0 = H, 1 = O),
-// 256 threads per block, blockIdx.y covering 128 * NCH * 2 threads of a tile.
+// one thread per (row of the tile, 8-column group, matrix: 0 = H, 1 = O):
+// blocks of 128 threads (the rows), blockIdx.y = (matrix, column group).
+// Every thread first issues the 2n loads of its residue bytes (8 per modulus
+// and part), then recombines: the loads of a warp cover 32 rows, 256
+// contiguous bytes per modulus and part.  158 registers: three blocks per SM.
 template <int BJ>
-__global__ void __launch_bounds__(256) oz_crt_kernel(DevParams p, const KDesc *ks, const int *tiles,
+__global__ void __launch_bounds__(128) oz_crt_kernel(DevParams p, const KDesc *ks, const int *tiles,
                                                      const __grid_constant__ OzScheme sch, const uint8_t *res)
 {
     using C = ResCfg<BJ>;
+    constexpr int NG = BJ / 8;                                   // 8-column groups
     const int tile = blockIdx.x;
-    const int t = blockIdx.y * blockDim.x + threadIdx.x;
-    const int row = t & 127, rest = t >> 7;
-    const int c = rest % C::NCH, half = rest / C::NCH;
-    if (half > 1) return;
+    const int row = threadIdx.x;
+    const int cg = blockIdx.y % NG, half = blockIdx.y / NG;
     const KDesc kd = ks[tiles[3 * tile]];
     const int i = tiles[3 * tile + 1] * OZ_BM + row;
-    const int jb = tiles[3 * tile + 2] * BJ + c * 16;
-    if (i >= kd.ngp || jb >= kd.ngp || jb + 15 < i) return;    // no element i <= j < ngp here
+    const int jb = tiles[3 * tile + 2] * BJ + cg * 8;
+    if (i >= kd.ngp || jb >= kd.ngp || jb + 7 < i) return;     // no element i <= j < ngp here
     const uint8_t *tres = res + (size_t)tile * sch.n * C::MOD_BYTES;
     const size_t stride = C::MOD_BYTES;                          // between moduli
-    const uint8_t *re_p = tres + ((size_t)((2 * half) * C::NCH + c) * 128 + row) * 16;
-    const uint8_t *im_p = tres + ((size_t)((2 * half + 1) * C::NCH + c) * 128 + row) * 16;
+    const size_t o_re = ((size_t)((2 * half) * C::NCH + (cg >> 1)) * 128 + row) * 16 + (cg & 1) * 8;
+    const size_t o_im = ((size_t)((2 * half + 1) * C::NCH + (cg >> 1)) * 128 + row) * 16 + (cg & 1) * 8;
+    uint2 wr[OZ_MAX_MODULI], wi[OZ_MAX_MODULI];
+#pragma unroll
+    for (int m = 0; m < OZ_MAX_MODULI; m++)
+        if (m < sch.n) {
+            wr[m] = *reinterpret_cast<const uint2 *>(tres + (size_t)m * stride + o_re);
+            wi[m] = *reinterpret_cast<const uint2 *>(tres + (size_t)m * stride + o_im);
+        }
     // row data
     int gi = kd.igpig[i] - 1;
     if (gi < 0 || gi >= p.ngrtot) {
@@ -1583,16 +1615,15 @@ __global__ void __launch_bounds__(256) oz_crt_kernel(DevParams p, const KDesc *k
     const int ivi[3] = {p.ivg[3 * gi], p.ivg[3 * gi + 1], p.ivg[3 * gi + 2]};
     const double vi[3] = {kd.vgpc[3 * i], kd.vgpc[3 * i + 1], kd.vgpc[3 * i + 2]};
     const double sai = oz_sigma(kd.oz_scale[i]);
-    const double *scol = kd.oz_scale + (half == 0 ? p.npad : 0);
+    // H: sigma_B(j); O: sigma_A(j), or sigma_C(j) with iora* (O = A^H C)
+    const double *scol = kd.oz_scale + (half == 0 ? p.npad : (p.relativity == EXS_REL_IORA ? 2 * p.npad : 0));
     const int kind = half == 0 ? EPI_HAM : EPI_OVL;
     exs_complex *out = half == 0 ? kd.h : kd.o;
-    double vre[2][8], vim[2][8];
-    oz_crt8(sch, re_p, stride, vre[0]);
-    oz_crt8(sch, re_p + 8, stride, vre[1]);
-    oz_crt8(sch, im_p, stride, vim[0]);
-    oz_crt8(sch, im_p + 8, stride, vim[1]);
+    double vre[8], vim[8];
+    oz_crt8(sch, wr, vre);
+    oz_crt8(sch, wi, vim);
 #pragma unroll
-    for (int e = 0; e < 16; e++) {
+    for (int e = 0; e < 8; e++) {
         const int j = jb + e;
         if (j >= kd.ngp || j < i) continue;
         int gj = kd.igpig[j] - 1;
@@ -1603,7 +1634,7 @@ __global__ void __launch_bounds__(256) oz_crt_kernel(DevParams p, const KDesc *k
         const int ivj[3] = {p.ivg[3 * gj], p.ivg[3 * gj + 1], p.ivg[3 * gj + 2]};
         const double vj[3] = {kd.vgpc[3 * j], kd.vgpc[3 * j + 1], kd.vgpc[3 * j + 2]};
         const double sc = sai * oz_sigma(scol[j]);
-        double re = vre[e >> 3][e & 7] * sc, im = vim[e >> 3][e & 7] * sc;
+        double re = vre[e] * sc, im = vim[e] * sc;
         double ar, ai;
         if (interstitial(p, kind, ivi, ivj, vi, vj, ar, ai)) {
             re += ar;
@@ -1623,7 +1654,7 @@ __global__ void __launch_bounds__(256) oz_crt_kernel(DevParams p, const KDesc *k
 // ------------------------------------------------------------ host side
 int oz_kpad(int K) { return (K + OZ_MAX_KCH * OZ_CHUNK - 1) / (OZ_MAX_KCH * OZ_CHUNK) * (OZ_MAX_KCH * OZ_CHUNK); }
 
-size_t oz_slot_bytes(int S, int npad, int kp8) { return (size_t)S * npad * OZ_NARR * (size_t)kp8; }
+size_t oz_slot_bytes(int S, int npad, int kp8, int narr) { return (size_t)S * npad * narr * (size_t)kp8; }
 
 int oz_seg_pairs(int S, int kp8)
 {
@@ -1743,16 +1774,16 @@ const int OZ_CFG_KCH[OZ_NCFG] = {2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1, 2, 1,
 const int OZ_CFG_NST[OZ_NCFG] = {2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4,
                                  2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4, 2, 4};
 
-cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int a0,
+cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const OzScheme &sch, int kp8, int which,
                             cudaStream_t s)
 {
-    oz_split_kernel<<<dim3(kp8 / SPLIT_F, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, sch, kp8, a0);
+    oz_split_kernel<<<dim3(kp8 / SPLIT_F, p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, sch, kp8, which);
     return cudaGetLastError();
 }
 
-cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, cudaStream_t s)
+cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, int norm, cudaStream_t s)
 {
-    oz_colnorm_kernel<<<dim3(p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, which);
+    oz_colnorm_kernel<<<dim3(p.npad / 32, nk), dim3(32, 8), 0, s>>>(p, d_k, which, norm);
     return cudaGetLastError();
 }
 
@@ -1837,7 +1868,7 @@ static cudaError_t launch_res_bj(const CUtensorMap *mapA, const CUtensorMap *map
                                                      res);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    oz_crt_kernel<BJ><<<dim3(ntiles, ResCfg<BJ>::NCH), 256, 0, s>>>(p, d_k, (const int *)d_tiles, sch, res);
+    oz_crt_kernel<BJ><<<dim3(ntiles, 2 * (BJ / 8)), 128, 0, s>>>(p, d_k, (const int *)d_tiles, sch, res);
     return cudaGetLastError();
 }
 
@@ -1869,15 +1900,15 @@ cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMa
 // TMA views of the slices of all slots (int8, 5D):
 //   d0: K byte within a 128-byte chunk                       stride 1
 //   d1: G row (npad)                                         stride kp8
-//   d2: array (Br, Bi, Ar, Ai)                               stride npad kp8
+//   d2: array (Br, Bi, Ar, Ai; iora*: Br, Bi, Cr, Ci, Ar, Ai) stride npad kp8
 //   d3: K chunk                                              stride 128
-//   d4: slot x slice                                         stride 4 npad kp8
+//   d4: slot x slice                                         stride narr npad kp8
 // A box {128, 128, 2, kch, 1}: Ar and Ai of 128 G rows; B box
 // {128, 32, 4, kch, 1}: the four arrays of 32 G rows.  d3 is outside d1, d2
 // in the box, so each K chunk lands in shared memory as contiguous
 // 128-byte rows (A: 2 x 128 rows, B: 4 x 32 rows).
-bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUtensorMap *mapA, CUtensorMap *mapB,
-                         CUtensorMap *mapB2)
+bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, int narr, CUtensorMap *mapA,
+                         CUtensorMap *mapB, CUtensorMap *mapB2)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -1888,10 +1919,10 @@ bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUt
         return false;
     EncodeFn encode = (EncodeFn)fn;
     if (kch < 1 || kch > OZ_MAX_KCH || kp8 % (OZ_MAX_KCH * OZ_CHUNK) != 0) return false;
-    const cuuint64_t dims[5] = {(cuuint64_t)OZ_CHUNK, (cuuint64_t)npad, OZ_NARR, (cuuint64_t)(kp8 / OZ_CHUNK),
+    const cuuint64_t dims[5] = {(cuuint64_t)OZ_CHUNK, (cuuint64_t)npad, (cuuint64_t)narr, (cuuint64_t)(kp8 / OZ_CHUNK),
                                 (cuuint64_t)nss};
     const cuuint64_t strides[4] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)OZ_CHUNK,
-                                   (cuuint64_t)OZ_NARR * npad * kp8};
+                                   (cuuint64_t)narr * npad * kp8};
     const cuuint32_t es[5] = {1, 1, 1, 1, 1};
     const cuuint32_t boxA[5] = {OZ_CHUNK, OZ_BM, 2, (cuuint32_t)kch, 1};
     const cuuint32_t boxB[5] = {OZ_CHUNK, OZ_BJ, OZ_NARR, (cuuint32_t)kch, 1};
@@ -1914,7 +1945,7 @@ bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, CUt
 
 // The B operand of the 128 x 64 residue tiles: the four arrays of 64 G rows,
 // one 128-byte K chunk (the 5D view of make_oz_tensor_maps, box {128, 64, 4, 1, 1}).
-bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, CUtensorMap *mapB64)
+bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -1925,10 +1956,10 @@ bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, CUtensorMap *map
         return false;
     EncodeFn encode = (EncodeFn)fn;
     if (kp8 % OZ_CHUNK != 0 || npad % 64 != 0) return false;
-    const cuuint64_t dims[5] = {(cuuint64_t)OZ_CHUNK, (cuuint64_t)npad, OZ_NARR, (cuuint64_t)(kp8 / OZ_CHUNK),
+    const cuuint64_t dims[5] = {(cuuint64_t)OZ_CHUNK, (cuuint64_t)npad, (cuuint64_t)narr, (cuuint64_t)(kp8 / OZ_CHUNK),
                                 (cuuint64_t)nss};
     const cuuint64_t strides[4] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)OZ_CHUNK,
-                                   (cuuint64_t)OZ_NARR * npad * kp8};
+                                   (cuuint64_t)narr * npad * kp8};
     const cuuint32_t es[5] = {1, 1, 1, 1, 1};
     const cuuint32_t box[5] = {OZ_CHUNK, 64, OZ_NARR, 1, 1};
     return encode(mapB64, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, box, es,
@@ -1943,7 +1974,7 @@ bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, CUtensorMap *map
 //     aligned);
 //   mapX: the X slices as [group][128 rows][lw bytes] viewed like the B tiles
 //     (4D, K chunked), box {128, 128, 1, 1}.
-bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, size_t xgroups, int lw,
+bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, int narr, void *xbase, size_t xgroups, int lw,
                        CUtensorMap *mapArow, CUtensorMap *mapX)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -1957,8 +1988,8 @@ bool make_oz_atom_maps(void *base, size_t nss, int npad, int kp8, void *xbase, s
     if (kp8 % OZ_CHUNK != 0 || lw % OZ_CHUNK != 0) return false;
     const cuuint32_t es[4] = {1, 1, 1, 1};
     {
-        const cuuint64_t dims[4] = {(cuuint64_t)kp8, (cuuint64_t)npad, OZ_NARR, (cuuint64_t)nss};
-        const cuuint64_t strides[3] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)OZ_NARR * npad * kp8};
+        const cuuint64_t dims[4] = {(cuuint64_t)kp8, (cuuint64_t)npad, (cuuint64_t)narr, (cuuint64_t)nss};
+        const cuuint64_t strides[3] = {(cuuint64_t)kp8, (cuuint64_t)npad * kp8, (cuuint64_t)narr * npad * kp8};
         const cuuint32_t box[4] = {OZ_CHUNK, OZ_BM, 2, 1};
         if (encode(mapArow, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, base, dims, strides, box, es,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

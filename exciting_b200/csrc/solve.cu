@@ -71,10 +71,11 @@ int lanes_reserve(exs_ctx *c, int nl)
 // Work space of a lane for one solve of order n (grown on demand).  Returns
 // EXS_OK or an error code; no context state is written (lanes run on
 // several host threads).
-int lane_reserve(SolveLane &l, int n, int nstfv, const exs_complex *a, const exs_complex *b)
+int lane_reserve(SolveLane &l, int n, int nstfv, const exs_complex *a, const exs_complex *b, bool vectors)
 {
     int lwork = 0, meig = 0;
-    if (cusolverDnZhegvdx_bufferSize(l.h, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+    if (cusolverDnZhegvdx_bufferSize(l.h, CUSOLVER_EIG_TYPE_1,
+                                     vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_RANGE_I,
                                      CUBLAS_FILL_MODE_UPPER, n, (const cuDoubleComplex *)a, n,
                                      (const cuDoubleComplex *)b, n, 0.0, 0.0, 1, nstfv, &meig, nullptr,
                                      &lwork) != CUSOLVER_STATUS_SUCCESS)
@@ -98,14 +99,17 @@ int lane_reserve(SolveLane &l, int n, int nstfv, const exs_complex *a, const exs
 
 // Solve one problem in place on a lane: the first nstfv columns of a become
 // the eigenvectors (leading dimension n), l.w[0 .. nstfv) the values; then
-// copy them to the caller's arrays on the lane's stream.
+// copy them to the caller's arrays on the lane's stream.  evec = NULL: the
+// values only (no vectors are formed: a far smaller work space).
 int lane_solve(SolveLane &l, int n, exs_complex *a, exs_complex *b, int nstfv, double *eval, exs_complex *evec,
                int ldv)
 {
-    int rc = lane_reserve(l, n, nstfv, a, b);
+    const bool vectors = evec != nullptr;
+    int rc = lane_reserve(l, n, nstfv, a, b, vectors);
     if (rc != EXS_OK) return rc;
     int meig = 0;
-    if (cusolverDnZhegvdx(l.h, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+    if (cusolverDnZhegvdx(l.h, CUSOLVER_EIG_TYPE_1, vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR,
+                          CUSOLVER_EIG_RANGE_I,
                           CUBLAS_FILL_MODE_UPPER, n, (cuDoubleComplex *)a, n, (cuDoubleComplex *)b, n, 0.0, 0.0, 1,
                           nstfv, &meig, l.w, (cuDoubleComplex *)l.work, (int)l.lwork,
                           l.info) != CUSOLVER_STATUS_SUCCESS)
@@ -115,9 +119,10 @@ int lane_solve(SolveLane &l, int n, exs_complex *a, exs_complex *b, int nstfv, d
         cudaStreamSynchronize(l.s) != cudaSuccess)
         return EXS_ERR_CUDA;
     if (info != 0 || meig < nstfv) return EXS_ERR_ARG;
-    if (cudaMemcpyAsync(eval, l.w, sizeof(double) * nstfv, cudaMemcpyDeviceToDevice, l.s) != cudaSuccess ||
-        cudaMemcpy2DAsync(evec, sizeof(exs_complex) * ldv, a, sizeof(exs_complex) * n, sizeof(exs_complex) * n,
-                          nstfv, cudaMemcpyDeviceToDevice, l.s) != cudaSuccess)
+    if (cudaMemcpyAsync(eval, l.w, sizeof(double) * nstfv, cudaMemcpyDeviceToDevice, l.s) != cudaSuccess)
+        return EXS_ERR_CUDA;
+    if (vectors && cudaMemcpy2DAsync(evec, sizeof(exs_complex) * ldv, a, sizeof(exs_complex) * n,
+                                     sizeof(exs_complex) * n, nstfv, cudaMemcpyDeviceToDevice, l.s) != cudaSuccess)
         return EXS_ERR_CUDA;
     return EXS_OK;
 }
@@ -150,10 +155,11 @@ int exs_solve_batched_device(exs_ctx *c, int nk, const int *nmat, exs_complex *c
                              exs_complex *const *o_dev, int nstfv, double *evalfv_dev,
                              exs_complex *const *evecfv_dev, int ldv)
 {
-    if (!c || nk < 0 || (nk > 0 && (!nmat || !h_dev || !o_dev || !evalfv_dev || !evecfv_dev)) || nstfv <= 0)
+    if (!c || nk < 0 || (nk > 0 && (!nmat || !h_dev || !o_dev || !evalfv_dev)) || nstfv <= 0)
         return sfail(c, EXS_ERR_ARG, "exs_solve_batched_device: bad argument");
     for (int k = 0; k < nk; k++)
-        if (nmat[k] <= 0 || nstfv > nmat[k] || ldv < nmat[k] || !h_dev[k] || !o_dev[k] || !evecfv_dev[k])
+        if (nmat[k] <= 0 || nstfv > nmat[k] || !h_dev[k] || !o_dev[k] ||
+            (evecfv_dev && (ldv < nmat[k] || !evecfv_dev[k])))
             return sfail(c, EXS_ERR_SIZE, "nmat, nstfv or ldv out of range");
     if (nk == 0) return EXS_OK;
     cudaSetDevice(c->device);
@@ -172,7 +178,7 @@ int exs_solve_batched_device(exs_ctx *c, int nk, const int *nmat, exs_complex *c
         SolveLane &ln = st->lanes[l];
         for (int k = l; k < nk && lrc[l] == EXS_OK; k += nl)
             lrc[l] = lane_solve(ln, nmat[k], h_dev[k], o_dev[k], nstfv, evalfv_dev + (size_t)nstfv * k,
-                                evecfv_dev[k], ldv);
+                                evecfv_dev ? evecfv_dev[k] : nullptr, ldv);
         if (cudaEventRecord(ln.done, ln.s) != cudaSuccess && lrc[l] == EXS_OK) lrc[l] = EXS_ERR_CUDA;
     });
     for (int l = 0; l < nl; l++) {   // the context's stream continues after every lane

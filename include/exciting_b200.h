@@ -254,7 +254,9 @@ int exs_interstitial_batched_device(exs_ctx *ctx, int which, int nk, const int *
  *   eigenvalues IL = 1 .. IU = nstfv of H x = e O x and their vectors)
  * by cuSOLVER zhegvdx with the same index range on the upper triangles.
  * Device form: h_dev[k], o_dev[k] (nmat_k x nmat_k, destroyed),
- * evalfv_dev(nstfv, nk), evecfv_dev[k] (ldv, nstfv).  Synchronous.
+ * evalfv_dev(nstfv, nk), evecfv_dev[k] (ldv, nstfv); evecfv_dev = NULL
+ * computes the eigenvalues only (no vectors: a much smaller work space, as
+ * needed for nmat of tens of thousands).  Synchronous.
  * EXS_ERR_ARG if O is not positive definite or the solver does not
  * converge. */
 int exs_solve_batched_device(exs_ctx *ctx, int nk, const int *nmat_host, exs_complex *const *h_dev,

@@ -168,8 +168,33 @@ def test_ozaki_mod_argument_errors():
     assert rel_fro(h, hr) <= TOL_FRO
 
 
-def test_ozaki_rejects_iora():
-    from exciting_b200.abi import ExsError
+@pytest.mark.parametrize("mode", MODES)
+def test_ozaki_iora_vs_oracle(mode):
+    """iora*: O = A^H (I + h1aa) A (overlapsetup.f90:72-101) takes C = (I +
+    h1aa) A as its right operand (int8 arrays Cr, Ci beside Br, Bi; sigma_C
+    from C's own columns), and the m2effig interstitial term."""
     s = W.si_fcc("text", relativity="iora*")
-    with pytest.raises(ExsError):
-        _setup(s)
+    st = _setup(s, mode=mode)
+    for ik in (1, 6):
+        gk = s.gkset(s.kpoints[ik])
+        h, o = st.hamiltonandoverlapsetup(gk)
+        hr, orf = O.hamiltonandoverlapsetup(s, gk)
+        assert rel_fro(h, hr) <= TOL_FRO, rel_fro(h, hr)
+        assert rel_fro(o, orf) <= TOL_FRO, rel_fro(o, orf)
+        w = sl.eigh(h, o, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
+        wr = sl.eigh(hr, orf, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
+        assert eig_dev(w, wr) <= 1.0
+
+
+def test_ozaki_mod_iora_cube8_batched():
+    s = W.si_cube8(relativity="iora*")
+    gks = s.gksets()[:4]
+    st = _setup(s, mode="ozaki_mod", max_batch=len(gks))
+    out = st.setup_batched(gks)
+    for k in (0, 3):
+        hr, orf = O.hamiltonandoverlapsetup(s, gks[k])
+        h, o = out[k]
+        assert rel_fro(h, hr) <= TOL_FRO and rel_fro(o, orf) <= TOL_FRO
+        w = sl.eigh(h, o, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
+        wr = sl.eigh(hr, orf, eigvals_only=True, subset_by_index=[0, NSTFV - 1])
+        assert eig_dev(w, wr) <= 1.0, np.max(np.abs(w - wr))

@@ -50,3 +50,37 @@ def test_setup_and_solve_cube8_split_precision():
     st.set_precision("ozaki_mod", 0)
     ev, vec = st.setup_and_solve(gks, 40)
     _check(s, gks, ev, vec, 40)
+
+
+def test_solve_values_only_matches_the_vector_solve():
+    """exs_solve_batched_device with evecfv = NULL (values only, the form used
+    for nmat of tens of thousands) gives the eigenvalues of the vector solve."""
+    import ctypes
+
+    import torch
+
+    from exciting_b200.fvsystem import Setup
+    s = W.si_fcc("text")
+    gks = s.gksets()[:2]
+    st = Setup(s, max_batch=2)
+    ev_ref, _ = st.setup_and_solve(gks, 12)
+    nmat = [g.ngp + st.nlotot for g in gks]
+    ig = np.zeros((2, st.ngkmax), dtype=np.int32)
+    vg = np.zeros((2, st.ngkmax, 3))
+    for k, g in enumerate(gks):
+        ig[k, : g.ngp] = g.igpig
+        vg[k, : g.ngp] = g.vgpc.T
+    d_ig, d_vg = torch.from_numpy(ig).cuda(), torch.from_numpy(vg).cuda()
+    d_h = [torch.zeros(2 * m * m, dtype=torch.float64, device="cuda") for m in nmat]
+    d_o = [torch.zeros(2 * m * m, dtype=torch.float64, device="cuda") for m in nmat]
+    st.setup_batched_device([g.ngp for g in gks], d_ig.data_ptr(), d_vg.data_ptr(), [t.data_ptr() for t in d_h],
+                            [t.data_ptr() for t in d_o])
+    st.synchronize()
+    ev = torch.zeros(12 * 2, dtype=torch.float64, device="cuda")
+    hp = (ctypes.c_void_p * 2)(*[t.data_ptr() for t in d_h])
+    op = (ctypes.c_void_p * 2)(*[t.data_ptr() for t in d_o])
+    st._check(st.lib.exs_solve_batched_device(st.ctx, 2, (ctypes.c_int * 2)(*nmat), hp, op, 12,
+                                              ctypes.c_void_p(ev.data_ptr()), None, 0))
+    w = ev.cpu().numpy().reshape(2, 12).T
+    assert np.max(np.abs(w - ev_ref)) <= 1e-10
+    st.close()
