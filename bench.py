@@ -202,11 +202,20 @@ HO_KERNEL = {"ozaki_mod": "oz_res_kernel (residue tiles, tcgen05.mma kind::i8) +
              "ozaki": "oz_mma_kernel (tcgen05.mma kind::i8, FP64 fold), MT contraction phase"}
 
 
+def ho_kernel(precision, kernel_config):
+    if precision == "ozaki_mod" and kernel_config >= 0 and (kernel_config & 8):
+        return HO_KERNEL[precision].replace("oz_res_kernel (residue tiles", "oz_res2_kernel (256 x 64 residue tiles "
+                                            "on SM pairs, tcgen05.mma.cta_group::2")
+    return HO_KERNEL[precision]
+
+
 def ho_tile_cols(precision, kernel_config):
     """Columns of the H/O tiles: 64 or 32 for the modular residue tiles
-    (configuration bit 0), 32 for the slice kernel."""
+    (configuration bit 0; the two-SM tiles of bit 3 are 64 wide), 32 for the
+    slice kernel.  The operation count is that of the 128-row tiles either
+    way: the two-SM tiles' extra tiles below the diagonal are not counted."""
     if precision == "ozaki_mod":
-        return 32 if (kernel_config & 1) else 64
+        return 32 if (kernel_config & 1) and not (kernel_config & 8) else 64
     return 32
 
 
@@ -757,7 +766,7 @@ def run_ours(args, emit=True):
             ops = ozaki_int8_ops(s, gks, products, ho_tile_cols(args.precision, tuned))
             peak8 = _measured_int8_peak(torch)
             a8 = ops / (main_ms * 1e-3) / 1e12
-            roof = {"bound": "tensor", "kernel": HO_KERNEL[args.precision],
+            roof = {"bound": "tensor", "kernel": ho_kernel(args.precision, tuned),
                     "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                     "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
                     "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_PER_K[args.precision] * nk,
@@ -903,18 +912,19 @@ def _lowest_generalized_reduced(h, o, m, nev, torch):
     return w
 
 
-def _ritz_compare(h8, o8, h64, o64, m, nev, torch, nx=64):
-    """Eigenvalue deviation of the split pencil from the FP64 pencil free of
-    the dense solver's own rounding: the FP64 pencil's lowest nx
-    eigenvectors X (Cholesky reduction, dense eigen-solve with vectors through
-    torch's MAGMA backend, X = L^-H Y), then the Ritz values of both pencils
-    on span(X) (nx x nx generalized problems).  For the FP64 pencil they are
-    its eigenvalues; for the split pencil they differ from its eigenvalues by
-    the square of the residual over the gap (second order in the ~1e-13
+def _ritz_compare(pencils, base, m, nev, torch, nx=64):
+    """Eigenvalue deviations between pencils (H, O) free of the dense
+    solver's own rounding: the lowest nx eigenvectors X of pencils[base]
+    (Cholesky reduction, dense eigen-solve with vectors through torch's MAGMA
+    backend, X = L^-H Y), then the Ritz values of every pencil on span(X)
+    (nx x nx generalized problems).  For pencils[base] they are its
+    eigenvalues; for another pencil they differ from its eigenvalues by the
+    square of the residual over the gap (second order in the ~1e-13
     difference of the matrices).  Returns (lowest nev eigenvalues of the
-    dense FP64 solve, FP64 Ritz values, split Ritz values)."""
+    dense solve, [lowest nev Ritz values of each pencil])."""
     c128 = torch.complex128
     prev = torch.backends.cuda.preferred_linalg_library()
+    h64, o64 = pencils[base]
     H = h64.cuda().view(c128).view(m, m)
     L = torch.linalg.cholesky(o64.cuda().view(c128).view(m, m))
     X1 = torch.linalg.solve_triangular(L, H, upper=False)
@@ -948,11 +958,10 @@ def _ritz_compare(h8, o8, h64, o64, m, nev, torch, nx=64):
         Ls = torch.linalg.cholesky(Os)
         Cs = torch.linalg.solve_triangular(Ls, torch.linalg.solve_triangular(Ls, Hs, upper=False).mH, upper=False)
         return torch.linalg.eigvalsh(0.5 * (Cs + Cs.mH))[:nev].cpu().numpy()
-    t64 = ritz(h64, o64)
-    t8 = ritz(h8, o8)
+    th = [ritz(h, o) for h, o in pencils]
     del X
     torch.cuda.empty_cache()
-    return w, t64, t8
+    return w, th
 
 
 def _progress(msg):
@@ -1154,13 +1163,15 @@ def run_large(args):
     args.precision = prec
     if args.kernel_config >= 0:
         st.set_kernel_config(args.kernel_config)
+    # the library's default until a configuration is chosen: two-SM residue tiles with moduli
+    kcfg = args.kernel_config if args.kernel_config >= 0 else (8 if prec == "ozaki_mod" else 0)
     planes, products, dtype_text, prec_text = split_scheme(args, s)
     ms, phase, rows = timed(args.steps, args.warmup, True)
     value = ws * args.steps / (ms * 1e-3)
     _progress("split: %.4f setups/s, phases %s" % (value, list(np.round(phase, 2))))
     m0 = gks[0].ngp + nlotot
     nf = len(gks)
-    fp64_value, phase64, acc, h8 = None, np.zeros(5), None, None
+    fp64_value, phase64, acc, h8, h16 = None, np.zeros(5), None, None, None
     if not args.skip_fp64:
         # ---- Gamma in split precision, kept on the host for the comparison
         one(0)
@@ -1177,6 +1188,19 @@ def run_large(args):
                "rel_fro_H": _rel_fro_host(h8, d_h[: 2 * m0 * m0]),
                "rel_fro_O": _rel_fro_host(o8, d_o[: 2 * m0 * m0])}
         h64, o64 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
+        if not args.skip_eig and rank == 0 and prec == "ozaki_mod" and args.moduli != 16:
+            # ---- a third Gamma pencil, the split path at its widest plan (16 moduli, 52-bit operands):
+            # the eigenvalue leg separates the split path's own error from the FP64 path's rounding
+            try:
+                st.set_precision("ozaki_mod", 16)
+                one(0)
+                st.synchronize()
+                acc.update({"rel_fro_H_16_moduli_vs_fp64": _rel_fro_host(h64, d_h[: 2 * m0 * m0]),
+                            "rel_fro_H_vs_16_moduli": _rel_fro_host(h8, d_h[: 2 * m0 * m0]),
+                            "rel_fro_O_vs_16_moduli": _rel_fro_host(o8, d_o[: 2 * m0 * m0])})
+                h16, o16 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
+            except Exception as e:      # reported, not fatal
+                acc["moduli_16_error"] = str(e)[:300]
     del d_h, d_o
     torch.cuda.empty_cache()
     # ---- end to end through the host-pointer entry point (pinned H and O, 13.6 GB each per k-point)
@@ -1202,7 +1226,7 @@ def run_large(args):
     st.close()
     torch.cuda.empty_cache()
     # ---- eigenvalues of both Gamma pairs
-    if not args.skip_eig and h8 is not None and rank == 0:
+    if args.dense_eig and not args.skip_eig and h8 is not None and rank == 0:
         t0 = time.perf_counter()
         how = "exs_solve_batched_device (cuSOLVER zhegvdx, lowest 40, values only) on each path's H and O"
         w8 = w64 = None
@@ -1224,29 +1248,44 @@ def run_large(args):
                 acc["eigen_solver_error"] = str(e2)[:300]
         if w8 is not None and w64 is not None:
             acc.update({"eigen_solver": how, "eig_solve_s": time.perf_counter() - t0,
-                        "max_abs_eig_dev_lowest40_Ha": float(np.max(np.abs(w8 - w64))),
+                        "max_abs_eig_dev_lowest40_dense_Ha": float(np.max(np.abs(w8 - w64))),
                         "lowest_eigenvalue_Ha": float(w64[0])})
-        try:      # the same comparison free of the dense solver's rounding (Ritz values on one subspace)
+            acc["dense_w64"] = w64
+    if not args.skip_eig and h8 is not None and rank == 0:
+        # the comparison free of the dense solver's rounding: Ritz values of every pencil on one subspace
+        try:
             t1 = time.perf_counter()
-            wd, t64, t8 = _ritz_compare(h8, o8, h64, o64, m0, 40, torch)
-            acc.update({"ritz": "Ritz values of both pencils on the FP64 pencil's lowest 64 eigenvectors "
-                                "(dense MAGMA eigen-solve with vectors); second order in the H/O difference",
+            pencils = [(h8, o8), (h64, o64)] + ([(h16, o16)] if h16 is not None else [])
+            wd, th = _ritz_compare(pencils, 1, m0, 40, torch)
+            t8, t64 = th[0], th[1]
+            dev = float(np.max(np.abs(t8 - t64)))
+            acc.update({"ritz": "Ritz values of each pencil on the FP64 pencil's lowest 64 eigenvectors "
+                                "(dense MAGMA eigen-solve with vectors); second order in the H/O differences",
                         "ritz_s": time.perf_counter() - t1,
-                        "max_abs_eig_dev_lowest40_ritz_Ha": float(np.max(np.abs(t8 - t64))),
+                        "max_abs_eig_dev_lowest40_Ha": dev,
                         "fp64_ritz_vs_dense_Ha": float(np.max(np.abs(t64 - wd))),
-                        "lowest_eigenvalue_Ha": float(wd[0])})
+                        "lowest_eigenvalue_Ha": float(wd[0]),
+                        "gate_abs_1e-8_Ha": bool(dev <= 1e-8)})
+            if h16 is not None:
+                # the widest split plan as the reference: the split path's own error, and the FP64 path's
+                acc.update({"split_vs_16_moduli_Ha": float(np.max(np.abs(t8 - th[2]))),
+                            "fp64_vs_16_moduli_Ha": float(np.max(np.abs(t64 - th[2])))})
+            w64 = acc.pop("dense_w64", None)
             if w64 is not None:
                 acc["dense_solver_repeat_vs_first_Ha"] = float(np.max(np.abs(wd - w64)))
-            acc["gate_abs_1e-8_Ha"] = bool(np.max(np.abs(t8 - t64)) <= 1e-8)
         except Exception as e:      # reported, not fatal
             acc["ritz_error"] = str(e)[:300]
-        _progress("eigenvalues: %s" % json.dumps({k: v for k, v in acc.items() if "eig" in k}))
+        _progress("eigenvalues: %s" % json.dumps({k: v for k, v in acc.items() if "eig" in k or "moduli" in k}))
+    if acc is not None:
+        acc.pop("dense_w64", None)
     if h8 is not None:
         del h8, o8, h64, o64
+    if h16 is not None:
+        del h16, o16
     if ws > 1:
         dist.barrier()
     if rank == 0:
-        ops = ozaki_int8_ops(s, gks_all, products, ho_tile_cols(prec, max(args.kernel_config, 0))) / len(gks_all)   # per k-point
+        ops = ozaki_int8_ops(s, gks_all, products, ho_tile_cols(prec, kcfg)) / len(gks_all)   # per k-point
         fl = main_flops(s, gks_all) / len(gks_all)
         peak8 = _measured_int8_peak(torch)
         peak8s, clk8s = _measured_int8_sustained(torch)
@@ -1283,13 +1322,13 @@ def run_large(args):
                        "kpoints": "Gamma, (1/2,0,0), (1/2,1/2,0), (1/2,1/2,1/2) in turn, one per step",
                        "ngp": [min(g.ngp for g in gks_all), max(g.ngp for g in gks_all)],
                        "nmat": [min(g.ngp for g in gks_all) + nlotot, max(g.ngp for g in gks_all) + nlotot],
-                       "precision": prec_text,
+                       "precision": prec_text, "kernel_config": kcfg,
                        "l2": "working set (A/B planes 30 GB, %d int8 planes of 4 arrays, H/O 27 GB) far above "
                              "L2, no flush" % planes},
             "e2e": e2e,
             "phases_ms_per_step": {"match": phase[0], "h_a_A": phase[1], "mt_contraction": phase[2],
                                    "lo_blocks": phase[3], "total": phase[4]},
-            "roofline": {"bound": "tensor", "kernel": HO_KERNEL[prec],
+            "roofline": {"bound": "tensor", "kernel": ho_kernel(prec, kcfg),
                          "achieved": a8, "peak": peak8s, "unit": "TOP/s (int8)", "frac": a8 / peak8s,
                          "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) back to back for 4 s in this "
                                         "run (sustained, under the power cap: the H/O kernel runs for seconds)",
@@ -1476,6 +1515,8 @@ def main():
                     help="split-precision kernel configuration (0..31); -1: the autotuner's choice (8-atom batch) "
                          "or the library default (216-atom cell)")
     ap.add_argument("--skip-eig", action="store_true", help="cube216: no eigenvalue comparison at Gamma")
+    ap.add_argument("--dense-eig", action="store_true",
+                    help="cube216: also compare the lowest 40 eigenvalues of two dense solves (about 4 minutes)")
     ap.add_argument("--skip-fp64", action="store_true", help="cube216: no FP64 leg and no accuracy comparison")
     ap.add_argument("--skip-cube8", action="store_true", help="cube216: no 8-atom secondary leg")
     ap.add_argument("--slices", type=int, default=7, help="int8 slices per operand (ozaki)")

@@ -412,12 +412,12 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     // either tile width (the upper tiles of ngkmax G+k per k-point)
     size_t res = 0;
     if (mode == EXS_PREC_OZAKI_MOD)
-        for (int q = 0; q < 2; q++) {
-            const int bj = exs::oz_res_cols(q);
-            size_t tiles = 0;
-            for (int ib = 0; ib < (c->ngkmax + 127) / 128; ib++)
+        for (int q : {0, 1, 8}) {
+            const int bj = exs::oz_res_cols(q), bi = exs::oz_res_rows(q);
+            size_t tiles = 0;      // 128-row residue tiles
+            for (int ib = 0; ib < (c->ngkmax + bi - 1) / bi; ib++)
                 for (int jb = 0; jb < (c->ngkmax + bj - 1) / bj; jb++)
-                    if (jb * bj + bj - 1 >= ib * 128) tiles++;
+                    if (jb * bj + bj - 1 >= ib * bi) tiles += bi / 128;
             res = std::max(res, tiles * exs::oz_res_tile_bytes(slices, q) * c->max_batch);
         }
     cudaError_t e = cudaMalloc((void **)&c->d_oz, slot * c->max_batch);
@@ -443,7 +443,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
                                                       &c->oz_mapA[q], &c->oz_mapB[q], &c->oz_mapB2[q]);
     maps_ok = maps_ok && exs::make_oz_atom_maps(c->d_oz, nss, c->npad, kp8, narr, c->d_xs, xgroups, c->oz_lw,
                                                 &c->oz_mapArow, &c->oz_mapX);
-    maps_ok = maps_ok && exs::make_oz_b64_map(c->d_oz, nss, c->npad, kp8, narr, &c->oz_mapB64);
+    maps_ok = maps_ok && exs::make_oz_b64_map(c->d_oz, nss, c->npad, kp8, narr, &c->oz_mapB64, &c->oz_mapB64h);
     if (!maps_ok) {
         cudaFree(c->d_oz); c->d_oz = nullptr;
         cudaFree(c->d_ozscale); c->d_ozscale = nullptr;
@@ -458,9 +458,10 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->oz_sch, c->stream));
         EXS_CUDA(cudaStreamSynchronize(c->stream));
     }
-    {   // a configuration the autotuner chose earlier for this shape
+    {   // a configuration the autotuner chose earlier for this shape; else, with moduli, the two-SM
+        // residue tiles (1.24x the 128 x 64 tiles on the 216-atom cell)
         auto it = c->oz_tuned.find(std::make_tuple((int)mode, c->npad, c->K, slices));
-        c->oz_cfg = it != c->oz_tuned.end() ? it->second : 0;
+        c->oz_cfg = it != c->oz_tuned.end() ? it->second : (mode == EXS_PREC_OZAKI_MOD ? 8 : 0);
     }
     return EXS_OK;
 }
@@ -660,25 +661,27 @@ struct Uploaded {
 };
 
 // Upper tiles (128 rows x 32 columns, 256 x 32 for the two-SM tiles with ib
-// counting pairs of 128-row blocks, 128 x 32 or 128 x 64 for the residue
-// tiles of the modular mode) of the split-precision contraction, in groups of
-// `group` x `group` tiles (row blocks outer, then column blocks, inside a
-// group row blocks outer again): the tiles that run at the same time (one
+// counting pairs of 128-row blocks, 128 x 32, 128 x 64 or 256 x 64 for the
+// residue tiles of the modular mode) of the split-precision contraction, in
+// groups of `group` row blocks x `gcols` column blocks (gcols 0: `group`;
+// row blocks outer, then column blocks, inside a group row blocks outer
+// again): the tiles that run at the same time (one
 // CTA per SM) then read about `group` row blocks of A and `group` column
 // blocks of B instead of one row block and ~148 column blocks, so the L2
 // serves the shared operand chunks and HBM streams each block about
 // (number of groups in its row or column) times instead of once per tile
 // row.  group = 1 is the plain row-major order.
-void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows, int cols, int group = 1)
+void oz_tiles(const std::vector<KDesc> &ks, std::vector<int> &t, int rows, int cols, int group = 1, int gcols = 0)
 {
     t.clear();
+    if (gcols <= 0) gcols = group;
     for (size_t k = 0; k < ks.size(); k++) {
         const int n = ks[k].ngp;
         const int nib = (n + rows - 1) / rows, njb = (n + cols - 1) / cols;
         for (int gi = 0; gi < nib; gi += group)
-            for (int gj = 0; gj < njb; gj += group)
+            for (int gj = 0; gj < njb; gj += gcols)
                 for (int ib = gi; ib < std::min(nib, gi + group); ib++)
-                    for (int jb = gj; jb < std::min(njb, gj + group); jb++)
+                    for (int jb = gj; jb < std::min(njb, gj + gcols); jb++)
                         if (jb * cols + cols - 1 >= ib * rows) {
                             t.push_back((int)k);
                             t.push_back(ib);
@@ -718,7 +721,16 @@ void pack_tables(exs_ctx *c, const std::vector<KDesc> &ks, std::vector<int> &ozt
     ozt.clear();
     std::vector<int> ozat;
     if (c->oz_on()) {
-        if (c->oz_sch.mod)   // grouped 12 x 12 (about one wave of 148 CTAs)
+        if (c->oz_sch.mod && (c->oz_cfg & 8)) {   // 256-row pairs, grouped 6 x 12, as two 128-row tiles each
+            std::vector<int> pairs;
+            oz_tiles(ks, pairs, 256, 64, 6, 12);
+            for (size_t t = 0; t < pairs.size(); t += 3)
+                for (int r = 0; r < 2; r++) {
+                    ozt.push_back(pairs[t]);
+                    ozt.push_back(2 * pairs[t + 1] + r);
+                    ozt.push_back(pairs[t + 2]);
+                }
+        } else if (c->oz_sch.mod)   // grouped 12 x 12 (about one wave of 148 CTAs)
             oz_tiles(ks, ozt, 128, exs::oz_res_cols(c->oz_cfg), 12);
         else
             oz_tiles(ks, ozt, (c->oz_cfg & 8) ? 256 : 128, 32);
@@ -878,8 +890,8 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
         EXS_CUDA(exs::launch_oz_split(p, u.d_k, (int)ks.size(), c->oz_sch, c->kp8, 1, s));
         const int q = c->oz_cfg;
         if (c->oz_sch.mod)   // residue tiles (one K chunk per stage: the maps of configuration 1), then the CRT
-            EXS_CUDA(exs::launch_oz_res(q, &c->oz_mapA[1], &c->oz_mapB[1], &c->oz_mapB64, p, u.d_k, u.d_oztiles,
-                                        u.noztiles, c->oz_sch, c->kp8, c->d_res, s));
+            EXS_CUDA(exs::launch_oz_res(q, &c->oz_mapA[1], &c->oz_mapB[1], &c->oz_mapB64, &c->oz_mapB64h, p, u.d_k,
+                                        u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, c->d_res, s));
         else
             EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,
                                         u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, s));
@@ -991,7 +1003,7 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
     int best_q = 0;
     for (int q = 0; q < exs::OZ_NCFG; q++) {
         if ((q & 8) && (q & 2)) continue;   // the two-SM tiles have no persistent form
-        if ((q & 8) && c->oz_sch.mod) continue;   // moduli: residue tiles, no two-SM form
+        if ((q & 8) && c->oz_sch.mod && (q & 1)) continue;   // moduli: the two-SM residue tiles are 64 wide
         if ((q & 16) && (q & 4)) continue;  // no per-atom int8 kernel to make persistent
         c->oz_cfg = q;
         Uploaded u{};                        // the tile list depends on the configuration

@@ -90,8 +90,12 @@ struct OzScheme {
     float fc[3][OZ_MAX_MODULI];        // 2^13, 2^26, 2^39 mod p
     unsigned long long c[OZ_MAX_MODULI];
     // the H/O products (residue tiles): C_m = round(2^96 y_m / p_m) in 32-bit
-    // words (low first), recombined exactly but for 2^-64 M; fin96 = M 2^-64 2^-2b
+    // words (low first); the recombination reads the 64 bits below the top
+    // crt_shift bits of the 96-bit sum (the bits that |X| <= 2^2b leaves as
+    // sign copies when M is far above 2^2b), exact but for 2^-(64+crt_shift) M;
+    // fin96 = M 2^-(64+crt_shift) 2^-2b
     unsigned c96[3][OZ_MAX_MODULI];
+    int crt_shift;
     double fin96;
 };
 
@@ -288,6 +292,7 @@ struct exs_ctx {
     CUtensorMap oz_mapA[exs::OZ_NCFG], oz_mapB[exs::OZ_NCFG];   // TMA views of d_oz per pipeline configuration
     CUtensorMap oz_mapB2[exs::OZ_NCFG];                            // half-B views (two-SM tiles)
     CUtensorMap oz_mapB64;                                         // B operand of the 128 x 64 residue tiles
+    CUtensorMap oz_mapB64h;                                        // one CTA's half of it in the 256 x 64 pairs
     uint8_t *d_res = nullptr;                                      // residue tiles of the modular H/O products
     size_t res_bytes = 0;
     int oz_cfg = 0;                   // pipeline configuration of the split-precision kernel
@@ -348,11 +353,12 @@ cudaError_t launch_oz_split(const DevParams &p, const KDesc *d_k, int nk, const 
 cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme &sch, cudaStream_t s);
 cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, int norm, cudaStream_t s);
 cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
-                          const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch,
-                          int kp8, uint8_t *res, cudaStream_t s);
+                          const CUtensorMap *mapB64h, const DevParams &p, const KDesc *d_k, const void *d_tiles,
+                          int ntiles, const OzScheme &sch, int kp8, uint8_t *res, cudaStream_t s);
 int oz_res_cols(int cfg);
+int oz_res_rows(int cfg);
 size_t oz_res_tile_bytes(int n, int cfg);
-bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64);
+bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64, CUtensorMap *mapB64h);
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,
                            const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
                            const OzAtomArgs &xa, cudaStream_t s);

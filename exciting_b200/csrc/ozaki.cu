@@ -1332,7 +1332,8 @@ oz_mma2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
 // the residues x = v mod p in [0, p) of the four values
 // v = Re H (r0 + i1), Im H (r1 - i0), Re O (r2 + i3), Im O (r3 - i2) as bytes.
 // oz_crt_kernel recombines the n residues of each value by the Chinese
-// remainder theorem with 96-bit constants (exact but for 2^-64 M; no
+// remainder theorem with 96-bit constants (exact but for 2^-(64+s) M, the
+// 64-bit window s bits below the top of the sum, s = 0 up to 13 moduli; no
 // headroom bits needed), scales by sigma_A(i) sigma_B(j) (sigma_A(j) for O),
 // adds the interstitial term and writes the upper triangle and its mirror.
 // With no running sums in tensor memory the tile is 128 x 64 (N = 256: r and
@@ -1543,6 +1544,194 @@ oz_res_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
     }
 }
 
+// ------------------------------------------------------------ two-SM residue tiles
+// A cluster of two CTAs computes a 256 (G_i) x BJ (G_j) tile with
+// tcgen05.mma.cta_group::2 (M = 256, N = 4 BJ): each CTA holds its own 128
+// rows of Ar, Ai and two of the four B arrays (CTA 0: Br, Bi; CTA 1: Ar, Ai
+// of the G_j, or Cr, Ci with iora*), 48 KB per K chunk instead of 64 KB, and
+// each CTA writes the residues of its own 128 rows as the 128-row residue
+// tile 2 pair + rank.  CTA 0 issues the MMAs; its full barriers count the
+// bytes of both CTAs' copies; MMA completion is signalled to both CTAs
+// (multicast commit); both CTAs' epilogues report to CTA 0's barrier.
+template <int BJ>
+struct Res2Cfg {
+    static constexpr int N = 4 * BJ;                     // MMA N: both CTAs' halves of B
+    static constexpr int ABOX = 2 * OZ_TILE;             // this CTA's Ar, Ai (128 rows), one K chunk
+    static constexpr int BBOX = 2 * BJ * OZ_CHUNK;       // this CTA's two arrays of B (BJ rows each)
+    static constexpr int STAGE = ABOX + BBOX;
+    static constexpr int NST = (192 * 1024) / STAGE;     // BJ 64: 4 stages of 48 KB
+    static constexpr int SMEM = NST * STAGE + 1024;
+};
+
+template <int BJ>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
+oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapBh, DevParams p,
+               const KDesc *ks, const int *tiles, const __grid_constant__ OzScheme sch, int kp8, uint8_t *res)
+{
+    using C = Res2Cfg<BJ>;
+    using R = ResCfg<BJ>;
+    constexpr int NST = C::NST, N = C::N;
+    static_assert(2 * N <= OZ_TMEM_COLS, "r and i fit tensor memory");
+    const int S = sch.n;
+    const int nch = kp8 / OZ_CHUNK;
+    extern __shared__ __align__(1024) uint8_t oz_smem[];
+    __shared__ uint64_t full[NST], empty[NST], accf, acce;
+    __shared__ uint32_t tmem_sh;
+    __shared__ int abort_sh;
+    volatile int *abort = &abort_sh;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_ctarank();
+    const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
+    // the 128-row tile list holds the pair's tiles at 2 pair and 2 pair + 1 (this CTA's: blockIdx.x),
+    // with the same k-point and column block
+    const int tile = blockIdx.x;
+    const KDesc kd = ks[tiles[3 * tile]];
+    const int i0 = tiles[3 * tile + 1] * OZ_BM, j0 = tiles[3 * tile + 2] * BJ;
+
+    if (warp == 3) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(OZ_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int q = 0; q < NST; q++) {
+            mbar_init(&full[q], 1);      // CTA 0: one arrive (with the bytes of both CTAs)
+            mbar_init(&empty[q], 1);
+        }
+        mbar_init(&accf, 1);
+        mbar_init(&acce, 16);            // CTA 0: eight epilogue warps in each CTA
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync_all();                  // the peer's barriers are initialised before anyone signals them
+    tc_fence_after();
+    const uint32_t tbase = tmem_sh;
+
+    if (warp < 2) {
+        // ------------------------------------------------ TMA producers (both CTAs)
+        if (lane == 0) {
+            const int role = warp;       // 0: this CTA's A rows, 1: this CTA's half of B
+            uint32_t fills[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) fills[q] = 0;
+            int st = 0;
+            bool bad = false;
+            const int slot = kd.oz_slot;
+            for (int g = 0; g < S && !bad; g++)
+                for (int kb = 0; kb < nch; kb++) {
+                    if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
+                        bad = true;
+                        break;
+                    }
+                    if (rank == 0 && role == 0) mbar_expect_tx(&full[st], 2 * C::STAGE);
+                    const uint32_t bar = smem_u32(&full[st]);
+                    if (role == 0)
+                        tma_load_5d_2sm(sbase + st * C::STAGE, &mapA, 0, i0, oz_narr(p.relativity) - 2, kb, slot * S + g,
+                                        bar);
+                    else
+                        tma_load_5d_2sm(sbase + st * C::STAGE + C::ABOX, &mapBh, 0, j0, 2 * (int)rank, kb,
+                                        slot * S + g, bar);
+                    fills[st]++;
+                    st = (st + 1 == NST) ? 0 : st + 1;
+                }
+            // CTA 0: copies already issued (both CTAs') must land before the pair goes away;
+            // CTA 1 stopped issuing at least one bounded wait ago
+            if (bad && rank == 0)
+                for (int q = 0; q < NST; q++)
+                    if (fills[q] > 0) mbar_drain(&full[q], (fills[q] - 1) & 1);
+        }
+    } else if (warp == 3) {
+        // ------------------------------------------------ MMA issuer (CTA 0)
+        if (lane == 0 && rank == 0) {
+            const uint32_t idesc = umma_idesc_i8(256, N);
+            uint32_t uses[NST];
+#pragma unroll
+            for (int q = 0; q < NST; q++) uses[q] = 0;
+            int st = 0;
+            bool bad = false;
+            for (int g = 0; g < S && !bad; g++) {
+                // the epilogues of both CTAs must have read the previous modulus
+                if (g > 0 && !mbar_wait_ab(&acce, (g - 1) & 1, abort, sch.wait)) {
+                    bad = true;
+                    break;
+                }
+                tc_fence_after();
+                for (int kb = 0; kb < nch; kb++) {
+                    if (!mbar_wait_ab(&full[st], uses[st] & 1, abort, sch.wait)) {
+                        bad = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = sbase + st * C::STAGE;
+#pragma unroll
+                    for (int q = 0; q < OZ_CHUNK / 32; q++) {
+                        const uint64_t bd = umma_desc_sw128(sa + C::ABOX + q * 32);
+                        const uint32_t acc = (kb == 0 && q == 0) ? 0u : 1u;
+                        umma_i8_2sm(tbase, umma_desc_sw128(sa + q * 32), bd, idesc, acc);
+                        umma_i8_2sm(tbase + N, umma_desc_sw128(sa + OZ_TILE + q * 32), bd, idesc, acc);
+                    }
+                    umma_commit_2sm(&empty[st]);
+                    uses[st]++;
+                    st = (st + 1 == NST) ? 0 : st + 1;
+                }
+                if (!bad) umma_commit_2sm(&accf);
+            }
+            if (bad)
+                for (int q = 0; q < NST; q++)
+                    if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
+        }
+    } else if (warp >= 4) {
+        // ------------------------------------------------ epilogue (both CTAs, warps 4..11)
+        const int qd = warp & 3;
+        const int half = (warp - 4) >> 2;                           // 0: Re H, Im H; 1: Re O, Im O
+        const int row = qd * 32 + lane;
+        const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
+        const uint32_t acce0 = mapa_shared(smem_u32(&acce), 0);
+        uint8_t *tres = res + (size_t)tile * S * R::MOD_BYTES;
+        for (int g = 0; g < S; g++) {
+            if (!__all_sync(0xffffffffu, mbar_wait_ab(&accf, g & 1, abort, sch.wait))) break;
+            tc_fence_after();
+            const int pm = sch.p[g], mg = sch.mg[g];
+            uint4 out[2][R::NCH];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int o = 2 * half + k, oi = o ^ 1;
+                const bool minus = (o & 1) != 0;
+#pragma unroll
+                for (int c = 0; c < R::NCH; c++) {
+                    uint32_t rv[16], iv[16];
+                    tm_ld16(t_lane + o * BJ + c * 16, rv);
+                    tm_ld16(t_lane + N + oi * BJ + c * 16, iv);
+                    tm_wait_ld();
+                    out[k][c] = make_uint4(oz_res4(rv, iv, 0, minus, pm, mg), oz_res4(rv, iv, 4, minus, pm, mg),
+                                           oz_res4(rv, iv, 8, minus, pm, mg), oz_res4(rv, iv, 12, minus, pm, mg));
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_remote(acce0);               // CTA 0's barrier (also from CTA 0)
+            uint8_t *gres = tres + (size_t)g * R::MOD_BYTES;
+#pragma unroll
+            for (int k = 0; k < 2; k++)
+#pragma unroll
+                for (int c = 0; c < R::NCH; c++)
+                    *reinterpret_cast<uint4 *>(gres + ((size_t)((2 * half + k) * R::NCH + c) * 128 + row) * 16) =
+                        out[k][c];
+        }
+    }
+    if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync_all();                  // neither CTA leaves while the pair still uses its memory
+    if (warp == 3) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(OZ_TMEM_COLS));
+    }
+}
+
 // Eight values from their n residues (w[m]: the 8 bytes of modulus m): per
 // value the 96-bit fixed-point sum t = sum_m x_m C_m (mod 2^96), C_m =
 // round(2^96 y_m / p_m) in three 32-bit words (three 32 x 32 -> 64-bit
@@ -1571,7 +1760,8 @@ __device__ __forceinline__ void oz_crt8(const OzScheme &sch, const uint2 (&w)[OZ
     for (int e = 0; e < 8; e++) {
         const unsigned long long a1 = a[e][1] + (a[e][0] >> 32);
         const unsigned long long a2 = a[e][2] + (a1 >> 32);
-        const unsigned long long top = (a2 << 32) | (a1 & 0xffffffffull);
+        const unsigned long long top = (((a2 << 32) | (a1 & 0xffffffffull)) << sch.crt_shift) |
+                                       ((a[e][0] & 0xffffffffull) >> (32 - sch.crt_shift));
         v[e] = (double)(long long)top * sch.fin96;
     }
 }
@@ -1740,7 +1930,10 @@ int oz_mod_plan(int n, int K, int kx, OzScheme *sch)
     for (int m = 0; m < n; m++) M *= (double)OZ_MODULI[m];
     s.fin = std::ldexp(M, -64 - h - 2 * b);
     s.finx = std::ldexp(M, -64 - h - b - bx);
-    s.fin96 = std::ldexp(M, -64 - 2 * b);
+    // |X| / M <= 2^(2b - log2 M) (1 + eps)^2 < 2^-(crt_shift + 1): the window's top bit is still the sign;
+    // its lowest bit, 2^(32 - crt_shift) units of 2^-96, stays above the constants' rounding (< 2^11 units)
+    s.crt_shift = std::max(0, std::min(20, (int)std::floor(oz_log2_modulus(n) - 1e-9 - 2.0 * b - 3.0)));
+    s.fin96 = std::ldexp(M, -64 - s.crt_shift - 2 * b);
     for (int m = 0; m < n; m++) {
         const int p = OZ_MODULI[m];
         long long mm = 1;   // (M / p) mod p
@@ -1872,20 +2065,44 @@ static cudaError_t launch_res_bj(const CUtensorMap *mapA, const CUtensorMap *map
     return cudaGetLastError();
 }
 
+static cudaError_t launch_res2(const CUtensorMap *mapA, const CUtensorMap *mapBh, const DevParams &p,
+                               const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
+                               uint8_t *res, cudaStream_t s)
+{
+    constexpr int BJ = 64;
+    constexpr int smem = Res2Cfg<BJ>::SMEM;
+    if (ntiles % 2 != 0) return cudaErrorInvalidValue;      // whole pairs
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(oz_res2_kernel<BJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    });
+    if (e != cudaSuccess) return e;
+    oz_res2_kernel<BJ><<<ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapBh, p, d_k, (const int *)d_tiles, sch, kp8, res);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    oz_crt_kernel<BJ><<<dim3(ntiles, 2 * (BJ / 8)), 128, 0, s>>>(p, d_k, (const int *)d_tiles, sch, res);
+    return cudaGetLastError();
+}
+
 // The modular H/O products: residue tiles then their recombination.
 // Configuration bit 0: 128 x 32 tiles (two accumulator pairs) instead of
-// 128 x 64; bit 1: persistent residue kernel (one CTA per SM).
+// 128 x 64; bit 1: persistent residue kernel (one CTA per SM); bit 3:
+// 256 x 64 tiles on two SMs (the tile list then holds each pair's two
+// 128-row tiles next to each other; bits 0 and 1 do not apply).
 cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
-                          const DevParams &p, const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch,
-                          int kp8, uint8_t *res, cudaStream_t s)
+                          const CUtensorMap *mapB64h, const DevParams &p, const KDesc *d_k, const void *d_tiles,
+                          int ntiles, const OzScheme &sch, int kp8, uint8_t *res, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
+    if (cfg & 8) return launch_res2(mapA, mapB64h, p, d_k, d_tiles, ntiles, sch, kp8, res, s);
     const bool persistent = (cfg & 2) != 0;
     if (cfg & 1) return launch_res_bj<32>(mapA, mapB32, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
     return launch_res_bj<64>(mapA, mapB64, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
 }
 
-int oz_res_cols(int cfg) { return (cfg & 1) ? 32 : 64; }
+int oz_res_cols(int cfg) { return (cfg & 1) && !(cfg & 8) ? 32 : 64; }
+
+int oz_res_rows(int cfg) { return (cfg & 8) ? 256 : 128; }
 
 size_t oz_res_tile_bytes(int n, int cfg) { return (size_t)n * 4 * 128 * oz_res_cols(cfg); }
 
@@ -1944,8 +2161,9 @@ bool make_oz_tensor_maps(void *base, size_t nss, int npad, int kp8, int kch, int
 }
 
 // The B operand of the 128 x 64 residue tiles: the four arrays of 64 G rows,
-// one 128-byte K chunk (the 5D view of make_oz_tensor_maps, box {128, 64, 4, 1, 1}).
-bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64)
+// one 128-byte K chunk (the 5D view of make_oz_tensor_maps, box {128, 64, 4, 1, 1});
+// and the half of it that one CTA of a 256 x 64 pair holds (box {128, 64, 2, 1, 1}).
+bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64, CUtensorMap *mapB64h)
 {
     typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -1962,7 +2180,11 @@ bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtens
                                    (cuuint64_t)narr * npad * kp8};
     const cuuint32_t es[5] = {1, 1, 1, 1, 1};
     const cuuint32_t box[5] = {OZ_CHUNK, 64, OZ_NARR, 1, 1};
+    const cuuint32_t boxh[5] = {OZ_CHUNK, 64, 2, 1, 1};
     return encode(mapB64, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+           encode(mapB64h, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, base, dims, strides, boxh, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }

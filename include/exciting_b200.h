@@ -330,16 +330,18 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
 
 /* Selects the split-precision kernel configuration by index
  * (0 .. EXS_OZ_NCONFIG-1) instead of the autotuner's choice: bit 0 picks the
- * pipeline shape of the H/O tiles (two 96 KB stages or four 48 KB stages),
- * bit 1 a persistent launch (one block per SM walking the tiles) of the H/O
- * tiles instead of one block per tile, bit 2 the same for the per-atom
- * products (h_a A, APW-lo rows), bit 3 two-SM H/O tiles (a pair of blocks
- * computes 256 x 32 with the B operand split between them; bit 1 is then
- * ignored), bit 4 the products h_a A and the APW-lo rows of H in native
- * FP64 (DMMA) instead of int8 slices (bit 2 is then ignored; only the H/O
- * contraction stays split).  Configurations with the same bit 4 give
- * bit-identical results; the two arithmetics for h_a A agree to FP64
- * rounding. */
+ * pipeline shape of the H/O tiles (slices: two 96 KB stages or four 48 KB
+ * stages; moduli: 128 x 64 or 128 x 32 residue tiles), bit 1 a persistent
+ * launch (one block per SM walking the tiles) of the H/O tiles instead of
+ * one block per tile, bit 2 the same for the per-atom products (h_a A,
+ * APW-lo rows), bit 3 two-SM H/O tiles (a pair of blocks computes 256 x 32,
+ * or 256 x 64 residue tiles with moduli, with the B operand split between
+ * them; bit 1, and with moduli bit 0, is then ignored), bit 4 the products
+ * h_a A and the APW-lo rows of H in native FP64 (DMMA) instead of int8
+ * slices (bit 2 is then ignored; only the H/O contraction stays split).
+ * Configurations with the same bit 4 give bit-identical results; the two
+ * arithmetics for h_a A agree to FP64 rounding.  Until the autotuner or
+ * this call chooses, exs_set_precision sets 0 for slices and 8 for moduli. */
 #define EXS_OZ_NCONFIG 32
 int exs_set_kernel_config(exs_ctx *ctx, int config);
 

@@ -120,12 +120,18 @@ def c96(ps):
     return out
 
 
-def emulate_crt(X, Y, ps):
+def crt_shift(ps, b):
+    """Bits the recombination skips below the top of the 96-bit sum: the sign
+    copies that |X| <= 2^2b leaves when M is far above 2^2b (at most 20)."""
+    return max(0, min(20, math.floor(sum(math.log2(p) for p in ps) - 1e-9 - 2 * b - 3)))
+
+
+def emulate_crt(X, Y, ps, sh=0):
     """Integer product X^T Y as the residue tiles give it: per modulus the
     residue x = (X^T Y) mod p in [0, p) (the kernel's multiply-high reduction
     of the exact int32 sum, then moved into [0, p)), recombined by the 96-bit
     sum of oz_crt_kernel (three 64-bit accumulators, carries at the end); the
-    result is the signed top 64 bits (2^64 X / M)."""
+    result is the signed 64-bit window sh bits below the top (2^(64+sh) X / M)."""
     C = c96(ps)
     a = [np.zeros((X.shape[1], Y.shape[1]), dtype=np.uint64) for _ in range(3)]
     for p, cw in zip(ps, C):
@@ -140,6 +146,7 @@ def emulate_crt(X, Y, ps):
         a1 = a[1] + (a[0] >> np.uint64(32))
         a2 = a[2] + (a1 >> np.uint64(32))
         top = (a2 << np.uint64(32)) | (a1 & np.uint64(0xffffffff))
+        top = (top << np.uint64(sh)) | ((a[0] & np.uint64(0xffffffff)) >> np.uint64(32 - sh))
     return top.view(np.int64)
 
 
@@ -170,24 +177,30 @@ def test_emulated_fold_reconstructs_per_atom_products(n):
             assert abs(err) <= (rsum[i, j] / 2 + 1) * M, (i, j)
 
 
-@pytest.mark.parametrize("n", [8, 12, 13, 16])
+@pytest.mark.parametrize("n", [8, 12, 13, 14, 15, 16])
 def test_emulated_crt_reconstructs_ho_products(n):
-    """The residue tiles' recombination: |X| <= 2^(2b), the top 64 bits of the
-    96-bit sum equal floor(2^64 X / M) up to one unit (the constants' rounding
-    is below 2^-85 of M)."""
+    """The residue tiles' recombination: |X| <= 2^(2b), the 64-bit window sh
+    bits below the top of the 96-bit sum equals floor(2^(64+sh) X / M) up to
+    one unit (the constants' rounding is below 2^-85 of M), and that unit,
+    M 2^-(64+sh), is at most 2^(2b-58): the window keeps ~58 bits of the
+    bound 2^2b for every plan (with sh = 0, 16 moduli and b = 52 would keep
+    only 42)."""
     rng = np.random.default_rng(100 + n)
     K = 300
     ps, _, b, _, _ = plan(n, K // 2, 8)
+    sh = crt_shift(ps, b)
+    assert sh == 0 or n >= 14
     X = _norm_columns(rng, K, 5, b)
     Y = _norm_columns(rng, K, 4, b)
     Y[:, 0] = -X[:, 0]
-    top = emulate_crt(X, Y, ps)
+    top = emulate_crt(X, Y, ps, sh)
     M = math.prod(ps)
+    assert M <= 2 ** (2 * b - 58 + 64 + sh)
     for i in range(X.shape[1]):
         for j in range(Y.shape[1]):
             exact = sum(int(a) * int(bb) for a, bb in zip(X[:, i], Y[:, j]))
-            assert 2 * abs(exact) < M
-            assert abs(int(top[i, j]) * M - exact * 2 ** 64) <= 2 * M, (i, j)
+            assert 2 ** (sh + 1) * abs(exact) < M
+            assert abs(int(top[i, j]) * M - exact * 2 ** (64 + sh)) <= 2 * M, (i, j)
 
 
 def _split_scaled(Z, b):
@@ -228,10 +241,11 @@ def _emulated_setup(s, gk, apwalm):
     XA = np.concatenate([ar, ai])                   # [Ar; Ai]
     YH = [np.concatenate([br, bi]), np.concatenate([bi, -br])]    # Re H, Im H
     YO = [np.concatenate([ar, ai]), np.concatenate([ai, -ar])]    # Re O, Im O
-    scale = M * 2.0 ** (-64 - 2 * b)
+    sh = crt_shift(ps, b)
+    scale = M * 2.0 ** (-64 - sh - 2 * b)
     out = []
     for Ys, sy in ((YH, sb), (YO, sa)):
-        parts = [emulate_crt(XA, Y, ps).astype(np.float64) * scale for Y in Ys]
+        parts = [emulate_crt(XA, Y, ps, sh).astype(np.float64) * scale for Y in Ys]
         out.append((parts[0] + 1j * parts[1]) * np.outer(sa, sy))
     Bx = np.concatenate([s.mt_aa[:, :, a] @ apwi[a] for a in range(s.natmtot)])
     return out[0], out[1], A.conj().T @ Bx, A.conj().T @ A, B, Bx
@@ -311,6 +325,7 @@ def test_emulated_eight_atom_eigenvalues():
     ar, ai, sa = _split_scaled(A, b)
     br, bi, sb = _split_scaled(B, b)
     XA = np.concatenate([ar, ai])
+    assert crt_shift(ps, b) == 0
     scale = M * 2.0 ** (-64 - 2 * b)
     got = []
     for Ys, sy in (([np.concatenate([br, bi]), np.concatenate([bi, -br])], sb),
