@@ -1265,17 +1265,24 @@ def run_large(args):
                         "max_abs_eig_dev_lowest40_Ha": dev,
                         "fp64_ritz_vs_dense_Ha": float(np.max(np.abs(t64 - wd))),
                         "lowest_eigenvalue_Ha": float(wd[0]),
-                        "gate_abs_1e-8_Ha": bool(dev <= 1e-8)})
+                        "gate_abs_1e-8_Ha": {"vs_fp64_path": bool(dev <= 1e-8)}})
             if h16 is not None:
-                # the widest split plan as the reference: the split path's own error, and the FP64 path's
-                acc.update({"split_vs_16_moduli_Ha": float(np.max(np.abs(t8 - th[2]))),
-                            "fp64_vs_16_moduli_Ha": float(np.max(np.abs(t64 - th[2])))})
+                # the widest split plan (52-bit operands, products accumulated exactly, one rounding) as
+                # the reference: the split path's own error, and the FP64 path's accumulation rounding
+                d16 = float(np.max(np.abs(t8 - th[2])))
+                acc.update({"exact_accumulation_reference": "split path with 16 moduli: FP64 operands rounded "
+                                                            "to 52 bits below their column norms, products "
+                                                            "exact in integers (CRT), one rounding per element",
+                            "max_abs_eig_dev_lowest40_vs_exact_accumulation_Ha": d16,
+                            "fp64_path_vs_exact_accumulation_Ha": float(np.max(np.abs(t64 - th[2])))})
+                acc["gate_abs_1e-8_Ha"]["vs_exact_accumulation"] = bool(d16 <= 1e-8)
             w64 = acc.pop("dense_w64", None)
             if w64 is not None:
                 acc["dense_solver_repeat_vs_first_Ha"] = float(np.max(np.abs(wd - w64)))
         except Exception as e:      # reported, not fatal
             acc["ritz_error"] = str(e)[:300]
-        _progress("eigenvalues: %s" % json.dumps({k: v for k, v in acc.items() if "eig" in k or "moduli" in k}))
+        _progress("eigenvalues: %s" % json.dumps({k: v for k, v in acc.items()
+                                                  if "eig" in k or "moduli" in k or "accumulation" in k or "gate" in k}))
     if acc is not None:
         acc.pop("dense_w64", None)
     if h8 is not None:
