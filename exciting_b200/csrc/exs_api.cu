@@ -1002,7 +1002,7 @@ int exs_autotune(exs_ctx *c, int nk, const int *ngp, const int *igpig_dev, const
     float best = 0.f;
     int best_q = 0;
     for (int q = 0; q < exs::OZ_NCFG; q++) {
-        if ((q & 8) && (q & 2)) continue;   // the two-SM tiles have no persistent form
+        if ((q & 8) && (q & 2) && !c->oz_sch.mod) continue;   // the slices' two-SM tiles have no persistent form
         if ((q & 8) && c->oz_sch.mod && (q & 1)) continue;   // moduli: the two-SM residue tiles are 64 wide
         if ((q & 16) && (q & 4)) continue;  // no per-atom int8 kernel to make persistent
         c->oz_cfg = q;

@@ -1566,7 +1566,8 @@ struct Res2Cfg {
 template <int BJ>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
 oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapBh, DevParams p,
-               const KDesc *ks, const int *tiles, const __grid_constant__ OzScheme sch, int kp8, uint8_t *res)
+               const KDesc *ks, const int *tiles, int npairs, const __grid_constant__ OzScheme sch, int kp8,
+               uint8_t *res)
 {
     using C = Res2Cfg<BJ>;
     using R = ResCfg<BJ>;
@@ -1583,11 +1584,11 @@ oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t rank = cluster_ctarank();
     const uint32_t sbase = (smem_u32(oz_smem) + 1023u) & ~1023u;
-    // the 128-row tile list holds the pair's tiles at 2 pair and 2 pair + 1 (this CTA's: blockIdx.x),
-    // with the same k-point and column block
-    const int tile = blockIdx.x;
-    const KDesc kd = ks[tiles[3 * tile]];
-    const int i0 = tiles[3 * tile + 1] * OZ_BM, j0 = tiles[3 * tile + 2] * BJ;
+    // pairs pair0, pair0 + npc, ...: one pair per cluster, or (persistent launch) the clusters walk the
+    // list together, so that the pairs running at one time share row and column blocks in the L2; the
+    // 128-row tile list holds the pair's tiles at 2 pair and 2 pair + 1 (this CTA's: 2 pair + rank), with
+    // the same k-point and column block
+    const int pair0 = (int)(blockIdx.x >> 1), npc = (int)(gridDim.x >> 1);
 
     if (warp == 3) {
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_sh)),
@@ -1619,24 +1620,28 @@ oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             for (int q = 0; q < NST; q++) fills[q] = 0;
             int st = 0;
             bool bad = false;
-            const int slot = kd.oz_slot;
-            for (int g = 0; g < S && !bad; g++)
-                for (int kb = 0; kb < nch; kb++) {
-                    if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
-                        bad = true;
-                        break;
+            for (int pr = pair0; pr < npairs && !bad; pr += npc) {
+                const int tile = 2 * pr + (int)rank;
+                const int slot = ks[tiles[3 * tile]].oz_slot;
+                const int i0 = tiles[3 * tile + 1] * OZ_BM, j0 = tiles[3 * tile + 2] * BJ;
+                for (int g = 0; g < S && !bad; g++)
+                    for (int kb = 0; kb < nch; kb++) {
+                        if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
+                            bad = true;
+                            break;
+                        }
+                        if (rank == 0 && role == 0) mbar_expect_tx(&full[st], 2 * C::STAGE);
+                        const uint32_t bar = smem_u32(&full[st]);
+                        if (role == 0)
+                            tma_load_5d_2sm(sbase + st * C::STAGE, &mapA, 0, i0, oz_narr(p.relativity) - 2, kb,
+                                            slot * S + g, bar);
+                        else
+                            tma_load_5d_2sm(sbase + st * C::STAGE + C::ABOX, &mapBh, 0, j0, 2 * (int)rank, kb,
+                                            slot * S + g, bar);
+                        fills[st]++;
+                        st = (st + 1 == NST) ? 0 : st + 1;
                     }
-                    if (rank == 0 && role == 0) mbar_expect_tx(&full[st], 2 * C::STAGE);
-                    const uint32_t bar = smem_u32(&full[st]);
-                    if (role == 0)
-                        tma_load_5d_2sm(sbase + st * C::STAGE, &mapA, 0, i0, oz_narr(p.relativity) - 2, kb, slot * S + g,
-                                        bar);
-                    else
-                        tma_load_5d_2sm(sbase + st * C::STAGE + C::ABOX, &mapBh, 0, j0, 2 * (int)rank, kb,
-                                        slot * S + g, bar);
-                    fills[st]++;
-                    st = (st + 1 == NST) ? 0 : st + 1;
-                }
+            }
             // CTA 0: copies already issued (both CTAs') must land before the pair goes away;
             // CTA 1 stopped issuing at least one bounded wait ago
             if (bad && rank == 0)
@@ -1650,35 +1655,36 @@ oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             uint32_t uses[NST];
 #pragma unroll
             for (int q = 0; q < NST; q++) uses[q] = 0;
-            int st = 0;
+            int st = 0, u = 0;
             bool bad = false;
-            for (int g = 0; g < S && !bad; g++) {
-                // the epilogues of both CTAs must have read the previous modulus
-                if (g > 0 && !mbar_wait_ab(&acce, (g - 1) & 1, abort, sch.wait)) {
-                    bad = true;
-                    break;
-                }
-                tc_fence_after();
-                for (int kb = 0; kb < nch; kb++) {
-                    if (!mbar_wait_ab(&full[st], uses[st] & 1, abort, sch.wait)) {
+            for (int pr = pair0; pr < npairs && !bad; pr += npc)
+                for (int g = 0; g < S && !bad; g++, u++) {
+                    // the epilogues of both CTAs must have read the previous modulus
+                    if (u > 0 && !mbar_wait_ab(&acce, (u - 1) & 1, abort, sch.wait)) {
                         bad = true;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t sa = sbase + st * C::STAGE;
+                    for (int kb = 0; kb < nch; kb++) {
+                        if (!mbar_wait_ab(&full[st], uses[st] & 1, abort, sch.wait)) {
+                            bad = true;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sa = sbase + st * C::STAGE;
 #pragma unroll
-                    for (int q = 0; q < OZ_CHUNK / 32; q++) {
-                        const uint64_t bd = umma_desc_sw128(sa + C::ABOX + q * 32);
-                        const uint32_t acc = (kb == 0 && q == 0) ? 0u : 1u;
-                        umma_i8_2sm(tbase, umma_desc_sw128(sa + q * 32), bd, idesc, acc);
-                        umma_i8_2sm(tbase + N, umma_desc_sw128(sa + OZ_TILE + q * 32), bd, idesc, acc);
+                        for (int q = 0; q < OZ_CHUNK / 32; q++) {
+                            const uint64_t bd = umma_desc_sw128(sa + C::ABOX + q * 32);
+                            const uint32_t acc = (kb == 0 && q == 0) ? 0u : 1u;
+                            umma_i8_2sm(tbase, umma_desc_sw128(sa + q * 32), bd, idesc, acc);
+                            umma_i8_2sm(tbase + N, umma_desc_sw128(sa + OZ_TILE + q * 32), bd, idesc, acc);
+                        }
+                        umma_commit_2sm(&empty[st]);
+                        uses[st]++;
+                        st = (st + 1 == NST) ? 0 : st + 1;
                     }
-                    umma_commit_2sm(&empty[st]);
-                    uses[st]++;
-                    st = (st + 1 == NST) ? 0 : st + 1;
+                    if (!bad) umma_commit_2sm(&accf);
                 }
-                if (!bad) umma_commit_2sm(&accf);
-            }
             if (bad)
                 for (int q = 0; q < NST; q++)
                     if (uses[q] > 0) mbar_drain(&empty[q], (uses[q] - 1) & 1);
@@ -1690,36 +1696,43 @@ oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
         const int row = qd * 32 + lane;
         const uint32_t t_lane = tbase + ((uint32_t)(qd * 32) << 16);
         const uint32_t acce0 = mapa_shared(smem_u32(&acce), 0);
-        uint8_t *tres = res + (size_t)tile * S * R::MOD_BYTES;
-        for (int g = 0; g < S; g++) {
-            if (!__all_sync(0xffffffffu, mbar_wait_ab(&accf, g & 1, abort, sch.wait))) break;
-            tc_fence_after();
-            const int pm = sch.p[g], mg = sch.mg[g];
-            uint4 out[2][R::NCH];
-#pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int o = 2 * half + k, oi = o ^ 1;
-                const bool minus = (o & 1) != 0;
-#pragma unroll
-                for (int c = 0; c < R::NCH; c++) {
-                    uint32_t rv[16], iv[16];
-                    tm_ld16(t_lane + o * BJ + c * 16, rv);
-                    tm_ld16(t_lane + N + oi * BJ + c * 16, iv);
-                    tm_wait_ld();
-                    out[k][c] = make_uint4(oz_res4(rv, iv, 0, minus, pm, mg), oz_res4(rv, iv, 4, minus, pm, mg),
-                                           oz_res4(rv, iv, 8, minus, pm, mg), oz_res4(rv, iv, 12, minus, pm, mg));
+        int u = 0;
+        bool bad = false;
+        for (int pr = pair0; pr < npairs && !bad; pr += npc) {
+            uint8_t *tres = res + (size_t)(2 * pr + (int)rank) * S * R::MOD_BYTES;
+            for (int g = 0; g < S; g++, u++) {
+                if (!__all_sync(0xffffffffu, mbar_wait_ab(&accf, u & 1, abort, sch.wait))) {
+                    bad = true;
+                    break;
                 }
+                tc_fence_after();
+                const int pm = sch.p[g], mg = sch.mg[g];
+                uint4 out[2][R::NCH];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int o = 2 * half + k, oi = o ^ 1;
+                    const bool minus = (o & 1) != 0;
+#pragma unroll
+                    for (int c = 0; c < R::NCH; c++) {
+                        uint32_t rv[16], iv[16];
+                        tm_ld16(t_lane + o * BJ + c * 16, rv);
+                        tm_ld16(t_lane + N + oi * BJ + c * 16, iv);
+                        tm_wait_ld();
+                        out[k][c] = make_uint4(oz_res4(rv, iv, 0, minus, pm, mg), oz_res4(rv, iv, 4, minus, pm, mg),
+                                               oz_res4(rv, iv, 8, minus, pm, mg), oz_res4(rv, iv, 12, minus, pm, mg));
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_remote(acce0);           // CTA 0's barrier (also from CTA 0)
+                uint8_t *gres = tres + (size_t)g * R::MOD_BYTES;
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+#pragma unroll
+                    for (int c = 0; c < R::NCH; c++)
+                        *reinterpret_cast<uint4 *>(gres + ((size_t)((2 * half + k) * R::NCH + c) * 128 + row) * 16) =
+                            out[k][c];
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_remote(acce0);               // CTA 0's barrier (also from CTA 0)
-            uint8_t *gres = tres + (size_t)g * R::MOD_BYTES;
-#pragma unroll
-            for (int k = 0; k < 2; k++)
-#pragma unroll
-                for (int c = 0; c < R::NCH; c++)
-                    *reinterpret_cast<uint4 *>(gres + ((size_t)((2 * half + k) * R::NCH + c) * 128 + row) * 16) =
-                        out[k][c];
         }
     }
     if (tid == 0 && *abort) atomicOr(p.err, DEV_ERR_TIMEOUT);
@@ -2067,17 +2080,36 @@ static cudaError_t launch_res_bj(const CUtensorMap *mapA, const CUtensorMap *map
 
 static cudaError_t launch_res2(const CUtensorMap *mapA, const CUtensorMap *mapBh, const DevParams &p,
                                const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
-                               uint8_t *res, cudaStream_t s)
+                               uint8_t *res, bool persistent, cudaStream_t s)
 {
     constexpr int BJ = 64;
     constexpr int smem = Res2Cfg<BJ>::SMEM;
     if (ntiles % 2 != 0) return cudaErrorInvalidValue;      // whole pairs
+    const int npairs = ntiles / 2;
     static std::atomic<unsigned long long> attr{0};
     cudaError_t e = once_per_device(attr, [] {
         return cudaFuncSetAttribute(oz_res2_kernel<BJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     });
     if (e != cudaSuccess) return e;
-    oz_res2_kernel<BJ><<<ntiles, OZ_THREADS, smem, s>>>(*mapA, *mapBh, p, d_k, (const int *)d_tiles, sch, kp8, res);
+    int ncl = npairs;
+    if (persistent) {   // as many pairs as can be resident at once (one cluster of two per SM pair)
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(ntiles);
+        lc.blockDim = dim3(OZ_THREADS);
+        lc.dynamicSmemBytes = smem;
+        lc.stream = s;
+        int act = 0;
+        if (cudaOccupancyMaxActiveClusters(&act, (void *)oz_res2_kernel<BJ>, &lc) != cudaSuccess || act < 1) {
+            (void)cudaGetLastError();
+            int dev = 0, nsm = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            act = nsm / 2;
+        }
+        ncl = std::min(npairs, act);
+    }
+    oz_res2_kernel<BJ><<<2 * ncl, OZ_THREADS, smem, s>>>(*mapA, *mapBh, p, d_k, (const int *)d_tiles, npairs, sch,
+                                                          kp8, res);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     oz_crt_kernel<BJ><<<dim3(ntiles, 2 * (BJ / 8)), 128, 0, s>>>(p, d_k, (const int *)d_tiles, sch, res);
@@ -2086,15 +2118,16 @@ static cudaError_t launch_res2(const CUtensorMap *mapA, const CUtensorMap *mapBh
 
 // The modular H/O products: residue tiles then their recombination.
 // Configuration bit 0: 128 x 32 tiles (two accumulator pairs) instead of
-// 128 x 64; bit 1: persistent residue kernel (one CTA per SM); bit 3:
-// 256 x 64 tiles on two SMs (the tile list then holds each pair's two
-// 128-row tiles next to each other; bits 0 and 1 do not apply).
+// 128 x 64; bit 1: persistent residue kernel (one CTA per SM, or one
+// cluster per SM pair); bit 3: 256 x 64 tiles on two SMs (the tile list then
+// holds each pair's two 128-row tiles next to each other; bit 0 does not
+// apply).
 cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
                           const CUtensorMap *mapB64h, const DevParams &p, const KDesc *d_k, const void *d_tiles,
                           int ntiles, const OzScheme &sch, int kp8, uint8_t *res, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
-    if (cfg & 8) return launch_res2(mapA, mapB64h, p, d_k, d_tiles, ntiles, sch, kp8, res, s);
+    if (cfg & 8) return launch_res2(mapA, mapB64h, p, d_k, d_tiles, ntiles, sch, kp8, res, (cfg & 2) != 0, s);
     const bool persistent = (cfg & 2) != 0;
     if (cfg & 1) return launch_res_bj<32>(mapA, mapB32, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
     return launch_res_bj<64>(mapA, mapB64, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);

@@ -336,7 +336,8 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
  * one block per tile, bit 2 the same for the per-atom products (h_a A,
  * APW-lo rows), bit 3 two-SM H/O tiles (a pair of blocks computes 256 x 32,
  * or 256 x 64 residue tiles with moduli, with the B operand split between
- * them; bit 1, and with moduli bit 0, is then ignored), bit 4 the products
+ * them; with slices bit 1 is then ignored, with moduli bit 0 is ignored and
+ * bit 1 makes the pairs persistent, one cluster per SM pair), bit 4 the products
  * h_a A and the APW-lo rows of H in native FP64 (DMMA) instead of int8
  * slices (bit 2 is then ignored; only the H/O contraction stays split).
  * Configurations with the same bit 4 give bit-identical results; the two

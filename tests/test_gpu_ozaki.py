@@ -108,6 +108,33 @@ def test_ozaki_mod_cube8_all_kpoints_eigenvalues():
     assert worst <= TOL_EIG, worst
 
 
+def test_ozaki_mod_eigenvalues_with_generated_integrals():
+    """A physically scaled case: the MT integrals generated from radial
+    functions and a potential by exs_hmlint (not seeded random matrices), so
+    that the lowest eigenvalues of the 2-atom cell lie between -10 Ha and 0;
+    for every k-point of the mesh the modular split path's lowest 40 within
+    the absolute 1e-8 Ha of the oracle's."""
+    import copy
+    s = W.si_fcc("shipped")
+    rad = W.mt_radial(s)
+    gks = s.gksets()
+    st = _setup(s, mode="ozaki_mod", max_batch=len(gks))
+    aa, loa, lolo = st.hmlint(rad)
+    st.set_scf_inputs(keep_mt=True)
+    s2 = copy.copy(s)
+    s2.mt_aa, s2.mt_loa, s2.mt_lolo = aa, loa, lolo
+    out = st.setup_batched(gks)
+    lowest = []
+    for gk, (h, o) in zip(gks, out):
+        hr, orf = O.hamiltonandoverlapsetup(s2, gk)
+        n = min(NSTFV, h.shape[0])
+        w = sl.eigh(h, o, eigvals_only=True, subset_by_index=[0, n - 1])
+        wr = sl.eigh(hr, orf, eigvals_only=True, subset_by_index=[0, n - 1])
+        assert eig_dev(w, wr) <= 1.0, np.max(np.abs(w - wr))
+        lowest.append(wr[0])
+    assert -20.0 < min(lowest) < 0.0
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_ozaki_two_species_vs_oracle(mode):
     """Different bases per species (apword 1 and 2, lmaxmat < lmaxapw, lo on
