@@ -155,6 +155,7 @@ int exs_ctx_destroy(exs_ctx *c)
         if (p) cudaFree(p);
     if (c->d_oz) cudaFree(c->d_oz);
     if (c->d_res) cudaFree(c->d_res);
+    if (c->d_pace) cudaFree(c->d_pace);
     if (c->d_ozscale) cudaFree(c->d_ozscale);
     if (c->d_xs) cudaFree(c->d_xs);
     if (c->d_xsig) cudaFree(c->d_xsig);
@@ -396,6 +397,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     const size_t slot = exs::oz_slot_bytes(slices, c->npad, kp8, narr);
     if (c->d_oz) { cudaFree(c->d_oz); c->d_oz = nullptr; }
     if (c->d_res) { cudaFree(c->d_res); c->d_res = nullptr; c->res_bytes = 0; }
+    if (c->d_pace) { cudaFree(c->d_pace); c->d_pace = nullptr; }
     if (c->d_ozscale) { cudaFree(c->d_ozscale); c->d_ozscale = nullptr; }
     if (c->d_xs) { cudaFree(c->d_xs); c->d_xs = nullptr; }
     if (c->d_xsig) { cudaFree(c->d_xsig); c->d_xsig = nullptr; }
@@ -424,6 +426,7 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
     if (e == cudaSuccess && res > 0) {
         e = cudaMalloc((void **)&c->d_res, res);
         if (e == cudaSuccess) c->res_bytes = res;
+        if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_pace, exs::oz_pace_bytes());
     }
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ozscale, sizeof(double) * 3 * c->npad * c->max_batch);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xs, xgroups * 128 * c->oz_lw);
@@ -891,7 +894,7 @@ int enqueue_setup(exs_ctx *c, const std::vector<KDesc> &ks, const Uploaded &u, b
         const int q = c->oz_cfg;
         if (c->oz_sch.mod)   // residue tiles (one K chunk per stage: the maps of configuration 1), then the CRT
             EXS_CUDA(exs::launch_oz_res(q, &c->oz_mapA[1], &c->oz_mapB[1], &c->oz_mapB64, &c->oz_mapB64h, p, u.d_k,
-                                        u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, c->d_res, s));
+                                        u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, c->d_res, c->d_pace, s));
         else
             EXS_CUDA(exs::launch_oz_mma(q, &c->oz_mapA[q], (q & 8) ? &c->oz_mapB2[q] : &c->oz_mapB[q], p, u.d_k,
                                         u.d_oztiles, u.noztiles, c->oz_sch, c->kp8, s));

@@ -294,6 +294,7 @@ struct exs_ctx {
     CUtensorMap oz_mapB64;                                         // B operand of the 128 x 64 residue tiles
     CUtensorMap oz_mapB64h;                                        // one CTA's half of it in the 256 x 64 pairs
     uint8_t *d_res = nullptr;                                      // residue tiles of the modular H/O products
+    int *d_pace = nullptr;                                         // pacing of the persistent pair kernel
     size_t res_bytes = 0;
     int oz_cfg = 0;                   // pipeline configuration of the split-precision kernel
     // per-atom products of the split-precision path (h_a A, loa A)
@@ -354,9 +355,10 @@ cudaError_t launch_oz_x(const DevParams &p, const OzAtomArgs &xa, const OzScheme
 cudaError_t launch_oz_colnorm(const DevParams &p, const KDesc *d_k, int nk, int which, int norm, cudaStream_t s);
 cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
                           const CUtensorMap *mapB64h, const DevParams &p, const KDesc *d_k, const void *d_tiles,
-                          int ntiles, const OzScheme &sch, int kp8, uint8_t *res, cudaStream_t s);
+                          int ntiles, const OzScheme &sch, int kp8, uint8_t *res, int *pace, cudaStream_t s);
 int oz_res_cols(int cfg);
 int oz_res_rows(int cfg);
+size_t oz_pace_bytes();
 size_t oz_res_tile_bytes(int n, int cfg);
 bool make_oz_b64_map(void *base, size_t nss, int npad, int kp8, int narr, CUtensorMap *mapB64, CUtensorMap *mapB64h);
 cudaError_t launch_oz_atom(int cfg, const CUtensorMap *mapArow, const CUtensorMap *mapX, const DevParams &p,

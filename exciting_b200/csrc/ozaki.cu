@@ -1553,6 +1553,43 @@ oz_res_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
 // tile 2 pair + rank.  CTA 0 issues the MMAs; its full barriers count the
 // bytes of both CTAs' copies; MMA completion is signalled to both CTAs
 // (multicast commit); both CTAs' epilogues report to CTA 0's barrier.
+// Pacing of the persistent pair kernel: every cluster publishes, every
+// OZ_PACE_CHUNKS K chunks it issues, its step count in pace[cluster] and,
+// before a new step, waits until the slowest cluster is at most OZ_PACE_LAG
+// steps behind, so that the pairs running at one time read the same row and
+// column blocks within a few MB of each other's position and the L2 serves
+// the repeats.  The wait is a hint, not a dependency: it gives up after
+// OZ_PACE_CYCLES (a cluster that is not resident, or a slow one, delays the
+// others by that much per step at most) and never raises an error.  A
+// finished cluster publishes INT_MAX.
+constexpr int OZ_PACE_CHUNKS = 32;
+constexpr int OZ_PACE_LAG = 2;
+constexpr long long OZ_PACE_CYCLES = 40000;
+constexpr int OZ_PACE_MAX = 1024;                 // clusters (ints of the pace array)
+
+__device__ __forceinline__ int ld_relaxed_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_gpu(int *p, int v)
+{
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void oz_pace(int *pace, int me, int ncl, int step)
+{
+    const long long t0 = clock64();
+    while (true) {
+        int mn = 0x7fffffff;
+        for (int c = 0; c < ncl; c++) mn = min(mn, ld_relaxed_gpu(pace + c));
+        if (mn >= step - OZ_PACE_LAG || clock64() - t0 > OZ_PACE_CYCLES) break;
+    }
+    st_relaxed_gpu(pace + me, step);
+}
+
 template <int BJ>
 struct Res2Cfg {
     static constexpr int N = 4 * BJ;                     // MMA N: both CTAs' halves of B
@@ -1567,7 +1604,7 @@ template <int BJ>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(OZ_THREADS, 1)
 oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapBh, DevParams p,
                const KDesc *ks, const int *tiles, int npairs, const __grid_constant__ OzScheme sch, int kp8,
-               uint8_t *res)
+               uint8_t *res, int *pace)
 {
     using C = Res2Cfg<BJ>;
     using R = ResCfg<BJ>;
@@ -1618,14 +1655,16 @@ oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
             uint32_t fills[NST];
 #pragma unroll
             for (int q = 0; q < NST; q++) fills[q] = 0;
-            int st = 0;
+            int st = 0, chunk = 0;
             bool bad = false;
+            const bool pacer = pace != nullptr && rank == 0 && role == 0;
             for (int pr = pair0; pr < npairs && !bad; pr += npc) {
                 const int tile = 2 * pr + (int)rank;
                 const int slot = ks[tiles[3 * tile]].oz_slot;
                 const int i0 = tiles[3 * tile + 1] * OZ_BM, j0 = tiles[3 * tile + 2] * BJ;
                 for (int g = 0; g < S && !bad; g++)
-                    for (int kb = 0; kb < nch; kb++) {
+                    for (int kb = 0; kb < nch; kb++, chunk++) {
+                        if (pacer && chunk % OZ_PACE_CHUNKS == 0) oz_pace(pace, pair0, npc, chunk / OZ_PACE_CHUNKS);
                         if (fills[st] > 0 && !mbar_wait_ab(&empty[st], (fills[st] - 1) & 1, abort, sch.wait)) {
                             bad = true;
                             break;
@@ -1642,6 +1681,7 @@ oz_res2_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__
                         st = (st + 1 == NST) ? 0 : st + 1;
                     }
             }
+            if (pacer) st_relaxed_gpu(pace + pair0, 0x7fffffff);     // done: nobody waits for this cluster
             // CTA 0: copies already issued (both CTAs') must land before the pair goes away;
             // CTA 1 stopped issuing at least one bounded wait ago
             if (bad && rank == 0)
@@ -2080,7 +2120,7 @@ static cudaError_t launch_res_bj(const CUtensorMap *mapA, const CUtensorMap *map
 
 static cudaError_t launch_res2(const CUtensorMap *mapA, const CUtensorMap *mapBh, const DevParams &p,
                                const KDesc *d_k, const void *d_tiles, int ntiles, const OzScheme &sch, int kp8,
-                               uint8_t *res, bool persistent, cudaStream_t s)
+                               uint8_t *res, int *pace, bool persistent, cudaStream_t s)
 {
     constexpr int BJ = 64;
     constexpr int smem = Res2Cfg<BJ>::SMEM;
@@ -2106,10 +2146,14 @@ static cudaError_t launch_res2(const CUtensorMap *mapA, const CUtensorMap *mapBh
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
             act = nsm / 2;
         }
-        ncl = std::min(npairs, act);
+        ncl = std::min(std::min(npairs, act), OZ_PACE_MAX);
+        if (pace) {
+            e = cudaMemsetAsync(pace, 0, sizeof(int) * ncl, s);
+            if (e != cudaSuccess) return e;
+        }
     }
     oz_res2_kernel<BJ><<<2 * ncl, OZ_THREADS, smem, s>>>(*mapA, *mapBh, p, d_k, (const int *)d_tiles, npairs, sch,
-                                                          kp8, res);
+                                                          kp8, res, persistent ? pace : nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     oz_crt_kernel<BJ><<<dim3(ntiles, 2 * (BJ / 8)), 128, 0, s>>>(p, d_k, (const int *)d_tiles, sch, res);
@@ -2124,10 +2168,10 @@ static cudaError_t launch_res2(const CUtensorMap *mapA, const CUtensorMap *mapBh
 // apply).
 cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *mapB32, const CUtensorMap *mapB64,
                           const CUtensorMap *mapB64h, const DevParams &p, const KDesc *d_k, const void *d_tiles,
-                          int ntiles, const OzScheme &sch, int kp8, uint8_t *res, cudaStream_t s)
+                          int ntiles, const OzScheme &sch, int kp8, uint8_t *res, int *pace, cudaStream_t s)
 {
     if (ntiles <= 0) return cudaSuccess;
-    if (cfg & 8) return launch_res2(mapA, mapB64h, p, d_k, d_tiles, ntiles, sch, kp8, res, (cfg & 2) != 0, s);
+    if (cfg & 8) return launch_res2(mapA, mapB64h, p, d_k, d_tiles, ntiles, sch, kp8, res, pace, (cfg & 2) != 0, s);
     const bool persistent = (cfg & 2) != 0;
     if (cfg & 1) return launch_res_bj<32>(mapA, mapB32, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
     return launch_res_bj<64>(mapA, mapB64, p, d_k, d_tiles, ntiles, sch, kp8, res, persistent, s);
@@ -2136,6 +2180,8 @@ cudaError_t launch_oz_res(int cfg, const CUtensorMap *mapA, const CUtensorMap *m
 int oz_res_cols(int cfg) { return (cfg & 1) && !(cfg & 8) ? 32 : 64; }
 
 int oz_res_rows(int cfg) { return (cfg & 8) ? 256 : 128; }
+
+size_t oz_pace_bytes() { return sizeof(int) * OZ_PACE_MAX; }
 
 size_t oz_res_tile_bytes(int n, int cfg) { return (size_t)n * 4 * 128 * oz_res_cols(cfg); }
 
