@@ -204,8 +204,9 @@ HO_KERNEL = {"ozaki_mod": "oz_res_kernel (residue tiles, tcgen05.mma kind::i8) +
 
 def ho_kernel(precision, kernel_config):
     if precision == "ozaki_mod" and kernel_config >= 0 and (kernel_config & 8):
+        how = "persistent paced clusters, " if kernel_config & 2 else ""
         return HO_KERNEL[precision].replace("oz_res_kernel (residue tiles", "oz_res2_kernel (256 x 64 residue tiles "
-                                            "on SM pairs, tcgen05.mma.cta_group::2")
+                                            "on SM pairs, %stcgen05.mma.cta_group::2" % how)
     return HO_KERNEL[precision]
 
 
@@ -1163,8 +1164,8 @@ def run_large(args):
     args.precision = prec
     if args.kernel_config >= 0:
         st.set_kernel_config(args.kernel_config)
-    # the library's default until a configuration is chosen: two-SM residue tiles with moduli
-    kcfg = args.kernel_config if args.kernel_config >= 0 else (8 if prec == "ozaki_mod" else 0)
+    # the library's default until a configuration is chosen: paced persistent two-SM residue tiles with moduli
+    kcfg = args.kernel_config if args.kernel_config >= 0 else (10 if prec == "ozaki_mod" else 0)
     planes, products, dtype_text, prec_text = split_scheme(args, s)
     ms, phase, rows = timed(args.steps, args.warmup, True)
     value = ws * args.steps / (ms * 1e-3)

@@ -461,10 +461,10 @@ int exs_set_precision(exs_ctx *c, int mode, int slices)
         EXS_CUDA(exs::launch_oz_x(c->params(), c->oz_atom_args(), c->oz_sch, c->stream));
         EXS_CUDA(cudaStreamSynchronize(c->stream));
     }
-    {   // a configuration the autotuner chose earlier for this shape; else, with moduli, the two-SM
-        // residue tiles (1.24x the 128 x 64 tiles on the 216-atom cell)
+    {   // a configuration the autotuner chose earlier for this shape; else, with moduli, the paced
+        // persistent two-SM residue tiles (1.5x the 128 x 64 tiles on the 216-atom cell)
         auto it = c->oz_tuned.find(std::make_tuple((int)mode, c->npad, c->K, slices));
-        c->oz_cfg = it != c->oz_tuned.end() ? it->second : (mode == EXS_PREC_OZAKI_MOD ? 8 : 0);
+        c->oz_cfg = it != c->oz_tuned.end() ? it->second : (mode == EXS_PREC_OZAKI_MOD ? 10 : 0);
     }
     return EXS_OK;
 }

@@ -342,7 +342,8 @@ int exs_autotune(exs_ctx *ctx, int nk, const int *ngp_host, const int *igpig_dev
  * slices (bit 2 is then ignored; only the H/O contraction stays split).
  * Configurations with the same bit 4 give bit-identical results; the two
  * arithmetics for h_a A agree to FP64 rounding.  Until the autotuner or
- * this call chooses, exs_set_precision sets 0 for slices and 8 for moduli. */
+ * this call chooses, exs_set_precision sets 0 for slices and 10 (persistent
+ * two-SM residue tiles) for moduli. */
 #define EXS_OZ_NCONFIG 32
 int exs_set_kernel_config(exs_ctx *ctx, int config);
 
