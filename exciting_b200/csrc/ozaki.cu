@@ -1558,12 +1558,14 @@ oz_res_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ 
 // before a new step, waits until the slowest cluster is at most OZ_PACE_LAG
 // steps behind, so that the pairs running at one time read the same row and
 // column blocks within a few MB of each other's position and the L2 serves
-// the repeats.  The wait is a hint, not a dependency: it gives up after
+// the repeats.  216-atom cell, setups/s by (lag, chunks): (1, 32) 0.955,
+// (2, 32) 0.944, (2, 16) 0.943, (2, 64) 0.935, (4, 16) 0.915; a 200,000
+// cycle cap 0.943.  The wait is a hint, not a dependency: it gives up after
 // OZ_PACE_CYCLES (a cluster that is not resident, or a slow one, delays the
 // others by that much per step at most) and never raises an error.  A
 // finished cluster publishes INT_MAX.
 constexpr int OZ_PACE_CHUNKS = 32;
-constexpr int OZ_PACE_LAG = 2;
+constexpr int OZ_PACE_LAG = 1;
 constexpr long long OZ_PACE_CYCLES = 40000;
 constexpr int OZ_PACE_MAX = 1024;                 // clusters (ints of the pace array)
 
