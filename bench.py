@@ -180,6 +180,24 @@ def split_scheme(args, sys_):
             "in the 64-bit recombination; tcgen05), Chinese-remainder recombination" % (n, b, h))
 
 
+def ozaki_tiles128(g, cols=64):
+    """128-row upper residue tiles of one k-point (128 x cols)."""
+    n = g.ngp
+    return sum(1 for ib in range((n + 127) // 128) for jb in range((n + cols - 1) // cols)
+               if jb * cols + cols - 1 >= ib * 128)
+
+
+def residue_bytes(sys_, g, moduli):
+    """Algorithmic DRAM bytes of the residue kernel for one k-point: the
+    residues of Ar, Ai, Br, Bi (npad rows x kp8 bytes per modulus) read once
+    and the residues of the four H/O values written once (128 x 64 bytes per
+    value, tile and modulus)."""
+    K = sum(sys_.basis.napw_atom(a) for a in range(sys_.natmtot))
+    kp8 = (K + 255) // 256 * 256
+    npad = (g.ngp + 63) // 64 * 64
+    return 4.0 * moduli * npad * kp8 + 4.0 * moduli * 128 * 64 * ozaki_tiles128(g)
+
+
 def ozaki_int8_ops(sys_, gks, products, cols=32):
     """int8 MMA operations the split-precision H/O kernel issues: per 128 x
     cols tile (B operand [Br|Bi|Ar|Ai] -> N = 4 cols), `products` int8
@@ -220,19 +238,27 @@ def ho_tile_cols(precision, kernel_config):
     return 32
 
 
-# DRAM bytes per k-point of the dominant kernel, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) of the 8-atom batch cut to a
-# few k-points; the traffic grows with the k-points (each k-point's operands
-# are read once and its H/O written once), so a launch's traffic is this
-# figure times its k-points:
-#   split precision, oz_mma_kernel<OZ_HO,2,2>, 2 k-points: 131.6 MB read +
-#     35.2 MB written with 7 slices, 227.2 MB read + 37.4 MB written with 13
-#     moduli;
+# DRAM bytes of the dominant kernel, from ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum) of the same kernels; a kernel change needs a new
+# capture.  The 8-atom batch, per k-point (a 2 k-point capture divided by 2;
+# the traffic grows with the k-points: each k-point's operands are read once
+# and its H/O written once):
+#   slices, oz_mma_kernel<OZ_HO,2,2>, 7 slices: 131.6 MB read + 35.2 MB written;
+#   moduli, oz_res_kernel<64> (configurations without bit 3): 218.4 MB read +
+#     47.4 MB written; oz_res2_kernel<64> (bit 3): 253.9 MB + 56.9 MB;
 #   FP64, zgemm_dmma_kernel<1> + <2>, 6 k-points: 673.5 MB read + 143.1 MB written.
-# The figures are reported with the capture they come from; a kernel change
-# needs a new capture.
+# The 216-atom cell, per k-point (one launch, captured at full size in one
+# pass): oz_res2_kernel<64> in configuration 10 (paced persistent pairs),
+# 1.23 TB read + 19.6 GB written; configuration 8, 4.61 TB + 19.9 GB.
 PROFILED_DRAM_BYTES_PER_K = {"ozaki": (131.6e6 + 35.2e6) / 2, "fp64": (673.5e6 + 143.1e6) / 6,
-                             "ozaki_mod": (227.2e6 + 37.4e6) / 2}
+                             "ozaki_mod": (218.4e6 + 47.4e6) / 2, "ozaki_mod_pairs": (253.9e6 + 56.9e6) / 2}
+PROFILED_DRAM_BYTES_216 = {10: 1.23e12 + 19.6e9, 8: 4.61e12 + 19.9e9}
+
+
+def profiled_traffic_per_k(precision, kernel_config):
+    if precision == "ozaki_mod" and kernel_config >= 0 and (kernel_config & 8):
+        return PROFILED_DRAM_BYTES_PER_K["ozaki_mod_pairs"]
+    return PROFILED_DRAM_BYTES_PER_K[precision]
 
 
 def main_bytes(sys_, gks, precision, slices):
@@ -770,7 +796,7 @@ def run_ours(args, emit=True):
             roof = {"bound": "tensor", "kernel": ho_kernel(args.precision, tuned),
                     "achieved": a8, "peak": peak8, "unit": "TOP/s (int8)", "frac": a8 / peak8,
                     "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) measured in this run",
-                    "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_PER_K[args.precision] * nk,
+                    "int8_ops_per_step": ops, "traffic": profiled_traffic_per_k(args.precision, tuned) * nk,
                     "traffic_note": "bytes per launch: ncu dram__bytes_read+write of a 2 k-point capture scaled "
                                     "by k-points; algorithmic %.3g" % main_bytes(s, gks, args.precision, planes),
                     "fp64_equivalent": {"achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
@@ -1341,9 +1367,10 @@ def run_large(args):
                          "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) back to back for 4 s in this "
                                         "run (sustained, under the power cap: the H/O kernel runs for seconds)",
                          "peak_burst": peak8, "frac_of_burst": a8 / peak8, "peak_sustained_clocks": clk8s,
-                         "int8_ops_per_step": ops, "traffic": None,
-                         "traffic_note": "not captured at this size (an ncu replay of a multi-second launch); "
-                                         "the 8-atom leg's capture is in the profiles",
+                         "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_216.get(kcfg),
+                         "traffic_note": "bytes per launch of the residue kernel: ncu dram__bytes_read+write of "
+                                         "one full-size launch (one pass); algorithmic %.3g (residue planes read "
+                                         "once, residues written once)" % residue_bytes(s, gks_all[0], planes),
                          "fp64_equivalent": {"achieved": fl / (mt_ms * 1e-3) / 1e12, "peak": peak64,
                                              "unit": "TFLOP/s", "frac": fl / (mt_ms * 1e-3) / 1e12 / peak64}},
             "cpu_baseline": cpu,
