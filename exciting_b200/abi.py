@@ -52,6 +52,7 @@ SIGNATURES = {
     "exs_set_wait_limit": ([P, ctypes.c_longlong], c_int),
     "exs_sort_index_1d": ([c_int, P, c_int, P], c_int),
     "exs_match": ([P, c_int, P, P, P, P], c_int),
+    "exs_wavefmt": ([P, c_int, P, c_int, P, c_int, c_int, c_int, P, c_int, P], c_int),
     "exs_hamiltonandoverlapsetup": ([P, c_int, P, P, P, P, P], c_int),
     "exs_setup_batched": ([P, c_int, P, P, P, P, P], c_int),
     "exs_setup_batched_device": ([P, c_int, P, P, P, P, P], c_int),

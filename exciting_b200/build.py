@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libexciting_b200.so")
 
-SOURCES = ["exs_api.cu", "match.cu", "setup_f64.cu", "ozaki.cu", "forcek.cu", "noalloc.cu", "interstitial.cu", "solve.cu", "mtint.cu", "rttddft.cu", "pmat.cu"]
+SOURCES = ["exs_api.cu", "match.cu", "setup_f64.cu", "ozaki.cu", "forcek.cu", "noalloc.cu", "interstitial.cu", "solve.cu", "mtint.cu", "rttddft.cu", "pmat.cu", "wavefmt.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
          "--expt-relaxed-constexpr", "-ccbin", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"]

@@ -182,6 +182,7 @@ int exs_ctx_destroy(exs_ctx *c)
     exs::mt_release(c);
     exs::rt_release(c);
     exs::pm_release(c);
+    exs::wf_release(c);
     if (c->d_eval) cudaFree(c->d_eval);
     if (c->d_evec) cudaFree(c->d_evec);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);

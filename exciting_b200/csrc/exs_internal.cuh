@@ -269,6 +269,7 @@ struct exs_ctx {
     // real-time TDDFT Hamiltonian update (rttddft.cu): momentum matrices, work space
     void *rt = nullptr;
     void *pm = nullptr;                  // momentum-matrix generation (pmat.cu)
+    void *wf = nullptr;                  // muffin-tin wavefunction coefficients (wavefmt.cu)
     // match-only buffers
     double *d_match_in = nullptr;      // gpc, tpgpc (ngkmax*3 doubles)
     exs_complex *d_match_sf = nullptr; // sfacgp (ngkmax, natmtot)
@@ -346,6 +347,7 @@ int rt_reserve_pmat(exs_ctx *c, int nk, const int *nmat, exs_complex **d_p, size
 double rt_combine_ms(exs_ctx *c);
 // Momentum-matrix generation (pmat.cu)
 void pm_release(exs_ctx *c);
+void wf_release(exs_ctx *c);
 // Stand-alone interstitial gather (interstitial.cu)
 cudaError_t launch_interstitial(const DevParams &p, int which, const KDesc *d_k, int nk, int ngp_max, cudaStream_t s);
 // Split-precision contraction (ozaki.cu)

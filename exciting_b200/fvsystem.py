@@ -160,6 +160,27 @@ class Setup:
         self._check(self.lib.exs_hmlint(self.ctx, ctypes.byref(r), _ptr(aa), _ptr(loa), _ptr(lolo)))
         return aa, loa, lolo
 
+    def wavefmt(self, gk, apwalm, evecfv, rad, *, lrstp: int = 1, lmax: int | None = None, ld: int | None = None):
+        """Muffin-tin wavefunction coefficients wfmt(ld, nrc, natmtot, nst)
+        of the states evecfv(nmat, nst) at the G+k set ``gk``, from the
+        matching coefficients ``apwalm`` (as match returns them) and the
+        radial functions of ``rad`` (system.MtRadial): src/wavefmt.f90 for
+        every atom and state."""
+        b = self.sys.basis
+        lmax = b.lmaxapw if lmax is None else lmax
+        ld = (lmax + 1) ** 2 if ld is None else ld
+        ev = np.asfortranarray(evecfv, dtype=np.complex128)
+        nst = ev.shape[1]
+        alm = np.zeros((self.ngkmax, b.apwordmax, b.lmmaxapw, self.sys.natmtot), dtype=np.complex128, order="F")
+        alm[: apwalm.shape[0]] = apwalm[: self.ngkmax]
+        apwfr, lofr = _f(rad.apwfr, np.float64), _f(rad.lofr, np.float64)
+        r, keep = self._mt_radial(rad, apwfr.ctypes.data, lofr.ctypes.data if lofr.size else None, None)
+        nrc = (int(rad.nrmtmax) - 1) // lrstp + 1
+        out = np.zeros((ld, nrc, self.sys.natmtot, nst), dtype=np.complex128, order="F")
+        self._check(self.lib.exs_wavefmt(self.ctx, gk.ngp, _ptr(alm), nst, _ptr(ev), ev.shape[0], lrstp, lmax,
+                                         ctypes.byref(r), ld, _ptr(out)))
+        return out
+
     def olprad(self, rad, *, outputs: bool = True):
         """Overlap radial integrals (oalo, ololo, h1aa, h1loa, h1lolo) of ``rad``,
         installed on the device; the h1 arrays are None unless relativity is iora*."""

@@ -316,6 +316,25 @@ int exs_rttddft_genpmat(exs_ctx *ctx, int nk, const int *ngp, const int *igpig, 
  * src/src_lib/clebgor.f90, as gradzfmtr uses it), else 0. */
 int exs_clebgor_unit(int l2, int m2, int q, int l, int m, double *value);
 
+/* Replaces the loop of  call wavefmt(lrstp, lmax, is, ia, ngp, apwalm,
+ * evecfv(:, ist), ld, wfmt)  (src/wavefmt.f90:13) over every atom and nst
+ * states, as rhovalk.f90:119-142 and gendmatmt.f90 call it after match:
+ *   apwalm(ngkmax, apwordmax, lmmaxapw, natmtot) HOST, as exs_match returns
+ *     it (rows 1..ngp used);
+ *   evecfv(ldv, nst) HOST, rows 1..nmat (nmat = ngp + nlotot);
+ *   *in: apwfr(nrmtmax, 2, apwordmax, 0:lmaxapw, natmtot) and, with local
+ *     orbitals, lofr(nrmtmax, 2, nlomax, natmtot), nrmt(nspecies) (HOST;
+ *     spr, lmaxvr and veffmt unused);
+ *   wfmt(ld, nrc, natmtot, nst) HOST out, nrc = (nrmtmax - 1) / lrstp + 1:
+ *     wfmt(lm, ir, ias, ist) for lm < (lmax + 1)^2 and the points
+ *     ir < (nrmt(is) - 1) / lrstp + 1 of the atom's species, as wavefmt
+ *     writes wfmt(lm, ir); zero elsewhere.
+ * lmax <= lmaxapw (the reference stops otherwise), ld >= (lmax + 1)^2.
+ * The G sums are one cuBLAS ZGEMM, the radial expansion one kernel.
+ * Synchronous. */
+int exs_wavefmt(exs_ctx *ctx, int ngp, const exs_complex *apwalm, int nst, const exs_complex *evecfv, int ldv,
+                int lrstp, int lmax, const exs_mt_radial *in, int ld, exs_complex *wfmt);
+
 /* Autotuner (no counterpart in the reference): runs the batch described as
  * for exs_setup_batched_device once per kernel configuration of the active
  * precision mode (for the split-precision contraction: K chunks per

@@ -12,6 +12,7 @@ CPU-baseline leg.  Never imported by the library itself.
                                   (src/src_eigensystem/modfvsystem.f90:48-101)
 * ``forcek``                   -- src/forcek.f90:83-390 (no second variation:
                                   ``tevecsv`` false, spin-unpolarised)
+* ``wavefmt``                  -- src/wavefmt.f90:82-174 (one state and atom)
 
 The zgemm calls go to numpy (OpenBLAS); the scalar loops are in C.
 Parity against the reference itself is not pinned for H, O or the IBS force
@@ -363,6 +364,48 @@ def overlapsetup_atom_aa(sys, apwalm, ngp, ias, o):
                 zm[:, f + io2] += apwi2[:, f + io2]
             f += n_io
     o[:ngp, :ngp] += apwi.conj().T @ zm.conj().T
+
+
+# ---------------------------------------------------------------- muffin-tin wavefunction
+def _wavefmt_add(wf, a, b, fr):
+    """src/wavefmt.f90:126-174: wf += (a + i b) fr with the reference's skips
+    of constants below 1e-14 in magnitude."""
+    eps = 1e-14
+    if abs(b) < eps:
+        if abs(a) < eps:
+            return
+        wf.real += a * fr
+    elif abs(a) < eps:
+        wf.imag += b * fr
+    else:
+        wf.real += a * fr
+        wf.imag += b * fr
+
+
+def wavefmt(sys, rad, lrstp, lmax, ias, ngp, apwalm, evecfv, ld):
+    """wfmt(ld, nr) of one state and atom: src/wavefmt.f90:82-123 (APW part
+    with zdotu over G, then the local orbitals of l <= lmax)."""
+    b = sys.basis
+    is_ = b.atom_species[ias]
+    if lmax > b.lmaxapw:
+        raise ValueError("lmax > lmaxapw")
+    nrmt = int(rad.nrmt[is_])
+    rs = np.arange(0, nrmt, lrstp)                       # ir = 1, 1 + lrstp, ... (0-based points)
+    nr = len(rs)
+    wf = np.zeros((ld, nr), dtype=np.complex128)
+    for l in range(lmax + 1):
+        for m in range(-l, l + 1):
+            lm = l * (l + 1) + m
+            for io in range(b.apword[is_][l]):
+                zt1 = np.sum(evecfv[:ngp] * apwalm[:ngp, io, lm, ias])
+                _wavefmt_add(wf[lm], zt1.real, zt1.imag, rad.apwfr[rs, 0, io, l, ias])
+    for ilo, l in enumerate(b.lorbl[is_]):
+        if l <= lmax:
+            for m in range(-l, l + 1):
+                lm = l * (l + 1) + m
+                i = ngp + int(b.idxlo[lm, ilo, ias]) - 1
+                _wavefmt_add(wf[lm], evecfv[i].real, evecfv[i].imag, rad.lofr[rs, 0, ilo, ias])
+    return wf
 
 
 # ---------------------------------------------------------------- muffin-tin integrals
