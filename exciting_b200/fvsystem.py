@@ -175,7 +175,7 @@ class Setup:
         alm[: apwalm.shape[0]] = apwalm[: self.ngkmax]
         apwfr, lofr = _f(rad.apwfr, np.float64), _f(rad.lofr, np.float64)
         r, keep = self._mt_radial(rad, apwfr.ctypes.data, lofr.ctypes.data if lofr.size else None, None)
-        nrc = (int(rad.nrmtmax) - 1) // lrstp + 1
+        nrc = (int(rad.nrmtmax) - 1) // lrstp + 1 if lrstp >= 1 else 1      # lrstp < 1: the library's error
         out = np.zeros((ld, nrc, self.sys.natmtot, nst), dtype=np.complex128, order="F")
         self._check(self.lib.exs_wavefmt(self.ctx, gk.ngp, _ptr(alm), nst, _ptr(ev), ev.shape[0], lrstp, lmax,
                                          ctypes.byref(r), ld, _ptr(out)))

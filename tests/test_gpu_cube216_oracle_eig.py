@@ -1,0 +1,93 @@
+"""The 216-atom cell at Gamma against the CPU oracle itself: the lowest 40
+generalized eigenvalues of four pencils, compared as Ritz values on the
+oracle pencil's lowest 64 eigenvectors (a Cholesky reduction and torch's
+MAGMA eigen-solve with vectors; cuSOLVER's dense solvers refuse n = 29,145).
+
+Pencils: the oracle (FP64 on the host: the reference's per-atom zgemm pairs,
+hamiltonsetup.f90:75-103 and overlapsetup.f90:88-101, through OpenBLAS), the
+device's native FP64 path, the split path with the default 13 moduli, and
+the split path with 16 moduli (52-bit operands, integer products, one
+rounding per element).
+
+The bar: the split path's lowest 40 eigenvalues within the absolute 1e-8 Ha
+of the 16-moduli pencil's.  The deviations of both FP64 computations (host
+and device) from the 16-moduli pencil, and of the split path from the
+oracle, are printed beside it.  The oracle needs about 15 minutes on 16
+cores and ~60 GB of host memory, so the test runs only with
+EXS_TEST_216_ORACLE=1.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import lapw_oracle as O
+from exciting_b200 import workloads as W
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(os.environ.get("EXS_TEST_216_ORACLE") != "1",
+                                 reason="set EXS_TEST_216_ORACLE=1 (about 20 minutes)")]
+
+NEV, NX = 40, 64
+
+
+def test_cube216_eigenvalues_against_the_oracle():
+    import time
+    import torch
+    from exciting_b200.fvsystem import Setup
+    c128 = torch.complex128
+    s = W.si_cube216()
+    gk = s.gksets()[0]
+    m = s.nmat(gk)
+    t0 = time.time()
+    h, o = O.hamiltonandoverlapsetup(s, gk)                  # Fortran order: the za layout
+    t_oracle = time.time() - t0
+    # the oracle pencil's lowest NX eigenvectors; every pencil is read as its transpose (conjugate)
+    hd = torch.from_numpy(h.reshape(-1, order="F").view(np.float64)).cuda().view(c128).view(m, m)
+    od = torch.from_numpy(o.reshape(-1, order="F").view(np.float64)).cuda().view(c128).view(m, m)
+    del h, o
+    L = torch.linalg.cholesky(od)
+    X1 = torch.linalg.solve_triangular(L, hd, upper=False)
+    C = torch.linalg.solve_triangular(L, X1.mH.contiguous(), upper=False)
+    del X1
+    torch.cuda.empty_cache()
+    prev = torch.backends.cuda.preferred_linalg_library()
+    torch.backends.cuda.preferred_linalg_library("magma")
+    try:
+        w, Y = torch.linalg.eigh(C)
+    finally:
+        torch.backends.cuda.preferred_linalg_library(prev)
+    del C
+    X = torch.linalg.solve_triangular(L.mH.contiguous(), Y[:, :NX].contiguous(), upper=True)
+    del Y, L
+    torch.cuda.empty_cache()
+
+    def ritz(H, Ov):
+        Hs = X.mH @ (H @ X)
+        Os = X.mH @ (Ov @ X)
+        Hs, Os = 0.5 * (Hs + Hs.mH), 0.5 * (Os + Os.mH)
+        Ls = torch.linalg.cholesky(Os)
+        Cs = torch.linalg.solve_triangular(Ls, torch.linalg.solve_triangular(Ls, Hs, upper=False).mH, upper=False)
+        return torch.linalg.eigvalsh(0.5 * (Cs + Cs.mH))[:NEV].cpu().numpy()
+
+    th = {"oracle": ritz(hd, od)}
+    del hd, od
+    torch.cuda.empty_cache()
+    st = Setup(s, ngkmax=gk.ngp, max_batch=1)
+    d_h = torch.empty(2 * m * m, dtype=torch.float64, device="cuda")
+    d_o = torch.empty_like(d_h)
+    ig = torch.from_numpy(np.asarray(gk.igpig, dtype=np.int32)).cuda()
+    vg = torch.from_numpy(np.ascontiguousarray(gk.vgpc.T)).cuda()
+    for name, mode, n in (("split13", "ozaki_mod", 0), ("fp64", "fp64", 0), ("split16", "ozaki_mod", 16)):
+        st.set_precision(mode, n)
+        st.setup_batched_device([gk.ngp], ig.data_ptr(), vg.data_ptr(), [d_h.data_ptr()], [d_o.data_ptr()])
+        st.synchronize()
+        th[name] = ritz(d_h.view(c128).view(m, m), d_o.view(c128).view(m, m))
+    st.close()
+    dev = lambda a, b: float(np.max(np.abs(th[a] - th[b])))
+    report = {"oracle_s": t_oracle, "lowest_Ha": float(w[0]), "oracle_ritz_vs_dense_Ha": float(np.max(np.abs(th["oracle"] - w[:NEV].cpu().numpy()))),
+              "split13_vs_split16": dev("split13", "split16"), "split13_vs_oracle": dev("split13", "oracle"),
+              "fp64_vs_oracle": dev("fp64", "oracle"), "fp64_vs_split16": dev("fp64", "split16"),
+              "oracle_vs_split16": dev("oracle", "split16"), "split13_vs_fp64": dev("split13", "fp64")}
+    print("cube216 Gamma eigenvalue ladder (max |d eps| over the lowest 40, Ha):", report)
+    assert report["split13_vs_split16"] <= 1e-8
