@@ -1200,21 +1200,23 @@ def run_large(args):
     nf = len(gks)
     fp64_value, phase64, acc, h8, h16 = None, np.zeros(5), None, None, None
     if not args.skip_fp64:
-        # ---- Gamma in split precision, kept on the host for the comparison
-        one(0)
-        st.synchronize()
-        h8, o8 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
-        # ---- the native FP64 path: a few stated steps (one per k-point)
+        # ---- Gamma in split precision, kept on the host for the comparison (rank 0: 27 GB per pencil)
+        if rank == 0:
+            one(0)
+            st.synchronize()
+            h8, o8 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
+        # ---- the native FP64 path: a few stated steps (one per k-point), every rank
         st.set_precision("fp64")
         ms64, phase64, _ = timed(nf, 1, False)
         fp64_value = ws * nf / (ms64 * 1e-3)
         _progress("fp64: %.4f setups/s, phases %s" % (fp64_value, list(np.round(phase64, 2))))
-        one(0)
-        st.synchronize()
-        acc = {"against": "native FP64 GPU path, Gamma, whole H and O",
-               "rel_fro_H": _rel_fro_host(h8, d_h[: 2 * m0 * m0]),
-               "rel_fro_O": _rel_fro_host(o8, d_o[: 2 * m0 * m0])}
-        h64, o64 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
+        if rank == 0:
+            one(0)
+            st.synchronize()
+            acc = {"against": "native FP64 GPU path, Gamma, whole H and O",
+                   "rel_fro_H": _rel_fro_host(h8, d_h[: 2 * m0 * m0]),
+                   "rel_fro_O": _rel_fro_host(o8, d_o[: 2 * m0 * m0])}
+            h64, o64 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
         if not args.skip_eig and rank == 0 and prec == "ozaki_mod" and args.moduli != 16:
             # ---- a third Gamma pencil, the split path at its widest plan (16 moduli, 52-bit operands):
             # the eigenvalue leg separates the split path's own error from the FP64 path's rounding
