@@ -156,6 +156,20 @@ def _measured_int8_sustained(torch, seconds=4.0):
     return v, _clock_summary(rows, torch.cuda.current_device())
 
 
+def _int8_from_bf16_peaks(achieved):
+    """The int8 dense rate as twice MEASURED_PEAKS.json's bf16 GEMM figures
+    (that file has no int8 entry; the tensor cores' int8 rate is twice the
+    bf16 rate), beside the in-run cuBLASLt int8 peaks."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mp = json.load(f)
+        b, bs = 2.0 * float(mp["bf16_tflops"]), 2.0 * float(mp["bf16_tflops_sustained"])
+    except (OSError, KeyError, ValueError):
+        return {}
+    return {"peak_2x_bf16_measured_peaks": b, "frac_of_2x_bf16": achieved / b,
+            "peak_2x_bf16_sustained_measured_peaks": bs, "frac_of_2x_bf16_sustained": achieved / bs}
+
+
 def _hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -1369,6 +1383,7 @@ def run_large(args):
                          "peak_source": "cuBLASLt int8 GEMM 8192^3 (torch._int_mm) back to back for 4 s in this "
                                         "run (sustained, under the power cap: the H/O kernel runs for seconds)",
                          "peak_burst": peak8, "frac_of_burst": a8 / peak8, "peak_sustained_clocks": clk8s,
+                         **_int8_from_bf16_peaks(a8),
                          "int8_ops_per_step": ops, "traffic": PROFILED_DRAM_BYTES_216.get(kcfg),
                          "traffic_note": "bytes per launch of the residue kernel: ncu dram__bytes_read+write of "
                                          "one full-size launch (one pass); algorithmic %.3g (residue planes read "
