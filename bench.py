@@ -1131,7 +1131,9 @@ def run_large(args):
     the split-precision setup (value), the native FP64 path, the adjoint, and
     the host-pointer entry point; accuracy at Gamma (Frobenius and the lowest
     40 generalized eigenvalues of both paths); the CPU restatement on a bounded
-    sample; the 8-atom batch as a secondary leg."""
+    sample; the 8-atom batch as a secondary leg.  With several ranks every
+    rank times the split and FP64 legs and the adjoint; the accuracy,
+    eigenvalue, CPU and 8-atom legs run in one-GPU runs only."""
     import torch
     import torch.distributed as dist
     from exciting_b200 import workloads as W
@@ -1214,8 +1216,8 @@ def run_large(args):
     nf = len(gks)
     fp64_value, phase64, acc, h8, h16 = None, np.zeros(5), None, None, None
     if not args.skip_fp64:
-        # ---- Gamma in split precision, kept on the host for the comparison (rank 0: 27 GB per pencil)
-        if rank == 0:
+        # ---- Gamma in split precision, kept on the host for the comparison (one GPU only: 27 GB per pencil)
+        if ws == 1:
             one(0)
             st.synchronize()
             h8, o8 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
@@ -1224,14 +1226,14 @@ def run_large(args):
         ms64, phase64, _ = timed(nf, 1, False)
         fp64_value = ws * nf / (ms64 * 1e-3)
         _progress("fp64: %.4f setups/s, phases %s" % (fp64_value, list(np.round(phase64, 2))))
-        if rank == 0:
+        if ws == 1:
             one(0)
             st.synchronize()
             acc = {"against": "native FP64 GPU path, Gamma, whole H and O",
                    "rel_fro_H": _rel_fro_host(h8, d_h[: 2 * m0 * m0]),
                    "rel_fro_O": _rel_fro_host(o8, d_o[: 2 * m0 * m0])}
             h64, o64 = _host(d_h, 2 * m0 * m0), _host(d_o, 2 * m0 * m0)
-        if not args.skip_eig and rank == 0 and prec == "ozaki_mod" and args.moduli != 16:
+        if not args.skip_eig and ws == 1 and prec == "ozaki_mod" and args.moduli != 16:
             # ---- a third Gamma pencil, the split path at its widest plan (16 moduli, 52-bit operands):
             # the eigenvalue leg separates the split path's own error from the FP64 path's rounding
             try:
@@ -1343,7 +1345,7 @@ def run_large(args):
         mt_ms = phase[2]
         a8 = ops / (mt_ms * 1e-3) / 1e12
         cpu = None
-        if not args.skip_cpu:
+        if not args.skip_cpu and ws == 1:
             try:
                 cpu_sample_216(s, gks_all[0], 1, 1000)                      # warm-up (libraries, pages)
                 full, dt = cpu_sample_216(s, gks_all[0], 2, 3000)
