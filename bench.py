@@ -1126,7 +1126,7 @@ def e2e_large(st, gks, nlotot, mmax, torch, ne=2):
 
 
 def run_large(args):
-    """The 216-atom cell, the north-star workload: one k-point per step (H and
+    """The 216-atom cell, the default workload: one k-point per step (H and
     O are ~13.6 GB each), Gamma and the three other k-points in turn.  Timed:
     the split-precision setup (value), the native FP64 path, the adjoint, and
     the host-pointer entry point; accuracy at Gamma (Frobenius and the lowest
