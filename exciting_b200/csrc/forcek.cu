@@ -151,20 +151,28 @@ __device__ inline void cdot(const double *ar, const double *ai, const double *br
     }
 }
 
-// MT APW-APW terms, one block per (atom, direction).
+// The force terms are sums over the atom's APW rows f, so each block takes
+// FK_FROWS of them and adds its share to the force atomically: many blocks
+// per (atom, direction) instead of one long serial loop over the rows.
+constexpr int FK_FROWS = 16;
+
+// MT APW-APW terms, one block per (atom, direction, chunk of FK_FROWS rows).
 __global__ void fk_terms_mt(DevParams p, ForceWork fw)
 {
     __shared__ double sh[32];
     const int ias = blockIdx.x, x = blockIdx.y;
     const AtomDesc at = p.atoms[ias];
+    const int fc = blockIdx.z * FK_FROWS;
+    if (fc >= at.napw) return;                  // the whole block: no barrier is skipped by part of it
+    const int f0 = at.apw_off + fc, nf = min(FK_FROWS, at.napw - fc);
     double acc = 0.0;
     for (int n = threadIdx.x; n < fw.nst; n += blockDim.x) {
         double zr, zi, z2r, z2i, yr, yi, y2r, y2i;
-        // z = u_x^H h u, z' = u^H h u_x, y = u_x^H M u, y' = u^H M u_x
-        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.hu[0][0], fw.hu[0][1], at.apw_off, at.napw, fw.nstp, n, zr, zi);
-        cdot(fw.u[0][0], fw.u[0][1], fw.hu[1 + x][0], fw.hu[1 + x][1], at.apw_off, at.napw, fw.nstp, n, z2r, z2i);
-        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.mu[0][0], fw.mu[0][1], at.apw_off, at.napw, fw.nstp, n, yr, yi);
-        cdot(fw.u[0][0], fw.u[0][1], fw.mu[1 + x][0], fw.mu[1 + x][1], at.apw_off, at.napw, fw.nstp, n, y2r, y2i);
+        // z = u_x^H h u, z' = u^H h u_x, y = u_x^H M u, y' = u^H M u_x (this block's rows)
+        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.hu[0][0], fw.hu[0][1], f0, nf, fw.nstp, n, zr, zi);
+        cdot(fw.u[0][0], fw.u[0][1], fw.hu[1 + x][0], fw.hu[1 + x][1], f0, nf, fw.nstp, n, z2r, z2i);
+        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.mu[0][0], fw.mu[0][1], f0, nf, fw.nstp, n, yr, yi);
+        cdot(fw.u[0][0], fw.u[0][1], fw.mu[1 + x][0], fw.mu[1 + x][1], f0, nf, fw.nstp, n, y2r, y2i);
         // Re[i w (z - z')] + Re[-i w eps (y - y')]
         acc += -fw.w[n] * (zi - z2i) + fw.w[n] * fw.eps[n] * (yi - y2i);
     }
@@ -172,12 +180,17 @@ __global__ void fk_terms_mt(DevParams p, ForceWork fw)
     if (threadIdx.x == 0) atomicAdd(&fw.force[x + 3 * ias], s);
 }
 
-// APW-lo terms, one block per (atom, direction); threads over (lo row, state).
+// APW-lo terms, one block per (atom, direction, chunk of FK_FROWS APW rows
+// of the loa U_x product); threads over (lo row, state).  The S U_x part,
+// a few rows per lo row, is added by the blocks of the first chunk.
 __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, const double *loa_i, int ldlo, int maxaa)
 {
     __shared__ double sh[32];
     const int ias = blockIdx.x, x = blockIdx.y;
     const AtomDesc at = p.atoms[ias];
+    const int fc = blockIdx.z * FK_FROWS;
+    if (fc >= at.napw) return;                  // the whole block
+    const int fe = min(at.napw, fc + FK_FROWS);
     const int is = at.species;
     const int *apw = p.apword + (size_t)(p.lmaxapw + 1) * is;
     const int nmat = fw.ngp + p.nlotot;
@@ -188,7 +201,7 @@ __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, cons
         // (loa U_x)(r, n)
         double lr = 0.0, li = 0.0;
         const double *lar = loa_r + (size_t)ldlo * maxaa * ias, *lai = loa_i + (size_t)ldlo * maxaa * ias;
-        for (int f = 0; f < at.napw; f++) {
+        for (int f = fc; f < fe; f++) {
             const double ar = lar[r + (size_t)ldlo * f], ai = lai[r + (size_t)ldlo * f];
             const size_t iu = (size_t)(at.apw_off + f) * fw.nstp + n;
             lr += ar * uxr[iu] - ai * uxi[iu];
@@ -206,7 +219,7 @@ __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, cons
         for (int ll = 0; ll < l; ll++) f += (2 * ll + 1) * apw[ll];
         f += (m + l) * apw[l];
         double sr = 0.0, si = 0.0;
-        for (int io = 0; io < apw[l]; io++) {
+        for (int io = 0; io < (blockIdx.z == 0 ? apw[l] : 0); io++) {
             double w = p.oalo[io + (size_t)p.apwordmax * (ilo + (size_t)p.nlomax * ias)];
             if (p.h1loa) w += p.h1loa[io + (size_t)p.apwordmax * (ilo + (size_t)p.nlomax * ias)];
             const size_t iu = (size_t)(f + io) * fw.nstp + n;
@@ -503,9 +516,10 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_w1, (int)w1.size(), d_k, s));
     FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_w2, (int)w2.size(), d_k, s));
     if (iora) exs::fk_iora_u<<<dim3((nstp + 63) / 64, c->natmtot, 4), 64, 0, s>>>(p, fw);
-    exs::fk_terms_mt<<<dim3(c->natmtot, 3), 128, 0, s>>>(p, fw);
+    const unsigned fch = (unsigned)((c->maxaa + exs::FK_FROWS - 1) / exs::FK_FROWS);
+    exs::fk_terms_mt<<<dim3(c->natmtot, 3, fch), 64, 0, s>>>(p, fw);
     if (c->nlotot > 0)
-        exs::fk_terms_lo<<<dim3(c->natmtot, 3), 256, 0, s>>>(p, fw, c->d_loa_r, c->d_loa_i, c->ldlo, c->maxaa);
+        exs::fk_terms_lo<<<dim3(c->natmtot, 3, fch), 256, 0, s>>>(p, fw, c->d_loa_r, c->d_loa_i, c->ldlo, c->maxaa);
     for (size_t b = 0; b + 1 < wb_off.size(); b++) {   // one band of P^T, Q^T, then its scatter
         const int i0 = (int)b * band, i1 = std::min(ngp, i0 + band);
         FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_wb + wb_off[b], (int)(wb_off[b + 1] - wb_off[b]),
