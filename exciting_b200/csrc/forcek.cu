@@ -277,7 +277,8 @@ __global__ void fk_terms_theta(DevParams p, ForceWork fw, int ngvec)
     const int ias = blockIdx.x;
     const AtomDesc at = p.atoms[ias];
     double acc[3] = {0.0, 0.0, 0.0};
-    for (int g = threadIdx.x; g < ngvec; g += blockDim.x) {
+    // blockIdx.y: one of gridDim.y interleaved shares of the G-vectors
+    for (int g = blockIdx.y * blockDim.x + threadIdx.x; g < ngvec; g += gridDim.y * blockDim.x) {
         const double *v = fw.vgc + 3 * (size_t)g;
         const double ff = fw.ffacg[g + (size_t)ngvec * at.species];
         double s, c;
@@ -527,7 +528,9 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
         exs::fk_scatter<<<dim3((i1 - i0 + 127) / 128, ngp), 128, 0, s>>>(p, fw, d_k, i0, i1);
         FK_CUDA(cudaGetLastError());
     }
-    exs::fk_terms_theta<<<c->natmtot, 256, 0, s>>>(p, fw, c->ngvec);
+    // about two waves of blocks whatever the number of atoms, at least 2,048 G-vectors per block
+    const int gsh = std::max(1, std::min((c->ngvec + 2047) / 2048, (2 * 148 * 8 + c->natmtot - 1) / c->natmtot));
+    exs::fk_terms_theta<<<dim3(c->natmtot, gsh), 256, 0, s>>>(p, fw, c->ngvec);
     FK_CUDA(cudaGetLastError());
     return EXS_OK;
 }
