@@ -29,13 +29,14 @@ namespace exs {
 
 struct ForceWork {
     int ngp, nst, nstp, ldt;         // ldt = Kpad (leading dim of At)
+    int ldu;                         // 4 nstp: row stride of Ct, U, hU, MU, whose four blocks q sit side by side
     const KDesc *k;                  // A planes of the k-point (slot 0)
     double *atr, *ati;               // At [G][f]
-    double *ct[4][2];                // Ct, Ct_x [G][n]  (q = 0: plain, 1..3: scaled by (k+G)_x)
+    double *ct[4][2];                // Ct, Ct_x [G][ldu], block q at column q nstp (q = 0: plain, 1..3: x (k+G)_x)
     double *cn[2], *wc[2], *wec[2];  // [n][G]
-    double *u[4][2];                 // U_q [f][n]
-    double *hu[4][2];                // h_a U_q
-    double *mu[4][2];                // M U_q (iora*) or == u
+    double *u[4][2];                 // U_q [f][ldu], block q at column q nstp
+    double *hu[4][2];                // h_a U_q, same layout
+    double *mu[4][2];                // M U_q (iora*) or == u, same layout
     double *pt[2], *qt[2];           // one band of rows of P^T, Q^T [i - i0][j], ld npad
     exs_complex *evec;               // (nmat, nst) dense
     const double *w, *eps;           // (nst)
@@ -80,7 +81,7 @@ __global__ void fk_pack_evec(ForceWork fw, int npad, const double *vgpc, int nma
         w = fw.w[n];
         we = fw.w[n] * fw.eps[n];
     }
-    const size_t it = (size_t)g * fw.nstp + n;
+    const size_t it = (size_t)g * fw.ldu + n;
     fw.ct[0][0][it] = re;
     fw.ct[0][1][it] = im;
     for (int x = 0; x < 3; x++) {
@@ -112,15 +113,15 @@ __global__ void fk_iora_u(DevParams p, ForceWork fw)
         const double *h1 = p.h1aa + (size_t)p.apwordmax * p.apwordmax * (l + (size_t)(p.lmaxapw + 1) * ias);
         for (int m = -l; m <= l; m++, f += no)
             for (int io2 = 0; io2 < no; io2++) {
-                double re = fw.u[q][0][(size_t)(f + io2) * fw.nstp + n];
-                double im = fw.u[q][1][(size_t)(f + io2) * fw.nstp + n];
+                double re = fw.u[q][0][(size_t)(f + io2) * fw.ldu + n];
+                double im = fw.u[q][1][(size_t)(f + io2) * fw.ldu + n];
                 for (int io1 = 0; io1 < no; io1++) {
                     const double w = h1[io1 + (size_t)p.apwordmax * io2];
-                    re += w * fw.u[q][0][(size_t)(f + io1) * fw.nstp + n];
-                    im += w * fw.u[q][1][(size_t)(f + io1) * fw.nstp + n];
+                    re += w * fw.u[q][0][(size_t)(f + io1) * fw.ldu + n];
+                    im += w * fw.u[q][1][(size_t)(f + io1) * fw.ldu + n];
                 }
-                fw.mu[q][0][(size_t)(f + io2) * fw.nstp + n] = re;
-                fw.mu[q][1][(size_t)(f + io2) * fw.nstp + n] = im;
+                fw.mu[q][0][(size_t)(f + io2) * fw.ldu + n] = re;
+                fw.mu[q][1][(size_t)(f + io2) * fw.ldu + n] = im;
             }
     }
 }
@@ -169,10 +170,10 @@ __global__ void fk_terms_mt(DevParams p, ForceWork fw)
     for (int n = threadIdx.x; n < fw.nst; n += blockDim.x) {
         double zr, zi, z2r, z2i, yr, yi, y2r, y2i;
         // z = u_x^H h u, z' = u^H h u_x, y = u_x^H M u, y' = u^H M u_x (this block's rows)
-        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.hu[0][0], fw.hu[0][1], f0, nf, fw.nstp, n, zr, zi);
-        cdot(fw.u[0][0], fw.u[0][1], fw.hu[1 + x][0], fw.hu[1 + x][1], f0, nf, fw.nstp, n, z2r, z2i);
-        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.mu[0][0], fw.mu[0][1], f0, nf, fw.nstp, n, yr, yi);
-        cdot(fw.u[0][0], fw.u[0][1], fw.mu[1 + x][0], fw.mu[1 + x][1], f0, nf, fw.nstp, n, y2r, y2i);
+        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.hu[0][0], fw.hu[0][1], f0, nf, fw.ldu, n, zr, zi);
+        cdot(fw.u[0][0], fw.u[0][1], fw.hu[1 + x][0], fw.hu[1 + x][1], f0, nf, fw.ldu, n, z2r, z2i);
+        cdot(fw.u[1 + x][0], fw.u[1 + x][1], fw.mu[0][0], fw.mu[0][1], f0, nf, fw.ldu, n, yr, yi);
+        cdot(fw.u[0][0], fw.u[0][1], fw.mu[1 + x][0], fw.mu[1 + x][1], f0, nf, fw.ldu, n, y2r, y2i);
         // Re[i w (z - z')] + Re[-i w eps (y - y')]
         acc += -fw.w[n] * (zi - z2i) + fw.w[n] * fw.eps[n] * (yi - y2i);
     }
@@ -203,7 +204,7 @@ __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, cons
         const double *lar = loa_r + (size_t)ldlo * maxaa * ias, *lai = loa_i + (size_t)ldlo * maxaa * ias;
         for (int f = fc; f < fe; f++) {
             const double ar = lar[r + (size_t)ldlo * f], ai = lai[r + (size_t)ldlo * f];
-            const size_t iu = (size_t)(at.apw_off + f) * fw.nstp + n;
+            const size_t iu = (size_t)(at.apw_off + f) * fw.ldu + n;
             lr += ar * uxr[iu] - ai * uxi[iu];
             li += ar * uxi[iu] + ai * uxr[iu];
         }
@@ -222,7 +223,7 @@ __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, cons
         for (int io = 0; io < (blockIdx.z == 0 ? apw[l] : 0); io++) {
             double w = p.oalo[io + (size_t)p.apwordmax * (ilo + (size_t)p.nlomax * ias)];
             if (p.h1loa) w += p.h1loa[io + (size_t)p.apwordmax * (ilo + (size_t)p.nlomax * ias)];
-            const size_t iu = (size_t)(f + io) * fw.nstp + n;
+            const size_t iu = (size_t)(f + io) * fw.ldu + n;
             sr += w * uxr[iu];
             si += w * uxi[iu];
         }
@@ -307,7 +308,7 @@ __global__ void fk_dh(DevParams p, ForceWork fw, exs_complex *dh, int maxaa)
     if (f < at.napw && f2 < at.napw) {
         const double *ur = fw.u[0][0], *ui = fw.u[0][1];
         for (int n = 0; n < fw.nst; n++) {
-            const size_t a = (size_t)(at.apw_off + f) * fw.nstp + n, b = (size_t)(at.apw_off + f2) * fw.nstp + n;
+            const size_t a = (size_t)(at.apw_off + f) * fw.ldu + n, b = (size_t)(at.apw_off + f2) * fw.ldu + n;
             re += fw.w[n] * (ur[a] * ur[b] + ui[a] * ui[b]);
             im += fw.w[n] * (ur[a] * ui[b] - ui[a] * ur[b]);
         }
@@ -396,18 +397,20 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     FK_CUDA(grow(&c->fk_dev, &c->fk_bytes, off, false));
     char *b = (char *)c->fk_dev;
     fw.ngp = ngp; fw.nst = nst; fw.nstp = nstp; fw.ldt = Kp;
+    const int ldu = 4 * nstp;
+    fw.ldu = ldu;
     fw.atr = (double *)(b + o_at); fw.ati = fw.atr + (size_t)npad * Kp;
     for (int q = 0; q < 4; q++)
-        for (int r = 0; r < 2; r++) fw.ct[q][r] = (double *)(b + o_ct) + (size_t)(2 * q + r) * npad * nstp;
+        for (int r = 0; r < 2; r++) fw.ct[q][r] = (double *)(b + o_ct) + (size_t)r * npad * ldu + (size_t)q * nstp;
     double *cn = (double *)(b + o_cn);
     fw.cn[0] = cn; fw.cn[1] = cn + (size_t)nstp * npad;
     fw.wc[0] = cn + 2 * (size_t)nstp * npad; fw.wc[1] = cn + 3 * (size_t)nstp * npad;
     fw.wec[0] = cn + 4 * (size_t)nstp * npad; fw.wec[1] = cn + 5 * (size_t)nstp * npad;
     for (int q = 0; q < 4; q++)
         for (int r = 0; r < 2; r++) {
-            fw.u[q][r] = (double *)(b + o_u) + (size_t)(2 * q + r) * Kp * nstp;
-            fw.hu[q][r] = (double *)(b + o_hu) + (size_t)(2 * q + r) * Kp * nstp;
-            fw.mu[q][r] = iora ? (double *)(b + o_mu) + (size_t)(2 * q + r) * Kp * nstp : fw.u[q][r];
+            fw.u[q][r] = (double *)(b + o_u) + (size_t)r * Kp * ldu + (size_t)q * nstp;
+            fw.hu[q][r] = (double *)(b + o_hu) + (size_t)r * Kp * ldu + (size_t)q * nstp;
+            fw.mu[q][r] = iora ? (double *)(b + o_mu) + (size_t)r * Kp * ldu + (size_t)q * nstp : fw.u[q][r];
         }
     double *pq = (double *)(b + o_pq);
     fw.pt[0] = pq; fw.pt[1] = pq + (size_t)band * npad;
@@ -450,12 +453,12 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
     std::vector<GemmProb> probs;
     std::vector<TileWork> w1, w2, wb;
     std::vector<size_t> wb_off;
-    for (int q = 0; q < 4; q++) {              // U_q = A C_q   (contraction over G)
+    {                                          // [U_0 .. U_3] = A [C_0 .. C_3]: one product over G, N = 4 nstp
         GemmProb P{};
         P.xr = fw.atr; P.xi = fw.ati; P.ldx = Kp;
-        P.yr = fw.ct[q][0]; P.yi = fw.ct[q][1]; P.ldy = nstp;
-        P.M = c->K; P.N = nstp; P.K = ngp; P.conjx = 0;
-        P.outr = fw.u[q][0]; P.outi = fw.u[q][1]; P.ldo = nstp;
+        P.yr = fw.ct[0][0]; P.yi = fw.ct[0][1]; P.ldy = ldu;
+        P.M = c->K; P.N = ldu; P.K = ngp; P.conjx = 0;
+        P.outr = fw.u[0][0]; P.outi = fw.u[0][1]; P.ldo = ldu;
         add_tiles(w1, (int)probs.size(), P.M, P.N, false);
         probs.push_back(P);
     }
@@ -472,19 +475,18 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
         }
     }
     wb_off.push_back(wb.size());
-    for (int q = 0; q < 4; q++)                // h_a U_q per atom
-        for (int ias = 0; ias < c->natmtot; ias++) {
-            const exs::AtomDesc &a = c->atoms[ias];
-            GemmProb P{};
-            P.xr = c->d_haa_r + (size_t)ias * c->ldh * c->ldh; P.xi = c->d_haa_i + (size_t)ias * c->ldh * c->ldh;
-            P.ldx = c->ldh;
-            P.yr = fw.u[q][0] + (size_t)a.apw_off * nstp; P.yi = fw.u[q][1] + (size_t)a.apw_off * nstp; P.ldy = nstp;
-            P.M = a.napw; P.N = nstp; P.K = a.napw; P.conjx = 0;
-            P.outr = fw.hu[q][0] + (size_t)a.apw_off * nstp; P.outi = fw.hu[q][1] + (size_t)a.apw_off * nstp;
-            P.ldo = nstp;
-            add_tiles(w2, (int)probs.size(), P.M, P.N, false);
-            probs.push_back(P);
-        }
+    for (int ias = 0; ias < c->natmtot; ias++) {   // h_a [U_0 .. U_3] per atom, N = 4 nstp
+        const exs::AtomDesc &a = c->atoms[ias];
+        GemmProb P{};
+        P.xr = c->d_haa_r + (size_t)ias * c->ldh * c->ldh; P.xi = c->d_haa_i + (size_t)ias * c->ldh * c->ldh;
+        P.ldx = c->ldh;
+        P.yr = fw.u[0][0] + (size_t)a.apw_off * ldu; P.yi = fw.u[0][1] + (size_t)a.apw_off * ldu; P.ldy = ldu;
+        P.M = a.napw; P.N = ldu; P.K = a.napw; P.conjx = 0;
+        P.outr = fw.hu[0][0] + (size_t)a.apw_off * ldu; P.outi = fw.hu[0][1] + (size_t)a.apw_off * ldu;
+        P.ldo = ldu;
+        add_tiles(w2, (int)probs.size(), P.M, P.N, false);
+        probs.push_back(P);
+    }
     const size_t kb = al256(sizeof(KDesc)), pb = al256(sizeof(GemmProb) * probs.size());
     const size_t wbytes = sizeof(TileWork) * (w1.size() + w2.size() + wb.size());
     const size_t tb = kb + pb + wbytes;
