@@ -297,26 +297,55 @@ __global__ void fk_terms_theta(DevParams p, ForceWork fw, int ngvec)
 }
 
 // dL/dh_a(f, f') = sum_n w_n conj(U(f, n)) U(f', n) per atom, into (maxaa, maxaa, natmtot).
+// One block per 32 x 32 tile (f, f') of one atom, 32 x 8 threads: chunks of
+// 32 states of the rows f and f' are staged in shared memory (coalesced over
+// n), and each thread sums four outputs f = tile + tx, f' = tile + ty + 8 j.
 __global__ void fk_dh(DevParams p, ForceWork fw, exs_complex *dh, int maxaa)
 {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    const int f2 = blockIdx.y;
-    const int ias = blockIdx.z;
-    if (f >= maxaa || f2 >= maxaa) return;
+    __shared__ double ar[32][33], ai[32][33], br[32][33], bi[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int fb = blockIdx.x * 32, f2b = blockIdx.y * 32, ias = blockIdx.z;
     const AtomDesc at = p.atoms[ias];
-    double re = 0.0, im = 0.0;
-    if (f < at.napw && f2 < at.napw) {
-        const double *ur = fw.u[0][0], *ui = fw.u[0][1];
-        for (int n = 0; n < fw.nst; n++) {
-            const size_t a = (size_t)(at.apw_off + f) * fw.ldu + n, b = (size_t)(at.apw_off + f2) * fw.ldu + n;
-            re += fw.w[n] * (ur[a] * ur[b] + ui[a] * ui[b]);
-            im += fw.w[n] * (ur[a] * ui[b] - ui[a] * ur[b]);
+    const double *ur = fw.u[0][0], *ui = fw.u[0][1];
+    double re[4] = {0.0, 0.0, 0.0, 0.0}, im[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int n0 = 0; n0 < fw.nst; n0 += 32) {
+        const int n = n0 + tx;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int r = ty + 8 * k;
+            const int f = fb + r, f2 = f2b + r;
+            const bool vn = n < fw.nst;
+            const double w = vn ? fw.w[n] : 0.0;
+            const bool va = vn && f < at.napw, vb = vn && f2 < at.napw;
+            const size_t ia = (size_t)(at.apw_off + f) * fw.ldu + n, ib = (size_t)(at.apw_off + f2) * fw.ldu + n;
+            ar[r][tx] = va ? ur[ia] : 0.0;
+            ai[r][tx] = va ? ui[ia] : 0.0;
+            br[r][tx] = vb ? w * ur[ib] : 0.0;
+            bi[r][tx] = vb ? w * ui[ib] : 0.0;
         }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < 32; c++) {
+            const double xr = ar[tx][c], xi = ai[tx][c];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const double yr = br[ty + 8 * j][c], yi = bi[ty + 8 * j][c];
+                re[j] += xr * yr + xi * yi;                 // conj(x) y
+                im[j] += xr * yi - xi * yr;
+            }
+        }
+        __syncthreads();
     }
-    exs_complex z;
-    z.re = re;
-    z.im = im;
-    dh[f + (size_t)maxaa * (f2 + (size_t)maxaa * ias)] = z;
+    const int f = fb + tx;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int f2 = f2b + ty + 8 * j;
+        if (f >= maxaa || f2 >= maxaa) continue;
+        exs_complex z;
+        z.re = re[j];
+        z.im = im[j];
+        dh[f + (size_t)maxaa * (f2 + (size_t)maxaa * ias)] = z;
+    }
 }
 
 }  // namespace exs
@@ -596,7 +625,8 @@ extern "C" int exs_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *
     if (dh) {
         const size_t n = (size_t)c->maxaa * c->maxaa * c->natmtot;
         FK_CUDA(cudaMalloc(&d_dh, sizeof(exs_complex) * n));
-        exs::fk_dh<<<dim3((c->maxaa + 63) / 64, c->maxaa, c->natmtot), 64, 0, s>>>(c->params(), fw, d_dh, c->maxaa);
+        exs::fk_dh<<<dim3((c->maxaa + 31) / 32, (c->maxaa + 31) / 32, c->natmtot), dim3(32, 8), 0, s>>>(c->params(), fw, d_dh,
+                                                                                                   c->maxaa);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(dh, d_dh, sizeof(exs_complex) * n, cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) { cudaFree(d_dh); return ffail(c, EXS_ERR_CUDA, cudaGetErrorString(e)); }
