@@ -1032,11 +1032,11 @@ def adjoint_leg(st, sys_, gk, torch, reps=3):
     """exs_adjoint (dL/dtau, dL/dV, dL/dh_a) on one k-point with the force-check
     states, wall clock of the synchronous call (uploads of the states included)."""
     c, w, eps = adjoint_recipe(sys_.nmat(gk))
-    st.adjoint(gk, c, w, eps, dveffig=True, dh=True)             # warm-up (work space)
+    out = st.adjoint(gk, c, w, eps, dveffig=True, dh=True)       # warm-up (work space, output arrays)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(reps):
-        dtau, _, _ = st.adjoint(gk, c, w, eps, dveffig=True, dh=True)
+    for _ in range(reps):                                         # the caller's arrays, as a Fortran caller passes them
+        dtau, _, _ = st.adjoint(gk, c, w, eps, dveffig=True, dh=True, out=out)
     dt = (time.perf_counter() - t0) / reps
     fl = adjoint_flops(sys_, gk, c.shape[1])
     return {"ms": dt * 1e3, "k_points_per_s": 1.0 / dt, "states": int(c.shape[1]),

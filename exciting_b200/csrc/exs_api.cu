@@ -161,6 +161,7 @@ int exs_ctx_destroy(exs_ctx *c)
     if (c->d_xsig) cudaFree(c->d_xsig);
     if (c->fk_dev) cudaFree(c->fk_dev);
     if (c->fk_tab_d) cudaFree(c->fk_tab_d);
+    if (c->fk_dh) cudaFree(c->fk_dh);
     if (c->fk_tab_h) cudaFreeHost(c->fk_tab_h);
     if (c->h_tables) cudaFreeHost(c->h_tables);
     if (c->h_igpig_pinned) cudaFreeHost(c->h_igpig_pinned);

@@ -278,6 +278,8 @@ struct exs_ctx {
     void *fk_dev = nullptr;
     size_t fk_bytes = 0;
     void *fk_tab_h = nullptr, *fk_tab_d = nullptr;
+    void *fk_dh = nullptr;                 // dL/dh_a of the adjoint (maxaa, maxaa, natmtot), kept between calls
+    size_t fk_dh_bytes = 0;
     size_t fk_tab_hbytes = 0, fk_tab_dbytes = 0;
     // precision
     int prec_mode = EXS_PREC_FP64;

@@ -242,8 +242,8 @@ __global__ void fk_terms_lo(DevParams p, ForceWork fw, const double *loa_r, cons
 __global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd, int i0, int i1)
 {
     const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= i1 || i >= fw.ngp) return;
+    const int j = i0 + blockIdx.y;                  // the band holds the columns j >= i0
+    if (i >= i1 || i >= fw.ngp || j < i) return;    // upper triangle; fk_fold_conj adds the lower one
     const int gi = kd->igpig[i] - 1, gj = kd->igpig[j] - 1;
     if (gi < 0 || gi >= p.ngrtot || gj < 0 || gj >= p.ngrtot) { atomicOr(p.err, DEV_ERR_INDEX); return; }
     const int d0 = p.ivg[3 * gi] - p.ivg[3 * gj] - p.intgv_lo[0];
@@ -258,8 +258,10 @@ __global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd, int i0, i
     if (ig <= 0 || ig > p.ngvec) return;
     const double *vi = kd->vgpc + 3 * i, *vj = kd->vgpc + 3 * j;
     const double dp = 0.5 * (vi[0] * vj[0] + vi[1] * vj[1] + vi[2] * vj[2]);
-    const size_t e = (size_t)(i - i0) * p.npad + j;
-    const double pr = fw.pt[0][e], pi = fw.pt[1][e], qr = fw.qt[0][e], qi = fw.qt[1][e];
+    const size_t e = (size_t)(i - i0) * p.npad + (j - i0);
+    // the diagonal (g = 0) is folded onto itself: half of it here, the fold doubles the real part
+    const double hf = (j == i) ? 0.5 : 1.0;
+    const double pr = hf * fw.pt[0][e], pi = hf * fw.pt[1][e], qr = hf * fw.qt[0][e], qi = hf * fw.qt[1][e];
     double *rh = reinterpret_cast<double *>(fw.rh + (ig - 1));
     double *ro = reinterpret_cast<double *>(fw.ro + (ig - 1));
     double *rv = reinterpret_cast<double *>(fw.rv + (ig - 1));
@@ -269,6 +271,40 @@ __global__ void fk_scatter(DevParams p, ForceWork fw, const KDesc *kd, int i0, i
     atomicAdd(ro + 1, qi);
     atomicAdd(rv, pr);
     atomicAdd(rv + 1, pi);
+}
+
+// P^T and Q^T are Hermitian and dp is symmetric in (i, j), so the lower
+// triangle's share of a G-vector g = G_i - G_j is the conjugate of the upper
+// triangle's share of -g: R(g) = R_up(g) + conj(R_up(-g)) for rh, ro, rv.
+// One thread per pair {g, -g} (the one with g <= -g in the list order).
+__global__ void fk_fold_conj(DevParams p, ForceWork fw)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= p.ngvec) return;
+    const int d0 = -p.ivg[3 * g] - p.intgv_lo[0], d1 = -p.ivg[3 * g + 1] - p.intgv_lo[1],
+              d2 = -p.ivg[3 * g + 2] - p.intgv_lo[2];
+    if ((unsigned)d0 >= (unsigned)p.intgv_n[0] || (unsigned)d1 >= (unsigned)p.intgv_n[1] ||
+        (unsigned)d2 >= (unsigned)p.intgv_n[2]) {
+        atomicOr(p.err, DEV_ERR_INDEX);
+        return;
+    }
+    const int ng = p.ivgig[d0 + p.intgv_n[0] * (d1 + p.intgv_n[1] * d2)] - 1;
+    if (ng < 0 || ng >= p.ngvec) {
+        atomicOr(p.err, DEV_ERR_INDEX);
+        return;
+    }
+    if (ng < g) return;                             // the partner thread does the pair
+    exs_complex *arr[3] = {fw.rh, fw.ro, fw.rv};
+    for (int k = 0; k < 3; k++) {
+        const exs_complex a = arr[k][g], b = arr[k][ng];
+        exs_complex x, y;
+        x.re = a.re + b.re;
+        x.im = a.im - b.im;
+        y.re = b.re + a.re;
+        y.im = b.im - a.im;
+        arr[k][g] = x;
+        if (ng != g) arr[k][ng] = y;
+    }
 }
 
 // Interstitial step-function terms, one block per atom, the three directions.
@@ -491,13 +527,14 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
         add_tiles(w1, (int)probs.size(), P.M, P.N, false);
         probs.push_back(P);
     }
-    for (int i0 = 0; i0 < ngp; i0 += band) {   // P^T = conj(C)^T (w C), Q^T = conj(C)^T (w eps C), rows i0..
-        wb_off.push_back(wb.size());
+    for (int i0 = 0; i0 < ngp; i0 += band) {   // P^T = conj(C)^T (w C), Q^T = conj(C)^T (w eps C): rows i0..,
+        wb_off.push_back(wb.size());             // columns j >= i0 (the scatter takes the upper triangle)
         for (int which = 0; which < 2; which++) {
             GemmProb P{};
             P.xr = fw.cn[0] + i0; P.xi = fw.cn[1] + i0; P.ldx = npad;
-            P.yr = which == 0 ? fw.wc[0] : fw.wec[0]; P.yi = which == 0 ? fw.wc[1] : fw.wec[1]; P.ldy = npad;
-            P.M = std::min(band, ngp - i0); P.N = ngp; P.K = nst; P.conjx = 1;
+            P.yr = (which == 0 ? fw.wc[0] : fw.wec[0]) + i0; P.yi = (which == 0 ? fw.wc[1] : fw.wec[1]) + i0;
+            P.ldy = npad;
+            P.M = std::min(band, ngp - i0); P.N = ngp - i0; P.K = nst; P.conjx = 1;
             P.outr = which == 0 ? fw.pt[0] : fw.qt[0]; P.outi = which == 0 ? fw.pt[1] : fw.qt[1]; P.ldo = npad;
             add_tiles(wb, (int)probs.size(), P.M, P.N, false);
             probs.push_back(P);
@@ -556,9 +593,10 @@ int run_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *vgpc, int n
         const int i0 = (int)b * band, i1 = std::min(ngp, i0 + band);
         FK_CUDA(exs::launch_gemm_kind(exs::EPI_PLANAR, p, d_p, d_wb + wb_off[b], (int)(wb_off[b + 1] - wb_off[b]),
                                       d_k, s));
-        exs::fk_scatter<<<dim3((i1 - i0 + 127) / 128, ngp), 128, 0, s>>>(p, fw, d_k, i0, i1);
+        exs::fk_scatter<<<dim3((i1 - i0 + 127) / 128, ngp - i0), 128, 0, s>>>(p, fw, d_k, i0, i1);
         FK_CUDA(cudaGetLastError());
     }
+    exs::fk_fold_conj<<<(c->ngvec + 255) / 256, 256, 0, s>>>(p, fw);
     // about two waves of blocks whatever the number of atoms, at least 2,048 G-vectors per block
     const int gsh = std::max(1, std::min((c->ngvec + 2047) / 2048, (2 * 148 * 8 + c->natmtot - 1) / c->natmtot));
     exs::fk_terms_theta<<<dim3(c->natmtot, gsh), 256, 0, s>>>(p, fw, c->ngvec);
@@ -621,18 +659,16 @@ extern "C" int exs_adjoint(exs_ctx *c, int ngp, const int *igpig, const double *
     FK_CUDA(cudaMemcpyAsync(f.data(), fw.force, sizeof(double) * f.size(), cudaMemcpyDeviceToHost, s));
     if (dveffig)
         FK_CUDA(cudaMemcpyAsync(dveffig, rv, sizeof(exs_complex) * (size_t)c->ngvec, cudaMemcpyDeviceToHost, s));
-    exs_complex *d_dh = nullptr;
-    if (dh) {
+    if (dh) {   // the work buffer stays with the context between calls
         const size_t n = (size_t)c->maxaa * c->maxaa * c->natmtot;
-        FK_CUDA(cudaMalloc(&d_dh, sizeof(exs_complex) * n));
+        FK_CUDA(grow(&c->fk_dh, &c->fk_dh_bytes, sizeof(exs_complex) * n, false));
+        exs_complex *d_dh = (exs_complex *)c->fk_dh;
         exs::fk_dh<<<dim3((c->maxaa + 31) / 32, (c->maxaa + 31) / 32, c->natmtot), dim3(32, 8), 0, s>>>(c->params(), fw, d_dh,
                                                                                                    c->maxaa);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dh, d_dh, sizeof(exs_complex) * n, cudaMemcpyDeviceToHost, s);
-        if (e != cudaSuccess) { cudaFree(d_dh); return ffail(c, EXS_ERR_CUDA, cudaGetErrorString(e)); }
+        FK_CUDA(cudaGetLastError());
+        FK_CUDA(cudaMemcpyAsync(dh, d_dh, sizeof(exs_complex) * n, cudaMemcpyDeviceToHost, s));
     }
     rc = exs_synchronize(c);
-    if (d_dh) cudaFree(d_dh);
     if (rc < 0) return rc;
     for (size_t i = 0; i < f.size(); i++) dtau[i] = -f[i];          // dL/dtau = -F_IBS
     return rc;

@@ -462,19 +462,32 @@ class Setup:
         return f
 
 
-    def adjoint(self, gk, c, w, eps, *, dveffig: bool = False, dh: bool = False):
+    def _force_inputs(self):
+        """ffacg(ngvec, nspecies) and vgc(3, ngvec): fixed for the crystal,
+        computed once (the reference's genffacg runs once per run too)."""
+        if getattr(self, "_fk_inputs", None) is None:
+            s = self.sys
+            ffacg = _f(np.stack([ffacg_species(s.gv.gc[: s.gv.ngvec], r, s.crystal.omega) for r in s.rmt], axis=1),
+                       np.float64)
+            self._fk_inputs = (ffacg, _f(s.gv.vgc[:, : s.gv.ngvec], np.float64))
+        return self._fk_inputs
+
+    def adjoint(self, gk, c, w, eps, *, dveffig: bool = False, dh: bool = False, out=None):
         """Adjoint of the setup for L = sum_n w_n c_n^H (H - eps_n O) c_n
         (exs_adjoint): (dL/dtau (3, natmtot), dL/dV (ngvec) or None,
-        dL/dh_a (maxaa, maxaa, natmtot) or None)."""
+        dL/dh_a (maxaa, maxaa, natmtot) or None).  ``out``: a tuple of such
+        arrays (as an earlier call returned them) to write into instead of
+        new ones."""
         s = self.sys
         ig, vg = self._gk_arrays(gk)
         cv = _f(c, np.complex128)
-        ffacg = _f(np.stack([ffacg_species(s.gv.gc[: s.gv.ngvec], r, s.crystal.omega) for r in s.rmt], axis=1),
-                   np.float64)
-        vgc = _f(s.gv.vgc[:, : s.gv.ngvec], np.float64)
-        dtau = np.zeros((3, s.natmtot), order="F")
-        dv = np.zeros(s.gv.ngvec, dtype=np.complex128) if dveffig else None
-        dhv = np.zeros((self.maxaa, self.maxaa, s.natmtot), dtype=np.complex128, order="F") if dh else None
+        ffacg, vgc = self._force_inputs()
+        if out is not None:
+            dtau, dv, dhv = out
+        else:
+            dtau = np.zeros((3, s.natmtot), order="F")
+            dv = np.zeros(s.gv.ngvec, dtype=np.complex128) if dveffig else None
+            dhv = np.zeros((self.maxaa, self.maxaa, s.natmtot), dtype=np.complex128, order="F") if dh else None
         self._check(self.lib.exs_adjoint(self.ctx, gk.ngp, _ptr(ig), _ptr(vg), cv.shape[1], _ptr(cv), cv.shape[0],
                                          _ptr(_f(w, np.float64)), _ptr(_f(eps, np.float64)), _ptr(ffacg),
                                          _ptr(vgc), _ptr(dtau), None if dv is None else _ptr(dv),
