@@ -12,7 +12,7 @@ rounding per element).
 The bar: the split path's lowest 40 eigenvalues within the absolute 1e-8 Ha
 of the 16-moduli pencil's.  The deviations of both FP64 computations (host
 and device) from the 16-moduli pencil, and of the split path from the
-oracle, are printed beside it.  The oracle needs about 15 minutes on 16
+oracle, are printed beside it.  The oracle needs about 30 minutes on 16
 cores and ~60 GB of host memory, so the test runs only with
 EXS_TEST_216_ORACLE=1.
 """
@@ -26,7 +26,7 @@ from exciting_b200 import workloads as W
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(os.environ.get("EXS_TEST_216_ORACLE") != "1",
-                                 reason="set EXS_TEST_216_ORACLE=1 (about 20 minutes)")]
+                                 reason="set EXS_TEST_216_ORACLE=1 (about 35 minutes)")]
 
 NEV, NX = 40, 64
 
